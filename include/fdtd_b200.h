@@ -1,0 +1,167 @@
+/*
+ * fdtd_b200.h - C ABI of the B200-native FDTD leapfrog step.
+ *
+ * This is the drop-in boundary for fdtd3d's GPU step path.  In the reference,
+ * Scheme<...> drives the step through the InternalSchemeGPU object protocol
+ * (initFromCPU / initOnGPU / copyFromCPU / copyToGPU / the *KernelLaunch
+ * methods / copyBackToCPU).  Each entry point below replaces one part of that
+ * protocol; the comment on each names the reference interface it replaces
+ * (paths relative to the fdtd3d source tree).
+ *
+ * Conventions
+ *  - Every entry returns an int status: 0 = FDTD_OK, negative = error
+ *    (fdtd_status_str gives the text).  No entry calls exit, abort or
+ *    __trap; the reference's cudaCheckError -> exit(1) and ALWAYS_ASSERT
+ *    become status codes the caller maps back.
+ *  - Arrays are x-major with z fastest, the order of the reference's
+ *    CudaGrid linear index x*sy*sz + y*sz + z (Source/Grid/CudaGrid.cu:1096)
+ *    and of its TXT dumps.  2-D TMz arrays are (x, y) with y fastest.
+ *  - Host input arrays are borrowed for the duration of the call and copied.
+ *    Output buffers are owned by the caller.
+ *  - Calls on one context are serialised by the caller; separate contexts
+ *    may live on separate host threads.
+ */
+#ifndef FDTD_B200_H
+#define FDTD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fdtd_ctx fdtd_ctx;
+
+/* status codes */
+#define FDTD_OK 0
+#define FDTD_ERR_ARG (-1)        /* invalid argument or configuration */
+#define FDTD_ERR_CUDA (-2)       /* a CUDA runtime call failed */
+#define FDTD_ERR_NOMEM (-3)      /* device or host allocation failed */
+#define FDTD_ERR_TIMEOUT (-4)    /* bounded wait ran out */
+#define FDTD_ERR_UNSUPPORTED (-5)/* mode/option combination not provided */
+#define FDTD_ERR_STATE (-6)      /* call out of order (e.g. step before setup) */
+#define FDTD_ERR_DEVICE (-7)     /* a kernel reported an error flag */
+
+/* modes (fdtd3d SchemeType) */
+#define FDTD_MODE_TMZ 2          /* Dim2_TMz: Ez, Hx, Hy */
+#define FDTD_MODE_DIM3 3         /* Dim3: Ex, Ey, Ez, Hx, Hy, Hz */
+
+/* arithmetic forms */
+#define FDTD_PREC_FP64_PLAIN 0   /* reference formulation, FP64, bit-faithful */
+#define FDTD_PREC_FP32 1         /* fused step, FP32 storage and compute */
+#define FDTD_PREC_FP16S 2        /* fused step, FP16 field storage, FP32 compute */
+
+/* field components (fdtd3d GridType order) */
+#define FDTD_EX 0
+#define FDTD_EY 1
+#define FDTD_EZ 2
+#define FDTD_HX 3
+#define FDTD_HY 4
+#define FDTD_HZ 5
+
+/* material grids (fdtd3d GridType EPS, MU, OMEGAPE, OMEGAPM, GAMMAE, GAMMAM) */
+#define FDTD_MAT_EPS 0
+#define FDTD_MAT_MU 1
+#define FDTD_MAT_OMEGAPE 2
+#define FDTD_MAT_OMEGAPM 3
+#define FDTD_MAT_GAMMAE 4
+#define FDTD_MAT_GAMMAM 5
+
+/* reductions */
+#define FDTD_REDUCE_ENERGY 0     /* sum over cells of eps*E^2 + mu*H^2 (FP64, compensated) */
+#define FDTD_REDUCE_L2 1         /* sum over cells of E^2 + H^2, per component (6 doubles) */
+
+/*
+ * Run configuration.  Mirrors fdtd3d's Settings flags (Source/Settings/Settings.inc.h):
+ * --3d/--2d-tmz, --size, --pml-size, --tfsf-size-left/right, --dx, --wavelength,
+ * --courant-factor, --angle-teta/phi/psi, --use-pml, --use-tfsf,
+ * --use-metamaterials, --point-source, --point-source-e*, --layout-type.
+ * Float flags hold the values exactly as the reference parses them
+ * (std::stof, i.e. rounded to float).
+ */
+typedef struct
+{
+  int mode;                 /* FDTD_MODE_DIM3 or FDTD_MODE_TMZ */
+  int size[3];              /* size[2] ignored for TMz */
+  int pml[3];
+  int tfsf_left[3];
+  int tfsf_right[3];
+  double dx;
+  double wavelength;
+  double courant;
+  double angle_teta;        /* degrees */
+  double angle_phi;
+  double angle_psi;
+  int use_pml;
+  int use_tfsf;
+  int use_metamaterials;    /* requires use_pml, as in the reference */
+  int point_source[3];
+  int point_source_mask;    /* bit c: hard sinusoidal source on component c */
+  int precision;            /* FDTD_PREC_* */
+  int layout;               /* 0 = E_CENTERED (the only layout provided) */
+  int reserved[8];
+} fdtd_config;
+
+/* Replaces InternalSchemeGPU::initFromCPU + initOnGPU
+ * (Source/Scheme/InternalScheme.specific.h:506-563) and the set-up half of
+ * InternalScheme::initScheme (Source/Scheme/InternalScheme.inc.h:3359-3394):
+ * computes dt, frequency, relPhaseVelocity, sigma profiles and the TF/SF
+ * geometry, and allocates device-resident SoA arrays on `device`. */
+int fdtd_create (const fdtd_config *cfg, int device, fdtd_ctx **out);
+
+/* Replaces the material half of InternalSchemeGPU::copyFromCPU/copyToGPU
+ * (InternalScheme.specific.h:200-362) for Eps, Mu, OmegaPE, OmegaPM, GammaE,
+ * GammaM.  `host` holds size-N doubles.  Unset grids keep the reference
+ * defaults (eps = mu = 1, Drude terms 0). */
+int fdtd_upload_material (fdtd_ctx *ctx, int which, const double *host);
+
+/* Sets the current time level (level 1 in the reference's Grid) of a field
+ * component from size-N host doubles; replaces copyFromCPU for Ex..Hz. */
+int fdtd_upload_field (fdtd_ctx *ctx, int component, const double *host);
+
+/* Replaces Scheme::performNStepsForBlock (Source/Scheme/Scheme.inc.h:28-473)
+ * for time steps t_start .. t_start + n_steps - 1: incident-wave steps,
+ * E and H updates with PML, Drude and TF/SF, point sources.  Asynchronous on
+ * the context's stream. */
+int fdtd_step (fdtd_ctx *ctx, uint32_t t_start, uint32_t n_steps);
+
+/* Waits for queued work.  timeout_ns < 0 waits without limit; otherwise the
+ * wait polls and returns FDTD_ERR_TIMEOUT when the limit passes (the work
+ * keeps running).  Also reports device-side error flags. */
+int fdtd_sync (fdtd_ctx *ctx, int64_t timeout_ns);
+
+/* Replaces InternalSchemeGPU::copyBackToCPU (InternalScheme.specific.h:363-504)
+ * for one component: writes the current time level (what Scheme::saveGrids
+ * dumps) as size-N doubles into caller-owned `host`.  Synchronous. */
+int fdtd_download_field (fdtd_ctx *ctx, int component, double *host);
+
+/* Device-resident variants for callers that keep their own device buffers
+ * (no host round trip): `dev` is a device pointer to size-N doubles. */
+int fdtd_upload_material_device (fdtd_ctx *ctx, int which, const double *dev);
+int fdtd_download_field_device (fdtd_ctx *ctx, int component, double *dev);
+
+/* Time-integrated / global quantities in FP64 with compensated summation
+ * (no reference counterpart; the reference's exact-norm kernel,
+ * InternalScheme.inc.h:310-348, is test-only).  `out` receives 1 double for
+ * FDTD_REDUCE_ENERGY and 6 for FDTD_REDUCE_L2. */
+int fdtd_reduce (fdtd_ctx *ctx, int what, double *out);
+
+/* Reported set-up scalars: out[0] = dt, out[1] = frequency,
+ * out[2] = relPhaseVelocity (InternalScheme.inc.h:3359-3394). */
+int fdtd_scalars (const fdtd_ctx *ctx, double out[3]);
+
+/* Number of kernel launches this context issued so far. */
+int64_t fdtd_launch_count (const fdtd_ctx *ctx);
+
+/* Releases every device resource of the context; replaces
+ * InternalSchemeGPU::uninitFromCPU/uninitOnGPU. */
+void fdtd_destroy (fdtd_ctx *ctx);
+
+const char *fdtd_status_str (int status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FDTD_B200_H */

@@ -1,0 +1,256 @@
+"""Python handle on the oracle (test infrastructure only).
+
+Two checkers live here, and nothing in the product imports this module:
+
+* ``Oracle`` wraps ``oracle/_ref/liboracle.so``, the project's plain-C
+  restatement of the fdtd3d leapfrog step (``oracle/fdtd_oracle.c``).
+* ``run_reference`` runs ``oracle/_ref/fdtd3d``, the unmodified reference CPU
+  solver compiled from its own sources by ``oracle/Makefile``, and parses the
+  ``--save-as-txt`` dumps it writes (``Source/File-Management/Dumper/TXTDumper.h``;
+  15 significant digits, z fastest).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg may use it, and only as the checker / the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes
+import glob
+import os
+import struct
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+LIB_PATH = os.path.join(REF_DIR, "liboracle.so")
+REF_BIN = os.path.join(REF_DIR, "fdtd3d")
+
+COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+MATERIALS = ("eps", "mu", "omegape", "omegapm", "gammae", "gammam")
+
+
+def f32(x: float) -> float:
+    """Round like std::stof: the reference parses float flags to float."""
+    return struct.unpack("f", struct.pack("f", float(x)))[0]
+
+
+class _Cfg(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_int),
+        ("size", ctypes.c_int * 3),
+        ("pml", ctypes.c_int * 3),
+        ("tfsf_left", ctypes.c_int * 3),
+        ("tfsf_right", ctypes.c_int * 3),
+        ("dx", ctypes.c_double),
+        ("wavelength", ctypes.c_double),
+        ("courant", ctypes.c_double),
+        ("angle_teta", ctypes.c_double),
+        ("angle_phi", ctypes.c_double),
+        ("angle_psi", ctypes.c_double),
+        ("use_pml", ctypes.c_int),
+        ("use_tfsf", ctypes.c_int),
+        ("use_metamaterials", ctypes.c_int),
+        ("point_source", ctypes.c_int * 3),
+        ("point_source_mask", ctypes.c_int),
+        ("skip_first_update", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            subprocess.run(["make", "-C", HERE, "oracle"], check=True, capture_output=True)
+        _lib = ctypes.CDLL(LIB_PATH)
+        _lib.fdtd_oracle_create.restype = ctypes.c_void_p
+        _lib.fdtd_oracle_create.argtypes = [ctypes.POINTER(_Cfg), ctypes.POINTER(ctypes.c_void_p)]
+        _lib.fdtd_oracle_destroy.argtypes = [ctypes.c_void_p]
+        _lib.fdtd_oracle_step.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]
+        _lib.fdtd_oracle_get.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        _lib.fdtd_oracle_get.restype = ctypes.c_int
+        _lib.fdtd_oracle_scalars.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        _lib.fdtd_oracle_incident.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        _lib.fdtd_oracle_exhy_1d.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_uint32,
+                                             ctypes.c_void_p, ctypes.c_void_p]
+    return _lib
+
+
+def _triple(v, default):
+    if v is None:
+        return (default,) * 3
+    if isinstance(v, int):
+        return (v, v, v)
+    return tuple(v)
+
+
+class Oracle:
+    """One simulation of the restated step; arrays are x-major, z fastest."""
+
+    def __init__(self, *, mode=3, size=(20, 20, 20), pml=None, tfsf_left=None, tfsf_right=None,
+                 dx=0.0005, wavelength=0.02, courant=0.5, teta=90.0, phi=0.0, psi=90.0,
+                 use_pml=False, use_tfsf=False, use_metamaterials=False,
+                 point_source=(0, 0, 0), point_source_mask=0, skip_first_update=True,
+                 materials=None):
+        c = _Cfg()
+        c.mode = mode
+        size = _triple(size, 1)
+        if mode == 2:
+            size = (size[0], size[1], 1)
+        c.size[:] = size
+        c.pml[:] = _triple(pml, 0)
+        c.tfsf_left[:] = _triple(tfsf_left, 0)
+        c.tfsf_right[:] = _triple(tfsf_right, 0)
+        c.dx, c.wavelength, c.courant = f32(dx), f32(wavelength), f32(courant)
+        c.angle_teta, c.angle_phi, c.angle_psi = f32(teta), f32(phi), f32(psi)
+        c.use_pml, c.use_tfsf, c.use_metamaterials = int(use_pml), int(use_tfsf), int(use_metamaterials)
+        c.point_source[:] = tuple(point_source)
+        c.point_source_mask = point_source_mask
+        c.skip_first_update = int(skip_first_update)
+        self.cfg = c
+        self.shape = (size[0], size[1], size[2]) if mode == 3 else (size[0], size[1])
+        self.n = int(np.prod(self.shape))
+        self._keep = []
+        ptrs = (ctypes.c_void_p * 6)()
+        for i, name in enumerate(MATERIALS):
+            arr = None if materials is None else materials.get(name)
+            if arr is not None:
+                a = np.ascontiguousarray(arr, dtype=np.float64).reshape(-1)
+                assert a.size == self.n
+                self._keep.append(a)
+                ptrs[i] = a.ctypes.data
+        self._h = lib().fdtd_oracle_create(ctypes.byref(c), ptrs)
+        if not self._h:
+            raise MemoryError("oracle allocation failed")
+        self.t = 0
+
+    def step(self, n: int) -> None:
+        lib().fdtd_oracle_step(self._h, self.t, n)
+        self.t += n
+
+    def field(self, comp, level: int = 1) -> np.ndarray:
+        k = COMPONENTS.index(comp) if isinstance(comp, str) else comp
+        out = np.empty(self.n, dtype=np.float64)
+        if lib().fdtd_oracle_get(self._h, k, level, out.ctypes.data) != 0:
+            raise KeyError(comp)
+        return out.reshape(self.shape)
+
+    def scalars(self):
+        out = np.empty(3, dtype=np.float64)
+        lib().fdtd_oracle_scalars(self._h, out.ctypes.data)
+        return {"dt": out[0], "frequency": out[1], "rel_phase_velocity": out[2]}
+
+    def incident(self):
+        m = 500 * self.shape[0]
+        e = np.empty(m)
+        h = np.empty(m)
+        lib().fdtd_oracle_incident(self._h, e.ctypes.data, h.ctypes.data)
+        return e, h
+
+    def close(self):
+        if self._h:
+            lib().fdtd_oracle_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def exhy_1d(size=20, tfsf=7, dx=0.002, wavelength=0.2, courant=0.5, steps=200):
+    s = np.empty(size)
+    c = np.empty(size)
+    lib().fdtd_oracle_exhy_1d(size, tfsf, dx, wavelength, courant, steps, s.ctypes.data, c.ctypes.data)
+    return s, c
+
+
+# --------------------------------------------------------------------------
+# reference binary
+
+
+def write_material_txt(path: str, arr: np.ndarray) -> None:
+    """TXT grid in the reference loader's layout: 'x y [z] value', z fastest."""
+    arr = np.asarray(arr, dtype=np.float64)
+    idx = np.indices(arr.shape).reshape(arr.ndim, -1).T
+    vals = arr.reshape(-1)
+    with open(path, "w") as f:
+        for i, v in zip(idx, vals):
+            f.write(" ".join(str(int(q)) for q in i) + " " + repr(float(v)) + "\n")
+
+
+def reference_args(*, mode=3, size=(20, 20, 20), pml=None, tfsf_left=None, tfsf_right=None,
+                   dx=0.0005, wavelength=0.02, courant=0.5, teta=90.0, phi=0.0, psi=90.0,
+                   use_pml=False, use_tfsf=False, use_metamaterials=False,
+                   point_source=(0, 0, 0), point_source_mask=0, steps=10):
+    size = _triple(size, 1)
+    ax = ("x", "y", "z") if mode == 3 else ("x", "y")
+
+    def coord(v):
+        v = _triple(v, 0)
+        return ",".join(f"{a}:{v[i]}" for i, a in enumerate(ax))
+
+    args = ["--3d" if mode == 3 else "--2d-tmz", "--size", coord(size),
+            "--dx", repr(dx), "--wavelength", repr(wavelength), "--courant-factor", repr(courant),
+            "--angle-teta", repr(teta), "--angle-phi", repr(phi), "--angle-psi", repr(psi),
+            "--time-steps", str(steps), "--use-ca-cb", "--log-level", "0"]
+    if use_pml:
+        args += ["--use-pml", "--pml-size", coord(pml), "--use-ca-cb-pml"]
+    if use_tfsf:
+        args += ["--use-tfsf", "--tfsf-size-left", coord(tfsf_left), "--tfsf-size-right", coord(tfsf_right)]
+    if use_metamaterials:
+        args += ["--use-metamaterials"]
+    if point_source_mask:
+        args += ["--point-source", coord(point_source)]
+        for k, name in enumerate(("ex", "ey", "ez", "hx", "hy", "hz")):
+            if point_source_mask & (1 << k):
+                args.append(f"--point-source-{name}")
+    return args
+
+
+def run_reference(materials=None, timeout=600, **kw):
+    """Run the reference CPU build; returns ({component: array}, total_seconds)."""
+    if not os.path.exists(REF_BIN):
+        raise FileNotFoundError(REF_BIN)
+    mode = kw.get("mode", 3)
+    size = _triple(kw.get("size", (20, 20, 20)), 1)
+    shape = size if mode == 3 else size[:2]
+    with tempfile.TemporaryDirectory() as tmp:
+        args = reference_args(**kw)
+        flags = {"eps": "--load-eps-from-file", "mu": "--load-mu-from-file",
+                 "omegape": "--load-omegape-from-file", "omegapm": "--load-omegapm-from-file",
+                 "gammae": "--load-gammae-from-file", "gammam": "--load-gammam-from-file"}
+        for name, arr in (materials or {}).items():
+            p = os.path.join(tmp, f"{name}.txt")
+            write_material_txt(p, np.asarray(arr).reshape(shape))
+            args += [flags[name], p]
+        ax = ("x", "y", "z") if mode == 3 else ("x", "y")
+        end = ",".join(f"{a}:{size[i]}" for i, a in enumerate(ax))
+        start = ",".join(f"{a}:0" for a in ax)
+        args += ["--save-res", "--save-as-txt", "--manual-save-coords",
+                 "--save-start-coord", start, "--save-end-coord", end]
+        r = subprocess.run([REF_BIN] + args, cwd=tmp, capture_output=True, text=True, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference failed ({r.returncode}): {r.stdout[-2000:]} {r.stderr[-2000:]}")
+        total = None
+        for line in r.stdout.splitlines():
+            if line.startswith("Total time = "):
+                total = float(line.split("=")[1].split()[0])
+        out = {}
+        for comp in COMPONENTS:
+            files = glob.glob(os.path.join(tmp, f"previous-1_*_[[]name={comp}].txt"))
+            if not files:
+                continue
+            data = np.loadtxt(files[0]).reshape(-1, len(shape) + 1)
+            arr = np.zeros(shape)
+            idx = tuple(data[:, i].astype(int) for i in range(len(shape)))
+            arr[idx] = data[:, -1]
+            out[comp] = arr
+        return out, total
