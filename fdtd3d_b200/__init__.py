@@ -1,0 +1,232 @@
+"""fdtd3d_b200 - B200-native FDTD leapfrog step behind a C ABI.
+
+The product is ``libfdtd_b200.so`` (built in-tree from ``csrc/`` by
+``fdtd3d_b200.build``) exporting the functions declared in
+``include/fdtd_b200.h``.  This module is a thin ctypes binding over that
+library, used by the tests and ``bench.py``.  There is no CPU fallback: every
+compute call goes to the CUDA library, and loading fails loudly when the
+library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import struct
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfdtd_b200.so")
+
+MODE_TMZ = 2
+MODE_DIM3 = 3
+PREC_FP64_PLAIN = 0
+PREC_FP32 = 1
+PREC_FP16S = 2
+COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+MATERIALS = ("eps", "mu", "omegape", "omegapm", "gammae", "gammam")
+REDUCE_ENERGY = 0
+REDUCE_L2 = 1
+
+EXPORTED = (
+    "fdtd_create", "fdtd_upload_material", "fdtd_upload_field", "fdtd_step", "fdtd_sync",
+    "fdtd_download_field", "fdtd_upload_material_device", "fdtd_download_field_device",
+    "fdtd_reduce", "fdtd_scalars", "fdtd_launch_count", "fdtd_destroy", "fdtd_status_str",
+    "fdtd_last_error",
+)
+
+
+class FdtdError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        super().__init__(f"{where}: status {status} ({detail})")
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_int),
+        ("size", ctypes.c_int * 3),
+        ("pml", ctypes.c_int * 3),
+        ("tfsf_left", ctypes.c_int * 3),
+        ("tfsf_right", ctypes.c_int * 3),
+        ("dx", ctypes.c_double),
+        ("wavelength", ctypes.c_double),
+        ("courant", ctypes.c_double),
+        ("angle_teta", ctypes.c_double),
+        ("angle_phi", ctypes.c_double),
+        ("angle_psi", ctypes.c_double),
+        ("use_pml", ctypes.c_int),
+        ("use_tfsf", ctypes.c_int),
+        ("use_metamaterials", ctypes.c_int),
+        ("point_source", ctypes.c_int * 3),
+        ("point_source_mask", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("layout", ctypes.c_int),
+        ("reserved", ctypes.c_int * 8),
+    ]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads the CUDA library; raises if it is absent (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python -m fdtd3d_b200.build`")
+    lib = ctypes.CDLL(path)
+    vp, i, d, u32, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_uint32, ctypes.c_int64
+    sig = {
+        "fdtd_create": ([ctypes.POINTER(Config), i, ctypes.POINTER(vp)], i),
+        "fdtd_upload_material": ([vp, i, vp], i),
+        "fdtd_upload_field": ([vp, i, vp], i),
+        "fdtd_step": ([vp, u32, u32], i),
+        "fdtd_sync": ([vp, i64], i),
+        "fdtd_download_field": ([vp, i, vp], i),
+        "fdtd_upload_material_device": ([vp, i, vp], i),
+        "fdtd_download_field_device": ([vp, i, vp], i),
+        "fdtd_reduce": ([vp, i, vp], i),
+        "fdtd_scalars": ([vp, vp], i),
+        "fdtd_launch_count": ([vp], i64),
+        "fdtd_destroy": ([vp], None),
+        "fdtd_status_str": ([i], ctypes.c_char_p),
+        "fdtd_last_error": ([], ctypes.c_char_p),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def f32(x: float) -> float:
+    """Rounds like std::stof: the reference parses its float flags to float."""
+    return struct.unpack("f", struct.pack("f", float(x)))[0]
+
+
+def _triple(v, default):
+    if v is None:
+        return (default,) * 3
+    if isinstance(v, (int, np.integer)):
+        return (int(v),) * 3
+    v = tuple(int(a) for a in v)
+    return v + (default,) * (3 - len(v))
+
+
+def make_config(*, mode=MODE_DIM3, size=(20, 20, 20), pml=None, tfsf_left=None, tfsf_right=None,
+                dx=0.0005, wavelength=0.02, courant=0.5, teta=90.0, phi=0.0, psi=90.0,
+                use_pml=False, use_tfsf=False, use_metamaterials=False,
+                point_source=(0, 0, 0), point_source_mask=0, precision=PREC_FP64_PLAIN) -> Config:
+    c = Config()
+    c.mode = mode
+    c.size[:] = _triple(size, 1)
+    c.pml[:] = _triple(pml, 0)
+    c.tfsf_left[:] = _triple(tfsf_left, 0)
+    c.tfsf_right[:] = _triple(tfsf_right, 0)
+    c.dx, c.wavelength, c.courant = f32(dx), f32(wavelength), f32(courant)
+    c.angle_teta, c.angle_phi, c.angle_psi = f32(teta), f32(phi), f32(psi)
+    c.use_pml, c.use_tfsf, c.use_metamaterials = int(use_pml), int(use_tfsf), int(use_metamaterials)
+    c.point_source[:] = _triple(point_source, 0)
+    c.point_source_mask = int(point_source_mask)
+    c.precision = int(precision)
+    c.layout = 0
+    return c
+
+
+class Simulation:
+    """One device-resident simulation (one fdtd_ctx), fdtd3d E_CENTERED layout.
+
+    Arrays are x-major with z fastest (3-D) or (x, y) with y fastest (TMz),
+    the reference's CudaGrid linear order.  ``step`` is asynchronous; reads
+    synchronise.
+    """
+
+    def __init__(self, device: int = 0, materials=None, **cfg):
+        self.lib = load_library()
+        self.cfg = make_config(**cfg)
+        self.mode = self.cfg.mode
+        size = tuple(self.cfg.size)
+        self.shape = size if self.mode == MODE_DIM3 else size[:2]
+        self.cells = int(np.prod(self.shape))
+        h = ctypes.c_void_p()
+        self._check(self.lib.fdtd_create(ctypes.byref(self.cfg), device, ctypes.byref(h)), "fdtd_create")
+        self._h = h
+        self.t = 0
+        for name, arr in (materials or {}).items():
+            self.set_material(name, arr)
+
+    def _check(self, st: int, where: str) -> None:
+        if st != 0:
+            detail = (self.lib.fdtd_last_error() or b"").decode()
+            raise FdtdError(st, where, detail or (self.lib.fdtd_status_str(st) or b"").decode())
+
+    def set_material(self, name: str, arr) -> None:
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(-1)
+        if a.size != self.cells:
+            raise ValueError("material array size does not match the grid")
+        self._check(self.lib.fdtd_upload_material(self._h, MATERIALS.index(name), a.ctypes.data), "upload_material")
+
+    def set_material_device(self, name: str, dev_ptr: int) -> None:
+        self._check(self.lib.fdtd_upload_material_device(self._h, MATERIALS.index(name), dev_ptr),
+                    "upload_material_device")
+
+    def set_field(self, comp, arr) -> None:
+        k = COMPONENTS.index(comp) if isinstance(comp, str) else comp
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(-1)
+        self._check(self.lib.fdtd_upload_field(self._h, k, a.ctypes.data), "upload_field")
+
+    def step(self, n: int, t_start: int | None = None) -> None:
+        t0 = self.t if t_start is None else t_start
+        self._check(self.lib.fdtd_step(self._h, t0, n), "fdtd_step")
+        self.t = t0 + n
+
+    def sync(self, timeout_ns: int = -1) -> None:
+        self._check(self.lib.fdtd_sync(self._h, timeout_ns), "fdtd_sync")
+
+    def field(self, comp, out: np.ndarray | None = None) -> np.ndarray:
+        k = COMPONENTS.index(comp) if isinstance(comp, str) else comp
+        if out is None:
+            out = np.empty(self.cells, dtype=np.float64)
+        self._check(self.lib.fdtd_download_field(self._h, k, out.ctypes.data), "download_field")
+        return out.reshape(self.shape)
+
+    def field_device(self, comp, dev_ptr: int) -> None:
+        k = COMPONENTS.index(comp) if isinstance(comp, str) else comp
+        self._check(self.lib.fdtd_download_field_device(self._h, k, dev_ptr), "download_field_device")
+
+    def reduce(self, what: int = REDUCE_ENERGY) -> np.ndarray:
+        out = np.zeros(6, dtype=np.float64)
+        self._check(self.lib.fdtd_reduce(self._h, what, out.ctypes.data), "fdtd_reduce")
+        return out[:1] if what == REDUCE_ENERGY else out
+
+    def scalars(self) -> dict:
+        out = np.empty(3)
+        self._check(self.lib.fdtd_scalars(self._h, out.ctypes.data), "fdtd_scalars")
+        return {"dt": out[0], "frequency": out[1], "rel_phase_velocity": out[2]}
+
+    def launch_count(self) -> int:
+        return int(self.lib.fdtd_launch_count(self._h))
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.lib.fdtd_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,392 @@
+// fast_kernels.cu - FP32 / FP16-storage form of the fdtd3d step, plus the
+// conversion and reduction kernels.
+//
+// Formulation (algebraically the reference's, re-scaled and with the PML
+// auxiliary fields kept only where sigma != 0):
+//   H is stored as H' = eta0 * H, so with S = c*dt/dx every update reads
+//     interior cells:  F += S / m * curl
+//     PML cells:       X_new = ca1 * X + S * q1 * curl
+//                      F     = p5 * F + (g4p * X_new - g4m * X) * q5 / m
+//   where m is the averaged eps (E) or mu (H), X = D/eps0 or c*B, and the
+//   1-D tables come from the reference's sigma profiles
+//   (Source/Scheme/InternalScheme.inc.h:2297-2349, 2551-2640; the PML
+//   coefficients of H use eps0 as in the reference).  In interior cells the
+//   reference's D/B chain with sigma = 0 reduces exactly to the first line.
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+
+namespace fdtdb {
+
+namespace {
+
+template <typename T>
+__device__ __forceinline__ float ld (const T *p, size_t i);
+template <>
+__device__ __forceinline__ float ld<float> (const float *p, size_t i)
+{
+  return p[i];
+}
+template <>
+__device__ __forceinline__ float ld<__half> (const __half *p, size_t i)
+{
+  return __half2float (p[i]);
+}
+
+template <typename T>
+__device__ __forceinline__ void st (T *p, size_t i, float v);
+template <>
+__device__ __forceinline__ void st<float> (float *p, size_t i, float v)
+{
+  p[i] = v;
+}
+template <>
+__device__ __forceinline__ void st<__half> (__half *p, size_t i, float v)
+{
+  p[i] = __float2half_rn (v);
+}
+
+__device__ __forceinline__ size_t flin (const GeomDev &g, int x, int y, int z)
+{
+  return ((size_t) x * g.n[1] + y) * g.n[2] + z;
+}
+
+// incident value in FP64 (1-D grid is FP64 in every form)
+__device__ __forceinline__ double fast_incident (const GeomDev &g, const double *inc, int inc_len, int *err, int k,
+                                                 int px, int py, int pz)
+{
+  double d_diff = k >= 3 ? 0.5 : 0.0;
+  double x = ((double) px + g.min_fp[k][0]) - g.zero_inc[0];
+  double y = ((double) py + g.min_fp[k][1]) - g.zero_inc[1];
+  double d;
+  if (!g.tmz)
+  {
+    double z = ((double) pz + g.min_fp[k][2]) - g.zero_inc[2];
+    d = x * g.s1 * g.c2 + y * g.s1 * g.s2 + z * g.c1 - d_diff;
+  }
+  else
+  {
+    d = x * g.c2 + y * g.s2 - d_diff;
+  }
+  int i1 = (int) d;
+  double pr2 = d - (double) i1;
+  if (i1 < 0 || i1 + 1 >= inc_len)
+  {
+    if (err)
+      *err = 1;
+    return 0.0;
+  }
+  return (inc[i1] * (1 - pr2) + inc[i1 + 1] * pr2) * g.proj[k];
+}
+
+template <typename T>
+__device__ __forceinline__ void fast_component (const FastHalf &p, int ci, int *err, int x, int y, int z)
+{
+  const GeomDev &g = p.g;
+  const CompDev &c = p.comp[ci];
+  const size_t id = flin (g, x, y, z);
+  T *F = (T *) p.f[ci];
+  const T *o1 = (const T *) p.opp[c.opp1];
+  const T *o2 = (const T *) p.opp[c.opp2];
+  float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
+  if (o1)
+  {
+    v0 = ld (o1, flin (g, x + c.d11[0], y + c.d11[1], z + c.d11[2]));
+    v1 = ld (o1, flin (g, x + c.d12[0], y + c.d12[1], z + c.d12[2]));
+  }
+  if (o2)
+  {
+    v2 = ld (o2, flin (g, x + c.d21[0], y + c.d21[1], z + c.d21[2]));
+    v3 = ld (o2, flin (g, x + c.d22[0], y + c.d22[1], z + c.d22[2]));
+  }
+  if (p.use_tfsf)
+  {
+    for (int t = 0; t < c.nterms; ++t)
+    {
+      const TermDev &tm = c.term[t];
+      if (x >= tm.lo[0] && x < tm.hi[0] && y >= tm.lo[1] && y < tm.hi[1] && z >= tm.lo[2] && z < tm.hi[2])
+      {
+        double diff = fast_incident (g, p.inc, p.inc_len, err, tm.inc_comp, x + tm.aux[0], y + tm.aux[1],
+                                     z + tm.aux[2]);
+        float dv = (float) (diff * tm.negate) * p.inc_scale[tm.inc_comp];
+        if (tm.slot == 0)
+          v0 -= dv;
+        else if (tm.slot == 1)
+          v1 -= dv;
+        else if (tm.slot == 2)
+          v2 -= dv;
+        else
+          v3 -= dv;
+      }
+    }
+  }
+  const float curl = (v1 - v0) - (v3 - v2);
+
+  float inv_m = 1.f;
+  if (p.mat)
+  {
+    float m;
+    if (c.nmat == 2)
+      m = 0.5f * (p.mat[flin (g, x, y, z)] + p.mat[flin (g, x + c.m[1][0], y + c.m[1][1], z + c.m[1][2])]);
+    else
+      m = 0.25f * (p.mat[flin (g, x, y, z)] + p.mat[flin (g, x + c.m[1][0], y + c.m[1][1], z + c.m[1][2])]
+                   + p.mat[flin (g, x + c.m[2][0], y + c.m[2][1], z + c.m[2][2])]
+                   + p.mat[flin (g, x + c.m[3][0], y + c.m[3][1], z + c.m[3][2])]);
+    inv_m = 1.f / m;
+  }
+
+  const int pos[3] = {x, y, z};
+  bool interior = true;
+  if (p.use_pml)
+  {
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+      interior = interior && pos[a] >= p.ilo[ci][a] && pos[a] < p.ihi[ci][a];
+  }
+  float f = ld (F, id);
+  if (interior)
+  {
+    f += p.courant * inv_m * curl;
+  }
+  else
+  {
+    const int a0 = c.sig4, a1 = c.sig_cacb, a2 = c.sig5;
+    const float ca1 = p.tab[ci][0][pos[a1]];
+    const float sq1 = p.tab[ci][1][pos[a1]];
+    const float p5 = p.tab[ci][2][pos[a2]];
+    const float q5 = p.tab[ci][3][pos[a2]];
+    const float g4p = p.tab[ci][4][pos[a0]];
+    const float g4m = p.tab[ci][5][pos[a0]];
+    float *X = p.aux[ci];
+    const float xo = X[id];
+    const float xn = ca1 * xo + sq1 * curl;
+    X[id] = xn;
+    f = p5 * f + (g4p * xn - g4m * xo) * q5 * inv_m;
+  }
+  st (F, id, f);
+}
+
+template <typename T>
+__global__ void __launch_bounds__ (256) fast_half_kernel (FastHalf p, int *err)
+{
+  const int ix = p.g.n[0] - 2;
+  const int iy = p.g.n[1] - 2;
+  const int iz = p.g.tmz ? 1 : p.g.n[2] - 2;
+  const int64_t total = (int64_t) ix * iy * iz;
+  for (int64_t tid = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; tid < total;
+       tid += (int64_t) gridDim.x * blockDim.x)
+  {
+    int z = (int) (tid % iz);
+    int64_t r = tid / iz;
+    int y = (int) (r % iy) + 1;
+    int x = (int) (r / iy) + 1;
+    if (!p.g.tmz)
+      z += 1;
+#pragma unroll 1
+    for (int ci = 0; ci < 3; ++ci)
+    {
+      if (p.comp[ci].exists)
+        fast_component<T> (p, ci, err, x, y, z);
+    }
+  }
+}
+
+template <typename T>
+__global__ void fast_point_source_kernel (T *f, size_t index, const double *src, int src_index, float scale)
+{
+  if (threadIdx.x == 0 && blockIdx.x == 0)
+    st (f, index, (float) src[src_index] * scale);
+}
+
+template <typename T>
+__global__ void convert_in_kernel (T *dst, const double *src, size_t n, double scale)
+{
+  for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
+    st (dst, i, (float) (src[i] * scale));
+}
+
+__global__ void convert_in_double_kernel (double *dst, const double *src, size_t n, double scale)
+{
+  for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
+    dst[i] = src[i] * scale;
+}
+
+template <typename T>
+__global__ void convert_out_kernel (double *dst, const T *src, size_t n, double scale)
+{
+  for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
+    dst[i] = (double) ld (src, i) * scale;
+}
+
+__global__ void convert_out_double_kernel (double *dst, const double *src, size_t n, double scale)
+{
+  for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
+    dst[i] = src[i] * scale;
+}
+
+// Neumaier (compensated) accumulation in FP64
+__device__ __forceinline__ void neumaier (double &s, double &c, double v)
+{
+  double t = s + v;
+  if (fabs (s) >= fabs (v))
+    c += (s - t) + v;
+  else
+    c += (v - t) + s;
+  s = t;
+}
+
+template <typename T>
+__device__ __forceinline__ double ldd (const void *p, size_t i)
+{
+  return (double) ld ((const T *) p, i);
+}
+
+template <int KIND>
+__global__ void __launch_bounds__ (256) reduce_sq_kernel (const void *src, size_t n, const void *weight,
+                                                          int wkind, double scale, double *partials)
+{
+  double s = 0.0, c = 0.0;
+  for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
+  {
+    double v;
+    if (KIND == 0)
+      v = ((const double *) src)[i];
+    else if (KIND == 1)
+      v = ldd<float> (src, i);
+    else
+      v = ldd<__half> (src, i);
+    double w = 1.0;
+    if (wkind == 1)
+      w = (double) ((const float *) weight)[i];
+    else if (wkind == 2)
+      w = ((const double *) weight)[i];
+    neumaier (s, c, w * v * v * scale);
+  }
+  __shared__ double ss[256];
+  __shared__ double sc[256];
+  ss[threadIdx.x] = s;
+  sc[threadIdx.x] = c;
+  __syncthreads ();
+  if (threadIdx.x == 0)
+  {
+    double bs = 0.0, bc = 0.0;
+    for (int i = 0; i < blockDim.x; ++i)
+    {
+      neumaier (bs, bc, ss[i]);
+      bc += sc[i];
+    }
+    partials[2 * blockIdx.x] = bs;
+    partials[2 * blockIdx.x + 1] = bc;
+  }
+}
+
+__global__ void reduce_final_kernel (const double *partials, int nblocks, double *out)
+{
+  if (threadIdx.x == 0 && blockIdx.x == 0)
+  {
+    double s = 0.0, c = 0.0;
+    for (int i = 0; i < nblocks; ++i)
+    {
+      neumaier (s, c, partials[2 * i]);
+      c += partials[2 * i + 1];
+    }
+    out[0] = s + c;
+  }
+}
+
+int grid_for (size_t n, int sm_count)
+{
+  size_t b = (n + 255) / 256;
+  size_t cap = (size_t) sm_count * 16;
+  if (b > cap)
+    b = cap;
+  return b < 1 ? 1 : (int) b;
+}
+
+}  // namespace
+
+int launch_fast_half (const FastHalf &p, int *err, int sm_count, cudaStream_t s)
+{
+  const int ix = p.g.n[0] - 2;
+  const int iy = p.g.n[1] - 2;
+  const int iz = p.g.tmz ? 1 : p.g.n[2] - 2;
+  int64_t total = (int64_t) ix * iy * iz;
+  int64_t blocks = (total + 255) / 256;
+  int64_t cap = (int64_t) sm_count * 8 * 16;
+  if (blocks > cap)
+    blocks = cap;
+  if (blocks < 1)
+    blocks = 1;
+  if (p.fp16)
+    fast_half_kernel<__half><<<(unsigned) blocks, 256, 0, s>>> (p, err);
+  else
+    fast_half_kernel<float><<<(unsigned) blocks, 256, 0, s>>> (p, err);
+  return 1;
+}
+
+int launch_fast_point_source (void *f, int fp16, size_t index, const double *src, int src_index, float scale,
+                              cudaStream_t s)
+{
+  if (fp16)
+    fast_point_source_kernel<__half><<<1, 32, 0, s>>> ((__half *) f, index, src, src_index, scale);
+  else
+    fast_point_source_kernel<float><<<1, 32, 0, s>>> ((float *) f, index, src, src_index, scale);
+  return 1;
+}
+
+int launch_convert_in (void *dst, int dst_kind, const double *src, size_t n, double scale, cudaStream_t s)
+{
+  int blocks = grid_for (n, 148);
+  if (dst_kind == 0)
+    convert_in_double_kernel<<<blocks, 256, 0, s>>> ((double *) dst, src, n, scale);
+  else if (dst_kind == 1)
+    convert_in_kernel<float><<<blocks, 256, 0, s>>> ((float *) dst, src, n, scale);
+  else
+    convert_in_kernel<__half><<<blocks, 256, 0, s>>> ((__half *) dst, src, n, scale);
+  return 1;
+}
+
+int launch_convert_out (double *dst, const void *src, int src_kind, size_t n, double scale, cudaStream_t s)
+{
+  int blocks = grid_for (n, 148);
+  if (src_kind == 0)
+    convert_out_double_kernel<<<blocks, 256, 0, s>>> (dst, (const double *) src, n, scale);
+  else if (src_kind == 1)
+    convert_out_kernel<float><<<blocks, 256, 0, s>>> (dst, (const float *) src, n, scale);
+  else
+    convert_out_kernel<__half><<<blocks, 256, 0, s>>> (dst, (const __half *) src, n, scale);
+  return 1;
+}
+
+int launch_reduce_sq (const void *src, int kind, size_t n, const void *weight, int wkind, double scale,
+                      double *partials, int nblocks, cudaStream_t s)
+{
+  if (kind == 0)
+    reduce_sq_kernel<0><<<nblocks, 256, 0, s>>> (src, n, weight, wkind, scale, partials);
+  else if (kind == 1)
+    reduce_sq_kernel<1><<<nblocks, 256, 0, s>>> (src, n, weight, wkind, scale, partials);
+  else
+    reduce_sq_kernel<2><<<nblocks, 256, 0, s>>> (src, n, weight, wkind, scale, partials);
+  return 1;
+}
+
+__global__ void fill_kernel (double *dst, size_t n, double value)
+{
+  for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
+    dst[i] = value;
+}
+
+int launch_fill (double *dst, size_t n, double value, cudaStream_t s)
+{
+  fill_kernel<<<grid_for (n, 148), 256, 0, s>>> (dst, n, value);
+  return 1;
+}
+
+int launch_reduce_final (const double *partials, int nblocks, double *out, cudaStream_t s)
+{
+  reduce_final_kernel<<<1, 32, 0, s>>> (partials, nblocks, out);
+  return 1;
+}
+
+}  // namespace fdtdb

@@ -1,0 +1,893 @@
+// fdtd_api.cu - the C ABI (include/fdtd_b200.h): context, device memory,
+// uploads/downloads and the per-time-step launch sequence.
+//
+// The step sequence mirrors Scheme::performNStepsForBlock
+// (Source/Scheme/Scheme.inc.h:28-473): incident E step, E half-step (skipped
+// at t == 0, Scheme.inc.h:1032), E point sources, incident H step, H
+// half-step, H point sources.  Time levels of the plain form rotate as
+// pointers on the host (Grid::shiftInTime, Source/Grid/Grid.h:1304-1319);
+// the fused forms update in place.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/fdtd_b200.h"
+#include "kernels.h"
+#include "setup.h"
+
+using namespace fdtdb;
+
+namespace {
+
+constexpr double kEta0 = 376.730313461770655;  // sqrt(mu0/eps0) for the reference constants
+
+thread_local std::string g_last_error;
+
+int kind_of (int prec)
+{
+  return prec == FDTD_PREC_FP64_PLAIN ? 0 : (prec == FDTD_PREC_FP32 ? 1 : 2);
+}
+
+size_t elem_size (int kind)
+{
+  return kind == 0 ? 8 : (kind == 1 ? 4 : 2);
+}
+
+}  // namespace
+
+struct fdtd_ctx
+{
+  Geometry g;
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  int prec = 0;
+  int kind = 0;
+  int64_t launches = 0;
+  int *d_err = nullptr;
+  double eta0 = 1.0;
+
+  // incident grids (FP64 in every form); cur = index of level 1
+  double *einc[2] = {nullptr, nullptr};
+  double *hinc[2] = {nullptr, nullptr};
+  int ecur = 0, hcur = 0;
+
+  // per-step source table: [incident, point source E, point source H]
+  double *d_src = nullptr;
+  double *h_src = nullptr;
+  size_t src_cap = 0;
+  cudaEvent_t src_ev = nullptr;
+
+  // plain form
+  double *f[6][3] = {};
+  double *dd[6][3] = {};
+  double *d1[6][3] = {};
+  double *mat64[6] = {};
+  double *sig64[3] = {};
+
+  // fused forms
+  void *ff[6] = {};
+  float *aux[6] = {};
+  float *mat32[2] = {};
+  float *tabs = nullptr;
+  size_t tab_off[6][6] = {};
+  FastHalf fast_e, fast_h;
+
+  double *staging = nullptr;
+  double *partials = nullptr;
+  double *d_out = nullptr;
+  int nparts = 0;
+
+  std::vector<void *> allocs;
+};
+
+namespace {
+
+int fail (fdtd_ctx *ctx, int code, const std::string &msg)
+{
+  (void) ctx;
+  g_last_error = msg;
+  return code;
+}
+
+#define CK(call)                                                                                   \
+  do                                                                                               \
+  {                                                                                                \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      return fail (ctx, e_ == cudaErrorMemoryAllocation ? FDTD_ERR_NOMEM : FDTD_ERR_CUDA,          \
+                   std::string (#call) + ": " + cudaGetErrorString (e_));                           \
+  } while (0)
+
+int dalloc (fdtd_ctx *ctx, void **p, size_t bytes, bool zero = true)
+{
+  cudaError_t e = cudaMalloc (p, bytes ? bytes : 16);
+  if (e != cudaSuccess)
+  {
+    *p = nullptr;
+    return fail (ctx, FDTD_ERR_NOMEM, std::string ("cudaMalloc: ") + cudaGetErrorString (e));
+  }
+  ctx->allocs.push_back (*p);
+  if (zero)
+  {
+    e = cudaMemsetAsync (*p, 0, bytes ? bytes : 16, ctx->stream);
+    if (e != cudaSuccess)
+      return fail (ctx, FDTD_ERR_CUDA, std::string ("cudaMemset: ") + cudaGetErrorString (e));
+  }
+  return FDTD_OK;
+}
+
+#define DALLOC(ptr, bytes)                                                                         \
+  do                                                                                               \
+  {                                                                                                \
+    int r_ = dalloc (ctx, (void **) &(ptr), (bytes));                                              \
+    if (r_ != FDTD_OK)                                                                             \
+      return r_;                                                                                   \
+  } while (0)
+
+GeomDev make_geom_dev (const Geometry &g)
+{
+  GeomDev d;
+  std::memset (&d, 0, sizeof (d));
+  for (int a = 0; a < 3; ++a)
+    d.n[a] = g.n[a];
+  d.tmz = g.tmz ? 1 : 0;
+  d.dt = g.dt;
+  d.dx = g.dx;
+  d.s1 = g.s1;
+  d.c1 = g.c1;
+  d.s2 = g.s2;
+  d.c2 = g.c2;
+  for (int a = 0; a < 3; ++a)
+    d.zero_inc[a] = g.zero_inc[a];
+  for (int k = 0; k < 6; ++k)
+  {
+    d.proj[k] = g.proj[k];
+    for (int a = 0; a < 3; ++a)
+      d.min_fp[k][a] = g.comp[k].min_fp[a];
+  }
+  return d;
+}
+
+CompDev make_comp_dev (const Geometry &g, int k)
+{
+  CompDev c;
+  std::memset (&c, 0, sizeof (c));
+  const CompLayout &l = g.comp[k];
+  c.exists = l.exists ? 1 : 0;
+  int base = k >= 3 ? 0 : 3;
+  c.opp1 = l.opp1 - base;
+  c.opp2 = l.opp2 - base;
+  for (int a = 0; a < 3; ++a)
+  {
+    c.d11[a] = l.d11[a];
+    c.d12[a] = l.d12[a];
+    c.d21[a] = l.d21[a];
+    c.d22[a] = l.d22[a];
+  }
+  c.sig_cacb = l.sig_cacb;
+  c.sig4 = l.sig4;
+  c.sig5 = l.sig5;
+  c.nmat = l.nmat;
+  for (int j = 0; j < 4; ++j)
+    for (int a = 0; a < 3; ++a)
+      c.m[j][a] = l.m[j][a];
+  c.nterms = 0;
+  for (const TfsfTerm &t : g.tfsf)
+  {
+    if (t.comp != k || c.nterms >= kMaxTerms)
+      continue;
+    TermDev &d = c.term[c.nterms++];
+    for (int a = 0; a < 3; ++a)
+    {
+      d.lo[a] = t.lo[a];
+      d.hi[a] = t.hi[a];
+      d.aux[a] = t.aux[a];
+    }
+    d.slot = t.slot;
+    d.inc_comp = t.inc_comp;
+    d.negate = t.negate;
+  }
+  return c;
+}
+
+// sigma profile of axis b averaged at the position of component k
+std::vector<double> sigma_at (const Geometry &g, int k, int b)
+{
+  const std::vector<double> &s = g.sigma[b];
+  int n = g.n[b];
+  std::vector<double> out (n, 0.0);
+  int a = k % 3;
+  bool isH = k >= 3;
+  bool averaged = isH ? (b != a) : (b == a);
+  if (g.tmz && b == 2)
+    averaged = false;
+  for (int i = 0; i < n; ++i)
+    out[i] = (averaged && i + 1 < n) ? (s[i] + s[i + 1]) / 2.0 : s[i];
+  return out;
+}
+
+}  // namespace
+
+namespace {
+
+int set_device (fdtd_ctx *ctx)
+{
+  CK (cudaSetDevice (ctx->device));
+  return FDTD_OK;
+}
+
+int ensure_staging (fdtd_ctx *ctx)
+{
+  if (!ctx->staging)
+    DALLOC (ctx->staging, (size_t) ctx->g.cells * sizeof (double));
+  return FDTD_OK;
+}
+
+int ensure_src (fdtd_ctx *ctx, size_t steps)
+{
+  if (steps > ctx->src_cap)
+  {
+    CK (cudaStreamSynchronize (ctx->stream));
+    if (ctx->d_src)
+    {
+      auto it = std::find (ctx->allocs.begin (), ctx->allocs.end (), (void *) ctx->d_src);
+      if (it != ctx->allocs.end ())
+        ctx->allocs.erase (it);
+      cudaFree (ctx->d_src);
+      ctx->d_src = nullptr;
+    }
+    if (ctx->h_src)
+    {
+      cudaFreeHost (ctx->h_src);
+      ctx->h_src = nullptr;
+    }
+    size_t cap = std::max<size_t> (steps, 1024);
+    DALLOC (ctx->d_src, cap * 3 * sizeof (double));
+    CK (cudaMallocHost ((void **) &ctx->h_src, cap * 3 * sizeof (double)));
+    ctx->src_cap = cap;
+  }
+  else
+  {
+    CK (cudaEventSynchronize (ctx->src_ev));
+  }
+  return FDTD_OK;
+}
+
+int alloc_plain (fdtd_ctx *ctx)
+{
+  const Geometry &g = ctx->g;
+  size_t nb = (size_t) g.cells * sizeof (double);
+  for (int k = 0; k < 6; ++k)
+  {
+    if (!g.comp[k].exists)
+      continue;
+    for (int l = 0; l < g.levels; ++l)
+    {
+      DALLOC (ctx->f[k][l], nb);
+      if (g.cfg.use_pml)
+        DALLOC (ctx->dd[k][l], nb);
+      if (g.cfg.use_metamaterials)
+        DALLOC (ctx->d1[k][l], nb);
+    }
+  }
+  int nmat = g.cfg.use_metamaterials ? 6 : 2;
+  for (int m = 0; m < nmat; ++m)
+  {
+    DALLOC (ctx->mat64[m], nb);
+    if (m < 2)
+      ctx->launches += launch_fill (ctx->mat64[m], (size_t) g.cells, 1.0, ctx->stream);
+  }
+  for (int a = 0; a < 3; ++a)
+  {
+    DALLOC (ctx->sig64[a], g.sigma[a].size () * sizeof (double));
+    CK (cudaMemcpyAsync (ctx->sig64[a], g.sigma[a].data (), g.sigma[a].size () * sizeof (double),
+                         cudaMemcpyHostToDevice, ctx->stream));
+  }
+  CK (cudaStreamSynchronize (ctx->stream));
+  return FDTD_OK;
+}
+
+int alloc_fast (fdtd_ctx *ctx)
+{
+  const Geometry &g = ctx->g;
+  size_t n = (size_t) g.cells;
+  if (g.cfg.use_metamaterials)
+    return fail (ctx, FDTD_ERR_UNSUPPORTED, "metamaterials are provided by the FP64 plain form only");
+  for (int k = 0; k < 6; ++k)
+  {
+    if (!g.comp[k].exists)
+      continue;
+    DALLOC (ctx->ff[k], n * elem_size (ctx->kind));
+    if (g.cfg.use_pml)
+      DALLOC (ctx->aux[k], n * sizeof (float));
+  }
+  // 1-D coefficient tables per component (see fast_kernels.cu)
+  std::vector<float> tabs;
+  const double S = kC * g.dt / g.dx;
+  for (int k = 0; k < 6; ++k)
+  {
+    const CompLayout &c = g.comp[k];
+    if (!c.exists)
+      continue;
+    int axes[6] = {c.sig_cacb, c.sig_cacb, c.sig5, c.sig5, c.sig4, c.sig4};
+    for (int j = 0; j < 6; ++j)
+    {
+      std::vector<double> s = sigma_at (g, k, axes[j]);
+      ctx->tab_off[k][j] = tabs.size ();
+      for (double sv : s)
+      {
+        double r = sv * g.dt / (2 * kEps0);
+        double v;
+        switch (j)
+        {
+          case 0: v = (1 - r) / (1 + r); break;
+          case 1: v = S / (1 + r); break;
+          case 2: v = (1 - r) / (1 + r); break;
+          case 3: v = 1 / (1 + r); break;
+          case 4: v = 1 + r; break;
+          default: v = 1 - r; break;
+        }
+        tabs.push_back ((float) v);
+      }
+    }
+  }
+  DALLOC (ctx->tabs, tabs.size () * sizeof (float));
+  CK (cudaMemcpyAsync (ctx->tabs, tabs.data (), tabs.size () * sizeof (float), cudaMemcpyHostToDevice, ctx->stream));
+
+  for (int h = 0; h < 2; ++h)
+  {
+    FastHalf &p = h ? ctx->fast_h : ctx->fast_e;
+    std::memset (&p, 0, sizeof (p));
+    p.g = make_geom_dev (g);
+    p.is_h = h;
+    p.use_pml = g.cfg.use_pml;
+    p.use_tfsf = g.cfg.use_tfsf;
+    p.fp16 = ctx->kind == 2;
+    p.courant = (float) S;
+    for (int k = 0; k < 6; ++k)
+      p.inc_scale[k] = (float) (k >= 3 ? kEta0 : 1.0);
+    p.inc_len = g.inc_len;
+    for (int ci = 0; ci < 3; ++ci)
+    {
+      int k = ci + 3 * h;
+      p.comp[ci] = make_comp_dev (g, k);
+      p.f[ci] = ctx->ff[k];
+      p.aux[ci] = ctx->aux[k];
+      p.opp[ci] = ctx->ff[ci + 3 * (1 - h)];
+      const CompLayout &c = g.comp[k];
+      for (int j = 0; j < 6; ++j)
+        p.tab[ci][j] = c.exists ? ctx->tabs + ctx->tab_off[k][j] : nullptr;
+      for (int a = 0; a < 3; ++a)
+      {
+        std::vector<double> s = sigma_at (g, k, a);
+        int lo = 0, hi = g.n[a];
+        if (g.cfg.use_pml)
+        {
+          lo = 0;
+          while (lo < g.n[a] && s[lo] != 0.0)
+            ++lo;
+          hi = lo;
+          while (hi < g.n[a] && s[hi] == 0.0)
+            ++hi;
+        }
+        p.ilo[ci][a] = lo;
+        p.ihi[ci][a] = hi;
+      }
+    }
+  }
+  CK (cudaStreamSynchronize (ctx->stream));
+  return FDTD_OK;
+}
+
+int create_impl (const fdtd_config *cfg, int device, fdtd_ctx *ctx)
+{
+  std::string err = build_geometry (*cfg, ctx->g);
+  if (!err.empty ())
+    return fail (ctx, FDTD_ERR_ARG, err);
+  int ndev = 0;
+  if (cudaGetDeviceCount (&ndev) != cudaSuccess || ndev <= 0)
+    return fail (ctx, FDTD_ERR_CUDA, "no CUDA device available");
+  if (device < 0 || device >= ndev)
+    return fail (ctx, FDTD_ERR_ARG, "device index out of range");
+  ctx->device = device;
+  ctx->prec = cfg->precision;
+  ctx->kind = kind_of (cfg->precision);
+  ctx->eta0 = ctx->kind == 0 ? 1.0 : kEta0;
+  CK (cudaSetDevice (device));
+  CK (cudaDeviceGetAttribute (&ctx->sm_count, cudaDevAttrMultiProcessorCount, device));
+  CK (cudaStreamCreateWithFlags (&ctx->stream, cudaStreamNonBlocking));
+  CK (cudaEventCreateWithFlags (&ctx->src_ev, cudaEventDisableTiming));
+  DALLOC (ctx->d_err, sizeof (int));
+  const Geometry &g = ctx->g;
+  if (g.cfg.use_tfsf)
+  {
+    for (int l = 0; l < 2; ++l)
+    {
+      DALLOC (ctx->einc[l], (size_t) g.inc_len * sizeof (double));
+      DALLOC (ctx->hinc[l], (size_t) g.inc_len * sizeof (double));
+    }
+  }
+  ctx->nparts = ctx->sm_count * 4;
+  DALLOC (ctx->partials, (size_t) ctx->nparts * 2 * sizeof (double));
+  DALLOC (ctx->d_out, 16 * sizeof (double));
+  int r = ctx->kind == 0 ? alloc_plain (ctx) : alloc_fast (ctx);
+  if (r != FDTD_OK)
+    return r;
+  CK (cudaStreamSynchronize (ctx->stream));
+  return FDTD_OK;
+}
+
+void release (fdtd_ctx *ctx)
+{
+  if (!ctx)
+    return;
+  cudaSetDevice (ctx->device);
+  if (ctx->stream)
+    cudaStreamSynchronize (ctx->stream);
+  for (void *p : ctx->allocs)
+    cudaFree (p);
+  ctx->allocs.clear ();
+  if (ctx->h_src)
+    cudaFreeHost (ctx->h_src);
+  if (ctx->src_ev)
+    cudaEventDestroy (ctx->src_ev);
+  if (ctx->stream)
+    cudaStreamDestroy (ctx->stream);
+  delete ctx;
+}
+
+size_t cell_index (const Geometry &g, int x, int y, int z)
+{
+  return ((size_t) x * g.n[1] + y) * g.n[2] + z;
+}
+
+bool point_source_index (const Geometry &g, size_t *idx)
+{
+  const int *ps = g.cfg.point_source;
+  int z = g.tmz ? 0 : ps[2];
+  if (ps[0] < 0 || ps[0] >= g.n[0] || ps[1] < 0 || ps[1] >= g.n[1] || z < 0 || z >= g.n[2])
+    return false;
+  *idx = cell_index (g, ps[0], ps[1], z);
+  return true;
+}
+
+void rotate (double **lv, int levels)
+{
+  if (!lv[0])
+    return;
+  double *oldest = lv[levels - 1];
+  for (int i = levels - 1; i >= 1; --i)
+    lv[i] = lv[i - 1];
+  lv[0] = oldest;
+}
+
+PlainHalf plain_half (fdtd_ctx *ctx, int h)
+{
+  const Geometry &g = ctx->g;
+  PlainHalf p;
+  std::memset (&p, 0, sizeof (p));
+  p.g = make_geom_dev (g);
+  p.is_h = h;
+  p.use_pml = g.cfg.use_pml;
+  p.use_tfsf = g.cfg.use_tfsf;
+  p.use_meta = g.cfg.use_metamaterials;
+  p.mat_modifier = h ? kMu0 : kEps0;
+  for (int ci = 0; ci < 3; ++ci)
+  {
+    int k = ci + 3 * h;
+    p.comp[ci] = make_comp_dev (g, k);
+    for (int l = 0; l < 3; ++l)
+    {
+      p.f[ci][l] = ctx->f[k][l];
+      p.dd[ci][l] = ctx->dd[k][l];
+      p.d1[ci][l] = ctx->d1[k][l];
+    }
+    p.opp[ci] = ctx->f[ci + 3 * (1 - h)][1];
+  }
+  p.mat = ctx->mat64[h ? 1 : 0];
+  p.omega = ctx->mat64[h ? 3 : 2];
+  p.gamma = ctx->mat64[h ? 5 : 4];
+  for (int a = 0; a < 3; ++a)
+    p.sigma[a] = ctx->sig64[a];
+  p.inc = h ? ctx->einc[ctx->ecur] : ctx->hinc[ctx->hcur];
+  return p;
+}
+
+int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
+{
+  const Geometry &g = ctx->g;
+  int r = ensure_src (ctx, n);
+  if (r != FDTD_OK)
+    return r;
+  for (uint32_t i = 0; i < n; ++i)
+  {
+    uint32_t t = t_start + i;
+    ctx->h_src[3 * i + 0] = incident_source (g, t);
+    ctx->h_src[3 * i + 1] = point_source (g, t, false);
+    ctx->h_src[3 * i + 2] = point_source (g, t, true);
+  }
+  CK (cudaMemcpyAsync (ctx->d_src, ctx->h_src, (size_t) n * 3 * sizeof (double), cudaMemcpyHostToDevice,
+                       ctx->stream));
+  CK (cudaEventRecord (ctx->src_ev, ctx->stream));
+  size_t ps_idx = 0;
+  bool ps_ok = g.cfg.point_source_mask && point_source_index (g, &ps_idx);
+  cudaStream_t s = ctx->stream;
+
+  for (uint32_t i = 0; i < n; ++i)
+  {
+    uint32_t t = t_start + i;
+    for (int h = 0; h < 2; ++h)
+    {
+      if (g.cfg.use_tfsf)
+      {
+        if (!h)
+        {
+          ctx->launches += launch_incident_e (ctx->einc[1 - ctx->ecur], ctx->einc[ctx->ecur],
+                                              ctx->hinc[ctx->hcur], g.inc_len, g.mod_e, ctx->d_src, 3 * i, s);
+          ctx->ecur ^= 1;
+        }
+        else
+        {
+          ctx->launches += launch_incident_h (ctx->hinc[1 - ctx->hcur], ctx->hinc[ctx->hcur],
+                                              ctx->einc[ctx->ecur], g.inc_len, g.mod_h, s);
+          ctx->hcur ^= 1;
+        }
+      }
+      if (ctx->kind == 0)
+      {
+        if (t > 0)
+        {
+          PlainHalf p = plain_half (ctx, h);
+          ctx->launches += launch_plain_half (p, g.inc_len, ctx->d_err, ctx->sm_count, s);
+        }
+        for (int ci = 0; ci < 3; ++ci)
+        {
+          int k = ci + 3 * h;
+          if (ps_ok && (g.cfg.point_source_mask & (1 << k)) && g.comp[k].exists)
+            ctx->launches += launch_point_source (ctx->f[k][0], ps_idx, ctx->d_src, 3 * i + 1 + h, s);
+        }
+        for (int ci = 0; ci < 3; ++ci)
+        {
+          int k = ci + 3 * h;
+          if (!g.comp[k].exists)
+            continue;
+          rotate (ctx->f[k], g.levels);
+          rotate (ctx->dd[k], g.levels);
+          rotate (ctx->d1[k], g.levels);
+        }
+      }
+      else
+      {
+        if (t > 0)
+        {
+          FastHalf &p = h ? ctx->fast_h : ctx->fast_e;
+          p.inc = h ? ctx->einc[ctx->ecur] : ctx->hinc[ctx->hcur];
+          p.mat = ctx->mat32[h];
+          ctx->launches += launch_fast_half (p, ctx->d_err, ctx->sm_count, s);
+        }
+        for (int ci = 0; ci < 3; ++ci)
+        {
+          int k = ci + 3 * h;
+          if (ps_ok && (g.cfg.point_source_mask & (1 << k)) && g.comp[k].exists)
+            ctx->launches += launch_fast_point_source (ctx->ff[k], ctx->kind == 2, ps_idx, ctx->d_src,
+                                                       3 * i + 1 + h, (float) (h ? kEta0 : 1.0), s);
+        }
+      }
+    }
+  }
+  CK (cudaGetLastError ());
+  return FDTD_OK;
+}
+
+}  // namespace
+
+// --------------------------------------------------------------------------
+// public C ABI
+
+extern "C" {
+
+int fdtd_create (const fdtd_config *cfg, int device, fdtd_ctx **out)
+{
+  if (!cfg || !out)
+  {
+    g_last_error = "null argument";
+    return FDTD_ERR_ARG;
+  }
+  *out = nullptr;
+  fdtd_ctx *ctx = new (std::nothrow) fdtd_ctx ();
+  if (!ctx)
+  {
+    g_last_error = "host allocation failed";
+    return FDTD_ERR_NOMEM;
+  }
+  int r = create_impl (cfg, device, ctx);
+  if (r != FDTD_OK)
+  {
+    std::string keep = g_last_error;
+    release (ctx);
+    g_last_error = keep;
+    return r;
+  }
+  *out = ctx;
+  return FDTD_OK;
+}
+
+int fdtd_upload_material (fdtd_ctx *ctx, int which, const double *host)
+{
+  if (!ctx || !host || which < 0 || which > 5)
+    return fail (ctx, FDTD_ERR_ARG, "bad argument");
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  size_t n = (size_t) ctx->g.cells;
+  if (ctx->kind == 0)
+  {
+    if (!ctx->mat64[which])
+      return fail (ctx, FDTD_ERR_UNSUPPORTED, "Drude grids need use_metamaterials");
+    CK (cudaMemcpyAsync (ctx->mat64[which], host, n * sizeof (double), cudaMemcpyHostToDevice, ctx->stream));
+    CK (cudaStreamSynchronize (ctx->stream));
+    return FDTD_OK;
+  }
+  if ((r = ensure_staging (ctx)) != FDTD_OK)
+    return r;
+  CK (cudaMemcpyAsync (ctx->staging, host, n * sizeof (double), cudaMemcpyHostToDevice, ctx->stream));
+  r = fdtd_upload_material_device (ctx, which, ctx->staging);
+  if (r != FDTD_OK)
+    return r;
+  CK (cudaStreamSynchronize (ctx->stream));
+  return FDTD_OK;
+}
+
+int fdtd_upload_material_device (fdtd_ctx *ctx, int which, const double *dev)
+{
+  if (!ctx || !dev || which < 0 || which > 5)
+    return fail (ctx, FDTD_ERR_ARG, "bad argument");
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  size_t n = (size_t) ctx->g.cells;
+  if (ctx->kind == 0)
+  {
+    if (!ctx->mat64[which])
+      return fail (ctx, FDTD_ERR_UNSUPPORTED, "Drude grids need use_metamaterials");
+    CK (cudaMemcpyAsync (ctx->mat64[which], dev, n * sizeof (double), cudaMemcpyDeviceToDevice, ctx->stream));
+    return FDTD_OK;
+  }
+  if (which > 1)
+    return fail (ctx, FDTD_ERR_UNSUPPORTED, "Drude grids are provided by the FP64 plain form only");
+  if (!ctx->mat32[which])
+    DALLOC (ctx->mat32[which], n * sizeof (float));
+  ctx->launches += launch_convert_in (ctx->mat32[which], 1, dev, n, 1.0, ctx->stream);
+  CK (cudaGetLastError ());
+  return FDTD_OK;
+}
+
+int fdtd_upload_field (fdtd_ctx *ctx, int component, const double *host)
+{
+  if (!ctx || !host || component < 0 || component > 5 || !ctx->g.comp[component].exists)
+    return fail (ctx, FDTD_ERR_ARG, "bad argument");
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  size_t n = (size_t) ctx->g.cells;
+  if (ctx->kind == 0)
+  {
+    CK (cudaMemcpyAsync (ctx->f[component][1], host, n * sizeof (double), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  else
+  {
+    if ((r = ensure_staging (ctx)) != FDTD_OK)
+      return r;
+    CK (cudaMemcpyAsync (ctx->staging, host, n * sizeof (double), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->launches += launch_convert_in (ctx->ff[component], ctx->kind, ctx->staging, n,
+                                        component >= 3 ? kEta0 : 1.0, ctx->stream);
+  }
+  CK (cudaStreamSynchronize (ctx->stream));
+  return FDTD_OK;
+}
+
+int fdtd_step (fdtd_ctx *ctx, uint32_t t_start, uint32_t n_steps)
+{
+  if (!ctx)
+    return FDTD_ERR_ARG;
+  if (n_steps == 0)
+    return FDTD_OK;
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  return step_impl (ctx, t_start, n_steps);
+}
+
+int fdtd_sync (fdtd_ctx *ctx, int64_t timeout_ns)
+{
+  if (!ctx)
+    return FDTD_ERR_ARG;
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  if (timeout_ns < 0)
+  {
+    CK (cudaStreamSynchronize (ctx->stream));
+  }
+  else
+  {
+    auto t0 = std::chrono::steady_clock::now ();
+    for (;;)
+    {
+      cudaError_t e = cudaStreamQuery (ctx->stream);
+      if (e == cudaSuccess)
+        break;
+      if (e != cudaErrorNotReady)
+        return fail (ctx, FDTD_ERR_CUDA, std::string ("cudaStreamQuery: ") + cudaGetErrorString (e));
+      auto dt = std::chrono::duration_cast<std::chrono::nanoseconds> (std::chrono::steady_clock::now () - t0);
+      if (dt.count () >= timeout_ns)
+        return fail (ctx, FDTD_ERR_TIMEOUT, "sync timed out");
+      std::this_thread::sleep_for (std::chrono::microseconds (50));
+    }
+  }
+  int flag = 0;
+  CK (cudaMemcpy (&flag, ctx->d_err, sizeof (int), cudaMemcpyDeviceToHost));
+  if (flag)
+    return fail (ctx, FDTD_ERR_DEVICE, "a kernel reported an out-of-range incident-grid index");
+  return FDTD_OK;
+}
+
+int fdtd_download_field_device (fdtd_ctx *ctx, int component, double *dev)
+{
+  if (!ctx || !dev || component < 0 || component > 5 || !ctx->g.comp[component].exists)
+    return fail (ctx, FDTD_ERR_ARG, "bad argument");
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  size_t n = (size_t) ctx->g.cells;
+  if (ctx->kind == 0)
+  {
+    CK (cudaMemcpyAsync (dev, ctx->f[component][1], n * sizeof (double), cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  else
+  {
+    ctx->launches += launch_convert_out (dev, ctx->ff[component], ctx->kind, n,
+                                         component >= 3 ? 1.0 / kEta0 : 1.0, ctx->stream);
+    CK (cudaGetLastError ());
+  }
+  return FDTD_OK;
+}
+
+int fdtd_download_field (fdtd_ctx *ctx, int component, double *host)
+{
+  if (!ctx || !host || component < 0 || component > 5 || !ctx->g.comp[component].exists)
+    return fail (ctx, FDTD_ERR_ARG, "bad argument");
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  size_t n = (size_t) ctx->g.cells;
+  if (ctx->kind == 0)
+  {
+    CK (cudaMemcpyAsync (host, ctx->f[component][1], n * sizeof (double), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  else
+  {
+    if ((r = ensure_staging (ctx)) != FDTD_OK)
+      return r;
+    if ((r = fdtd_download_field_device (ctx, component, ctx->staging)) != FDTD_OK)
+      return r;
+    CK (cudaMemcpyAsync (host, ctx->staging, n * sizeof (double), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  CK (cudaStreamSynchronize (ctx->stream));
+  return FDTD_OK;
+}
+
+int fdtd_reduce (fdtd_ctx *ctx, int what, double *out)
+{
+  if (!ctx || !out || (what != FDTD_REDUCE_ENERGY && what != FDTD_REDUCE_L2))
+    return fail (ctx, FDTD_ERR_ARG, "bad argument");
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  size_t n = (size_t) ctx->g.cells;
+  for (int k = 0; k < 6; ++k)
+  {
+    if (!ctx->g.comp[k].exists)
+    {
+      CK (cudaMemsetAsync (ctx->d_out + k, 0, sizeof (double), ctx->stream));
+      continue;
+    }
+    const void *src = ctx->kind == 0 ? (const void *) ctx->f[k][1] : (const void *) ctx->ff[k];
+    const void *w = nullptr;
+    int wkind = 0;
+    double scale = 1.0;
+    bool isH = k >= 3;
+    if (what == FDTD_REDUCE_ENERGY)
+    {
+      if (ctx->kind == 0)
+      {
+        w = ctx->mat64[isH ? 1 : 0];
+        wkind = 2;
+        scale = isH ? kEta0 * kEta0 : 1.0;
+      }
+      else
+      {
+        w = ctx->mat32[isH ? 1 : 0];
+        wkind = w ? 1 : 0;
+      }
+    }
+    else if (ctx->kind != 0 && isH)
+    {
+      scale = 1.0 / (kEta0 * kEta0);
+    }
+    ctx->launches += launch_reduce_sq (src, ctx->kind, n, w, wkind, scale, ctx->partials, ctx->nparts, ctx->stream);
+    ctx->launches += launch_reduce_final (ctx->partials, ctx->nparts, ctx->d_out + k, ctx->stream);
+  }
+  double vals[6];
+  CK (cudaMemcpyAsync (vals, ctx->d_out, 6 * sizeof (double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK (cudaStreamSynchronize (ctx->stream));
+  if (what == FDTD_REDUCE_L2)
+  {
+    for (int k = 0; k < 6; ++k)
+      out[k] = vals[k];
+  }
+  else
+  {
+    double s = 0.0, c = 0.0;
+    for (int k = 0; k < 6; ++k)
+    {
+      double t = s + vals[k];
+      c += std::fabs (s) >= std::fabs (vals[k]) ? (s - t) + vals[k] : (vals[k] - t) + s;
+      s = t;
+    }
+    out[0] = s + c;
+  }
+  return FDTD_OK;
+}
+
+int fdtd_scalars (const fdtd_ctx *ctx, double out[3])
+{
+  if (!ctx || !out)
+    return FDTD_ERR_ARG;
+  out[0] = ctx->g.dt;
+  out[1] = ctx->g.freq;
+  out[2] = ctx->g.rpv;
+  return FDTD_OK;
+}
+
+int64_t fdtd_launch_count (const fdtd_ctx *ctx)
+{
+  return ctx ? ctx->launches : -1;
+}
+
+void fdtd_destroy (fdtd_ctx *ctx)
+{
+  release (ctx);
+}
+
+const char *fdtd_status_str (int status)
+{
+  switch (status)
+  {
+    case FDTD_OK: return "ok";
+    case FDTD_ERR_ARG: return "invalid argument or configuration";
+    case FDTD_ERR_CUDA: return "CUDA runtime error";
+    case FDTD_ERR_NOMEM: return "out of memory";
+    case FDTD_ERR_TIMEOUT: return "timed out";
+    case FDTD_ERR_UNSUPPORTED: return "unsupported mode or option";
+    case FDTD_ERR_STATE: return "call out of order";
+    case FDTD_ERR_DEVICE: return "device-side error flag";
+    default: return "unknown status";
+  }
+}
+
+const char *fdtd_last_error (void)
+{
+  return g_last_error.c_str ();
+}
+
+}  // extern "C"

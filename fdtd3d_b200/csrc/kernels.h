@@ -1,0 +1,59 @@
+// kernels.h - launchers of the device kernels (host-callable, no CUDA types
+// beyond cudaStream_t).  Each launcher returns the number of kernels it
+// launched so the context can count its launches.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "params.h"
+
+namespace fdtdb {
+
+// FP32 / FP16-storage fused form: one half-step of all E or all H components.
+// Fields are stored in place (one time level); the PML auxiliary fields are
+// touched only in PML cells; H is stored scaled by the free-space impedance
+// so E and H share one magnitude range (needed for FP16 storage).
+struct FastHalf
+{
+  GeomDev g;
+  int is_h;
+  int use_pml;
+  int use_tfsf;
+  int fp16;                   // 1: fields stored as __half
+  CompDev comp[3];
+  void *f[3];                 // updated family (float* or __half*)
+  float *aux[3];              // PML auxiliary (D/eps0 or c*B), full size, PML cells only
+  const void *opp[3];         // opposite family (null when absent)
+  const float *mat;           // eps (E) or mu (H); null = uniform 1
+  float courant;              // c*dt/dx
+  float inc_scale[6];         // incident value -> stored units (eta0 for H, 1 for E)
+  const float *tab[3][6];     // per component: ca1, sq1 (curl axis), p5, q5 (axis c2), g4p, g4m (axis c0)
+  int ilo[3][3], ihi[3][3];   // per component per axis: sigma == 0 range
+  const double *inc;          // incident grid at level 1
+  int inc_len;
+};
+
+int launch_plain_half (const PlainHalf &p, int inc_len, int *err, int sm_count, cudaStream_t s);
+int launch_incident_e (double *e_new, const double *e_old, const double *h_old, int len, double modifier,
+                       const double *src, int src_index, cudaStream_t s);
+int launch_incident_h (double *h_new, const double *h_old, const double *e_new, int len, double modifier,
+                       cudaStream_t s);
+int launch_point_source (double *f, size_t index, const double *src, int src_index, cudaStream_t s);
+
+int launch_fast_half (const FastHalf &p, int *err, int sm_count, cudaStream_t s);
+int launch_fast_point_source (void *f, int fp16, size_t index, const double *src, int src_index, float scale,
+                              cudaStream_t s);
+
+// conversions between host-order FP64 arrays and the stored forms
+int launch_convert_in (void *dst, int dst_kind, const double *src, size_t n, double scale, cudaStream_t s);
+int launch_convert_out (double *dst, const void *src, int src_kind, size_t n, double scale, cudaStream_t s);
+// kinds: 0 = double, 1 = float, 2 = __half
+
+// compensated FP64 reductions: out[0..parts) partial pairs (sum, compensation)
+// weight kinds: 0 = none, 1 = float, 2 = double
+int launch_reduce_sq (const void *src, int kind, size_t n, const void *weight, int wkind, double scale,
+                      double *partials, int nblocks, cudaStream_t s);
+int launch_fill (double *dst, size_t n, double value, cudaStream_t s);
+int launch_reduce_final (const double *partials, int nblocks, double *out, cudaStream_t s);
+
+}  // namespace fdtdb

@@ -1,0 +1,455 @@
+// setup.cpp - geometry, physics scalars and TF/SF terms of the fdtd3d step.
+//
+// Reference behaviour followed (zer011b/fdtd3d, paths under Source/):
+//   dt, frequency, relPhaseVelocity ... Scheme/InternalScheme.inc.h:3359-3394
+//   numerical phase velocity .......... Layout/Approximation.cpp:259-359
+//   sigma profiles (x vs y/z quirk) ... Scheme/SchemeHelper.h:574-718
+//   Yee offsets / circuit diffs ....... Layout/YeeGridLayout.cpp:1937-1990
+//   TF/SF border predicates ........... Layout/YeeGridLayout.h:498-512,
+//                                       Layout/YeeGridLayout.cpp:257-1720
+//   incident projections .............. Layout/YeeGridLayout.h:2227-2357
+//   zeroIncCoordFP .................... Layout/YeeGridLayout.cpp:2600-2660
+//   TF/SF slot selection .............. Scheme/InternalScheme.inc.h:1386-1835
+#include "setup.h"
+
+#include <cmath>
+#include <cstring>
+
+namespace fdtdb {
+
+namespace {
+
+constexpr double kApproxAcc = 0.0000001;   // Layout/Approximation.h:27
+constexpr double kFpExact = 0.0000001;     // Kernels/FieldValue.h:153 (double)
+
+bool fp_exact (double a, double b)
+{
+  return (a > b ? a - b : b - a) < kFpExact;
+}
+
+bool axis_angle (double a)
+{
+  return a == 0 || a == kPi / 2 || a == kPi || a == 3 * kPi / 2;
+}
+
+bool diag_angle (double a)
+{
+  return a == kPi / 4 || a == 3 * kPi / 4 || a == 5 * kPi / 4 || a == 7 * kPi / 4;
+}
+
+double wave_number (double delta, double lambda, double courant, double n_lambda, double a1, double a2)
+{
+  if (axis_angle (a1) && axis_angle (a2))
+  {
+    return 2.0 / delta * std::asin (std::sin (kPi * courant / n_lambda) / courant);
+  }
+  if ((axis_angle (a1) && diag_angle (a2)) || (diag_angle (a1) && axis_angle (a2)))
+  {
+    return 2.0 * std::sqrt (2.0) / delta
+           * std::asin (std::sin (kPi * courant / n_lambda) / (courant * std::sqrt (2.0)));
+  }
+  // Newton iteration on the 3-D numerical dispersion relation
+  double k = 2 * kPi;
+  double k_prev = k + 2 * std::sqrt (kApproxAcc);
+  double nd = delta / lambda;
+  double A = nd * std::sin (a1) * std::cos (a2) / 2;
+  double B = nd * std::sin (a1) * std::sin (a2) / 2;
+  double C = nd * std::cos (a1) / 2;
+  double s = std::sin (kPi * courant / n_lambda);
+  double D = (s * s) / (courant * courant);
+  int guard = 0;
+  while ((k_prev - k) * (k_prev - k) >= kApproxAcc && guard++ < 100000)
+  {
+    k_prev = k;
+    double sa = std::sin (A * k), sb = std::sin (B * k), sc = std::sin (C * k);
+    double f = sa * sa + sb * sb + sc * sc - D;
+    double df = A * std::sin (2 * A * k) + B * std::sin (2 * B * k) + C * std::sin (2 * C * k);
+    k -= f / df;
+  }
+  return k / lambda;
+}
+
+double phase_velocity (double delta, double lambda, double courant, double n_lambda, double a1, double a2)
+{
+  return kC * 2 * kPi / lambda / wave_number (delta, lambda, courant, n_lambda, a1, a2);
+}
+
+double sigma_value (double dist, double boundary, double step)
+{
+  const uint32_t m = 6;
+  const double r_err = 1e-16;
+  double sigma_max = -std::log (r_err) * (m + 1.0) / (2.0 * std::sqrt (kMu0 / kEps0) * boundary);
+  double factor = sigma_max / (step * (std::pow (boundary, m)) * (m + 1));
+  double x1 = (dist + 1) * step;
+  double x2 = dist * step;
+  return factor * (std::pow (x1, (m + 1)) - std::pow (x2, (m + 1)));
+}
+
+// Axis 0 keeps the fractional distance and compares against size; axes 1, 2
+// truncate the distance and compare against size + 0.5 (the reference's
+// initSigmaX / initSigmaY / initSigmaZ differ exactly this way).
+void sigma_profile (std::vector<double> &out, int axis, int n, int pml, double dx)
+{
+  out.assign (n, 0.0);
+  double p = (double) pml;
+  double boundary = p * dx;
+  for (int i = 0; i < n; ++i)
+  {
+    double pos = i + 0.5;
+    if (axis == 0)
+    {
+      double size = (double) n;
+      if (pos < p)
+        out[i] = sigma_value (p - pos, boundary, dx);
+      else if (pos >= size - p)
+        out[i] = sigma_value (pos - (size - p), boundary, dx);
+    }
+    else
+    {
+      double size = n + 0.5;
+      if (pos < p)
+        out[i] = sigma_value ((int32_t) (p - pos), boundary, dx);
+      else if (pos >= size - p)
+        out[i] = sigma_value ((int32_t) (pos - (size - p)), boundary, dx);
+    }
+  }
+}
+
+void set3 (int *v, int a, int b, int c)
+{
+  v[0] = a;
+  v[1] = b;
+  v[2] = c;
+}
+
+// Axis tests of one TF/SF border predicate.
+enum { T_ANY, T_EXL, T_EXR, T_RANGE };
+struct AxisTest
+{
+  int kind, o1, o2;
+};
+struct Pred
+{
+  bool valid;
+  AxisTest ax[3];
+};
+enum { DL, DR, DD, DU, DB, DF, DNONE };
+
+Pred pred (int k0, int a0, int b0, int k1, int a1, int b1, int k2, int a2, int b2)
+{
+  Pred p;
+  p.valid = true;
+  p.ax[0] = {k0, a0, b0};
+  p.ax[1] = {k1, a1, b1};
+  p.ax[2] = {k2, a2, b2};
+  return p;
+}
+
+}  // namespace
+
+namespace {
+
+// Dim3 E_CENTERED layout of component k; TMz drops the z axis afterwards.
+void init_components (Geometry &g, Pred preds[6][6], int slot_dir[6][4])
+{
+  for (int k = 0; k < 6; ++k)
+  {
+    CompLayout &c = g.comp[k];
+    std::memset (&c, 0, sizeof (c));
+    int a = k % 3;
+    bool isH = k >= 3;
+    for (int ax = 0; ax < 3; ++ax)
+      c.min_fp[ax] = isH ? (ax == a ? 0.5 : 1.0) : (ax == a ? 1.0 : 0.5);
+    c.sig_cacb = (a + 1) % 3;
+    c.sig4 = a;
+    c.sig5 = (a + 2) % 3;
+    if (!isH)
+    {
+      c.nmat = 2;
+      c.m[1][a] = 1;
+    }
+    else
+    {
+      int lo = a == 0 ? 1 : 0;
+      int hi = a == 2 ? 1 : 2;
+      c.nmat = 4;
+      c.m[1][hi] = 1;
+      c.m[2][lo] = 1;
+      c.m[3][lo] = 1;
+      c.m[3][hi] = 1;
+    }
+    for (int d = 0; d < 6; ++d)
+      preds[k][d].valid = false;
+  }
+  CompLayout *c;
+  c = &g.comp[EX];
+  c->opp1 = HZ; c->opp2 = HY;
+  set3 (c->d11, 0, -1, 0); set3 (c->d12, 0, 0, 0); set3 (c->d21, 0, 0, -1); set3 (c->d22, 0, 0, 0);
+  slot_dir[EX][0] = DD; slot_dir[EX][1] = DU; slot_dir[EX][2] = DB; slot_dir[EX][3] = DF;
+  preds[EX][DD] = pred (T_RANGE, -1, 1, T_EXL, -5, 0, T_RANGE, 4, -4);
+  preds[EX][DU] = pred (T_RANGE, -1, 1, T_EXR, 5, 0, T_RANGE, 4, -4);
+  preds[EX][DB] = pred (T_RANGE, -1, 1, T_RANGE, 4, -4, T_EXL, -5, 0);
+  preds[EX][DF] = pred (T_RANGE, -1, 1, T_RANGE, 4, -4, T_EXR, 5, 0);
+  c = &g.comp[EY];
+  c->opp1 = HX; c->opp2 = HZ;
+  set3 (c->d11, 0, 0, -1); set3 (c->d12, 0, 0, 0); set3 (c->d21, -1, 0, 0); set3 (c->d22, 0, 0, 0);
+  slot_dir[EY][0] = DB; slot_dir[EY][1] = DF; slot_dir[EY][2] = DL; slot_dir[EY][3] = DR;
+  preds[EY][DL] = pred (T_EXL, -5, 0, T_RANGE, -1, 1, T_RANGE, 4, -4);
+  preds[EY][DR] = pred (T_EXR, 5, 0, T_RANGE, -1, 1, T_RANGE, 4, -4);
+  preds[EY][DB] = pred (T_RANGE, 4, -4, T_RANGE, -1, 1, T_EXL, -5, 0);
+  preds[EY][DF] = pred (T_RANGE, 4, -4, T_RANGE, -1, 1, T_EXR, 5, 0);
+  c = &g.comp[EZ];
+  c->opp1 = HY; c->opp2 = HX;
+  set3 (c->d11, -1, 0, 0); set3 (c->d12, 0, 0, 0); set3 (c->d21, 0, -1, 0); set3 (c->d22, 0, 0, 0);
+  slot_dir[EZ][0] = DL; slot_dir[EZ][1] = DR; slot_dir[EZ][2] = DD; slot_dir[EZ][3] = DU;
+  preds[EZ][DL] = pred (T_EXL, -5, 0, T_RANGE, 4, -4, T_RANGE, -1, 1);
+  preds[EZ][DR] = pred (T_EXR, 5, 0, T_RANGE, 4, -4, T_RANGE, -1, 1);
+  preds[EZ][DD] = pred (T_RANGE, 4, -4, T_EXL, -5, 0, T_RANGE, -1, 1);
+  preds[EZ][DU] = pred (T_RANGE, 4, -4, T_EXR, 5, 0, T_RANGE, -1, 1);
+  c = &g.comp[HX];
+  c->opp1 = EY; c->opp2 = EZ;
+  set3 (c->d11, 0, 0, 0); set3 (c->d12, 0, 0, 1); set3 (c->d21, 0, 0, 0); set3 (c->d22, 0, 1, 0);
+  slot_dir[HX][0] = DB; slot_dir[HX][1] = DF; slot_dir[HX][2] = DD; slot_dir[HX][3] = DU;
+  preds[HX][DD] = pred (T_RANGE, 4, -4, T_EXL, 0, 0, T_RANGE, -1, 1);
+  preds[HX][DU] = pred (T_RANGE, 4, -4, T_EXR, 0, 0, T_RANGE, -1, 1);
+  preds[HX][DB] = pred (T_RANGE, 4, -4, T_RANGE, -1, 1, T_EXL, 0, 0);
+  preds[HX][DF] = pred (T_RANGE, 4, -4, T_RANGE, -1, 1, T_EXR, 0, 0);
+  c = &g.comp[HY];
+  c->opp1 = EZ; c->opp2 = EX;
+  set3 (c->d11, 0, 0, 0); set3 (c->d12, 1, 0, 0); set3 (c->d21, 0, 0, 0); set3 (c->d22, 0, 0, 1);
+  slot_dir[HY][0] = DL; slot_dir[HY][1] = DR; slot_dir[HY][2] = DB; slot_dir[HY][3] = DF;
+  preds[HY][DL] = pred (T_EXL, 0, 0, T_RANGE, 4, -4, T_RANGE, -1, 1);
+  preds[HY][DR] = pred (T_EXR, 0, 0, T_RANGE, 4, -4, T_RANGE, -1, 1);
+  preds[HY][DB] = pred (T_RANGE, -1, 1, T_RANGE, 4, -4, T_EXL, 0, 0);
+  preds[HY][DF] = pred (T_RANGE, -1, 1, T_RANGE, 4, -4, T_EXR, 0, 0);
+  c = &g.comp[HZ];
+  c->opp1 = EX; c->opp2 = EY;
+  set3 (c->d11, 0, 0, 0); set3 (c->d12, 0, 1, 0); set3 (c->d21, 0, 0, 0); set3 (c->d22, 1, 0, 0);
+  slot_dir[HZ][0] = DD; slot_dir[HZ][1] = DU; slot_dir[HZ][2] = DL; slot_dir[HZ][3] = DR;
+  preds[HZ][DL] = pred (T_EXL, 0, 0, T_RANGE, -1, 1, T_RANGE, 4, -4);
+  preds[HZ][DR] = pred (T_EXR, 0, 0, T_RANGE, -1, 1, T_RANGE, 4, -4);
+  preds[HZ][DD] = pred (T_RANGE, -1, 1, T_EXL, 0, 0, T_RANGE, 4, -4);
+  preds[HZ][DU] = pred (T_RANGE, -1, 1, T_EXR, 0, 0, T_RANGE, 4, -4);
+
+  for (int k = 0; k < 6; ++k)
+    g.comp[k].exists = g.tmz ? (k == EZ || k == HX || k == HY) : true;
+  if (g.tmz)
+  {
+    for (int k = 0; k < 6; ++k)
+    {
+      CompLayout &cc = g.comp[k];
+      cc.d11[2] = cc.d12[2] = cc.d21[2] = cc.d22[2] = 0;
+      for (int j = 0; j < 4; ++j)
+        cc.m[j][2] = 0;
+      for (int d = 0; d < 6; ++d)
+        preds[k][d].ax[2].kind = T_ANY;
+      preds[k][DB].valid = false;
+      preds[k][DF].valid = false;
+    }
+  }
+}
+
+bool axis_ok (const AxisTest &t, double coord, double left, double right)
+{
+  switch (t.kind)
+  {
+    case T_ANY:
+      return true;
+    case T_EXL:
+      return fp_exact (coord, left + t.o1 * 1.0 / 10.0);
+    case T_EXR:
+      return fp_exact (coord, right + t.o1 * 1.0 / 10.0);
+    default:
+      return coord > left + t.o1 * 1.0 / 10.0 && coord < right + t.o2 * 1.0 / 10.0;
+  }
+}
+
+}  // namespace
+
+std::string build_geometry (const fdtd_config &cfg, Geometry &g)
+{
+  g = Geometry ();
+  g.cfg = cfg;
+  if (cfg.mode != FDTD_MODE_DIM3 && cfg.mode != FDTD_MODE_TMZ)
+    return "mode must be FDTD_MODE_DIM3 or FDTD_MODE_TMZ";
+  if (cfg.layout != 0)
+    return "only the E_CENTERED layout (0) is provided";
+  if (cfg.precision < FDTD_PREC_FP64_PLAIN || cfg.precision > FDTD_PREC_FP16S)
+    return "unknown precision";
+  if (cfg.use_metamaterials && !cfg.use_pml)
+    return "metamaterials require PML (as in the reference)";
+  g.tmz = cfg.mode == FDTD_MODE_TMZ;
+  g.n[0] = cfg.size[0];
+  g.n[1] = cfg.size[1];
+  g.n[2] = g.tmz ? 1 : cfg.size[2];
+  int dims = g.tmz ? 2 : 3;
+  for (int a = 0; a < dims; ++a)
+  {
+    if (g.n[a] < 3 || g.n[a] > (1 << 20))
+      return "grid size out of range";
+    if (cfg.use_pml && (cfg.pml[a] < 0 || 2 * cfg.pml[a] >= g.n[a]))
+      return "PML size out of range";
+    if (cfg.use_tfsf && (cfg.tfsf_left[a] < 1 || cfg.tfsf_right[a] < 1
+                         || cfg.tfsf_left[a] + cfg.tfsf_right[a] >= g.n[a]))
+      return "TF/SF size out of range";
+  }
+  if (!(cfg.dx > 0) || !(cfg.wavelength > 0) || !(cfg.courant > 0))
+    return "dx, wavelength and courant factor must be positive";
+  g.cells = (int64_t) g.n[0] * g.n[1] * g.n[2];
+  g.levels = (cfg.use_metamaterials && cfg.use_pml) ? 3 : 2;
+  g.dx = cfg.dx;
+
+  // InternalScheme::initScheme
+  g.freq = kC / cfg.wavelength;
+  g.dt = cfg.dx * cfg.courant / kC;
+  g.a1 = cfg.angle_teta * kPi / 180.0;
+  g.a2 = cfg.angle_phi * kPi / 180.0;
+  g.a3 = cfg.angle_psi * kPi / 180.0;
+  double n_lambda = cfg.wavelength / cfg.dx;
+  double pv0 = phase_velocity (cfg.dx, cfg.wavelength, cfg.courant, n_lambda, kPi / 2, 0);
+  double pv = phase_velocity (cfg.dx, cfg.wavelength, cfg.courant, n_lambda, g.a1, g.a2);
+  g.rpv = pv0 / pv;
+  if (!std::isfinite (g.rpv) || !(g.rpv > 0))
+    return "phase-velocity correction did not converge";
+  g.mod_e = g.dt / (g.rpv * kEps0 * g.dx);
+  g.mod_h = g.dt / (g.rpv * kMu0 * g.dx);
+  g.s1 = std::sin (g.a1);
+  g.c1 = std::cos (g.a1);
+  g.s2 = std::sin (g.a2);
+  g.c2 = std::cos (g.a2);
+  double s3 = std::sin (g.a3), c3 = std::cos (g.a3);
+  for (int k = 0; k < 6; ++k)
+    g.proj[k] = 0;
+  if (!g.tmz)
+  {
+    // the Hz projection carries the reference's leading minus sign
+    g.proj[EX] = c3 * g.s2 - s3 * g.c1 * g.c2;
+    g.proj[EY] = -c3 * g.c2 - s3 * g.c1 * g.s2;
+    g.proj[EZ] = s3 * g.s1;
+    g.proj[HX] = s3 * g.s2 + c3 * g.c1 * g.c2;
+    g.proj[HY] = -s3 * g.c2 + c3 * g.c1 * g.s2;
+    g.proj[HZ] = -(c3 * g.s1);
+    g.zero_inc[0] = cfg.tfsf_left[0] - 2.5 * std::sin (g.a1) * std::cos (g.a2);
+    g.zero_inc[1] = cfg.tfsf_left[1] - 2.5 * std::sin (g.a1) * std::sin (g.a2);
+    g.zero_inc[2] = cfg.tfsf_left[2] - 2.5 * std::cos (g.a1);
+  }
+  else
+  {
+    g.proj[EZ] = 1.0;
+    g.proj[HX] = std::sin (g.a2);
+    g.proj[HY] = -std::cos (g.a2);
+    g.zero_inc[0] = cfg.tfsf_left[0] - 2.5 * std::cos (g.a2);
+    g.zero_inc[1] = cfg.tfsf_left[1] - 2.5 * std::sin (g.a2);
+    g.zero_inc[2] = 0;
+  }
+  g.inc_len = 500 * g.n[0];
+
+  for (int a = 0; a < 3; ++a)
+  {
+    g.sigma[a].assign (g.n[a], 0.0);
+    if (cfg.use_pml && a < dims)
+      sigma_profile (g.sigma[a], a, g.n[a], cfg.pml[a], cfg.dx);
+  }
+
+  Pred preds[6][6];
+  int slot_dir[6][4];
+  init_components (g, preds, slot_dir);
+
+  if (cfg.use_tfsf)
+  {
+    double left[3], right[3];
+    for (int a = 0; a < 3; ++a)
+    {
+      left[a] = 0.0 + (double) cfg.tfsf_left[a];
+      right[a] = 0.0 + (double) (g.n[a] - cfg.tfsf_right[a]);
+    }
+    for (int k = 0; k < 6; ++k)
+    {
+      const CompLayout &c = g.comp[k];
+      if (!c.exists)
+        continue;
+      bool isH = k >= 3;
+      int slot_box[4][2][3];
+      bool slot_on[4] = {false, false, false, false};
+      for (int s = 0; s < 4; ++s)
+      {
+        const Pred &p = preds[k][slot_dir[k][s]];
+        if (!p.valid)
+          continue;
+        bool empty = false;
+        for (int a = 0; a < 3; ++a)
+        {
+          int lo_r = (a < dims) ? 1 : 0;
+          int hi_r = (a < dims) ? g.n[a] - 1 : 1;
+          int first = -1, last = -2, count = 0;
+          for (int i = lo_r; i < hi_r; ++i)
+          {
+            if (axis_ok (p.ax[a], i + c.min_fp[a], left[a], right[a]))
+            {
+              if (first < 0)
+                first = i;
+              last = i;
+              ++count;
+            }
+          }
+          if (count == 0)
+          {
+            empty = true;
+            break;
+          }
+          if (count != last - first + 1)
+            return "TF/SF border set is not a box";
+          slot_box[s][0][a] = first;
+          slot_box[s][1][a] = last + 1;
+        }
+        slot_on[s] = !empty;
+      }
+      for (int s = 0; s < 4; ++s)
+      {
+        if (!slot_on[s])
+          continue;
+        // slots 11/12 (and 21/22) never hold on the same cell; keep the
+        // reference's "if 11 ... else if 12" priority explicit anyway
+        int partner = s ^ 1;
+        if (slot_on[partner] && partner < s)
+        {
+          bool overlap = true;
+          for (int a = 0; a < 3; ++a)
+            overlap = overlap && slot_box[s][0][a] < slot_box[partner][1][a]
+                      && slot_box[partner][0][a] < slot_box[s][1][a];
+          if (overlap)
+            return "TF/SF slots overlap";
+        }
+        TfsfTerm t;
+        t.comp = k;
+        t.slot = isH ? s : (s ^ 1);
+        t.inc_comp = s < 2 ? c.opp1 : c.opp2;
+        const int *diffs[4] = {c.d11, c.d12, c.d21, c.d22};
+        for (int a = 0; a < 3; ++a)
+        {
+          t.lo[a] = slot_box[s][0][a];
+          t.hi[a] = slot_box[s][1][a];
+          t.aux[a] = diffs[t.slot][a];
+        }
+        t.negate = isH ? -1.0 : 1.0;
+        if (!g.comp[t.inc_comp].exists)
+          continue;
+        g.tfsf.push_back (t);
+      }
+    }
+  }
+  return "";
+}
+
+double incident_source (const Geometry &g, uint32_t t)
+{
+  return std::sin (g.dt * t * 2 * kPi * g.freq);
+}
+
+double point_source (const Geometry &g, uint32_t t, bool h)
+{
+  double ts = t + (h ? 1.0 : 0.5);
+  return std::sin (g.dt * ts * 2 * kPi * g.freq);
+}
+
+}  // namespace fdtdb

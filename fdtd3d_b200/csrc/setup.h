@@ -1,0 +1,79 @@
+// setup.h - host-side set-up of the fdtd3d leapfrog step for the B200 kernels.
+//
+// Everything here runs once per context on the host, in FP64, with the same
+// operation order as the reference so that the FP64 plain form can be
+// bit-faithful.  The kernels receive the results as plain numbers, 1-D tables
+// and integer boxes (no per-cell predicate evaluation on the device).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/fdtd_b200.h"
+
+namespace fdtdb {
+
+// Source/Physics/PhysicsConst.h:28-32
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kC = 299792458.0;
+constexpr double kMu0 = 4 * kPi * 0.0000001;
+constexpr double kEps0 = 1 / (kMu0 * (kC * kC));
+
+enum Comp { EX = 0, EY = 1, EZ = 2, HX = 3, HY = 4, HZ = 5 };
+
+// One TF/SF correction term: on the cells of `box`, the curl of component
+// `comp` uses neighbour slot `slot` (0 = p11, 1 = p12, 2 = p21, 3 = p22)
+// minus the incident value of component `inc_comp` taken at the real
+// coordinate of cell + aux.  InternalScheme.inc.h:1386-1835.
+struct TfsfTerm
+{
+  int comp;
+  int slot;
+  int inc_comp;
+  int lo[3];
+  int hi[3];       // exclusive
+  int aux[3];
+  double negate;   // -1 for H components (E_CENTERED), +1 for E
+};
+
+// Per-component layout (E_CENTERED).  YeeGridLayout.cpp:1937-1990.
+struct CompLayout
+{
+  bool exists;
+  double min_fp[3];
+  int opp1, opp2;
+  int d11[3], d12[3], d21[3], d22[3];
+  int sig_cacb, sig4, sig5;   // sigma axes
+  int nmat;                   // 2 or 4 point material average
+  int m[4][3];                // material offsets
+};
+
+struct Geometry
+{
+  fdtd_config cfg;
+  int n[3];                   // grid size (n[2] = 1 for TMz)
+  int64_t cells;
+  bool tmz;
+  int levels;                 // stored time levels (2, or 3 with metamaterials)
+  double dt, freq, rpv, dx;
+  double a1, a2, a3;
+  double s1, c1, s2, c2;
+  double proj[6];
+  double zero_inc[3];
+  int inc_len;
+  double mod_e, mod_h;        // incident-grid update modifiers
+  CompLayout comp[6];
+  std::vector<double> sigma[3];   // 1-D sigma profiles (zero when PML off)
+  std::vector<TfsfTerm> tfsf;     // every TF/SF correction term
+};
+
+// Builds the geometry; returns an error message or "" on success.
+std::string build_geometry (const fdtd_config &cfg, Geometry &g);
+
+// sin(2 pi f dt t) hard source of the incident grid at time step t.
+double incident_source (const Geometry &g, uint32_t t);
+// point-source value for an E (h = false) or H (h = true) component.
+double point_source (const Geometry &g, uint32_t t, bool h);
+
+}  // namespace fdtdb

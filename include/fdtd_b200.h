@@ -160,6 +160,9 @@ void fdtd_destroy (fdtd_ctx *ctx);
 
 const char *fdtd_status_str (int status);
 
+/* Text of the last error raised on the calling host thread (diagnostics). */
+const char *fdtd_last_error (void);
+
 #ifdef __cplusplus
 }
 #endif
