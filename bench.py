@@ -1,0 +1,382 @@
+"""Benchmark of the B200 FDTD leapfrog step (one JSON line on rank 0).
+
+Workload (N = 1): the 3-D dielectric-sphere case - 512^3 Yee grid, eps = 4
+sphere of radius 0.3*N at the centre (stair-cased on cell centres), PML 16 on
+every face, TF/SF plane wave theta = 30, phi = 45, psi = 0 (TF/SF box inset
+32 cells), dx = 0.5 mm, lambda = 20 mm, Courant 0.5.  Synthetic input
+(seeded, generated here).  One "step" is one leapfrog time step of the whole
+grid.  Fields, PML auxiliaries and eps (~3.7 GB) are far larger than L2, so
+no flush is needed between steps.
+
+  value  : Gcell-updates/s of the chosen form (FP32 fused step), inputs
+           resident in HBM, CUDA events on the library's stream, max over
+           ranks.
+  e2e    : the same metric through the C ABI with host buffers: each e2e
+           step uploads eps from pinned host memory, advances a chunk of
+           time steps and downloads Ez to pinned host memory.
+  roofline: field half-step kernel, algorithmic bytes per launch
+           (cells * B/2, B = 4*(12 + m + 12*f_PML) bytes per cell-update)
+           over its measured average launch time, against the measured
+           HBM copy bandwidth.
+  cpu_baseline: the reference fdtd3d CPU build (oracle/_ref/fdtd3d) on a
+           bounded sample of the same physics (one process).
+
+`--impl reference` runs only the reference CPU build on the host cores
+(concurrent independent processes, one per core used) and prints its line.
+Multi-GPU (--gpus N under torchrun): independent replicas, no collective
+("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gcell-updates/s"
+N_DEFAULT = 512
+PML = 16
+TFSF = 32
+
+
+def workload_kw(n: int, precision: int) -> dict:
+    return dict(mode=3, size=n, use_pml=True, pml=PML, use_tfsf=True, tfsf_left=TFSF, tfsf_right=TFSF,
+                teta=30.0, phi=45.0, psi=0.0, dx=0.0005, wavelength=0.02, courant=0.5, precision=precision)
+
+
+def sphere_eps(n: int) -> np.ndarray:
+    c = (np.arange(n, dtype=np.float64) + 0.5 - n / 2.0) ** 2
+    r2 = (0.3 * n) ** 2
+    eps = np.ones((n, n, n), dtype=np.float64)
+    for i in range(n):
+        inside = (c[i] + c[:, None] + c[None, :]) < r2
+        eps[i][inside] = 4.0
+    return eps
+
+
+def algorithmic_bytes_per_cell(n: int, word: int) -> tuple[float, float]:
+    """B per cell-update: word * (12 + m + 12 f_PML), m = 1 (eps)."""
+    inner = n - 2 * PML
+    f_pml = 1.0 - (inner / n) ** 3
+    return word * (12 + 1 + 12 * f_pml), f_pml
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference_sample(n: int, steps: int, procs: int = 1, timeout: int = 900) -> dict:
+    """Times the reference CPU build on an n^3 sample with the workload's physics.
+
+    Each process prints the reference's own 'Total time' (step loop only).
+    Returns aggregate Gcell-updates/s over `procs` concurrent processes."""
+    from oracle.oracle import REF_BIN, reference_args, write_material_txt
+
+    if not os.path.exists(REF_BIN):
+        raise FileNotFoundError(REF_BIN)
+    kw = workload_kw(n, 0)
+    kw.pop("precision")
+    if n < 2 * TFSF + 16:
+        raise ValueError("reference sample grid must keep the workload's PML 16 and TF/SF 32")
+    with tempfile.TemporaryDirectory() as tmp:
+        epath = os.path.join(tmp, "eps.txt")
+        write_material_txt(epath, sphere_eps(n))
+        args = [REF_BIN] + reference_args(steps=steps, **kw) + ["--load-eps-from-file", epath]
+        ps = []
+        for i in range(procs):
+            d = os.path.join(tmp, f"p{i}")
+            os.makedirs(d)
+            ps.append(subprocess.Popen(args, cwd=d, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True))
+        rates, times = [], []
+        for p in ps:
+            out, _ = p.communicate(timeout=timeout)
+            if p.returncode != 0:
+                raise RuntimeError(f"reference exited {p.returncode}: {out[-500:]}")
+            t = None
+            for line in out.splitlines():
+                if line.startswith("Total time = "):
+                    t = float(line.split("=")[1].split()[0])
+            times.append(t)
+            rates.append(n ** 3 * steps / t / 1e9)
+    return {"value": sum(rates), "per_process": rates, "seconds": times, "grid": n, "steps": steps,
+            "pml": kw["pml"], "tfsf": kw["tfsf_left"]}
+
+
+def reference_arm(args) -> None:
+    """--impl reference: the reference CPU build on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    procs = max(1, min(os.cpu_count() or 1, args.ref_procs))
+    n = args.ref_grid
+    steps = max(1, min(args.steps, args.ref_steps))
+    try:
+        r = run_reference_sample(n, steps, procs=procs)
+    except Exception as e:  # the binary is built in-tree; report why if it is not there
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build could not run: {e}"}))
+        return
+    sample = (f"{procs} concurrent reference processes, each {n}^3 x {steps} steps of the sphere workload "
+              f"(PML {r['pml']}, TF/SF {r['tfsf']}, theta 30, phi 45), --use-ca-cb --use-ca-cb-pml")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": "Gcell-updates/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": 0, "ms_per_step": max(r["seconds"]) * 1e3 / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"3-D dielectric sphere (sample {n}^3 of the 512^3 case)", "grid": n,
+                   "pml": r["pml"], "tfsf_inset": r["tfsf"], "parallelism": f"{procs} CPU processes"},
+        "cpu_baseline": {"value": r["value"], "unit": "Gcell-updates/s", "cores": procs, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": r["value"], "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, default=N_DEFAULT)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16s", "fp64"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-chunk", type=int, default=50)
+    ap.add_argument("--plain-steps", type=int, default=10)
+    ap.add_argument("--ref-grid", type=int, default=96)
+    ap.add_argument("--ref-steps", type=int, default=30)
+    ap.add_argument("--ref-procs", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the plain-FP64 / FP16 side measurements")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+
+    import torch
+
+    import fdtd3d_b200 as fd
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    prec = {"fp32": fd.PREC_FP32, "fp16s": fd.PREC_FP16S, "fp64": fd.PREC_FP64_PLAIN}[args.precision]
+    word = {"fp32": 4, "fp16s": 2, "fp64": 8}[args.precision]
+    n = args.grid
+    cells = n ** 3
+    eps = sphere_eps(n)
+
+    sim = fd.Simulation(device=local, **workload_kw(n, prec))
+    sim.set_material("eps", eps)
+    stream = torch.cuda.ExternalStream(sim.stream, device=local)
+    sim.step(args.warmup)
+    sim.sync()
+
+    # timed region: K time steps, events on the library's stream
+    sim.profile(True)
+    l0 = sim.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        sim.step(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    sim.sync()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    kernel_ms, kernel_launches = sim.kernel_time()
+    sim.profile(False)
+    launches = sim.launch_count() - l0
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * cells * args.steps / (ms * 1e-3) / 1e9
+
+    # roofline of the field half-step kernel
+    peaks = measured_peaks()
+    b_cell, f_pml = algorithmic_bytes_per_cell(n, word)
+    avg_launch_ms = kernel_ms / max(kernel_launches, 1)
+    achieved = cells * b_cell / 2 / (avg_launch_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                "kernel": "field half-step (E or H family)", "avg_launch_ms": avg_launch_ms,
+                "algorithmic_bytes_per_cell_update": b_cell, "f_pml": f_pml,
+                "peak_source": peaks["source"], "kernel_share_of_step": kernel_ms / ms}
+    traffic_file = os.path.join(ROOT, "profiles", f"traffic_{args.precision}.json")
+    if os.path.exists(traffic_file):
+        roofline["traffic"] = json.load(open(traffic_file)).get("bytes_per_launch")
+
+    # e2e through the C ABI with pinned host buffers
+    h_eps = torch.from_numpy(eps.reshape(-1)).pin_memory()
+    h_out = torch.empty(cells, dtype=torch.float64).pin_memory()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    lib = fd.load_library()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        sim._check(lib.fdtd_upload_material(sim._h, 0, h_eps.data_ptr()), "upload_material")
+        sim.step(args.e2e_chunk)
+        sim._check(lib.fdtd_download_field(sim._h, 2, h_out.data_ptr()), "download_field")
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * cells * args.e2e_steps * args.e2e_chunk / (e2e_ms * 1e-3) / 1e9
+    finite = bool(np.isfinite(h_out.numpy()).all())
+    sim.close()
+
+    extras = {}
+    if not args.no_extras and rank == 0:
+        for name, p2, w2 in (("plain_fp64", fd.PREC_FP64_PLAIN, 8), ("fp16_storage", fd.PREC_FP16S, 2)):
+            if p2 == prec:
+                continue
+            s2 = fd.Simulation(device=local, **workload_kw(n, p2))
+            s2.set_material("eps", eps)
+            s2.step(3)
+            s2.sync()
+            st = torch.cuda.ExternalStream(s2.stream, device=local)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            s2.profile(True)
+            a.record(st)
+            s2.step(args.plain_steps)
+            b.record(st)
+            b.synchronize()
+            kms, kl = s2.kernel_time()
+            s2.close()
+            t2 = a.elapsed_time(b)
+            bc, _ = algorithmic_bytes_per_cell(n, w2)
+            extras[name] = {"value": cells * args.plain_steps / (t2 * 1e-3) / 1e9, "unit": METRIC,
+                            "steps": args.plain_steps, "ms_per_step": t2 / args.plain_steps,
+                            "hbm_frac": cells * bc / 2 / (kms / max(kl, 1) * 1e-3) / 1e9 / peaks["hbm_gbs"]}
+        if "plain_fp64" in extras:
+            extras["speedup_vs_plain_fp64"] = value / world / extras["plain_fp64"]["value"]
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            r = run_reference_sample(args.ref_grid, args.ref_steps, procs=1)
+            cpu = {"value": r["value"], "unit": "Gcell-updates/s", "cores": 1, "kind": "reference",
+                   "sample": f"reference CPU build, 1 process, {r['grid']}^3 x {r['steps']} steps of the sphere "
+                             f"workload (PML {r['pml']}, TF/SF {r['tfsf']}), --use-ca-cb --use-ca-cb-pml"}
+        except Exception as e:
+            cpu = {"value": None, "unit": "Gcell-updates/s", "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Gcell-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": {"fp32": "f32", "fp16s": "f16-storage/f32-compute", "fp64": "f64"}[args.precision],
+            "data": "synthetic",
+            "config": {"workload": f"3-D dielectric sphere eps=4 r=0.3N, {n}^3, PML {PML}, TF/SF inset {TFSF}, "
+                                   "theta=30 phi=45 psi=0, dx=0.5mm, lambda=20mm, Courant 0.5",
+                       "grid": n, "form": args.precision, "l2": "inputs larger than L2 (no flush)",
+                       "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "Gcell-updates/s", "h2d_bytes_per_step": cells * 8,
+                    "d2h_bytes_per_step": cells * 8, "time_steps_per_e2e_step": args.e2e_chunk,
+                    "result_finite": finite},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "extras": extras,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

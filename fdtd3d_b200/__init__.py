@@ -32,7 +32,7 @@ EXPORTED = (
     "fdtd_create", "fdtd_upload_material", "fdtd_upload_field", "fdtd_step", "fdtd_sync",
     "fdtd_download_field", "fdtd_upload_material_device", "fdtd_download_field_device",
     "fdtd_reduce", "fdtd_scalars", "fdtd_launch_count", "fdtd_destroy", "fdtd_status_str",
-    "fdtd_last_error",
+    "fdtd_last_error", "fdtd_stream", "fdtd_profile", "fdtd_kernel_time",
 )
 
 
@@ -93,6 +93,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fdtd_destroy": ([vp], None),
         "fdtd_status_str": ([i], ctypes.c_char_p),
         "fdtd_last_error": ([], ctypes.c_char_p),
+        "fdtd_stream": ([vp], vp),
+        "fdtd_profile": ([vp, i], i),
+        "fdtd_kernel_time": ([vp, ctypes.POINTER(d), ctypes.POINTER(i64)], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -209,6 +212,21 @@ class Simulation:
 
     def launch_count(self) -> int:
         return int(self.lib.fdtd_launch_count(self._h))
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of the context (as an integer), for CUDA events."""
+        return int(self.lib.fdtd_stream(self._h) or 0)
+
+    def profile(self, enable: bool = True) -> None:
+        self._check(self.lib.fdtd_profile(self._h, int(enable)), "fdtd_profile")
+
+    def kernel_time(self):
+        """(summed field-kernel milliseconds, timed launches) since the last call."""
+        ms = ctypes.c_double()
+        n = ctypes.c_int64()
+        self._check(self.lib.fdtd_kernel_time(self._h, ctypes.byref(ms), ctypes.byref(n)), "fdtd_kernel_time")
+        return ms.value, n.value
 
     @property
     def handle(self) -> int:

@@ -87,6 +87,11 @@ struct fdtd_ctx
   int nparts = 0;
 
   std::vector<void *> allocs;
+
+  // field-kernel timing
+  bool profiling = false;
+  std::vector<cudaEvent_t> prof_events;   // pairs (start, end)
+  size_t prof_used = 0;                   // events used since the last read
 };
 
 namespace {
@@ -438,6 +443,8 @@ void release (fdtd_ctx *ctx)
   ctx->allocs.clear ();
   if (ctx->h_src)
     cudaFreeHost (ctx->h_src);
+  for (cudaEvent_t e : ctx->prof_events)
+    cudaEventDestroy (e);
   if (ctx->src_ev)
     cudaEventDestroy (ctx->src_ev);
   if (ctx->stream)
@@ -502,6 +509,30 @@ PlainHalf plain_half (fdtd_ctx *ctx, int h)
   return p;
 }
 
+int prof_begin (fdtd_ctx *ctx, cudaEvent_t *end_out)
+{
+  *end_out = nullptr;
+  if (!ctx->profiling)
+    return FDTD_OK;
+  while (ctx->prof_events.size () < ctx->prof_used + 2)
+  {
+    cudaEvent_t e;
+    CK (cudaEventCreate (&e));
+    ctx->prof_events.push_back (e);
+  }
+  CK (cudaEventRecord (ctx->prof_events[ctx->prof_used], ctx->stream));
+  *end_out = ctx->prof_events[ctx->prof_used + 1];
+  ctx->prof_used += 2;
+  return FDTD_OK;
+}
+
+int prof_end (fdtd_ctx *ctx, cudaEvent_t end)
+{
+  if (end)
+    CK (cudaEventRecord (end, ctx->stream));
+  return FDTD_OK;
+}
+
 int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
 {
   const Geometry &g = ctx->g;
@@ -547,7 +578,12 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
         if (t > 0)
         {
           PlainHalf p = plain_half (ctx, h);
+          cudaEvent_t pe;
+          if ((r = prof_begin (ctx, &pe)) != FDTD_OK)
+            return r;
           ctx->launches += launch_plain_half (p, g.inc_len, ctx->d_err, ctx->sm_count, s);
+          if ((r = prof_end (ctx, pe)) != FDTD_OK)
+            return r;
         }
         for (int ci = 0; ci < 3; ++ci)
         {
@@ -572,7 +608,12 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
           FastHalf &p = h ? ctx->fast_h : ctx->fast_e;
           p.inc = h ? ctx->einc[ctx->ecur] : ctx->hinc[ctx->hcur];
           p.mat = ctx->mat32[h];
+          cudaEvent_t pe;
+          if ((r = prof_begin (ctx, &pe)) != FDTD_OK)
+            return r;
           ctx->launches += launch_fast_half (p, ctx->d_err, ctx->sm_count, s);
+          if ((r = prof_end (ctx, pe)) != FDTD_OK)
+            return r;
         }
         for (int ci = 0; ci < 3; ++ci)
         {
@@ -862,6 +903,45 @@ int fdtd_scalars (const fdtd_ctx *ctx, double out[3])
 int64_t fdtd_launch_count (const fdtd_ctx *ctx)
 {
   return ctx ? ctx->launches : -1;
+}
+
+void *fdtd_stream (const fdtd_ctx *ctx)
+{
+  return ctx ? (void *) ctx->stream : nullptr;
+}
+
+int fdtd_profile (fdtd_ctx *ctx, int enable)
+{
+  if (!ctx)
+    return FDTD_ERR_ARG;
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  CK (cudaStreamSynchronize (ctx->stream));
+  ctx->profiling = enable != 0;
+  ctx->prof_used = 0;
+  return FDTD_OK;
+}
+
+int fdtd_kernel_time (fdtd_ctx *ctx, double *ms, int64_t *launches)
+{
+  if (!ctx || !ms || !launches)
+    return FDTD_ERR_ARG;
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  CK (cudaStreamSynchronize (ctx->stream));
+  double total = 0.0;
+  for (size_t i = 0; i + 1 < ctx->prof_used; i += 2)
+  {
+    float t = 0.f;
+    CK (cudaEventElapsedTime (&t, ctx->prof_events[i], ctx->prof_events[i + 1]));
+    total += t;
+  }
+  *ms = total;
+  *launches = (int64_t) (ctx->prof_used / 2);
+  ctx->prof_used = 0;
+  return FDTD_OK;
 }
 
 void fdtd_destroy (fdtd_ctx *ctx)

@@ -154,6 +154,19 @@ int fdtd_scalars (const fdtd_ctx *ctx, double out[3]);
 /* Number of kernel launches this context issued so far. */
 int64_t fdtd_launch_count (const fdtd_ctx *ctx);
 
+/* The cudaStream_t (as void *) every launch of this context goes to, so a
+ * caller can order its own work or record CUDA events against it. */
+void *fdtd_stream (const fdtd_ctx *ctx);
+
+/* Field-kernel timing (no reference counterpart; the reference only prints
+ * wall-clock "Total time", Source/main.cpp:1175-1213).  While enabled, every
+ * field half-step launch is bracketed by CUDA events on the context stream.
+ * fdtd_kernel_time waits for the stream, then returns the summed kernel
+ * milliseconds and the number of timed launches since the last call (or
+ * since enabling), and resets both. */
+int fdtd_profile (fdtd_ctx *ctx, int enable);
+int fdtd_kernel_time (fdtd_ctx *ctx, double *ms, int64_t *launches);
+
 /* Releases every device resource of the context; replaces
  * InternalSchemeGPU::uninitFromCPU/uninitOnGPU. */
 void fdtd_destroy (fdtd_ctx *ctx);

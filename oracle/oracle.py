@@ -85,9 +85,10 @@ def lib() -> ctypes.CDLL:
 def _triple(v, default):
     if v is None:
         return (default,) * 3
-    if isinstance(v, int):
-        return (v, v, v)
-    return tuple(v)
+    if isinstance(v, (int, np.integer)):
+        return (int(v),) * 3
+    v = tuple(int(a) for a in v)
+    return v + (default,) * (3 - len(v))
 
 
 class Oracle:
@@ -110,7 +111,7 @@ class Oracle:
         c.dx, c.wavelength, c.courant = f32(dx), f32(wavelength), f32(courant)
         c.angle_teta, c.angle_phi, c.angle_psi = f32(teta), f32(phi), f32(psi)
         c.use_pml, c.use_tfsf, c.use_metamaterials = int(use_pml), int(use_tfsf), int(use_metamaterials)
-        c.point_source[:] = tuple(point_source)
+        c.point_source[:] = _triple(point_source, 0)
         c.point_source_mask = point_source_mask
         c.skip_first_update = int(skip_first_update)
         self.cfg = c
