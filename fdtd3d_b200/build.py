@@ -8,6 +8,7 @@ Translation units and flags:
   csrc/fast_kernels.cu    nvcc                          FP32 / FP16-storage fused form, reductions
   csrc/fused3d.cu         nvcc                          3-D single-sweep E+H kernel
   csrc/fdtd_api.cu        nvcc                          C ABI, context, launch sequence
+  csrc/cli.cpp            g++ -> fdtd3d-b200            command-line drop-in over the C ABI
 """
 from __future__ import annotations
 
@@ -22,6 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfdtd_b200.so")
+CLI = os.path.join(HERE, "fdtd3d-b200")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -83,6 +85,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if r.returncode != 0:
         raise RuntimeError(f"link failed: {' '.join(link)}\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, LIB)
+    # the command-line drop-in, linked against the library next to it
+    cli = ["g++", "-O2", "-std=c++17", os.path.join(CSRC, "cli.cpp"), "-o", CLI + ".tmp", "-L", HERE,
+           "-lfdtd_b200", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cli, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"cli build failed: {' '.join(cli)}\n{r.stdout}\n{r.stderr}")
+    os.replace(CLI + ".tmp", CLI)
     return LIB
 
 

@@ -1,0 +1,386 @@
+// cli.cpp - fdtd3d-b200: command-line drop-in for fdtd3d's step path.
+//
+// Accepts fdtd3d's own flags for the modes this library provides
+// (Source/Settings/Settings.inc.h; coordinate syntax "x:N,y:N,z:N",
+// Source/Settings/Settings.cpp:74-131; float flags parsed with std::stof as
+// the reference does, Settings.cpp:186-191), runs the time loop through the
+// C ABI and writes the reference's outputs: "Total time = ... seconds"
+// around the step loop (Source/main.cpp:1175-1213) and --save-as-txt dumps
+// named previous-1_[timestep=T]_[pid=0]_[name=F].txt with 15 significant
+// digits (Source/File-Management/Commons.h:63-120,
+// Source/File-Management/Dumper/TXTDumper.h:60-84).  The default save region
+// is the reference's: the whole grid, one z slice at size/2 in 3-D
+// (Source/Scheme/SchemeHelper.h:870-889).
+//
+// Extra flag: --precision fp64|fp32|fp16s (default fp64 = the plain form).
+// Flags of subsystems outside the step path (MPI, NTFF, BMP/DAT output,
+// test callbacks) are rejected with a message instead of being ignored.
+#include <sys/time.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <limits>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/fdtd_b200.h"
+
+namespace {
+
+struct Opts
+{
+  fdtd_config cfg;
+  int steps = 100;
+  bool same_size = false, same_pml = false, same_tfsf = false;
+  bool save_res = false, save_txt = false, manual = false;
+  int save_start[3] = {0, 0, 0}, save_end[3] = {0, 0, 0};
+  std::string mat_file[6];
+  int device = 0;
+};
+
+int fail (const std::string &m)
+{
+  std::fprintf (stderr, "fdtd3d-b200: %s\n", m.c_str ());
+  return 1;
+}
+
+bool parse_coord (const std::string &s, int out[3])
+{
+  std::stringstream ss (s);
+  std::string tok;
+  while (std::getline (ss, tok, ','))
+  {
+    if (tok.size () < 3 || tok[1] != ':')
+      return false;
+    int axis = tok[0] == 'x' ? 0 : (tok[0] == 'y' ? 1 : (tok[0] == 'z' ? 2 : -1));
+    if (axis < 0)
+      return false;
+    out[axis] = std::atoi (tok.c_str () + 2);
+  }
+  return true;
+}
+
+double stof_like (const std::string &s)
+{
+  return (double) std::stof (s);
+}
+
+std::vector<std::string> read_cmd_file (const std::string &path)
+{
+  std::vector<std::string> out;
+  std::ifstream f (path);
+  std::string line;
+  while (std::getline (f, line))
+  {
+    size_t b = line.find_first_not_of (" \t\r");
+    if (b == std::string::npos)
+      continue;
+    line = line.substr (b);
+    if (line[0] == '#' || line.compare (0, 2, "//") == 0)
+      continue;
+    size_t e = line.find_last_not_of (" \t\r");
+    out.push_back (line.substr (0, e + 1));
+  }
+  return out;
+}
+
+int parse (std::vector<std::string> args, Opts &o)
+{
+  std::memset (&o.cfg, 0, sizeof (o.cfg));
+  fdtd_config &c = o.cfg;
+  c.mode = FDTD_MODE_DIM3;
+  for (int a = 0; a < 3; ++a)
+  {
+    c.size[a] = 100;
+    c.pml[a] = 2;
+    c.tfsf_left[a] = 4;
+    c.tfsf_right[a] = 4;
+  }
+  c.dx = stof_like ("0.0005");
+  c.wavelength = stof_like ("0.02");
+  c.courant = stof_like ("0.5");
+  c.angle_teta = 90.0;
+  c.angle_phi = 0.0;
+  c.angle_psi = 90.0;
+  c.precision = FDTD_PREC_FP64_PLAIN;
+  static const char *mat_flags[6] = {"--load-eps-from-file", "--load-mu-from-file", "--load-omegape-from-file",
+                                     "--load-omegapm-from-file", "--load-gammae-from-file",
+                                     "--load-gammam-from-file"};
+  static const char *ps_flags[6] = {"--point-source-ex", "--point-source-ey", "--point-source-ez",
+                                    "--point-source-hx", "--point-source-hy", "--point-source-hz"};
+  static const char *ignored[] = {"--use-ca-cb", "--use-ca-cb-pml", "--use-ca-cb-pml-metamaterials", "--use-cuda",
+                                  "--same-size-ntff", nullptr};
+  static const char *ignored_arg[] = {"--log-level", "--cuda-buffer-size", "--num-cuda-threads", "--layout-type",
+                                      nullptr};
+  for (size_t i = 0; i < args.size (); ++i)
+  {
+    const std::string &a = args[i];
+    auto next = [&] (std::string &v) -> bool {
+      if (i + 1 >= args.size ())
+        return false;
+      v = args[++i];
+      return true;
+    };
+    std::string v;
+    bool handled = true;
+    if (a == "--3d")
+      c.mode = FDTD_MODE_DIM3;
+    else if (a == "--2d-tmz")
+      c.mode = FDTD_MODE_TMZ;
+    else if (a == "--size" && next (v))
+    {
+      if (!parse_coord (v, c.size))
+        return fail ("bad --size");
+    }
+    else if (a == "--same-size")
+      o.same_size = true;
+    else if (a == "--pml-size" && next (v))
+    {
+      if (!parse_coord (v, c.pml))
+        return fail ("bad --pml-size");
+    }
+    else if (a == "--same-size-pml")
+      o.same_pml = true;
+    else if (a == "--tfsf-size-left" && next (v))
+    {
+      if (!parse_coord (v, c.tfsf_left))
+        return fail ("bad --tfsf-size-left");
+    }
+    else if (a == "--tfsf-size-right" && next (v))
+    {
+      if (!parse_coord (v, c.tfsf_right))
+        return fail ("bad --tfsf-size-right");
+    }
+    else if (a == "--same-size-tfsf")
+      o.same_tfsf = true;
+    else if (a == "--time-steps" && next (v))
+      o.steps = std::atoi (v.c_str ());
+    else if (a == "--angle-teta" && next (v))
+      c.angle_teta = stof_like (v);
+    else if (a == "--angle-phi" && next (v))
+      c.angle_phi = stof_like (v);
+    else if (a == "--angle-psi" && next (v))
+      c.angle_psi = stof_like (v);
+    else if (a == "--dx" && next (v))
+      c.dx = stof_like (v);
+    else if (a == "--wavelength" && next (v))
+      c.wavelength = stof_like (v);
+    else if (a == "--courant-factor" && next (v))
+      c.courant = stof_like (v);
+    else if (a == "--use-pml")
+      c.use_pml = 1;
+    else if (a == "--use-tfsf")
+      c.use_tfsf = 1;
+    else if (a == "--use-metamaterials")
+      c.use_metamaterials = 1;
+    else if (a == "--point-source" && next (v))
+    {
+      if (!parse_coord (v, c.point_source))
+        return fail ("bad --point-source");
+    }
+    else if (a == "--save-res")
+      o.save_res = true;
+    else if (a == "--save-as-txt")
+      o.save_txt = true;
+    else if (a == "--manual-save-coords")
+      o.manual = true;
+    else if (a == "--save-start-coord" && next (v))
+    {
+      if (!parse_coord (v, o.save_start))
+        return fail ("bad --save-start-coord");
+    }
+    else if (a == "--save-end-coord" && next (v))
+    {
+      if (!parse_coord (v, o.save_end))
+        return fail ("bad --save-end-coord");
+    }
+    else if (a == "--cuda-gpus" && next (v))
+      o.device = std::atoi (v.c_str ());
+    else if (a == "--precision" && next (v))
+    {
+      if (v == "fp64")
+        c.precision = FDTD_PREC_FP64_PLAIN;
+      else if (v == "fp32")
+        c.precision = FDTD_PREC_FP32;
+      else if (v == "fp16s")
+        c.precision = FDTD_PREC_FP16S;
+      else
+        return fail ("--precision must be fp64, fp32 or fp16s");
+    }
+    else if (a == "--cmd-from-file" && next (v))
+    {
+      std::vector<std::string> more = read_cmd_file (v);
+      args.insert (args.begin () + i + 1, more.begin (), more.end ());
+    }
+    else
+      handled = false;
+    if (handled)
+      continue;
+    bool done = false;
+    for (int m = 0; m < 6 && !done; ++m)
+    {
+      if (a == mat_flags[m] && next (v))
+      {
+        o.mat_file[m] = v;
+        done = true;
+      }
+      else if (a == ps_flags[m])
+      {
+        c.point_source_mask |= 1 << m;
+        done = true;
+      }
+    }
+    for (int m = 0; ignored[m] && !done; ++m)
+      done = a == ignored[m];
+    for (int m = 0; ignored_arg[m] && !done; ++m)
+    {
+      if (a == ignored_arg[m])
+      {
+        if (a == "--layout-type" && next (v) && std::atoi (v.c_str ()) != 0)
+          return fail ("only --layout-type 0 (E_CENTERED) is provided");
+        else if (a != "--layout-type")
+          next (v);
+        done = true;
+      }
+    }
+    if (!done)
+      return fail ("unsupported flag " + a + " (outside the step path this binary provides)");
+  }
+  for (int a = 1; a < 3; ++a)
+  {
+    if (o.same_size)
+      c.size[a] = c.size[0];
+    if (o.same_pml)
+      c.pml[a] = c.pml[0];
+    if (o.same_tfsf)
+    {
+      c.tfsf_left[a] = c.tfsf_left[0];
+      c.tfsf_right[a] = c.tfsf_right[0];
+    }
+  }
+  if (c.mode == FDTD_MODE_TMZ)
+    c.size[2] = 1;
+  return 0;
+}
+
+// TXT grid loader: "x y [z] value" per line, z fastest; values through stof
+// (Source/File-Management/Loader/TXTLoader.h:60-100).
+bool load_txt (const std::string &path, size_t n, int coords, std::vector<double> &out)
+{
+  std::ifstream f (path);
+  if (!f)
+    return false;
+  out.assign (n, 0.0);
+  std::string line;
+  size_t i = 0;
+  while (i < n && std::getline (f, line))
+  {
+    std::stringstream ss (line);
+    std::string tok;
+    for (int k = 0; k <= coords; ++k)
+      ss >> tok;
+    out[i++] = (double) std::stof (tok);
+  }
+  return i == n;
+}
+
+bool save_txt (const std::string &name, const std::vector<double> &v, const int n[3], bool tmz, const int lo[3],
+               const int hi[3])
+{
+  std::ofstream f (name);
+  if (!f)
+    return false;
+  f << std::setprecision (std::numeric_limits<double>::digits10);
+  for (int x = lo[0]; x < hi[0]; ++x)
+    for (int y = lo[1]; y < hi[1]; ++y)
+      for (int z = lo[2]; z < hi[2]; ++z)
+      {
+        size_t id = ((size_t) x * n[1] + y) * n[2] + z;
+        if (tmz)
+          f << x << " " << y << " " << v[id] << std::endl;
+        else
+          f << x << " " << y << " " << z << " " << v[id] << std::endl;
+      }
+  return true;
+}
+
+}  // namespace
+
+int main (int argc, char **argv)
+{
+  Opts o;
+  std::vector<std::string> args (argv + 1, argv + argc);
+  if (parse (args, o))
+    return 1;
+  fdtd_ctx *ctx = nullptr;
+  int st = fdtd_create (&o.cfg, o.device, &ctx);
+  if (st)
+    return fail (std::string ("fdtd_create: ") + fdtd_status_str (st) + ": " + fdtd_last_error ());
+  bool tmz = o.cfg.mode == FDTD_MODE_TMZ;
+  int n[3] = {o.cfg.size[0], o.cfg.size[1], tmz ? 1 : o.cfg.size[2]};
+  size_t cells = (size_t) n[0] * n[1] * n[2];
+  for (int m = 0; m < 6; ++m)
+  {
+    if (o.mat_file[m].empty ())
+      continue;
+    std::vector<double> a;
+    if (!load_txt (o.mat_file[m], cells, tmz ? 2 : 3, a))
+      return fail ("cannot read " + o.mat_file[m]);
+    st = fdtd_upload_material (ctx, m, a.data ());
+    if (st)
+      return fail (std::string ("fdtd_upload_material: ") + fdtd_last_error ());
+  }
+  struct timeval tv1, tv2;
+  gettimeofday (&tv1, nullptr);
+  st = fdtd_step (ctx, 0, (uint32_t) o.steps);
+  if (!st)
+    st = fdtd_sync (ctx, -1);
+  gettimeofday (&tv2, nullptr);
+  if (st)
+    return fail (std::string ("step: ") + fdtd_status_str (st) + ": " + fdtd_last_error ());
+  std::printf ("Total time = %f seconds\n",
+               (double) (tv2.tv_usec - tv1.tv_usec) / 1000000 + (double) (tv2.tv_sec - tv1.tv_sec));
+  if (o.save_res && o.save_txt)
+  {
+    static const char *names[6] = {"Ex", "Ey", "Ez", "Hx", "Hy", "Hz"};
+    int lo[3] = {0, 0, 0}, hi[3] = {n[0], n[1], n[2]};
+    if (o.manual)
+    {
+      for (int a = 0; a < 3; ++a)
+      {
+        lo[a] = o.save_start[a];
+        hi[a] = o.save_end[a];
+      }
+      if (tmz)
+      {
+        lo[2] = 0;
+        hi[2] = 1;
+      }
+    }
+    else if (!tmz)
+    {
+      lo[2] = n[2] / 2;
+      hi[2] = n[2] / 2 + 1;
+    }
+    std::vector<double> buf (cells);
+    for (int k = 0; k < 6; ++k)
+    {
+      if (tmz && k != FDTD_EZ && k != FDTD_HX && k != FDTD_HY)
+        continue;
+      st = fdtd_download_field (ctx, k, buf.data ());
+      if (st)
+        return fail (std::string ("download: ") + fdtd_last_error ());
+      std::string fname = "previous-1_[timestep=" + std::to_string (o.steps) + "]_[pid=0]_[name=" + names[k] + "].txt";
+      if (!save_txt (fname, buf, n, tmz, lo, hi))
+        return fail ("cannot write " + fname);
+    }
+  }
+  fdtd_destroy (ctx);
+  return 0;
+}

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/fdtd_b200.h"
+#include "fused3d.h"
 #include "kernels.h"
 #include "setup.h"
 
@@ -73,13 +74,21 @@ struct fdtd_ctx
   double *mat64[6] = {};
   double *sig64[3] = {};
 
-  // fused forms
+  // fused forms: two buffer sets; set fcur holds the current time level.
+  // The per-cell path updates set fcur in place; the one-sweep 3-D kernel
+  // reads set fcur and writes set 1 - fcur.
+  void *ffb[2][6] = {};
+  float *auxb[2][6] = {};
+  int fcur = 0;
+  bool has_second = false;
   void *ff[6] = {};
   float *aux[6] = {};
   float *mat32[2] = {};
   float *tabs = nullptr;
   size_t tab_off[6][6] = {};
   FastHalf fast_e, fast_h;
+  FusedParams fused;
+  bool ps_interior = true;
 
   double *staging = nullptr;
   double *partials = nullptr;
@@ -307,13 +316,22 @@ int alloc_fast (fdtd_ctx *ctx)
   size_t n = (size_t) g.cells;
   if (g.cfg.use_metamaterials)
     return fail (ctx, FDTD_ERR_UNSUPPORTED, "metamaterials are provided by the FP64 plain form only");
+  ctx->has_second = !g.tmz;
+  for (int b = 0; b < (ctx->has_second ? 2 : 1); ++b)
+  {
+    for (int k = 0; k < 6; ++k)
+    {
+      if (!g.comp[k].exists)
+        continue;
+      DALLOC (ctx->ffb[b][k], n * elem_size (ctx->kind));
+      if (g.cfg.use_pml)
+        DALLOC (ctx->auxb[b][k], n * sizeof (float));
+    }
+  }
   for (int k = 0; k < 6; ++k)
   {
-    if (!g.comp[k].exists)
-      continue;
-    DALLOC (ctx->ff[k], n * elem_size (ctx->kind));
-    if (g.cfg.use_pml)
-      DALLOC (ctx->aux[k], n * sizeof (float));
+    ctx->ff[k] = ctx->ffb[0][k];
+    ctx->aux[k] = ctx->auxb[0][k];
   }
   // 1-D coefficient tables per component (see fast_kernels.cu)
   std::vector<float> tabs;
@@ -393,6 +411,102 @@ int alloc_fast (fdtd_ctx *ctx)
   return FDTD_OK;
 }
 
+// Points ff/aux and the per-cell kernel parameters at buffer set fcur.
+void select_fast_set (fdtd_ctx *ctx)
+{
+  for (int k = 0; k < 6; ++k)
+  {
+    ctx->ff[k] = ctx->ffb[ctx->fcur][k];
+    ctx->aux[k] = ctx->auxb[ctx->fcur][k];
+  }
+  for (int h = 0; h < 2; ++h)
+  {
+    FastHalf &p = h ? ctx->fast_h : ctx->fast_e;
+    for (int ci = 0; ci < 3; ++ci)
+    {
+      p.f[ci] = ctx->ff[ci + 3 * h];
+      p.aux[ci] = ctx->aux[ci + 3 * h];
+      p.opp[ci] = ctx->ff[ci + 3 * (1 - h)];
+    }
+  }
+}
+
+void init_fused (fdtd_ctx *ctx)
+{
+  const Geometry &g = ctx->g;
+  FusedParams &f = ctx->fused;
+  std::memset (&f, 0, sizeof (f));
+  f.g = make_geom_dev (g);
+  f.use_pml = g.cfg.use_pml;
+  f.use_tfsf = g.cfg.use_tfsf;
+  f.fp16 = ctx->kind == 2;
+  f.courant = ctx->fast_e.courant;
+  for (int k = 0; k < 6; ++k)
+  {
+    f.inc_scale[k] = ctx->fast_e.inc_scale[k];
+    f.comp[k] = make_comp_dev (g, k);
+    const FastHalf &h = k >= 3 ? ctx->fast_h : ctx->fast_e;
+    for (int j = 0; j < 6; ++j)
+      f.tab[k][j] = h.tab[k % 3][j];
+    for (int a = 0; a < 3; ++a)
+    {
+      f.ilo[k][a] = h.ilo[k % 3][a];
+      f.ihi[k][a] = h.ihi[k % 3][a];
+    }
+  }
+  // TF/SF face planes for the kernel's quick rejection: every term box is
+  // one cell thick along some axis; a cell can only need a correction when
+  // its coordinate equals one of those planes
+  int nf[3] = {0, 0, 0};
+  for (int a = 0; a < 3; ++a)
+    for (int j = 0; j < 4; ++j)
+      f.face[a][j] = -1;
+  bool overflow = false;
+  for (const TfsfTerm &t : g.tfsf)
+  {
+    int best = 0;
+    for (int a = 1; a < 3; ++a)
+      if (t.hi[a] - t.lo[a] < t.hi[best] - t.lo[best])
+        best = a;
+    if (t.hi[best] - t.lo[best] != 1)
+    {
+      overflow = true;
+      continue;
+    }
+    bool seen = false;
+    for (int j = 0; j < nf[best]; ++j)
+      seen = seen || f.face[best][j] == t.lo[best];
+    if (seen)
+      continue;
+    if (nf[best] == 4)
+    {
+      overflow = true;
+      continue;
+    }
+    f.face[best][nf[best]++] = t.lo[best];
+  }
+  if (overflow)
+  {
+    // no quick rejection possible: make every y coordinate a face plane
+    // would need more slots, so fall back to the per-cell kernel instead
+    ctx->has_second = false;
+  }
+  f.inc_len = g.inc_len;
+  int tiles = ((g.n[2] - 2 + 31) / 32) * ((g.n[1] - 2 + 7) / 8);
+  int64_t want = (int64_t) ctx->sm_count * 3 * 8;
+  int64_t chunk = ((int64_t) (g.n[0] - 2) * tiles) / std::max<int64_t> (want, 1);
+  f.x_chunk = (int) std::min<int64_t> (128, std::max<int64_t> (16, chunk));
+  const int *ps = g.cfg.point_source;
+  f.ps_mask = g.cfg.point_source_mask;
+  for (int a = 0; a < 3; ++a)
+    f.ps[a] = ps[a];
+  ctx->ps_interior = true;
+  if (f.ps_mask)
+    for (int a = 0; a < 3; ++a)
+      ctx->ps_interior = ctx->ps_interior && ps[a] >= 1 && ps[a] <= g.n[a] - 2;
+  f.ps_scale_h = (float) kEta0;
+}
+
 int create_impl (const fdtd_config *cfg, int device, fdtd_ctx *ctx)
 {
   std::string err = build_geometry (*cfg, ctx->g);
@@ -427,6 +541,11 @@ int create_impl (const fdtd_config *cfg, int device, fdtd_ctx *ctx)
   int r = ctx->kind == 0 ? alloc_plain (ctx) : alloc_fast (ctx);
   if (r != FDTD_OK)
     return r;
+  if (ctx->kind != 0)
+  {
+    select_fast_set (ctx);
+    init_fused (ctx);
+  }
   CK (cudaStreamSynchronize (ctx->stream));
   return FDTD_OK;
 }
@@ -552,10 +671,53 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
   size_t ps_idx = 0;
   bool ps_ok = g.cfg.point_source_mask && point_source_index (g, &ps_idx);
   cudaStream_t s = ctx->stream;
+  const bool fused = ctx->kind != 0 && ctx->has_second && !ctx->mat32[1] && ctx->ps_interior;
 
   for (uint32_t i = 0; i < n; ++i)
   {
     uint32_t t = t_start + i;
+    if (fused && t > 0)
+    {
+      // incident E then H steps, then one sweep for both field families
+      int hprev = ctx->hcur;
+      if (g.cfg.use_tfsf)
+      {
+        ctx->launches += launch_incident_e (ctx->einc[1 - ctx->ecur], ctx->einc[ctx->ecur], ctx->hinc[ctx->hcur],
+                                            g.inc_len, g.mod_e, ctx->d_src, 3 * i, s);
+        ctx->ecur ^= 1;
+        ctx->launches += launch_incident_h (ctx->hinc[1 - ctx->hcur], ctx->hinc[ctx->hcur], ctx->einc[ctx->ecur],
+                                            g.inc_len, g.mod_h, s);
+        ctx->hcur ^= 1;
+      }
+      FusedParams &f = ctx->fused;
+      int o = ctx->fcur, nw = 1 - ctx->fcur;
+      for (int c = 0; c < 3; ++c)
+      {
+        f.e_old[c] = ctx->ffb[o][c];
+        f.h_old[c] = ctx->ffb[o][c + 3];
+        f.e_new[c] = ctx->ffb[nw][c];
+        f.h_new[c] = ctx->ffb[nw][c + 3];
+      }
+      for (int k = 0; k < 6; ++k)
+      {
+        f.aux_old[k] = ctx->auxb[o][k];
+        f.aux_new[k] = ctx->auxb[nw][k];
+      }
+      f.eps = ctx->mat32[0];
+      f.inc_h = ctx->hinc[hprev];
+      f.inc_e = ctx->einc[ctx->ecur];
+      f.src = ctx->d_src;
+      f.src_index = 3 * i + 1;
+      cudaEvent_t pe;
+      if ((r = prof_begin (ctx, &pe)) != FDTD_OK)
+        return r;
+      ctx->launches += launch_fused3d (f, ctx->d_err, s);
+      if ((r = prof_end (ctx, pe)) != FDTD_OK)
+        return r;
+      ctx->fcur = nw;
+      select_fast_set (ctx);
+      continue;
+    }
     for (int h = 0; h < 2; ++h)
     {
       if (g.cfg.use_tfsf)
@@ -729,8 +891,11 @@ int fdtd_upload_field (fdtd_ctx *ctx, int component, const double *host)
     if ((r = ensure_staging (ctx)) != FDTD_OK)
       return r;
     CK (cudaMemcpyAsync (ctx->staging, host, n * sizeof (double), cudaMemcpyHostToDevice, ctx->stream));
-    ctx->launches += launch_convert_in (ctx->ff[component], ctx->kind, ctx->staging, n,
-                                        component >= 3 ? kEta0 : 1.0, ctx->stream);
+    // both buffer sets: cells the step never updates must keep these values
+    for (int b = 0; b < 2; ++b)
+      if (ctx->ffb[b][component])
+        ctx->launches += launch_convert_in (ctx->ffb[b][component], ctx->kind, ctx->staging, n,
+                                            component >= 3 ? kEta0 : 1.0, ctx->stream);
   }
   CK (cudaStreamSynchronize (ctx->stream));
   return FDTD_OK;

@@ -31,6 +31,15 @@ CASES = {
                          teta=90, phi=30, psi=90),
     "tmz_point_source": dict(mode=2, size=(33, 30), point_source=(15, 14), point_source_mask=1 << 2,
                              teta=90, phi=0, psi=90),
+    # non-uniform mu and a point source on the outer shell take the per-cell
+    # kernels of the fused forms instead of the one-sweep 3-D kernel
+    "dim3_mu_per_cell": dict(mode=3, size=(15, 17, 14), use_pml=True, pml=3, use_tfsf=True, tfsf_left=5,
+                             tfsf_right=5, teta=60, phi=20, psi=45),
+    "dim3_boundary_source": dict(mode=3, size=14, point_source=(0, 7, 7), point_source_mask=1 << 1,
+                                 teta=0, phi=0, psi=0),
+    "dim3_large_tiles": dict(mode=3, size=(40, 37, 70), use_pml=True, pml=(5, 4, 6), use_tfsf=True,
+                             tfsf_left=(9, 8, 12), tfsf_right=(10, 9, 11), teta=30, phi=45, psi=0,
+                             point_source=(20, 18, 35), point_source_mask=(1 << 0) | (1 << 5)),
 }
 
 
@@ -47,6 +56,11 @@ def materials(name, shape):
         return {"omegape": om, "gammae": ga, "omegapm": om, "gammam": ga}
     if name == "tmz_pml_tfsf":
         return {"eps": np.round(rng.uniform(1, 12, shape)).astype(np.float64)}
+    if name == "dim3_mu_per_cell":
+        return {"eps": np.round(rng.uniform(1, 6, shape)), "mu": np.round(rng.uniform(1, 3, shape))}
+    if name == "dim3_large_tiles":
+        x, y, z = np.indices(shape)
+        return {"eps": np.where((x - 20) ** 2 + (y - 18) ** 2 + (z - 35) ** 2 < 64, 4.0, 1.0)}
     return None
 
 
@@ -104,7 +118,8 @@ def test_plain_fp64_config1_full(fdtd):
 
 
 @pytest.mark.parametrize("name", ["dim3_point_source", "dim3_tfsf_axis", "dim3_pml_tfsf_oblique",
-                                  "dim3_pml_only", "tmz_pml_tfsf", "tmz_point_source"])
+                                  "dim3_pml_only", "tmz_pml_tfsf", "tmz_point_source", "dim3_mu_per_cell",
+                                  "dim3_boundary_source", "dim3_large_tiles"])
 @pytest.mark.parametrize("prec,tol", [(1, 1e-5), (2, 2e-2)])
 def test_fused_forms_match_fp64(fdtd, name, prec, tol):
     pairs = run_pair(fdtd, name, 40, prec)
@@ -160,3 +175,32 @@ def test_sync_with_timeout_returns(fdtd):
 def test_unsupported_combination_is_reported(fdtd):
     with pytest.raises(fdtd.FdtdError):
         fdtd.Simulation(mode=3, size=12, use_pml=True, pml=2, use_metamaterials=True, precision=1)
+
+
+def test_cli_dropin_matches_reference_txt(fdtd, tmp_path):
+    """fdtd3d-b200 takes the reference's flags and writes the same TXT dumps as
+    the reference CPU build (oracle/_ref/fdtd3d) for the same run."""
+    import subprocess
+
+    from oracle.oracle import REF_BIN
+
+    if not os.path.exists(REF_BIN):
+        pytest.skip("reference binary not built")
+    cli = os.path.join(os.path.dirname(fdtd.__file__), "fdtd3d-b200")
+    flags = ["--3d", "--size", "x:18,y:16,z:20", "--use-pml", "--pml-size", "x:3", "--same-size-pml",
+             "--use-tfsf", "--tfsf-size-left", "x:5", "--same-size-tfsf", "--tfsf-size-right", "x:5",
+             "--angle-teta", "30", "--angle-phi", "45", "--angle-psi", "10", "--dx", "0.0005",
+             "--wavelength", "0.02", "--courant-factor", "0.5", "--time-steps", "25", "--save-res",
+             "--save-as-txt", "--manual-save-coords", "--save-start-coord", "x:0,y:0,z:0",
+             "--save-end-coord", "x:18,y:16,z:20"]
+    out = {}
+    for name, exe, extra in (("ref", REF_BIN, ["--use-ca-cb", "--use-ca-cb-pml"]), ("b200", cli, [])):
+        d = tmp_path / name
+        d.mkdir()
+        r = subprocess.run([exe] + flags + extra, cwd=d, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+        assert "Total time = " in r.stdout
+        out[name] = {f.name: f.read_text() for f in d.iterdir()}
+    assert sorted(out["ref"]) == sorted(out["b200"])
+    for fname, text in out["ref"].items():
+        assert out["b200"][fname] == text, fname
