@@ -46,7 +46,7 @@ def _units():
     ]
     if os.path.exists(os.path.join(CSRC, "fused3d.cu")):
         units.append(("fused3d.cu", [nvcc] + common))
-    for extra in ("tmz_batch.cu", "adjoint.cu"):
+    for extra in ("tmz_batch.cu", "adjoint.cu", "noalloc.cu"):
         if os.path.exists(os.path.join(CSRC, extra)):
             units.append((extra, [nvcc] + common))
     return units

@@ -171,6 +171,22 @@ int fdtd_kernel_time (fdtd_ctx *ctx, double *ms, int64_t *launches);
  * InternalSchemeGPU::uninitFromCPU/uninitOnGPU. */
 void fdtd_destroy (fdtd_ctx *ctx);
 
+/* Compensated FP64 sum of weight[i] * src[i]^2 * scale over n elements,
+ * written to out_dev (a caller-owned device double), for callers that must
+ * not allocate device memory while they run (an application whose own
+ * allocator owns the device memory budget, or a real-time step loop where
+ * cudaMalloc can stall and cudaFree synchronises the device).  It allocates
+ * nothing: the per-block partial sums live in one fixed static device array
+ * of 1024 (sum, compensation) pairs.  src_kind / weight_kind: 0 double,
+ * 1 float, 2 half (weight: 0 = no weight).  blocks = 0 picks the block
+ * count; blocks > 1024 is rejected with FDTD_ERR_ARG.  The first call on a
+ * device resolves the array's address with that device current and caches
+ * it, so that call must come before any capture of work into a stream.
+ * All calls share the array: calls that overlap on the GPU race, and the
+ * caller must order them.  No counterpart in the reference. */
+int fdtd_reduce_sq_noalloc (const void *src, int src_kind, size_t n, const void *weight, int weight_kind,
+                            double scale, int blocks, double *out_dev, void *stream);
+
 const char *fdtd_status_str (int status);
 
 /* Text of the last error raised on the calling host thread (diagnostics). */
