@@ -10,7 +10,9 @@
 // digits (Source/File-Management/Commons.h:63-120,
 // Source/File-Management/Dumper/TXTDumper.h:60-84).  The default save region
 // is the reference's: the whole grid, one z slice at size/2 in 3-D
-// (Source/Scheme/SchemeHelper.h:870-889).
+// (Source/Scheme/SchemeHelper.h:870-889).  The --same-size* flags copy x
+// to y and z at the point where they are parsed, so a later coordinate flag
+// overrides them (Source/Settings/Settings.cpp:249-261).
 //
 // Extra flag: --precision fp64|fp32|fp16s (default fp64 = the plain form).
 // Flags of subsystems outside the step path (MPI, NTFF, BMP/DAT output,
@@ -37,7 +39,6 @@ struct Opts
 {
   fdtd_config cfg;
   int steps = 100;
-  bool same_size = false, same_pml = false, same_tfsf = false;
   bool save_res = false, save_txt = false, manual = false;
   int save_start[3] = {0, 0, 0}, save_end[3] = {0, 0, 0};
   std::string mat_file[6];
@@ -139,14 +140,14 @@ int parse (std::vector<std::string> args, Opts &o)
         return fail ("bad --size");
     }
     else if (a == "--same-size")
-      o.same_size = true;
+      c.size[1] = c.size[2] = c.size[0];   // applied when parsed, as the reference does
     else if (a == "--pml-size" && next (v))
     {
       if (!parse_coord (v, c.pml))
         return fail ("bad --pml-size");
     }
     else if (a == "--same-size-pml")
-      o.same_pml = true;
+      c.pml[1] = c.pml[2] = c.pml[0];
     else if (a == "--tfsf-size-left" && next (v))
     {
       if (!parse_coord (v, c.tfsf_left))
@@ -158,7 +159,10 @@ int parse (std::vector<std::string> args, Opts &o)
         return fail ("bad --tfsf-size-right");
     }
     else if (a == "--same-size-tfsf")
-      o.same_tfsf = true;
+    {
+      c.tfsf_left[1] = c.tfsf_left[2] = c.tfsf_left[0];
+      c.tfsf_right[1] = c.tfsf_right[2] = c.tfsf_right[0];
+    }
     else if (a == "--time-steps" && next (v))
       o.steps = std::atoi (v.c_str ());
     else if (a == "--angle-teta" && next (v))
@@ -251,18 +255,6 @@ int parse (std::vector<std::string> args, Opts &o)
     }
     if (!done)
       return fail ("unsupported flag " + a + " (outside the step path this binary provides)");
-  }
-  for (int a = 1; a < 3; ++a)
-  {
-    if (o.same_size)
-      c.size[a] = c.size[0];
-    if (o.same_pml)
-      c.pml[a] = c.pml[0];
-    if (o.same_tfsf)
-    {
-      c.tfsf_left[a] = c.tfsf_left[0];
-      c.tfsf_right[a] = c.tfsf_right[0];
-    }
   }
   if (c.mode == FDTD_MODE_TMZ)
     c.size[2] = 1;

@@ -84,6 +84,9 @@ struct fdtd_ctx
   void *ff[6] = {};
   float *aux[6] = {};
   float *mat32[2] = {};
+  float *drude32[4] = {};                 // omegape, omegapm, gammae, gammam (FP32)
+  unsigned char *dflag = nullptr;
+  float *xppb[2][6] = {}, *zb[2][6] = {}, *zppb[2][6] = {};
   float *tabs = nullptr;
   size_t tab_off[6][6] = {};
   FastHalf fast_e, fast_h;
@@ -314,8 +317,8 @@ int alloc_fast (fdtd_ctx *ctx)
 {
   const Geometry &g = ctx->g;
   size_t n = (size_t) g.cells;
-  if (g.cfg.use_metamaterials)
-    return fail (ctx, FDTD_ERR_UNSUPPORTED, "metamaterials are provided by the FP64 plain form only");
+  if (g.cfg.use_metamaterials && g.tmz)
+    return fail (ctx, FDTD_ERR_UNSUPPORTED, "2-D metamaterials are provided by the FP64 plain form only");
   ctx->has_second = !g.tmz;
   for (int b = 0; b < (ctx->has_second ? 2 : 1); ++b)
   {
@@ -332,6 +335,19 @@ int alloc_fast (fdtd_ctx *ctx)
   {
     ctx->ff[k] = ctx->ffb[0][k];
     ctx->aux[k] = ctx->auxb[0][k];
+  }
+  if (g.cfg.use_metamaterials)
+  {
+    for (int m = 0; m < 4; ++m)
+      DALLOC (ctx->drude32[m], n * sizeof (float));
+    DALLOC (ctx->dflag, n);
+    for (int b = 0; b < 2; ++b)
+      for (int k = 0; k < 6; ++k)
+      {
+        DALLOC (ctx->xppb[b][k], n * sizeof (float));
+        DALLOC (ctx->zb[b][k], n * sizeof (float));
+        DALLOC (ctx->zppb[b][k], n * sizeof (float));
+      }
   }
   // 1-D coefficient tables per component (see fast_kernels.cu)
   std::vector<float> tabs;
@@ -505,6 +521,13 @@ void init_fused (fdtd_ctx *ctx)
     for (int a = 0; a < 3; ++a)
       ctx->ps_interior = ctx->ps_interior && ps[a] >= 1 && ps[a] <= g.n[a] - 2;
   f.ps_scale_h = (float) kEta0;
+  f.use_meta = g.cfg.use_metamaterials;
+  f.dt = (float) g.dt;
+  f.dflag = ctx->dflag;
+  f.omega[0] = ctx->drude32[0];
+  f.omega[1] = ctx->drude32[1];
+  f.gamma[0] = ctx->drude32[2];
+  f.gamma[1] = ctx->drude32[3];
 }
 
 int create_impl (const fdtd_config *cfg, int device, fdtd_ctx *ctx)
@@ -672,6 +695,9 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
   bool ps_ok = g.cfg.point_source_mask && point_source_index (g, &ps_idx);
   cudaStream_t s = ctx->stream;
   const bool fused = ctx->kind != 0 && ctx->has_second && !ctx->mat32[1] && ctx->ps_interior;
+  if (ctx->kind != 0 && g.cfg.use_metamaterials && !fused)
+    return fail (ctx, FDTD_ERR_UNSUPPORTED,
+                 "FP32/FP16 metamaterials need the one-sweep 3-D kernel (uniform mu, interior point source)");
 
   for (uint32_t i = 0; i < n; ++i)
   {
@@ -702,6 +728,12 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
       {
         f.aux_old[k] = ctx->auxb[o][k];
         f.aux_new[k] = ctx->auxb[nw][k];
+        f.xpp_old[k] = ctx->xppb[o][k];
+        f.xpp_new[k] = ctx->xppb[nw][k];
+        f.z_old[k] = ctx->zb[o][k];
+        f.z_new[k] = ctx->zb[nw][k];
+        f.zpp_old[k] = ctx->zppb[o][k];
+        f.zpp_new[k] = ctx->zppb[nw][k];
       }
       f.eps = ctx->mat32[0];
       f.inc_h = ctx->hinc[hprev];
@@ -866,7 +898,16 @@ int fdtd_upload_material_device (fdtd_ctx *ctx, int which, const double *dev)
     return FDTD_OK;
   }
   if (which > 1)
-    return fail (ctx, FDTD_ERR_UNSUPPORTED, "Drude grids are provided by the FP64 plain form only");
+  {
+    if (!ctx->dflag)
+      return fail (ctx, FDTD_ERR_UNSUPPORTED, "Drude grids need use_metamaterials");
+    // FDTD_MAT_OMEGAPE..GAMMAM = 2..5 -> omegape, omegapm, gammae, gammam
+    ctx->launches += launch_convert_in (ctx->drude32[which - 2], 1, dev, n, 1.0, ctx->stream);
+    ctx->launches += launch_drude_flags (ctx->dflag, ctx->drude32[0], ctx->drude32[2], ctx->drude32[1],
+                                         ctx->drude32[3], ctx->g.n[0], ctx->g.n[1], ctx->g.n[2], ctx->stream);
+    CK (cudaGetLastError ());
+    return FDTD_OK;
+  }
   if (!ctx->mat32[which])
     DALLOC (ctx->mat32[which], n * sizeof (float));
   ctx->launches += launch_convert_in (ctx->mat32[which], 1, dev, n, 1.0, ctx->stream);

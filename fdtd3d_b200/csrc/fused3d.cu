@@ -96,6 +96,79 @@ __device__ __forceinline__ void tfsf_apply (const FusedParams &p, int k, const d
   }
 }
 
+// Drude coefficients of component k at (x, y, z) in the scaled formulation
+// (X = D/eps0 or c*B, Z = D1 or eta0*B1): the reference's b0..a2
+// (Source/Scheme/InternalScheme.inc.h:2527-2532) multiplied through by the
+// vacuum constant, with the plasma frequency and collision rate averaged as
+// getMetaMaterial does (two points for E, the plain mean of four for H).
+__device__ __forceinline__ void drude_coeffs (const FusedParams &p, int k, int x, int y, int z, float c[5])
+{
+  const int ny = p.g.n[1], nz = p.g.n[2];
+  const size_t stride[3] = {(size_t) ny * nz, (size_t) nz, 1};
+  const size_t id = ((size_t) x * ny + y) * nz + z;
+  const int side = k >= 3 ? 1 : 0;
+  const float *om = p.omega[side];
+  const float *ga = p.gamma[side];
+  float w, g, m = 1.f;
+  if (k < 3)
+  {
+    const size_t j = id + stride[k];
+    w = 0.5f * (om[id] + om[j]);
+    g = 0.5f * (ga[id] + ga[j]);
+    if (p.eps)
+      m = 0.5f * (p.eps[id] + p.eps[j]);
+  }
+  else
+  {
+    const int a = k - 3;
+    const int lo = a == 0 ? 1 : 0;
+    const int hi = a == 2 ? 1 : 2;
+    const size_t j1 = id + stride[hi], j2 = id + stride[lo], j3 = id + stride[lo] + stride[hi];
+    w = 0.25f * (om[id] + om[j1] + om[j2] + om[j3]);
+    g = 0.25f * (ga[id] + ga[j1] + ga[j2] + ga[j3]);
+  }
+  const float dt = p.dt;
+  const float sq = (dt * w) * (dt * w);
+  const float inv = 1.f / (4.f * m + 2.f * dt * m * g + sq);
+  c[0] = (4.f + 2.f * dt * g) * inv;
+  c[1] = -8.f * inv;
+  c[2] = (4.f - 2.f * dt * g) * inv;
+  c[3] = (2.f * sq - 8.f * m) * inv;
+  c[4] = (4.f * m - 2.f * dt * m * g + sq) * inv;
+}
+
+// Dispersive cell: curl step of X (PML coefficients, sigma = 0 inside),
+// Drude recurrence to Z, then F from Z with modifier 1 (the reference's
+// metamaterial PML path, InternalScheme.inc.h:2551-2640).
+__device__ __forceinline__ float update_drude (const FusedParams &p, int k, float f, float curl, int x, int y, int z,
+                                               size_t id, bool store)
+{
+  const int pos[3] = {x, y, z};
+  const CompDev &c = p.comp[k];
+  const float ca1 = p.tab[k][0][pos[c.sig_cacb]];
+  const float sq1 = p.tab[k][1][pos[c.sig_cacb]];
+  const float p5 = p.tab[k][2][pos[c.sig5]];
+  const float q5 = p.tab[k][3][pos[c.sig5]];
+  const float g4p = p.tab[k][4][pos[c.sig4]];
+  const float g4m = p.tab[k][5][pos[c.sig4]];
+  const float xo = p.aux_old[k][id];
+  const float xpp = p.xpp_old[k][id];
+  const float zo = p.z_old[k][id];
+  const float zpp = p.zpp_old[k][id];
+  float b[5];
+  drude_coeffs (p, k, x, y, z, b);
+  const float xn = ca1 * xo + sq1 * curl;
+  const float zn = b[0] * xn + b[1] * xo + b[2] * xpp - b[3] * zo - b[4] * zpp;
+  if (store)
+  {
+    p.aux_new[k][id] = xn;
+    p.xpp_new[k][id] = xo;
+    p.z_new[k][id] = zn;
+    p.zpp_new[k][id] = zo;
+  }
+  return p5 * f + (g4p * zn - g4m * zo) * q5;
+}
+
 // Update of one component at one cell given its curl: interior or PML.
 // `store_aux` is false for recomputed ring values (owned by another tile).
 __device__ __forceinline__ float update (const FusedParams &p, int k, bool interior, float f, float curl, float inv_m,
@@ -124,7 +197,7 @@ __device__ __forceinline__ bool on_face (const int *planes, int v)
   return v == planes[0] || v == planes[1] || v == planes[2] || v == planes[3];
 }
 
-template <typename T, int TY, int TZ>
+template <typename T, int TY, int TZ, bool META>
 __global__ void __launch_bounds__ ((TY + 1) * (TZ + 1)) fused3d_kernel (FusedParams p, int *err)
 {
   const int nx = p.g.n[0], ny = p.g.n[1], nz = p.g.n[2];
@@ -162,12 +235,15 @@ __global__ void __launch_bounds__ ((TY + 1) * (TZ + 1)) fused3d_kernel (FusedPar
   // the plane before the chunk is only needed by H_new(xa - 1), not owned)
   float hp[3] = {0.f, 0.f, 0.f};
   float ep[3] = {0.f, 0.f, 0.f};
+  unsigned flp = 0;   // Drude bitmask of the previous plane
   if (valid)
   {
     size_t id = (size_t) (xa - 1) * sx + col;
 #pragma unroll
     for (int c = 0; c < 3; ++c)
       hp[c] = ldf (Ho[c], id);
+    if (META)
+      flp = p.dflag[id];
   }
 
   for (int x = xa; x <= xb + 1; ++x)
@@ -177,6 +253,9 @@ __global__ void __launch_bounds__ ((TY + 1) * (TZ + 1)) fused3d_kernel (FusedPar
     // 1. stage
     float eo[3] = {0.f, 0.f, 0.f};
     float epsx1 = 1.f;
+    unsigned fl = 0;
+    if (META && valid)
+      fl = p.dflag[id];
     if (valid)
     {
 #pragma unroll
@@ -247,12 +326,16 @@ __global__ void __launch_bounds__ ((TY + 1) * (TZ + 1)) fused3d_kernel (FusedPar
         tfsf_apply (p, 2, p.inc_h, err, x, y, z, c0, c1, c2, c3);
       }
       const bool st_aux = owner && x <= xb;
-      en[0] = update (p, 0, yz_in[0] && x >= p.ilo[0][0] && x < p.ihi[0][0], eo[0], (a1 - a0) - (a3 - a2), inv[0],
-                      x, y, z, id, st_aux);
-      en[1] = update (p, 1, yz_in[1] && x >= p.ilo[1][0] && x < p.ihi[1][0], eo[1], (b1 - b0) - (b3 - b2), inv[1],
-                      x, y, z, id, st_aux);
-      en[2] = update (p, 2, yz_in[2] && x >= p.ilo[2][0] && x < p.ihi[2][0], eo[2], (c1 - c0) - (c3 - c2), inv[2],
-                      x, y, z, id, st_aux);
+      const float cu[3] = {(a1 - a0) - (a3 - a2), (b1 - b0) - (b3 - b2), (c1 - c0) - (c3 - c2)};
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+      {
+        if (META && (fl & (1u << c)))
+          en[c] = update_drude (p, c, eo[c], cu[c], x, y, z, id, st_aux);
+        else
+          en[c] = update (p, c, yz_in[c] && x >= p.ilo[c][0] && x < p.ihi[c][0], eo[c], cu[c], inv[c], x, y, z, id,
+                          st_aux);
+      }
       if (p.ps_mask & 7)
       {
         if (x == p.ps[0] && y == p.ps[1] && z == p.ps[2])
@@ -290,12 +373,16 @@ __global__ void __launch_bounds__ ((TY + 1) * (TZ + 1)) fused3d_kernel (FusedPar
         tfsf_apply (p, 5, p.inc_e, err, xh, y, z, c0, c1, c2, c3);
       }
       float hn[3];
-      hn[0] = update (p, 3, yz_in[3] && xh >= p.ilo[3][0] && xh < p.ihi[3][0], hp[0], (a1 - a0) - (a3 - a2), 1.f,
-                      xh, y, z, hid, true);
-      hn[1] = update (p, 4, yz_in[4] && xh >= p.ilo[4][0] && xh < p.ihi[4][0], hp[1], (b1 - b0) - (b3 - b2), 1.f,
-                      xh, y, z, hid, true);
-      hn[2] = update (p, 5, yz_in[5] && xh >= p.ilo[5][0] && xh < p.ihi[5][0], hp[2], (c1 - c0) - (c3 - c2), 1.f,
-                      xh, y, z, hid, true);
+      const float cu[3] = {(a1 - a0) - (a3 - a2), (b1 - b0) - (b3 - b2), (c1 - c0) - (c3 - c2)};
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+      {
+        if (META && (flp & (8u << c)))
+          hn[c] = update_drude (p, 3 + c, hp[c], cu[c], xh, y, z, hid, true);
+        else
+          hn[c] = update (p, 3 + c, yz_in[3 + c] && xh >= p.ilo[3 + c][0] && xh < p.ihi[3 + c][0], hp[c], cu[c], 1.f,
+                          xh, y, z, hid, true);
+      }
       if (p.ps_mask & 56)
       {
         if (xh == p.ps[0] && y == p.ps[1] && z == p.ps[2])
@@ -321,6 +408,58 @@ __global__ void __launch_bounds__ ((TY + 1) * (TZ + 1)) fused3d_kernel (FusedPar
       ep[c] = en[c];
       hp[c] = sH[c][ty + 1][tz + 1];
     }
+    flp = fl;
+  }
+}
+
+// bit k of flags[cell]: component k averages a non-zero plasma frequency or
+// collision rate (the averaging stencils of getMetaMaterial)
+__global__ void drude_flags_kernel (unsigned char *flags, const float *ome, const float *gae, const float *omm,
+                                    const float *gam, int nx, int ny, int nz)
+{
+  const size_t n = (size_t) nx * ny * nz;
+  const size_t stride[3] = {(size_t) ny * nz, (size_t) nz, 1};
+  for (size_t id = (size_t) blockIdx.x * blockDim.x + threadIdx.x; id < n; id += (size_t) gridDim.x * blockDim.x)
+  {
+    const int z = (int) (id % nz);
+    const int y = (int) ((id / nz) % ny);
+    const int x = (int) (id / stride[0]);
+    const int pos[3] = {x, y, z};
+    const int lim[3] = {nx, ny, nz};
+    unsigned f = 0;
+    for (int k = 0; k < 6; ++k)
+    {
+      const float *om = k < 3 ? ome : omm;
+      const float *ga = k < 3 ? gae : gam;
+      const int a = k % 3;
+      size_t pts[4] = {id, id, id, id};
+      int npt;
+      bool ok = true;
+      if (k < 3)
+      {
+        npt = 2;
+        ok = pos[a] + 1 < lim[a];
+        pts[1] = id + stride[a];
+      }
+      else
+      {
+        const int lo = a == 0 ? 1 : 0;
+        const int hi = a == 2 ? 1 : 2;
+        npt = 4;
+        ok = pos[lo] + 1 < lim[lo] && pos[hi] + 1 < lim[hi];
+        pts[1] = id + stride[hi];
+        pts[2] = id + stride[lo];
+        pts[3] = id + stride[lo] + stride[hi];
+      }
+      if (!ok)
+        continue;
+      bool any = false;
+      for (int j = 0; j < npt; ++j)
+        any = any || om[pts[j]] != 0.f || ga[pts[j]] != 0.f;
+      if (any)
+        f |= 1u << k;
+    }
+    flags[id] = (unsigned char) f;
   }
 }
 
@@ -332,10 +471,31 @@ int launch_fused3d (const FusedParams &p, int *err, cudaStream_t s)
   const int ny = p.g.n[1], nz = p.g.n[2], nx = p.g.n[0];
   dim3 block (TZ + 1, TY + 1);
   dim3 grid ((nz - 2 + TZ - 1) / TZ, (ny - 2 + TY - 1) / TY, (nx - 2 + p.x_chunk - 1) / p.x_chunk);
-  if (p.fp16)
-    fused3d_kernel<__half, TY, TZ><<<grid, block, 0, s>>> (p, err);
+  if (p.use_meta)
+  {
+    if (p.fp16)
+      fused3d_kernel<__half, TY, TZ, true><<<grid, block, 0, s>>> (p, err);
+    else
+      fused3d_kernel<float, TY, TZ, true><<<grid, block, 0, s>>> (p, err);
+  }
   else
-    fused3d_kernel<float, TY, TZ><<<grid, block, 0, s>>> (p, err);
+  {
+    if (p.fp16)
+      fused3d_kernel<__half, TY, TZ, false><<<grid, block, 0, s>>> (p, err);
+    else
+      fused3d_kernel<float, TY, TZ, false><<<grid, block, 0, s>>> (p, err);
+  }
+  return 1;
+}
+
+int launch_drude_flags (unsigned char *flags, const float *ome, const float *gae, const float *omm, const float *gam,
+                        int nx, int ny, int nz, cudaStream_t s)
+{
+  size_t n = (size_t) nx * ny * nz;
+  size_t blocks = (n + 255) / 256;
+  if (blocks > 148 * 32)
+    blocks = 148 * 32;
+  drude_flags_kernel<<<(unsigned) blocks, 256, 0, s>>> (flags, ome, gae, omm, gam, nx, ny, nz);
   return 1;
 }
 

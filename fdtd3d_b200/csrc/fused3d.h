@@ -35,8 +35,27 @@ struct FusedParams
   const double *src;           // per-step table; src[src_index] E value, src[src_index + 1] H value
   int src_index;
   float ps_scale_h;
+
+  // Drude (metamaterials): per-cell bit k set when component k sees a
+  // non-zero averaged plasma frequency or collision rate; state of those
+  // cells: X (in aux), X two steps back, Z = D1/eps0... scaled, Z one step back
+  int use_meta;
+  float dt;
+  const unsigned char *dflag;
+  const float *omega[2];       // omegape (E side), omegapm (H side)
+  const float *gamma[2];       // gammae, gammam
+  const float *xpp_old[6];
+  float *xpp_new[6];
+  const float *z_old[6];
+  float *z_new[6];
+  const float *zpp_old[6];
+  float *zpp_new[6];
 };
 
 int launch_fused3d (const FusedParams &p, int *err, cudaStream_t s);
+
+// Recomputes the per-cell Drude bitmask from the four material arrays.
+int launch_drude_flags (unsigned char *flags, const float *ome, const float *gae, const float *omm, const float *gam,
+                        int nx, int ny, int nz, cudaStream_t s);
 
 }  // namespace fdtdb
