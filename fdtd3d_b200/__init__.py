@@ -33,6 +33,8 @@ EXPORTED = (
     "fdtd_download_field", "fdtd_upload_material_device", "fdtd_download_field_device",
     "fdtd_reduce", "fdtd_scalars", "fdtd_launch_count", "fdtd_destroy", "fdtd_status_str",
     "fdtd_last_error", "fdtd_stream", "fdtd_profile", "fdtd_kernel_time",
+    "fdtd_batch_create", "fdtd_batch_upload_eps", "fdtd_batch_tune", "fdtd_batch_step", "fdtd_batch_sync",
+    "fdtd_batch_download", "fdtd_batch_info", "fdtd_batch_last_error", "fdtd_batch_destroy",
 )
 
 
@@ -60,6 +62,8 @@ class Config(ctypes.Structure):
         ("use_metamaterials", ctypes.c_int),
         ("point_source", ctypes.c_int * 3),
         ("point_source_mask", ctypes.c_int),
+        ("point_source_kind", ctypes.c_int),
+        ("point_source_bandwidth", ctypes.c_double),
         ("precision", ctypes.c_int),
         ("layout", ctypes.c_int),
         ("reserved", ctypes.c_int * 8),
@@ -96,6 +100,15 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fdtd_stream": ([vp], vp),
         "fdtd_profile": ([vp, i], i),
         "fdtd_kernel_time": ([vp, ctypes.POINTER(d), ctypes.POINTER(i64)], i),
+        "fdtd_batch_create": ([ctypes.POINTER(Config), i, vp, i, ctypes.POINTER(vp)], i),
+        "fdtd_batch_upload_eps": ([vp, i, vp], i),
+        "fdtd_batch_tune": ([vp, i, vp], i),
+        "fdtd_batch_step": ([vp, u32, u32], i),
+        "fdtd_batch_sync": ([vp, i64], i),
+        "fdtd_batch_download": ([vp, i, i, vp], i),
+        "fdtd_batch_info": ([vp, ctypes.POINTER(i64), ctypes.POINTER(i), ctypes.POINTER(d)], i),
+        "fdtd_batch_last_error": ([vp], ctypes.c_char_p),
+        "fdtd_batch_destroy": ([vp], None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -122,7 +135,8 @@ def _triple(v, default):
 def make_config(*, mode=MODE_DIM3, size=(20, 20, 20), pml=None, tfsf_left=None, tfsf_right=None,
                 dx=0.0005, wavelength=0.02, courant=0.5, teta=90.0, phi=0.0, psi=90.0,
                 use_pml=False, use_tfsf=False, use_metamaterials=False,
-                point_source=(0, 0, 0), point_source_mask=0, precision=PREC_FP64_PLAIN) -> Config:
+                point_source=(0, 0, 0), point_source_mask=0, point_source_kind=0, point_source_bandwidth=0.0,
+                precision=PREC_FP64_PLAIN) -> Config:
     c = Config()
     c.mode = mode
     c.size[:] = _triple(size, 1)
@@ -134,6 +148,8 @@ def make_config(*, mode=MODE_DIM3, size=(20, 20, 20), pml=None, tfsf_left=None, 
     c.use_pml, c.use_tfsf, c.use_metamaterials = int(use_pml), int(use_tfsf), int(use_metamaterials)
     c.point_source[:] = _triple(point_source, 0)
     c.point_source_mask = int(point_source_mask)
+    c.point_source_kind = int(point_source_kind)
+    c.point_source_bandwidth = float(point_source_bandwidth)
     c.precision = int(precision)
     c.layout = 0
     return c
@@ -235,6 +251,84 @@ class Simulation:
     def close(self) -> None:
         if getattr(self, "_h", None):
             self.lib.fdtd_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many 2-D TMz simulations of different sizes advanced by one persistent
+    kernel launch per ``step`` call (captured in a CUDA graph), FP32.
+
+    ``sizes`` is a list of (nx, ny); every instance has its point source at
+    its centre and shares the physics given as keyword arguments."""
+
+    def __init__(self, sizes, device: int = 0, **cfg):
+        self.lib = load_library()
+        cfg.setdefault("mode", MODE_TMZ)
+        cfg.setdefault("precision", PREC_FP32)
+        cfg.setdefault("size", (3, 3))
+        self.cfg = make_config(**cfg)
+        self.sizes = [(int(a), int(b)) for a, b in sizes]
+        arr = (ctypes.c_int * (2 * len(self.sizes)))(*[v for pair in self.sizes for v in pair])
+        h = ctypes.c_void_p()
+        st = self.lib.fdtd_batch_create(ctypes.byref(self.cfg), len(self.sizes), arr, device, ctypes.byref(h))
+        if st != 0:
+            raise FdtdError(st, "fdtd_batch_create", (self.lib.fdtd_status_str(st) or b"").decode())
+        self._h = h
+        self.t = 0
+
+    def _check(self, st: int, where: str) -> None:
+        if st != 0:
+            raise FdtdError(st, where, (self.lib.fdtd_batch_last_error(self._h) or b"").decode())
+
+    def set_eps(self, i: int, eps) -> None:
+        a = np.ascontiguousarray(eps, dtype=np.float64).reshape(-1)
+        assert a.size == self.sizes[i][0] * self.sizes[i][1]
+        self._check(self.lib.fdtd_batch_upload_eps(self._h, i, a.ctypes.data), "batch_upload_eps")
+
+    def tune(self, steps: int = 8):
+        out = (ctypes.c_int * 3)()
+        self._check(self.lib.fdtd_batch_tune(self._h, steps, out), "batch_tune")
+        self.t = 0
+        return tuple(out)
+
+    def step(self, n: int, t_start: int | None = None) -> None:
+        t0 = self.t if t_start is None else t_start
+        self._check(self.lib.fdtd_batch_step(self._h, t0, n), "batch_step")
+        self.t = t0 + n
+
+    def sync(self, timeout_ns: int = -1) -> None:
+        self._check(self.lib.fdtd_batch_sync(self._h, timeout_ns), "batch_sync")
+
+    def field(self, i: int, comp) -> np.ndarray:
+        k = COMPONENTS.index(comp) if isinstance(comp, str) else comp
+        nx, ny = self.sizes[i]
+        out = np.empty(nx * ny)
+        self._check(self.lib.fdtd_batch_download(self._h, i, k, out.ctypes.data), "batch_download")
+        return out.reshape(nx, ny)
+
+    def info(self) -> dict:
+        cells = ctypes.c_int64()
+        graph = ctypes.c_int()
+        ms = ctypes.c_double()
+        self._check(self.lib.fdtd_batch_info(self._h, ctypes.byref(cells), ctypes.byref(graph), ctypes.byref(ms)),
+                    "batch_info")
+        return {"cells": cells.value, "graph": bool(graph.value), "last_ms": ms.value}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.lib.fdtd_batch_destroy(self._h)
             self._h = None
 
     def __enter__(self):

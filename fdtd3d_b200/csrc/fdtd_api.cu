@@ -13,6 +13,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -216,21 +217,6 @@ CompDev make_comp_dev (const Geometry &g, int k)
   return c;
 }
 
-// sigma profile of axis b averaged at the position of component k
-std::vector<double> sigma_at (const Geometry &g, int k, int b)
-{
-  const std::vector<double> &s = g.sigma[b];
-  int n = g.n[b];
-  std::vector<double> out (n, 0.0);
-  int a = k % 3;
-  bool isH = k >= 3;
-  bool averaged = isH ? (b != a) : (b == a);
-  if (g.tmz && b == 2)
-    averaged = false;
-  for (int i = 0; i < n; ++i)
-    out[i] = (averaged && i + 1 < n) ? (s[i] + s[i + 1]) / 2.0 : s[i];
-  return out;
-}
 
 }  // namespace
 
@@ -449,6 +435,7 @@ void select_fast_set (fdtd_ctx *ctx)
 
 void init_fused (fdtd_ctx *ctx)
 {
+  int chunk_override = 0;
   const Geometry &g = ctx->g;
   FusedParams &f = ctx->fused;
   std::memset (&f, 0, sizeof (f));
@@ -508,10 +495,21 @@ void init_fused (fdtd_ctx *ctx)
     ctx->has_second = false;
   }
   f.inc_len = g.inc_len;
-  int tiles = ((g.n[2] - 2 + 31) / 32) * ((g.n[1] - 2 + 7) / 8);
+  // tile / occupancy variant of the one-sweep kernel; FDTDB_FUSED_SHAPE
+  // overrides the default for tuning runs
+  f.shape = 1;
+  if (const char *v = std::getenv ("FDTDB_FUSED_SHAPE"))
+    f.shape = std::atoi (v);
+  const int ty_of_shape[5] = {8, 8, 4, 16, 4};
+  int tyv = ty_of_shape[(f.shape >= 0 && f.shape < 5) ? f.shape : 1];
+  if (const char *v = std::getenv ("FDTDB_FUSED_CHUNK"))
+    chunk_override = std::atoi (v);
+  int tiles = ((g.n[2] - 2 + 31) / 32) * ((g.n[1] - 2 + tyv - 1) / tyv);
   int64_t want = (int64_t) ctx->sm_count * 3 * 8;
   int64_t chunk = ((int64_t) (g.n[0] - 2) * tiles) / std::max<int64_t> (want, 1);
   f.x_chunk = (int) std::min<int64_t> (128, std::max<int64_t> (16, chunk));
+  if (chunk_override > 0)
+    f.x_chunk = chunk_override;
   const int *ps = g.cfg.point_source;
   f.ps_mask = g.cfg.point_source_mask;
   for (int a = 0; a < 3; ++a)

@@ -197,8 +197,42 @@ __device__ __forceinline__ bool on_face (const int *planes, int v)
   return v == planes[0] || v == planes[1] || v == planes[2] || v == planes[3];
 }
 
-template <typename T, int TY, int TZ, bool META>
-__global__ void __launch_bounds__ ((TY + 1) * (TZ + 1)) fused3d_kernel (FusedParams p, int *err)
+// Per-component update with the component fixed at compile time, so the
+// PML table axes are constants (axis a = K % 3; curl-step coefficients along
+// a + 1, E-from-D coefficients along a + 2 and a, as the reference's
+// SigmaY/SigmaZ/SigmaX choice for Ex and its rotations).
+template <int K>
+__device__ __forceinline__ float update_k (const FusedParams &p, bool interior, float f, float curl, float inv_m,
+                                           int x, int y, int z, size_t id, bool store)
+{
+  if (interior)
+    return f + p.courant * inv_m * curl;
+  constexpr int A = K % 3, C1 = (K + 1) % 3, C2 = (K + 2) % 3;
+  const int pos[3] = {x, y, z};
+  const float ca1 = __ldg (p.tab[K][0] + pos[C1]);
+  const float sq1 = __ldg (p.tab[K][1] + pos[C1]);
+  const float p5 = __ldg (p.tab[K][2] + pos[C2]);
+  const float q5 = __ldg (p.tab[K][3] + pos[C2]);
+  const float g4p = __ldg (p.tab[K][4] + pos[A]);
+  const float g4m = __ldg (p.tab[K][5] + pos[A]);
+  const float xo = p.aux_old[K][id];
+  const float xn = ca1 * xo + sq1 * curl;
+  if (store)
+    p.aux_new[K][id] = xn;
+  return p5 * f + (g4p * xn - g4m * xo) * q5 * inv_m;
+}
+
+template <int K, bool META>
+__device__ __forceinline__ float update_any (const FusedParams &p, unsigned fl, bool interior, float f, float curl,
+                                             float inv_m, int x, int y, int z, size_t id, bool store)
+{
+  if (META && (fl & (1u << K)))
+    return update_drude (p, K, f, curl, x, y, z, id, store);
+  return update_k<K> (p, interior, f, curl, inv_m, x, y, z, id, store);
+}
+
+template <typename T, int TY, int TZ, bool META, int MINB>
+__global__ void __launch_bounds__ ((TY + 1) * (TZ + 1), MINB) fused3d_kernel (FusedParams p, int *err)
 {
   const int nx = p.g.n[0], ny = p.g.n[1], nz = p.g.n[2];
   const int tz = threadIdx.x;
@@ -214,200 +248,203 @@ __global__ void __launch_bounds__ ((TY + 1) * (TZ + 1)) fused3d_kernel (FusedPar
   const bool owner = tz < TZ && ty < TY && inner;
   const size_t sx = (size_t) ny * nz;
   const size_t col = (size_t) y * nz + z;
+  const bool halo_y = ty == 0 && z <= nz - 1;              // loads (y - 1) for Hx, Hz
+  const bool halo_z = tz == 0 && y <= ny - 1;              // loads (z - 1) for Hx, Hy
+  const bool ring_y = ty == TY && p.eps && y + 1 <= ny - 1 && z <= nz - 1;
+  const bool ring_z = tz == TZ && p.eps && z + 1 <= nz - 1 && y <= ny - 1;
 
   __shared__ float sH[3][TY + 2][TZ + 2];
   __shared__ float sE[3][TY + 1][TZ + 1];
   __shared__ float sEps[TY + 2][TZ + 2];
 
-  // PML classification: y, z are fixed per thread, x is uniform per plane
   bool yz_in[6];
 #pragma unroll
   for (int k = 0; k < 6; ++k)
     yz_in[k] = !p.use_pml || (y >= p.ilo[k][1] && y < p.ihi[k][1] && z >= p.ilo[k][2] && z < p.ihi[k][2]);
   const bool yz_face = p.use_tfsf && (on_face (p.face[1], y) || on_face (p.face[2], z));
 
-  const T *Eo[3] = {(const T *) p.e_old[0], (const T *) p.e_old[1], (const T *) p.e_old[2]};
-  const T *Ho[3] = {(const T *) p.h_old[0], (const T *) p.h_old[1], (const T *) p.h_old[2]};
-  T *En[3] = {(T *) p.e_new[0], (T *) p.e_new[1], (T *) p.e_new[2]};
-  T *Hn[3] = {(T *) p.h_new[0], (T *) p.h_new[1], (T *) p.h_new[2]};
+  const T *Eo0 = (const T *) p.e_old[0], *Eo1 = (const T *) p.e_old[1], *Eo2 = (const T *) p.e_old[2];
+  const T *Ho0 = (const T *) p.h_old[0], *Ho1 = (const T *) p.h_old[1], *Ho2 = (const T *) p.h_old[2];
+  T *En0 = (T *) p.e_new[0], *En1 = (T *) p.e_new[1], *En2 = (T *) p.e_new[2];
+  T *Hn0 = (T *) p.h_new[0], *Hn1 = (T *) p.h_new[1], *Hn2 = (T *) p.h_new[2];
 
-  // state at x = xa - 1: H_old and E_new (= recomputed below only for x >= xa;
-  // the plane before the chunk is only needed by H_new(xa - 1), not owned)
-  float hp[3] = {0.f, 0.f, 0.f};
-  float ep[3] = {0.f, 0.f, 0.f};
-  unsigned flp = 0;   // Drude bitmask of the previous plane
+  // registers of the plane being fetched (software pipeline, one plane ahead)
+  float fh0 = 0.f, fh1 = 0.f, fh2 = 0.f, fe0 = 0.f, fe1 = 0.f, fe2 = 0.f;
+  float feps = 1.f, feps1 = 1.f, fhy0 = 0.f, fhy2 = 0.f, fhz0 = 0.f, fhz1 = 0.f, fry = 1.f, frz = 1.f;
+  unsigned ffl = 0;
+  auto fetch = [&] (int x) {
+    const size_t id = (size_t) x * sx + col;
+    if (valid)
+    {
+      fh0 = ldf (Ho0, id);
+      fh1 = ldf (Ho1, id);
+      fh2 = ldf (Ho2, id);
+      fe0 = ldf (Eo0, id);
+      fe1 = ldf (Eo1, id);
+      fe2 = ldf (Eo2, id);
+      if (p.eps)
+      {
+        feps = __ldg (p.eps + id);
+        feps1 = x + 1 <= nx - 1 ? __ldg (p.eps + id + sx) : 1.f;
+      }
+      if (META)
+        ffl = p.dflag[id];
+    }
+    if (halo_y)
+    {
+      fhy0 = ldf (Ho0, id - nz);
+      fhy2 = ldf (Ho2, id - nz);
+    }
+    if (halo_z)
+    {
+      fhz0 = ldf (Ho0, id - 1);
+      fhz1 = ldf (Ho1, id - 1);
+    }
+    if (ring_y)
+      fry = __ldg (p.eps + id + nz);
+    if (ring_z)
+      frz = __ldg (p.eps + id + 1);
+  };
+
+  float hp0 = 0.f, hp1 = 0.f, hp2 = 0.f;   // H_old(x - 1), own cell
+  float ep0 = 0.f, ep1 = 0.f, ep2 = 0.f;   // E_new(x - 1), own cell
+  unsigned flp = 0;
   if (valid)
   {
-    size_t id = (size_t) (xa - 1) * sx + col;
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-      hp[c] = ldf (Ho[c], id);
+    const size_t id = (size_t) (xa - 1) * sx + col;
+    hp0 = ldf (Ho0, id);
+    hp1 = ldf (Ho1, id);
+    hp2 = ldf (Ho2, id);
     if (META)
       flp = p.dflag[id];
   }
+  fetch (xa);
 
   for (int x = xa; x <= xb + 1; ++x)
   {
     const size_t id = (size_t) x * sx + col;
-    const bool xin = x <= nx - 2;
-    // 1. stage
-    float eo[3] = {0.f, 0.f, 0.f};
-    float epsx1 = 1.f;
-    unsigned fl = 0;
-    if (META && valid)
-      fl = p.dflag[id];
-    if (valid)
-    {
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-      {
-        sH[c][ty + 1][tz + 1] = ldf (Ho[c], id);
-        eo[c] = ldf (Eo[c], id);
-      }
-      if (p.eps)
-      {
-        sEps[ty][tz] = __ldg (p.eps + id);
-        if (x + 1 <= nx - 1)
-          epsx1 = __ldg (p.eps + id + sx);
-      }
-    }
-    else
-    {
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-        sH[c][ty + 1][tz + 1] = 0.f;
-      sEps[ty][tz] = 1.f;
-    }
+    // 1. stage the fetched plane
+    sH[0][ty + 1][tz + 1] = fh0;
+    sH[1][ty + 1][tz + 1] = fh1;
+    sH[2][ty + 1][tz + 1] = fh2;
+    sEps[ty][tz] = feps;
     if (ty == 0)
     {
-      bool v = z <= nz - 1;
-      size_t hid = id - nz;
-      sH[0][0][tz + 1] = v ? ldf (Ho[0], hid) : 0.f;
-      sH[2][0][tz + 1] = v ? ldf (Ho[2], hid) : 0.f;
+      sH[0][0][tz + 1] = fhy0;
+      sH[2][0][tz + 1] = fhy2;
     }
     if (tz == 0)
     {
-      bool v = y <= ny - 1;
-      size_t hid = id - 1;
-      sH[0][ty + 1][0] = v ? ldf (Ho[0], hid) : 0.f;
-      sH[1][ty + 1][0] = v ? ldf (Ho[1], hid) : 0.f;
+      sH[0][ty + 1][0] = fhz0;
+      sH[1][ty + 1][0] = fhz1;
     }
-    if (p.eps)
-    {
-      if (ty == TY)
-        sEps[TY + 1][tz] = (y + 1 <= ny - 1 && z <= nz - 1) ? __ldg (p.eps + id + nz) : 1.f;
-      if (tz == TZ)
-        sEps[ty][TZ + 1] = (z + 1 <= nz - 1 && y <= ny - 1) ? __ldg (p.eps + id + 1) : 1.f;
-    }
+    if (ty == TY)
+      sEps[TY + 1][tz] = fry;
+    if (tz == TZ)
+      sEps[ty][TZ + 1] = frz;
+    const float eo0 = fe0, eo1 = fe1, eo2 = fe2;
+    const float epsx1 = feps1;
+    const unsigned fl = ffl;
+    const float h0 = fh0, h1 = fh1, h2 = fh2;
     __syncthreads ();
+    // 2. next plane in flight while this one computes
+    if (x + 1 <= xb + 1)
+      fetch (x + 1);
 
-    // 2. E_new(x) on tile + ring
-    float en[3] = {eo[0], eo[1], eo[2]};
-    if (inner && xin)
+    // 3. E_new(x) on tile + ring
+    float en0 = eo0, en1 = eo1, en2 = eo2;
+    if (inner && x <= nx - 2)
     {
-      float inv[3] = {1.f, 1.f, 1.f};
+      float i0 = 1.f, i1 = 1.f, i2 = 1.f;
       if (p.eps)
       {
         const float e0 = sEps[ty][tz];
-        inv[0] = __fdividef (2.f, e0 + epsx1);
-        inv[1] = __fdividef (2.f, e0 + sEps[ty + 1][tz]);
-        inv[2] = __fdividef (2.f, e0 + sEps[ty][tz + 1]);
+        i0 = __fdividef (2.f, e0 + epsx1);
+        i1 = __fdividef (2.f, e0 + sEps[ty + 1][tz]);
+        i2 = __fdividef (2.f, e0 + sEps[ty][tz + 1]);
       }
-      // Ex: Hz(y-1), Hz, Hy(z-1), Hy
-      float a0 = sH[2][ty][tz + 1], a1 = sH[2][ty + 1][tz + 1], a2 = sH[1][ty + 1][tz], a3 = sH[1][ty + 1][tz + 1];
-      // Ey: Hx(z-1), Hx, Hz(x-1), Hz
-      float b0 = sH[0][ty + 1][tz], b1 = sH[0][ty + 1][tz + 1], b2 = hp[2], b3 = sH[2][ty + 1][tz + 1];
-      // Ez: Hy(x-1), Hy, Hx(y-1), Hx
-      float c0 = hp[1], c1 = sH[1][ty + 1][tz + 1], c2 = sH[0][ty][tz + 1], c3 = sH[0][ty + 1][tz + 1];
+      // Ex: Hz(y-1), Hz, Hy(z-1), Hy ; Ey: Hx(z-1), Hx, Hz(x-1), Hz ; Ez: Hy(x-1), Hy, Hx(y-1), Hx
+      float a0 = sH[2][ty][tz + 1], a1 = h2, a2 = sH[1][ty + 1][tz], a3 = h1;
+      float b0 = sH[0][ty + 1][tz], b1 = h0, b2 = hp2, b3 = h2;
+      float c0 = hp1, c1 = h1, c2 = sH[0][ty][tz + 1], c3 = h0;
       if (yz_face || (p.use_tfsf && on_face (p.face[0], x)))
       {
         tfsf_apply (p, 0, p.inc_h, err, x, y, z, a0, a1, a2, a3);
         tfsf_apply (p, 1, p.inc_h, err, x, y, z, b0, b1, b2, b3);
         tfsf_apply (p, 2, p.inc_h, err, x, y, z, c0, c1, c2, c3);
       }
-      const bool st_aux = owner && x <= xb;
-      const float cu[3] = {(a1 - a0) - (a3 - a2), (b1 - b0) - (b3 - b2), (c1 - c0) - (c3 - c2)};
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
+      const bool st = owner && x <= xb;
+      en0 = update_any<0, META> (p, fl, yz_in[0] && x >= p.ilo[0][0] && x < p.ihi[0][0], eo0, (a1 - a0) - (a3 - a2),
+                                 i0, x, y, z, id, st);
+      en1 = update_any<1, META> (p, fl, yz_in[1] && x >= p.ilo[1][0] && x < p.ihi[1][0], eo1, (b1 - b0) - (b3 - b2),
+                                 i1, x, y, z, id, st);
+      en2 = update_any<2, META> (p, fl, yz_in[2] && x >= p.ilo[2][0] && x < p.ihi[2][0], eo2, (c1 - c0) - (c3 - c2),
+                                 i2, x, y, z, id, st);
+      if ((p.ps_mask & 7) && x == p.ps[0] && y == p.ps[1] && z == p.ps[2])
       {
-        if (META && (fl & (1u << c)))
-          en[c] = update_drude (p, c, eo[c], cu[c], x, y, z, id, st_aux);
-        else
-          en[c] = update (p, c, yz_in[c] && x >= p.ilo[c][0] && x < p.ihi[c][0], eo[c], cu[c], inv[c], x, y, z, id,
-                          st_aux);
+        const float v = (float) p.src[p.src_index];
+        if (p.ps_mask & 1)
+          en0 = v;
+        if (p.ps_mask & 2)
+          en1 = v;
+        if (p.ps_mask & 4)
+          en2 = v;
       }
-      if (p.ps_mask & 7)
+      if (st)
       {
-        if (x == p.ps[0] && y == p.ps[1] && z == p.ps[2])
-        {
-          float v = (float) p.src[p.src_index];
-#pragma unroll
-          for (int c = 0; c < 3; ++c)
-            if (p.ps_mask & (1 << c))
-              en[c] = v;
-        }
-      }
-      if (owner && x <= xb)
-      {
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-          stf (En[c], id, en[c]);
+        stf (En0, id, en0);
+        stf (En1, id, en1);
+        stf (En2, id, en2);
       }
     }
 
-    // 3. H_new(x-1) on the tile
+    // 4. H_new(x - 1) on the tile
     const int xh = x - 1;
     if (owner && xh >= xa)
     {
       const size_t hid = id - sx;
-      // Hx: Ey, Ey(z+1), Ez, Ez(y+1)
-      float a0 = ep[1], a1 = sE[1][ty][tz + 1], a2 = ep[2], a3 = sE[2][ty + 1][tz];
-      // Hy: Ez, Ez(x+1), Ex, Ex(z+1)
-      float b0 = ep[2], b1 = en[2], b2 = ep[0], b3 = sE[0][ty][tz + 1];
-      // Hz: Ex, Ex(y+1), Ey, Ey(x+1)
-      float c0 = ep[0], c1 = sE[0][ty + 1][tz], c2 = ep[1], c3 = en[1];
+      // Hx: Ey, Ey(z+1), Ez, Ez(y+1) ; Hy: Ez, Ez(x+1), Ex, Ex(z+1) ; Hz: Ex, Ex(y+1), Ey, Ey(x+1)
+      float a0 = ep1, a1 = sE[1][ty][tz + 1], a2 = ep2, a3 = sE[2][ty + 1][tz];
+      float b0 = ep2, b1 = en2, b2 = ep0, b3 = sE[0][ty][tz + 1];
+      float c0 = ep0, c1 = sE[0][ty + 1][tz], c2 = ep1, c3 = en1;
       if (yz_face || (p.use_tfsf && on_face (p.face[0], xh)))
       {
         tfsf_apply (p, 3, p.inc_e, err, xh, y, z, a0, a1, a2, a3);
         tfsf_apply (p, 4, p.inc_e, err, xh, y, z, b0, b1, b2, b3);
         tfsf_apply (p, 5, p.inc_e, err, xh, y, z, c0, c1, c2, c3);
       }
-      float hn[3];
-      const float cu[3] = {(a1 - a0) - (a3 - a2), (b1 - b0) - (b3 - b2), (c1 - c0) - (c3 - c2)};
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
+      float hn0 = update_any<3, META> (p, flp, yz_in[3] && xh >= p.ilo[3][0] && xh < p.ihi[3][0], hp0,
+                                       (a1 - a0) - (a3 - a2), 1.f, xh, y, z, hid, true);
+      float hn1 = update_any<4, META> (p, flp, yz_in[4] && xh >= p.ilo[4][0] && xh < p.ihi[4][0], hp1,
+                                       (b1 - b0) - (b3 - b2), 1.f, xh, y, z, hid, true);
+      float hn2 = update_any<5, META> (p, flp, yz_in[5] && xh >= p.ilo[5][0] && xh < p.ihi[5][0], hp2,
+                                       (c1 - c0) - (c3 - c2), 1.f, xh, y, z, hid, true);
+      if ((p.ps_mask & 56) && xh == p.ps[0] && y == p.ps[1] && z == p.ps[2])
       {
-        if (META && (flp & (8u << c)))
-          hn[c] = update_drude (p, 3 + c, hp[c], cu[c], xh, y, z, hid, true);
-        else
-          hn[c] = update (p, 3 + c, yz_in[3 + c] && xh >= p.ilo[3 + c][0] && xh < p.ihi[3 + c][0], hp[c], cu[c], 1.f,
-                          xh, y, z, hid, true);
+        const float v = (float) p.src[p.src_index + 1] * p.ps_scale_h;
+        if (p.ps_mask & 8)
+          hn0 = v;
+        if (p.ps_mask & 16)
+          hn1 = v;
+        if (p.ps_mask & 32)
+          hn2 = v;
       }
-      if (p.ps_mask & 56)
-      {
-        if (xh == p.ps[0] && y == p.ps[1] && z == p.ps[2])
-        {
-          float v = (float) p.src[p.src_index + 1] * p.ps_scale_h;
-#pragma unroll
-          for (int c = 0; c < 3; ++c)
-            if (p.ps_mask & (8 << c))
-              hn[c] = v;
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-        stf (Hn[c], hid, hn[c]);
+      stf (Hn0, hid, hn0);
+      stf (Hn1, hid, hn1);
+      stf (Hn2, hid, hn2);
     }
     __syncthreads ();
 
-    // 4. carry plane x into the next iteration
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-    {
-      sE[c][ty][tz] = valid ? en[c] : 0.f;
-      ep[c] = en[c];
-      hp[c] = sH[c][ty + 1][tz + 1];
-    }
+    // 5. carry plane x into the next iteration
+    sE[0][ty][tz] = valid ? en0 : 0.f;
+    sE[1][ty][tz] = valid ? en1 : 0.f;
+    sE[2][ty][tz] = valid ? en2 : 0.f;
+    ep0 = en0;
+    ep1 = en1;
+    ep2 = en2;
+    hp0 = h0;
+    hp1 = h1;
+    hp2 = h2;
     flp = fl;
   }
 }
@@ -465,25 +502,38 @@ __global__ void drude_flags_kernel (unsigned char *flags, const float *ome, cons
 
 }  // namespace
 
-int launch_fused3d (const FusedParams &p, int *err, cudaStream_t s)
+template <int TY, int MINB>
+void launch_shape (const FusedParams &p, int *err, cudaStream_t s)
 {
-  constexpr int TY = 8, TZ = 32;
+  constexpr int TZ = 32;
   const int ny = p.g.n[1], nz = p.g.n[2], nx = p.g.n[0];
   dim3 block (TZ + 1, TY + 1);
   dim3 grid ((nz - 2 + TZ - 1) / TZ, (ny - 2 + TY - 1) / TY, (nx - 2 + p.x_chunk - 1) / p.x_chunk);
   if (p.use_meta)
   {
     if (p.fp16)
-      fused3d_kernel<__half, TY, TZ, true><<<grid, block, 0, s>>> (p, err);
+      fused3d_kernel<__half, TY, TZ, true, MINB><<<grid, block, 0, s>>> (p, err);
     else
-      fused3d_kernel<float, TY, TZ, true><<<grid, block, 0, s>>> (p, err);
+      fused3d_kernel<float, TY, TZ, true, MINB><<<grid, block, 0, s>>> (p, err);
   }
   else
   {
     if (p.fp16)
-      fused3d_kernel<__half, TY, TZ, false><<<grid, block, 0, s>>> (p, err);
+      fused3d_kernel<__half, TY, TZ, false, MINB><<<grid, block, 0, s>>> (p, err);
     else
-      fused3d_kernel<float, TY, TZ, false><<<grid, block, 0, s>>> (p, err);
+      fused3d_kernel<float, TY, TZ, false, MINB><<<grid, block, 0, s>>> (p, err);
+  }
+}
+
+int launch_fused3d (const FusedParams &p, int *err, cudaStream_t s)
+{
+  switch (p.shape)
+  {
+    case 0: launch_shape<8, 2> (p, err, s); break;
+    case 1: launch_shape<8, 3> (p, err, s); break;
+    case 2: launch_shape<4, 4> (p, err, s); break;
+    case 3: launch_shape<16, 1> (p, err, s); break;
+    default: launch_shape<4, 6> (p, err, s); break;
   }
   return 1;
 }

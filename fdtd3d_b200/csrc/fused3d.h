@@ -14,6 +14,7 @@ struct FusedParams
   int use_tfsf;
   int fp16;
   int x_chunk;                 // x planes per CTA
+  int shape;                   // tile / occupancy variant (see launch_fused3d)
   CompDev comp[6];             // Ex..Hz
   const void *e_old[3];
   const void *h_old[3];

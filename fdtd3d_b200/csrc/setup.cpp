@@ -278,6 +278,10 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
     return "unknown precision";
   if (cfg.use_metamaterials && !cfg.use_pml)
     return "metamaterials require PML (as in the reference)";
+  if (cfg.point_source_kind != FDTD_SOURCE_SINE && cfg.point_source_kind != FDTD_SOURCE_GAUSSIAN)
+    return "unknown point-source kind";
+  if (cfg.point_source_kind == FDTD_SOURCE_GAUSSIAN && !(cfg.point_source_bandwidth > 0))
+    return "Gaussian point source needs a positive bandwidth";
   g.tmz = cfg.mode == FDTD_MODE_TMZ;
   g.n[0] = cfg.size[0];
   g.n[1] = cfg.size[1];
@@ -441,6 +445,21 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
   return "";
 }
 
+std::vector<double> sigma_at (const Geometry &g, int k, int b)
+{
+  const std::vector<double> &s = g.sigma[b];
+  int n = g.n[b];
+  std::vector<double> out (n, 0.0);
+  int a = k % 3;
+  bool isH = k >= 3;
+  bool averaged = isH ? (b != a) : (b == a);
+  if (g.tmz && b == 2)
+    averaged = false;
+  for (int i = 0; i < n; ++i)
+    out[i] = (averaged && i + 1 < n) ? (s[i] + s[i + 1]) / 2.0 : s[i];
+  return out;
+}
+
 double incident_source (const Geometry &g, uint32_t t)
 {
   return std::sin (g.dt * t * 2 * kPi * g.freq);
@@ -449,6 +468,13 @@ double incident_source (const Geometry &g, uint32_t t)
 double point_source (const Geometry &g, uint32_t t, bool h)
 {
   double ts = t + (h ? 1.0 : 0.5);
+  if (g.cfg.point_source_kind == FDTD_SOURCE_GAUSSIAN)
+  {
+    // Gaussian-modulated pulse: spectral FWHM = bandwidth * f
+    double w = 4.0 * std::sqrt (std::log (2.0)) / (kPi * g.freq * g.cfg.point_source_bandwidth);
+    double tau = g.dt * ts - 3.0 * w;
+    return std::exp (-(tau / w) * (tau / w)) * std::sin (2 * kPi * g.freq * tau);
+  }
   return std::sin (g.dt * ts * 2 * kPi * g.freq);
 }
 

@@ -71,6 +71,11 @@ struct Geometry
 // Builds the geometry; returns an error message or "" on success.
 std::string build_geometry (const fdtd_config &cfg, Geometry &g);
 
+// Sigma profile of axis b averaged at the position of component k, as the
+// reference's getMaterial averages the sigma grids (two points along the
+// component's own axis for E, along the other two axes for H).
+std::vector<double> sigma_at (const Geometry &g, int k, int b);
+
 // sin(2 pi f dt t) hard source of the incident grid at time step t.
 double incident_source (const Geometry &g, uint32_t t);
 // point-source value for an E (h = false) or H (h = true) component.

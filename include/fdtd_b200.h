@@ -97,11 +97,21 @@ typedef struct
   int use_tfsf;
   int use_metamaterials;    /* requires use_pml, as in the reference */
   int point_source[3];
-  int point_source_mask;    /* bit c: hard sinusoidal source on component c */
+  int point_source_mask;    /* bit c: hard source on component c */
+  int point_source_kind;    /* 0: the reference's sin(2 pi f t); 1: Gaussian-modulated (see below) */
+  double point_source_bandwidth; /* kind 1: spectral FWHM / f (e.g. 0.5) */
   int precision;            /* FDTD_PREC_* */
   int layout;               /* 0 = E_CENTERED (the only layout provided) */
   int reserved[8];
 } fdtd_config;
+
+/* Point-source kinds.  Kind 0 is the reference's hard source
+ * sin(2 pi f dt (t + 1/2)) on E, (t + 1) on H (InternalScheme.inc.h:2818-2895).
+ * Kind 1 (no counterpart in the reference) is a Gaussian-modulated pulse at
+ * the same instants tau: exp(-((tau - t0) / w)^2) sin(2 pi f (tau - t0)),
+ * w = 4 sqrt(ln 2) / (pi f B), t0 = 3 w, B = point_source_bandwidth. */
+#define FDTD_SOURCE_SINE 0
+#define FDTD_SOURCE_GAUSSIAN 1
 
 /* Replaces InternalSchemeGPU::initFromCPU + initOnGPU
  * (Source/Scheme/InternalScheme.specific.h:506-563) and the set-up half of
@@ -170,6 +180,35 @@ int fdtd_kernel_time (fdtd_ctx *ctx, double *ms, int64_t *launches);
 /* Releases every device resource of the context; replaces
  * InternalSchemeGPU::uninitFromCPU/uninitOnGPU. */
 void fdtd_destroy (fdtd_ctx *ctx);
+
+/*
+ * Batched 2-D TMz (no counterpart in the reference, whose runs are one grid
+ * per process): many Dim2_TMz simulations of different sizes advanced
+ * together by one persistent kernel launch per fdtd_batch_step call,
+ * captured in a CUDA graph.  `base` gives the shared physics (dx,
+ * wavelength, Courant factor, PML width, point-source kind/bandwidth and the
+ * Ez bit of point_source_mask); precision must be FDTD_PREC_FP32 and TF/SF
+ * and metamaterials are not provided.  `sizes` holds count (nx, ny) pairs;
+ * every instance's point source sits at (nx/2, ny/2).  Semantics per
+ * instance are those of fdtd_step on the same configuration.
+ */
+typedef struct fdtd_batch fdtd_batch;
+int fdtd_batch_create (const fdtd_config *base, int count, const int *sizes, int device, fdtd_batch **out);
+/* eps of one instance: nx*ny host doubles, (x, y) with y fastest */
+int fdtd_batch_upload_eps (fdtd_batch *b, int instance, const double *host);
+/* Times every candidate launch shape (x chunk of a warp tile, warps per CTA,
+ * CTAs per SM) over `steps` steps of the real batch, keeps the fastest,
+ * then resets the fields to t = 0.  choice[3] receives the shape. */
+int fdtd_batch_tune (fdtd_batch *b, int steps, int *choice);
+int fdtd_batch_step (fdtd_batch *b, uint32_t t_start, uint32_t n_steps);
+int fdtd_batch_sync (fdtd_batch *b, int64_t timeout_ns);
+/* component: FDTD_EZ, FDTD_HX or FDTD_HY of one instance, nx*ny doubles */
+int fdtd_batch_download (fdtd_batch *b, int instance, int component, double *host);
+/* total cells, whether the last step ran from a CUDA graph, and the device
+ * milliseconds of the last launch (valid after fdtd_batch_sync) */
+int fdtd_batch_info (const fdtd_batch *b, int64_t *cells, int *graph_used, double *last_ms);
+const char *fdtd_batch_last_error (const fdtd_batch *b);
+void fdtd_batch_destroy (fdtd_batch *b);
 
 /* Compensated FP64 sum of weight[i] * src[i]^2 * scale over n elements,
  * written to out_dev (a caller-owned device double), for callers that must

@@ -798,7 +798,19 @@ static void field_half_step (struct fdtd_oracle *o, int k, uint32_t t)
     if (ps[0] >= 0 && ps[0] < o->nx && ps[1] >= 0 && ps[1] < o->ny && pz >= 0 && pz < o->nz)
     {
       double ts = t + (k >= 3 ? 1.0 : 0.5);
-      o->f[k][0][idx (o, ps[0], ps[1], pz)] = sin (o->dt * ts * 2 * ORC_PI * o->freq);
+      double v;
+      if (o->cfg.point_source_kind == 1)
+      {
+        /* project-defined Gaussian-modulated pulse (no reference counterpart) */
+        double w = 4.0 * sqrt (log (2.0)) / (ORC_PI * o->freq * o->cfg.point_source_bandwidth);
+        double tau = o->dt * ts - 3.0 * w;
+        v = exp (-(tau / w) * (tau / w)) * sin (2 * ORC_PI * o->freq * tau);
+      }
+      else
+      {
+        v = sin (o->dt * ts * 2 * ORC_PI * o->freq);
+      }
+      o->f[k][0][idx (o, ps[0], ps[1], pz)] = v;
     }
   }
 }

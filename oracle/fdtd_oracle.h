@@ -41,6 +41,8 @@ typedef struct
   int point_source[3];
   int point_source_mask;      /* bit c set -> hard source on component c (Ex..Hz) */
   int skip_first_update;      /* 1 = fdtd3d driver (no field update at t == 0) */
+  int point_source_kind;      /* 0 = reference sine, 1 = Gaussian-modulated pulse */
+  double point_source_bandwidth;
 } fdtd_oracle_cfg;
 
 typedef struct fdtd_oracle fdtd_oracle;

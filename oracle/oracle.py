@@ -56,6 +56,8 @@ class _Cfg(ctypes.Structure):
         ("point_source", ctypes.c_int * 3),
         ("point_source_mask", ctypes.c_int),
         ("skip_first_update", ctypes.c_int),
+        ("point_source_kind", ctypes.c_int),
+        ("point_source_bandwidth", ctypes.c_double),
     ]
 
 
@@ -98,7 +100,7 @@ class Oracle:
                  dx=0.0005, wavelength=0.02, courant=0.5, teta=90.0, phi=0.0, psi=90.0,
                  use_pml=False, use_tfsf=False, use_metamaterials=False,
                  point_source=(0, 0, 0), point_source_mask=0, skip_first_update=True,
-                 materials=None):
+                 point_source_kind=0, point_source_bandwidth=0.0, materials=None, precision=None):
         c = _Cfg()
         c.mode = mode
         size = _triple(size, 1)
@@ -114,6 +116,8 @@ class Oracle:
         c.point_source[:] = _triple(point_source, 0)
         c.point_source_mask = point_source_mask
         c.skip_first_update = int(skip_first_update)
+        c.point_source_kind = int(point_source_kind)
+        c.point_source_bandwidth = float(point_source_bandwidth)
         self.cfg = c
         self.shape = (size[0], size[1], size[2]) if mode == 3 else (size[0], size[1])
         self.n = int(np.prod(self.shape))
