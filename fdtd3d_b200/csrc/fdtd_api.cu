@@ -497,15 +497,14 @@ void init_fused (fdtd_ctx *ctx)
   f.inc_len = g.inc_len;
   // tile / occupancy variant of the one-sweep kernel; FDTDB_FUSED_SHAPE
   // overrides the default for tuning runs
-  f.shape = 1;
+  f.shape = 3;
   if (const char *v = std::getenv ("FDTDB_FUSED_SHAPE"))
     f.shape = std::atoi (v);
-  const int ty_of_shape[5] = {8, 8, 4, 16, 4};
-  int tyv = ty_of_shape[(f.shape >= 0 && f.shape < 5) ? f.shape : 1];
+  int tyv = fused_rows_per_cta (f.shape);
   if (const char *v = std::getenv ("FDTDB_FUSED_CHUNK"))
     chunk_override = std::atoi (v);
-  int tiles = ((g.n[2] - 2 + 31) / 32) * ((g.n[1] - 2 + tyv - 1) / tyv);
-  int64_t want = (int64_t) ctx->sm_count * 3 * 8;
+  int tiles = ((g.n[2] - 2 + 30) / 31) * ((g.n[1] - 2 + tyv - 1) / tyv);
+  int64_t want = (int64_t) ctx->sm_count * 8 * 4;
   int64_t chunk = ((int64_t) (g.n[0] - 2) * tiles) / std::max<int64_t> (want, 1);
   f.x_chunk = (int) std::min<int64_t> (128, std::max<int64_t> (16, chunk));
   if (chunk_override > 0)

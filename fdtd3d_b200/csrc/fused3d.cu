@@ -231,221 +231,251 @@ __device__ __forceinline__ float update_any (const FusedParams &p, unsigned fl, 
   return update_k<K> (p, interior, f, curl, inv_m, x, y, z, id, store);
 }
 
-template <typename T, int TY, int TZ, bool META, int MINB>
-__global__ void __launch_bounds__ ((TY + 1) * (TZ + 1), MINB) fused3d_kernel (FusedParams p, int *err)
+// One-sweep kernel.  CTA = W warps stacked along y; a warp covers 32 z
+// positions (lanes 0..30 owned, lane 31 the z ring) and R consecutive y
+// rows per thread, so each thread keeps a small column of cells in
+// registers.  The last row of the last warp is the CTA's y ring, so a CTA
+// owns 31 x (R*W - 1) cells of every x plane of its chunk.  Neighbours move
+// by warp shuffles (z), registers (y inside a warp, x between planes) and
+// a parity-double-buffered shared row per warp boundary (y), so one
+// __syncthreads per plane is enough.
+template <typename T, int R, int W, bool META>
+__global__ void __launch_bounds__ (32 * W) fused3d_kernel (FusedParams p, int *err)
 {
   const int nx = p.g.n[0], ny = p.g.n[1], nz = p.g.n[2];
-  const int tz = threadIdx.x;
-  const int ty = threadIdx.y;
-  const int y0 = 1 + blockIdx.y * TY;
-  const int z0 = 1 + blockIdx.x * TZ;
-  const int y = y0 + ty;
-  const int z = z0 + tz;
+  const int lane = threadIdx.x;
+  const int w = threadIdx.y;
+  const int z0 = 1 + blockIdx.x * 31;
+  const int z = z0 + lane;
+  const int yw = 1 + blockIdx.y * (R * W - 1) + w * R;
   const int xa = 1 + blockIdx.z * p.x_chunk;
   const int xb = min (xa + p.x_chunk - 1, nx - 2);
-  const bool valid = y <= ny - 1 && z <= nz - 1;
-  const bool inner = y <= ny - 2 && z <= nz - 2;          // y, z >= 1 always
-  const bool owner = tz < TZ && ty < TY && inner;
+  const bool zvalid = z <= nz - 1;
+  const bool zinner = z <= nz - 2;
+  const bool zown = lane < 31 && zinner;
+  const unsigned FULL = 0xffffffffu;
   const size_t sx = (size_t) ny * nz;
-  const size_t col = (size_t) y * nz + z;
-  const bool halo_y = ty == 0 && z <= nz - 1;              // loads (y - 1) for Hx, Hz
-  const bool halo_z = tz == 0 && y <= ny - 1;              // loads (z - 1) for Hx, Hy
-  const bool ring_y = ty == TY && p.eps && y + 1 <= ny - 1 && z <= nz - 1;
-  const bool ring_z = tz == TZ && p.eps && z + 1 <= nz - 1 && y <= ny - 1;
 
-  __shared__ float sH[3][TY + 2][TZ + 2];
-  __shared__ float sE[3][TY + 1][TZ + 1];
-  __shared__ float sEps[TY + 2][TZ + 2];
+  __shared__ float sHb[2][W + 1][2][32];   // [parity][warp + 1][Hz, Hx][lane]: row above each warp
+  __shared__ float sEb[2][W][2][32];       // [parity][warp][Ex, Ez][lane]: E_new of each warp's first row
 
-  bool yz_in[6];
+  bool rvalid[R], rinner[R], rown[R];
+  unsigned yzin = 0;                       // bit k*R + r: component k, row r has sigma == 0 along y and z
+  unsigned face = 0;                       // bit r: row r lies on a TF/SF face plane along y or z
 #pragma unroll
-  for (int k = 0; k < 6; ++k)
-    yz_in[k] = !p.use_pml || (y >= p.ilo[k][1] && y < p.ihi[k][1] && z >= p.ilo[k][2] && z < p.ihi[k][2]);
-  const bool yz_face = p.use_tfsf && (on_face (p.face[1], y) || on_face (p.face[2], z));
+  for (int r = 0; r < R; ++r)
+  {
+    const int y = yw + r;
+    rvalid[r] = y <= ny - 1 && zvalid;
+    rinner[r] = y <= ny - 2 && zinner;
+    rown[r] = rinner[r] && lane < 31 && !(w == W - 1 && r == R - 1);
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+      if (!p.use_pml || (y >= p.ilo[k][1] && y < p.ihi[k][1] && z >= p.ilo[k][2] && z < p.ihi[k][2]))
+        yzin |= 1u << (k * R + r);
+    if (p.use_tfsf && (on_face (p.face[1], y) || on_face (p.face[2], z)))
+      face |= 1u << r;
+  }
 
-  const T *Eo0 = (const T *) p.e_old[0], *Eo1 = (const T *) p.e_old[1], *Eo2 = (const T *) p.e_old[2];
   const T *Ho0 = (const T *) p.h_old[0], *Ho1 = (const T *) p.h_old[1], *Ho2 = (const T *) p.h_old[2];
+  const T *Eo0 = (const T *) p.e_old[0], *Eo1 = (const T *) p.e_old[1], *Eo2 = (const T *) p.e_old[2];
   T *En0 = (T *) p.e_new[0], *En1 = (T *) p.e_new[1], *En2 = (T *) p.e_new[2];
   T *Hn0 = (T *) p.h_new[0], *Hn1 = (T *) p.h_new[1], *Hn2 = (T *) p.h_new[2];
+  const float *eps = p.eps;
 
-  // registers of the plane being fetched (software pipeline, one plane ahead)
-  float fh0 = 0.f, fh1 = 0.f, fh2 = 0.f, fe0 = 0.f, fe1 = 0.f, fe2 = 0.f;
-  float feps = 1.f, feps1 = 1.f, fhy0 = 0.f, fhy2 = 0.f, fhz0 = 0.f, fhz1 = 0.f, fry = 1.f, frz = 1.f;
-  unsigned ffl = 0;
-  auto fetch = [&] (int x) {
-    const size_t id = (size_t) x * sx + col;
-    if (valid)
-    {
-      fh0 = ldf (Ho0, id);
-      fh1 = ldf (Ho1, id);
-      fh2 = ldf (Ho2, id);
-      fe0 = ldf (Eo0, id);
-      fe1 = ldf (Eo1, id);
-      fe2 = ldf (Eo2, id);
-      if (p.eps)
-      {
-        feps = __ldg (p.eps + id);
-        feps1 = x + 1 <= nx - 1 ? __ldg (p.eps + id + sx) : 1.f;
-      }
-      if (META)
-        ffl = p.dflag[id];
-    }
-    if (halo_y)
-    {
-      fhy0 = ldf (Ho0, id - nz);
-      fhy2 = ldf (Ho2, id - nz);
-    }
-    if (halo_z)
-    {
-      fhz0 = ldf (Ho0, id - 1);
-      fhz1 = ldf (Ho1, id - 1);
-    }
-    if (ring_y)
-      fry = __ldg (p.eps + id + nz);
-    if (ring_z)
-      frz = __ldg (p.eps + id + 1);
-  };
-
-  float hp0 = 0.f, hp1 = 0.f, hp2 = 0.f;   // H_old(x - 1), own cell
-  float ep0 = 0.f, ep1 = 0.f, ep2 = 0.f;   // E_new(x - 1), own cell
-  unsigned flp = 0;
-  if (valid)
+  float hp[3][R], ep[3][R], epsc[R];
+  unsigned char flp[R];
   {
-    const size_t id = (size_t) (xa - 1) * sx + col;
-    hp0 = ldf (Ho0, id);
-    hp1 = ldf (Ho1, id);
-    hp2 = ldf (Ho2, id);
-    if (META)
-      flp = p.dflag[id];
+    const size_t b0 = (size_t) (xa - 1) * sx + (size_t) yw * nz + z;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+    {
+      const size_t id = b0 + (size_t) r * nz;
+      hp[0][r] = rvalid[r] ? ldf (Ho0, id) : 0.f;
+      hp[1][r] = rvalid[r] ? ldf (Ho1, id) : 0.f;
+      hp[2][r] = rvalid[r] ? ldf (Ho2, id) : 0.f;
+      ep[0][r] = ep[1][r] = ep[2][r] = 0.f;
+      epsc[r] = (eps && rvalid[r]) ? __ldg (eps + id + sx) : 1.f;
+      flp[r] = (META && rvalid[r]) ? p.dflag[id] : 0;
+    }
   }
-  fetch (xa);
 
   for (int x = xa; x <= xb + 1; ++x)
   {
-    const size_t id = (size_t) x * sx + col;
-    // 1. stage the fetched plane
-    sH[0][ty + 1][tz + 1] = fh0;
-    sH[1][ty + 1][tz + 1] = fh1;
-    sH[2][ty + 1][tz + 1] = fh2;
-    sEps[ty][tz] = feps;
-    if (ty == 0)
+    const int par = x & 1;
+    const size_t b = (size_t) x * sx + (size_t) yw * nz + z;
+    // ---- loads of plane x (independent, all in flight together)
+    float h[3][R], e[3][R], epsn[R];
+    unsigned char fl[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
     {
-      sH[0][0][tz + 1] = fhy0;
-      sH[2][0][tz + 1] = fhy2;
+      const size_t id = b + (size_t) r * nz;
+      h[0][r] = rvalid[r] ? ldf (Ho0, id) : 0.f;
+      h[1][r] = rvalid[r] ? ldf (Ho1, id) : 0.f;
+      h[2][r] = rvalid[r] ? ldf (Ho2, id) : 0.f;
+      e[0][r] = rvalid[r] ? ldf (Eo0, id) : 0.f;
+      e[1][r] = rvalid[r] ? ldf (Eo1, id) : 0.f;
+      e[2][r] = rvalid[r] ? ldf (Eo2, id) : 0.f;
+      epsn[r] = (eps && rvalid[r] && x + 1 <= nx - 1) ? __ldg (eps + id + sx) : 1.f;
+      fl[r] = (META && rvalid[r]) ? p.dflag[id] : 0;
     }
-    if (tz == 0)
+    float hzl_x[R], hzl_y[R], epz[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
     {
-      sH[0][ty + 1][0] = fhz0;
-      sH[1][ty + 1][0] = fhz1;
+      const size_t id = b + (size_t) r * nz;
+      const bool rv = yw + r <= ny - 1;
+      hzl_x[r] = (lane == 0 && rv) ? ldf (Ho0, id - 1) : 0.f;
+      hzl_y[r] = (lane == 0 && rv) ? ldf (Ho1, id - 1) : 0.f;
+      epz[r] = (eps && lane == 31 && rv && z + 1 <= nz - 1) ? __ldg (eps + id + 1) : 1.f;
     }
-    if (ty == TY)
-      sEps[TY + 1][tz] = fry;
-    if (tz == TZ)
-      sEps[ty][TZ + 1] = frz;
-    const float eo0 = fe0, eo1 = fe1, eo2 = fe2;
-    const float epsx1 = feps1;
-    const unsigned fl = ffl;
-    const float h0 = fh0, h1 = fh1, h2 = fh2;
+    const float epsy = (eps && zvalid && yw + R <= ny - 1) ? __ldg (eps + b + (size_t) R * nz) : 1.f;
+    if (w == 0)
+    {
+      sHb[par][0][0][lane] = zvalid ? ldf (Ho2, b - nz) : 0.f;
+      sHb[par][0][1][lane] = zvalid ? ldf (Ho0, b - nz) : 0.f;
+    }
+    sHb[par][w + 1][0][lane] = h[2][R - 1];
+    sHb[par][w + 1][1][lane] = h[0][R - 1];
     __syncthreads ();
-    // 2. next plane in flight while this one computes
-    if (x + 1 <= xb + 1)
-      fetch (x + 1);
 
-    // 3. E_new(x) on tile + ring
-    float en0 = eo0, en1 = eo1, en2 = eo2;
-    if (inner && x <= nx - 2)
+    // ---- E_new(x), all rows of this warp including the rings
+    const bool xin = x <= nx - 2;
+    const bool xface = p.use_tfsf && on_face (p.face[0], x);
+    const bool xi0 = x >= p.ilo[0][0] && x < p.ihi[0][0];
+    const bool xi1 = x >= p.ilo[1][0] && x < p.ihi[1][0];
+    const bool xi2 = x >= p.ilo[2][0] && x < p.ihi[2][0];
+    const bool ps_e = (p.ps_mask & 7) && x == p.ps[0];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
     {
-      float i0 = 1.f, i1 = 1.f, i2 = 1.f;
-      if (p.eps)
+      const float hz_ym = r == 0 ? sHb[par][w][0][lane] : h[2][r - 1];
+      const float hx_ym = r == 0 ? sHb[par][w][1][lane] : h[0][r - 1];
+      float hy_zm = __shfl_up_sync (FULL, h[1][r], 1);
+      float hx_zm = __shfl_up_sync (FULL, h[0][r], 1);
+      if (lane == 0)
       {
-        const float e0 = sEps[ty][tz];
-        i0 = __fdividef (2.f, e0 + epsx1);
-        i1 = __fdividef (2.f, e0 + sEps[ty + 1][tz]);
-        i2 = __fdividef (2.f, e0 + sEps[ty][tz + 1]);
+        hy_zm = hzl_y[r];
+        hx_zm = hzl_x[r];
       }
-      // Ex: Hz(y-1), Hz, Hy(z-1), Hy ; Ey: Hx(z-1), Hx, Hz(x-1), Hz ; Ez: Hy(x-1), Hy, Hx(y-1), Hx
-      float a0 = sH[2][ty][tz + 1], a1 = h2, a2 = sH[1][ty + 1][tz], a3 = h1;
-      float b0 = sH[0][ty + 1][tz], b1 = h0, b2 = hp2, b3 = h2;
-      float c0 = hp1, c1 = h1, c2 = sH[0][ty][tz + 1], c3 = h0;
-      if (yz_face || (p.use_tfsf && on_face (p.face[0], x)))
+      float ez1 = __shfl_down_sync (FULL, epsc[r], 1);
+      if (lane == 31)
+        ez1 = epz[r];
+      if (rinner[r] && xin)
       {
-        tfsf_apply (p, 0, p.inc_h, err, x, y, z, a0, a1, a2, a3);
-        tfsf_apply (p, 1, p.inc_h, err, x, y, z, b0, b1, b2, b3);
-        tfsf_apply (p, 2, p.inc_h, err, x, y, z, c0, c1, c2, c3);
-      }
-      const bool st = owner && x <= xb;
-      en0 = update_any<0, META> (p, fl, yz_in[0] && x >= p.ilo[0][0] && x < p.ihi[0][0], eo0, (a1 - a0) - (a3 - a2),
-                                 i0, x, y, z, id, st);
-      en1 = update_any<1, META> (p, fl, yz_in[1] && x >= p.ilo[1][0] && x < p.ihi[1][0], eo1, (b1 - b0) - (b3 - b2),
-                                 i1, x, y, z, id, st);
-      en2 = update_any<2, META> (p, fl, yz_in[2] && x >= p.ilo[2][0] && x < p.ihi[2][0], eo2, (c1 - c0) - (c3 - c2),
-                                 i2, x, y, z, id, st);
-      if ((p.ps_mask & 7) && x == p.ps[0] && y == p.ps[1] && z == p.ps[2])
-      {
-        const float v = (float) p.src[p.src_index];
-        if (p.ps_mask & 1)
-          en0 = v;
-        if (p.ps_mask & 2)
-          en1 = v;
-        if (p.ps_mask & 4)
-          en2 = v;
-      }
-      if (st)
-      {
-        stf (En0, id, en0);
-        stf (En1, id, en1);
-        stf (En2, id, en2);
+        const int y = yw + r;
+        const size_t id = b + (size_t) r * nz;
+        float i0 = 1.f, i1 = 1.f, i2 = 1.f;
+        if (eps)
+        {
+          const float e0 = epsc[r];
+          i0 = __fdividef (2.f, e0 + epsn[r]);
+          i1 = __fdividef (2.f, e0 + (r < R - 1 ? epsc[r + 1] : epsy));
+          i2 = __fdividef (2.f, e0 + ez1);
+        }
+        float a0 = hz_ym, a1 = h[2][r], a2 = hy_zm, a3 = h[1][r];
+        float b0 = hx_zm, b1 = h[0][r], b2 = hp[2][r], b3 = h[2][r];
+        float c0 = hp[1][r], c1 = h[1][r], c2 = hx_ym, c3 = h[0][r];
+        if (xface || (face & (1u << r)))
+        {
+          tfsf_apply (p, 0, p.inc_h, err, x, y, z, a0, a1, a2, a3);
+          tfsf_apply (p, 1, p.inc_h, err, x, y, z, b0, b1, b2, b3);
+          tfsf_apply (p, 2, p.inc_h, err, x, y, z, c0, c1, c2, c3);
+        }
+        const bool st = rown[r] && x <= xb;
+        e[0][r] = update_any<0, META> (p, fl[r], xi0 && (yzin & (1u << (0 * R + r))), e[0][r],
+                                       (a1 - a0) - (a3 - a2), i0, x, y, z, id, st);
+        e[1][r] = update_any<1, META> (p, fl[r], xi1 && (yzin & (1u << (1 * R + r))), e[1][r],
+                                       (b1 - b0) - (b3 - b2), i1, x, y, z, id, st);
+        e[2][r] = update_any<2, META> (p, fl[r], xi2 && (yzin & (1u << (2 * R + r))), e[2][r],
+                                       (c1 - c0) - (c3 - c2), i2, x, y, z, id, st);
+        if (ps_e && y == p.ps[1] && z == p.ps[2])
+        {
+          const float v = (float) p.src[p.src_index];
+          if (p.ps_mask & 1)
+            e[0][r] = v;
+          if (p.ps_mask & 2)
+            e[1][r] = v;
+          if (p.ps_mask & 4)
+            e[2][r] = v;
+        }
+        if (st)
+        {
+          stf (En0, id, e[0][r]);
+          stf (En1, id, e[1][r]);
+          stf (En2, id, e[2][r]);
+        }
       }
     }
+    sEb[par][w][0][lane] = e[0][0];
+    sEb[par][w][1][lane] = e[2][0];
 
-    // 4. H_new(x - 1) on the tile
+    // ---- H_new(x - 1) on the owned rows
     const int xh = x - 1;
-    if (owner && xh >= xa)
+    if (xh >= xa)
     {
-      const size_t hid = id - sx;
-      // Hx: Ey, Ey(z+1), Ez, Ez(y+1) ; Hy: Ez, Ez(x+1), Ex, Ex(z+1) ; Hz: Ex, Ex(y+1), Ey, Ey(x+1)
-      float a0 = ep1, a1 = sE[1][ty][tz + 1], a2 = ep2, a3 = sE[2][ty + 1][tz];
-      float b0 = ep2, b1 = en2, b2 = ep0, b3 = sE[0][ty][tz + 1];
-      float c0 = ep0, c1 = sE[0][ty + 1][tz], c2 = ep1, c3 = en1;
-      if (yz_face || (p.use_tfsf && on_face (p.face[0], xh)))
+      const bool hface = p.use_tfsf && on_face (p.face[0], xh);
+      const bool xi3 = xh >= p.ilo[3][0] && xh < p.ihi[3][0];
+      const bool xi4 = xh >= p.ilo[4][0] && xh < p.ihi[4][0];
+      const bool xi5 = xh >= p.ilo[5][0] && xh < p.ihi[5][0];
+      const bool ps_h = (p.ps_mask & 56) && xh == p.ps[0];
+#pragma unroll
+      for (int r = 0; r < R; ++r)
       {
-        tfsf_apply (p, 3, p.inc_e, err, xh, y, z, a0, a1, a2, a3);
-        tfsf_apply (p, 4, p.inc_e, err, xh, y, z, b0, b1, b2, b3);
-        tfsf_apply (p, 5, p.inc_e, err, xh, y, z, c0, c1, c2, c3);
+        const float ey_zp = __shfl_down_sync (FULL, ep[1][r], 1);
+        const float ex_zp = __shfl_down_sync (FULL, ep[0][r], 1);
+        if (rown[r])
+        {
+          const int y = yw + r;
+          const size_t hid = b - sx + (size_t) r * nz;
+          const float ez_yp = r < R - 1 ? ep[2][r + 1] : sEb[par ^ 1][w + 1 < W ? w + 1 : w][1][lane];
+          const float ex_yp = r < R - 1 ? ep[0][r + 1] : sEb[par ^ 1][w + 1 < W ? w + 1 : w][0][lane];
+          float a0 = ep[1][r], a1 = ey_zp, a2 = ep[2][r], a3 = ez_yp;
+          float b0 = ep[2][r], b1 = e[2][r], b2 = ep[0][r], b3 = ex_zp;
+          float c0 = ep[0][r], c1 = ex_yp, c2 = ep[1][r], c3 = e[1][r];
+          if (hface || (face & (1u << r)))
+          {
+            tfsf_apply (p, 3, p.inc_e, err, xh, y, z, a0, a1, a2, a3);
+            tfsf_apply (p, 4, p.inc_e, err, xh, y, z, b0, b1, b2, b3);
+            tfsf_apply (p, 5, p.inc_e, err, xh, y, z, c0, c1, c2, c3);
+          }
+          float hn0 = update_any<3, META> (p, flp[r], xi3 && (yzin & (1u << (3 * R + r))), hp[0][r],
+                                           (a1 - a0) - (a3 - a2), 1.f, xh, y, z, hid, true);
+          float hn1 = update_any<4, META> (p, flp[r], xi4 && (yzin & (1u << (4 * R + r))), hp[1][r],
+                                           (b1 - b0) - (b3 - b2), 1.f, xh, y, z, hid, true);
+          float hn2 = update_any<5, META> (p, flp[r], xi5 && (yzin & (1u << (5 * R + r))), hp[2][r],
+                                           (c1 - c0) - (c3 - c2), 1.f, xh, y, z, hid, true);
+          if (ps_h && y == p.ps[1] && z == p.ps[2])
+          {
+            const float v = (float) p.src[p.src_index + 1] * p.ps_scale_h;
+            if (p.ps_mask & 8)
+              hn0 = v;
+            if (p.ps_mask & 16)
+              hn1 = v;
+            if (p.ps_mask & 32)
+              hn2 = v;
+          }
+          stf (Hn0, hid, hn0);
+          stf (Hn1, hid, hn1);
+          stf (Hn2, hid, hn2);
+        }
       }
-      float hn0 = update_any<3, META> (p, flp, yz_in[3] && xh >= p.ilo[3][0] && xh < p.ihi[3][0], hp0,
-                                       (a1 - a0) - (a3 - a2), 1.f, xh, y, z, hid, true);
-      float hn1 = update_any<4, META> (p, flp, yz_in[4] && xh >= p.ilo[4][0] && xh < p.ihi[4][0], hp1,
-                                       (b1 - b0) - (b3 - b2), 1.f, xh, y, z, hid, true);
-      float hn2 = update_any<5, META> (p, flp, yz_in[5] && xh >= p.ilo[5][0] && xh < p.ihi[5][0], hp2,
-                                       (c1 - c0) - (c3 - c2), 1.f, xh, y, z, hid, true);
-      if ((p.ps_mask & 56) && xh == p.ps[0] && y == p.ps[1] && z == p.ps[2])
-      {
-        const float v = (float) p.src[p.src_index + 1] * p.ps_scale_h;
-        if (p.ps_mask & 8)
-          hn0 = v;
-        if (p.ps_mask & 16)
-          hn1 = v;
-        if (p.ps_mask & 32)
-          hn2 = v;
-      }
-      stf (Hn0, hid, hn0);
-      stf (Hn1, hid, hn1);
-      stf (Hn2, hid, hn2);
     }
-    __syncthreads ();
 
-    // 5. carry plane x into the next iteration
-    sE[0][ty][tz] = valid ? en0 : 0.f;
-    sE[1][ty][tz] = valid ? en1 : 0.f;
-    sE[2][ty][tz] = valid ? en2 : 0.f;
-    ep0 = en0;
-    ep1 = en1;
-    ep2 = en2;
-    hp0 = h0;
-    hp1 = h1;
-    hp2 = h2;
-    flp = fl;
+    // ---- carry plane x
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+    {
+      hp[0][r] = h[0][r];
+      hp[1][r] = h[1][r];
+      hp[2][r] = h[2][r];
+      ep[0][r] = e[0][r];
+      ep[1][r] = e[1][r];
+      ep[2][r] = e[2][r];
+      epsc[r] = epsn[r];
+      flp[r] = fl[r];
+    }
   }
 }
 
@@ -502,26 +532,38 @@ __global__ void drude_flags_kernel (unsigned char *flags, const float *ome, cons
 
 }  // namespace
 
-template <int TY, int MINB>
+template <int R, int W>
 void launch_shape (const FusedParams &p, int *err, cudaStream_t s)
 {
-  constexpr int TZ = 32;
   const int ny = p.g.n[1], nz = p.g.n[2], nx = p.g.n[0];
-  dim3 block (TZ + 1, TY + 1);
-  dim3 grid ((nz - 2 + TZ - 1) / TZ, (ny - 2 + TY - 1) / TY, (nx - 2 + p.x_chunk - 1) / p.x_chunk);
+  dim3 block (32, W);
+  dim3 grid ((nz - 2 + 30) / 31, (ny - 2 + R * W - 2) / (R * W - 1), (nx - 2 + p.x_chunk - 1) / p.x_chunk);
   if (p.use_meta)
   {
     if (p.fp16)
-      fused3d_kernel<__half, TY, TZ, true, MINB><<<grid, block, 0, s>>> (p, err);
+      fused3d_kernel<__half, R, W, true><<<grid, block, 0, s>>> (p, err);
     else
-      fused3d_kernel<float, TY, TZ, true, MINB><<<grid, block, 0, s>>> (p, err);
+      fused3d_kernel<float, R, W, true><<<grid, block, 0, s>>> (p, err);
   }
   else
   {
     if (p.fp16)
-      fused3d_kernel<__half, TY, TZ, false, MINB><<<grid, block, 0, s>>> (p, err);
+      fused3d_kernel<__half, R, W, false><<<grid, block, 0, s>>> (p, err);
     else
-      fused3d_kernel<float, TY, TZ, false, MINB><<<grid, block, 0, s>>> (p, err);
+      fused3d_kernel<float, R, W, false><<<grid, block, 0, s>>> (p, err);
+  }
+}
+
+// rows per CTA for each shape (R * W - 1 owned)
+int fused_rows_per_cta (int shape)
+{
+  switch (shape)
+  {
+    case 0: return 4 * 4 - 1;
+    case 1: return 4 * 8 - 1;
+    case 2: return 8 * 4 - 1;
+    case 3: return 2 * 8 - 1;
+    default: return 6 * 4 - 1;
   }
 }
 
@@ -529,11 +571,11 @@ int launch_fused3d (const FusedParams &p, int *err, cudaStream_t s)
 {
   switch (p.shape)
   {
-    case 0: launch_shape<8, 2> (p, err, s); break;
-    case 1: launch_shape<8, 3> (p, err, s); break;
-    case 2: launch_shape<4, 4> (p, err, s); break;
-    case 3: launch_shape<16, 1> (p, err, s); break;
-    default: launch_shape<4, 6> (p, err, s); break;
+    case 0: launch_shape<4, 4> (p, err, s); break;
+    case 1: launch_shape<4, 8> (p, err, s); break;
+    case 2: launch_shape<8, 4> (p, err, s); break;
+    case 3: launch_shape<2, 8> (p, err, s); break;
+    default: launch_shape<6, 4> (p, err, s); break;
   }
   return 1;
 }

@@ -54,6 +54,8 @@ struct FusedParams
 };
 
 int launch_fused3d (const FusedParams &p, int *err, cudaStream_t s);
+// owned y rows of one CTA for a shape variant
+int fused_rows_per_cta (int shape);
 
 // Recomputes the per-cell Drude bitmask from the four material arrays.
 int launch_drude_flags (unsigned char *flags, const float *ome, const float *gae, const float *omm, const float *gam,
