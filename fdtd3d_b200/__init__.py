@@ -32,7 +32,7 @@ EXPORTED = (
     "fdtd_create", "fdtd_upload_material", "fdtd_upload_field", "fdtd_step", "fdtd_sync",
     "fdtd_download_field", "fdtd_upload_material_device", "fdtd_download_field_device",
     "fdtd_reduce", "fdtd_scalars", "fdtd_launch_count", "fdtd_destroy", "fdtd_status_str",
-    "fdtd_last_error", "fdtd_stream", "fdtd_profile", "fdtd_kernel_time",
+    "fdtd_last_error", "fdtd_stream", "fdtd_profile", "fdtd_kernel_time", "fdtd_step_kernel",
     "fdtd_batch_create", "fdtd_batch_upload_eps", "fdtd_batch_tune", "fdtd_batch_step", "fdtd_batch_sync",
     "fdtd_batch_download", "fdtd_batch_info", "fdtd_batch_last_error", "fdtd_batch_destroy",
 )
@@ -94,6 +94,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fdtd_reduce": ([vp, i, vp], i),
         "fdtd_scalars": ([vp, vp], i),
         "fdtd_launch_count": ([vp], i64),
+        "fdtd_step_kernel": ([vp], ctypes.c_char_p),
         "fdtd_destroy": ([vp], None),
         "fdtd_status_str": ([i], ctypes.c_char_p),
         "fdtd_last_error": ([], ctypes.c_char_p),
@@ -228,6 +229,11 @@ class Simulation:
 
     def launch_count(self) -> int:
         return int(self.lib.fdtd_launch_count(self._h))
+
+    @property
+    def step_kernel(self) -> str:
+        """Kernel that performed the last field update (see fdtd_step_kernel)."""
+        return self.lib.fdtd_step_kernel(self._h).decode()
 
     @property
     def stream(self) -> int:

@@ -6,7 +6,8 @@ Translation units and flags:
   csrc/setup.cpp          g++  -O2 -ffp-contract=off   host geometry/set-up (FP64, reference op order)
   csrc/plain_kernels.cu   nvcc --fmad=false            FP64 plain form + incident grid kernels
   csrc/fast_kernels.cu    nvcc                          FP32 / FP16-storage fused form, reductions
-  csrc/fused3d.cu         nvcc                          3-D single-sweep E+H kernel
+  csrc/fused3d.cu         nvcc                          3-D single-sweep E+H kernel (register-blocked)
+  csrc/sweep3d.cu         nvcc                          3-D single-sweep E+H kernel (TMA-pipelined)
   csrc/fdtd_api.cu        nvcc                          C ABI, context, launch sequence
   csrc/cli.cpp            g++ -> fdtd3d-b200            command-line drop-in over the C ABI
 """
@@ -46,7 +47,7 @@ def _units():
     ]
     if os.path.exists(os.path.join(CSRC, "fused3d.cu")):
         units.append(("fused3d.cu", [nvcc] + common))
-    for extra in ("tmz_batch.cu", "adjoint.cu", "noalloc.cu"):
+    for extra in ("sweep3d.cu", "tmz_batch.cu", "adjoint.cu", "noalloc.cu"):
         if os.path.exists(os.path.join(CSRC, extra)):
             units.append((extra, [nvcc] + common))
     return units

@@ -22,6 +22,7 @@
 
 #include "../../include/fdtd_b200.h"
 #include "fused3d.h"
+#include "sweep3d.h"
 #include "kernels.h"
 #include "setup.h"
 
@@ -93,6 +94,16 @@ struct fdtd_ctx
   FastHalf fast_e, fast_h;
   FusedParams fused;
   bool ps_interior = true;
+  // TMA-pipelined one-sweep kernel: plan built at the first step (and again
+  // when the permittivity buffer appears); state 0 = not built, 1 = in use,
+  // -1 = not applicable (the register-blocked kernel runs instead)
+  SweepPlan sweep;
+  int sweep_state = 0;
+  const float *sweep_eps = nullptr;
+  unsigned long long *sweep_ctr = nullptr;
+  std::string sweep_why;
+  const char *step_kernel = "not_stepped";
+  TfsfBand band;                          // TF/SF post pass of the sweep (band.cells > 0 when in use)
 
   double *staging = nullptr;
   double *partials = nullptr;
@@ -527,6 +538,109 @@ void init_fused (fdtd_ctx *ctx)
   f.gamma[1] = ctx->drude32[3];
 }
 
+// x chunk of the TMA sweep: items of (chunk + 2) planes each (one halo
+// plane, one recomputed E plane) over the persistent CTAs, plus on average
+// half an item of tail.  Candidates start at 16 planes, below which the
+// halo planes dominate.
+int sweep_chunk (const int n[3], int wy, int ctas)
+{
+  static const int cand[] = {16, 24, 32, 48, 64};
+  int best = 32;
+  double best_t = 1e300;
+  for (int c : cand)
+  {
+    SweepWork w{};
+    sweep3d_items (n, wy, c, w);
+    double t = (double) w.nitems * (c + 2) / std::max (ctas, 1) + 0.5 * (c + 2);
+    if (t < best_t)
+    {
+      best_t = t;
+      best = c;
+    }
+  }
+  return best;
+}
+
+// (Re)builds the TMA sweep plan for the current buffers.  FDTDB_SWEEP=0
+// keeps the register-blocked kernel; FDTDB_SWEEP_CHUNK overrides the x
+// chunk and FDTDB_SWEEP_VERBOSE=1 prints the plan, for tuning runs.
+int plan_sweep (fdtd_ctx *ctx)
+{
+  const Geometry &g = ctx->g;
+  ctx->sweep_state = -1;
+  if (const char *v = std::getenv ("FDTDB_SWEEP"))
+    if (std::atoi (v) == 0)
+    {
+      ctx->sweep_why = "disabled by FDTDB_SWEEP=0";
+      return FDTD_OK;
+    }
+  const int wy = 8;
+  if (!ctx->sweep_ctr)
+    DALLOC (ctx->sweep_ctr, 2 * sizeof (unsigned long long));
+  void *e[2][3], *h[2][3];
+  float *aux[2][6];
+  for (int b = 0; b < 2; ++b)
+  {
+    for (int c = 0; c < 3; ++c)
+    {
+      e[b][c] = ctx->ffb[b][c];
+      h[b][c] = ctx->ffb[b][c + 3];
+    }
+    for (int k = 0; k < 6; ++k)
+      aux[b][k] = ctx->auxb[b][k];
+  }
+  // a first plan gives the CTA count the chunk choice depends on
+  std::string why = sweep3d_plan (ctx->sweep, ctx->fused, e, h, aux, ctx->mat32[0], ctx->sm_count, wy, 32,
+                                  ctx->sweep_ctr);
+  if (why.empty ())
+  {
+    int chunk = sweep_chunk (g.n, wy, ctx->sweep.ctas);
+    if (const char *v = std::getenv ("FDTDB_SWEEP_CHUNK"))
+      chunk = std::max (1, std::atoi (v));
+    why = sweep3d_plan (ctx->sweep, ctx->fused, e, h, aux, ctx->mat32[0], ctx->sm_count, wy, chunk,
+                        ctx->sweep_ctr);
+  }
+  ctx->sweep_why = why;
+  if (why.empty ())
+  {
+    ctx->sweep_state = 1;
+    ctx->sweep_eps = ctx->mat32[0];
+    // TF/SF as a post pass over the face band when the band is PML-free
+    // (FDTDB_TFSF_POST=0 keeps the corrections inside the sweep)
+    bool post = g.cfg.use_tfsf && ctx->band.cells == 0;
+    if (const char *v = std::getenv ("FDTDB_TFSF_POST"))
+      post = post && std::atoi (v) != 0;
+    if (post)
+    {
+      std::vector<int> boxes;
+      std::vector<long long> offset;
+      std::string bwhy = tfsf_band_boxes (ctx->fused, boxes, offset);
+      if (bwhy.empty () && !boxes.empty ())
+      {
+        DALLOC (ctx->band.boxes, boxes.size () * sizeof (int));
+        DALLOC (ctx->band.offset, offset.size () * sizeof (long long));
+        CK (cudaMemcpyAsync (ctx->band.boxes, boxes.data (), boxes.size () * sizeof (int), cudaMemcpyHostToDevice,
+                             ctx->stream));
+        CK (cudaMemcpyAsync (ctx->band.offset, offset.data (), offset.size () * sizeof (long long),
+                             cudaMemcpyHostToDevice, ctx->stream));
+        CK (cudaStreamSynchronize (ctx->stream));
+        ctx->band.nbox = (int) boxes.size () / 6;
+        ctx->band.cells = offset.back ();
+      }
+    }
+  }
+  if (const char *v = std::getenv ("FDTDB_SWEEP_VERBOSE"))
+    if (std::atoi (v) != 0)
+    {
+      const SweepWork &w = ctx->sweep.work;
+      std::fprintf (stderr, "sweep3d: %s wy=%d ctas=%d smem=%u tiles z=%d y=%d chunks=%d (x chunk %d) items=%d "
+                    "tfsf band boxes=%d cells=%lld\n",
+                    why.empty () ? "in use" : why.c_str (), ctx->sweep.wy, ctx->sweep.ctas, ctx->sweep.smem, w.nzt,
+                    w.nyt, w.nch, w.chunk, w.nitems, ctx->band.nbox, ctx->band.cells);
+    }
+  return FDTD_OK;
+}
+
 int create_impl (const fdtd_config *cfg, int device, fdtd_ctx *ctx)
 {
   std::string err = build_geometry (*cfg, ctx->g);
@@ -737,10 +851,26 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
       f.inc_e = ctx->einc[ctx->ecur];
       f.src = ctx->d_src;
       f.src_index = 3 * i + 1;
+      if (ctx->sweep_state == 0 || (ctx->sweep_state == 1 && ctx->sweep_eps != ctx->mat32[0]))
+        if ((r = plan_sweep (ctx)) != FDTD_OK)
+          return r;
       cudaEvent_t pe;
       if ((r = prof_begin (ctx, &pe)) != FDTD_OK)
         return r;
-      ctx->launches += launch_fused3d (f, ctx->d_err, s);
+      if (ctx->sweep_state == 1)
+      {
+        f.tfsf_post = ctx->band.cells > 0 ? 1 : 0;
+        ctx->launches += launch_sweep3d (ctx->sweep, o, f, ctx->d_err, s);
+        if (f.tfsf_post)
+          ctx->launches += launch_tfsf_post (ctx->band, f, ctx->d_err, s);
+        f.tfsf_post = 0;
+        ctx->step_kernel = "sweep3d_tma";
+      }
+      else
+      {
+        ctx->launches += launch_fused3d (f, ctx->d_err, s);
+        ctx->step_kernel = "fused3d_regblock";
+      }
       if ((r = prof_end (ctx, pe)) != FDTD_OK)
         return r;
       ctx->fcur = nw;
@@ -773,6 +903,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
           if ((r = prof_begin (ctx, &pe)) != FDTD_OK)
             return r;
           ctx->launches += launch_plain_half (p, g.inc_len, ctx->d_err, ctx->sm_count, s);
+          ctx->step_kernel = "plain_fp64";
           if ((r = prof_end (ctx, pe)) != FDTD_OK)
             return r;
         }
@@ -803,6 +934,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
           if ((r = prof_begin (ctx, &pe)) != FDTD_OK)
             return r;
           ctx->launches += launch_fast_half (p, ctx->d_err, ctx->sm_count, s);
+          ctx->step_kernel = "per_cell";
           if ((r = prof_end (ctx, pe)) != FDTD_OK)
             return r;
         }
@@ -1101,6 +1233,11 @@ int fdtd_scalars (const fdtd_ctx *ctx, double out[3])
   out[1] = ctx->g.freq;
   out[2] = ctx->g.rpv;
   return FDTD_OK;
+}
+
+const char *fdtd_step_kernel (const fdtd_ctx *ctx)
+{
+  return ctx ? ctx->step_kernel : nullptr;
 }
 
 int64_t fdtd_launch_count (const fdtd_ctx *ctx)

@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include "fused3d.h"
+#include "incident_dev.cuh"
 
 namespace fdtdb {
 
@@ -51,24 +52,6 @@ template <>
 __device__ __forceinline__ void stf<__half> (__half *p, size_t i, float v)
 {
   p[i] = __float2half_rn (v);
-}
-
-__device__ __forceinline__ double inc_at (const GeomDev &g, const double *inc, int inc_len, int *err, int k,
-                                          int px, int py, int pz)
-{
-  double d_diff = k >= 3 ? 0.5 : 0.0;
-  double x = ((double) px + g.min_fp[k][0]) - g.zero_inc[0];
-  double y = ((double) py + g.min_fp[k][1]) - g.zero_inc[1];
-  double z = ((double) pz + g.min_fp[k][2]) - g.zero_inc[2];
-  double d = x * g.s1 * g.c2 + y * g.s1 * g.s2 + z * g.c1 - d_diff;
-  int i1 = (int) d;
-  double pr2 = d - (double) i1;
-  if (i1 < 0 || i1 + 1 >= inc_len)
-  {
-    *err = 1;
-    return 0.0;
-  }
-  return (inc[i1] * (1 - pr2) + inc[i1 + 1] * pr2) * g.proj[k];
 }
 
 // TF/SF corrections of component k at (x, y, z): subtract the incident

@@ -12,6 +12,7 @@ struct FusedParams
   GeomDev g;
   int use_pml;
   int use_tfsf;
+  int tfsf_post;               // TF/SF corrections applied by the post-pass kernel (sweep3d only)
   int fp16;
   int x_chunk;                 // x planes per CTA
   int shape;                   // tile / occupancy variant (see launch_fused3d)

@@ -1,0 +1,1074 @@
+// sweep3d.cu - TMA-pipelined one-sweep E+H leapfrog step (3-D, FP32 and
+// FP16-storage forms).
+//
+// Same arithmetic and double-buffered data flow as fused3d.cu (every value
+// is read from the old buffers and written to the new ones once per step),
+// reorganised for the B200 memory system:
+//
+//  * A CTA owns a tile of 128 z cells x (WY - 1) y rows and marches x over a
+//    chunk of planes.  Lane l of warp w handles the four cells
+//    z0 + 4l .. z0 + 4l + 3 of row y0 + w, so every global access is a
+//    16-byte vector per lane.  Warp WY - 1 is the y ring: it recomputes E on
+//    the row after the tile (needed by H of the last owned row) and stores
+//    nothing; lane 31 recomputes E on the z ring cell z0 + 128.
+//  * Per plane x, one elected thread streams H(x) (with the y - 1 row and a
+//    16-byte z halo on both sides), E_old(x), eps(x), eps(x + 1) and, on
+//    planes that hold PML cells, the PML auxiliaries into shared memory with
+//    cp.async.bulk.tensor, three stages deep, completion signalled on an
+//    mbarrier (bounded waits).  Neighbour values then come from shared
+//    memory, so the compute is plain vector arithmetic with no global-memory
+//    latency on its critical path.
+//  * E_new(x) goes to global memory and to a three-deep shared exchange
+//    buffer; H_new(x - 1) reads E_new(x - 1) (with its y + 1 / z + 1
+//    neighbours) from there and E_new(x) from registers.  One __syncthreads
+//    per plane orders everything.
+//  * CTAs are persistent and take (z tile, y tile, x chunk) items from an
+//    atomic counter, so tiles with PML or TF/SF work balance out.
+// PML auxiliaries, TF/SF corrections and the point source are applied only
+// on the lanes whose cells need them.
+#include <cuda.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <mutex>
+#include <vector>
+
+#include "incident_dev.cuh"
+#include "sweep3d.h"
+
+namespace fdtdb {
+
+namespace {
+
+constexpr int TZ = 128;           // z cells per tile: 32 lanes x 4
+constexpr int PW = TZ + 4;        // eps / auxiliary / exchange row width in floats (z0 .. z0 + 131)
+constexpr int NST = 3;            // pipeline stages
+
+template <typename T, int WY>
+struct Smem
+{
+  static constexpr int HZ = 16 / (int) sizeof (T);   // z halo: one 16-byte unit
+  static constexpr int HW = TZ + 2 * HZ;             // H row: z0 - HZ .. z0 + TZ + HZ - 1
+  static constexpr int EW = TZ + HZ;                 // E row: z0 .. z0 + TZ + HZ - 1
+  static constexpr unsigned rnd (unsigned b) { return (b + 127u) / 128u * 128u; }
+  static constexpr unsigned H_B = rnd (sizeof (T) * HW * (WY + 1));
+  static constexpr unsigned E_B = rnd (sizeof (T) * EW * WY);
+  static constexpr unsigned P_B = rnd (sizeof (float) * PW * WY);   // one eps or auxiliary plane
+  // stage: H x3, E x3, eps(x), eps(x + 1), auxiliaries of Ex..Ez at x and Hx..Hz at x - 1
+  static constexpr unsigned OFF_E = 3 * H_B;
+  static constexpr unsigned OFF_P = OFF_E + 3 * E_B;
+  static constexpr unsigned OFF_A = OFF_P + 2 * P_B;
+  static constexpr unsigned STAGE = OFF_A + 6 * P_B;
+  static constexpr unsigned OFF_N = NST * STAGE;     // exchange: [3 buffers][Ex, Ey, Ez]
+  static constexpr unsigned OFF_BAR = OFF_N + 9 * P_B;
+  static constexpr unsigned TOTAL = OFF_BAR + 128 + 128;   // + room to align the base to 128 bytes
+  // bytes each group of copies delivers (full boxes, halo and fill included)
+  static constexpr unsigned TX_HE = 3u * sizeof (T) * HW * (WY + 1) + 3u * sizeof (T) * EW * WY;
+  static constexpr unsigned TX_P = 2u * sizeof (float) * PW * WY;
+  static constexpr unsigned TX_A = 6u * sizeof (float) * PW * WY;
+};
+
+// ---------------------------------------------------------------- PTX helpers
+
+__device__ __forceinline__ uint32_t smem_addr (const void *p)
+{
+  return (uint32_t) __cvta_generic_to_shared (p);
+}
+
+__device__ __forceinline__ void mbar_init (uint32_t bar, unsigned count)
+{
+  asm volatile ("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx (uint32_t bar, unsigned bytes)
+{
+  asm volatile ("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait (uint32_t bar, unsigned parity)
+{
+  unsigned ok;
+  asm volatile (
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns ()
+{
+  unsigned long long t;
+  asm volatile ("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Wait for the phase with the given parity; false after about one second.
+__device__ __noinline__ bool mbar_wait (uint32_t bar, unsigned parity)
+{
+  if (mbar_try_wait (bar, parity))
+    return true;
+  const unsigned long long t0 = global_ns ();
+  while (!mbar_try_wait (bar, parity))
+    if (global_ns () - t0 > 1000000000ull)
+      return false;
+  return true;
+}
+
+__device__ __forceinline__ void tma_load_3d (uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                             uint32_t bar)
+{
+  asm volatile (
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+      : "memory");
+}
+
+// ------------------------------------------------------- element conversions
+
+template <typename T>
+struct Vec;
+
+template <>
+struct Vec<float>
+{
+  static __device__ __forceinline__ void ld4 (const float *s, float v[4])
+  {
+    const float4 t = *reinterpret_cast<const float4 *> (s);
+    v[0] = t.x;
+    v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+  }
+  static __device__ __forceinline__ float ld1 (const float *s) { return *s; }
+  static __device__ __forceinline__ void st4 (float *g, const float v[4])
+  {
+    *reinterpret_cast<float4 *> (g) = make_float4 (v[0], v[1], v[2], v[3]);
+  }
+};
+
+template <>
+struct Vec<__half>
+{
+  static __device__ __forceinline__ void ld4 (const __half *s, float v[4])
+  {
+    const uint2 t = *reinterpret_cast<const uint2 *> (s);
+    const float2 a = __half22float2 (*reinterpret_cast<const __half2 *> (&t.x));
+    const float2 b = __half22float2 (*reinterpret_cast<const __half2 *> (&t.y));
+    v[0] = a.x;
+    v[1] = a.y;
+    v[2] = b.x;
+    v[3] = b.y;
+  }
+  static __device__ __forceinline__ float ld1 (const __half *s) { return __half2float (*s); }
+  static __device__ __forceinline__ void st4 (__half *g, const float v[4])
+  {
+    __half2 a = __floats2half2_rn (v[0], v[1]);
+    __half2 b = __floats2half2_rn (v[2], v[3]);
+    uint2 t;
+    t.x = *reinterpret_cast<unsigned *> (&a);
+    t.y = *reinterpret_cast<unsigned *> (&b);
+    *reinterpret_cast<uint2 *> (g) = t;
+  }
+};
+
+__device__ __forceinline__ void lds4f (const float *s, float v[4])
+{
+  Vec<float>::ld4 (s, v);
+}
+
+__device__ __forceinline__ void sts4f (float *s, const float v[4])
+{
+  *reinterpret_cast<float4 *> (s) = make_float4 (v[0], v[1], v[2], v[3]);
+}
+
+// ------------------------------------------------------------ cell physics
+
+__device__ __forceinline__ bool on_face (const int *planes, int v)
+{
+  return v == planes[0] || v == planes[1] || v == planes[2] || v == planes[3];
+}
+
+// TF/SF change of the curl of component k at (x, y, z).  Each matching term
+// subtracts the incident value from one neighbour of the curl
+// (n1 - n0) - (n3 - n2): slots 0 and 3 raise the curl by that value, slots
+// 1 and 2 lower it (InternalScheme.inc.h:1386-1835).
+__device__ __forceinline__ float tfsf_curl (const FusedParams &p, int k, const double *inc, int *err, int x, int y,
+                                            int z)
+{
+  const CompDev &c = p.comp[k];
+  float d = 0.f;
+  for (int t = 0; t < c.nterms; ++t)
+  {
+    const TermDev &tm = c.term[t];
+    if (x >= tm.lo[0] && x < tm.hi[0] && y >= tm.lo[1] && y < tm.hi[1] && z >= tm.lo[2] && z < tm.hi[2])
+    {
+      const double diff =
+          inc_at (p.g, inc, p.inc_len, err, tm.inc_comp, x + tm.aux[0], y + tm.aux[1], z + tm.aux[2]);
+      const float dv = (float) (diff * tm.negate) * p.inc_scale[tm.inc_comp];
+      d += (tm.slot == 0 || tm.slot == 3) ? dv : -dv;
+    }
+  }
+  return d;
+}
+
+// PML update of component K at one cell: curl step of the auxiliary X with
+// the 1-D coefficient tables (ca1/sq1 along axis K+1, p5/q5 along K+2, g4
+// along K, the reference's sigma choice per component), then the field from
+// the change of X.  Returns the field; *xn receives the new auxiliary.
+template <int K>
+__device__ __forceinline__ float pml_cell (const FusedParams &p, int x, int y, int z, float xo, float cu, float im,
+                                           float fo, float *xn)
+{
+  constexpr int A = K % 3, C1 = (K + 1) % 3, C2 = (K + 2) % 3;
+  const int i1 = C1 == 0 ? x : (C1 == 1 ? y : z);
+  const int i2 = C2 == 0 ? x : (C2 == 1 ? y : z);
+  const int ia = A == 0 ? x : (A == 1 ? y : z);
+  const float ca1 = __ldg (p.tab[K][0] + i1);
+  const float sq1 = __ldg (p.tab[K][1] + i1);
+  const float p5 = __ldg (p.tab[K][2] + i2);
+  const float q5 = __ldg (p.tab[K][3] + i2);
+  const float g4p = __ldg (p.tab[K][4] + ia);
+  const float g4m = __ldg (p.tab[K][5] + ia);
+  const float n = ca1 * xo + sq1 * cu;
+  *xn = n;
+  return p5 * fo + (g4p * n - g4m * xo) * q5 * im;
+}
+
+// PML update of component K on the cells of mask pm among a lane's four
+// cells (z = zc .. zc + 3); other cells keep fn and their auxiliary value.
+template <int K>
+__device__ __forceinline__ void pml_lane (const FusedParams &p, unsigned pm, int x, int y, int zc, const float xo[4],
+                                          const float cu[4], const float im[4], const float fo[4], float fn[4],
+                                          float xn[4])
+{
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+  {
+    xn[j] = xo[j];
+    if ((pm >> j) & 1u)
+      fn[j] = pml_cell<K> (p, x, y, zc + j, xo[j], cu[j], im[j], fo[j], &xn[j]);
+  }
+}
+
+// ------------------------------------------------------------------ kernel
+
+template <typename T, int WY>
+__global__ void __launch_bounds__ (32 * WY, 1)
+    sweep3d_kernel (const __grid_constant__ SweepMaps maps, const __grid_constant__ FusedParams p,
+                    const SweepWork wk, int *err)
+{
+  using L = Smem<T, WY>;
+  constexpr int HZ = L::HZ, HW = L::HW, EW = L::EW;
+  constexpr int HS = L::H_B / sizeof (T), ES = L::E_B / sizeof (T), PS = L::P_B / sizeof (float);
+  extern __shared__ __align__ (128) unsigned char smem_raw[];
+  __shared__ int s_item;
+  __shared__ int s_abort[2];   // per plane parity: a copy did not arrive in time
+
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const bool leader = w == 0 && lane == 0;
+  const int nx = p.g.n[0], ny = p.g.n[1], nz = p.g.n[2];
+  const size_t sx = (size_t) ny * nz;
+  // 128-byte aligned base of the dynamic shared memory (TMA destinations)
+  const uint32_t raw = smem_addr (smem_raw);
+  const uint32_t sbase = (raw + 127u) & ~127u;
+  unsigned char *const smem = smem_raw + (sbase - raw);
+  const uint32_t bar = sbase + L::OFF_BAR;
+  const bool has_eps = p.eps != nullptr;
+  const float S = p.courant;
+  const float one4[4] = {1.f, 1.f, 1.f, 1.f};
+  const bool tfsf_in = p.use_tfsf && !p.tfsf_post;   // corrections inside the sweep
+
+  if (leader)
+  {
+#pragma unroll
+    for (int st = 0; st < NST; ++st)
+      mbar_init (bar + 8 * st, 1);
+    asm volatile ("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_abort[0] = s_abort[1] = 0;
+  }
+  __syncthreads ();
+
+  // Does plane x of the tile at (z0, y0) hold a PML cell of Ex..Ez (at x)
+  // or of Hx..Hz (at x - 1)?  Then its stage also carries the auxiliaries.
+  auto need_aux = [&] (int x, int z0, int y0) -> bool {
+    if (!p.use_pml)
+      return false;
+    const int yhi = min (y0 + WY - 1, ny - 2);
+    const int zlo = max (z0, 1), zhi = min (z0 + TZ, nz - 2);
+    bool in = true;
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+    {
+      const int xx = k < 3 ? x : x - 1;
+      in = in && xx >= p.ilo[k][0] && xx < p.ihi[k][0] && y0 >= p.ilo[k][1] && yhi < p.ihi[k][1] &&
+           zlo >= p.ilo[k][2] && zhi < p.ihi[k][2];
+    }
+    return !in;
+  };
+
+  // stage `st` <- plane x of the tile at (z0, y0)
+  auto issue = [&] (unsigned st, int x, int z0, int y0) {
+    const uint32_t s = sbase + st * L::STAGE;
+    const uint32_t b = bar + 8 * st;
+    const bool na = need_aux (x, z0, y0);
+    mbar_expect_tx (b, L::TX_HE + (has_eps ? L::TX_P : 0u) + (na ? L::TX_A : 0u));
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      tma_load_3d (s + c * L::H_B, &maps.h[c], z0 - HZ, y0 - 1, x, b);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      tma_load_3d (s + L::OFF_E + c * L::E_B, &maps.e[c], z0, y0, x, b);
+    if (has_eps)
+    {
+      tma_load_3d (s + L::OFF_P, &maps.eps, z0, y0, x, b);
+      tma_load_3d (s + L::OFF_P + L::P_B, &maps.eps, z0, y0, min (x + 1, nx - 1), b);
+    }
+    if (na)
+    {
+#pragma unroll
+      for (int c = 0; c < 6; ++c)
+        tma_load_3d (s + L::OFF_A + c * L::P_B, &maps.aux[c], z0, y0, c < 3 ? x : max (x - 1, 0), b);
+    }
+  };
+
+  unsigned phase = 0;   // bit s: parity of the next completion of stage s
+  unsigned gst = 0;     // stage of the next plane to stream
+  bool aborted = false;
+  for (;;)
+  {
+    if (leader)
+      s_item = (int) atomicAdd (wk.ctr, 1ull);
+    __syncthreads ();
+    const int item = s_item;
+    if (item >= wk.nitems)
+      break;
+    const int zt = item % wk.nzt;
+    const int yt = (item / wk.nzt) % wk.nyt;
+    const int ch = item / (wk.nzt * wk.nyt);
+    const int z0 = zt * TZ;
+    const int y0 = 1 + yt * (WY - 1);
+    const int xa = 1 + ch * wk.chunk;
+    const int xb = min (xa + wk.chunk - 1, nx - 2);
+    const int np = xb - xa + 3;   // planes xa - 1 .. xb + 1 (at least 3)
+    if (leader)
+    {
+#pragma unroll
+      for (int k = 0; k < NST; ++k)
+        issue ((gst + k) % NST, xa - 1 + k, z0, y0);
+    }
+
+    // ---- per-lane / per-row constants of this item
+    const int zl = 4 * lane;
+    const int zc = z0 + zl;
+    const bool lane_ok = zc < nz;
+    const int y = y0 + w;
+    const bool yupd = y <= ny - 2;
+    const bool own_row = w < WY - 1 && yupd;
+    const size_t rowoff = (size_t) y * nz + zc;
+    unsigned zupd = 0, zface = 0, zin = 0, yin = 0;   // zin bit 4k + j, yin bit k
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+    {
+      const int z = zc + j;
+      if (z >= 1 && z <= nz - 2)
+        zupd |= 1u << j;
+      if (tfsf_in && on_face (p.face[2], z))
+        zface |= 1u << j;
+#pragma unroll
+      for (int k = 0; k < 6; ++k)
+        if (z >= p.ilo[k][2] && z < p.ihi[k][2])
+          zin |= 1u << (4 * k + j);
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+      if (y >= p.ilo[k][1] && y < p.ihi[k][1])
+        yin |= 1u << k;
+    const bool yface = tfsf_in && on_face (p.face[1], y);
+    const int zr = z0 + TZ;   // z ring cell (lane 31)
+    const bool ring_lane = lane == 31 && w < WY - 1;
+
+    float hp[3][4];           // H_old(x - 1) on the lane's cells
+    float hpr = 0.f;          // lane 31: Hz_old(x - 1) on the z ring cell
+    float en[3][4];           // E_new(x)
+    unsigned nbuf = 0;        // exchange buffer of this plane (plane index mod 3)
+    unsigned st = gst;
+    for (int i = 0; i < np; ++i)
+    {
+      const int x = xa - 1 + i;
+      if (!mbar_wait (bar + 8 * st, (phase >> st) & 1u))
+      {
+        s_abort[i & 1] = 1;
+        atomicOr (err, 4);
+      }
+      phase ^= 1u << st;
+      const bool na = need_aux (x, z0, y0);
+      const unsigned char *stg = smem + st * L::STAGE;
+      const T *sH = reinterpret_cast<const T *> (stg);
+      const T *sE = reinterpret_cast<const T *> (stg + L::OFF_E);
+      const float *P0 = reinterpret_cast<const float *> (stg + L::OFF_P);
+      const float *P1 = P0 + PS;
+      const float *A = reinterpret_cast<const float *> (stg + L::OFF_A);
+      float *N = reinterpret_cast<float *> (smem + L::OFF_N + nbuf * 3 * L::P_B);
+
+      float hc[3][4];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        Vec<T>::ld4 (sH + c * HS + (w + 1) * HW + HZ + zl, hc[c]);
+      const float hzr = Vec<T>::ld1 (sH + 2 * HS + (w + 1) * HW + HZ + TZ);
+      // auxiliaries of H(x - 1) for the H step (the stage is refilled after the barrier)
+      float ha[3][4];
+      const bool hpml = i > 1 && own_row && na;
+      if (hpml)
+      {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          lds4f (A + (3 + c) * PS + w * PW + zl, ha[c]);
+      }
+
+      if (i > 0)
+      {
+        // ================= E_new(x) on every row of the CTA (ring row included)
+        const bool rowupd = x <= nx - 2 && yupd;
+        const unsigned upd = rowupd ? zupd : 0u;
+        float hzm[4], hxym[4], eo[3][4];
+        Vec<T>::ld4 (sH + 2 * HS + w * HW + HZ + zl, hzm);
+        Vec<T>::ld4 (sH + 0 * HS + w * HW + HZ + zl, hxym);
+        const float hym1 = Vec<T>::ld1 (sH + 1 * HS + (w + 1) * HW + HZ + zl - 1);
+        const float hxm1 = Vec<T>::ld1 (sH + 0 * HS + (w + 1) * HW + HZ + zl - 1);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          Vec<T>::ld4 (sE + c * ES + w * EW + zl, eo[c]);
+        float ix[4], iy[4], iz[4];
+        if (has_eps)
+        {
+          float e0[4], ex1[4], ey1[4];
+          lds4f (P0 + w * PW + zl, e0);
+          lds4f (P1 + w * PW + zl, ex1);
+          lds4f (P0 + min (w + 1, WY - 1) * PW + zl, ey1);
+          const float ez1 = P0[w * PW + zl + 4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+          {
+            ix[j] = __fdividef (2.f, e0[j] + ex1[j]);
+            iy[j] = __fdividef (2.f, e0[j] + ey1[j]);
+            iz[j] = __fdividef (2.f, e0[j] + (j < 3 ? e0[j + 1] : ez1));
+          }
+        }
+        else
+        {
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            ix[j] = iy[j] = iz[j] = 1.f;
+        }
+        float cx[4], cy[4], cz[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+          const float hyl = j ? hc[1][j - 1] : hym1;
+          const float hxl = j ? hc[0][j - 1] : hxm1;
+          cx[j] = (hc[2][j] - hzm[j]) - (hc[1][j] - hyl);
+          cy[j] = (hc[0][j] - hxl) - (hc[2][j] - hp[2][j]);
+          cz[j] = (hc[1][j] - hp[1][j]) - (hc[0][j] - hxym[j]);
+        }
+        const size_t id = (size_t) x * sx + rowoff;
+        const bool xface = tfsf_in && on_face (p.face[0], x);
+        const unsigned fm = (xface || yface) ? upd : (zface & upd);
+        if (fm)
+        {
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if ((fm >> j) & 1u)
+            {
+              cx[j] += tfsf_curl (p, 0, p.inc_h, err, x, y, zc + j);
+              cy[j] += tfsf_curl (p, 1, p.inc_h, err, x, y, zc + j);
+              cz[j] += tfsf_curl (p, 2, p.inc_h, err, x, y, zc + j);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+          const bool u = (upd >> j) & 1u;
+          en[0][j] = u ? eo[0][j] + (S * ix[j]) * cx[j] : eo[0][j];
+          en[1][j] = u ? eo[1][j] + (S * iy[j]) * cy[j] : eo[1][j];
+          en[2][j] = u ? eo[2][j] + (S * iz[j]) * cz[j] : eo[2][j];
+        }
+        const bool store_e = own_row && x <= xb && lane_ok;
+        if (na && upd)
+        {
+          const unsigned pm0 = upd & ~((x >= p.ilo[0][0] && x < p.ihi[0][0] && (yin & 1u)) ? zin : 0u);
+          const unsigned pm1 = upd & ~(((x >= p.ilo[1][0] && x < p.ihi[1][0] && (yin & 2u)) ? zin : 0u) >> 4);
+          const unsigned pm2 = upd & ~(((x >= p.ilo[2][0] && x < p.ihi[2][0] && (yin & 4u)) ? zin : 0u) >> 8);
+          if (pm0 & 15u)
+          {
+            float xo[4], xn[4];
+            lds4f (A + 0 * PS + w * PW + zl, xo);
+            pml_lane<0> (p, pm0 & 15u, x, y, zc, xo, cx, ix, eo[0], en[0], xn);
+            if (store_e)
+              Vec<float>::st4 (p.aux_new[0] + id, xn);
+          }
+          if (pm1 & 15u)
+          {
+            float xo[4], xn[4];
+            lds4f (A + 1 * PS + w * PW + zl, xo);
+            pml_lane<1> (p, pm1 & 15u, x, y, zc, xo, cy, iy, eo[1], en[1], xn);
+            if (store_e)
+              Vec<float>::st4 (p.aux_new[1] + id, xn);
+          }
+          if (pm2 & 15u)
+          {
+            float xo[4], xn[4];
+            lds4f (A + 2 * PS + w * PW + zl, xo);
+            pml_lane<2> (p, pm2 & 15u, x, y, zc, xo, cz, iz, eo[2], en[2], xn);
+            if (store_e)
+              Vec<float>::st4 (p.aux_new[2] + id, xn);
+          }
+        }
+        if ((p.ps_mask & 7) && rowupd && x == p.ps[0] && y == p.ps[1] && p.ps[2] >= zc && p.ps[2] < zc + 4)
+        {
+          const float v = (float) p.src[p.src_index];
+          const int j = p.ps[2] - zc;
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            if (p.ps_mask & (1 << c))
+            {
+#pragma unroll
+              for (int jj = 0; jj < 4; ++jj)
+                if (jj == j)
+                  en[c][jj] = v;
+            }
+        }
+        if (store_e)
+        {
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            Vec<T>::st4 (reinterpret_cast<T *> (p.e_new[c]) + id, en[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          sts4f (N + c * PS + w * PW + zl, en[c]);
+
+        // z ring: Ex and Ey at z0 + 128 for H of the lane's last cell
+        if (ring_lane)
+        {
+          float rx = 0.f, ry = 0.f;
+          if (zr <= nz - 1)
+          {
+            rx = Vec<T>::ld1 (sE + 0 * ES + w * EW + TZ);
+            ry = Vec<T>::ld1 (sE + 1 * ES + w * EW + TZ);
+            if (rowupd && zr <= nz - 2)
+            {
+              const float hz = hzr;
+              const float hzym = Vec<T>::ld1 (sH + 2 * HS + w * HW + HZ + TZ);
+              const float hy = Vec<T>::ld1 (sH + 1 * HS + (w + 1) * HW + HZ + TZ);
+              const float hx = Vec<T>::ld1 (sH + 0 * HS + (w + 1) * HW + HZ + TZ);
+              float crx = (hz - hzym) - (hy - hc[1][3]);
+              float cry = (hx - hc[0][3]) - (hz - hpr);
+              float irx = 1.f, iry = 1.f;
+              if (has_eps)
+              {
+                const float e0 = P0[w * PW + TZ];
+                irx = __fdividef (2.f, e0 + P1[w * PW + TZ]);
+                iry = __fdividef (2.f, e0 + P0[(w + 1) * PW + TZ]);
+              }
+              if (tfsf_in && (xface || yface || on_face (p.face[2], zr)))
+              {
+                crx += tfsf_curl (p, 0, p.inc_h, err, x, y, zr);
+                cry += tfsf_curl (p, 1, p.inc_h, err, x, y, zr);
+              }
+              const bool in0 = x >= p.ilo[0][0] && x < p.ihi[0][0] && (yin & 1u) && zr >= p.ilo[0][2] &&
+                               zr < p.ihi[0][2];
+              const bool in1 = x >= p.ilo[1][0] && x < p.ihi[1][0] && (yin & 2u) && zr >= p.ilo[1][2] &&
+                               zr < p.ihi[1][2];
+              float dummy;
+              if (p.use_pml && !in0)
+                rx = pml_cell<0> (p, x, y, zr, A[0 * PS + w * PW + TZ], crx, irx, rx, &dummy);
+              else
+                rx = rx + (S * irx) * crx;
+              if (p.use_pml && !in1)
+                ry = pml_cell<1> (p, x, y, zr, A[1 * PS + w * PW + TZ], cry, iry, ry, &dummy);
+              else
+                ry = ry + (S * iry) * cry;
+              if ((p.ps_mask & 3) && x == p.ps[0] && y == p.ps[1] && zr == p.ps[2])
+              {
+                const float v = (float) p.src[p.src_index];
+                if (p.ps_mask & 1)
+                  rx = v;
+                if (p.ps_mask & 2)
+                  ry = v;
+              }
+            }
+          }
+          N[0 * PS + w * PW + TZ] = rx;
+          N[1 * PS + w * PW + TZ] = ry;
+        }
+      }
+
+      __syncthreads ();
+      if (s_abort[i & 1])
+      {
+        // wait (bounded) for the copies still in flight into the other stages
+        aborted = true;
+        if (leader)
+          for (int k = 1; k < NST && i + k < np; ++k)
+          {
+            const unsigned so = (st + k) % NST;
+            mbar_wait (bar + 8 * so, (phase >> so) & 1u);
+          }
+        break;
+      }
+      if (leader && i + NST < np)
+        issue (st, x + NST, z0, y0);
+
+      if (i > 1 && own_row)
+      {
+        // ================= H_new(x - 1) on the owned rows
+        const int xh = x - 1;
+        const float *Np =
+            reinterpret_cast<const float *> (smem + L::OFF_N + (nbuf == 0 ? 2u : nbuf - 1u) * 3 * L::P_B);
+        float ex[4], ey[4], ez[4], exy[4], ezy[4];
+        lds4f (Np + 0 * PS + w * PW + zl, ex);
+        lds4f (Np + 1 * PS + w * PW + zl, ey);
+        lds4f (Np + 2 * PS + w * PW + zl, ez);
+        lds4f (Np + 0 * PS + (w + 1) * PW + zl, exy);
+        lds4f (Np + 2 * PS + (w + 1) * PW + zl, ezy);
+        const float exz = Np[0 * PS + w * PW + zl + 4];
+        const float eyz = Np[1 * PS + w * PW + zl + 4];
+        float ax[4], ay[4], az[4], hn[3][4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+          const float eyn = j < 3 ? ey[j + 1] : eyz;
+          const float exn = j < 3 ? ex[j + 1] : exz;
+          ax[j] = (eyn - ey[j]) - (ezy[j] - ez[j]);
+          ay[j] = (en[2][j] - ez[j]) - (exn - ex[j]);
+          az[j] = (exy[j] - ex[j]) - (en[1][j] - ey[j]);
+        }
+        const size_t idh = (size_t) xh * sx + rowoff;
+        const bool xface = tfsf_in && on_face (p.face[0], xh);
+        const unsigned fm = (xface || yface) ? zupd : (zface & zupd);
+        if (fm)
+        {
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if ((fm >> j) & 1u)
+            {
+              ax[j] += tfsf_curl (p, 3, p.inc_e, err, xh, y, zc + j);
+              ay[j] += tfsf_curl (p, 4, p.inc_e, err, xh, y, zc + j);
+              az[j] += tfsf_curl (p, 5, p.inc_e, err, xh, y, zc + j);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+          const bool u = (zupd >> j) & 1u;
+          hn[0][j] = u ? hp[0][j] + S * ax[j] : hp[0][j];
+          hn[1][j] = u ? hp[1][j] + S * ay[j] : hp[1][j];
+          hn[2][j] = u ? hp[2][j] + S * az[j] : hp[2][j];
+        }
+        if (hpml && zupd)
+        {
+          const unsigned pm3 = zupd & ~(((xh >= p.ilo[3][0] && xh < p.ihi[3][0] && (yin & 8u)) ? zin : 0u) >> 12);
+          const unsigned pm4 = zupd & ~(((xh >= p.ilo[4][0] && xh < p.ihi[4][0] && (yin & 16u)) ? zin : 0u) >> 16);
+          const unsigned pm5 = zupd & ~(((xh >= p.ilo[5][0] && xh < p.ihi[5][0] && (yin & 32u)) ? zin : 0u) >> 20);
+          if (pm3 & 15u)
+          {
+            float xn[4];
+            pml_lane<3> (p, pm3 & 15u, xh, y, zc, ha[0], ax, one4, hp[0], hn[0], xn);
+            if (lane_ok)
+              Vec<float>::st4 (p.aux_new[3] + idh, xn);
+          }
+          if (pm4 & 15u)
+          {
+            float xn[4];
+            pml_lane<4> (p, pm4 & 15u, xh, y, zc, ha[1], ay, one4, hp[1], hn[1], xn);
+            if (lane_ok)
+              Vec<float>::st4 (p.aux_new[4] + idh, xn);
+          }
+          if (pm5 & 15u)
+          {
+            float xn[4];
+            pml_lane<5> (p, pm5 & 15u, xh, y, zc, ha[2], az, one4, hp[2], hn[2], xn);
+            if (lane_ok)
+              Vec<float>::st4 (p.aux_new[5] + idh, xn);
+          }
+        }
+        if ((p.ps_mask & 56) && xh == p.ps[0] && y == p.ps[1] && p.ps[2] >= zc && p.ps[2] < zc + 4)
+        {
+          const float v = (float) p.src[p.src_index + 1] * p.ps_scale_h;
+          const int j = p.ps[2] - zc;
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            if (p.ps_mask & (8 << c))
+            {
+#pragma unroll
+              for (int jj = 0; jj < 4; ++jj)
+                if (jj == j)
+                  hn[c][jj] = v;
+            }
+        }
+        if (lane_ok)
+        {
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            Vec<T>::st4 (reinterpret_cast<T *> (p.h_new[c]) + idh, hn[c]);
+        }
+      }
+
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          hp[c][j] = hc[c][j];
+      hpr = hzr;
+      nbuf = nbuf == 2u ? 0u : nbuf + 1u;
+      st = st == NST - 1 ? 0u : st + 1u;
+    }
+    gst = (gst + (unsigned) np) % NST;
+    if (aborted)
+      break;
+  }
+
+  if (leader)
+  {
+    __threadfence ();
+    const unsigned long long done = atomicAdd (wk.ctr + 1, 1ull);
+    if (done == gridDim.x - 1)
+    {
+      atomicExch (wk.ctr, 0ull);
+      atomicExch (wk.ctr + 1, 0ull);
+    }
+  }
+}
+
+// ------------------------------------------------------ TF/SF post pass
+
+// The sweep ran without TF/SF, so on the band around the faces its E_new
+// lacks (S im) dE for every corrected E cell and its H_new lacks
+// S (curl of that dE + the H-side correction).  Both are linear in the
+// correction, so adding them afterwards gives the corrected step (PML-free
+// cells only, which the host guarantees).  One thread per band cell
+// touches only its own cell; the E corrections of neighbours are recomputed,
+// never read, so there are no races.
+template <typename T>
+__global__ void __launch_bounds__ (256) tfsf_post_kernel (const __grid_constant__ FusedParams p, const int *boxes,
+                                                          const long long *offset, int nbox, long long cells, int *err)
+{
+  const int nx = p.g.n[0], ny = p.g.n[1], nz = p.g.n[2];
+  const size_t sx = (size_t) ny * nz;
+  const float S = p.courant;
+  // correction of E component k at (cx, cy, cz): zero off the updated interior and on the source
+  auto de = [&] (int k, int cx, int cy, int cz) -> float {
+    if (cx < 1 || cx > nx - 2 || cy < 1 || cy > ny - 2 || cz < 1 || cz > nz - 2)
+      return 0.f;
+    if (((p.ps_mask >> k) & 1) && cx == p.ps[0] && cy == p.ps[1] && cz == p.ps[2])
+      return 0.f;
+    const float d = tfsf_curl (p, k, p.inc_h, err, cx, cy, cz);
+    if (d == 0.f)
+      return 0.f;
+    float im = 1.f;
+    if (p.eps)
+    {
+      const size_t c = (size_t) cx * sx + (size_t) cy * nz + cz;
+      const size_t st = k == 0 ? sx : (k == 1 ? (size_t) nz : 1);
+      im = __fdividef (2.f, p.eps[c] + p.eps[c + st]);
+    }
+    return (S * im) * d;
+  };
+  for (long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x; t < cells;
+       t += (long long) gridDim.x * blockDim.x)
+  {
+    int lo = 0, hi = nbox;
+    while (hi - lo > 1)
+    {
+      const int mid = (lo + hi) >> 1;
+      if (offset[mid] <= t)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const int *b = boxes + 6 * lo;
+    long long r = t - offset[lo];
+    const int ez = b[5] - b[2], ey = b[4] - b[1];
+    const int z = b[2] + (int) (r % ez);
+    r /= ez;
+    const int y = b[1] + (int) (r % ey);
+    r /= ey;
+    const int x = b[0] + (int) r;
+    const size_t id = (size_t) x * sx + (size_t) y * nz + z;
+    const float d0 = de (0, x, y, z), d1 = de (1, x, y, z), d2 = de (2, x, y, z);
+    const float dd[3] = {d0, d1, d2};
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      if (dd[k] != 0.f)
+      {
+        T *f = reinterpret_cast<T *> (p.e_new[k]) + id;
+        *f = (T) ((float) *f + dd[k]);
+      }
+    const float a[3] = {
+        (de (1, x, y, z + 1) - d1) - (de (2, x, y + 1, z) - d2) + tfsf_curl (p, 3, p.inc_e, err, x, y, z),
+        (de (2, x + 1, y, z) - d2) - (de (0, x, y, z + 1) - d0) + tfsf_curl (p, 4, p.inc_e, err, x, y, z),
+        (de (0, x, y + 1, z) - d0) - (de (1, x + 1, y, z) - d1) + tfsf_curl (p, 5, p.inc_e, err, x, y, z)};
+    const bool at_src = x == p.ps[0] && y == p.ps[1] && z == p.ps[2];
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+      if (a[m] != 0.f && !(at_src && ((p.ps_mask >> (3 + m)) & 1)))
+      {
+        T *f = reinterpret_cast<T *> (p.h_new[m]) + id;
+        *f = (T) ((float) *f + S * a[m]);
+      }
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host side
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn ()
+{
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once (once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint ("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000> (f);
+  });
+  return fn;
+}
+
+// 3-D map over an (nx, ny, nz) array, z fastest, box bw x bh x 1
+bool make_map (CUtensorMap &m, const void *base, bool half, const int n[3], int bw, int bh)
+{
+  auto fn = encode_fn ();
+  if (!fn)
+    return false;
+  const cuuint64_t es = half ? 2 : 4;
+  cuuint64_t dims[3] = {(cuuint64_t) n[2], (cuuint64_t) n[1], (cuuint64_t) n[0]};
+  cuuint64_t strides[2] = {(cuuint64_t) n[2] * es, (cuuint64_t) n[2] * (cuuint64_t) n[1] * es};
+  cuuint32_t box[3] = {(cuuint32_t) bw, (cuuint32_t) bh, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn (&m, half ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                   const_cast<void *> (base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <typename T, int WY>
+std::string plan_t (SweepPlan &pl, const FusedParams &p, void *const e[2][3], void *const h[2][3],
+                    float *const aux[2][6], const float *eps, int sm_count)
+{
+  using L = Smem<T, WY>;
+  const bool half = sizeof (T) == 2;
+  for (int b = 0; b < 2; ++b)
+  {
+    SweepMaps &m = pl.maps[b];
+    for (int c = 0; c < 3; ++c)
+      if (!make_map (m.h[c], h[b][c], half, p.g.n, L::HW, WY + 1) ||
+          !make_map (m.e[c], e[b][c], half, p.g.n, L::EW, WY))
+        return "tensor map encoding failed";
+    // descriptors the kernel never uses are copies of a valid one
+    if (eps)
+    {
+      if (!make_map (m.eps, eps, false, p.g.n, PW, WY))
+        return "tensor map encoding failed";
+    }
+    else
+      m.eps = m.e[0];
+    for (int k = 0; k < 6; ++k)
+    {
+      if (p.use_pml)
+      {
+        if (!aux[b][k] || !make_map (m.aux[k], aux[b][k], false, p.g.n, PW, WY))
+          return "tensor map encoding failed";
+      }
+      else
+        m.aux[k] = m.e[0];
+    }
+  }
+  auto kern = sweep3d_kernel<T, WY>;
+  if (cudaFuncSetAttribute (kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) L::TOTAL) != cudaSuccess)
+  {
+    cudaGetLastError ();
+    return "shared memory request refused";
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor (&per_sm, kern, 32 * WY, L::TOTAL) != cudaSuccess || per_sm < 1)
+  {
+    cudaGetLastError ();
+    return "kernel does not fit on an SM";
+  }
+  pl.smem = L::TOTAL;
+  pl.ctas = sm_count * per_sm;
+  return "";
+}
+
+template <typename T, int WY>
+void launch_t (const SweepPlan &pl, int set, const FusedParams &p, int *err, cudaStream_t s)
+{
+  sweep3d_kernel<T, WY><<<pl.ctas, dim3 (32, WY), Smem<T, WY>::TOTAL, s>>> (pl.maps[set], p, pl.work, err);
+}
+
+}  // namespace
+
+void sweep3d_items (const int n[3], int wy, int chunk, SweepWork &w)
+{
+  w.nzt = (n[2] - 1 + TZ - 1) / TZ;
+  w.nyt = (n[1] - 2 + wy - 2) / (wy - 1);
+  w.chunk = chunk;
+  w.nch = (n[0] - 2 + chunk - 1) / chunk;
+  w.nitems = w.nzt * w.nyt * w.nch;
+}
+
+std::string sweep3d_plan (SweepPlan &plan, const FusedParams &p, void *const e[2][3], void *const h[2][3],
+                          float *const aux[2][6], const float *eps, int sm_count, int wy, int chunk,
+                          unsigned long long *ctr)
+{
+  const int *n = p.g.n;
+  if (p.g.tmz)
+    return "2-D grid";
+  if (p.use_meta)
+    return "metamaterials";
+  const int unit = p.fp16 ? 8 : 4;
+  if (n[2] % unit != 0)
+    return "nz is not a multiple of one 16-byte unit";
+  if (n[0] < 3 || n[1] < 3 || n[2] < 3)
+    return "grid too small";
+  if (wy != 8)
+    return "unsupported CTA height";
+  if (chunk < 1)
+    return "bad x chunk";
+  plan.wy = wy;
+  std::string why = p.fp16 ? plan_t<__half, 8> (plan, p, e, h, aux, eps, sm_count)
+                           : plan_t<float, 8> (plan, p, e, h, aux, eps, sm_count);
+  if (!why.empty ())
+    return why;
+  sweep3d_items (n, wy, chunk, plan.work);
+  plan.work.ctr = ctr;
+  if (plan.ctas > plan.work.nitems)
+    plan.ctas = plan.work.nitems;
+  return "";
+}
+
+int launch_sweep3d (const SweepPlan &plan, int set, const FusedParams &p, int *err, cudaStream_t s)
+{
+  if (p.fp16)
+    launch_t<__half, 8> (plan, set, p, err, s);
+  else
+    launch_t<float, 8> (plan, set, p, err, s);
+  return 1;
+}
+
+}  // namespace fdtdb
+
+// --------------------------------------------------- TF/SF post pass (host)
+
+namespace fdtdb {
+
+std::string tfsf_band_boxes (const FusedParams &p, std::vector<int> &boxes, std::vector<long long> &offset)
+{
+  struct Box
+  {
+    int lo[3], hi[3];
+  };
+  std::vector<Box> cand;
+  const int *n = p.g.n;
+  auto add = [&] (const TermDev &t, int shift_axis) {
+    Box b;
+    for (int a = 0; a < 3; ++a)
+    {
+      const int d = a == shift_axis ? 1 : 0;
+      b.lo[a] = std::max (t.lo[a] - d, 1);
+      b.hi[a] = std::min (t.hi[a] - d, n[a] - 1);
+    }
+    if (b.lo[0] < b.hi[0] && b.lo[1] < b.hi[1] && b.lo[2] < b.hi[2])
+      cand.push_back (b);
+  };
+  for (int k = 0; k < 6; ++k)
+    for (int t = 0; t < p.comp[k].nterms; ++t)
+    {
+      add (p.comp[k].term[t], -1);
+      if (k < 3)
+        for (int a = 0; a < 3; ++a)
+          add (p.comp[k].term[t], a);
+    }
+  boxes.clear ();
+  offset.assign (1, 0);
+  if (cand.empty ())
+    return "";
+  // disjoint cover: compress coordinates, mark covered elementary boxes,
+  // merge runs along z
+  std::vector<int> cut[3];
+  for (const Box &b : cand)
+    for (int a = 0; a < 3; ++a)
+    {
+      cut[a].push_back (b.lo[a]);
+      cut[a].push_back (b.hi[a]);
+    }
+  for (int a = 0; a < 3; ++a)
+  {
+    std::sort (cut[a].begin (), cut[a].end ());
+    cut[a].erase (std::unique (cut[a].begin (), cut[a].end ()), cut[a].end ());
+  }
+  const size_t mx = cut[0].size () - 1, my = cut[1].size () - 1, mz = cut[2].size () - 1;
+  for (size_t i = 0; i < mx; ++i)
+    for (size_t j = 0; j < my; ++j)
+    {
+      size_t l = 0;
+      while (l < mz)
+      {
+        auto covered = [&] (size_t ll) {
+          for (const Box &b : cand)
+            if (cut[0][i] >= b.lo[0] && cut[0][i + 1] <= b.hi[0] && cut[1][j] >= b.lo[1] && cut[1][j + 1] <= b.hi[1] &&
+                cut[2][ll] >= b.lo[2] && cut[2][ll + 1] <= b.hi[2])
+              return true;
+          return false;
+        };
+        if (!covered (l))
+        {
+          ++l;
+          continue;
+        }
+        size_t e = l + 1;
+        while (e < mz && covered (e))
+          ++e;
+        const int bx[6] = {cut[0][i], cut[1][j], cut[2][l], cut[0][i + 1], cut[1][j + 1], cut[2][e]};
+        for (int k = 0; k < 6; ++k)
+        {
+          // a band cell must not be a PML cell of any component
+          for (int a = 0; a < 3; ++a)
+            if (p.use_pml && (bx[a] < p.ilo[k][a] || bx[3 + a] > p.ihi[k][a]))
+              return "the TF/SF band reaches into the PML";
+        }
+        boxes.insert (boxes.end (), bx, bx + 6);
+        offset.push_back (offset.back () + (long long) (bx[3] - bx[0]) * (bx[4] - bx[1]) * (bx[5] - bx[2]));
+        l = e;
+      }
+    }
+  return "";
+}
+
+int launch_tfsf_post (const TfsfBand &band, const FusedParams &p, int *err, cudaStream_t s)
+{
+  if (band.cells <= 0)
+    return 0;
+  long long blocks = (band.cells + 255) / 256;
+  if (blocks > 148 * 16)
+    blocks = 148 * 16;
+  if (p.fp16)
+    tfsf_post_kernel<__half><<<(unsigned) blocks, 256, 0, s>>> (p, band.boxes, band.offset, band.nbox, band.cells, err);
+  else
+    tfsf_post_kernel<float><<<(unsigned) blocks, 256, 0, s>>> (p, band.boxes, band.offset, band.nbox, band.cells, err);
+  return 1;
+}
+
+}  // namespace fdtdb

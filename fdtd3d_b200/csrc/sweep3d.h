@@ -1,0 +1,80 @@
+// sweep3d.h - TMA-pipelined one-sweep E+H step for the 3-D FP32 and
+// FP16-storage forms (uniform mu, no metamaterials, nz a multiple of one
+// 16-byte unit).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "fused3d.h"
+
+namespace fdtdb {
+
+// Tensor-map descriptors of one "old" buffer set.  H boxes carry a one-row
+// halo in y and one 16-byte halo on both sides in z; E, eps and PML
+// auxiliary boxes start at the tile origin.
+struct SweepMaps
+{
+  CUtensorMap h[3];
+  CUtensorMap e[3];
+  CUtensorMap eps;
+  CUtensorMap aux[6];
+};
+
+struct SweepWork
+{
+  int nzt, nyt, nch, nitems, chunk;
+  unsigned long long *ctr;     // [0] next item, [1] CTAs finished; the last CTA resets both
+};
+
+struct SweepPlan
+{
+  int wy = 0;                  // warps per CTA, one y row each (last row = ring)
+  int ctas = 0;                // persistent CTAs
+  unsigned smem = 0;           // dynamic shared memory per CTA
+  SweepWork work{};
+  SweepMaps maps[2];           // maps[b]: buffer set b as the old set
+};
+
+// Tiles per axis and items for a given CTA height and x chunk.
+void sweep3d_items (const int n[3], int wy, int chunk, SweepWork &w);
+
+// Builds the tensor maps and launch shape.  e/h[b][c] are the field buffers
+// of set b, aux[b][k] the PML auxiliaries of set b (null without PML), eps
+// the FP32 permittivity (or null).  Returns "" or the reason the kernel
+// cannot serve this geometry.
+std::string sweep3d_plan (SweepPlan &plan, const FusedParams &p, void *const e[2][3], void *const h[2][3],
+                          float *const aux[2][6], const float *eps, int sm_count, int wy, int chunk,
+                          unsigned long long *ctr);
+
+// One time step with buffer set `set` as the old set.
+int launch_sweep3d (const SweepPlan &plan, int set, const FusedParams &p, int *err, cudaStream_t s);
+
+}  // namespace fdtdb
+
+namespace fdtdb {
+
+// TF/SF post pass of the sweep: the cells within one cell of a TF/SF face,
+// as disjoint boxes with running cell offsets (device arrays).
+struct TfsfBand
+{
+  int nbox = 0;
+  long long cells = 0;
+  int *boxes = nullptr;         // nbox x {lo0, lo1, lo2, hi0, hi1, hi2}
+  long long *offset = nullptr;  // nbox + 1 running cell counts
+};
+
+// Host part: the band's boxes from the TF/SF terms (E terms and their
+// -x/-y/-z neighbours, H terms), made disjoint.  Returns "" when the post
+// pass can serve the geometry (no band cell is a PML cell of any
+// component), else the reason; fills host vectors for the caller to upload.
+std::string tfsf_band_boxes (const FusedParams &p, std::vector<int> &boxes, std::vector<long long> &offset);
+
+// Adds the TF/SF corrections to the new E and H buffers after a sweep step
+// that ran with tfsf_post = 1.
+int launch_tfsf_post (const TfsfBand &band, const FusedParams &p, int *err, cudaStream_t s);
+
+}  // namespace fdtdb

@@ -164,6 +164,13 @@ int fdtd_scalars (const fdtd_ctx *ctx, double out[3]);
 /* Number of kernel launches this context issued so far. */
 int64_t fdtd_launch_count (const fdtd_ctx *ctx);
 
+/* Name of the kernel that performs this context's field update (no
+ * reference counterpart): "plain_fp64" (FP64 plain form), "sweep3d_tma"
+ * (TMA-pipelined one-sweep 3-D kernel), "fused3d_regblock" (register-blocked
+ * one-sweep 3-D kernel), "per_cell" (one launch per half-step), or
+ * "not_stepped" before the first update.  Null for a null context. */
+const char *fdtd_step_kernel (const fdtd_ctx *ctx);
+
 /* The cudaStream_t (as void *) every launch of this context goes to, so a
  * caller can order its own work or record CUDA events against it. */
 void *fdtd_stream (const fdtd_ctx *ctx);
