@@ -46,6 +46,7 @@ namespace {
 constexpr int TZ = 128;           // z cells per tile: 32 lanes x 4
 constexpr int PW = TZ + 4;        // eps / auxiliary / exchange row width in floats (z0 .. z0 + 131)
 constexpr int NST = 3;            // pipeline stages
+constexpr int MAXC = 64;          // largest x chunk when PML coefficient tables are staged
 
 template <typename T, int WY>
 struct Smem
@@ -53,22 +54,30 @@ struct Smem
   static constexpr int HZ = 16 / (int) sizeof (T);   // z halo: one 16-byte unit
   static constexpr int HW = TZ + 2 * HZ;             // H row: z0 - HZ .. z0 + TZ + HZ - 1
   static constexpr int EW = TZ + HZ;                 // E row: z0 .. z0 + TZ + HZ - 1
+  static constexpr int AN = 32;                      // narrow auxiliary box width (floats)
+  static constexpr int XW = MAXC + 2;                // x-table entries per item (planes xa - 1 .. xb + 1)
   static constexpr unsigned rnd (unsigned b) { return (b + 127u) / 128u * 128u; }
   static constexpr unsigned H_B = rnd (sizeof (T) * HW * (WY + 1));
   static constexpr unsigned E_B = rnd (sizeof (T) * EW * WY);
-  static constexpr unsigned P_B = rnd (sizeof (float) * PW * WY);   // one eps or auxiliary plane
+  static constexpr unsigned P_B = rnd (sizeof (float) * PW * WY);   // one eps / auxiliary / exchange plane
   // stage: H x3, E x3, eps(x), eps(x + 1), auxiliaries of Ex..Ez at x and Hx..Hz at x - 1
   static constexpr unsigned OFF_E = 3 * H_B;
   static constexpr unsigned OFF_P = OFF_E + 3 * E_B;
   static constexpr unsigned OFF_A = OFF_P + 2 * P_B;
   static constexpr unsigned STAGE = OFF_A + 6 * P_B;
-  static constexpr unsigned OFF_N = NST * STAGE;     // exchange: [3 buffers][Ex, Ey, Ez]
-  static constexpr unsigned OFF_BAR = OFF_N + 9 * P_B;
+  static constexpr unsigned OFF_N = NST * STAGE;     // exchange: [3 buffers][Ex, Ez] rows
+  // PML coefficient pairs of the item: along z [6][2][PW], y [6][2][WY], x [6][2][XW]
+  static constexpr unsigned OFF_T = OFF_N + 6 * P_B;
+  static constexpr int TY0 = 6 * 2 * PW;
+  static constexpr int TX0 = TY0 + 6 * 2 * WY;
+  static constexpr unsigned T_B = rnd (sizeof (float) * (TX0 + 6 * 2 * XW));
+  static constexpr unsigned OFF_BAR = OFF_T + T_B;
   static constexpr unsigned TOTAL = OFF_BAR + 128 + 128;   // + room to align the base to 128 bytes
   // bytes each group of copies delivers (full boxes, halo and fill included)
   static constexpr unsigned TX_HE = 3u * sizeof (T) * HW * (WY + 1) + 3u * sizeof (T) * EW * WY;
   static constexpr unsigned TX_P = 2u * sizeof (float) * PW * WY;
   static constexpr unsigned TX_A = 6u * sizeof (float) * PW * WY;
+  static constexpr unsigned TX_AN = 6u * sizeof (float) * AN * WY;
 };
 
 // ---------------------------------------------------------------- PTX helpers
@@ -218,43 +227,74 @@ __device__ __forceinline__ float tfsf_curl (const FusedParams &p, int k, const d
   return d;
 }
 
-// PML update of component K at one cell: curl step of the auxiliary X with
-// the 1-D coefficient tables (ca1/sq1 along axis K+1, p5/q5 along K+2, g4
-// along K, the reference's sigma choice per component), then the field from
-// the change of X.  Returns the field; *xn receives the new auxiliary.
-template <int K>
-__device__ __forceinline__ float pml_cell (const FusedParams &p, int x, int y, int z, float xo, float cu, float im,
-                                           float fo, float *xn)
+// Pair of PML coefficient tables of component k that runs along an axis:
+// pair 0 (ca1, sq1) runs along axis k + 1, pair 1 (p5, q5) along k + 2,
+// pair 2 (g4p, g4m) along k itself (the reference's sigma choice per
+// component, InternalScheme.inc.h:2551-2640).
+__host__ __device__ constexpr int pair_along (int k, int axis)
 {
-  constexpr int A = K % 3, C1 = (K + 1) % 3, C2 = (K + 2) % 3;
-  const int i1 = C1 == 0 ? x : (C1 == 1 ? y : z);
-  const int i2 = C2 == 0 ? x : (C2 == 1 ? y : z);
-  const int ia = A == 0 ? x : (A == 1 ? y : z);
-  const float ca1 = __ldg (p.tab[K][0] + i1);
-  const float sq1 = __ldg (p.tab[K][1] + i1);
-  const float p5 = __ldg (p.tab[K][2] + i2);
-  const float q5 = __ldg (p.tab[K][3] + i2);
-  const float g4p = __ldg (p.tab[K][4] + ia);
-  const float g4m = __ldg (p.tab[K][5] + ia);
-  const float n = ca1 * xo + sq1 * cu;
-  *xn = n;
-  return p5 * fo + (g4p * n - g4m * xo) * q5 * im;
+  return (k + 1) % 3 == axis ? 0 : ((k + 2) % 3 == axis ? 1 : 2);
 }
 
-// PML update of component K on the cells of mask pm among a lane's four
-// cells (z = zc .. zc + 3); other cells keep fn and their auxiliary value.
-template <int K>
-__device__ __forceinline__ void pml_lane (const FusedParams &p, unsigned pm, int x, int y, int zc, const float xo[4],
-                                          const float cu[4], const float im[4], const float fo[4], float fn[4],
-                                          float xn[4])
+// The item's PML coefficient pairs staged in shared memory, per component k
+// and pair element t: z[(2k + t) * PW + column], y[(2k + t) * WY + row],
+// x[(2k + t) * (MAXC + 2) + plane - (xa - 1)].
+struct PmlTabs
 {
+  const float *z, *y, *x;
+};
+
+// PML update of component K on the cells of mask pm among a lane's four
+// cells: X_new = ca1 X + sq1 curl, F = p5 F + (g4p X_new - g4m X) q5 / m.
+// Branch-free over the cells; cells outside pm keep fn and their X.
+template <int K, int WY>
+__device__ __forceinline__ void pml_vec (const PmlTabs &t, int row, int plane, int col, unsigned pm,
+                                         const float xo[4], const float cu[4], const float im[4], const float fo[4],
+                                         float fn[4], float xn[4])
+{
+  constexpr int pz = pair_along (K, 2), py = pair_along (K, 1), px = pair_along (K, 0);
+  constexpr int XW = MAXC + 2;
+  float c[3][2][4];
+#pragma unroll
+  for (int e = 0; e < 2; ++e)
+  {
+    lds4f (t.z + (2 * K + e) * PW + col, c[pz][e]);
+    const float vy = t.y[(2 * K + e) * WY + row];
+    const float vx = t.x[(2 * K + e) * XW + plane];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+    {
+      c[py][e][j] = vy;
+      c[px][e][j] = vx;
+    }
+  }
 #pragma unroll
   for (int j = 0; j < 4; ++j)
   {
-    xn[j] = xo[j];
-    if ((pm >> j) & 1u)
-      fn[j] = pml_cell<K> (p, x, y, zc + j, xo[j], cu[j], im[j], fo[j], &xn[j]);
+    const float n = c[0][0][j] * xo[j] + c[0][1][j] * cu[j];
+    const float f = c[1][0][j] * fo[j] + (c[2][0][j] * n - c[2][1][j] * xo[j]) * c[1][1][j] * im[j];
+    const bool on = (pm >> j) & 1u;
+    fn[j] = on ? f : fn[j];
+    xn[j] = on ? n : xo[j];
   }
+}
+
+// The same for one cell (the z ring cell, column 128 of the tile).
+template <int K, int WY>
+__device__ __forceinline__ float pml_one (const PmlTabs &t, int row, int plane, int col, float xo, float cu,
+                                          float im, float fo)
+{
+  constexpr int pz = pair_along (K, 2), py = pair_along (K, 1);
+  constexpr int XW = MAXC + 2;
+  float c[3][2];
+#pragma unroll
+  for (int e = 0; e < 2; ++e)
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+      c[q][e] = q == pz ? t.z[(2 * K + e) * PW + col]
+                        : (q == py ? t.y[(2 * K + e) * WY + row] : t.x[(2 * K + e) * XW + plane]);
+  const float n = c[0][0] * xo + c[0][1] * cu;
+  return c[1][0] * fo + (c[2][0] * n - c[2][1] * xo) * c[1][1] * im;
 }
 
 // ------------------------------------------------------------------ kernel
@@ -265,14 +305,16 @@ __global__ void __launch_bounds__ (32 * WY, 1)
                     const SweepWork wk, int *err)
 {
   using L = Smem<T, WY>;
-  constexpr int HZ = L::HZ, HW = L::HW, EW = L::EW;
+  constexpr int HZ = L::HZ, HW = L::HW, EW = L::EW, AN = L::AN, XW = L::XW;
   constexpr int HS = L::H_B / sizeof (T), ES = L::E_B / sizeof (T), PS = L::P_B / sizeof (float);
+  constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__ (128) unsigned char smem_raw[];
   __shared__ int s_item;
   __shared__ int s_abort[2];   // per plane parity: a copy did not arrive in time
 
   const int lane = threadIdx.x, w = threadIdx.y;
-  const bool leader = w == 0 && lane == 0;
+  const int tid = w * 32 + lane;
+  const bool leader = tid == 0;
   const int nx = p.g.n[0], ny = p.g.n[1], nz = p.g.n[2];
   const size_t sx = (size_t) ny * nz;
   // 128-byte aligned base of the dynamic shared memory (TMA destinations)
@@ -284,6 +326,16 @@ __global__ void __launch_bounds__ (32 * WY, 1)
   const float S = p.courant;
   const float one4[4] = {1.f, 1.f, 1.f, 1.f};
   const bool tfsf_in = p.use_tfsf && !p.tfsf_post;   // corrections inside the sweep
+  float *const Tab = reinterpret_cast<float *> (smem + L::OFF_T);
+  const PmlTabs tabs{Tab, Tab + L::TY0, Tab + L::TX0};
+  // interior z range common to every component (cells outside it are PML for some component)
+  int zin_lo = 0, zin_hi = nz;
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+  {
+    zin_lo = max (zin_lo, p.ilo[k][2]);
+    zin_hi = min (zin_hi, p.ihi[k][2]);
+  }
 
   if (leader)
   {
@@ -295,30 +347,31 @@ __global__ void __launch_bounds__ (32 * WY, 1)
   }
   __syncthreads ();
 
-  // Does plane x of the tile at (z0, y0) hold a PML cell of Ex..Ez (at x)
-  // or of Hx..Hz (at x - 1)?  Then its stage also carries the auxiliaries.
-  auto need_aux = [&] (int x, int z0, int y0) -> bool {
+  // Auxiliary mode of plane x of the tile at (z0, y0): 0 = no PML cell of
+  // Ex..Ez at x nor of Hx..Hz at x - 1; 1 = PML cells only in the z columns
+  // of the narrow window (az0 is its first column, nar_ok whether the
+  // tile's z-PML columns fit in one); 2 = full-width auxiliary planes.
+  auto aux_mode = [&] (int x, int y0, bool zpml, bool nar_ok) -> int {
     if (!p.use_pml)
-      return false;
+      return 0;
     const int yhi = min (y0 + WY - 1, ny - 2);
-    const int zlo = max (z0, 1), zhi = min (z0 + TZ, nz - 2);
-    bool in = true;
+    bool xyin = true;
 #pragma unroll
     for (int k = 0; k < 6; ++k)
     {
       const int xx = k < 3 ? x : x - 1;
-      in = in && xx >= p.ilo[k][0] && xx < p.ihi[k][0] && y0 >= p.ilo[k][1] && yhi < p.ihi[k][1] &&
-           zlo >= p.ilo[k][2] && zhi < p.ihi[k][2];
+      xyin = xyin && xx >= p.ilo[k][0] && xx < p.ihi[k][0] && y0 >= p.ilo[k][1] && yhi < p.ihi[k][1];
     }
-    return !in;
+    if (xyin && !zpml)
+      return 0;
+    return (xyin && nar_ok) ? 1 : 2;
   };
 
   // stage `st` <- plane x of the tile at (z0, y0)
-  auto issue = [&] (unsigned st, int x, int z0, int y0) {
+  auto issue = [&] (unsigned st, int x, int z0, int y0, int mode, int az0) {
     const uint32_t s = sbase + st * L::STAGE;
     const uint32_t b = bar + 8 * st;
-    const bool na = need_aux (x, z0, y0);
-    mbar_expect_tx (b, L::TX_HE + (has_eps ? L::TX_P : 0u) + (na ? L::TX_A : 0u));
+    mbar_expect_tx (b, L::TX_HE + (has_eps ? L::TX_P : 0u) + (mode == 2 ? L::TX_A : (mode == 1 ? L::TX_AN : 0u)));
 #pragma unroll
     for (int c = 0; c < 3; ++c)
       tma_load_3d (s + c * L::H_B, &maps.h[c], z0 - HZ, y0 - 1, x, b);
@@ -330,11 +383,17 @@ __global__ void __launch_bounds__ (32 * WY, 1)
       tma_load_3d (s + L::OFF_P, &maps.eps, z0, y0, x, b);
       tma_load_3d (s + L::OFF_P + L::P_B, &maps.eps, z0, y0, min (x + 1, nx - 1), b);
     }
-    if (na)
+    if (mode)
     {
 #pragma unroll
       for (int c = 0; c < 6; ++c)
-        tma_load_3d (s + L::OFF_A + c * L::P_B, &maps.aux[c], z0, y0, c < 3 ? x : max (x - 1, 0), b);
+      {
+        const int xx = c < 3 ? x : max (x - 1, 0);
+        if (mode == 2)
+          tma_load_3d (s + L::OFF_A + c * L::P_B, &maps.aux[c], z0, y0, xx, b);
+        else
+          tma_load_3d (s + L::OFF_A + c * L::P_B, &maps.auxn[c], z0 + az0, y0, xx, b);
+      }
     }
   };
 
@@ -357,11 +416,51 @@ __global__ void __launch_bounds__ (32 * WY, 1)
     const int xa = 1 + ch * wk.chunk;
     const int xb = min (xa + wk.chunk - 1, nx - 2);
     const int np = xb - xa + 3;   // planes xa - 1 .. xb + 1 (at least 3)
+
+    // z-PML columns of the tile (ring column included) and whether one
+    // narrow window of AN columns holds them
+    const int cmin = max (0, 1 - z0), cmax = min (TZ, nz - 2 - z0);
+    const int lo_end = min (zin_lo - z0, cmax + 1);    // low-side PML columns [cmin, lo_end)
+    const int hi_beg = max (zin_hi - z0, cmin);        // high-side PML columns [hi_beg, cmax]
+    const bool zlow = lo_end > cmin, zhigh = hi_beg <= cmax;
+    const bool zpml = zlow || zhigh;
+    int az0 = 0;
+    bool nar_ok = false;
+    if (zlow && !zhigh)
+    {
+      az0 = cmin & ~3;
+      nar_ok = lo_end - az0 <= AN;
+    }
+    else if (zhigh && !zlow)
+    {
+      az0 = hi_beg & ~3;
+      nar_ok = cmax + 1 - az0 <= AN;
+    }
+
     if (leader)
     {
 #pragma unroll
       for (int k = 0; k < NST; ++k)
-        issue ((gst + k) % NST, xa - 1 + k, z0, y0);
+        issue ((gst + k) % NST, xa - 1 + k, z0, y0, aux_mode (xa - 1 + k, y0, zpml, nar_ok), az0);
+    }
+    // PML coefficient pairs of this item (read after the first plane's barrier)
+    if (p.use_pml)
+    {
+      for (int q = tid; q < 6 * 2 * PW; q += 32 * WY)
+      {
+        const int k = q / (2 * PW), e = (q / PW) % 2, z = z0 + q % PW;
+        Tab[q] = z < nz ? __ldg (p.tab[k][2 * pair_along (k, 2) + e] + z) : 0.f;
+      }
+      for (int q = tid; q < 6 * 2 * WY; q += 32 * WY)
+      {
+        const int k = q / (2 * WY), e = (q / WY) % 2, yy = min (y0 + q % WY, ny - 1);
+        Tab[L::TY0 + q] = __ldg (p.tab[k][2 * pair_along (k, 1) + e] + yy);
+      }
+      for (int q = tid; q < 6 * 2 * XW; q += 32 * WY)
+      {
+        const int k = q / (2 * XW), e = (q / XW) % 2, xx = min (max (xa - 1 + q % XW, 0), nx - 1);
+        Tab[L::TX0 + q] = __ldg (p.tab[k][2 * pair_along (k, 0) + e] + xx);
+      }
     }
 
     // ---- per-lane / per-row constants of this item
@@ -395,8 +494,9 @@ __global__ void __launch_bounds__ (32 * WY, 1)
     const bool ring_lane = lane == 31 && w < WY - 1;
 
     float hp[3][4];           // H_old(x - 1) on the lane's cells
+    float ep[3][4];           // E_new(x - 1) on the lane's cells
     float hpr = 0.f;          // lane 31: Hz_old(x - 1) on the z ring cell
-    float en[3][4];           // E_new(x)
+    float rxp = 0.f, ryp = 0.f;   // lane 31: Ex_new, Ey_new(x - 1) on the z ring cell
     unsigned nbuf = 0;        // exchange buffer of this plane (plane index mod 3)
     unsigned st = gst;
     for (int i = 0; i < np; ++i)
@@ -408,29 +508,41 @@ __global__ void __launch_bounds__ (32 * WY, 1)
         atomicOr (err, 4);
       }
       phase ^= 1u << st;
-      const bool na = need_aux (x, z0, y0);
+      const int amode = aux_mode (x, y0, zpml, nar_ok);
+      const int apitch = amode == 2 ? PW : AN;
+      const int acol = amode == 2 ? zl : zl - az0;      // only read on lanes with PML cells
       const unsigned char *stg = smem + st * L::STAGE;
       const T *sH = reinterpret_cast<const T *> (stg);
       const T *sE = reinterpret_cast<const T *> (stg + L::OFF_E);
       const float *P0 = reinterpret_cast<const float *> (stg + L::OFF_P);
       const float *P1 = P0 + PS;
       const float *A = reinterpret_cast<const float *> (stg + L::OFF_A);
-      float *N = reinterpret_cast<float *> (smem + L::OFF_N + nbuf * 3 * L::P_B);
+      float *N = reinterpret_cast<float *> (smem + L::OFF_N + nbuf * 2 * L::P_B);
 
       float hc[3][4];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
         Vec<T>::ld4 (sH + c * HS + (w + 1) * HW + HZ + zl, hc[c]);
       const float hzr = Vec<T>::ld1 (sH + 2 * HS + (w + 1) * HW + HZ + TZ);
-      // auxiliaries of H(x - 1) for the H step (the stage is refilled after the barrier)
+      // PML masks and auxiliaries of H(x - 1) for the H step (the stage is
+      // refilled after the barrier)
+      const int xh = x - 1;
+      unsigned pmh[3] = {0u, 0u, 0u};
       float ha[3][4];
-      const bool hpml = i > 1 && own_row && na;
-      if (hpml)
+      if (amode && i > 1 && own_row && zupd)
       {
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-          lds4f (A + (3 + c) * PS + w * PW + zl, ha[c]);
+        {
+          const int k = 3 + c;
+          const bool xy = xh >= p.ilo[k][0] && xh < p.ihi[k][0] && ((yin >> k) & 1u);
+          pmh[c] = zupd & ~((xy ? zin : 0u) >> (4 * k)) & 15u;
+          if (pmh[c])
+            lds4f (A + (3 + c) * PS + w * apitch + acol, ha[c]);
+        }
       }
+      float en[3][4];           // E_new(x)
+      float rx = 0.f, ry = 0.f; // lane 31: E_new(x) on the z ring cell
 
       if (i > 0)
       {
@@ -500,32 +612,36 @@ __global__ void __launch_bounds__ (32 * WY, 1)
           en[2][j] = u ? eo[2][j] + (S * iz[j]) * cz[j] : eo[2][j];
         }
         const bool store_e = own_row && x <= xb && lane_ok;
-        if (na && upd)
+        if (amode && upd)
         {
-          const unsigned pm0 = upd & ~((x >= p.ilo[0][0] && x < p.ihi[0][0] && (yin & 1u)) ? zin : 0u);
-          const unsigned pm1 = upd & ~(((x >= p.ilo[1][0] && x < p.ihi[1][0] && (yin & 2u)) ? zin : 0u) >> 4);
-          const unsigned pm2 = upd & ~(((x >= p.ilo[2][0] && x < p.ihi[2][0] && (yin & 4u)) ? zin : 0u) >> 8);
-          if (pm0 & 15u)
+          unsigned pm[3];
+#pragma unroll
+          for (int k = 0; k < 3; ++k)
+          {
+            const bool xy = x >= p.ilo[k][0] && x < p.ihi[k][0] && ((yin >> k) & 1u);
+            pm[k] = upd & ~((xy ? zin : 0u) >> (4 * k)) & 15u;
+          }
+          if (pm[0])
           {
             float xo[4], xn[4];
-            lds4f (A + 0 * PS + w * PW + zl, xo);
-            pml_lane<0> (p, pm0 & 15u, x, y, zc, xo, cx, ix, eo[0], en[0], xn);
+            lds4f (A + 0 * PS + w * apitch + acol, xo);
+            pml_vec<0, WY> (tabs, w, i, zl, pm[0], xo, cx, ix, eo[0], en[0], xn);
             if (store_e)
               Vec<float>::st4 (p.aux_new[0] + id, xn);
           }
-          if (pm1 & 15u)
+          if (pm[1])
           {
             float xo[4], xn[4];
-            lds4f (A + 1 * PS + w * PW + zl, xo);
-            pml_lane<1> (p, pm1 & 15u, x, y, zc, xo, cy, iy, eo[1], en[1], xn);
+            lds4f (A + 1 * PS + w * apitch + acol, xo);
+            pml_vec<1, WY> (tabs, w, i, zl, pm[1], xo, cy, iy, eo[1], en[1], xn);
             if (store_e)
               Vec<float>::st4 (p.aux_new[1] + id, xn);
           }
-          if (pm2 & 15u)
+          if (pm[2])
           {
             float xo[4], xn[4];
-            lds4f (A + 2 * PS + w * PW + zl, xo);
-            pml_lane<2> (p, pm2 & 15u, x, y, zc, xo, cz, iz, eo[2], en[2], xn);
+            lds4f (A + 2 * PS + w * apitch + acol, xo);
+            pml_vec<2, WY> (tabs, w, i, zl, pm[2], xo, cz, iz, eo[2], en[2], xn);
             if (store_e)
               Vec<float>::st4 (p.aux_new[2] + id, xn);
           }
@@ -550,63 +666,57 @@ __global__ void __launch_bounds__ (32 * WY, 1)
           for (int c = 0; c < 3; ++c)
             Vec<T>::st4 (reinterpret_cast<T *> (p.e_new[c]) + id, en[c]);
         }
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-          sts4f (N + c * PS + w * PW + zl, en[c]);
+        // Ex and Ez rows for the H step of the warp below (its y + 1 neighbours)
+        sts4f (N + 0 * PS + w * PW + zl, en[0]);
+        sts4f (N + 1 * PS + w * PW + zl, en[2]);
 
-        // z ring: Ex and Ey at z0 + 128 for H of the lane's last cell
-        if (ring_lane)
+        // z ring: Ex and Ey at z0 + 128 for H of lane 31's last cell
+        if (ring_lane && zr <= nz - 1)
         {
-          float rx = 0.f, ry = 0.f;
-          if (zr <= nz - 1)
+          rx = Vec<T>::ld1 (sE + 0 * ES + w * EW + TZ);
+          ry = Vec<T>::ld1 (sE + 1 * ES + w * EW + TZ);
+          if (rowupd && zr <= nz - 2)
           {
-            rx = Vec<T>::ld1 (sE + 0 * ES + w * EW + TZ);
-            ry = Vec<T>::ld1 (sE + 1 * ES + w * EW + TZ);
-            if (rowupd && zr <= nz - 2)
+            const float hz = hzr;
+            const float hzym = Vec<T>::ld1 (sH + 2 * HS + w * HW + HZ + TZ);
+            const float hy = Vec<T>::ld1 (sH + 1 * HS + (w + 1) * HW + HZ + TZ);
+            const float hx = Vec<T>::ld1 (sH + 0 * HS + (w + 1) * HW + HZ + TZ);
+            float crx = (hz - hzym) - (hy - hc[1][3]);
+            float cry = (hx - hc[0][3]) - (hz - hpr);
+            float irx = 1.f, iry = 1.f;
+            if (has_eps)
             {
-              const float hz = hzr;
-              const float hzym = Vec<T>::ld1 (sH + 2 * HS + w * HW + HZ + TZ);
-              const float hy = Vec<T>::ld1 (sH + 1 * HS + (w + 1) * HW + HZ + TZ);
-              const float hx = Vec<T>::ld1 (sH + 0 * HS + (w + 1) * HW + HZ + TZ);
-              float crx = (hz - hzym) - (hy - hc[1][3]);
-              float cry = (hx - hc[0][3]) - (hz - hpr);
-              float irx = 1.f, iry = 1.f;
-              if (has_eps)
-              {
-                const float e0 = P0[w * PW + TZ];
-                irx = __fdividef (2.f, e0 + P1[w * PW + TZ]);
-                iry = __fdividef (2.f, e0 + P0[(w + 1) * PW + TZ]);
-              }
-              if (tfsf_in && (xface || yface || on_face (p.face[2], zr)))
-              {
-                crx += tfsf_curl (p, 0, p.inc_h, err, x, y, zr);
-                cry += tfsf_curl (p, 1, p.inc_h, err, x, y, zr);
-              }
-              const bool in0 = x >= p.ilo[0][0] && x < p.ihi[0][0] && (yin & 1u) && zr >= p.ilo[0][2] &&
-                               zr < p.ihi[0][2];
-              const bool in1 = x >= p.ilo[1][0] && x < p.ihi[1][0] && (yin & 2u) && zr >= p.ilo[1][2] &&
-                               zr < p.ihi[1][2];
-              float dummy;
-              if (p.use_pml && !in0)
-                rx = pml_cell<0> (p, x, y, zr, A[0 * PS + w * PW + TZ], crx, irx, rx, &dummy);
-              else
-                rx = rx + (S * irx) * crx;
-              if (p.use_pml && !in1)
-                ry = pml_cell<1> (p, x, y, zr, A[1 * PS + w * PW + TZ], cry, iry, ry, &dummy);
-              else
-                ry = ry + (S * iry) * cry;
-              if ((p.ps_mask & 3) && x == p.ps[0] && y == p.ps[1] && zr == p.ps[2])
-              {
-                const float v = (float) p.src[p.src_index];
-                if (p.ps_mask & 1)
-                  rx = v;
-                if (p.ps_mask & 2)
-                  ry = v;
-              }
+              const float e0 = P0[w * PW + TZ];
+              irx = __fdividef (2.f, e0 + P1[w * PW + TZ]);
+              iry = __fdividef (2.f, e0 + P0[(w + 1) * PW + TZ]);
+            }
+            if (tfsf_in && (xface || yface || on_face (p.face[2], zr)))
+            {
+              crx += tfsf_curl (p, 0, p.inc_h, err, x, y, zr);
+              cry += tfsf_curl (p, 1, p.inc_h, err, x, y, zr);
+            }
+            const bool in0 = x >= p.ilo[0][0] && x < p.ihi[0][0] && (yin & 1u) && zr >= p.ilo[0][2] &&
+                             zr < p.ihi[0][2];
+            const bool in1 = x >= p.ilo[1][0] && x < p.ihi[1][0] && (yin & 2u) && zr >= p.ilo[1][2] &&
+                             zr < p.ihi[1][2];
+            const int rcol = amode == 2 ? TZ : TZ - az0;
+            if (amode && !in0)
+              rx = pml_one<0, WY> (tabs, w, i, TZ, A[0 * PS + w * apitch + rcol], crx, irx, rx);
+            else
+              rx = rx + (S * irx) * crx;
+            if (amode && !in1)
+              ry = pml_one<1, WY> (tabs, w, i, TZ, A[1 * PS + w * apitch + rcol], cry, iry, ry);
+            else
+              ry = ry + (S * iry) * cry;
+            if ((p.ps_mask & 3) && x == p.ps[0] && y == p.ps[1] && zr == p.ps[2])
+            {
+              const float v = (float) p.src[p.src_index];
+              if (p.ps_mask & 1)
+                rx = v;
+              if (p.ps_mask & 2)
+                ry = v;
             }
           }
-          N[0 * PS + w * PW + TZ] = rx;
-          N[1 * PS + w * PW + TZ] = ry;
         }
       }
 
@@ -624,31 +734,32 @@ __global__ void __launch_bounds__ (32 * WY, 1)
         break;
       }
       if (leader && i + NST < np)
-        issue (st, x + NST, z0, y0);
+        issue (st, x + NST, z0, y0, aux_mode (x + NST, y0, zpml, nar_ok), az0);
 
       if (i > 1 && own_row)
       {
         // ================= H_new(x - 1) on the owned rows
-        const int xh = x - 1;
         const float *Np =
-            reinterpret_cast<const float *> (smem + L::OFF_N + (nbuf == 0 ? 2u : nbuf - 1u) * 3 * L::P_B);
-        float ex[4], ey[4], ez[4], exy[4], ezy[4];
-        lds4f (Np + 0 * PS + w * PW + zl, ex);
-        lds4f (Np + 1 * PS + w * PW + zl, ey);
-        lds4f (Np + 2 * PS + w * PW + zl, ez);
+            reinterpret_cast<const float *> (smem + L::OFF_N + (nbuf == 0 ? 2u : nbuf - 1u) * 2 * L::P_B);
+        float exy[4], ezy[4];
         lds4f (Np + 0 * PS + (w + 1) * PW + zl, exy);
-        lds4f (Np + 2 * PS + (w + 1) * PW + zl, ezy);
-        const float exz = Np[0 * PS + w * PW + zl + 4];
-        const float eyz = Np[1 * PS + w * PW + zl + 4];
+        lds4f (Np + 1 * PS + (w + 1) * PW + zl, ezy);
+        float exz = __shfl_down_sync (FULL, ep[0][0], 1);
+        float eyz = __shfl_down_sync (FULL, ep[1][0], 1);
+        if (lane == 31)
+        {
+          exz = rxp;
+          eyz = ryp;
+        }
         float ax[4], ay[4], az[4], hn[3][4];
 #pragma unroll
         for (int j = 0; j < 4; ++j)
         {
-          const float eyn = j < 3 ? ey[j + 1] : eyz;
-          const float exn = j < 3 ? ex[j + 1] : exz;
-          ax[j] = (eyn - ey[j]) - (ezy[j] - ez[j]);
-          ay[j] = (en[2][j] - ez[j]) - (exn - ex[j]);
-          az[j] = (exy[j] - ex[j]) - (en[1][j] - ey[j]);
+          const float eyn = j < 3 ? ep[1][j + 1] : eyz;
+          const float exn = j < 3 ? ep[0][j + 1] : exz;
+          ax[j] = (eyn - ep[1][j]) - (ezy[j] - ep[2][j]);
+          ay[j] = (en[2][j] - ep[2][j]) - (exn - ep[0][j]);
+          az[j] = (exy[j] - ep[0][j]) - (en[1][j] - ep[1][j]);
         }
         const size_t idh = (size_t) xh * sx + rowoff;
         const bool xface = tfsf_in && on_face (p.face[0], xh);
@@ -672,32 +783,26 @@ __global__ void __launch_bounds__ (32 * WY, 1)
           hn[1][j] = u ? hp[1][j] + S * ay[j] : hp[1][j];
           hn[2][j] = u ? hp[2][j] + S * az[j] : hp[2][j];
         }
-        if (hpml && zupd)
+        if (pmh[0])
         {
-          const unsigned pm3 = zupd & ~(((xh >= p.ilo[3][0] && xh < p.ihi[3][0] && (yin & 8u)) ? zin : 0u) >> 12);
-          const unsigned pm4 = zupd & ~(((xh >= p.ilo[4][0] && xh < p.ihi[4][0] && (yin & 16u)) ? zin : 0u) >> 16);
-          const unsigned pm5 = zupd & ~(((xh >= p.ilo[5][0] && xh < p.ihi[5][0] && (yin & 32u)) ? zin : 0u) >> 20);
-          if (pm3 & 15u)
-          {
-            float xn[4];
-            pml_lane<3> (p, pm3 & 15u, xh, y, zc, ha[0], ax, one4, hp[0], hn[0], xn);
-            if (lane_ok)
-              Vec<float>::st4 (p.aux_new[3] + idh, xn);
-          }
-          if (pm4 & 15u)
-          {
-            float xn[4];
-            pml_lane<4> (p, pm4 & 15u, xh, y, zc, ha[1], ay, one4, hp[1], hn[1], xn);
-            if (lane_ok)
-              Vec<float>::st4 (p.aux_new[4] + idh, xn);
-          }
-          if (pm5 & 15u)
-          {
-            float xn[4];
-            pml_lane<5> (p, pm5 & 15u, xh, y, zc, ha[2], az, one4, hp[2], hn[2], xn);
-            if (lane_ok)
-              Vec<float>::st4 (p.aux_new[5] + idh, xn);
-          }
+          float xn[4];
+          pml_vec<3, WY> (tabs, w, i - 1, zl, pmh[0], ha[0], ax, one4, hp[0], hn[0], xn);
+          if (lane_ok)
+            Vec<float>::st4 (p.aux_new[3] + idh, xn);
+        }
+        if (pmh[1])
+        {
+          float xn[4];
+          pml_vec<4, WY> (tabs, w, i - 1, zl, pmh[1], ha[1], ay, one4, hp[1], hn[1], xn);
+          if (lane_ok)
+            Vec<float>::st4 (p.aux_new[4] + idh, xn);
+        }
+        if (pmh[2])
+        {
+          float xn[4];
+          pml_vec<5, WY> (tabs, w, i - 1, zl, pmh[2], ha[2], az, one4, hp[2], hn[2], xn);
+          if (lane_ok)
+            Vec<float>::st4 (p.aux_new[5] + idh, xn);
         }
         if ((p.ps_mask & 56) && xh == p.ps[0] && y == p.ps[1] && p.ps[2] >= zc && p.ps[2] < zc + 4)
         {
@@ -725,8 +830,13 @@ __global__ void __launch_bounds__ (32 * WY, 1)
       for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int j = 0; j < 4; ++j)
+        {
           hp[c][j] = hc[c][j];
+          ep[c][j] = en[c][j];
+        }
       hpr = hzr;
+      rxp = rx;
+      ryp = ry;
       nbuf = nbuf == 2u ? 0u : nbuf + 1u;
       st = st == NST - 1 ? 0u : st + 1u;
     }
@@ -888,11 +998,12 @@ std::string plan_t (SweepPlan &pl, const FusedParams &p, void *const e[2][3], vo
     {
       if (p.use_pml)
       {
-        if (!aux[b][k] || !make_map (m.aux[k], aux[b][k], false, p.g.n, PW, WY))
+        if (!aux[b][k] || !make_map (m.aux[k], aux[b][k], false, p.g.n, PW, WY) ||
+            !make_map (m.auxn[k], aux[b][k], false, p.g.n, L::AN, WY))
           return "tensor map encoding failed";
       }
       else
-        m.aux[k] = m.e[0];
+        m.aux[k] = m.auxn[k] = m.e[0];
     }
   }
   auto kern = sweep3d_kernel<T, WY>;
@@ -947,6 +1058,8 @@ std::string sweep3d_plan (SweepPlan &plan, const FusedParams &p, void *const e[2
     return "unsupported CTA height";
   if (chunk < 1)
     return "bad x chunk";
+  if (p.use_pml && chunk > MAXC)
+    chunk = MAXC;   // the item's x coefficient table holds MAXC + 2 planes
   plan.wy = wy;
   std::string why = p.fp16 ? plan_t<__half, 8> (plan, p, e, h, aux, eps, sm_count)
                            : plan_t<float, 8> (plan, p, e, h, aux, eps, sm_count);

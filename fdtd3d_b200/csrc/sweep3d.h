@@ -22,6 +22,7 @@ struct SweepMaps
   CUtensorMap e[3];
   CUtensorMap eps;
   CUtensorMap aux[6];
+  CUtensorMap auxn[6];         // narrow (32-cell) boxes for planes whose PML cells are all at a z edge
 };
 
 struct SweepWork
