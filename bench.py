@@ -14,10 +14,12 @@ no flush is needed between steps.
   e2e    : the same metric through the C ABI with host buffers: each e2e
            step uploads eps from pinned host memory, advances a chunk of
            time steps and downloads Ez to pinned host memory.
-  roofline: field half-step kernel, algorithmic bytes per launch
-           (cells * B/2, B = 4*(12 + m + 12*f_PML) bytes per cell-update)
-           over its measured average launch time, against the measured
-           HBM copy bandwidth.
+  roofline: the field-update launches of one time step (the sweep kernel
+           of each item class and the TF/SF post pass, timed together by
+           CUDA events on the library's stream), algorithmic bytes per step
+           (cells * B, B = 4*(12 + m + 12*f_PML) bytes per cell-update) over
+           their measured time per step, against the measured HBM copy
+           bandwidth.
   cpu_baseline: the reference fdtd3d CPU build (oracle/_ref/fdtd3d) on a
            bounded sample of the same physics (one process).
 
@@ -47,6 +49,13 @@ METRIC = "Gcell-updates/s"
 N_DEFAULT = 512
 PML = 16
 TFSF = 32
+
+
+def kernel_label(step_kernel: str) -> str:
+    if step_kernel == "sweep3d_tma":
+        return ("sweep3d_kernel (lean / z-edge PML / full item classes) + tfsf_post_kernel: "
+                "E and H of one time step")
+    return f"{step_kernel}: E and H of one time step"
 
 
 def workload_kw(n: int, precision: int) -> dict:
@@ -271,6 +280,7 @@ def main() -> None:
     ms = ev0.elapsed_time(ev1)
     kernel_ms, kernel_launches = sim.kernel_time()
     sim.profile(False)
+    sim_kernel = sim.step_kernel
     launches = sim.launch_count() - l0
     if dist:
         t = torch.tensor([ms], device=f"cuda:{local}")
@@ -282,14 +292,15 @@ def main() -> None:
     peaks = measured_peaks()
     b_cell, f_pml = algorithmic_bytes_per_cell(n, word)
     avg_launch_ms = kernel_ms / max(kernel_launches, 1)
-    # the one-sweep kernel advances a whole time step per launch; the
-    # per-cell kernels take two launches (E, H) per step
+    # one timed unit per time step on the sweep path (the sweep kernels of
+    # the three item classes plus the TF/SF post pass); the per-cell kernels
+    # take two timed units (E, H) per step
     steps_per_launch = args.steps / max(kernel_launches, 1)
     bytes_per_launch = cells * b_cell * steps_per_launch
     achieved = bytes_per_launch / (avg_launch_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": None,
-                "kernel": "fused3d_kernel (E and H of one time step)" if steps_per_launch > 0.75
+                "kernel": kernel_label(sim_kernel) if steps_per_launch > 0.75
                 else "fast_half_kernel (E or H family)", "avg_launch_ms": avg_launch_ms,
                 "bytes_per_launch": bytes_per_launch,
                 "algorithmic_bytes_per_cell_update": b_cell, "f_pml": f_pml,

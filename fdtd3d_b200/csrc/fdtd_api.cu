@@ -538,11 +538,10 @@ void init_fused (fdtd_ctx *ctx)
   f.gamma[1] = ctx->drude32[3];
 }
 
-// x chunk of the TMA sweep: items of (chunk + 2) planes each (one halo
-// plane, one recomputed E plane) over the persistent CTAs, plus on average
-// half an item of tail.  Candidates start at 16 planes, below which the
-// halo planes dominate.
-int sweep_chunk (const int n[3], int wy, int ctas)
+// x chunk of the TMA sweep: every item streams its planes plus one halo
+// plane and one recomputed E plane over the persistent CTAs, and the last
+// item to start sets the tail; ties go to the shorter chunk.
+int sweep_chunk (const FusedParams &p, int wy, int ctas)
 {
   static const int cand[] = {16, 24, 32, 48, 64};
   int best = 32;
@@ -550,9 +549,12 @@ int sweep_chunk (const int n[3], int wy, int ctas)
   for (int c : cand)
   {
     SweepWork w{};
-    sweep3d_items (n, wy, c, w);
-    double t = (double) w.nitems * (c + 2) / std::max (ctas, 1) + 0.5 * (c + 2);
-    if (t < best_t)
+    sweep3d_items (p, wy, c, w);
+    double planes = 0;
+    for (int j = 0; j < w.nch; ++j)
+      planes += w.xcut[j + 1] - w.xcut[j] + 2;
+    const double t = planes * w.nzt * w.nyt / std::max (ctas, 1) + (w.chunk + 2);
+    if (t < best_t * 0.999)
     {
       best_t = t;
       best = c;
@@ -575,8 +577,11 @@ int plan_sweep (fdtd_ctx *ctx)
       return FDTD_OK;
     }
   const int wy = 8;
+  bool lean = true;
+  if (const char *v = std::getenv ("FDTDB_SWEEP_LEAN"))
+    lean = std::atoi (v) != 0;
   if (!ctx->sweep_ctr)
-    DALLOC (ctx->sweep_ctr, 2 * sizeof (unsigned long long));
+    DALLOC (ctx->sweep_ctr, 6 * sizeof (unsigned long long));
   void *e[2][3], *h[2][3];
   float *aux[2][6];
   for (int b = 0; b < 2; ++b)
@@ -589,54 +594,56 @@ int plan_sweep (fdtd_ctx *ctx)
     for (int k = 0; k < 6; ++k)
       aux[b][k] = ctx->auxb[b][k];
   }
+  // TF/SF as a post pass over the face band when the band is PML-free
+  // (FDTDB_TFSF_POST=0 keeps the corrections inside the sweep).  Decided
+  // before the plan: the item classes depend on it.
+  bool post = g.cfg.use_tfsf && ctx->band.cells == 0;
+  if (const char *v = std::getenv ("FDTDB_TFSF_POST"))
+    post = post && std::atoi (v) != 0;
+  if (post)
+  {
+    std::vector<int> boxes;
+    std::vector<long long> offset;
+    std::string bwhy = tfsf_band_boxes (ctx->fused, boxes, offset);
+    if (bwhy.empty () && !boxes.empty ())
+    {
+      DALLOC (ctx->band.boxes, boxes.size () * sizeof (int));
+      DALLOC (ctx->band.offset, offset.size () * sizeof (long long));
+      CK (cudaMemcpyAsync (ctx->band.boxes, boxes.data (), boxes.size () * sizeof (int), cudaMemcpyHostToDevice,
+                           ctx->stream));
+      CK (cudaMemcpyAsync (ctx->band.offset, offset.data (), offset.size () * sizeof (long long),
+                           cudaMemcpyHostToDevice, ctx->stream));
+      CK (cudaStreamSynchronize (ctx->stream));
+      ctx->band.nbox = (int) boxes.size () / 6;
+      ctx->band.cells = offset.back ();
+    }
+  }
+  ctx->fused.tfsf_post = ctx->band.cells > 0 ? 1 : 0;   // read only by the sweep kernels
   // a first plan gives the CTA count the chunk choice depends on
   std::string why = sweep3d_plan (ctx->sweep, ctx->fused, e, h, aux, ctx->mat32[0], ctx->sm_count, wy, 32,
-                                  ctx->sweep_ctr);
+                                  ctx->sweep_ctr, lean);
   if (why.empty ())
   {
-    int chunk = sweep_chunk (g.n, wy, ctx->sweep.ctas);
+    int chunk = sweep_chunk (ctx->fused, wy, ctx->sweep.ctas);
     if (const char *v = std::getenv ("FDTDB_SWEEP_CHUNK"))
       chunk = std::max (1, std::atoi (v));
     why = sweep3d_plan (ctx->sweep, ctx->fused, e, h, aux, ctx->mat32[0], ctx->sm_count, wy, chunk,
-                        ctx->sweep_ctr);
+                        ctx->sweep_ctr, lean);
   }
   ctx->sweep_why = why;
   if (why.empty ())
   {
     ctx->sweep_state = 1;
     ctx->sweep_eps = ctx->mat32[0];
-    // TF/SF as a post pass over the face band when the band is PML-free
-    // (FDTDB_TFSF_POST=0 keeps the corrections inside the sweep)
-    bool post = g.cfg.use_tfsf && ctx->band.cells == 0;
-    if (const char *v = std::getenv ("FDTDB_TFSF_POST"))
-      post = post && std::atoi (v) != 0;
-    if (post)
-    {
-      std::vector<int> boxes;
-      std::vector<long long> offset;
-      std::string bwhy = tfsf_band_boxes (ctx->fused, boxes, offset);
-      if (bwhy.empty () && !boxes.empty ())
-      {
-        DALLOC (ctx->band.boxes, boxes.size () * sizeof (int));
-        DALLOC (ctx->band.offset, offset.size () * sizeof (long long));
-        CK (cudaMemcpyAsync (ctx->band.boxes, boxes.data (), boxes.size () * sizeof (int), cudaMemcpyHostToDevice,
-                             ctx->stream));
-        CK (cudaMemcpyAsync (ctx->band.offset, offset.data (), offset.size () * sizeof (long long),
-                             cudaMemcpyHostToDevice, ctx->stream));
-        CK (cudaStreamSynchronize (ctx->stream));
-        ctx->band.nbox = (int) boxes.size () / 6;
-        ctx->band.cells = offset.back ();
-      }
-    }
   }
   if (const char *v = std::getenv ("FDTDB_SWEEP_VERBOSE"))
     if (std::atoi (v) != 0)
     {
       const SweepWork &w = ctx->sweep.work;
       std::fprintf (stderr, "sweep3d: %s wy=%d ctas=%d smem=%u tiles z=%d y=%d chunks=%d (x chunk %d) items=%d "
-                    "tfsf band boxes=%d cells=%lld\n",
+                    "items lean/z-edge/full=%d/%d/%d tfsf band boxes=%d cells=%lld\n",
                     why.empty () ? "in use" : why.c_str (), ctx->sweep.wy, ctx->sweep.ctas, ctx->sweep.smem, w.nzt,
-                    w.nyt, w.nch, w.chunk, w.nitems, ctx->band.nbox, ctx->band.cells);
+                    w.nyt, w.nch, w.chunk, w.nitems, ctx->sweep.items[0], ctx->sweep.items[1], ctx->sweep.items[2], ctx->band.nbox, ctx->band.cells);
     }
   return FDTD_OK;
 }
@@ -859,11 +866,9 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
         return r;
       if (ctx->sweep_state == 1)
       {
-        f.tfsf_post = ctx->band.cells > 0 ? 1 : 0;
         ctx->launches += launch_sweep3d (ctx->sweep, o, f, ctx->d_err, s);
         if (f.tfsf_post)
           ctx->launches += launch_tfsf_post (ctx->band, f, ctx->d_err, s);
-        f.tfsf_post = 0;
         ctx->step_kernel = "sweep3d_tma";
       }
       else
@@ -1113,7 +1118,9 @@ int fdtd_sync (fdtd_ctx *ctx, int64_t timeout_ns)
   int flag = 0;
   CK (cudaMemcpy (&flag, ctx->d_err, sizeof (int), cudaMemcpyDeviceToHost));
   if (flag)
-    return fail (ctx, FDTD_ERR_DEVICE, "a kernel reported an out-of-range incident-grid index");
+    return fail (ctx, FDTD_ERR_DEVICE,
+                 (flag & 4) ? "a sweep kernel gave up waiting for its tensor copies (pipeline timeout)"
+                            : "a kernel reported an out-of-range incident-grid index");
   return FDTD_OK;
 }
 

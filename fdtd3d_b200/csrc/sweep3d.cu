@@ -34,6 +34,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "incident_dev.cuh"
@@ -45,7 +46,7 @@ namespace {
 
 constexpr int TZ = 128;           // z cells per tile: 32 lanes x 4
 constexpr int PW = TZ + 4;        // eps / auxiliary / exchange row width in floats (z0 .. z0 + 131)
-constexpr int NST = 3;            // pipeline stages
+constexpr int NST = 3;            // pipeline stages (plane index mod 3 = stage = exchange buffer)
 constexpr int MAXC = 64;          // largest x chunk when PML coefficient tables are staged
 
 template <typename T, int WY>
@@ -227,6 +228,15 @@ __device__ __forceinline__ float tfsf_curl (const FusedParams &p, int k, const d
   return d;
 }
 
+// Out-of-line TF/SF curl change for the sweep's rarely taken in-kernel path
+// (TF/SF bands that reach the PML), so that its code stays out of the hot
+// loop body.
+__device__ __noinline__ float tfsf_curl_cold (const FusedParams *p, int k, const double *inc, int *err, int x, int y,
+                                              int z)
+{
+  return tfsf_curl (*p, k, inc, err, x, y, z);
+}
+
 // Pair of PML coefficient tables of component k that runs along an axis:
 // pair 0 (ca1, sq1) runs along axis k + 1, pair 1 (p5, q5) along k + 2,
 // pair 2 (g4p, g4m) along k itself (the reference's sigma choice per
@@ -297,9 +307,68 @@ __device__ __forceinline__ float pml_one (const PmlTabs &t, int row, int plane, 
   return c[1][0] * fo + (c[2][0] * n - c[2][1] * xo) * c[1][1] * im;
 }
 
+// ------------------------------------------------------------ item classes
+
+// Class of work item `item` (the kernel instantiation that runs it):
+//   2 (full): TF/SF corrections inside the sweep, a point source on a plane
+//     the item updates (E on x = xa .. xb + 1, H on x = xa .. xb), or a PML
+//     cell of any component off the z edges of the tile;
+//   1 (z edge): PML cells only in z columns that one narrow window of the
+//     tile holds (the ring column included), x and y interior;
+//   0 (lean): none of these.
+// Shared by the host (launch and counts) and the kernels (item pick).
+__host__ __device__ inline int sweep_item_class (const FusedParams &p, const SweepWork &wk, int wy, int item,
+                                                 bool tfsf_in)
+{
+  const int nx = p.g.n[0], ny = p.g.n[1], nz = p.g.n[2];
+  const int zt = item % wk.nzt;
+  const int yt = (item / wk.nzt) % wk.nyt;
+  const int ch = item / (wk.nzt * wk.nyt);
+  const int z0 = zt * TZ, y0 = 1 + yt * (wy - 1), xa = wk.xcut[ch];
+  const int xb = wk.xcut[ch + 1] - 1;
+  if (tfsf_in || !wk.lean)
+    return 2;
+  if (p.ps_mask && p.ps[0] >= xa && p.ps[0] <= xb + 1)
+    return 2;
+  if (!p.use_pml)
+    return 0;
+  const int yhi = y0 + wy - 1 < ny - 2 ? y0 + wy - 1 : ny - 2;
+  // x and y must be interior for every component
+  for (int k = 0; k < 6; ++k)
+  {
+    const int xhi = k < 3 ? (xb + 1 < nx - 2 ? xb + 1 : nx - 2) : xb;
+    if (xa < p.ilo[k][0] || xhi >= p.ihi[k][0] || y0 < p.ilo[k][1] || yhi >= p.ihi[k][1])
+      return 2;
+  }
+  // z: updated columns cmin .. cmax of the tile against the common interior
+  int zin_lo = 0, zin_hi = nz;
+  for (int k = 0; k < 6; ++k)
+  {
+    zin_lo = p.ilo[k][2] > zin_lo ? p.ilo[k][2] : zin_lo;
+    zin_hi = p.ihi[k][2] < zin_hi ? p.ihi[k][2] : zin_hi;
+  }
+  const int cmin = 1 - z0 > 0 ? 1 - z0 : 0;
+  const int cmax = nz - 2 - z0 < TZ ? nz - 2 - z0 : TZ;
+  const int lo_end = zin_lo - z0 < cmax + 1 ? zin_lo - z0 : cmax + 1;
+  const int hi_beg = zin_hi - z0 > cmin ? zin_hi - z0 : cmin;
+  const bool zlow = lo_end > cmin, zhigh = hi_beg <= cmax;
+  if (!zlow && !zhigh)
+    return 0;
+  if (zlow && zhigh)
+    return 2;
+  const int az0 = (zlow ? cmin : hi_beg) & ~3;
+  const int width = (zlow ? lo_end : cmax + 1) - az0;
+  return width <= 32 ? 1 : 2;
+}
+
 // ------------------------------------------------------------------ kernel
 
-template <typename T, int WY>
+// MODE (item class, see sweep_item_class): 0 = lean, no PML cell, point
+// source or in-sweep TF/SF (straight-line planes); 1 = z edge, PML cells
+// only in the z columns of one narrow window; 2 = full.  Classes 0 and 1
+// unroll the plane loop by the stage count (compile-time stage indices).
+// Each instantiation takes only its own items from its own counter.
+template <typename T, int WY, int MODE>
 __global__ void __launch_bounds__ (32 * WY, 1)
     sweep3d_kernel (const __grid_constant__ SweepMaps maps, const __grid_constant__ FusedParams p,
                     const SweepWork wk, int *err)
@@ -307,7 +376,7 @@ __global__ void __launch_bounds__ (32 * WY, 1)
   using L = Smem<T, WY>;
   constexpr int HZ = L::HZ, HW = L::HW, EW = L::EW, AN = L::AN, XW = L::XW;
   constexpr int HS = L::H_B / sizeof (T), ES = L::E_B / sizeof (T), PS = L::P_B / sizeof (float);
-  constexpr unsigned FULL = 0xffffffffu;
+  constexpr unsigned kLanes = 0xffffffffu;   // shuffle mask: the whole warp
   extern __shared__ __align__ (128) unsigned char smem_raw[];
   __shared__ int s_item;
   __shared__ int s_abort[2];   // per plane parity: a copy did not arrive in time
@@ -398,23 +467,24 @@ __global__ void __launch_bounds__ (32 * WY, 1)
   };
 
   unsigned phase = 0;   // bit s: parity of the next completion of stage s
-  unsigned gst = 0;     // stage of the next plane to stream
   bool aborted = false;
   for (;;)
   {
     if (leader)
-      s_item = (int) atomicAdd (wk.ctr, 1ull);
+      s_item = (int) atomicAdd (wk.ctr + 2 * MODE, 1ull);
     __syncthreads ();
     const int item = s_item;
     if (item >= wk.nitems)
       break;
+    if (sweep_item_class (p, wk, WY, item, tfsf_in) != MODE)
+      continue;
     const int zt = item % wk.nzt;
     const int yt = (item / wk.nzt) % wk.nyt;
     const int ch = item / (wk.nzt * wk.nyt);
     const int z0 = zt * TZ;
     const int y0 = 1 + yt * (WY - 1);
-    const int xa = 1 + ch * wk.chunk;
-    const int xb = min (xa + wk.chunk - 1, nx - 2);
+    const int xa = wk.xcut[ch];
+    const int xb = wk.xcut[ch + 1] - 1;
     const int np = xb - xa + 3;   // planes xa - 1 .. xb + 1 (at least 3)
 
     // z-PML columns of the tile (ring column included) and whether one
@@ -441,10 +511,11 @@ __global__ void __launch_bounds__ (32 * WY, 1)
     {
 #pragma unroll
       for (int k = 0; k < NST; ++k)
-        issue ((gst + k) % NST, xa - 1 + k, z0, y0, aux_mode (xa - 1 + k, y0, zpml, nar_ok), az0);
+        issue (k, xa - 1 + k, z0, y0, MODE == 0 ? 0 : (MODE == 1 ? 1 : aux_mode (xa - 1 + k, y0, zpml, nar_ok)),
+               az0);
     }
     // PML coefficient pairs of this item (read after the first plane's barrier)
-    if (p.use_pml)
+    if (MODE != 0 && p.use_pml)
     {
       for (int q = tid; q < 6 * 2 * PW; q += 32 * WY)
       {
@@ -494,353 +565,379 @@ __global__ void __launch_bounds__ (32 * WY, 1)
     const bool ring_lane = lane == 31 && w < WY - 1;
 
     float hp[3][4];           // H_old(x - 1) on the lane's cells
-    float ep[3][4];           // E_new(x - 1) on the lane's cells
+    float ep[3][4] = {};      // E_new(x - 1) on the lane's cells
     float hpr = 0.f;          // lane 31: Hz_old(x - 1) on the z ring cell
     float rxp = 0.f, ryp = 0.f;   // lane 31: Ex_new, Ey_new(x - 1) on the z ring cell
-    unsigned nbuf = 0;        // exchange buffer of this plane (plane index mod 3)
-    unsigned st = gst;
-    for (int i = 0; i < np; ++i)
-    {
+    // yface / zface only matter when the corrections run inside the sweep
+    // One plane: stage st (= plane index mod 3, as every item restarts the
+    // pipeline at stage 0) and exchange buffer st; kFull includes the PML,
+    // in-sweep TF/SF and point-source code, the lean form is straight-line.
+    auto plane = [&] (int i, auto st_c, auto full_c) __attribute__ ((always_inline)) -> bool {
+      const unsigned st = st_c;       // a compile-time constant on the lean path
+      const unsigned nbuf = st;
+      constexpr bool kFull = decltype (full_c)::value;
       const int x = xa - 1 + i;
-      if (!mbar_wait (bar + 8 * st, (phase >> st) & 1u))
-      {
-        s_abort[i & 1] = 1;
-        atomicOr (err, 4);
-      }
-      phase ^= 1u << st;
-      const int amode = aux_mode (x, y0, zpml, nar_ok);
-      const int apitch = amode == 2 ? PW : AN;
-      const int acol = amode == 2 ? zl : zl - az0;      // only read on lanes with PML cells
-      const unsigned char *stg = smem + st * L::STAGE;
-      const T *sH = reinterpret_cast<const T *> (stg);
-      const T *sE = reinterpret_cast<const T *> (stg + L::OFF_E);
-      const float *P0 = reinterpret_cast<const float *> (stg + L::OFF_P);
-      const float *P1 = P0 + PS;
-      const float *A = reinterpret_cast<const float *> (stg + L::OFF_A);
-      float *N = reinterpret_cast<float *> (smem + L::OFF_N + nbuf * 2 * L::P_B);
-
-      float hc[3][4];
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-        Vec<T>::ld4 (sH + c * HS + (w + 1) * HW + HZ + zl, hc[c]);
-      const float hzr = Vec<T>::ld1 (sH + 2 * HS + (w + 1) * HW + HZ + TZ);
-      // PML masks and auxiliaries of H(x - 1) for the H step (the stage is
-      // refilled after the barrier)
-      const int xh = x - 1;
-      unsigned pmh[3] = {0u, 0u, 0u};
-      float ha[3][4];
-      if (amode && i > 1 && own_row && zupd)
-      {
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
+        if (!mbar_wait (bar + 8 * st, (phase >> st) & 1u))
         {
-          const int k = 3 + c;
-          const bool xy = xh >= p.ilo[k][0] && xh < p.ihi[k][0] && ((yin >> k) & 1u);
-          pmh[c] = zupd & ~((xy ? zin : 0u) >> (4 * k)) & 15u;
-          if (pmh[c])
-            lds4f (A + (3 + c) * PS + w * apitch + acol, ha[c]);
+          s_abort[i & 1] = 1;
+          atomicOr (err, 4);
         }
-      }
-      float en[3][4];           // E_new(x)
-      float rx = 0.f, ry = 0.f; // lane 31: E_new(x) on the z ring cell
+        phase ^= 1u << st;
+        const int amode = kFull ? aux_mode (x, y0, zpml, nar_ok) : (MODE == 1 ? 1 : 0);
+        const int apitch = amode == 2 ? PW : AN;
+        const int acol = amode == 2 ? zl : zl - az0;      // only read on lanes with PML cells
+        const unsigned char *stg = smem + st * L::STAGE;
+        const T *sH = reinterpret_cast<const T *> (stg);
+        const T *sE = reinterpret_cast<const T *> (stg + L::OFF_E);
+        const float *P0 = reinterpret_cast<const float *> (stg + L::OFF_P);
+        const float *P1 = P0 + PS;
+        const float *A = reinterpret_cast<const float *> (stg + L::OFF_A);
+        float *N = reinterpret_cast<float *> (smem + L::OFF_N + nbuf * 2 * L::P_B);
 
-      if (i > 0)
-      {
-        // ================= E_new(x) on every row of the CTA (ring row included)
-        const bool rowupd = x <= nx - 2 && yupd;
-        const unsigned upd = rowupd ? zupd : 0u;
-        float hzm[4], hxym[4], eo[3][4];
-        Vec<T>::ld4 (sH + 2 * HS + w * HW + HZ + zl, hzm);
-        Vec<T>::ld4 (sH + 0 * HS + w * HW + HZ + zl, hxym);
-        const float hym1 = Vec<T>::ld1 (sH + 1 * HS + (w + 1) * HW + HZ + zl - 1);
-        const float hxm1 = Vec<T>::ld1 (sH + 0 * HS + (w + 1) * HW + HZ + zl - 1);
+        float hc[3][4];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-          Vec<T>::ld4 (sE + c * ES + w * EW + zl, eo[c]);
-        float ix[4], iy[4], iz[4];
-        if (has_eps)
+          Vec<T>::ld4 (sH + c * HS + (w + 1) * HW + HZ + zl, hc[c]);
+        const float hzr = Vec<T>::ld1 (sH + 2 * HS + (w + 1) * HW + HZ + TZ);
+        // PML masks and auxiliaries of H(x - 1) for the H step (the stage is
+        // refilled after the barrier)
+        const int xh = x - 1;
+        unsigned pmh[3] = {0u, 0u, 0u};
+        float ha[3][4];
+        if (amode && i > 1 && own_row && zupd)
         {
-          float e0[4], ex1[4], ey1[4];
-          lds4f (P0 + w * PW + zl, e0);
-          lds4f (P1 + w * PW + zl, ex1);
-          lds4f (P0 + min (w + 1, WY - 1) * PW + zl, ey1);
-          const float ez1 = P0[w * PW + zl + 4];
 #pragma unroll
-          for (int j = 0; j < 4; ++j)
+          for (int c = 0; c < 3; ++c)
           {
-            ix[j] = __fdividef (2.f, e0[j] + ex1[j]);
-            iy[j] = __fdividef (2.f, e0[j] + ey1[j]);
-            iz[j] = __fdividef (2.f, e0[j] + (j < 3 ? e0[j + 1] : ez1));
+            const int k = 3 + c;
+            const bool xy = xh >= p.ilo[k][0] && xh < p.ihi[k][0] && ((yin >> k) & 1u);
+            pmh[c] = zupd & ~((xy ? zin : 0u) >> (4 * k)) & 15u;
+            if (pmh[c])
+              lds4f (A + (3 + c) * PS + w * apitch + acol, ha[c]);
           }
         }
-        else
+        float en[3][4];           // E_new(x)
+        float rx = 0.f, ry = 0.f; // lane 31: E_new(x) on the z ring cell
+
+        if (i > 0)
         {
+          // ================= E_new(x) on every row of the CTA (ring row included)
+          const bool rowupd = x <= nx - 2 && yupd;
+          const unsigned upd = rowupd ? zupd : 0u;
+          const size_t id = (size_t) x * sx + rowoff;
+          // PML cells of Ex..Ez on this lane and their auxiliaries (issued
+          // first so that global reads overlap the curl arithmetic)
+          unsigned pm[3] = {0u, 0u, 0u};
+          float xo[3][4];
+          if (amode && upd)
+          {
 #pragma unroll
-          for (int j = 0; j < 4; ++j)
-            ix[j] = iy[j] = iz[j] = 1.f;
-        }
-        float cx[4], cy[4], cz[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-        {
-          const float hyl = j ? hc[1][j - 1] : hym1;
-          const float hxl = j ? hc[0][j - 1] : hxm1;
-          cx[j] = (hc[2][j] - hzm[j]) - (hc[1][j] - hyl);
-          cy[j] = (hc[0][j] - hxl) - (hc[2][j] - hp[2][j]);
-          cz[j] = (hc[1][j] - hp[1][j]) - (hc[0][j] - hxym[j]);
-        }
-        const size_t id = (size_t) x * sx + rowoff;
-        const bool xface = tfsf_in && on_face (p.face[0], x);
-        const unsigned fm = (xface || yface) ? upd : (zface & upd);
-        if (fm)
-        {
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if ((fm >> j) & 1u)
+            for (int k = 0; k < 3; ++k)
             {
-              cx[j] += tfsf_curl (p, 0, p.inc_h, err, x, y, zc + j);
-              cy[j] += tfsf_curl (p, 1, p.inc_h, err, x, y, zc + j);
-              cz[j] += tfsf_curl (p, 2, p.inc_h, err, x, y, zc + j);
+              const bool xy = x >= p.ilo[k][0] && x < p.ihi[k][0] && ((yin >> k) & 1u);
+              pm[k] = upd & ~((xy ? zin : 0u) >> (4 * k)) & 15u;
+              if (pm[k])
+                lds4f (A + k * PS + w * apitch + acol, xo[k]);
             }
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-        {
-          const bool u = (upd >> j) & 1u;
-          en[0][j] = u ? eo[0][j] + (S * ix[j]) * cx[j] : eo[0][j];
-          en[1][j] = u ? eo[1][j] + (S * iy[j]) * cy[j] : eo[1][j];
-          en[2][j] = u ? eo[2][j] + (S * iz[j]) * cz[j] : eo[2][j];
-        }
-        const bool store_e = own_row && x <= xb && lane_ok;
-        if (amode && upd)
-        {
-          unsigned pm[3];
-#pragma unroll
-          for (int k = 0; k < 3; ++k)
-          {
-            const bool xy = x >= p.ilo[k][0] && x < p.ihi[k][0] && ((yin >> k) & 1u);
-            pm[k] = upd & ~((xy ? zin : 0u) >> (4 * k)) & 15u;
           }
+          float hzm[4], hxym[4], eo[3][4];
+          Vec<T>::ld4 (sH + 2 * HS + w * HW + HZ + zl, hzm);
+          Vec<T>::ld4 (sH + 0 * HS + w * HW + HZ + zl, hxym);
+          const float hym1 = Vec<T>::ld1 (sH + 1 * HS + (w + 1) * HW + HZ + zl - 1);
+          const float hxm1 = Vec<T>::ld1 (sH + 0 * HS + (w + 1) * HW + HZ + zl - 1);
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            Vec<T>::ld4 (sE + c * ES + w * EW + zl, eo[c]);
+          float ix[4], iy[4], iz[4];
+          if (has_eps)
+          {
+            float e0[4], ex1[4], ey1[4];
+            lds4f (P0 + w * PW + zl, e0);
+            lds4f (P1 + w * PW + zl, ex1);
+            lds4f (P0 + min (w + 1, WY - 1) * PW + zl, ey1);
+            const float ez1 = P0[w * PW + zl + 4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+              ix[j] = __fdividef (2.f, e0[j] + ex1[j]);
+              iy[j] = __fdividef (2.f, e0[j] + ey1[j]);
+              iz[j] = __fdividef (2.f, e0[j] + (j < 3 ? e0[j + 1] : ez1));
+            }
+          }
+          else
+          {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              ix[j] = iy[j] = iz[j] = 1.f;
+          }
+          float cx[4], cy[4], cz[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+          {
+            const float hyl = j ? hc[1][j - 1] : hym1;
+            const float hxl = j ? hc[0][j - 1] : hxm1;
+            cx[j] = (hc[2][j] - hzm[j]) - (hc[1][j] - hyl);
+            cy[j] = (hc[0][j] - hxl) - (hc[2][j] - hp[2][j]);
+            cz[j] = (hc[1][j] - hp[1][j]) - (hc[0][j] - hxym[j]);
+          }
+          const bool xface = kFull && tfsf_in && on_face (p.face[0], x);
+          const unsigned fm = (xface || yface) ? upd : (zface & upd);
+          if (fm)
+          {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              if ((fm >> j) & 1u)
+              {
+                cx[j] += tfsf_curl_cold (&p, 0, p.inc_h, err, x, y, zc + j);
+                cy[j] += tfsf_curl_cold (&p, 1, p.inc_h, err, x, y, zc + j);
+                cz[j] += tfsf_curl_cold (&p, 2, p.inc_h, err, x, y, zc + j);
+              }
+          }
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+          {
+            const bool u = (upd >> j) & 1u;
+            en[0][j] = u ? eo[0][j] + (S * ix[j]) * cx[j] : eo[0][j];
+            en[1][j] = u ? eo[1][j] + (S * iy[j]) * cy[j] : eo[1][j];
+            en[2][j] = u ? eo[2][j] + (S * iz[j]) * cz[j] : eo[2][j];
+          }
+          const bool store_e = own_row && x <= xb && lane_ok;
           if (pm[0])
           {
-            float xo[4], xn[4];
-            lds4f (A + 0 * PS + w * apitch + acol, xo);
-            pml_vec<0, WY> (tabs, w, i, zl, pm[0], xo, cx, ix, eo[0], en[0], xn);
+            float xn[4];
+            pml_vec<0, WY> (tabs, w, i, zl, pm[0], xo[0], cx, ix, eo[0], en[0], xn);
             if (store_e)
               Vec<float>::st4 (p.aux_new[0] + id, xn);
           }
           if (pm[1])
           {
-            float xo[4], xn[4];
-            lds4f (A + 1 * PS + w * apitch + acol, xo);
-            pml_vec<1, WY> (tabs, w, i, zl, pm[1], xo, cy, iy, eo[1], en[1], xn);
+            float xn[4];
+            pml_vec<1, WY> (tabs, w, i, zl, pm[1], xo[1], cy, iy, eo[1], en[1], xn);
             if (store_e)
               Vec<float>::st4 (p.aux_new[1] + id, xn);
           }
           if (pm[2])
           {
-            float xo[4], xn[4];
-            lds4f (A + 2 * PS + w * apitch + acol, xo);
-            pml_vec<2, WY> (tabs, w, i, zl, pm[2], xo, cz, iz, eo[2], en[2], xn);
+            float xn[4];
+            pml_vec<2, WY> (tabs, w, i, zl, pm[2], xo[2], cz, iz, eo[2], en[2], xn);
             if (store_e)
               Vec<float>::st4 (p.aux_new[2] + id, xn);
           }
-        }
-        if ((p.ps_mask & 7) && rowupd && x == p.ps[0] && y == p.ps[1] && p.ps[2] >= zc && p.ps[2] < zc + 4)
-        {
-          const float v = (float) p.src[p.src_index];
-          const int j = p.ps[2] - zc;
-#pragma unroll
-          for (int c = 0; c < 3; ++c)
-            if (p.ps_mask & (1 << c))
-            {
-#pragma unroll
-              for (int jj = 0; jj < 4; ++jj)
-                if (jj == j)
-                  en[c][jj] = v;
-            }
-        }
-        if (store_e)
-        {
-#pragma unroll
-          for (int c = 0; c < 3; ++c)
-            Vec<T>::st4 (reinterpret_cast<T *> (p.e_new[c]) + id, en[c]);
-        }
-        // Ex and Ez rows for the H step of the warp below (its y + 1 neighbours)
-        sts4f (N + 0 * PS + w * PW + zl, en[0]);
-        sts4f (N + 1 * PS + w * PW + zl, en[2]);
-
-        // z ring: Ex and Ey at z0 + 128 for H of lane 31's last cell
-        if (ring_lane && zr <= nz - 1)
-        {
-          rx = Vec<T>::ld1 (sE + 0 * ES + w * EW + TZ);
-          ry = Vec<T>::ld1 (sE + 1 * ES + w * EW + TZ);
-          if (rowupd && zr <= nz - 2)
+          if (kFull && (p.ps_mask & 7) && rowupd && x == p.ps[0] && y == p.ps[1] && p.ps[2] >= zc && p.ps[2] < zc + 4)
           {
-            const float hz = hzr;
-            const float hzym = Vec<T>::ld1 (sH + 2 * HS + w * HW + HZ + TZ);
-            const float hy = Vec<T>::ld1 (sH + 1 * HS + (w + 1) * HW + HZ + TZ);
-            const float hx = Vec<T>::ld1 (sH + 0 * HS + (w + 1) * HW + HZ + TZ);
-            float crx = (hz - hzym) - (hy - hc[1][3]);
-            float cry = (hx - hc[0][3]) - (hz - hpr);
-            float irx = 1.f, iry = 1.f;
-            if (has_eps)
+            const float v = (float) p.src[p.src_index];
+            const int j = p.ps[2] - zc;
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+              if (p.ps_mask & (1 << c))
+              {
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj)
+                  if (jj == j)
+                    en[c][jj] = v;
+              }
+          }
+          if (store_e)
+          {
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+              Vec<T>::st4 (reinterpret_cast<T *> (p.e_new[c]) + id, en[c]);
+          }
+          // Ex and Ez rows for the H step of the warp below (its y + 1 neighbours)
+          sts4f (N + 0 * PS + w * PW + zl, en[0]);
+          sts4f (N + 1 * PS + w * PW + zl, en[2]);
+
+          // z ring: Ex and Ey at z0 + 128 for H of lane 31's last cell
+          if (ring_lane && zr <= nz - 1)
+          {
+            rx = Vec<T>::ld1 (sE + 0 * ES + w * EW + TZ);
+            ry = Vec<T>::ld1 (sE + 1 * ES + w * EW + TZ);
+            if (rowupd && zr <= nz - 2)
             {
-              const float e0 = P0[w * PW + TZ];
-              irx = __fdividef (2.f, e0 + P1[w * PW + TZ]);
-              iry = __fdividef (2.f, e0 + P0[(w + 1) * PW + TZ]);
-            }
-            if (tfsf_in && (xface || yface || on_face (p.face[2], zr)))
-            {
-              crx += tfsf_curl (p, 0, p.inc_h, err, x, y, zr);
-              cry += tfsf_curl (p, 1, p.inc_h, err, x, y, zr);
-            }
-            const bool in0 = x >= p.ilo[0][0] && x < p.ihi[0][0] && (yin & 1u) && zr >= p.ilo[0][2] &&
-                             zr < p.ihi[0][2];
-            const bool in1 = x >= p.ilo[1][0] && x < p.ihi[1][0] && (yin & 2u) && zr >= p.ilo[1][2] &&
-                             zr < p.ihi[1][2];
-            const int rcol = amode == 2 ? TZ : TZ - az0;
-            if (amode && !in0)
-              rx = pml_one<0, WY> (tabs, w, i, TZ, A[0 * PS + w * apitch + rcol], crx, irx, rx);
-            else
-              rx = rx + (S * irx) * crx;
-            if (amode && !in1)
-              ry = pml_one<1, WY> (tabs, w, i, TZ, A[1 * PS + w * apitch + rcol], cry, iry, ry);
-            else
-              ry = ry + (S * iry) * cry;
-            if ((p.ps_mask & 3) && x == p.ps[0] && y == p.ps[1] && zr == p.ps[2])
-            {
-              const float v = (float) p.src[p.src_index];
-              if (p.ps_mask & 1)
-                rx = v;
-              if (p.ps_mask & 2)
-                ry = v;
+              const float hz = hzr;
+              const float hzym = Vec<T>::ld1 (sH + 2 * HS + w * HW + HZ + TZ);
+              const float hy = Vec<T>::ld1 (sH + 1 * HS + (w + 1) * HW + HZ + TZ);
+              const float hx = Vec<T>::ld1 (sH + 0 * HS + (w + 1) * HW + HZ + TZ);
+              float crx = (hz - hzym) - (hy - hc[1][3]);
+              float cry = (hx - hc[0][3]) - (hz - hpr);
+              float irx = 1.f, iry = 1.f;
+              if (has_eps)
+              {
+                const float e0 = P0[w * PW + TZ];
+                irx = __fdividef (2.f, e0 + P1[w * PW + TZ]);
+                iry = __fdividef (2.f, e0 + P0[(w + 1) * PW + TZ]);
+              }
+              if (kFull && tfsf_in && (xface || yface || on_face (p.face[2], zr)))
+              {
+                crx += tfsf_curl_cold (&p, 0, p.inc_h, err, x, y, zr);
+                cry += tfsf_curl_cold (&p, 1, p.inc_h, err, x, y, zr);
+              }
+              const bool in0 = x >= p.ilo[0][0] && x < p.ihi[0][0] && (yin & 1u) && zr >= p.ilo[0][2] &&
+                               zr < p.ihi[0][2];
+              const bool in1 = x >= p.ilo[1][0] && x < p.ihi[1][0] && (yin & 2u) && zr >= p.ilo[1][2] &&
+                               zr < p.ihi[1][2];
+              const int rcol = amode == 2 ? TZ : TZ - az0;
+              if (amode && !in0)
+                rx = pml_one<0, WY> (tabs, w, i, TZ, A[0 * PS + w * apitch + rcol], crx, irx, rx);
+              else
+                rx = rx + (S * irx) * crx;
+              if (amode && !in1)
+                ry = pml_one<1, WY> (tabs, w, i, TZ, A[1 * PS + w * apitch + rcol], cry, iry, ry);
+              else
+                ry = ry + (S * iry) * cry;
+              if (kFull && (p.ps_mask & 3) && x == p.ps[0] && y == p.ps[1] && zr == p.ps[2])
+              {
+                const float v = (float) p.src[p.src_index];
+                if (p.ps_mask & 1)
+                  rx = v;
+                if (p.ps_mask & 2)
+                  ry = v;
+              }
             }
           }
         }
-      }
 
-      __syncthreads ();
-      if (s_abort[i & 1])
-      {
-        // wait (bounded) for the copies still in flight into the other stages
-        aborted = true;
-        if (leader)
-          for (int k = 1; k < NST && i + k < np; ++k)
+        __syncthreads ();
+        if (s_abort[i & 1])
+        {
+          // wait (bounded) for the copies still in flight into the other stages
+          aborted = true;
+          if (leader)
+            for (int k = 1; k < NST && i + k < np; ++k)
+            {
+              const unsigned so = (st + k) % NST;
+              mbar_wait (bar + 8 * so, (phase >> so) & 1u);
+            }
+          return false;
+        }
+        if (leader && i + NST < np)
+          issue (st, x + NST, z0, y0, MODE == 0 ? 0 : (MODE == 1 ? 1 : aux_mode (x + NST, y0, zpml, nar_ok)), az0);
+
+        if (i > 1 && own_row)
+        {
+          // ================= H_new(x - 1) on the owned rows
+          const size_t idh = (size_t) xh * sx + rowoff;
+          const float *Np =
+              reinterpret_cast<const float *> (smem + L::OFF_N + (nbuf == 0 ? 2u : nbuf - 1u) * 2 * L::P_B);
+          float exy[4], ezy[4];
+          lds4f (Np + 0 * PS + (w + 1) * PW + zl, exy);
+          lds4f (Np + 1 * PS + (w + 1) * PW + zl, ezy);
+          float exz = __shfl_down_sync (kLanes, ep[0][0], 1);
+          float eyz = __shfl_down_sync (kLanes, ep[1][0], 1);
+          if (lane == 31)
           {
-            const unsigned so = (st + k) % NST;
-            mbar_wait (bar + 8 * so, (phase >> so) & 1u);
+            exz = rxp;
+            eyz = ryp;
           }
-        break;
-      }
-      if (leader && i + NST < np)
-        issue (st, x + NST, z0, y0, aux_mode (x + NST, y0, zpml, nar_ok), az0);
-
-      if (i > 1 && own_row)
-      {
-        // ================= H_new(x - 1) on the owned rows
-        const float *Np =
-            reinterpret_cast<const float *> (smem + L::OFF_N + (nbuf == 0 ? 2u : nbuf - 1u) * 2 * L::P_B);
-        float exy[4], ezy[4];
-        lds4f (Np + 0 * PS + (w + 1) * PW + zl, exy);
-        lds4f (Np + 1 * PS + (w + 1) * PW + zl, ezy);
-        float exz = __shfl_down_sync (FULL, ep[0][0], 1);
-        float eyz = __shfl_down_sync (FULL, ep[1][0], 1);
-        if (lane == 31)
-        {
-          exz = rxp;
-          eyz = ryp;
-        }
-        float ax[4], ay[4], az[4], hn[3][4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-        {
-          const float eyn = j < 3 ? ep[1][j + 1] : eyz;
-          const float exn = j < 3 ? ep[0][j + 1] : exz;
-          ax[j] = (eyn - ep[1][j]) - (ezy[j] - ep[2][j]);
-          ay[j] = (en[2][j] - ep[2][j]) - (exn - ep[0][j]);
-          az[j] = (exy[j] - ep[0][j]) - (en[1][j] - ep[1][j]);
-        }
-        const size_t idh = (size_t) xh * sx + rowoff;
-        const bool xface = tfsf_in && on_face (p.face[0], xh);
-        const unsigned fm = (xface || yface) ? zupd : (zface & zupd);
-        if (fm)
-        {
+          float ax[4], ay[4], az[4], hn[3][4];
 #pragma unroll
           for (int j = 0; j < 4; ++j)
-            if ((fm >> j) & 1u)
-            {
-              ax[j] += tfsf_curl (p, 3, p.inc_e, err, xh, y, zc + j);
-              ay[j] += tfsf_curl (p, 4, p.inc_e, err, xh, y, zc + j);
-              az[j] += tfsf_curl (p, 5, p.inc_e, err, xh, y, zc + j);
-            }
-        }
+          {
+            const float eyn = j < 3 ? ep[1][j + 1] : eyz;
+            const float exn = j < 3 ? ep[0][j + 1] : exz;
+            ax[j] = (eyn - ep[1][j]) - (ezy[j] - ep[2][j]);
+            ay[j] = (en[2][j] - ep[2][j]) - (exn - ep[0][j]);
+            az[j] = (exy[j] - ep[0][j]) - (en[1][j] - ep[1][j]);
+          }
+          const bool xface = kFull && tfsf_in && on_face (p.face[0], xh);
+          const unsigned fm = (xface || yface) ? zupd : (zface & zupd);
+          if (fm)
+          {
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-        {
-          const bool u = (zupd >> j) & 1u;
-          hn[0][j] = u ? hp[0][j] + S * ax[j] : hp[0][j];
-          hn[1][j] = u ? hp[1][j] + S * ay[j] : hp[1][j];
-          hn[2][j] = u ? hp[2][j] + S * az[j] : hp[2][j];
-        }
-        if (pmh[0])
-        {
-          float xn[4];
-          pml_vec<3, WY> (tabs, w, i - 1, zl, pmh[0], ha[0], ax, one4, hp[0], hn[0], xn);
+            for (int j = 0; j < 4; ++j)
+              if ((fm >> j) & 1u)
+              {
+                ax[j] += tfsf_curl_cold (&p, 3, p.inc_e, err, xh, y, zc + j);
+                ay[j] += tfsf_curl_cold (&p, 4, p.inc_e, err, xh, y, zc + j);
+                az[j] += tfsf_curl_cold (&p, 5, p.inc_e, err, xh, y, zc + j);
+              }
+          }
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+          {
+            const bool u = (zupd >> j) & 1u;
+            hn[0][j] = u ? hp[0][j] + S * ax[j] : hp[0][j];
+            hn[1][j] = u ? hp[1][j] + S * ay[j] : hp[1][j];
+            hn[2][j] = u ? hp[2][j] + S * az[j] : hp[2][j];
+          }
+          if (pmh[0])
+          {
+            float xn[4];
+            pml_vec<3, WY> (tabs, w, i - 1, zl, pmh[0], ha[0], ax, one4, hp[0], hn[0], xn);
+            if (lane_ok)
+              Vec<float>::st4 (p.aux_new[3] + idh, xn);
+          }
+          if (pmh[1])
+          {
+            float xn[4];
+            pml_vec<4, WY> (tabs, w, i - 1, zl, pmh[1], ha[1], ay, one4, hp[1], hn[1], xn);
+            if (lane_ok)
+              Vec<float>::st4 (p.aux_new[4] + idh, xn);
+          }
+          if (pmh[2])
+          {
+            float xn[4];
+            pml_vec<5, WY> (tabs, w, i - 1, zl, pmh[2], ha[2], az, one4, hp[2], hn[2], xn);
+            if (lane_ok)
+              Vec<float>::st4 (p.aux_new[5] + idh, xn);
+          }
+          if (kFull && (p.ps_mask & 56) && xh == p.ps[0] && y == p.ps[1] && p.ps[2] >= zc && p.ps[2] < zc + 4)
+          {
+            const float v = (float) p.src[p.src_index + 1] * p.ps_scale_h;
+            const int j = p.ps[2] - zc;
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+              if (p.ps_mask & (8 << c))
+              {
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj)
+                  if (jj == j)
+                    hn[c][jj] = v;
+              }
+          }
           if (lane_ok)
-            Vec<float>::st4 (p.aux_new[3] + idh, xn);
-        }
-        if (pmh[1])
-        {
-          float xn[4];
-          pml_vec<4, WY> (tabs, w, i - 1, zl, pmh[1], ha[1], ay, one4, hp[1], hn[1], xn);
-          if (lane_ok)
-            Vec<float>::st4 (p.aux_new[4] + idh, xn);
-        }
-        if (pmh[2])
-        {
-          float xn[4];
-          pml_vec<5, WY> (tabs, w, i - 1, zl, pmh[2], ha[2], az, one4, hp[2], hn[2], xn);
-          if (lane_ok)
-            Vec<float>::st4 (p.aux_new[5] + idh, xn);
-        }
-        if ((p.ps_mask & 56) && xh == p.ps[0] && y == p.ps[1] && p.ps[2] >= zc && p.ps[2] < zc + 4)
-        {
-          const float v = (float) p.src[p.src_index + 1] * p.ps_scale_h;
-          const int j = p.ps[2] - zc;
+          {
 #pragma unroll
-          for (int c = 0; c < 3; ++c)
-            if (p.ps_mask & (8 << c))
-            {
-#pragma unroll
-              for (int jj = 0; jj < 4; ++jj)
-                if (jj == j)
-                  hn[c][jj] = v;
-            }
+            for (int c = 0; c < 3; ++c)
+              Vec<T>::st4 (reinterpret_cast<T *> (p.h_new[c]) + idh, hn[c]);
+          }
         }
-        if (lane_ok)
-        {
-#pragma unroll
-          for (int c = 0; c < 3; ++c)
-            Vec<T>::st4 (reinterpret_cast<T *> (p.h_new[c]) + idh, hn[c]);
-        }
-      }
 
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
+        for (int c = 0; c < 3; ++c)
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-        {
-          hp[c][j] = hc[c][j];
-          ep[c][j] = en[c][j];
-        }
-      hpr = hzr;
-      rxp = rx;
-      ryp = ry;
-      nbuf = nbuf == 2u ? 0u : nbuf + 1u;
-      st = st == NST - 1 ? 0u : st + 1u;
+          for (int j = 0; j < 4; ++j)
+          {
+            hp[c][j] = hc[c][j];
+            ep[c][j] = en[c][j];
+          }
+        hpr = hzr;
+        rxp = rx;
+        ryp = ry;
+        return true;
+    };
+    if (MODE != 2)
+    {
+      // stage and exchange buffer as compile-time constants
+      using S0 = std::integral_constant<unsigned, 0>;
+      using S1 = std::integral_constant<unsigned, 1>;
+      using S2 = std::integral_constant<unsigned, 2>;
+      for (int i = 0; i < np; i += 3)
+      {
+        if (!plane (i, S0{}, std::false_type{}))
+          break;
+        if (i + 1 < np && !plane (i + 1, S1{}, std::false_type{}))
+          break;
+        if (i + 2 < np && !plane (i + 2, S2{}, std::false_type{}))
+          break;
+      }
     }
-    gst = (gst + (unsigned) np) % NST;
+    else
+    {
+      for (int i = 0; i < np; ++i)
+        if (!plane (i, (unsigned) (i % 3), std::true_type{}))
+          break;
+    }
     if (aborted)
       break;
   }
@@ -848,11 +945,11 @@ __global__ void __launch_bounds__ (32 * WY, 1)
   if (leader)
   {
     __threadfence ();
-    const unsigned long long done = atomicAdd (wk.ctr + 1, 1ull);
+    const unsigned long long done = atomicAdd (wk.ctr + 2 * MODE + 1, 1ull);
     if (done == gridDim.x - 1)
     {
-      atomicExch (wk.ctr, 0ull);
-      atomicExch (wk.ctr + 1, 0ull);
+      atomicExch (wk.ctr + 2 * MODE, 0ull);
+      atomicExch (wk.ctr + 2 * MODE + 1, 0ull);
     }
   }
 }
@@ -1006,17 +1103,22 @@ std::string plan_t (SweepPlan &pl, const FusedParams &p, void *const e[2][3], vo
         m.aux[k] = m.auxn[k] = m.e[0];
     }
   }
-  auto kern = sweep3d_kernel<T, WY>;
-  if (cudaFuncSetAttribute (kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) L::TOTAL) != cudaSuccess)
-  {
-    cudaGetLastError ();
-    return "shared memory request refused";
-  }
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor (&per_sm, kern, 32 * WY, L::TOTAL) != cudaSuccess || per_sm < 1)
+  for (int mode = 0; mode < 3; ++mode)
   {
-    cudaGetLastError ();
-    return "kernel does not fit on an SM";
+    auto kern = mode == 0 ? sweep3d_kernel<T, WY, 0> : (mode == 1 ? sweep3d_kernel<T, WY, 1> : sweep3d_kernel<T, WY, 2>);
+    if (cudaFuncSetAttribute (kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) L::TOTAL) != cudaSuccess)
+    {
+      cudaGetLastError ();
+      return "shared memory request refused";
+    }
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor (&n, kern, 32 * WY, L::TOTAL) != cudaSuccess || n < 1)
+    {
+      cudaGetLastError ();
+      return "kernel does not fit on an SM";
+    }
+    per_sm = mode ? std::min (per_sm, n) : n;
   }
   pl.smem = L::TOTAL;
   pl.ctas = sm_count * per_sm;
@@ -1024,25 +1126,73 @@ std::string plan_t (SweepPlan &pl, const FusedParams &p, void *const e[2][3], vo
 }
 
 template <typename T, int WY>
-void launch_t (const SweepPlan &pl, int set, const FusedParams &p, int *err, cudaStream_t s)
+int launch_t (const SweepPlan &pl, int set, const FusedParams &p, int *err, cudaStream_t s)
 {
-  sweep3d_kernel<T, WY><<<pl.ctas, dim3 (32, WY), Smem<T, WY>::TOTAL, s>>> (pl.maps[set], p, pl.work, err);
+  // heaviest class first, so that the lighter items fill in behind it
+  constexpr unsigned sm = Smem<T, WY>::TOTAL;
+  int n = 0;
+  if (pl.items[2] > 0)
+  {
+    sweep3d_kernel<T, WY, 2><<<pl.ctas, dim3 (32, WY), sm, s>>> (pl.maps[set], p, pl.work, err);
+    ++n;
+  }
+  if (pl.items[1] > 0)
+  {
+    sweep3d_kernel<T, WY, 1><<<pl.ctas, dim3 (32, WY), sm, s>>> (pl.maps[set], p, pl.work, err);
+    ++n;
+  }
+  if (pl.items[0] > 0)
+  {
+    sweep3d_kernel<T, WY, 0><<<pl.ctas, dim3 (32, WY), sm, s>>> (pl.maps[set], p, pl.work, err);
+    ++n;
+  }
+  return n;
 }
 
 }  // namespace
 
-void sweep3d_items (const int n[3], int wy, int chunk, SweepWork &w)
+void sweep3d_items (const FusedParams &p, int wy, int chunk, SweepWork &w)
 {
+  const int *n = p.g.n;
   w.nzt = (n[2] - 1 + TZ - 1) / TZ;
   w.nyt = (n[1] - 2 + wy - 2) / (wy - 1);
+  if (p.use_pml && chunk > MAXC)
+    chunk = MAXC;   // the item's x coefficient table holds MAXC + 2 planes
+  chunk = std::max (chunk, (n[0] - 2 + kMaxChunks - 1) / kMaxChunks);
   w.chunk = chunk;
-  w.nch = (n[0] - 2 + chunk - 1) / chunk;
+  // x segments: the planes where every component is PML-free (E on
+  // x .. x + 1, H on x) form the middle segment, so that no item mixes PML
+  // and interior planes; each segment is split into near-equal chunks
+  int lo = 1, hi = n[0] - 2;   // interior segment [lo, hi]
+  if (p.use_pml)
+  {
+    for (int k = 0; k < 6; ++k)
+    {
+      lo = std::max (lo, p.ilo[k][0]);
+      hi = std::min (hi, k < 3 ? p.ihi[k][0] - 2 : p.ihi[k][0] - 1);
+    }
+  }
+  std::vector<int> seg = {1};
+  if (lo > 1 && lo <= hi)
+    seg.push_back (lo);
+  if (hi + 1 <= n[0] - 2 && lo <= hi)
+    seg.push_back (hi + 1);
+  seg.push_back (n[0] - 1);
+  w.nch = 0;
+  w.xcut[0] = 1;
+  for (size_t sg = 0; sg + 1 < seg.size (); ++sg)
+  {
+    const int len = seg[sg + 1] - seg[sg];
+    const int m = (len + chunk - 1) / chunk;
+    for (int j = 1; j <= m; ++j)
+      w.xcut[++w.nch] = seg[sg] + (int) ((long long) len * j / m);
+  }
   w.nitems = w.nzt * w.nyt * w.nch;
 }
 
 std::string sweep3d_plan (SweepPlan &plan, const FusedParams &p, void *const e[2][3], void *const h[2][3],
                           float *const aux[2][6], const float *eps, int sm_count, int wy, int chunk,
-                          unsigned long long *ctr)
+                          unsigned long long *ctr, bool lean)
 {
   const int *n = p.g.n;
   if (p.g.tmz)
@@ -1058,15 +1208,20 @@ std::string sweep3d_plan (SweepPlan &plan, const FusedParams &p, void *const e[2
     return "unsupported CTA height";
   if (chunk < 1)
     return "bad x chunk";
-  if (p.use_pml && chunk > MAXC)
-    chunk = MAXC;   // the item's x coefficient table holds MAXC + 2 planes
   plan.wy = wy;
   std::string why = p.fp16 ? plan_t<__half, 8> (plan, p, e, h, aux, eps, sm_count)
                            : plan_t<float, 8> (plan, p, e, h, aux, eps, sm_count);
   if (!why.empty ())
     return why;
-  sweep3d_items (n, wy, chunk, plan.work);
+  sweep3d_items (p, wy, chunk, plan.work);
+  if (p.use_pml && plan.work.chunk > MAXC)
+    return "grid too long in x for the staged PML coefficients";
   plan.work.ctr = ctr;
+  plan.work.lean = lean ? 1 : 0;
+  const bool tfsf_in = p.use_tfsf && !p.tfsf_post;
+  plan.items[0] = plan.items[1] = plan.items[2] = 0;
+  for (int it = 0; it < plan.work.nitems; ++it)
+    ++plan.items[sweep_item_class (p, plan.work, wy, it, tfsf_in)];
   if (plan.ctas > plan.work.nitems)
     plan.ctas = plan.work.nitems;
   return "";
@@ -1074,11 +1229,7 @@ std::string sweep3d_plan (SweepPlan &plan, const FusedParams &p, void *const e[2
 
 int launch_sweep3d (const SweepPlan &plan, int set, const FusedParams &p, int *err, cudaStream_t s)
 {
-  if (p.fp16)
-    launch_t<__half, 8> (plan, set, p, err, s);
-  else
-    launch_t<float, 8> (plan, set, p, err, s);
-  return 1;
+  return p.fp16 ? launch_t<__half, 8> (plan, set, p, err, s) : launch_t<float, 8> (plan, set, p, err, s);
 }
 
 }  // namespace fdtdb

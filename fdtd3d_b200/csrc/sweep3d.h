@@ -25,10 +25,15 @@ struct SweepMaps
   CUtensorMap auxn[6];         // narrow (32-cell) boxes for planes whose PML cells are all at a z edge
 };
 
+constexpr int kMaxChunks = 256;   // x chunks per step (the chunk grows for larger grids)
+
 struct SweepWork
 {
   int nzt, nyt, nch, nitems, chunk;
-  unsigned long long *ctr;     // [0] next item, [1] CTAs finished; the last CTA resets both
+  int xcut[kMaxChunks + 4];    // chunk c covers planes xcut[c] .. xcut[c + 1] - 1
+  int lean;                    // 0: every item goes to the full class
+  unsigned long long *ctr;     // per item class c: [2c] next item, [2c + 1] CTAs finished; the last
+                               // CTA of a launch resets both
 };
 
 struct SweepPlan
@@ -36,12 +41,14 @@ struct SweepPlan
   int wy = 0;                  // warps per CTA, one y row each (last row = ring)
   int ctas = 0;                // persistent CTAs
   unsigned smem = 0;           // dynamic shared memory per CTA
+  int items[3] = {0, 0, 0};    // items per class: lean, z-edge PML, full
   SweepWork work{};
   SweepMaps maps[2];           // maps[b]: buffer set b as the old set
 };
 
-// Tiles per axis and items for a given CTA height and x chunk.
-void sweep3d_items (const int n[3], int wy, int chunk, SweepWork &w);
+// Tiles per axis, x chunks (cut at the PML edges, at most `chunk` planes
+// each) and items for a given CTA height.
+void sweep3d_items (const FusedParams &p, int wy, int chunk, SweepWork &w);
 
 // Builds the tensor maps and launch shape.  e/h[b][c] are the field buffers
 // of set b, aux[b][k] the PML auxiliaries of set b (null without PML), eps
@@ -49,9 +56,10 @@ void sweep3d_items (const int n[3], int wy, int chunk, SweepWork &w);
 // cannot serve this geometry.
 std::string sweep3d_plan (SweepPlan &plan, const FusedParams &p, void *const e[2][3], void *const h[2][3],
                           float *const aux[2][6], const float *eps, int sm_count, int wy, int chunk,
-                          unsigned long long *ctr);
+                          unsigned long long *ctr, bool lean = true);
 
-// One time step with buffer set `set` as the old set.
+// One time step with buffer set `set` as the old set (one launch per item
+// class that has items; returns how many).
 int launch_sweep3d (const SweepPlan &plan, int set, const FusedParams &p, int *err, cudaStream_t s);
 
 }  // namespace fdtdb
