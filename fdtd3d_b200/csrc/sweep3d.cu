@@ -257,8 +257,11 @@ struct PmlTabs
 // PML update of component K on the cells of mask pm among a lane's four
 // cells: X_new = ca1 X + sq1 curl, F = p5 F + (g4p X_new - g4m X) q5 / m.
 // Branch-free over the cells; cells outside pm keep fn and their X.
-template <int K, int WY>
-__device__ __forceinline__ void pml_vec (const PmlTabs &t, int row, int plane, int col, unsigned pm,
+// ZONLY: the cell is interior along x and y, where every pair is the
+// sigma = 0 identity (ca1 = 1, sq1 = S, p5 = q5 = g4p = g4m = 1; exact in
+// FP32), so only the z pair is read.
+template <int K, int WY, bool ZONLY = false>
+__device__ __forceinline__ void pml_vec (const PmlTabs &t, float S, int row, int plane, int col, unsigned pm,
                                          const float xo[4], const float cu[4], const float im[4], const float fo[4],
                                          float fn[4], float xn[4])
 {
@@ -269,8 +272,8 @@ __device__ __forceinline__ void pml_vec (const PmlTabs &t, int row, int plane, i
   for (int e = 0; e < 2; ++e)
   {
     lds4f (t.z + (2 * K + e) * PW + col, c[pz][e]);
-    const float vy = t.y[(2 * K + e) * WY + row];
-    const float vx = t.x[(2 * K + e) * XW + plane];
+    const float vy = ZONLY ? (py == 0 && e == 1 ? S : 1.f) : t.y[(2 * K + e) * WY + row];
+    const float vx = ZONLY ? (px == 0 && e == 1 ? S : 1.f) : t.x[(2 * K + e) * XW + plane];
 #pragma unroll
     for (int j = 0; j < 4; ++j)
     {
@@ -290,8 +293,8 @@ __device__ __forceinline__ void pml_vec (const PmlTabs &t, int row, int plane, i
 }
 
 // The same for one cell (the z ring cell, column 128 of the tile).
-template <int K, int WY>
-__device__ __forceinline__ float pml_one (const PmlTabs &t, int row, int plane, int col, float xo, float cu,
+template <int K, int WY, bool ZONLY = false>
+__device__ __forceinline__ float pml_one (const PmlTabs &t, float S, int row, int plane, int col, float xo, float cu,
                                           float im, float fo)
 {
   constexpr int pz = pair_along (K, 2), py = pair_along (K, 1);
@@ -302,7 +305,8 @@ __device__ __forceinline__ float pml_one (const PmlTabs &t, int row, int plane, 
 #pragma unroll
     for (int q = 0; q < 3; ++q)
       c[q][e] = q == pz ? t.z[(2 * K + e) * PW + col]
-                        : (q == py ? t.y[(2 * K + e) * WY + row] : t.x[(2 * K + e) * XW + plane]);
+                        : (ZONLY ? (q == 0 && e == 1 ? S : 1.f)
+                                 : (q == py ? t.y[(2 * K + e) * WY + row] : t.x[(2 * K + e) * XW + plane]));
   const float n = c[0][0] * xo + c[0][1] * cu;
   return c[1][0] * fo + (c[2][0] * n - c[2][1] * xo) * c[1][1] * im;
 }
@@ -705,21 +709,21 @@ __global__ void __launch_bounds__ (32 * WY, 1)
           if (pm[0])
           {
             float xn[4];
-            pml_vec<0, WY> (tabs, w, i, zl, pm[0], xo[0], cx, ix, eo[0], en[0], xn);
+            pml_vec<0, WY, MODE == 1> (tabs, S, w, i, zl, pm[0], xo[0], cx, ix, eo[0], en[0], xn);
             if (store_e)
               Vec<float>::st4 (p.aux_new[0] + id, xn);
           }
           if (pm[1])
           {
             float xn[4];
-            pml_vec<1, WY> (tabs, w, i, zl, pm[1], xo[1], cy, iy, eo[1], en[1], xn);
+            pml_vec<1, WY, MODE == 1> (tabs, S, w, i, zl, pm[1], xo[1], cy, iy, eo[1], en[1], xn);
             if (store_e)
               Vec<float>::st4 (p.aux_new[1] + id, xn);
           }
           if (pm[2])
           {
             float xn[4];
-            pml_vec<2, WY> (tabs, w, i, zl, pm[2], xo[2], cz, iz, eo[2], en[2], xn);
+            pml_vec<2, WY, MODE == 1> (tabs, S, w, i, zl, pm[2], xo[2], cz, iz, eo[2], en[2], xn);
             if (store_e)
               Vec<float>::st4 (p.aux_new[2] + id, xn);
           }
@@ -778,11 +782,11 @@ __global__ void __launch_bounds__ (32 * WY, 1)
                                zr < p.ihi[1][2];
               const int rcol = amode == 2 ? TZ : TZ - az0;
               if (amode && !in0)
-                rx = pml_one<0, WY> (tabs, w, i, TZ, A[0 * PS + w * apitch + rcol], crx, irx, rx);
+                rx = pml_one<0, WY, MODE == 1> (tabs, S, w, i, TZ, A[0 * PS + w * apitch + rcol], crx, irx, rx);
               else
                 rx = rx + (S * irx) * crx;
               if (amode && !in1)
-                ry = pml_one<1, WY> (tabs, w, i, TZ, A[1 * PS + w * apitch + rcol], cry, iry, ry);
+                ry = pml_one<1, WY, MODE == 1> (tabs, S, w, i, TZ, A[1 * PS + w * apitch + rcol], cry, iry, ry);
               else
                 ry = ry + (S * iry) * cry;
               if (kFull && (p.ps_mask & 3) && x == p.ps[0] && y == p.ps[1] && zr == p.ps[2])
@@ -863,21 +867,21 @@ __global__ void __launch_bounds__ (32 * WY, 1)
           if (pmh[0])
           {
             float xn[4];
-            pml_vec<3, WY> (tabs, w, i - 1, zl, pmh[0], ha[0], ax, one4, hp[0], hn[0], xn);
+            pml_vec<3, WY, MODE == 1> (tabs, S, w, i - 1, zl, pmh[0], ha[0], ax, one4, hp[0], hn[0], xn);
             if (lane_ok)
               Vec<float>::st4 (p.aux_new[3] + idh, xn);
           }
           if (pmh[1])
           {
             float xn[4];
-            pml_vec<4, WY> (tabs, w, i - 1, zl, pmh[1], ha[1], ay, one4, hp[1], hn[1], xn);
+            pml_vec<4, WY, MODE == 1> (tabs, S, w, i - 1, zl, pmh[1], ha[1], ay, one4, hp[1], hn[1], xn);
             if (lane_ok)
               Vec<float>::st4 (p.aux_new[4] + idh, xn);
           }
           if (pmh[2])
           {
             float xn[4];
-            pml_vec<5, WY> (tabs, w, i - 1, zl, pmh[2], ha[2], az, one4, hp[2], hn[2], xn);
+            pml_vec<5, WY, MODE == 1> (tabs, S, w, i - 1, zl, pmh[2], ha[2], az, one4, hp[2], hn[2], xn);
             if (lane_ok)
               Vec<float>::st4 (p.aux_new[5] + idh, xn);
           }
