@@ -33,6 +33,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <mutex>
 #include <type_traits>
 #include <vector>
@@ -157,9 +158,11 @@ struct Vec<float>
     v[3] = t.w;
   }
   static __device__ __forceinline__ float ld1 (const float *s) { return *s; }
+  // streaming (evict-first) store: the new buffers are read again only in
+  // the next step, after far more than L2 holds has passed through it
   static __device__ __forceinline__ void st4 (float *g, const float v[4])
   {
-    *reinterpret_cast<float4 *> (g) = make_float4 (v[0], v[1], v[2], v[3]);
+    __stcs (reinterpret_cast<float4 *> (g), make_float4 (v[0], v[1], v[2], v[3]));
   }
 };
 
@@ -184,7 +187,7 @@ struct Vec<__half>
     uint2 t;
     t.x = *reinterpret_cast<unsigned *> (&a);
     t.y = *reinterpret_cast<unsigned *> (&b);
-    *reinterpret_cast<uint2 *> (g) = t;
+    __stcs (reinterpret_cast<uint2 *> (g), t);
   }
 };
 
@@ -1060,6 +1063,15 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn ()
 // 3-D map over an (nx, ny, nz) array, z fastest, box bw x bh x 1
 bool make_map (CUtensorMap &m, const void *base, bool half, const int n[3], int bw, int bh)
 {
+  // L2 fetch granularity of the copies (FDTDB_TMA_L2PROMO 0..3 = none,
+  // 64, 128, 256 bytes; tuning runs)
+  static const CUtensorMapL2promotion promo = [] {
+    const char *v = std::getenv ("FDTDB_TMA_L2PROMO");
+    const int k = v ? std::atoi (v) : 2;
+    return k == 0 ? CU_TENSOR_MAP_L2_PROMOTION_NONE
+                  : (k == 1 ? CU_TENSOR_MAP_L2_PROMOTION_L2_64B
+                            : (k == 3 ? CU_TENSOR_MAP_L2_PROMOTION_L2_256B : CU_TENSOR_MAP_L2_PROMOTION_L2_128B));
+  }();
   auto fn = encode_fn ();
   if (!fn)
     return false;
@@ -1070,7 +1082,7 @@ bool make_map (CUtensorMap &m, const void *base, bool half, const int n[3], int 
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = fn (&m, half ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
                    const_cast<void *> (base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                   CU_TENSOR_MAP_SWIZZLE_NONE, promo, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
 
