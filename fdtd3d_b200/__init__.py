@@ -35,6 +35,7 @@ EXPORTED = (
     "fdtd_last_error", "fdtd_stream", "fdtd_profile", "fdtd_kernel_time", "fdtd_step_kernel",
     "fdtd_batch_create", "fdtd_batch_upload_eps", "fdtd_batch_tune", "fdtd_batch_step", "fdtd_batch_sync",
     "fdtd_batch_download", "fdtd_batch_info", "fdtd_batch_last_error", "fdtd_batch_destroy",
+    "fdtd_objective", "fdtd_backward",
 )
 
 
@@ -67,6 +68,17 @@ class Config(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("layout", ctypes.c_int),
         ("reserved", ctypes.c_int * 8),
+    ]
+
+
+class AdjointCfg(ctypes.Structure):
+    _fields_ = [
+        ("steps", ctypes.c_uint32),
+        ("checkpoint_every", ctypes.c_uint32),
+        ("probe_lo", ctypes.c_int * 2),
+        ("probe_hi", ctypes.c_int * 2),
+        ("precision", ctypes.c_int),
+        ("reserved", ctypes.c_int * 3),
     ]
 
 
@@ -110,6 +122,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fdtd_batch_info": ([vp, ctypes.POINTER(i64), ctypes.POINTER(i), ctypes.POINTER(d)], i),
         "fdtd_batch_last_error": ([vp], ctypes.c_char_p),
         "fdtd_batch_destroy": ([vp], None),
+        "fdtd_objective": ([vp, ctypes.POINTER(AdjointCfg), vp], i),
+        "fdtd_backward": ([vp, ctypes.POINTER(AdjointCfg), vp, vp], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -229,6 +243,31 @@ class Simulation:
 
     def launch_count(self) -> int:
         return int(self.lib.fdtd_launch_count(self._h))
+
+    def _adjoint_cfg(self, steps, every, probe_lo, probe_hi, precision):
+        c = AdjointCfg()
+        c.steps = int(steps)
+        c.checkpoint_every = int(every)
+        c.probe_lo[:] = [int(v) for v in probe_lo]
+        c.probe_hi[:] = [int(v) for v in probe_hi]
+        c.precision = int(precision)
+        return c
+
+    def objective(self, steps, probe_lo, probe_hi, precision=PREC_FP32) -> float:
+        """J = sum over t < steps of sum over the probe box of Ez_t^2 (2-D TMz, from t = 0)."""
+        c = self._adjoint_cfg(steps, 1, probe_lo, probe_hi, precision)
+        out = ctypes.c_double()
+        self._check(self.lib.fdtd_objective(self._h, ctypes.byref(c), ctypes.byref(out)), "fdtd_objective")
+        return out.value
+
+    def backward(self, steps, every, probe_lo, probe_hi, precision=PREC_FP32):
+        """(J, dJ/d eps on the (nx, ny) grid) by the checkpointed adjoint."""
+        c = self._adjoint_cfg(steps, every, probe_lo, probe_hi, precision)
+        out = ctypes.c_double()
+        grad = np.empty(self.shape, dtype=np.float64)
+        self._check(self.lib.fdtd_backward(self._h, ctypes.byref(c), ctypes.byref(out), grad.ctypes.data),
+                    "fdtd_backward")
+        return out.value, grad
 
     @property
     def step_kernel(self) -> str:

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/fdtd_b200.h"
+#include "adjoint.h"
 #include "fused3d.h"
 #include "sweep3d.h"
 #include "kernels.h"
@@ -1240,6 +1241,52 @@ int fdtd_scalars (const fdtd_ctx *ctx, double out[3])
   out[1] = ctx->g.freq;
   out[2] = ctx->g.rpv;
   return FDTD_OK;
+}
+
+namespace {
+
+int adjoint_entry (fdtd_ctx *ctx, const fdtd_adjoint_cfg *cfg, double *objective, double *grad)
+{
+  if (!ctx || !cfg || !objective)
+    return fail (ctx, FDTD_ERR_ARG, "null argument");
+  if (cfg->precision != FDTD_PREC_FP32 && cfg->precision != FDTD_PREC_FP64_PLAIN)
+    return fail (ctx, FDTD_ERR_ARG, "adjoint precision must be FP32 or FP64");
+  const Geometry &g = ctx->g;
+  if (!g.tmz || g.cfg.use_tfsf || g.cfg.use_metamaterials)
+    return fail (ctx, FDTD_ERR_UNSUPPORTED, "the adjoint covers 2-D TMz point-source runs");
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  AdjointRun run;
+  run.steps = cfg->steps;
+  run.every = cfg->checkpoint_every;
+  for (int a = 0; a < 2; ++a)
+  {
+    run.probe_lo[a] = cfg->probe_lo[a];
+    run.probe_hi[a] = cfg->probe_hi[a];
+  }
+  run.fp64 = cfg->precision == FDTD_PREC_FP64_PLAIN;
+  // eps as the context holds it: FP64 (plain form) or FP32 (null = uniform 1)
+  const void *eps = ctx->kind == 0 ? (const void *) ctx->mat64[0] : (const void *) ctx->mat32[0];
+  CK (cudaStreamSynchronize (ctx->stream));
+  std::string why = adjoint_run (g, eps, ctx->kind == 0, run, objective, grad, ctx->sm_count, ctx->stream);
+  if (!why.empty ())
+    return fail (ctx, why.find ("failed") != std::string::npos ? FDTD_ERR_CUDA : FDTD_ERR_ARG, why);
+  return FDTD_OK;
+}
+
+}  // namespace
+
+int fdtd_objective (fdtd_ctx *ctx, const fdtd_adjoint_cfg *cfg, double *objective)
+{
+  return adjoint_entry (ctx, cfg, objective, nullptr);
+}
+
+int fdtd_backward (fdtd_ctx *ctx, const fdtd_adjoint_cfg *cfg, double *objective, double *dobj_deps)
+{
+  if (!dobj_deps)
+    return fail (ctx, FDTD_ERR_ARG, "null gradient buffer");
+  return adjoint_entry (ctx, cfg, objective, dobj_deps);
 }
 
 const char *fdtd_step_kernel (const fdtd_ctx *ctx)

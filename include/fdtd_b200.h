@@ -189,6 +189,38 @@ int fdtd_kernel_time (fdtd_ctx *ctx, double *ms, int64_t *launches);
 void fdtd_destroy (fdtd_ctx *ctx);
 
 /*
+ * Adjoint (reverse-mode) gradient of a 2-D TMz run (no counterpart in the
+ * reference, which has no differentiation; the backward entry the
+ * reference-side glue would call to get design gradients).  The context
+ * supplies the geometry, PML, point source and eps as uploaded; the run
+ * starts from zero fields at t = 0 on the context's stream and leaves the
+ * context's own fields untouched.  The objective is
+ *   J = sum over t = 0 .. steps - 1 of sum over the probe box of Ez_t^2
+ * (Ez after the E half-step and point source of step t), accumulated in
+ * FP64 with compensation.  precision FDTD_PREC_FP32 runs the library's FP32
+ * TMz step and its exact discrete adjoint; FDTD_PREC_FP64_PLAIN runs the
+ * same formulation in FP64.  The reverse sweep keeps the state every
+ * checkpoint_every steps and recomputes one segment at a time, so device
+ * memory is about (steps / K + K) grids.  TF/SF and metamaterials are not
+ * provided (FDTD_ERR_UNSUPPORTED).
+ */
+typedef struct
+{
+  uint32_t steps;              /* time steps of the forward run */
+  uint32_t checkpoint_every;   /* K */
+  int probe_lo[2];             /* probe box [lo, hi) in x and y, inside 1 .. n - 2 */
+  int probe_hi[2];
+  int precision;               /* FDTD_PREC_FP32 or FDTD_PREC_FP64_PLAIN */
+  int reserved[3];
+} fdtd_adjoint_cfg;
+
+/* Forward run only: the objective. */
+int fdtd_objective (fdtd_ctx *ctx, const fdtd_adjoint_cfg *cfg, double *objective);
+/* Forward run with checkpoints, then the reverse sweep: the objective and
+ * dJ/d eps for every cell (host buffer of nx * ny doubles, y fastest). */
+int fdtd_backward (fdtd_ctx *ctx, const fdtd_adjoint_cfg *cfg, double *objective, double *dobj_deps);
+
+/*
  * Batched 2-D TMz (no counterpart in the reference, whose runs are one grid
  * per process): many Dim2_TMz simulations of different sizes advanced
  * together by one persistent kernel launch per fdtd_batch_step call,
