@@ -129,9 +129,44 @@ __global__ void fwd_e_kernel (AdjDev<R> p, R *Ez, R *Hx, R *Hy, R *Xz, R *dedm, 
   }
 }
 
+__device__ __forceinline__ void kahan_add (double &s, double &c, double v);
+
+// J += sum of Ez^2 over the probe, by one block; probe values optionally kept
 template <typename R>
-__global__ void fwd_h_kernel (AdjDev<R> p, const R *Ez, R *Hx, R *Hy, R *Xx, R *Xy, int k, int do_update)
+__device__ void probe_sum (const AdjDev<R> &p, const R *Ez, double *acc, double *keep)
 {
+  __shared__ double part[256];
+  const int w = p.pr_hi[1] - p.pr_lo[1];
+  const int n = (p.pr_hi[0] - p.pr_lo[0]) * w;
+  double s = 0.0;
+  for (int t = threadIdx.x; t < n; t += blockDim.x)
+  {
+    const int x = p.pr_lo[0] + t / w, y = p.pr_lo[1] + t % w;
+    const double v = (double) Ez[x * p.ny + y];
+    if (keep)
+      keep[t] = v;
+    s += v * v;
+  }
+  part[threadIdx.x] = s;
+  __syncthreads ();
+  for (int h = 128; h > 0; h >>= 1)
+  {
+    if (threadIdx.x < h)
+      part[threadIdx.x] += part[threadIdx.x + h];
+    __syncthreads ();
+  }
+  if (threadIdx.x == 0 && acc)
+    kahan_add (acc[0], acc[1], part[0]);
+}
+
+// H half-step (and H point source); block 0 first adds the probe term of
+// Ez_k, which the E kernel before it completed
+template <typename R>
+__global__ void __launch_bounds__ (256) fwd_h_kernel (AdjDev<R> p, const R *Ez, R *Hx, R *Hy, R *Xx, R *Xy, int k,
+                                                      int do_update, double *acc, double *keep)
+{
+  if (blockIdx.x == 0)
+    probe_sum (p, Ez, acc, keep);
   const int n = (p.nx - 2) * (p.ny - 2);
   const R *F[3] = {Ez, Hx, Hy};
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
@@ -165,78 +200,61 @@ __device__ __forceinline__ void kahan_add (double &s, double &c, double v)
   s = t;
 }
 
-// J += sum of Ez^2 over the probe (one block); probe values optionally kept
-template <typename R>
-__global__ void __launch_bounds__ (256) probe_kernel (AdjDev<R> p, const R *Ez, double *acc, double *keep)
-{
-  __shared__ double part[256];
-  const int w = p.pr_hi[1] - p.pr_lo[1];
-  const int n = (p.pr_hi[0] - p.pr_lo[0]) * w;
-  double s = 0.0;
-  for (int t = threadIdx.x; t < n; t += blockDim.x)
-  {
-    const int x = p.pr_lo[0] + t / w, y = p.pr_lo[1] + t % w;
-    const double v = (double) Ez[x * p.ny + y];
-    if (keep)
-      keep[t] = v;
-    s += v * v;
-  }
-  part[threadIdx.x] = s;
-  __syncthreads ();
-  for (int h = 128; h > 0; h >>= 1)
-  {
-    if (threadIdx.x < h)
-      part[threadIdx.x] += part[threadIdx.x + h];
-    __syncthreads ();
-  }
-  if (threadIdx.x == 0 && acc)
-    kahan_add (acc[0], acc[1], part[0]);
-}
-
 // ---- reverse
+//
+// Each reverse half-step is one kernel over all cells with double-buffered
+// adjoint fields: a thread updates its own cell from the old buffers and
+// gathers the curl adjoints of its neighbours by recomputing them (they are
+// pointwise in the old buffers), so no thread reads what another writes.
 
-// transpose of the H half-step (and H point source) at every updated H cell
 template <typename R>
-__global__ void adj_h1_kernel (AdjDev<R> p, R *aHx, R *aHy, R *aXx, R *aXy, R *acx, R *acy)
+struct CurlAdj
 {
-  const int n = (p.nx - 2) * (p.ny - 2);
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
-  {
-    const int x = 1 + t / (p.ny - 2), y = 1 + t % (p.ny - 2);
-    const int id = x * p.ny + y;
-    const bool at_src = x == p.ps[0] && y == p.ps[1];
-#pragma unroll
-    for (int q = 0; q < 2; ++q)
-    {
-      const int c = q ? kHy : kHx;
-      R *aH = q ? aHy : aHx;
-      R *aX = q ? aXy : aXx;
-      R *acu = q ? acy : acx;
-      R a = aH[id];
-      if (at_src && p.ps_on[c])
-        a = 0;
-      if (interior (p, c, x, y))
-      {
-        acu[id] = p.S * a;
-        aH[id] = a;
-      }
-      else
-      {
-        const R ca1 = tabv (p, c, 0, x, y), sq1 = tabv (p, c, 1, x, y);
-        const R p5 = tabv (p, c, 2, x, y), q5 = tabv (p, c, 3, x, y);
-        const R g4p = tabv (p, c, 4, x, y), g4m = tabv (p, c, 5, x, y);
-        const R t1 = aX[id] + g4p * q5 * a;
-        acu[id] = sq1 * t1;
-        aX[id] = ca1 * t1 - g4m * q5 * a;
-        aH[id] = p5 * a;
-      }
-    }
-  }
+  R acu, a_new, x_new;
+};
+
+// transpose of one H half-step at an updated H cell (point source included)
+template <typename R>
+__device__ __forceinline__ CurlAdj<R> h_adj (const AdjDev<R> &p, int c, R a, R ax, int x, int y)
+{
+  if (x == p.ps[0] && y == p.ps[1] && p.ps_on[c])
+    a = 0;
+  if (interior (p, c, x, y))
+    return {p.S * a, a, ax};
+  const R ca1 = tabv (p, c, 0, x, y), sq1 = tabv (p, c, 1, x, y);
+  const R p5 = tabv (p, c, 2, x, y), q5 = tabv (p, c, 3, x, y);
+  const R g4p = tabv (p, c, 4, x, y), g4m = tabv (p, c, 5, x, y);
+  const R t1 = ax + g4p * q5 * a;
+  return {sq1 * t1, p5 * a, ca1 * t1 - g4m * q5 * a};
 }
 
-// aE += (curl of E)^T of the H curl adjoints, plus 2 Ez_k on the probe
+// transpose of one E half-step at an updated Ez cell (point source included)
 template <typename R>
-__global__ void adj_h2_kernel (AdjDev<R> p, R *aE, const R *acx, const R *acy, const double *probe)
+__device__ __forceinline__ CurlAdj<R> e_adj (const AdjDev<R> &p, R a, R ax, R im, int x, int y)
+{
+  if (x == p.ps[0] && y == p.ps[1] && p.ps_on[kEz])
+    a = 0;
+  if (interior (p, kEz, x, y))
+    return {p.S * im * a, a, ax};
+  const R ca1 = tabv (p, kEz, 0, x, y), sq1 = tabv (p, kEz, 1, x, y);
+  const R p5 = tabv (p, kEz, 2, x, y), q5 = tabv (p, kEz, 3, x, y);
+  const R g4p = tabv (p, kEz, 4, x, y), g4m = tabv (p, kEz, 5, x, y);
+  const R t1 = ax + g4p * q5 * im * a;
+  return {sq1 * t1, p5 * a, ca1 * t1 - g4m * q5 * im * a};
+}
+
+template <typename R>
+__device__ __forceinline__ bool updated (const AdjDev<R> &p, int x, int y)
+{
+  return x >= 1 && x <= p.nx - 2 && y >= 1 && y <= p.ny - 2;
+}
+
+// transpose of the H half-step: new aH, aX of H; aE += curl-of-E adjoint
+// gathers + 2 Ez_k on the probe
+template <typename R>
+__global__ void __launch_bounds__ (256) adj_h_kernel (AdjDev<R> p, const R *aHx0, const R *aHy0, const R *aXx0,
+                                                      const R *aXy0, R *aHx1, R *aHy1, R *aXx1, R *aXy1, R *aE,
+                                                      const double *probe)
 {
   const int n = p.nx * p.ny;
   const int pw = p.pr_hi[1] - p.pr_lo[1];
@@ -248,12 +266,22 @@ __global__ void adj_h2_kernel (AdjDev<R> p, R *aE, const R *acx, const R *acy, c
     for (int q = 0; q < 2; ++q)
     {
       const int c = q ? kHy : kHx;
-      const R *acu = q ? acy : acx;
-      // H cell h reads Ez at h + d: Ez cell (x, y) is read by h = (x, y) - d
+      const R *aH0 = q ? aHy0 : aHx0;
+      const R *aX0 = q ? aXy0 : aXx0;
+      if (updated (p, x, y))
+      {
+        const CurlAdj<R> r = h_adj (p, c, aH0[t], aX0[t], x, y);
+        (q ? aHy1 : aHx1)[t] = r.a_new;
+        (q ? aXy1 : aXx1)[t] = r.x_new;
+      }
+      // Ez (x, y) is read by the H cell h = (x, y) - d of each Ez term
       auto take = [&] (const int d[2], R sgn) {
         const int hx = x - d[0], hy = y - d[1];
-        if (hx >= 1 && hx <= p.nx - 2 && hy >= 1 && hy <= p.ny - 2)
-          g += sgn * acu[hx * p.ny + hy];
+        if (updated (p, hx, hy))
+        {
+          const int h = hx * p.ny + hy;
+          g += sgn * h_adj (p, c, aH0[h], aX0[h], hx, hy).acu;
+        }
       };
       if (p.o1[c] == kEz)
       {
@@ -273,53 +301,34 @@ __global__ void adj_h2_kernel (AdjDev<R> p, R *aE, const R *acx, const R *acy, c
   }
 }
 
-// transpose of the E half-step (and E point source); gradient of im
+// transpose of the E half-step: gradient of im, new aE, aXz; aH += curl-of-H
+// adjoint gathers
 template <typename R>
-__global__ void adj_e1_kernel (AdjDev<R> p, R *aE, R *aXz, R *acz, const R *dedm, double *gim)
-{
-  const int n = (p.nx - 2) * (p.ny - 2);
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
-  {
-    const int x = 1 + t / (p.ny - 2), y = 1 + t % (p.ny - 2);
-    const int id = x * p.ny + y;
-    R a = aE[id];
-    if (p.ps_on[kEz] && x == p.ps[0] && y == p.ps[1])
-      a = 0;
-    gim[id] += (double) a * (double) dedm[id];
-    const R im = p.im[id];
-    if (interior (p, kEz, x, y))
-    {
-      acz[id] = p.S * im * a;
-      aE[id] = a;
-    }
-    else
-    {
-      const R ca1 = tabv (p, kEz, 0, x, y), sq1 = tabv (p, kEz, 1, x, y);
-      const R p5 = tabv (p, kEz, 2, x, y), q5 = tabv (p, kEz, 3, x, y);
-      const R g4p = tabv (p, kEz, 4, x, y), g4m = tabv (p, kEz, 5, x, y);
-      const R t1 = aXz[id] + g4p * q5 * im * a;
-      acz[id] = sq1 * t1;
-      aXz[id] = ca1 * t1 - g4m * q5 * im * a;
-      aE[id] = p5 * a;
-    }
-  }
-}
-
-// aH += (curl of H)^T of the Ez curl adjoints
-template <typename R>
-__global__ void adj_e2_kernel (AdjDev<R> p, R *aHx, R *aHy, const R *acz)
+__global__ void __launch_bounds__ (256) adj_e_kernel (AdjDev<R> p, const R *aE0, const R *aXz0, R *aE1, R *aXz1,
+                                                      R *aHx, R *aHy, const R *dedm, double *gim)
 {
   const int n = p.nx * p.ny;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
   {
     const int x = t / p.ny, y = t % p.ny;
-    R g[2] = {0, 0};
+    if (updated (p, x, y))
+    {
+      R a = aE0[t];
+      if (x == p.ps[0] && y == p.ps[1] && p.ps_on[kEz])
+        a = 0;
+      gim[t] += (double) a * (double) dedm[t];
+      const CurlAdj<R> r = e_adj (p, aE0[t], aXz0[t], p.im[t], x, y);
+      aE1[t] = r.a_new;
+      aXz1[t] = r.x_new;
+    }
     auto take = [&] (const int d[2], R sgn) -> R {
       const int ex = x - d[0], ey = y - d[1];
-      if (ex >= 1 && ex <= p.nx - 2 && ey >= 1 && ey <= p.ny - 2)
-        return sgn * acz[ex * p.ny + ey];
-      return R (0);
+      if (!updated (p, ex, ey))
+        return R (0);
+      const int e = ex * p.ny + ey;
+      return sgn * e_adj (p, aE0[e], aXz0[e], p.im[e], ex, ey).acu;
     };
+    R g[2] = {0, 0};
 #pragma unroll
     for (int q = 0; q < 2; ++q)
     {
@@ -571,8 +580,7 @@ std::string run_t (const Geometry &g, const void *eps_dev, bool eps_is_double, c
   };
   auto step = [&] (uint32_t k, R *dedm, double *keep, double *a) {
     fwd_e_kernel<R><<<blocks, 256, 0, s>>> (p, Ez, Hx, Hy, Xz, dedm, (int) k, k > 0);
-    probe_kernel<R><<<1, 256, 0, s>>> (p, Ez, a, keep);
-    fwd_h_kernel<R><<<blocks, 256, 0, s>>> (p, Ez, Hx, Hy, Xx, Xy, (int) k, k > 0);
+    fwd_h_kernel<R><<<blocks, 256, 0, s>>> (p, Ez, Hx, Hy, Xx, Xy, (int) k, k > 0, a, keep);
   };
 
   for (uint32_t k = 0; k < run.steps; ++k)
@@ -590,16 +598,18 @@ std::string run_t (const Geometry &g, const void *eps_dev, bool eps_is_double, c
   if (!grad_host)
     return "";
 
-  // reverse sweep, one checkpoint segment at a time
-  R *A[9];
-  for (int q = 0; q < 9; ++q)
+  // reverse sweep, one checkpoint segment at a time; adjoint fields double
+  // buffered (index 0 / 1 of each pair is swapped every half-step)
+  R *A[12];
+  for (int q = 0; q < 12; ++q)
   {
     A[q] = mem.get<R> (N);
     if (!A[q] || cudaMemsetAsync (A[q], 0, N * sizeof (R), s) != cudaSuccess)
       return "adjoint allocation failed";
   }
-  R *aE = A[0], *aHx = A[1], *aHy = A[2], *aXz = A[3], *aXx = A[4], *aXy = A[5], *acx = A[6], *acy = A[7],
-    *acz = A[8];
+  R *aE[2] = {A[0], A[1]}, *aXz[2] = {A[2], A[3]}, *aHx[2] = {A[4], A[5]}, *aHy[2] = {A[6], A[7]},
+    *aXx[2] = {A[8], A[9]}, *aXy[2] = {A[10], A[11]};
+  int ie = 0, ih = 0;
   double *gim = mem.get<double> (N);
   double *gout = mem.get<double> (N);
   R *dedm = mem.get<R> ((size_t) K * N);
@@ -615,10 +625,12 @@ std::string run_t (const Geometry &g, const void *eps_dev, bool eps_is_double, c
     for (int64_t k = (int64_t) k1 - 1; k >= (int64_t) k0 && k > 0; --k)
     {
       const size_t off = (size_t) (k - k0);
-      adj_h1_kernel<R><<<blocks, 256, 0, s>>> (p, aHx, aHy, aXx, aXy, acx, acy);
-      adj_h2_kernel<R><<<blocks, 256, 0, s>>> (p, aE, acx, acy, probe + off * npr);
-      adj_e1_kernel<R><<<blocks, 256, 0, s>>> (p, aE, aXz, acz, dedm + off * N, gim);
-      adj_e2_kernel<R><<<blocks, 256, 0, s>>> (p, aHx, aHy, acz);
+      adj_h_kernel<R><<<blocks, 256, 0, s>>> (p, aHx[ih], aHy[ih], aXx[ih], aXy[ih], aHx[1 - ih], aHy[1 - ih],
+                                              aXx[1 - ih], aXy[1 - ih], aE[ie], probe + off * npr);
+      ih ^= 1;
+      adj_e_kernel<R><<<blocks, 256, 0, s>>> (p, aE[ie], aXz[ie], aE[1 - ie], aXz[1 - ie], aHx[ih], aHy[ih],
+                                              dedm + off * N, gim);
+      ie ^= 1;
     }
   }
   grad_eps_kernel<R><<<blocks, 256, 0, s>>> (p, gim, imd, LE.nmat, LE.m[0][0], LE.m[0][1], LE.m[1][0], LE.m[1][1],

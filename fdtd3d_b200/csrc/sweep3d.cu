@@ -385,7 +385,10 @@ __global__ void __launch_bounds__ (32 * WY, 1)
   constexpr int HS = L::H_B / sizeof (T), ES = L::E_B / sizeof (T), PS = L::P_B / sizeof (float);
   constexpr unsigned kLanes = 0xffffffffu;   // shuffle mask: the whole warp
   extern __shared__ __align__ (128) unsigned char smem_raw[];
-  __shared__ int s_item;
+  // grabbed item, double buffered by grab parity: a CTA that skips an item
+  // of another class passes only one barrier before its next grab, so the
+  // next write must not land in the slot slower warps may still be reading
+  __shared__ int s_item[2];
   __shared__ int s_abort[2];   // per plane parity: a copy did not arrive in time
 
   const int lane = threadIdx.x, w = threadIdx.y;
@@ -475,12 +478,14 @@ __global__ void __launch_bounds__ (32 * WY, 1)
 
   unsigned phase = 0;   // bit s: parity of the next completion of stage s
   bool aborted = false;
+  unsigned grab = 0;    // items grabbed by this CTA (selects the s_item slot)
   for (;;)
   {
     if (leader)
-      s_item = (int) atomicAdd (wk.ctr + 2 * MODE, 1ull);
+      s_item[grab & 1u] = (int) atomicAdd (wk.ctr + 2 * MODE, 1ull);
     __syncthreads ();
-    const int item = s_item;
+    const int item = s_item[grab & 1u];
+    ++grab;
     if (item >= wk.nitems)
       break;
     if (sweep_item_class (p, wk, WY, item, tfsf_in) != MODE)
