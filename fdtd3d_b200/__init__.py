@@ -35,7 +35,7 @@ EXPORTED = (
     "fdtd_last_error", "fdtd_stream", "fdtd_profile", "fdtd_kernel_time", "fdtd_step_kernel",
     "fdtd_batch_create", "fdtd_batch_upload_eps", "fdtd_batch_tune", "fdtd_batch_step", "fdtd_batch_sync",
     "fdtd_batch_download", "fdtd_batch_info", "fdtd_batch_last_error", "fdtd_batch_destroy",
-    "fdtd_objective", "fdtd_backward",
+    "fdtd_objective", "fdtd_backward", "fdtd_dft_setup", "fdtd_dft_read",
 )
 
 
@@ -123,6 +123,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fdtd_batch_last_error": ([vp], ctypes.c_char_p),
         "fdtd_batch_destroy": ([vp], None),
         "fdtd_objective": ([vp, ctypes.POINTER(AdjointCfg), vp], i),
+        "fdtd_dft_setup": ([vp, i, i, i, i, vp], i),
+        "fdtd_dft_read": ([vp, vp], i),
         "fdtd_backward": ([vp, ctypes.POINTER(AdjointCfg), vp, vp], i),
     }
     for name, (args, res) in sig.items():
@@ -268,6 +270,21 @@ class Simulation:
         self._check(self.lib.fdtd_backward(self._h, ctypes.byref(c), ctypes.byref(out), grad.ctypes.data),
                     "fdtd_backward")
         return out.value, grad
+
+    def dft_setup(self, comp, axis: int, index: int, freqs) -> None:
+        """Starts a running DFT of `comp` on the plane x_axis = index at the given frequencies (Hz)."""
+        k = COMPONENTS.index(comp) if isinstance(comp, str) else int(comp)
+        f = np.ascontiguousarray(freqs, dtype=np.float64).reshape(-1)
+        self._check(self.lib.fdtd_dft_setup(self._h, k, int(axis), int(index), int(f.size), f.ctypes.data),
+                    "fdtd_dft_setup")
+        n = list(self.cfg.size)
+        self._dft_shape = (int(f.size),) + tuple(v for a, v in enumerate(n) if a != int(axis))
+
+    def dft(self) -> np.ndarray:
+        """Complex running DFT, shape (frequencies, plane axis a, plane axis b)."""
+        out = np.empty(int(np.prod(self._dft_shape)) * 2)
+        self._check(self.lib.fdtd_dft_read(self._h, out.ctypes.data), "fdtd_dft_read")
+        return (out[0::2] + 1j * out[1::2]).reshape(self._dft_shape)
 
     @property
     def step_kernel(self) -> str:

@@ -390,3 +390,87 @@ int launch_reduce_final (const double *partials, int nblocks, double *out, cudaS
 }
 
 }  // namespace fdtdb
+
+// ------------------------------------------------------------ running DFT
+
+namespace fdtdb {
+
+namespace {
+
+__device__ __forceinline__ double ldd (const double *p, size_t i)
+{
+  return p[i];
+}
+__device__ __forceinline__ double ldd (const float *p, size_t i)
+{
+  return (double) p[i];
+}
+__device__ __forceinline__ double ldd (const __half *p, size_t i)
+{
+  return (double) __half2float (p[i]);
+}
+
+__device__ __forceinline__ void neumaier (double *s, double *c, double v)
+{
+  const double t = *s + v;
+  if (fabs (*s) >= fabs (v))
+    *c += (*s - t) + v;
+  else
+    *c += (v - t) + *s;
+  *s = t;
+}
+
+// One time step of the running DFT of a stored field on the plane
+// x_axis = index: for every plane cell and frequency j,
+//   sum_j += v * exp(-i phase_j),  phase table = (cos, sin) per frequency,
+// in FP64 with Neumaier compensation (acc: re, re compensation, im, im
+// compensation per cell and frequency).
+template <typename T>
+__global__ void dft_kernel (const T *src, int axis, int index, int n0, int n1, int n2, double scale,
+                            const double *phase, int nf, double *acc)
+{
+  const int ma = axis == 0 ? n1 : n0;             // plane extents (first, second remaining axis)
+  const int mb = axis == 2 ? n1 : n2;
+  const long long cells = (long long) ma * mb;
+  for (long long q = (long long) blockIdx.x * blockDim.x + threadIdx.x; q < cells * nf;
+       q += (long long) gridDim.x * blockDim.x)
+  {
+    const int j = (int) (q / cells);
+    const long long c = q % cells;
+    const int a = (int) (c / mb), b = (int) (c % mb);
+    long long id;
+    if (axis == 0)
+      id = ((long long) index * n1 + a) * n2 + b;
+    else if (axis == 1)
+      id = ((long long) a * n1 + index) * n2 + b;
+    else
+      id = ((long long) a * n1 + b) * n2 + index;
+    const double v = ldd (src, (size_t) id) * scale;
+    double *r = acc + q * 4;
+    neumaier (r + 0, r + 1, v * phase[2 * j]);
+    neumaier (r + 2, r + 3, -v * phase[2 * j + 1]);
+  }
+}
+
+}  // namespace
+
+int launch_dft (const void *src, int kind, int axis, int index, const int n[3], double scale, const double *phase,
+                int nf, double *acc, int sm_count, cudaStream_t s)
+{
+  const long long cells = (long long) (axis == 0 ? n[1] : n[0]) * (axis == 2 ? n[1] : n[2]) * nf;
+  long long blocks = (cells + 255) / 256;
+  if (blocks > (long long) sm_count * 16)
+    blocks = (long long) sm_count * 16;
+  if (kind == 0)
+    dft_kernel<double><<<(unsigned) blocks, 256, 0, s>>> ((const double *) src, axis, index, n[0], n[1], n[2], scale,
+                                                          phase, nf, acc);
+  else if (kind == 1)
+    dft_kernel<float><<<(unsigned) blocks, 256, 0, s>>> ((const float *) src, axis, index, n[0], n[1], n[2], scale,
+                                                         phase, nf, acc);
+  else
+    dft_kernel<__half><<<(unsigned) blocks, 256, 0, s>>> ((const __half *) src, axis, index, n[0], n[1], n[2], scale,
+                                                          phase, nf, acc);
+  return 1;
+}
+
+}  // namespace fdtdb

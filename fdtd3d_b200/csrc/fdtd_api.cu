@@ -106,6 +106,14 @@ struct fdtd_ctx
   const char *step_kernel = "not_stepped";
   TfsfBand band;                          // TF/SF post pass of the sweep (band.cells > 0 when in use)
 
+  // running DFT of one component on one plane (dft_comp < 0: none)
+  int dft_comp = -1, dft_axis = 0, dft_index = 0, dft_nf = 0;
+  std::vector<double> dft_freq;
+  double *dft_acc = nullptr;              // (re, re comp., im, im comp.) per frequency and plane cell
+  double *dft_phase = nullptr;            // per step of the current fdtd_step call: (cos, sin) per frequency
+  size_t dft_phase_cap = 0;               // steps the phase table holds
+  std::vector<double> h_dft_phase;
+
   double *staging = nullptr;
   double *partials = nullptr;
   double *d_out = nullptr;
@@ -794,6 +802,54 @@ int prof_end (fdtd_ctx *ctx, cudaEvent_t end)
   return FDTD_OK;
 }
 
+// Phase table of the running DFT for steps t_start .. t_start + n - 1: E is
+// taken at (t + 1/2) dt and H at (t + 1) dt, the times of the point
+// sources of the same step.
+int dft_prepare (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
+{
+  if (ctx->dft_comp < 0)
+    return FDTD_OK;
+  const size_t need = (size_t) n * ctx->dft_nf * 2;
+  if (n > ctx->dft_phase_cap)
+  {
+    CK (cudaStreamSynchronize (ctx->stream));
+    if (ctx->dft_phase)
+    {
+      cudaFree (ctx->dft_phase);
+      ctx->allocs.erase (std::remove (ctx->allocs.begin (), ctx->allocs.end (), (void *) ctx->dft_phase),
+                         ctx->allocs.end ());
+      ctx->dft_phase = nullptr;
+    }
+    DALLOC (ctx->dft_phase, need * sizeof (double));
+    ctx->dft_phase_cap = n;
+    ctx->h_dft_phase.resize (need);
+  }
+  const double shift = ctx->dft_comp >= 3 ? 1.0 : 0.5;
+  for (uint32_t i = 0; i < n; ++i)
+    for (int j = 0; j < ctx->dft_nf; ++j)
+    {
+      const double ph = 2 * kPi * ctx->dft_freq[j] * ((double) (t_start + i) + shift) * ctx->g.dt;
+      ctx->h_dft_phase[((size_t) i * ctx->dft_nf + j) * 2] = std::cos (ph);
+      ctx->h_dft_phase[((size_t) i * ctx->dft_nf + j) * 2 + 1] = std::sin (ph);
+    }
+  CK (cudaMemcpyAsync (ctx->dft_phase, ctx->h_dft_phase.data (), need * sizeof (double), cudaMemcpyHostToDevice,
+                       ctx->stream));
+  return FDTD_OK;
+}
+
+// adds step i of the current call to the running DFT
+void dft_step (fdtd_ctx *ctx, uint32_t i)
+{
+  if (ctx->dft_comp < 0)
+    return;
+  const int k = ctx->dft_comp;
+  const void *src = ctx->kind == 0 ? (const void *) ctx->f[k][1] : (const void *) ctx->ff[k];
+  const double scale = k >= 3 ? 1.0 / ctx->eta0 : 1.0;
+  ctx->launches += launch_dft (src, ctx->kind, ctx->dft_axis, ctx->dft_index, ctx->g.n, scale,
+                               ctx->dft_phase + (size_t) i * ctx->dft_nf * 2, ctx->dft_nf, ctx->dft_acc,
+                               ctx->sm_count, ctx->stream);
+}
+
 int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
 {
   const Geometry &g = ctx->g;
@@ -810,6 +866,8 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
   CK (cudaMemcpyAsync (ctx->d_src, ctx->h_src, (size_t) n * 3 * sizeof (double), cudaMemcpyHostToDevice,
                        ctx->stream));
   CK (cudaEventRecord (ctx->src_ev, ctx->stream));
+  if ((r = dft_prepare (ctx, t_start, n)) != FDTD_OK)
+    return r;
   size_t ps_idx = 0;
   bool ps_ok = g.cfg.point_source_mask && point_source_index (g, &ps_idx);
   cudaStream_t s = ctx->stream;
@@ -881,6 +939,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
         return r;
       ctx->fcur = nw;
       select_fast_set (ctx);
+      dft_step (ctx, i);
       continue;
     }
     for (int h = 0; h < 2; ++h)
@@ -953,6 +1012,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
         }
       }
     }
+    dft_step (ctx, i);
   }
   CK (cudaGetLastError ());
   return FDTD_OK;
@@ -1287,6 +1347,58 @@ int fdtd_backward (fdtd_ctx *ctx, const fdtd_adjoint_cfg *cfg, double *objective
   if (!dobj_deps)
     return fail (ctx, FDTD_ERR_ARG, "null gradient buffer");
   return adjoint_entry (ctx, cfg, objective, dobj_deps);
+}
+
+int fdtd_dft_setup (fdtd_ctx *ctx, int component, int axis, int index, int nfreq, const double *freq_hz)
+{
+  if (!ctx || component < 0 || component > 5 || !ctx->g.comp[component].exists || axis < 0 || axis > 2 ||
+      index < 0 || index >= ctx->g.n[axis] || nfreq < 1 || nfreq > 64 || !freq_hz)
+    return fail (ctx, FDTD_ERR_ARG, "bad DFT plane, component or frequency list");
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  const int *n = ctx->g.n;
+  const size_t cells = (size_t) (axis == 0 ? n[1] : n[0]) * (axis == 2 ? n[1] : n[2]);
+  CK (cudaStreamSynchronize (ctx->stream));
+  if (ctx->dft_acc)
+  {
+    cudaFree (ctx->dft_acc);
+    ctx->allocs.erase (std::remove (ctx->allocs.begin (), ctx->allocs.end (), (void *) ctx->dft_acc),
+                       ctx->allocs.end ());
+    ctx->dft_acc = nullptr;
+  }
+  DALLOC (ctx->dft_acc, cells * nfreq * 4 * sizeof (double));
+  ctx->dft_comp = component;
+  ctx->dft_axis = axis;
+  ctx->dft_index = index;
+  ctx->dft_nf = nfreq;
+  ctx->dft_freq.assign (freq_hz, freq_hz + nfreq);
+  CK (cudaStreamSynchronize (ctx->stream));
+  return FDTD_OK;
+}
+
+int fdtd_dft_read (fdtd_ctx *ctx, double *out)
+{
+  if (!ctx || !out)
+    return fail (ctx, FDTD_ERR_ARG, "bad argument");
+  if (ctx->dft_comp < 0)
+    return fail (ctx, FDTD_ERR_STATE, "no DFT set up");
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  const int *n = ctx->g.n;
+  const int axis = ctx->dft_axis;
+  const size_t cells = (size_t) (axis == 0 ? n[1] : n[0]) * (axis == 2 ? n[1] : n[2]);
+  std::vector<double> acc (cells * ctx->dft_nf * 4);
+  CK (cudaMemcpyAsync (acc.data (), ctx->dft_acc, acc.size () * sizeof (double), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+  CK (cudaStreamSynchronize (ctx->stream));
+  for (size_t q = 0; q < cells * ctx->dft_nf; ++q)
+  {
+    out[2 * q] = acc[4 * q] + acc[4 * q + 1];
+    out[2 * q + 1] = acc[4 * q + 2] + acc[4 * q + 3];
+  }
+  return FDTD_OK;
 }
 
 const char *fdtd_step_kernel (const fdtd_ctx *ctx)

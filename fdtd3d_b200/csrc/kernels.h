@@ -54,6 +54,11 @@ int launch_convert_out (double *dst, const void *src, int src_kind, size_t n, do
 int launch_reduce_sq (const void *src, int kind, size_t n, const void *weight, int wkind, double scale,
                       double *partials, int nblocks, cudaStream_t s);
 int launch_fill (double *dst, size_t n, double value, cudaStream_t s);
+// one step of the running DFT of a stored field (kind 0 double, 1 float,
+// 2 half) on the plane x_axis = index; phase: (cos, sin) per frequency;
+// acc: (re, re comp., im, im comp.) per frequency and plane cell
+int launch_dft (const void *src, int kind, int axis, int index, const int n[3], double scale, const double *phase,
+                int nf, double *acc, int sm_count, cudaStream_t s);
 int launch_reduce_final (const double *partials, int nblocks, double *out, cudaStream_t s);
 
 }  // namespace fdtdb

@@ -164,6 +164,19 @@ int fdtd_scalars (const fdtd_ctx *ctx, double out[3]);
 /* Number of kernel launches this context issued so far. */
 int64_t fdtd_launch_count (const fdtd_ctx *ctx);
 
+/* Running DFT (no counterpart in the reference, which saves snapshots
+ * only): from this call on, every time step adds
+ *   F_j += v * exp(-i 2 pi f_j t_c)
+ * for component `component` (FDTD_EX..FDTD_HZ) on the plane x_axis = index
+ * (axis 0, 1, 2 = x, y, z; in 2-D the plane z = 0 is the whole grid), with
+ * t_c = (t + 1/2) dt for E and (t + 1) dt for H, the times of the step's
+ * point sources.  Sums are FP64 with compensation, whatever the field
+ * precision.  Up to 64 frequencies; calling it again restarts from zero.
+ * fdtd_dft_read writes nfreq x plane cells x (re, im) doubles, the plane's
+ * cells ordered as the two remaining axes with the later one fastest. */
+int fdtd_dft_setup (fdtd_ctx *ctx, int component, int axis, int index, int nfreq, const double *freq_hz);
+int fdtd_dft_read (fdtd_ctx *ctx, double *out);
+
 /* Name of the kernel that performs this context's field update (no
  * reference counterpart): "plain_fp64" (FP64 plain form), "sweep3d_tma"
  * (TMA-pipelined one-sweep 3-D kernel), "fused3d_regblock" (register-blocked
