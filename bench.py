@@ -172,6 +172,40 @@ def precision_extra(fd, n: int, steps: int, every: int, eps: np.ndarray) -> dict
     return {"config": f"{n}^3 sphere workload, {steps} steps, relative to the FP64 plain form", "checkpoints": rows}
 
 
+def drude_extra(fd, n: int = 384, steps: int = 3000) -> dict:
+    """Drude slab, 64 cells thick normal to z at the centre over the whole
+    transverse extent, eps_inf = 1, omega_p = 2 pi 30 GHz, gamma = 2 pi 1 GHz
+    for eps and mu; plane wave at normal incidence (15 GHz), PML 16, FP32;
+    running DFT of Ex on the slab's back face every step."""
+    z0 = n // 2 - 32
+    z1 = z0 + 64
+    om = np.zeros((n, n, n))
+    ga = np.zeros((n, n, n))
+    om[:, :, z0:z1] = np.float32(2 * np.pi * 30e9)
+    ga[:, :, z0:z1] = np.float32(2 * np.pi * 1e9)
+    kw = dict(mode=3, size=n, use_pml=True, pml=16, use_tfsf=True, tfsf_left=24, tfsf_right=24, teta=0.0,
+              phi=0.0, psi=0.0, dx=0.0005, wavelength=0.02, courant=0.5, use_metamaterials=True,
+              precision=fd.PREC_FP32)
+    with fd.Simulation(**kw) as sim:
+        for name in ("omegape", "omegapm"):
+            sim.set_material(name, om)
+        for name in ("gammae", "gammam"):
+            sim.set_material(name, ga)
+        del om, ga
+        sim.dft_setup("Ex", 2, z1, [15e9])
+        sim.step(3)
+        sim.sync()
+        t0 = time.perf_counter()
+        sim.step(steps, t_start=3)
+        sim.sync()
+        t = time.perf_counter() - t0
+        spec = sim.dft()
+        kernel = sim.step_kernel
+    return {"config": f"{n}^3 Drude slab, {steps} steps, FP32, running DFT of Ex at z = {z1}",
+            "value": n ** 3 * steps / t / 1e9, "unit": METRIC, "seconds": t, "kernel": kernel,
+            "dft_max_abs": float(np.max(np.abs(spec))), "dft_finite": bool(np.isfinite(spec).all())}
+
+
 def workload_kw(n: int, precision: int) -> dict:
     return dict(mode=3, size=n, use_pml=True, pml=PML, use_tfsf=True, tfsf_left=TFSF, tfsf_right=TFSF,
                 teta=30.0, phi=45.0, psi=0.0, dx=0.0005, wavelength=0.02, courant=0.5, precision=precision)
@@ -192,6 +226,24 @@ def algorithmic_bytes_per_cell(n: int, word: int) -> tuple[float, float]:
     inner = n - 2 * PML
     f_pml = 1.0 - (inner / n) ** 3
     return word * (12 + 1 + 12 * f_pml), f_pml
+
+
+def max_over_ranks(value: float, dist, device) -> float:
+    """The largest of every rank's value (a timed region is as long as its
+    slowest replica); the value itself without a process group."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world: int, cells: int, steps: int, ms: float) -> float:
+    """Whole-job Gcell-updates/s: every replica advanced `cells` cells `steps`
+    times within `ms` (the max over ranks)."""
+    return world * cells * steps / (ms * 1e-3) / 1e9
 
 
 def measured_peaks() -> dict:
@@ -399,11 +451,8 @@ def main() -> None:
     sim.profile(False)
     sim_kernel = sim.step_kernel
     launches = sim.launch_count() - l0
-    if dist:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * cells * args.steps / (ms * 1e-3) / 1e9
+    ms = max_over_ranks(ms, dist, f"cuda:{local}")
+    value = job_rate(world, cells, args.steps, ms)
 
     # roofline of the field half-step kernel
     peaks = measured_peaks()
@@ -441,11 +490,8 @@ def main() -> None:
     e1.record(stream)
     e1.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * cells * args.e2e_steps * args.e2e_chunk / (e2e_ms * 1e-3) / 1e9
+    e2e_ms = max_over_ranks(e2e_ms, dist, f"cuda:{local}")
+    e2e_value = job_rate(world, cells, args.e2e_steps * args.e2e_chunk, e2e_ms)
     finite = bool(np.isfinite(h_out.numpy()).all())
     sim.close()
 
@@ -477,6 +523,7 @@ def main() -> None:
         if "plain_fp64" in extras:
             extras["speedup_vs_plain_fp64"] = value / world / extras["plain_fp64"]["value"]
         for name, fn in (("adjoint_tmz", lambda: adjoint_extra(fd)), ("batch_tmz", lambda: batch_extra(fd)),
+                         ("drude_slab", lambda: drude_extra(fd)),
                          ("precision", lambda: precision_extra(fd, n, args.precision_steps, args.precision_every,
                                                                 eps))):
             try:
