@@ -80,6 +80,7 @@ struct Smem
   static constexpr unsigned TX_P = 2u * sizeof (float) * PW * WY;
   static constexpr unsigned TX_A = 6u * sizeof (float) * PW * WY;
   static constexpr unsigned TX_AN = 6u * sizeof (float) * AN * WY;
+  static constexpr unsigned TX_AN4 = 4u * sizeof (float) * AN * WY;   // z-edge items: no Ex / Hx auxiliary
 };
 
 // ---------------------------------------------------------------- PTX helpers
@@ -260,10 +261,7 @@ struct PmlTabs
 // PML update of component K on the cells of mask pm among a lane's four
 // cells: X_new = ca1 X + sq1 curl, F = p5 F + (g4p X_new - g4m X) q5 / m.
 // Branch-free over the cells; cells outside pm keep fn and their X.
-// ZONLY: the cell is interior along x and y, where every pair is the
-// sigma = 0 identity (ca1 = 1, sq1 = S, p5 = q5 = g4p = g4m = 1; exact in
-// FP32), so only the z pair is read.
-template <int K, int WY, bool ZONLY = false>
+template <int K, int WY>
 __device__ __forceinline__ void pml_vec (const PmlTabs &t, float S, int row, int plane, int col, unsigned pm,
                                          const float xo[4], const float cu[4], const float im[4], const float fo[4],
                                          float fn[4], float xn[4])
@@ -275,8 +273,8 @@ __device__ __forceinline__ void pml_vec (const PmlTabs &t, float S, int row, int
   for (int e = 0; e < 2; ++e)
   {
     lds4f (t.z + (2 * K + e) * PW + col, c[pz][e]);
-    const float vy = ZONLY ? (py == 0 && e == 1 ? S : 1.f) : t.y[(2 * K + e) * WY + row];
-    const float vx = ZONLY ? (px == 0 && e == 1 ? S : 1.f) : t.x[(2 * K + e) * XW + plane];
+    const float vy = t.y[(2 * K + e) * WY + row];
+    const float vx = t.x[(2 * K + e) * XW + plane];
 #pragma unroll
     for (int j = 0; j < 4; ++j)
     {
@@ -296,7 +294,7 @@ __device__ __forceinline__ void pml_vec (const PmlTabs &t, float S, int row, int
 }
 
 // The same for one cell (the z ring cell, column 128 of the tile).
-template <int K, int WY, bool ZONLY = false>
+template <int K, int WY>
 __device__ __forceinline__ float pml_one (const PmlTabs &t, float S, int row, int plane, int col, float xo, float cu,
                                           float im, float fo)
 {
@@ -308,10 +306,65 @@ __device__ __forceinline__ float pml_one (const PmlTabs &t, float S, int row, in
 #pragma unroll
     for (int q = 0; q < 3; ++q)
       c[q][e] = q == pz ? t.z[(2 * K + e) * PW + col]
-                        : (ZONLY ? (q == 0 && e == 1 ? S : 1.f)
-                                 : (q == py ? t.y[(2 * K + e) * WY + row] : t.x[(2 * K + e) * XW + plane]));
+                        : (q == py ? t.y[(2 * K + e) * WY + row] : t.x[(2 * K + e) * XW + plane]);
   const float n = c[0][0] * xo + c[0][1] * cu;
   return c[1][0] * fo + (c[2][0] * n - c[2][1] * xo) * c[1][1] * im;
+}
+
+// z-edge items (x and y interior): only the z pair of each component
+// differs from the sigma = 0 identity, and the item's z tables hold it in
+// the form of one branch-free update for PML and interior cells alike:
+//   (p5, q5) along z (Ex, Hx) as (p5, S q5): F = p5 F + S q5 im curl; the
+//     auxiliary cancels, since ca1 = 1, sq1 = S, g4p = g4m = 1 make
+//     X_new - X = S curl, so none is kept;
+//   (ca1, sq1) along z (Ey, Hy) as (ca1 - 1, sq1):
+//     X_new = ca1 X + sq1 curl, F = F + ((ca1 - 1) X + sq1 curl) im;
+//   (g4p, g4m) along z (Ez, Hz) as (S g4p, g4p - g4m):
+//     X_new = X + S curl, F = F + ((g4p - g4m) X + S g4p curl) im.
+// With the identity values each form is exactly the lean update
+// F + (S im) curl, so interior cells match the lean class bit for bit; X is
+// taken as 0 on cells that are not PML cells of the component.
+__host__ __device__ inline void zedge_pair (int k, float a, float b, float S, float &c0, float &c1)
+{
+  switch (pair_along (k, 2))
+  {
+    case 1: c0 = a; c1 = S * b; break;
+    case 0: c0 = a - 1.f; c1 = b; break;
+    default: c0 = S * a; c1 = a - b; break;
+  }
+}
+
+// Component K on a lane's four cells of a z-edge item; xn gets X_new on the
+// cells of pm (0 elsewhere) for the two components that keep an auxiliary.
+template <int K>
+__device__ __forceinline__ void zedge_vec (const float *tz, int col, float S, unsigned upd, unsigned pm,
+                                           const float xo[4], const float cu[4], const float im[4],
+                                           const float fo[4], float fn[4], float xn[4])
+{
+  constexpr int pz = pair_along (K, 2);
+  float c0[4], c1[4];
+  lds4f (tz + (2 * K) * PW + col, c0);
+  lds4f (tz + (2 * K + 1) * PW + col, c1);
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+  {
+    const bool on = (pm >> j) & 1u;
+    const float x = on ? xo[j] : 0.f;
+    float f;
+    if (pz == 1)
+      f = fmaf (im[j] * c1[j], cu[j], c0[j] * fo[j]);
+    else if (pz == 0)
+    {
+      f = fmaf (c1[j] * im[j], cu[j], fmaf (c0[j] * im[j], x, fo[j]));
+      xn[j] = on ? fmaf (c0[j], x, fmaf (c1[j], cu[j], x)) : 0.f;
+    }
+    else
+    {
+      f = fmaf (c0[j] * im[j], cu[j], fmaf (c1[j] * im[j], x, fo[j]));
+      xn[j] = on ? fmaf (S, cu[j], x) : 0.f;
+    }
+    fn[j] = ((upd >> j) & 1u) ? f : fo[j];
+  }
 }
 
 // ------------------------------------------------------------ item classes
@@ -450,7 +503,8 @@ __global__ void __launch_bounds__ (32 * WY, 1)
   auto issue = [&] (unsigned st, int x, int z0, int y0, int mode, int az0) {
     const uint32_t s = sbase + st * L::STAGE;
     const uint32_t b = bar + 8 * st;
-    mbar_expect_tx (b, L::TX_HE + (has_eps ? L::TX_P : 0u) + (mode == 2 ? L::TX_A : (mode == 1 ? L::TX_AN : 0u)));
+    mbar_expect_tx (b, L::TX_HE + (has_eps ? L::TX_P : 0u) +
+                           (mode == 2 ? L::TX_A : (mode == 1 ? (MODE == 1 ? L::TX_AN4 : L::TX_AN) : 0u)));
 #pragma unroll
     for (int c = 0; c < 3; ++c)
       tma_load_3d (s + c * L::H_B, &maps.h[c], z0 - HZ, y0 - 1, x, b);
@@ -467,6 +521,8 @@ __global__ void __launch_bounds__ (32 * WY, 1)
 #pragma unroll
       for (int c = 0; c < 6; ++c)
       {
+        if (MODE == 1 && (c == 0 || c == 3))
+          continue;
         const int xx = c < 3 ? x : max (x - 1, 0);
         if (mode == 2)
           tma_load_3d (s + L::OFF_A + c * L::P_B, &maps.aux[c], z0, y0, xx, b);
@@ -527,7 +583,20 @@ __global__ void __launch_bounds__ (32 * WY, 1)
                az0);
     }
     // PML coefficient pairs of this item (read after the first plane's barrier)
-    if (MODE != 0 && p.use_pml)
+    if (MODE == 1 && p.use_pml)
+    {
+      for (int q = tid; q < 6 * PW; q += 32 * WY)
+      {
+        const int k = q / PW, col = q % PW, z = z0 + col;
+        const int pz = pair_along (k, 2);
+        float c0 = 0.f, c1 = 0.f;
+        if (z < nz)
+          zedge_pair (k, __ldg (p.tab[k][2 * pz] + z), __ldg (p.tab[k][2 * pz + 1] + z), S, c0, c1);
+        Tab[(2 * k) * PW + col] = c0;
+        Tab[(2 * k + 1) * PW + col] = c1;
+      }
+    }
+    else if (MODE == 2 && p.use_pml)
     {
       for (int q = tid; q < 6 * 2 * PW; q += 32 * WY)
       {
@@ -624,7 +693,7 @@ __global__ void __launch_bounds__ (32 * WY, 1)
             const int k = 3 + c;
             const bool xy = xh >= p.ilo[k][0] && xh < p.ihi[k][0] && ((yin >> k) & 1u);
             pmh[c] = zupd & ~((xy ? zin : 0u) >> (4 * k)) & 15u;
-            if (pmh[c])
+            if (pmh[c] && !(MODE == 1 && c == 0))
               lds4f (A + (3 + c) * PS + w * apitch + acol, ha[c]);
           }
         }
@@ -648,7 +717,7 @@ __global__ void __launch_bounds__ (32 * WY, 1)
             {
               const bool xy = x >= p.ilo[k][0] && x < p.ihi[k][0] && ((yin >> k) & 1u);
               pm[k] = upd & ~((xy ? zin : 0u) >> (4 * k)) & 15u;
-              if (pm[k])
+              if (pm[k] && !(MODE == 1 && k == 0))
                 lds4f (A + k * PS + w * apitch + acol, xo[k]);
             }
           }
@@ -705,35 +774,49 @@ __global__ void __launch_bounds__ (32 * WY, 1)
                 cz[j] += tfsf_curl_cold (&p, 2, p.inc_h, err, x, y, zc + j);
               }
           }
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-          {
-            const bool u = (upd >> j) & 1u;
-            en[0][j] = u ? eo[0][j] + (S * ix[j]) * cx[j] : eo[0][j];
-            en[1][j] = u ? eo[1][j] + (S * iy[j]) * cy[j] : eo[1][j];
-            en[2][j] = u ? eo[2][j] + (S * iz[j]) * cz[j] : eo[2][j];
-          }
           const bool store_e = own_row && x <= xb && lane_ok;
-          if (pm[0])
+          if constexpr (MODE == 1)
           {
             float xn[4];
-            pml_vec<0, WY, MODE == 1> (tabs, S, w, i, zl, pm[0], xo[0], cx, ix, eo[0], en[0], xn);
-            if (store_e)
-              Vec<float>::st4 (p.aux_new[0] + id, xn);
-          }
-          if (pm[1])
-          {
-            float xn[4];
-            pml_vec<1, WY, MODE == 1> (tabs, S, w, i, zl, pm[1], xo[1], cy, iy, eo[1], en[1], xn);
-            if (store_e)
+            zedge_vec<0> (tabs.z, zl, S, upd, pm[0], xo[0], cx, ix, eo[0], en[0], xn);
+            zedge_vec<1> (tabs.z, zl, S, upd, pm[1], xo[1], cy, iy, eo[1], en[1], xn);
+            if (pm[1] && store_e)
               Vec<float>::st4 (p.aux_new[1] + id, xn);
-          }
-          if (pm[2])
-          {
-            float xn[4];
-            pml_vec<2, WY, MODE == 1> (tabs, S, w, i, zl, pm[2], xo[2], cz, iz, eo[2], en[2], xn);
-            if (store_e)
+            zedge_vec<2> (tabs.z, zl, S, upd, pm[2], xo[2], cz, iz, eo[2], en[2], xn);
+            if (pm[2] && store_e)
               Vec<float>::st4 (p.aux_new[2] + id, xn);
+          }
+          else
+          {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+              const bool u = (upd >> j) & 1u;
+              en[0][j] = u ? eo[0][j] + (S * ix[j]) * cx[j] : eo[0][j];
+              en[1][j] = u ? eo[1][j] + (S * iy[j]) * cy[j] : eo[1][j];
+              en[2][j] = u ? eo[2][j] + (S * iz[j]) * cz[j] : eo[2][j];
+            }
+            if (pm[0])
+            {
+              float xn[4];
+              pml_vec<0, WY> (tabs, S, w, i, zl, pm[0], xo[0], cx, ix, eo[0], en[0], xn);
+              if (store_e)
+                Vec<float>::st4 (p.aux_new[0] + id, xn);
+            }
+            if (pm[1])
+            {
+              float xn[4];
+              pml_vec<1, WY> (tabs, S, w, i, zl, pm[1], xo[1], cy, iy, eo[1], en[1], xn);
+              if (store_e)
+                Vec<float>::st4 (p.aux_new[1] + id, xn);
+            }
+            if (pm[2])
+            {
+              float xn[4];
+              pml_vec<2, WY> (tabs, S, w, i, zl, pm[2], xo[2], cz, iz, eo[2], en[2], xn);
+              if (store_e)
+                Vec<float>::st4 (p.aux_new[2] + id, xn);
+            }
           }
           if (kFull && (p.ps_mask & 7) && rowupd && x == p.ps[0] && y == p.ps[1] && p.ps[2] >= zc && p.ps[2] < zc + 4)
           {
@@ -789,14 +872,24 @@ __global__ void __launch_bounds__ (32 * WY, 1)
               const bool in1 = x >= p.ilo[1][0] && x < p.ihi[1][0] && (yin & 2u) && zr >= p.ilo[1][2] &&
                                zr < p.ihi[1][2];
               const int rcol = amode == 2 ? TZ : TZ - az0;
-              if (amode && !in0)
-                rx = pml_one<0, WY, MODE == 1> (tabs, S, w, i, TZ, A[0 * PS + w * apitch + rcol], crx, irx, rx);
+              if constexpr (MODE == 1)
+              {
+                const float *tz = tabs.z;
+                const float xo1 = in1 ? 0.f : A[1 * PS + w * apitch + rcol];
+                rx = fmaf (irx * tz[1 * PW + TZ], crx, tz[0 * PW + TZ] * rx);
+                ry = fmaf (tz[3 * PW + TZ] * iry, cry, fmaf (tz[2 * PW + TZ] * iry, xo1, ry));
+              }
               else
-                rx = rx + (S * irx) * crx;
-              if (amode && !in1)
-                ry = pml_one<1, WY, MODE == 1> (tabs, S, w, i, TZ, A[1 * PS + w * apitch + rcol], cry, iry, ry);
-              else
-                ry = ry + (S * iry) * cry;
+              {
+                if (amode && !in0)
+                  rx = pml_one<0, WY> (tabs, S, w, i, TZ, A[0 * PS + w * apitch + rcol], crx, irx, rx);
+                else
+                  rx = rx + (S * irx) * crx;
+                if (amode && !in1)
+                  ry = pml_one<1, WY> (tabs, S, w, i, TZ, A[1 * PS + w * apitch + rcol], cry, iry, ry);
+                else
+                  ry = ry + (S * iry) * cry;
+              }
               if (kFull && (p.ps_mask & 3) && x == p.ps[0] && y == p.ps[1] && zr == p.ps[2])
               {
                 const float v = (float) p.src[p.src_index];
@@ -864,34 +957,48 @@ __global__ void __launch_bounds__ (32 * WY, 1)
                 az[j] += tfsf_curl_cold (&p, 5, p.inc_e, err, xh, y, zc + j);
               }
           }
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-          {
-            const bool u = (zupd >> j) & 1u;
-            hn[0][j] = u ? hp[0][j] + S * ax[j] : hp[0][j];
-            hn[1][j] = u ? hp[1][j] + S * ay[j] : hp[1][j];
-            hn[2][j] = u ? hp[2][j] + S * az[j] : hp[2][j];
-          }
-          if (pmh[0])
+          if constexpr (MODE == 1)
           {
             float xn[4];
-            pml_vec<3, WY, MODE == 1> (tabs, S, w, i - 1, zl, pmh[0], ha[0], ax, one4, hp[0], hn[0], xn);
-            if (lane_ok)
-              Vec<float>::st4 (p.aux_new[3] + idh, xn);
-          }
-          if (pmh[1])
-          {
-            float xn[4];
-            pml_vec<4, WY, MODE == 1> (tabs, S, w, i - 1, zl, pmh[1], ha[1], ay, one4, hp[1], hn[1], xn);
-            if (lane_ok)
+            zedge_vec<3> (tabs.z, zl, S, zupd, pmh[0], ha[0], ax, one4, hp[0], hn[0], xn);
+            zedge_vec<4> (tabs.z, zl, S, zupd, pmh[1], ha[1], ay, one4, hp[1], hn[1], xn);
+            if (pmh[1] && lane_ok)
               Vec<float>::st4 (p.aux_new[4] + idh, xn);
-          }
-          if (pmh[2])
-          {
-            float xn[4];
-            pml_vec<5, WY, MODE == 1> (tabs, S, w, i - 1, zl, pmh[2], ha[2], az, one4, hp[2], hn[2], xn);
-            if (lane_ok)
+            zedge_vec<5> (tabs.z, zl, S, zupd, pmh[2], ha[2], az, one4, hp[2], hn[2], xn);
+            if (pmh[2] && lane_ok)
               Vec<float>::st4 (p.aux_new[5] + idh, xn);
+          }
+          else
+          {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+              const bool u = (zupd >> j) & 1u;
+              hn[0][j] = u ? hp[0][j] + S * ax[j] : hp[0][j];
+              hn[1][j] = u ? hp[1][j] + S * ay[j] : hp[1][j];
+              hn[2][j] = u ? hp[2][j] + S * az[j] : hp[2][j];
+            }
+            if (pmh[0])
+            {
+              float xn[4];
+              pml_vec<3, WY> (tabs, S, w, i - 1, zl, pmh[0], ha[0], ax, one4, hp[0], hn[0], xn);
+              if (lane_ok)
+                Vec<float>::st4 (p.aux_new[3] + idh, xn);
+            }
+            if (pmh[1])
+            {
+              float xn[4];
+              pml_vec<4, WY> (tabs, S, w, i - 1, zl, pmh[1], ha[1], ay, one4, hp[1], hn[1], xn);
+              if (lane_ok)
+                Vec<float>::st4 (p.aux_new[4] + idh, xn);
+            }
+            if (pmh[2])
+            {
+              float xn[4];
+              pml_vec<5, WY> (tabs, S, w, i - 1, zl, pmh[2], ha[2], az, one4, hp[2], hn[2], xn);
+              if (lane_ok)
+                Vec<float>::st4 (p.aux_new[5] + idh, xn);
+            }
           }
           if (kFull && (p.ps_mask & 56) && xh == p.ps[0] && y == p.ps[1] && p.ps[2] >= zc && p.ps[2] < zc + 4)
           {
