@@ -611,20 +611,24 @@ int plan_sweep (fdtd_ctx *ctx)
     post = post && std::atoi (v) != 0;
   if (post)
   {
-    std::vector<int> boxes;
-    std::vector<long long> offset;
-    std::string bwhy = tfsf_band_boxes (ctx->fused, boxes, offset);
+    std::vector<BandBox> boxes;
+    std::vector<int2> blk;
+    std::string bwhy = tfsf_band_boxes (ctx->fused, boxes, blk);
     if (bwhy.empty () && !boxes.empty ())
     {
-      DALLOC (ctx->band.boxes, boxes.size () * sizeof (int));
-      DALLOC (ctx->band.offset, offset.size () * sizeof (long long));
-      CK (cudaMemcpyAsync (ctx->band.boxes, boxes.data (), boxes.size () * sizeof (int), cudaMemcpyHostToDevice,
+      DALLOC (ctx->band.boxes, boxes.size () * sizeof (BandBox));
+      CK (cudaMemcpyAsync (ctx->band.boxes, boxes.data (), boxes.size () * sizeof (BandBox), cudaMemcpyHostToDevice,
                            ctx->stream));
-      CK (cudaMemcpyAsync (ctx->band.offset, offset.data (), offset.size () * sizeof (long long),
-                           cudaMemcpyHostToDevice, ctx->stream));
+      DALLOC (ctx->band.blk, blk.size () * sizeof (int2));
+      CK (cudaMemcpyAsync (ctx->band.blk, blk.data (), blk.size () * sizeof (int2), cudaMemcpyHostToDevice,
+                           ctx->stream));
+      ctx->band.nblk = (int) blk.size ();
       CK (cudaStreamSynchronize (ctx->stream));
-      ctx->band.nbox = (int) boxes.size () / 6;
-      ctx->band.cells = offset.back ();
+      ctx->band.nbox = (int) boxes.size ();
+      long long cells = 0;
+      for (const BandBox &bb : boxes)
+        cells += (long long) (bb.hi[0] - bb.lo[0]) * (bb.hi[1] - bb.lo[1]) * (bb.hi[2] - bb.lo[2]);
+      ctx->band.cells = cells;
     }
   }
   ctx->fused.tfsf_post = ctx->band.cells > 0 ? 1 : 0;   // read only by the sweep kernels

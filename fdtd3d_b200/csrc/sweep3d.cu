@@ -1075,27 +1075,70 @@ __global__ void __launch_bounds__ (32 * WY, 1)
 
 // ------------------------------------------------------ TF/SF post pass
 
+// Sum of the TF/SF terms of component k in mask m at (x, y, z): the terms
+// of tfsf_curl that cover the cell, in the same order, without the box tests.
+__device__ __forceinline__ float tfsf_terms (const FusedParams &p, int k, unsigned m, const double *inc, int *err,
+                                             int x, int y, int z)
+{
+  const CompDev &c = p.comp[k];
+  float d = 0.f;
+#pragma unroll
+  for (int t = 0; t < kMaxTerms; ++t)
+    if ((m >> t) & 1u)
+    {
+      const TermDev &tm = c.term[t];
+      const double diff =
+          inc_at (p.g, inc, p.inc_len, err, tm.inc_comp, x + tm.aux[0], y + tm.aux[1], z + tm.aux[2]);
+      const float dv = (float) (diff * tm.negate) * p.inc_scale[tm.inc_comp];
+      d += (tm.slot == 0 || tm.slot == 3) ? dv : -dv;
+    }
+  return d;
+}
+
+// Cell of band box b taken by this thread (false past the box's end).
+__device__ __forceinline__ bool band_cell (const BandBox &b, int first, int &x, int &y, int &z)
+{
+  const unsigned ez = (unsigned) (b.hi[2] - b.lo[2]), ey = (unsigned) (b.hi[1] - b.lo[1]);
+  const unsigned n = ez * ey * (unsigned) (b.hi[0] - b.lo[0]);
+  const unsigned r = (unsigned) first + threadIdx.x;
+  if (r >= n)
+    return false;
+  const unsigned q = r / ez;
+  z = b.lo[2] + (int) (r - q * ez);
+  y = b.lo[1] + (int) (q % ey);
+  x = b.lo[0] + (int) (q / ey);
+  return true;
+}
+
 // The sweep ran without TF/SF, so on the band around the faces its E_new
 // lacks (S im) dE for every corrected E cell and its H_new lacks
 // S (curl of that dE + the H-side correction).  Both are linear in the
 // correction, so adding them afterwards gives the corrected step (PML-free
-// cells only, which the host guarantees).  One thread per band cell
-// touches only its own cell; the E corrections of neighbours are recomputed,
-// never read, so there are no races.
+// cells only, which the host guarantees).  One thread per band cell touches
+// only its own cell; the E corrections of the +x / +y / +z neighbours are
+// recomputed from the box's neighbour masks, never read, so there are no
+// races.
 template <typename T>
-__global__ void __launch_bounds__ (256) tfsf_post_kernel (const __grid_constant__ FusedParams p, const int *boxes,
-                                                          const long long *offset, int nbox, long long cells, int *err)
+__global__ void __launch_bounds__ (256) tfsf_post_kernel (const __grid_constant__ FusedParams p, const BandBox *boxes,
+                                                          const int2 *blk, int *err)
 {
+  const int2 bk = blk[blockIdx.x];
+  const BandBox b = boxes[bk.x];
+  int x, y, z;
+  if (!band_cell (b, bk.y, x, y, z))
+    return;
   const int nx = p.g.n[0], ny = p.g.n[1], nz = p.g.n[2];
   const size_t sx = (size_t) ny * nz;
   const float S = p.courant;
-  // correction of E component k at (cx, cy, cz): zero off the updated interior and on the source
-  auto de = [&] (int k, int cx, int cy, int cz) -> float {
-    if (cx < 1 || cx > nx - 2 || cy < 1 || cy > ny - 2 || cz < 1 || cz > nz - 2)
+  // correction of E component k at (cx, cy, cz) from its terms in mask m:
+  // zero where the step does not update the cell and on the point source
+  // (band cells and their neighbours are >= 1 on every axis)
+  auto de = [&] (int k, unsigned m, int cx, int cy, int cz) -> float {
+    if (!m || cx > nx - 2 || cy > ny - 2 || cz > nz - 2)
       return 0.f;
     if (((p.ps_mask >> k) & 1) && cx == p.ps[0] && cy == p.ps[1] && cz == p.ps[2])
       return 0.f;
-    const float d = tfsf_curl (p, k, p.inc_h, err, cx, cy, cz);
+    const float d = tfsf_terms (p, k, m, p.inc_h, err, cx, cy, cz);
     if (d == 0.f)
       return 0.f;
     float im = 1.f;
@@ -1107,49 +1150,34 @@ __global__ void __launch_bounds__ (256) tfsf_post_kernel (const __grid_constant_
     }
     return (S * im) * d;
   };
-  for (long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x; t < cells;
-       t += (long long) gridDim.x * blockDim.x)
-  {
-    int lo = 0, hi = nbox;
-    while (hi - lo > 1)
+  auto em = [] (unsigned mask, int k) { return (mask >> (4 * k)) & 15u; };
+  const size_t id = (size_t) x * sx + (size_t) y * nz + z;
+  const float d0 = de (0, em (b.mask, 0), x, y, z), d1 = de (1, em (b.mask, 1), x, y, z),
+              d2 = de (2, em (b.mask, 2), x, y, z);
+  const float dd[3] = {d0, d1, d2};
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    if (dd[k] != 0.f)
     {
-      const int mid = (lo + hi) >> 1;
-      if (offset[mid] <= t)
-        lo = mid;
-      else
-        hi = mid;
+      T *f = reinterpret_cast<T *> (p.e_new[k]) + id;
+      *f = (T) ((float) *f + dd[k]);
     }
-    const int *b = boxes + 6 * lo;
-    long long r = t - offset[lo];
-    const int ez = b[5] - b[2], ey = b[4] - b[1];
-    const int z = b[2] + (int) (r % ez);
-    r /= ez;
-    const int y = b[1] + (int) (r % ey);
-    r /= ey;
-    const int x = b[0] + (int) r;
-    const size_t id = (size_t) x * sx + (size_t) y * nz + z;
-    const float d0 = de (0, x, y, z), d1 = de (1, x, y, z), d2 = de (2, x, y, z);
-    const float dd[3] = {d0, d1, d2};
+  const unsigned hm[3] = {em (b.mask, 3), em (b.mask, 4), em (b.mask, 5)};
+  const float a[3] = {
+      (de (1, em (b.nmask[2], 1), x, y, z + 1) - d1) - (de (2, em (b.nmask[1], 2), x, y + 1, z) - d2) +
+          (hm[0] ? tfsf_terms (p, 3, hm[0], p.inc_e, err, x, y, z) : 0.f),
+      (de (2, em (b.nmask[0], 2), x + 1, y, z) - d2) - (de (0, em (b.nmask[2], 0), x, y, z + 1) - d0) +
+          (hm[1] ? tfsf_terms (p, 4, hm[1], p.inc_e, err, x, y, z) : 0.f),
+      (de (0, em (b.nmask[1], 0), x, y + 1, z) - d0) - (de (1, em (b.nmask[0], 1), x + 1, y, z) - d1) +
+          (hm[2] ? tfsf_terms (p, 5, hm[2], p.inc_e, err, x, y, z) : 0.f)};
+  const bool at_src = x == p.ps[0] && y == p.ps[1] && z == p.ps[2];
 #pragma unroll
-    for (int k = 0; k < 3; ++k)
-      if (dd[k] != 0.f)
-      {
-        T *f = reinterpret_cast<T *> (p.e_new[k]) + id;
-        *f = (T) ((float) *f + dd[k]);
-      }
-    const float a[3] = {
-        (de (1, x, y, z + 1) - d1) - (de (2, x, y + 1, z) - d2) + tfsf_curl (p, 3, p.inc_e, err, x, y, z),
-        (de (2, x + 1, y, z) - d2) - (de (0, x, y, z + 1) - d0) + tfsf_curl (p, 4, p.inc_e, err, x, y, z),
-        (de (0, x, y + 1, z) - d0) - (de (1, x + 1, y, z) - d1) + tfsf_curl (p, 5, p.inc_e, err, x, y, z)};
-    const bool at_src = x == p.ps[0] && y == p.ps[1] && z == p.ps[2];
-#pragma unroll
-    for (int m = 0; m < 3; ++m)
-      if (a[m] != 0.f && !(at_src && ((p.ps_mask >> (3 + m)) & 1)))
-      {
-        T *f = reinterpret_cast<T *> (p.h_new[m]) + id;
-        *f = (T) ((float) *f + S * a[m]);
-      }
-  }
+  for (int m = 0; m < 3; ++m)
+    if (a[m] != 0.f && !(at_src && ((p.ps_mask >> (3 + m)) & 1)))
+    {
+      T *f = reinterpret_cast<T *> (p.h_new[m]) + id;
+      *f = (T) ((float) *f + S * a[m]);
+    }
 }
 
 }  // namespace
@@ -1366,7 +1394,7 @@ int launch_sweep3d (const SweepPlan &plan, int set, const FusedParams &p, int *e
 
 namespace fdtdb {
 
-std::string tfsf_band_boxes (const FusedParams &p, std::vector<int> &boxes, std::vector<long long> &offset)
+std::string tfsf_band_boxes (const FusedParams &p, std::vector<BandBox> &boxes, std::vector<int2> &blk)
 {
   struct Box
   {
@@ -1394,11 +1422,12 @@ std::string tfsf_band_boxes (const FusedParams &p, std::vector<int> &boxes, std:
           add (p.comp[k].term[t], a);
     }
   boxes.clear ();
-  offset.assign (1, 0);
+  blk.clear ();
   if (cand.empty ())
     return "";
-  // disjoint cover: compress coordinates, mark covered elementary boxes,
-  // merge runs along z
+  // disjoint cover: compress coordinates (every term box edge is a cut, so
+  // an elementary box lies wholly inside or outside each term), keep the
+  // covered elementary boxes, merge runs along z with equal term masks
   std::vector<int> cut[3];
   for (const Box &b : cand)
     for (int a = 0; a < 3; ++a)
@@ -1412,54 +1441,98 @@ std::string tfsf_band_boxes (const FusedParams &p, std::vector<int> &boxes, std:
     cut[a].erase (std::unique (cut[a].begin (), cut[a].end ()), cut[a].end ());
   }
   const size_t mx = cut[0].size () - 1, my = cut[1].size () - 1, mz = cut[2].size () - 1;
+  // the elementary box (i, j, l), moved by +1 along axis sh (-1: not moved),
+  // inside the box lo .. hi - 1
+  auto inside = [&] (const int lo[3], const int hi[3], size_t i, size_t j, size_t l, int sh = -1) {
+    const size_t ix[3] = {i, j, l};
+    for (int a = 0; a < 3; ++a)
+    {
+      const int d = a == sh ? 1 : 0;
+      if (cut[a][ix[a]] + d < lo[a] || cut[a][ix[a] + 1] + d > hi[a])
+        return false;
+    }
+    return true;
+  };
+  auto covered = [&] (size_t i, size_t j, size_t l) {
+    for (const Box &b : cand)
+      if (inside (b.lo, b.hi, i, j, l))
+        return true;
+    return false;
+  };
+  // term masks of the elementary box (every component) or of the box moved
+  // by +1 along sh (E components only); uniform over the box because the
+  // term boxes and the E term boxes moved by -1 along each axis are all cut
+  auto mask_of = [&] (size_t i, size_t j, size_t l, int sh = -1) {
+    unsigned m = 0;
+    for (int k = 0; k < (sh < 0 ? 6 : 3); ++k)
+      for (int t = 0; t < p.comp[k].nterms; ++t)
+        if (inside (p.comp[k].term[t].lo, p.comp[k].term[t].hi, i, j, l, sh))
+          m |= 1u << (4 * k + t);
+    return m;
+  };
+  auto masks_of = [&] (size_t i, size_t j, size_t l, unsigned m[4]) {
+    m[0] = mask_of (i, j, l);
+    for (int a = 0; a < 3; ++a)
+      m[1 + a] = mask_of (i, j, l, a);
+  };
+  auto same = [] (const unsigned u[4], const unsigned v[4]) {
+    return u[0] == v[0] && u[1] == v[1] && u[2] == v[2] && u[3] == v[3];
+  };
   for (size_t i = 0; i < mx; ++i)
     for (size_t j = 0; j < my; ++j)
     {
       size_t l = 0;
       while (l < mz)
       {
-        auto covered = [&] (size_t ll) {
-          for (const Box &b : cand)
-            if (cut[0][i] >= b.lo[0] && cut[0][i + 1] <= b.hi[0] && cut[1][j] >= b.lo[1] && cut[1][j + 1] <= b.hi[1] &&
-                cut[2][ll] >= b.lo[2] && cut[2][ll + 1] <= b.hi[2])
-              return true;
-          return false;
-        };
-        if (!covered (l))
+        if (!covered (i, j, l))
         {
           ++l;
           continue;
         }
+        unsigned m[4], me[4];
+        masks_of (i, j, l, m);
         size_t e = l + 1;
-        while (e < mz && covered (e))
+        while (e < mz && covered (i, j, e) && (masks_of (i, j, e, me), same (m, me)))
           ++e;
-        const int bx[6] = {cut[0][i], cut[1][j], cut[2][l], cut[0][i + 1], cut[1][j + 1], cut[2][e]};
+        BandBox bb;
+        bb.lo[0] = cut[0][i];
+        bb.lo[1] = cut[1][j];
+        bb.lo[2] = cut[2][l];
+        bb.hi[0] = cut[0][i + 1];
+        bb.hi[1] = cut[1][j + 1];
+        bb.hi[2] = cut[2][e];
+        bb.mask = m[0];
+        for (int a = 0; a < 3; ++a)
+          bb.nmask[a] = m[1 + a];
+        // a band cell must not be a PML cell of any component
         for (int k = 0; k < 6; ++k)
-        {
-          // a band cell must not be a PML cell of any component
           for (int a = 0; a < 3; ++a)
-            if (p.use_pml && (bx[a] < p.ilo[k][a] || bx[3 + a] > p.ihi[k][a]))
+            if (p.use_pml && (bb.lo[a] < p.ilo[k][a] || bb.hi[a] > p.ihi[k][a]))
               return "the TF/SF band reaches into the PML";
-        }
-        boxes.insert (boxes.end (), bx, bx + 6);
-        offset.push_back (offset.back () + (long long) (bx[3] - bx[0]) * (bx[4] - bx[1]) * (bx[5] - bx[2]));
+        boxes.push_back (bb);
         l = e;
       }
     }
+  for (size_t q = 0; q < boxes.size (); ++q)
+  {
+    const BandBox &bb = boxes[q];
+    const long long cells = (long long) (bb.hi[0] - bb.lo[0]) * (bb.hi[1] - bb.lo[1]) * (bb.hi[2] - bb.lo[2]);
+    if (cells >= (1ll << 31))
+      return "TF/SF band box too large";
+    for (long long f = 0; f < cells; f += 256)
+      blk.push_back (make_int2 ((int) q, (int) f));
+  }
   return "";
 }
 
 int launch_tfsf_post (const TfsfBand &band, const FusedParams &p, int *err, cudaStream_t s)
 {
-  if (band.cells <= 0)
+  if (band.cells <= 0 || band.nblk <= 0)
     return 0;
-  long long blocks = (band.cells + 255) / 256;
-  if (blocks > 148 * 16)
-    blocks = 148 * 16;
   if (p.fp16)
-    tfsf_post_kernel<__half><<<(unsigned) blocks, 256, 0, s>>> (p, band.boxes, band.offset, band.nbox, band.cells, err);
+    tfsf_post_kernel<__half><<<band.nblk, 256, 0, s>>> (p, band.boxes, band.blk, err);
   else
-    tfsf_post_kernel<float><<<(unsigned) blocks, 256, 0, s>>> (p, band.boxes, band.offset, band.nbox, band.cells, err);
+    tfsf_post_kernel<float><<<band.nblk, 256, 0, s>>> (p, band.boxes, band.blk, err);
   return 1;
 }
 

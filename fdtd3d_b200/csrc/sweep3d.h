@@ -66,24 +66,33 @@ int launch_sweep3d (const SweepPlan &plan, int set, const FusedParams &p, int *e
 
 namespace fdtdb {
 
-// TF/SF post pass of the sweep: the cells within one cell of a TF/SF face,
-// as disjoint boxes with running cell offsets (device arrays).
+// TF/SF post pass of the sweep: the cells within one cell of a TF/SF face
+// as disjoint boxes.  Every TF/SF term covers a box whole or misses it, so
+// the terms that act on a box are one mask per component.
+struct BandBox
+{
+  int lo[3], hi[3];            // cells lo .. hi - 1 per axis
+  unsigned mask;               // bit 4k + t: term t of component k (Ex..Hz) covers the box
+  unsigned nmask[3];           // the same for Ex..Ez over the box moved by +1 along x, y, z
+};
+
 struct TfsfBand
 {
   int nbox = 0;
   long long cells = 0;
-  int *boxes = nullptr;         // nbox x {lo0, lo1, lo2, hi0, hi1, hi2}
-  long long *offset = nullptr;  // nbox + 1 running cell counts
+  BandBox *boxes = nullptr;    // device array
+  int nblk = 0;                // CTAs of the post pass
+  int2 *blk = nullptr;         // per CTA: the box and the first of its cells the CTA takes
 };
 
 // Host part: the band's boxes from the TF/SF terms (E terms and their
-// -x/-y/-z neighbours, H terms), made disjoint.  Returns "" when the post
-// pass can serve the geometry (no band cell is a PML cell of any
-// component), else the reason; fills host vectors for the caller to upload.
-std::string tfsf_band_boxes (const FusedParams &p, std::vector<int> &boxes, std::vector<long long> &offset);
+// -x/-y/-z neighbours, H terms) with their term masks, and the CTA table.
+// Returns "" when the post pass can serve the geometry (no band cell is a
+// PML cell of any component), else the reason.
+std::string tfsf_band_boxes (const FusedParams &p, std::vector<BandBox> &boxes, std::vector<int2> &blk);
 
 // Adds the TF/SF corrections to the new E and H buffers after a sweep step
-// that ran with tfsf_post = 1.
+// that ran with tfsf_post = 1 (one launch; returns how many).
 int launch_tfsf_post (const TfsfBand &band, const FusedParams &p, int *err, cudaStream_t s);
 
 }  // namespace fdtdb
