@@ -53,7 +53,7 @@ TFSF = 32
 
 def kernel_label(step_kernel: str) -> str:
     if step_kernel == "sweep3d_tma":
-        return ("sweep3d_kernel (lean / z-edge PML / full item classes) + tfsf_post_kernel: "
+        return ("sweep3d_kernel (lean / z-edge PML / PML / full item classes) + tfsf_post_kernel: "
                 "E and H of one time step")
     return f"{step_kernel}: E and H of one time step"
 

@@ -590,7 +590,7 @@ int plan_sweep (fdtd_ctx *ctx)
   if (const char *v = std::getenv ("FDTDB_SWEEP_LEAN"))
     lean = std::atoi (v) != 0;
   if (!ctx->sweep_ctr)
-    DALLOC (ctx->sweep_ctr, 6 * sizeof (unsigned long long));
+    DALLOC (ctx->sweep_ctr, 8 * sizeof (unsigned long long));
   void *e[2][3], *h[2][3];
   float *aux[2][6];
   for (int b = 0; b < 2; ++b)
@@ -654,9 +654,10 @@ int plan_sweep (fdtd_ctx *ctx)
     {
       const SweepWork &w = ctx->sweep.work;
       std::fprintf (stderr, "sweep3d: %s wy=%d ctas=%d smem=%u tiles z=%d y=%d chunks=%d (x chunk %d) items=%d "
-                    "items lean/z-edge/full=%d/%d/%d tfsf band boxes=%d cells=%lld\n",
+                    "items lean/z-edge/full/PML=%d/%d/%d/%d tfsf band boxes=%d cells=%lld\n",
                     why.empty () ? "in use" : why.c_str (), ctx->sweep.wy, ctx->sweep.ctas, ctx->sweep.smem, w.nzt,
-                    w.nyt, w.nch, w.chunk, w.nitems, ctx->sweep.items[0], ctx->sweep.items[1], ctx->sweep.items[2], ctx->band.nbox, ctx->band.cells);
+                    w.nyt, w.nch, w.chunk, w.nitems, ctx->sweep.items[0], ctx->sweep.items[1], ctx->sweep.items[2], ctx->sweep.items[3],
+                    ctx->band.nbox, ctx->band.cells);
     }
   return FDTD_OK;
 }

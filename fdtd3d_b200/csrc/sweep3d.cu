@@ -370,9 +370,10 @@ __device__ __forceinline__ void zedge_vec (const float *tz, int col, float S, un
 // ------------------------------------------------------------ item classes
 
 // Class of work item `item` (the kernel instantiation that runs it):
-//   2 (full): TF/SF corrections inside the sweep, a point source on a plane
-//     the item updates (E on x = xa .. xb + 1, H on x = xa .. xb), or a PML
-//     cell of any component off the z edges of the tile;
+//   2 (full): TF/SF corrections inside the sweep, or a point source on a
+//     plane the item updates (E on x = xa .. xb + 1, H on x = xa .. xb);
+//   3 (PML): otherwise, a PML cell of any component off the z edges of the
+//     tile (full-width auxiliary boxes on every plane);
 //   1 (z edge): PML cells only in z columns that one narrow window of the
 //     tile holds (the ring column included), x and y interior;
 //   0 (lean): none of these.
@@ -398,7 +399,7 @@ __host__ __device__ inline int sweep_item_class (const FusedParams &p, const Swe
   {
     const int xhi = k < 3 ? (xb + 1 < nx - 2 ? xb + 1 : nx - 2) : xb;
     if (xa < p.ilo[k][0] || xhi >= p.ihi[k][0] || y0 < p.ilo[k][1] || yhi >= p.ihi[k][1])
-      return 2;
+      return 3;
   }
   // z: updated columns cmin .. cmax of the tile against the common interior
   int zin_lo = 0, zin_hi = nz;
@@ -415,19 +416,21 @@ __host__ __device__ inline int sweep_item_class (const FusedParams &p, const Swe
   if (!zlow && !zhigh)
     return 0;
   if (zlow && zhigh)
-    return 2;
+    return 3;
   const int az0 = (zlow ? cmin : hi_beg) & ~3;
   const int width = (zlow ? lo_end : cmax + 1) - az0;
-  return width <= 32 ? 1 : 2;
+  return width <= 32 ? 1 : 3;
 }
 
 // ------------------------------------------------------------------ kernel
 
 // MODE (item class, see sweep_item_class): 0 = lean, no PML cell, point
 // source or in-sweep TF/SF (straight-line planes); 1 = z edge, PML cells
-// only in the z columns of one narrow window; 2 = full.  Classes 0 and 1
-// unroll the plane loop by the stage count (compile-time stage indices).
-// Each instantiation takes only its own items from its own counter.
+// only in the z columns of one narrow window; 3 = PML anywhere, full-width
+// auxiliary boxes on every plane; 2 = full (in-sweep TF/SF, point sources,
+// auxiliary box width chosen per plane).  Classes 0, 1 and 3 unroll the
+// plane loop by the stage count (compile-time stage indices).  Each
+// instantiation takes only its own items from its own counter.
 template <typename T, int WY, int MODE>
 __global__ void __launch_bounds__ (32 * WY, 1)
     sweep3d_kernel (const __grid_constant__ SweepMaps maps, const __grid_constant__ FusedParams p,
@@ -579,8 +582,8 @@ __global__ void __launch_bounds__ (32 * WY, 1)
     {
 #pragma unroll
       for (int k = 0; k < NST; ++k)
-        issue (k, xa - 1 + k, z0, y0, MODE == 0 ? 0 : (MODE == 1 ? 1 : aux_mode (xa - 1 + k, y0, zpml, nar_ok)),
-               az0);
+        issue (k, xa - 1 + k, z0, y0,
+               MODE == 0 ? 0 : (MODE == 1 ? 1 : (MODE == 3 ? 2 : aux_mode (xa - 1 + k, y0, zpml, nar_ok))), az0);
     }
     // PML coefficient pairs of this item (read after the first plane's barrier)
     if (MODE == 1 && p.use_pml)
@@ -596,7 +599,7 @@ __global__ void __launch_bounds__ (32 * WY, 1)
         Tab[(2 * k + 1) * PW + col] = c1;
       }
     }
-    else if (MODE == 2 && p.use_pml)
+    else if ((MODE == 2 || MODE == 3) && p.use_pml)
     {
       for (int q = tid; q < 6 * 2 * PW; q += 32 * WY)
       {
@@ -664,7 +667,7 @@ __global__ void __launch_bounds__ (32 * WY, 1)
           atomicOr (err, 4);
         }
         phase ^= 1u << st;
-        const int amode = kFull ? aux_mode (x, y0, zpml, nar_ok) : (MODE == 1 ? 1 : 0);
+        const int amode = kFull ? aux_mode (x, y0, zpml, nar_ok) : (MODE == 1 ? 1 : (MODE == 3 ? 2 : 0));
         const int apitch = amode == 2 ? PW : AN;
         const int acol = amode == 2 ? zl : zl - az0;      // only read on lanes with PML cells
         const unsigned char *stg = smem + st * L::STAGE;
@@ -916,7 +919,8 @@ __global__ void __launch_bounds__ (32 * WY, 1)
           return false;
         }
         if (leader && i + NST < np)
-          issue (st, x + NST, z0, y0, MODE == 0 ? 0 : (MODE == 1 ? 1 : aux_mode (x + NST, y0, zpml, nar_ok)), az0);
+          issue (st, x + NST, z0, y0,
+                 MODE == 0 ? 0 : (MODE == 1 ? 1 : (MODE == 3 ? 2 : aux_mode (x + NST, y0, zpml, nar_ok))), az0);
 
         if (i > 1 && own_row)
         {
@@ -1260,9 +1264,12 @@ std::string plan_t (SweepPlan &pl, const FusedParams &p, void *const e[2][3], vo
     }
   }
   int per_sm = 0;
-  for (int mode = 0; mode < 3; ++mode)
+  for (int mode = 0; mode < 4; ++mode)
   {
-    auto kern = mode == 0 ? sweep3d_kernel<T, WY, 0> : (mode == 1 ? sweep3d_kernel<T, WY, 1> : sweep3d_kernel<T, WY, 2>);
+    auto kern = mode == 0   ? sweep3d_kernel<T, WY, 0>
+                : mode == 1 ? sweep3d_kernel<T, WY, 1>
+                : mode == 2 ? sweep3d_kernel<T, WY, 2>
+                            : sweep3d_kernel<T, WY, 3>;
     if (cudaFuncSetAttribute (kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) L::TOTAL) != cudaSuccess)
     {
       cudaGetLastError ();
@@ -1290,6 +1297,11 @@ int launch_t (const SweepPlan &pl, int set, const FusedParams &p, int *err, cuda
   if (pl.items[2] > 0)
   {
     sweep3d_kernel<T, WY, 2><<<pl.ctas, dim3 (32, WY), sm, s>>> (pl.maps[set], p, pl.work, err);
+    ++n;
+  }
+  if (pl.items[3] > 0)
+  {
+    sweep3d_kernel<T, WY, 3><<<pl.ctas, dim3 (32, WY), sm, s>>> (pl.maps[set], p, pl.work, err);
     ++n;
   }
   if (pl.items[1] > 0)
@@ -1375,7 +1387,7 @@ std::string sweep3d_plan (SweepPlan &plan, const FusedParams &p, void *const e[2
   plan.work.ctr = ctr;
   plan.work.lean = lean ? 1 : 0;
   const bool tfsf_in = p.use_tfsf && !p.tfsf_post;
-  plan.items[0] = plan.items[1] = plan.items[2] = 0;
+  plan.items[0] = plan.items[1] = plan.items[2] = plan.items[3] = 0;
   for (int it = 0; it < plan.work.nitems; ++it)
     ++plan.items[sweep_item_class (p, plan.work, wy, it, tfsf_in)];
   if (plan.ctas > plan.work.nitems)

@@ -41,7 +41,7 @@ struct SweepPlan
   int wy = 0;                  // warps per CTA, one y row each (last row = ring)
   int ctas = 0;                // persistent CTAs
   unsigned smem = 0;           // dynamic shared memory per CTA
-  int items[3] = {0, 0, 0};    // items per class: lean, z-edge PML, full
+  int items[4] = {0, 0, 0, 0}; // items per class: lean, z-edge PML, full, PML
   SweepWork work{};
   SweepMaps maps[2];           // maps[b]: buffer set b as the old set
 };
