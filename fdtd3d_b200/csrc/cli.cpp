@@ -8,15 +8,23 @@
 // around the step loop (Source/main.cpp:1175-1213) and --save-as-txt dumps
 // named previous-1_[timestep=T]_[pid=0]_[name=F].txt with 15 significant
 // digits (Source/File-Management/Commons.h:63-120,
-// Source/File-Management/Dumper/TXTDumper.h:60-84).  The default save region
+// Source/File-Management/Dumper/TXTDumper.h:60-84).  --save-as-dat writes the
+// same region as raw FP64 values, z fastest, to previous-1_[...].dat
+// (Source/File-Management/Dumper/DATDumper.h:52-90); the reference's DAT
+// dumper names one file but opens the second name and writes nothing
+// (DATDumper.h:129 passes the time level as the file count), so this takes
+// the TXT dumper's naming, the evident intent.  Material files load by
+// extension like GridFileManager::getFileType (Commons.cpp:46-67): .txt
+// through the TXT loader, .dat as raw FP64 values of the whole grid, z
+// fastest, with nothing after them (DATLoader.h:52-90).  The default save region
 // is the reference's: the whole grid, one z slice at size/2 in 3-D
 // (Source/Scheme/SchemeHelper.h:870-889).  The --same-size* flags copy x
 // to y and z at the point where they are parsed, so a later coordinate flag
 // overrides them (Source/Settings/Settings.cpp:249-261).
 //
 // Extra flag: --precision fp64|fp32|fp16s (default fp64 = the plain form).
-// Flags of subsystems outside the step path (MPI, NTFF, BMP/DAT output,
-// test callbacks) are rejected with a message instead of being ignored.
+// Flags of subsystems outside the step path (MPI, NTFF, BMP output, test
+// callbacks) are rejected with a message instead of being ignored.
 #include <sys/time.h>
 
 #include <cmath>
@@ -39,7 +47,7 @@ struct Opts
 {
   fdtd_config cfg;
   int steps = 100;
-  bool save_res = false, save_txt = false, manual = false;
+  bool save_res = false, save_txt = false, save_dat = false, manual = false;
   int save_start[3] = {0, 0, 0}, save_end[3] = {0, 0, 0};
   std::string mat_file[6];
   int device = 0;
@@ -192,6 +200,8 @@ int parse (std::vector<std::string> args, Opts &o)
       o.save_res = true;
     else if (a == "--save-as-txt")
       o.save_txt = true;
+    else if (a == "--save-as-dat")
+      o.save_dat = true;
     else if (a == "--manual-save-coords")
       o.manual = true;
     else if (a == "--save-start-coord" && next (v))
@@ -282,6 +292,49 @@ bool load_txt (const std::string &path, size_t n, int coords, std::vector<double
   return i == n;
 }
 
+// DAT grid loader: raw FP64 values of the whole grid, z fastest, and
+// nothing after them (Source/File-Management/Loader/DATLoader.h:52-90).
+bool load_dat (const std::string &path, size_t n, std::vector<double> &out)
+{
+  std::ifstream f (path, std::ios::binary);
+  if (!f)
+    return false;
+  out.assign (n, 0.0);
+  f.read (reinterpret_cast<char *> (out.data ()), (std::streamsize) (n * sizeof (double)));
+  if (!f || (size_t) f.gcount () != n * sizeof (double))
+    return false;
+  f.peek ();
+  return f.eof ();
+}
+
+// Material file by extension (GridFileManager::getFileType, Commons.cpp:46-67).
+bool load_material (const std::string &path, size_t n, int coords, std::vector<double> &out, std::string &why)
+{
+  const size_t dot = path.find_last_of ('.');
+  const std::string ext = dot == std::string::npos ? "" : path.substr (dot + 1);
+  if (ext == "txt")
+    return load_txt (path, n, coords, out) || (why = "cannot read " + path, false);
+  if (ext == "dat")
+    return load_dat (path, n, out) || (why = "cannot read " + path + " (expects " + std::to_string (n) +
+                                               " FP64 values)", false);
+  why = path + ": material files are .txt or .dat";
+  return false;
+}
+
+bool save_dat (const std::string &name, const std::vector<double> &v, const int n[3], const int lo[3], const int hi[3])
+{
+  std::ofstream f (name, std::ios::binary);
+  if (!f)
+    return false;
+  for (int x = lo[0]; x < hi[0]; ++x)
+    for (int y = lo[1]; y < hi[1]; ++y)
+    {
+      const size_t id = ((size_t) x * n[1] + y) * n[2] + lo[2];
+      f.write (reinterpret_cast<const char *> (v.data () + id), (std::streamsize) ((hi[2] - lo[2]) * sizeof (double)));
+    }
+  return (bool) f;
+}
+
 bool save_txt (const std::string &name, const std::vector<double> &v, const int n[3], bool tmz, const int lo[3],
                const int hi[3])
 {
@@ -322,8 +375,9 @@ int main (int argc, char **argv)
     if (o.mat_file[m].empty ())
       continue;
     std::vector<double> a;
-    if (!load_txt (o.mat_file[m], cells, tmz ? 2 : 3, a))
-      return fail ("cannot read " + o.mat_file[m]);
+    std::string why;
+    if (!load_material (o.mat_file[m], cells, tmz ? 2 : 3, a, why))
+      return fail (why);
     st = fdtd_upload_material (ctx, m, a.data ());
     if (st)
       return fail (std::string ("fdtd_upload_material: ") + fdtd_last_error ());
@@ -338,7 +392,7 @@ int main (int argc, char **argv)
     return fail (std::string ("step: ") + fdtd_status_str (st) + ": " + fdtd_last_error ());
   std::printf ("Total time = %f seconds\n",
                (double) (tv2.tv_usec - tv1.tv_usec) / 1000000 + (double) (tv2.tv_sec - tv1.tv_sec));
-  if (o.save_res && o.save_txt)
+  if (o.save_res && (o.save_txt || o.save_dat))
   {
     static const char *names[6] = {"Ex", "Ey", "Ez", "Hx", "Hy", "Hz"};
     int lo[3] = {0, 0, 0}, hi[3] = {n[0], n[1], n[2]};
@@ -368,9 +422,11 @@ int main (int argc, char **argv)
       st = fdtd_download_field (ctx, k, buf.data ());
       if (st)
         return fail (std::string ("download: ") + fdtd_last_error ());
-      std::string fname = "previous-1_[timestep=" + std::to_string (o.steps) + "]_[pid=0]_[name=" + names[k] + "].txt";
-      if (!save_txt (fname, buf, n, tmz, lo, hi))
-        return fail ("cannot write " + fname);
+      const std::string base = "previous-1_[timestep=" + std::to_string (o.steps) + "]_[pid=0]_[name=" + names[k] + "]";
+      if (o.save_txt && !save_txt (base + ".txt", buf, n, tmz, lo, hi))
+        return fail ("cannot write " + base + ".txt");
+      if (o.save_dat && !save_dat (base + ".dat", buf, n, lo, hi))
+        return fail ("cannot write " + base + ".dat");
     }
   }
   fdtd_destroy (ctx);

@@ -209,3 +209,51 @@ def test_cli_dropin_matches_reference_txt(fdtd, tmp_path):
         if mine != text:
             diffs = [(a, b) for a, b in zip(text.splitlines(), mine.splitlines()) if a != b]
             raise AssertionError(f"{fname}: {len(diffs)} lines differ, first: {diffs[:4]}")
+
+
+def test_cli_dat_output_and_material_files(fdtd, tmp_path):
+    """--save-as-dat writes the values of the TXT dump as raw FP64 (z fastest)
+    under the same name with .dat; a permittivity map gives the same run from
+    a .txt file (the reference's TXT loader) and from a .dat file (raw FP64);
+    a partial save region is the matching sub-block; a .dat of the wrong size
+    and an unknown extension are refused."""
+    import subprocess
+
+    from oracle.oracle import write_material_txt
+
+    cli = os.path.join(os.path.dirname(fdtd.__file__), "fdtd3d-b200")
+    n = (14, 12, 16)
+    rng = np.random.default_rng(7)
+    eps = np.where(rng.random(n) < 0.3, 4.0, 1.0)   # exact in FP32, as the TXT loader's stof keeps it
+    write_material_txt(str(tmp_path / "eps.txt"), eps)
+    eps.astype(np.float64).tofile(str(tmp_path / "eps.dat"))
+    eps[:2].astype(np.float64).tofile(str(tmp_path / "short.dat"))
+    (tmp_path / "eps.bin").write_bytes(b"")
+    flags = ["--3d", "--size", "x:14,y:12,z:16", "--use-pml", "--pml-size", "x:2", "--same-size-pml",
+             "--use-tfsf", "--tfsf-size-left", "x:4", "--same-size-tfsf", "--tfsf-size-right", "x:4",
+             "--angle-teta", "30", "--angle-phi", "45", "--angle-psi", "10", "--time-steps", "15",
+             "--save-res", "--save-as-txt", "--save-as-dat", "--manual-save-coords"]
+    full = ["--save-start-coord", "x:0,y:0,z:0", "--save-end-coord", "x:14,y:12,z:16"]
+    part = ["--save-start-coord", "x:1,y:2,z:3", "--save-end-coord", "x:10,y:9,z:11"]
+
+    def run(name, mat, region, ok=True):
+        d = tmp_path / name
+        d.mkdir()
+        r = subprocess.run([cli] + flags + region + ["--load-eps-from-file", str(tmp_path / mat)], cwd=d,
+                           capture_output=True, text=True, timeout=300)
+        assert (r.returncode == 0) == ok, r.stdout + r.stderr
+        return d
+
+    a, b, c = run("txt", "eps.txt", full), run("dat", "eps.dat", full), run("part", "eps.txt", part)
+    run("short", "short.dat", full, ok=False)
+    run("ext", "eps.bin", full, ok=False)
+    for comp in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+        name = f"previous-1_[timestep=15]_[pid=0]_[name={comp}]"
+        va = np.fromfile(str(a / (name + ".dat")), dtype=np.float64)
+        assert va.size == np.prod(n)
+        assert (b / (name + ".dat")).read_bytes() == (a / (name + ".dat")).read_bytes(), comp
+        txt = np.array([float(line.split()[3]) for line in (a / (name + ".txt")).read_text().splitlines()])
+        scale = max(np.max(np.abs(va)), 1e-300)
+        assert np.max(np.abs(txt - va)) <= 1e-14 * scale, comp
+        vp = np.fromfile(str(c / (name + ".dat")), dtype=np.float64)
+        assert np.array_equal(vp, va.reshape(n)[1:10, 2:9, 3:11].reshape(-1)), comp
