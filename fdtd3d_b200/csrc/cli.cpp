@@ -53,6 +53,39 @@ struct Opts
   int device = 0;
 };
 
+// Axis a 2-D mode drops (-1 in 3-D) and the components it keeps (bit k).
+int flat_axis (int mode)
+{
+  switch (mode)
+  {
+    case FDTD_MODE_TEX:
+    case FDTD_MODE_TMX:
+      return 0;
+    case FDTD_MODE_TEY:
+    case FDTD_MODE_TMY:
+      return 1;
+    case FDTD_MODE_TEZ:
+    case FDTD_MODE_TMZ:
+      return 2;
+    default:
+      return -1;
+  }
+}
+
+unsigned mode_components (int mode)
+{
+  switch (mode)
+  {
+    case FDTD_MODE_TMZ: return (1u << FDTD_EZ) | (1u << FDTD_HX) | (1u << FDTD_HY);
+    case FDTD_MODE_TEZ: return (1u << FDTD_EX) | (1u << FDTD_EY) | (1u << FDTD_HZ);
+    case FDTD_MODE_TEX: return (1u << FDTD_EY) | (1u << FDTD_EZ) | (1u << FDTD_HX);
+    case FDTD_MODE_TMX: return (1u << FDTD_EX) | (1u << FDTD_HY) | (1u << FDTD_HZ);
+    case FDTD_MODE_TEY: return (1u << FDTD_EX) | (1u << FDTD_EZ) | (1u << FDTD_HY);
+    case FDTD_MODE_TMY: return (1u << FDTD_EY) | (1u << FDTD_HX) | (1u << FDTD_HZ);
+    default: return 0x3fu;
+  }
+}
+
 int fail (const std::string &m)
 {
   std::fprintf (stderr, "fdtd3d-b200: %s\n", m.c_str ());
@@ -142,6 +175,16 @@ int parse (std::vector<std::string> args, Opts &o)
       c.mode = FDTD_MODE_DIM3;
     else if (a == "--2d-tmz")
       c.mode = FDTD_MODE_TMZ;
+    else if (a == "--2d-tez")
+      c.mode = FDTD_MODE_TEZ;
+    else if (a == "--2d-tex")
+      c.mode = FDTD_MODE_TEX;
+    else if (a == "--2d-tmx")
+      c.mode = FDTD_MODE_TMX;
+    else if (a == "--2d-tey")
+      c.mode = FDTD_MODE_TEY;
+    else if (a == "--2d-tmy")
+      c.mode = FDTD_MODE_TMY;
     else if (a == "--size" && next (v))
     {
       if (!parse_coord (v, c.size))
@@ -266,8 +309,9 @@ int parse (std::vector<std::string> args, Opts &o)
     if (!done)
       return fail ("unsupported flag " + a + " (outside the step path this binary provides)");
   }
-  if (c.mode == FDTD_MODE_TMZ)
-    c.size[2] = 1;
+  const int f = flat_axis (c.mode);
+  if (f >= 0)
+    c.size[f] = 1;
   return 0;
 }
 
@@ -335,7 +379,7 @@ bool save_dat (const std::string &name, const std::vector<double> &v, const int 
   return (bool) f;
 }
 
-bool save_txt (const std::string &name, const std::vector<double> &v, const int n[3], bool tmz, const int lo[3],
+bool save_txt (const std::string &name, const std::vector<double> &v, const int n[3], int flat, const int lo[3],
                const int hi[3])
 {
   std::ofstream f (name);
@@ -347,10 +391,15 @@ bool save_txt (const std::string &name, const std::vector<double> &v, const int 
       for (int z = lo[2]; z < hi[2]; ++z)
       {
         size_t id = ((size_t) x * n[1] + y) * n[2] + z;
-        if (tmz)
-          f << x << " " << y << " " << v[id] << std::endl;
-        else
-          f << x << " " << y << " " << z << " " << v[id] << std::endl;
+        const int c[3] = {x, y, z};
+        bool first = true;
+        for (int a = 0; a < 3; ++a)
+          if (a != flat)
+          {
+            f << (first ? "" : " ") << c[a];
+            first = false;
+          }
+        f << " " << v[id] << std::endl;
       }
   return true;
 }
@@ -367,8 +416,10 @@ int main (int argc, char **argv)
   int st = fdtd_create (&o.cfg, o.device, &ctx);
   if (st)
     return fail (std::string ("fdtd_create: ") + fdtd_status_str (st) + ": " + fdtd_last_error ());
-  bool tmz = o.cfg.mode == FDTD_MODE_TMZ;
-  int n[3] = {o.cfg.size[0], o.cfg.size[1], tmz ? 1 : o.cfg.size[2]};
+  const int flat = flat_axis (o.cfg.mode);
+  int n[3] = {o.cfg.size[0], o.cfg.size[1], o.cfg.size[2]};
+  if (flat >= 0)
+    n[flat] = 1;
   size_t cells = (size_t) n[0] * n[1] * n[2];
   for (int m = 0; m < 6; ++m)
   {
@@ -376,7 +427,7 @@ int main (int argc, char **argv)
       continue;
     std::vector<double> a;
     std::string why;
-    if (!load_material (o.mat_file[m], cells, tmz ? 2 : 3, a, why))
+    if (!load_material (o.mat_file[m], cells, flat >= 0 ? 2 : 3, a, why))
       return fail (why);
     st = fdtd_upload_material (ctx, m, a.data ());
     if (st)
@@ -403,13 +454,13 @@ int main (int argc, char **argv)
         lo[a] = o.save_start[a];
         hi[a] = o.save_end[a];
       }
-      if (tmz)
+      if (flat >= 0)
       {
-        lo[2] = 0;
-        hi[2] = 1;
+        lo[flat] = 0;
+        hi[flat] = 1;
       }
     }
-    else if (!tmz)
+    else if (flat < 0)
     {
       lo[2] = n[2] / 2;
       hi[2] = n[2] / 2 + 1;
@@ -417,13 +468,13 @@ int main (int argc, char **argv)
     std::vector<double> buf (cells);
     for (int k = 0; k < 6; ++k)
     {
-      if (tmz && k != FDTD_EZ && k != FDTD_HX && k != FDTD_HY)
+      if (!((mode_components (o.cfg.mode) >> k) & 1u))
         continue;
       st = fdtd_download_field (ctx, k, buf.data ());
       if (st)
         return fail (std::string ("download: ") + fdtd_last_error ());
       const std::string base = "previous-1_[timestep=" + std::to_string (o.steps) + "]_[pid=0]_[name=" + names[k] + "]";
-      if (o.save_txt && !save_txt (base + ".txt", buf, n, tmz, lo, hi))
+      if (o.save_txt && !save_txt (base + ".txt", buf, n, flat, lo, hi))
         return fail ("cannot write " + base + ".txt");
       if (o.save_dat && !save_dat (base + ".dat", buf, n, lo, hi))
         return fail ("cannot write " + base + ".dat");

@@ -57,17 +57,21 @@ __device__ __forceinline__ double fast_incident (const GeomDev &g, const double 
                                                  int px, int py, int pz)
 {
   double d_diff = k >= 3 ? 0.5 : 0.0;
-  double x = ((double) px + g.min_fp[k][0]) - g.zero_inc[0];
-  double y = ((double) py + g.min_fp[k][1]) - g.zero_inc[1];
   double d;
-  if (!g.tmz)
+  const int pos[3] = {px, py, pz};
+  if (g.flat < 0)
   {
+    double x = ((double) px + g.min_fp[k][0]) - g.zero_inc[0];
+    double y = ((double) py + g.min_fp[k][1]) - g.zero_inc[1];
     double z = ((double) pz + g.min_fp[k][2]) - g.zero_inc[2];
     d = x * g.s1 * g.c2 + y * g.s1 * g.s2 + z * g.c1 - d_diff;
   }
   else
   {
-    d = x * g.c2 + y * g.s2 - d_diff;
+    const int a0 = g.inc_ax[0], a1 = g.inc_ax[1];
+    double u = ((double) pos[a0] + g.min_fp[k][a0]) - g.zero_inc[a0];
+    double v = ((double) pos[a1] + g.min_fp[k][a1]) - g.zero_inc[a1];
+    d = u * g.inc_k[0] + v * g.inc_k[1] - d_diff;
   }
   int i1 = (int) d;
   double pr2 = d - (double) i1;
@@ -170,19 +174,18 @@ __device__ __forceinline__ void fast_component (const FastHalf &p, int ci, int *
 template <typename T>
 __global__ void __launch_bounds__ (256) fast_half_kernel (FastHalf p, int *err)
 {
-  const int ix = p.g.n[0] - 2;
-  const int iy = p.g.n[1] - 2;
-  const int iz = p.g.tmz ? 1 : p.g.n[2] - 2;
+  // interior cells: 1 .. n - 2 on every axis but the one a 2-D mode drops
+  const int ix = p.g.flat == 0 ? 1 : p.g.n[0] - 2;
+  const int iy = p.g.flat == 1 ? 1 : p.g.n[1] - 2;
+  const int iz = p.g.flat == 2 ? 1 : p.g.n[2] - 2;
   const int64_t total = (int64_t) ix * iy * iz;
   for (int64_t tid = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; tid < total;
        tid += (int64_t) gridDim.x * blockDim.x)
   {
-    int z = (int) (tid % iz);
-    int64_t r = tid / iz;
-    int y = (int) (r % iy) + 1;
-    int x = (int) (r / iy) + 1;
-    if (!p.g.tmz)
-      z += 1;
+    const int z = (int) (tid % iz) + (p.g.flat == 2 ? 0 : 1);
+    const int64_t r = tid / iz;
+    const int y = (int) (r % iy) + (p.g.flat == 1 ? 0 : 1);
+    const int x = (int) (r / iy) + (p.g.flat == 0 ? 0 : 1);
 #pragma unroll 1
     for (int ci = 0; ci < 3; ++ci)
     {
@@ -308,9 +311,9 @@ int grid_for (size_t n, int sm_count)
 
 int launch_fast_half (const FastHalf &p, int *err, int sm_count, cudaStream_t s)
 {
-  const int ix = p.g.n[0] - 2;
-  const int iy = p.g.n[1] - 2;
-  const int iz = p.g.tmz ? 1 : p.g.n[2] - 2;
+  const int ix = p.g.flat == 0 ? 1 : p.g.n[0] - 2;
+  const int iy = p.g.flat == 1 ? 1 : p.g.n[1] - 2;
+  const int iz = p.g.flat == 2 ? 1 : p.g.n[2] - 2;
   int64_t total = (int64_t) ix * iy * iz;
   int64_t blocks = (total + 255) / 256;
   int64_t cap = (int64_t) sm_count * 8 * 16;

@@ -177,7 +177,12 @@ GeomDev make_geom_dev (const Geometry &g)
   std::memset (&d, 0, sizeof (d));
   for (int a = 0; a < 3; ++a)
     d.n[a] = g.n[a];
-  d.tmz = g.tmz ? 1 : 0;
+  d.flat = g.flat;
+  for (int j = 0; j < 2; ++j)
+  {
+    d.inc_ax[j] = g.inc_ax[j];
+    d.inc_k[j] = g.inc_k[j];
+  }
   d.dt = g.dt;
   d.dx = g.dx;
   d.s1 = g.s1;
@@ -323,9 +328,9 @@ int alloc_fast (fdtd_ctx *ctx)
 {
   const Geometry &g = ctx->g;
   size_t n = (size_t) g.cells;
-  if (g.cfg.use_metamaterials && g.tmz)
+  if (g.cfg.use_metamaterials && g.flat >= 0)
     return fail (ctx, FDTD_ERR_UNSUPPORTED, "2-D metamaterials are provided by the FP64 plain form only");
-  ctx->has_second = !g.tmz;
+  ctx->has_second = g.flat < 0;
   for (int b = 0; b < (ctx->has_second ? 2 : 1); ++b)
   {
     for (int k = 0; k < 6; ++k)
@@ -733,11 +738,14 @@ size_t cell_index (const Geometry &g, int x, int y, int z)
 
 bool point_source_index (const Geometry &g, size_t *idx)
 {
-  const int *ps = g.cfg.point_source;
-  int z = g.tmz ? 0 : ps[2];
-  if (ps[0] < 0 || ps[0] >= g.n[0] || ps[1] < 0 || ps[1] >= g.n[1] || z < 0 || z >= g.n[2])
-    return false;
-  *idx = cell_index (g, ps[0], ps[1], z);
+  int p[3];
+  for (int a = 0; a < 3; ++a)
+  {
+    p[a] = a == g.flat ? 0 : g.cfg.point_source[a];
+    if (p[a] < 0 || p[a] >= g.n[a])
+      return false;
+  }
+  *idx = cell_index (g, p[0], p[1], p[2]);
   return true;
 }
 

@@ -75,16 +75,21 @@ FDTDB_HD inline double incident_value (const GeomDev &g, const double *inc, int 
 {
   double d_diff = k >= 3 ? 0.5 : 0.0;
   double d;
-  double x = ((double) px + g.min_fp[k][0]) - g.zero_inc[0];
-  double y = ((double) py + g.min_fp[k][1]) - g.zero_inc[1];
-  if (!g.tmz)
+  const int pos[3] = {px, py, pz};
+  if (g.flat < 0)
   {
+    double x = ((double) px + g.min_fp[k][0]) - g.zero_inc[0];
+    double y = ((double) py + g.min_fp[k][1]) - g.zero_inc[1];
     double z = ((double) pz + g.min_fp[k][2]) - g.zero_inc[2];
     d = x * g.s1 * g.c2 + y * g.s1 * g.s2 + z * g.c1 - d_diff;
   }
   else
   {
-    d = x * g.c2 + y * g.s2 - d_diff;
+    // 2-D: the mode's own two-axis form (InternalScheme.cpp:229-307)
+    const int a0 = g.inc_ax[0], a1 = g.inc_ax[1];
+    double u = ((double) pos[a0] + g.min_fp[k][a0]) - g.zero_inc[a0];
+    double v = ((double) pos[a1] + g.min_fp[k][a1]) - g.zero_inc[a1];
+    d = u * g.inc_k[0] + v * g.inc_k[1] - d_diff;
   }
   double cd1 = (double) ((int) d);
   double cd2 = cd1 + 1;

@@ -88,7 +88,12 @@ double sigma_value (double dist, double boundary, double step)
 // Axis 0 keeps the fractional distance and compares against size; axes 1, 2
 // truncate the distance and compare against size + 0.5 (the reference's
 // initSigmaX / initSigmaY / initSigmaZ differ exactly this way).
-void sigma_profile (std::vector<double> &out, int axis, int n, int pml, double dx)
+// Sigma profile of one axis.  first_variant: the reference's initSigmaX
+// form (FP distance, grid size as is), which it applies to the first axis
+// of the grid's coordinates (x in 3-D, the plane's first axis in 2-D); the
+// other axes take the initSigmaY/Z form (distance truncated to an integer,
+// size + 0.5).  SchemeHelper.h:596-718, Scheme.cpp:141-330.
+void sigma_profile (std::vector<double> &out, bool first_variant, int n, int pml, double dx)
 {
   out.assign (n, 0.0);
   double p = (double) pml;
@@ -96,7 +101,7 @@ void sigma_profile (std::vector<double> &out, int axis, int n, int pml, double d
   for (int i = 0; i < n; ++i)
   {
     double pos = i + 0.5;
-    if (axis == 0)
+    if (first_variant)
     {
       double size = (double) n;
       if (pos < p)
@@ -149,8 +154,40 @@ Pred pred (int k0, int a0, int b0, int k1, int a1, int b1, int k2, int a2, int b
 
 namespace {
 
-// Dim3 E_CENTERED layout of component k; TMz drops the z axis afterwards.
-void init_components (Geometry &g, Pred preds[6][6], int slot_dir[6][4])
+// One mode of the reference (SchemeType): the axis a 2-D mode drops, its
+// components, and how the incident wave enters (Source/Scheme/InternalScheme.cpp:
+// 229-324 distance along the wave vector, Source/Layout/YeeGridLayout.h:
+// 1765-2270 projections, Source/Layout/YeeGridLayout.cpp:2318-2580 origin).
+struct ModeSpec
+{
+  int mode;
+  int flat;          // dropped axis, -1 in 3-D
+  unsigned comps;    // bit k: component k exists
+  bool by_teta;      // 2-D distance y sin(teta) + z cos(teta) form (else x cos(phi) + y sin(phi))
+};
+
+const ModeSpec kModes[] = {
+    {FDTD_MODE_DIM3, -1, 0x3f, false},
+    {FDTD_MODE_TMZ, 2, (1u << EZ) | (1u << HX) | (1u << HY), false},
+    {FDTD_MODE_TEZ, 2, (1u << EX) | (1u << EY) | (1u << HZ), false},
+    {FDTD_MODE_TEX, 0, (1u << EY) | (1u << EZ) | (1u << HX), true},
+    {FDTD_MODE_TMX, 0, (1u << EX) | (1u << HY) | (1u << HZ), true},
+    {FDTD_MODE_TEY, 1, (1u << EX) | (1u << EZ) | (1u << HY), true},
+    {FDTD_MODE_TMY, 1, (1u << EY) | (1u << HX) | (1u << HZ), true},
+};
+
+const ModeSpec *mode_spec (int mode)
+{
+  for (const ModeSpec &m : kModes)
+    if (m.mode == mode)
+      return &m;
+  return nullptr;
+}
+
+// Dim3 E_CENTERED layout of component k; a 2-D mode then drops one axis
+// (YeeGridLayout's initAxesCoordinate keeps the plane's coordinates of
+// every offset and position).
+void init_components (Geometry &g, unsigned comps, Pred preds[6][6], int slot_dir[6][4])
 {
   for (int k = 0; k < 6; ++k)
   {
@@ -232,19 +269,23 @@ void init_components (Geometry &g, Pred preds[6][6], int slot_dir[6][4])
   preds[HZ][DU] = pred (T_RANGE, -1, 1, T_EXR, 0, 0, T_RANGE, 4, -4);
 
   for (int k = 0; k < 6; ++k)
-    g.comp[k].exists = g.tmz ? (k == EZ || k == HX || k == HY) : true;
-  if (g.tmz)
+    g.comp[k].exists = (comps >> k) & 1u;
+  const int f = g.flat;
+  if (f >= 0)
   {
+    // border directions along each axis: x left/right, y down/up, z back/front
+    const int dir_lo[3] = {DL, DD, DB}, dir_hi[3] = {DR, DU, DF};
     for (int k = 0; k < 6; ++k)
     {
       CompLayout &cc = g.comp[k];
-      cc.d11[2] = cc.d12[2] = cc.d21[2] = cc.d22[2] = 0;
+      cc.d11[f] = cc.d12[f] = cc.d21[f] = cc.d22[f] = 0;
       for (int j = 0; j < 4; ++j)
-        cc.m[j][2] = 0;
+        cc.m[j][f] = 0;
+      cc.min_fp[f] = 0.0;
       for (int d = 0; d < 6; ++d)
-        preds[k][d].ax[2].kind = T_ANY;
-      preds[k][DB].valid = false;
-      preds[k][DF].valid = false;
+        preds[k][d].ax[f].kind = T_ANY;
+      preds[k][dir_lo[f]].valid = false;
+      preds[k][dir_hi[f]].valid = false;
     }
   }
 }
@@ -270,8 +311,9 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
 {
   g = Geometry ();
   g.cfg = cfg;
-  if (cfg.mode != FDTD_MODE_DIM3 && cfg.mode != FDTD_MODE_TMZ)
-    return "mode must be FDTD_MODE_DIM3 or FDTD_MODE_TMZ";
+  const ModeSpec *ms = mode_spec (cfg.mode);
+  if (!ms)
+    return "unknown mode (FDTD_MODE_DIM3 or one of the six 2-D modes)";
   if (cfg.layout != 0)
     return "only the E_CENTERED layout (0) is provided";
   if (cfg.precision < FDTD_PREC_FP64_PLAIN || cfg.precision > FDTD_PREC_FP16S)
@@ -283,12 +325,14 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
   if (cfg.point_source_kind == FDTD_SOURCE_GAUSSIAN && !(cfg.point_source_bandwidth > 0))
     return "Gaussian point source needs a positive bandwidth";
   g.tmz = cfg.mode == FDTD_MODE_TMZ;
-  g.n[0] = cfg.size[0];
-  g.n[1] = cfg.size[1];
-  g.n[2] = g.tmz ? 1 : cfg.size[2];
-  int dims = g.tmz ? 2 : 3;
-  for (int a = 0; a < dims; ++a)
+  g.flat = ms->flat;
+  for (int a = 0; a < 3; ++a)
+    g.n[a] = a == g.flat ? 1 : cfg.size[a];
+  auto active = [&] (int a) { return a != g.flat; };
+  for (int a = 0; a < 3; ++a)
   {
+    if (!active (a))
+      continue;
     if (g.n[a] < 3 || g.n[a] > (1 << 20))
       return "grid size out of range";
     if (cfg.use_pml && (cfg.pml[a] < 0 || 2 * cfg.pml[a] >= g.n[a]))
@@ -324,7 +368,7 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
   double s3 = std::sin (g.a3), c3 = std::cos (g.a3);
   for (int k = 0; k < 6; ++k)
     g.proj[k] = 0;
-  if (!g.tmz)
+  if (g.flat < 0)
   {
     // the Hz projection carries the reference's leading minus sign
     g.proj[EX] = c3 * g.s2 - s3 * g.c1 * g.c2;
@@ -339,25 +383,72 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
   }
   else
   {
-    g.proj[EZ] = 1.0;
-    g.proj[HX] = std::sin (g.a2);
-    g.proj[HY] = -std::cos (g.a2);
-    g.zero_inc[0] = cfg.tfsf_left[0] - 2.5 * std::cos (g.a2);
-    g.zero_inc[1] = cfg.tfsf_left[1] - 2.5 * std::sin (g.a2);
-    g.zero_inc[2] = 0;
+    // plane axes (a0, a1) in x, y, z order; the origin is the left TF/SF
+    // corner moved back 2.5 cells along the in-plane wave vector
+    const int a0 = g.flat == 0 ? 1 : 0, a1 = g.flat == 2 ? 1 : 2;
+    g.inc_ax[0] = a0;
+    g.inc_ax[1] = a1;
+    g.zero_inc[0] = g.zero_inc[1] = g.zero_inc[2] = 0;
+    if (ms->by_teta)
+    {
+      g.inc_k[0] = std::sin (g.a1);
+      g.inc_k[1] = std::cos (g.a1);
+      g.zero_inc[a0] = cfg.tfsf_left[a0] - 2.5 * std::sin (g.a1);
+      g.zero_inc[a1] = cfg.tfsf_left[a1] - 2.5 * std::cos (g.a1);
+    }
+    else
+    {
+      g.inc_k[0] = std::cos (g.a2);
+      g.inc_k[1] = std::sin (g.a2);
+      g.zero_inc[a0] = cfg.tfsf_left[a0] - 2.5 * std::cos (g.a2);
+      g.zero_inc[a1] = cfg.tfsf_left[a1] - 2.5 * std::sin (g.a2);
+    }
+    switch (cfg.mode)
+    {
+      case FDTD_MODE_TMZ:
+        g.proj[EZ] = 1.0;
+        g.proj[HX] = std::sin (g.a2);
+        g.proj[HY] = -std::cos (g.a2);
+        break;
+      case FDTD_MODE_TEZ:
+        g.proj[EX] = std::sin (g.a2);
+        g.proj[EY] = -std::cos (g.a2);
+        g.proj[HZ] = -1.0;
+        break;
+      case FDTD_MODE_TEX:
+        g.proj[EY] = -std::cos (g.a1);
+        g.proj[EZ] = std::sin (g.a1);
+        g.proj[HX] = 1.0;
+        break;
+      case FDTD_MODE_TMX:
+        g.proj[EX] = 1.0;
+        g.proj[HY] = std::cos (g.a1);
+        g.proj[HZ] = -std::sin (g.a1);
+        break;
+      case FDTD_MODE_TEY:
+        g.proj[EX] = -std::cos (g.a1);
+        g.proj[EZ] = std::sin (g.a1);
+        g.proj[HY] = -1.0;
+        break;
+      default:   // FDTD_MODE_TMY
+        g.proj[EY] = -1.0;
+        g.proj[HX] = std::cos (g.a1);
+        g.proj[HZ] = -std::sin (g.a1);
+        break;
+    }
   }
   g.inc_len = 500 * g.n[0];
 
   for (int a = 0; a < 3; ++a)
   {
     g.sigma[a].assign (g.n[a], 0.0);
-    if (cfg.use_pml && a < dims)
-      sigma_profile (g.sigma[a], a, g.n[a], cfg.pml[a], cfg.dx);
+    if (cfg.use_pml && active (a))
+      sigma_profile (g.sigma[a], a == (g.flat == 0 ? 1 : 0), g.n[a], cfg.pml[a], cfg.dx);
   }
 
   Pred preds[6][6];
   int slot_dir[6][4];
-  init_components (g, preds, slot_dir);
+  init_components (g, ms->comps, preds, slot_dir);
 
   if (cfg.use_tfsf)
   {
@@ -383,8 +474,8 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
         bool empty = false;
         for (int a = 0; a < 3; ++a)
         {
-          int lo_r = (a < dims) ? 1 : 0;
-          int hi_r = (a < dims) ? g.n[a] - 1 : 1;
+          int lo_r = active (a) ? 1 : 0;
+          int hi_r = active (a) ? g.n[a] - 1 : 1;
           int first = -1, last = -2, count = 0;
           for (int i = lo_r; i < hi_r; ++i)
           {
@@ -453,7 +544,7 @@ std::vector<double> sigma_at (const Geometry &g, int k, int b)
   int a = k % 3;
   bool isH = k >= 3;
   bool averaged = isH ? (b != a) : (b == a);
-  if (g.tmz && b == 2)
+  if (b == g.flat)
     averaged = false;
   for (int i = 0; i < n; ++i)
     out[i] = (averaged && i + 1 < n) ? (s[i] + s[i + 1]) / 2.0 : s[i];

@@ -43,9 +43,17 @@ typedef struct fdtd_ctx fdtd_ctx;
 #define FDTD_ERR_STATE (-6)      /* call out of order (e.g. step before setup) */
 #define FDTD_ERR_DEVICE (-7)     /* a kernel reported an error flag */
 
-/* modes (fdtd3d SchemeType) */
-#define FDTD_MODE_TMZ 2          /* Dim2_TMz: Ez, Hx, Hy */
+/* modes (fdtd3d SchemeType).  A 2-D mode keeps the fields of one plane;
+ * its grid has size 1 along the third axis (size[] of that axis is ignored)
+ * and its arrays are the plane's two axes in x, y, z order, the second
+ * fastest. */
+#define FDTD_MODE_TMZ 2          /* Dim2_TMz: Ez, Hx, Hy in the x-y plane */
 #define FDTD_MODE_DIM3 3         /* Dim3: Ex, Ey, Ez, Hx, Hy, Hz */
+#define FDTD_MODE_TEX 4          /* Dim2_TEx: Ey, Ez, Hx in the y-z plane */
+#define FDTD_MODE_TEY 5          /* Dim2_TEy: Ex, Ez, Hy in the x-z plane */
+#define FDTD_MODE_TEZ 6          /* Dim2_TEz: Ex, Ey, Hz in the x-y plane */
+#define FDTD_MODE_TMX 7          /* Dim2_TMx: Ex, Hy, Hz in the y-z plane */
+#define FDTD_MODE_TMY 8          /* Dim2_TMy: Ey, Hx, Hz in the x-z plane */
 
 /* arithmetic forms */
 #define FDTD_PREC_FP64_PLAIN 0   /* reference formulation, FP64, bit-faithful */
@@ -74,7 +82,7 @@ typedef struct fdtd_ctx fdtd_ctx;
 
 /*
  * Run configuration.  Mirrors fdtd3d's Settings flags (Source/Settings/Settings.inc.h):
- * --3d/--2d-tmz, --size, --pml-size, --tfsf-size-left/right, --dx, --wavelength,
+ * --3d/--2d-te{x,y,z}/--2d-tm{x,y,z}, --size, --pml-size, --tfsf-size-left/right, --dx, --wavelength,
  * --courant-factor, --angle-teta/phi/psi, --use-pml, --use-tfsf,
  * --use-metamaterials, --point-source, --point-source-e*, --layout-type.
  * Float flags hold the values exactly as the reference parses them
@@ -82,8 +90,8 @@ typedef struct fdtd_ctx fdtd_ctx;
  */
 typedef struct
 {
-  int mode;                 /* FDTD_MODE_DIM3 or FDTD_MODE_TMZ */
-  int size[3];              /* size[2] ignored for TMz */
+  int mode;                 /* FDTD_MODE_* */
+  int size[3];              /* the axis a 2-D mode drops is ignored */
   int pml[3];
   int tfsf_left[3];
   int tfsf_right[3];

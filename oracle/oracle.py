@@ -191,18 +191,39 @@ def write_material_txt(path: str, arr: np.ndarray) -> None:
             f.write(" ".join(str(int(q)) for q in i) + " " + repr(float(v)) + "\n")
 
 
+# reference mode flags (Source/Settings/Settings.inc.h:48-60) and the axis
+# each 2-D mode drops
+MODE_FLAGS = {2: "--2d-tmz", 3: "--3d", 4: "--2d-tex", 5: "--2d-tey", 6: "--2d-tez", 7: "--2d-tmx", 8: "--2d-tmy"}
+MODE_FLAT = {2: 2, 4: 0, 5: 1, 6: 2, 7: 0, 8: 1}
+
+
+def mode_axes(mode):
+    """The axes a mode keeps (x, y, z order)."""
+    return tuple(a for a in range(3) if a != MODE_FLAT.get(mode))
+
+
+def _plane(v, mode, default):
+    """Per-axis triple of a mode: a pair gives the kept axes of a 2-D mode."""
+    axes = mode_axes(mode)
+    if v is not None and not isinstance(v, (int, np.integer)) and len(v) == 2 and len(axes) == 2:
+        t = [default] * 3
+        t[axes[0]], t[axes[1]] = int(v[0]), int(v[1])
+        return tuple(t)
+    return _triple(v, default)
+
+
 def reference_args(*, mode=3, size=(20, 20, 20), pml=None, tfsf_left=None, tfsf_right=None,
                    dx=0.0005, wavelength=0.02, courant=0.5, teta=90.0, phi=0.0, psi=90.0,
                    use_pml=False, use_tfsf=False, use_metamaterials=False,
                    point_source=(0, 0, 0), point_source_mask=0, steps=10):
-    size = _triple(size, 1)
-    ax = ("x", "y", "z") if mode == 3 else ("x", "y")
+    size = _plane(size, mode, 1)
+    names = ("x", "y", "z")
 
     def coord(v):
-        v = _triple(v, 0)
-        return ",".join(f"{a}:{v[i]}" for i, a in enumerate(ax))
+        v = _plane(v, mode, 0)
+        return ",".join(f"{names[a]}:{v[a]}" for a in mode_axes(mode))
 
-    args = ["--3d" if mode == 3 else "--2d-tmz", "--size", coord(size),
+    args = [MODE_FLAGS[mode], "--size", coord(size),
             "--dx", repr(dx), "--wavelength", repr(wavelength), "--courant-factor", repr(courant),
             "--angle-teta", repr(teta), "--angle-phi", repr(phi), "--angle-psi", repr(psi),
             "--time-steps", str(steps), "--use-ca-cb", "--log-level", "0"]
@@ -225,8 +246,8 @@ def run_reference(materials=None, timeout=600, **kw):
     if not os.path.exists(REF_BIN):
         raise FileNotFoundError(REF_BIN)
     mode = kw.get("mode", 3)
-    size = _triple(kw.get("size", (20, 20, 20)), 1)
-    shape = size if mode == 3 else size[:2]
+    size = _plane(kw.get("size", (20, 20, 20)), mode, 1)
+    shape = tuple(size[a] for a in mode_axes(mode))
     with tempfile.TemporaryDirectory() as tmp:
         args = reference_args(**kw)
         flags = {"eps": "--load-eps-from-file", "mu": "--load-mu-from-file",
@@ -236,9 +257,9 @@ def run_reference(materials=None, timeout=600, **kw):
             p = os.path.join(tmp, f"{name}.txt")
             write_material_txt(p, np.asarray(arr).reshape(shape))
             args += [flags[name], p]
-        ax = ("x", "y", "z") if mode == 3 else ("x", "y")
-        end = ",".join(f"{a}:{size[i]}" for i, a in enumerate(ax))
-        start = ",".join(f"{a}:0" for a in ax)
+        names = ("x", "y", "z")
+        end = ",".join(f"{names[a]}:{size[a]}" for a in mode_axes(mode))
+        start = ",".join(f"{names[a]}:0" for a in mode_axes(mode))
         args += ["--save-res", "--save-as-txt", "--manual-save-coords",
                  "--save-start-coord", start, "--save-end-coord", end]
         r = subprocess.run([REF_BIN] + args, cwd=tmp, capture_output=True, text=True, timeout=timeout)

@@ -36,7 +36,8 @@ def test_status_strings(fdtd):
 
 
 @pytest.mark.parametrize("bad", [
-    dict(mode=5),
+    dict(mode=9),
+    dict(mode=1),
     dict(size=(2, 10, 10)),
     dict(use_pml=True, pml=10, size=(12, 12, 12)),
     dict(use_tfsf=True, tfsf_left=0, tfsf_right=3),

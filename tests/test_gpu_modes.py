@@ -1,0 +1,111 @@
+"""The six 2-D modes of the reference (Dim2_TEx .. Dim2_TMz) against the
+reference CPU build (oracle/_ref/fdtd3d, all modes compiled in).
+
+* fdtd3d-b200 (the FP64 plain form) and the reference write byte-identical
+  TXT dumps (15 significant digits) for the same flags: PML, TF/SF plane
+  wave at an oblique in-plane angle, a permittivity map from a TXT file,
+  and, in a second set, a point source on every component of the mode.
+* The FP32 form through the C ABI agrees with the reference to <= 1e-5
+  relative L2 per field family.
+The angles follow each mode's own plane (TEx/TMx: phi = 90, TEy/TMy:
+phi = 0, TEz/TMz: teta = 90; Source/Layout/YeeGridLayout.cpp:2318-2580).
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle.oracle import REF_BIN, mode_axes, run_reference, write_material_txt
+
+pytestmark = pytest.mark.gpu
+
+MODES = {  # mode: (flag, components, teta, phi, psi)
+    4: ("--2d-tex", ("Ey", "Ez", "Hx"), 30, 90, 90),
+    5: ("--2d-tey", ("Ex", "Ez", "Hy"), 25, 0, 90),
+    6: ("--2d-tez", ("Ex", "Ey", "Hz"), 90, 35, 0),
+    7: ("--2d-tmx", ("Ex", "Hy", "Hz"), 40, 90, 0),
+    8: ("--2d-tmy", ("Ey", "Hx", "Hz"), 20, 0, 0),
+    2: ("--2d-tmz", ("Ez", "Hx", "Hy"), 90, 30, 90),
+}
+SIZE = (22, 19, 24)      # x, y, z; a mode drops one axis
+NAMES = ("x", "y", "z")
+
+
+def _need_ref():
+    if not os.path.exists(REF_BIN):
+        pytest.skip("reference binary not built")
+
+
+def _plane_shape(mode):
+    return tuple(SIZE[a] for a in mode_axes(mode))
+
+
+def _eps_map(mode, seed):
+    rng = np.random.default_rng(seed)
+    return np.where(rng.random(_plane_shape(mode)) < 0.35, 4.0, 1.0)
+
+
+def _flags(mode, steps, source):
+    flag, comps, teta, phi, psi = MODES[mode]
+    size = ",".join(f"{n}:{v}" for n, v in zip(NAMES, SIZE))
+    f = [flag, "--size", size, "--use-pml", "--pml-size", "x:3", "--same-size-pml",
+         "--use-tfsf", "--tfsf-size-left", "x:5", "--same-size-tfsf", "--tfsf-size-right", "x:6",
+         "--angle-teta", str(teta), "--angle-phi", str(phi), "--angle-psi", str(psi),
+         "--dx", "0.0005", "--wavelength", "0.02", "--courant-factor", "0.5", "--time-steps", str(steps),
+         "--save-res", "--save-as-txt", "--manual-save-coords",
+         "--save-start-coord", "x:0,y:0,z:0", "--save-end-coord", size]
+    if source:
+        ps = [9, 8, 11]
+        f += ["--point-source", ",".join(f"{n}:{v}" for n, v in zip(NAMES, ps))]
+        f += [f"--point-source-{c.lower()}" for c in comps]
+    return f
+
+
+@pytest.mark.parametrize("source", [False, True], ids=["tfsf", "point_source"])
+@pytest.mark.parametrize("mode", sorted(MODES), ids=[MODES[m][0][2:] for m in sorted(MODES)])
+def test_cli_2d_mode_matches_reference_txt(fdtd, tmp_path, mode, source):
+    _need_ref()
+    cli = os.path.join(os.path.dirname(fdtd.__file__), "fdtd3d-b200")
+    eps_file = tmp_path / "eps.txt"
+    write_material_txt(str(eps_file), _eps_map(mode, mode))
+    flags = _flags(mode, 30, source) + ["--load-eps-from-file", str(eps_file)]
+    out = {}
+    for name, exe, extra in (("ref", REF_BIN, ["--use-ca-cb", "--use-ca-cb-pml"]), ("b200", cli, [])):
+        d = tmp_path / name
+        d.mkdir()
+        r = subprocess.run([exe] + flags + extra, cwd=d, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+        out[name] = {f.name: f.read_text() for f in d.iterdir()}
+    names = sorted(out["ref"])
+    assert names == sorted(out["b200"])
+    assert len(names) == 3, names
+    for fname in names:
+        ref, mine = out["ref"][fname], out["b200"][fname]
+        assert ref.count("\n") == np.prod(_plane_shape(mode))
+        if mine != ref:
+            diffs = [(a, b) for a, b in zip(ref.splitlines(), mine.splitlines()) if a != b]
+            raise AssertionError(f"{fname}: {len(diffs)} lines differ, first: {diffs[:4]}")
+        # the run must carry signal in every component of the mode
+        vals = np.array([float(line.split()[-1]) for line in ref.splitlines()])
+        assert np.max(np.abs(vals)) > 0, fname
+
+
+@pytest.mark.parametrize("mode", sorted(MODES), ids=[MODES[m][0][2:] for m in sorted(MODES)])
+def test_fp32_2d_mode_matches_reference(fdtd, mode):
+    _need_ref()
+    flag, comps, teta, phi, psi = MODES[mode]
+    eps = _eps_map(mode, 100 + mode)
+    kw = dict(mode=mode, size=_plane_shape(mode), use_pml=True, pml=3, use_tfsf=True, tfsf_left=5,
+              tfsf_right=6, teta=teta, phi=phi, psi=psi)
+    ref, _ = run_reference(materials={"eps": eps}, steps=40, **kw)
+    assert sorted(ref) == sorted(comps)
+    with fdtd.Simulation(materials={"eps": eps}, precision=fdtd.PREC_FP32, **kw) as sim:
+        sim.step(40)
+        got = {c: sim.field(c) for c in comps}
+    for fam in ("E", "H"):
+        names = [c for c in comps if c[0] == fam]
+        num = sum(np.sum((got[c] - ref[c]) ** 2) for c in names)
+        den = sum(np.sum(ref[c] ** 2) for c in names)
+        assert den > 0
+        assert np.sqrt(num / den) <= 1e-5, (fam, np.sqrt(num / den))
