@@ -25,15 +25,25 @@ MODE_TEY = 5
 MODE_TEZ = 6
 MODE_TMX = 7
 MODE_TMY = 8
-# axis each 2-D mode drops (its arrays are the other two axes, in x, y, z order)
-FLAT_AXIS = {MODE_TMZ: 2, MODE_TEZ: 2, MODE_TEX: 0, MODE_TMX: 0, MODE_TEY: 1, MODE_TMY: 1}
+MODE_EXHY = 10
+MODE_EXHZ = 11
+MODE_EYHX = 12
+MODE_EYHZ = 13
+MODE_EZHX = 14
+MODE_EZHY = 15
+# axes each mode keeps (its arrays are these axes, in x, y, z order, the last fastest)
+KEPT_AXES = {MODE_DIM3: (0, 1, 2), MODE_TMZ: (0, 1), MODE_TEZ: (0, 1), MODE_TEX: (1, 2), MODE_TMX: (1, 2),
+             MODE_TEY: (0, 2), MODE_TMY: (0, 2), MODE_EXHY: (2,), MODE_EYHX: (2,), MODE_EXHZ: (1,),
+             MODE_EZHX: (1,), MODE_EYHZ: (0,), MODE_EZHY: (0,)}
 PREC_FP64_PLAIN = 0
 PREC_FP32 = 1
 PREC_FP16S = 2
 COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
 MODE_COMPONENTS = {MODE_DIM3: COMPONENTS, MODE_TMZ: ("Ez", "Hx", "Hy"), MODE_TEZ: ("Ex", "Ey", "Hz"),
                    MODE_TEX: ("Ey", "Ez", "Hx"), MODE_TMX: ("Ex", "Hy", "Hz"), MODE_TEY: ("Ex", "Ez", "Hy"),
-                   MODE_TMY: ("Ey", "Hx", "Hz")}
+                   MODE_TMY: ("Ey", "Hx", "Hz"), MODE_EXHY: ("Ex", "Hy"), MODE_EXHZ: ("Ex", "Hz"),
+                   MODE_EYHX: ("Ey", "Hx"), MODE_EYHZ: ("Ey", "Hz"), MODE_EZHX: ("Ez", "Hx"),
+                   MODE_EZHY: ("Ez", "Hy")}
 MATERIALS = ("eps", "mu", "omegape", "omegapm", "gammae", "gammam")
 REDUCE_ENERGY = 0
 REDUCE_L2 = 1
@@ -150,23 +160,22 @@ def f32(x: float) -> float:
     return struct.unpack("f", struct.pack("f", float(x)))[0]
 
 
-def _triple(v, default, flat=None):
-    """Per-axis triple; with a 2-D mode's dropped axis `flat`, a pair gives
-    the plane's two axes in x, y, z order and the dropped axis gets `default`."""
+def _triple(v, default, kept=(0, 1, 2)):
+    """Per-axis triple for a mode that keeps axes `kept`: a sequence as long
+    as `kept` gives those axes in x, y, z order; dropped axes get `default`."""
     if v is None:
-        t = (default,) * 3
+        t = [default] * 3
     elif isinstance(v, (int, np.integer)):
-        t = (int(v),) * 3
+        t = [int(v)] * 3
     else:
-        v = tuple(int(a) for a in v)
-        if flat is not None and len(v) == 2:
-            t = tuple(default if a == flat else v[0] if a == min(b for b in range(3) if b != flat) else v[1]
-                      for a in range(3))
+        v = [int(a) for a in v]
+        if len(v) == len(kept) and len(kept) < 3:
+            t = [default] * 3
+            for a, val in zip(kept, v):
+                t[a] = val
         else:
-            t = v + (default,) * (3 - len(v))
-    if flat is not None:
-        t = tuple(default if a == flat else t[a] for a in range(3))
-    return t
+            t = v + [default] * (3 - len(v))
+    return tuple(t[a] if a in kept else default for a in range(3))
 
 
 def make_config(*, mode=MODE_DIM3, size=(20, 20, 20), pml=None, tfsf_left=None, tfsf_right=None,
@@ -176,15 +185,15 @@ def make_config(*, mode=MODE_DIM3, size=(20, 20, 20), pml=None, tfsf_left=None, 
                 precision=PREC_FP64_PLAIN) -> Config:
     c = Config()
     c.mode = mode
-    flat = FLAT_AXIS.get(mode)
-    c.size[:] = _triple(size, 1, flat)
-    c.pml[:] = _triple(pml, 0, flat)
-    c.tfsf_left[:] = _triple(tfsf_left, 0, flat)
-    c.tfsf_right[:] = _triple(tfsf_right, 0, flat)
+    kept = KEPT_AXES.get(mode, (0, 1, 2))
+    c.size[:] = _triple(size, 1, kept)
+    c.pml[:] = _triple(pml, 0, kept)
+    c.tfsf_left[:] = _triple(tfsf_left, 0, kept)
+    c.tfsf_right[:] = _triple(tfsf_right, 0, kept)
     c.dx, c.wavelength, c.courant = f32(dx), f32(wavelength), f32(courant)
     c.angle_teta, c.angle_phi, c.angle_psi = f32(teta), f32(phi), f32(psi)
     c.use_pml, c.use_tfsf, c.use_metamaterials = int(use_pml), int(use_tfsf), int(use_metamaterials)
-    c.point_source[:] = _triple(point_source, 0, flat)
+    c.point_source[:] = _triple(point_source, 0, kept)
     c.point_source_mask = int(point_source_mask)
     c.point_source_kind = int(point_source_kind)
     c.point_source_bandwidth = float(point_source_bandwidth)
@@ -206,8 +215,7 @@ class Simulation:
         self.cfg = make_config(**cfg)
         self.mode = self.cfg.mode
         size = tuple(self.cfg.size)
-        flat = FLAT_AXIS.get(self.mode)
-        self.shape = size if flat is None else tuple(v for a, v in enumerate(size) if a != flat)
+        self.shape = tuple(size[a] for a in KEPT_AXES.get(self.mode, (0, 1, 2)))
         self.cells = int(np.prod(self.shape))
         h = ctypes.c_void_p()
         self._check(self.lib.fdtd_create(ctypes.byref(self.cfg), device, ctypes.byref(h)), "fdtd_create")

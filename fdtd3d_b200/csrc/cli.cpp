@@ -53,22 +53,31 @@ struct Opts
   int device = 0;
 };
 
-// Axis a 2-D mode drops (-1 in 3-D) and the components it keeps (bit k).
-int flat_axis (int mode)
+// Axes a mode drops (bit a) and the components it keeps (bit k).
+unsigned dropped_axes (int mode)
 {
   switch (mode)
   {
     case FDTD_MODE_TEX:
     case FDTD_MODE_TMX:
-      return 0;
+      return 1u;
     case FDTD_MODE_TEY:
     case FDTD_MODE_TMY:
-      return 1;
+      return 2u;
     case FDTD_MODE_TEZ:
     case FDTD_MODE_TMZ:
-      return 2;
+      return 4u;
+    case FDTD_MODE_EXHY:
+    case FDTD_MODE_EYHX:
+      return 3u;
+    case FDTD_MODE_EXHZ:
+    case FDTD_MODE_EZHX:
+      return 5u;
+    case FDTD_MODE_EYHZ:
+    case FDTD_MODE_EZHY:
+      return 6u;
     default:
-      return -1;
+      return 0u;
   }
 }
 
@@ -82,6 +91,12 @@ unsigned mode_components (int mode)
     case FDTD_MODE_TMX: return (1u << FDTD_EX) | (1u << FDTD_HY) | (1u << FDTD_HZ);
     case FDTD_MODE_TEY: return (1u << FDTD_EX) | (1u << FDTD_EZ) | (1u << FDTD_HY);
     case FDTD_MODE_TMY: return (1u << FDTD_EY) | (1u << FDTD_HX) | (1u << FDTD_HZ);
+    case FDTD_MODE_EXHY: return (1u << FDTD_EX) | (1u << FDTD_HY);
+    case FDTD_MODE_EXHZ: return (1u << FDTD_EX) | (1u << FDTD_HZ);
+    case FDTD_MODE_EYHX: return (1u << FDTD_EY) | (1u << FDTD_HX);
+    case FDTD_MODE_EYHZ: return (1u << FDTD_EY) | (1u << FDTD_HZ);
+    case FDTD_MODE_EZHX: return (1u << FDTD_EZ) | (1u << FDTD_HX);
+    case FDTD_MODE_EZHY: return (1u << FDTD_EZ) | (1u << FDTD_HY);
     default: return 0x3fu;
   }
 }
@@ -185,6 +200,18 @@ int parse (std::vector<std::string> args, Opts &o)
       c.mode = FDTD_MODE_TEY;
     else if (a == "--2d-tmy")
       c.mode = FDTD_MODE_TMY;
+    else if (a == "--1d-exhy")
+      c.mode = FDTD_MODE_EXHY;
+    else if (a == "--1d-exhz")
+      c.mode = FDTD_MODE_EXHZ;
+    else if (a == "--1d-eyhx")
+      c.mode = FDTD_MODE_EYHX;
+    else if (a == "--1d-eyhz")
+      c.mode = FDTD_MODE_EYHZ;
+    else if (a == "--1d-ezhx")
+      c.mode = FDTD_MODE_EZHX;
+    else if (a == "--1d-ezhy")
+      c.mode = FDTD_MODE_EZHY;
     else if (a == "--size" && next (v))
     {
       if (!parse_coord (v, c.size))
@@ -309,9 +336,9 @@ int parse (std::vector<std::string> args, Opts &o)
     if (!done)
       return fail ("unsupported flag " + a + " (outside the step path this binary provides)");
   }
-  const int f = flat_axis (c.mode);
-  if (f >= 0)
-    c.size[f] = 1;
+  for (int a = 0; a < 3; ++a)
+    if ((dropped_axes (c.mode) >> a) & 1u)
+      c.size[a] = 1;
   return 0;
 }
 
@@ -379,8 +406,8 @@ bool save_dat (const std::string &name, const std::vector<double> &v, const int 
   return (bool) f;
 }
 
-bool save_txt (const std::string &name, const std::vector<double> &v, const int n[3], int flat, const int lo[3],
-               const int hi[3])
+bool save_txt (const std::string &name, const std::vector<double> &v, const int n[3], unsigned drop,
+               const int lo[3], const int hi[3])
 {
   std::ofstream f (name);
   if (!f)
@@ -394,7 +421,7 @@ bool save_txt (const std::string &name, const std::vector<double> &v, const int 
         const int c[3] = {x, y, z};
         bool first = true;
         for (int a = 0; a < 3; ++a)
-          if (a != flat)
+          if (!((drop >> a) & 1u))
           {
             f << (first ? "" : " ") << c[a];
             first = false;
@@ -416,10 +443,16 @@ int main (int argc, char **argv)
   int st = fdtd_create (&o.cfg, o.device, &ctx);
   if (st)
     return fail (std::string ("fdtd_create: ") + fdtd_status_str (st) + ": " + fdtd_last_error ());
-  const int flat = flat_axis (o.cfg.mode);
+  const unsigned drop = dropped_axes (o.cfg.mode);
   int n[3] = {o.cfg.size[0], o.cfg.size[1], o.cfg.size[2]};
-  if (flat >= 0)
-    n[flat] = 1;
+  int kept = 0;
+  for (int a = 0; a < 3; ++a)
+  {
+    if ((drop >> a) & 1u)
+      n[a] = 1;
+    else
+      ++kept;
+  }
   size_t cells = (size_t) n[0] * n[1] * n[2];
   for (int m = 0; m < 6; ++m)
   {
@@ -427,7 +460,7 @@ int main (int argc, char **argv)
       continue;
     std::vector<double> a;
     std::string why;
-    if (!load_material (o.mat_file[m], cells, flat >= 0 ? 2 : 3, a, why))
+    if (!load_material (o.mat_file[m], cells, kept, a, why))
       return fail (why);
     st = fdtd_upload_material (ctx, m, a.data ());
     if (st)
@@ -454,13 +487,14 @@ int main (int argc, char **argv)
         lo[a] = o.save_start[a];
         hi[a] = o.save_end[a];
       }
-      if (flat >= 0)
-      {
-        lo[flat] = 0;
-        hi[flat] = 1;
-      }
+      for (int a = 0; a < 3; ++a)
+        if ((drop >> a) & 1u)
+        {
+          lo[a] = 0;
+          hi[a] = 1;
+        }
     }
-    else if (flat < 0)
+    else if (drop == 0)
     {
       lo[2] = n[2] / 2;
       hi[2] = n[2] / 2 + 1;
@@ -474,7 +508,7 @@ int main (int argc, char **argv)
       if (st)
         return fail (std::string ("download: ") + fdtd_last_error ());
       const std::string base = "previous-1_[timestep=" + std::to_string (o.steps) + "]_[pid=0]_[name=" + names[k] + "]";
-      if (o.save_txt && !save_txt (base + ".txt", buf, n, flat, lo, hi))
+      if (o.save_txt && !save_txt (base + ".txt", buf, n, drop, lo, hi))
         return fail ("cannot write " + base + ".txt");
       if (o.save_dat && !save_dat (base + ".dat", buf, n, lo, hi))
         return fail ("cannot write " + base + ".dat");

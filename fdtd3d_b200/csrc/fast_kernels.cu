@@ -59,7 +59,7 @@ __device__ __forceinline__ double fast_incident (const GeomDev &g, const double 
   double d_diff = k >= 3 ? 0.5 : 0.0;
   double d;
   const int pos[3] = {px, py, pz};
-  if (g.flat < 0)
+  if (g.drop == 0)
   {
     double x = ((double) px + g.min_fp[k][0]) - g.zero_inc[0];
     double y = ((double) py + g.min_fp[k][1]) - g.zero_inc[1];
@@ -174,18 +174,18 @@ __device__ __forceinline__ void fast_component (const FastHalf &p, int ci, int *
 template <typename T>
 __global__ void __launch_bounds__ (256) fast_half_kernel (FastHalf p, int *err)
 {
-  // interior cells: 1 .. n - 2 on every axis but the one a 2-D mode drops
-  const int ix = p.g.flat == 0 ? 1 : p.g.n[0] - 2;
-  const int iy = p.g.flat == 1 ? 1 : p.g.n[1] - 2;
-  const int iz = p.g.flat == 2 ? 1 : p.g.n[2] - 2;
+  // interior cells: 1 .. n - 2 on every axis a mode keeps, 0 on a dropped one
+  const int ix = (p.g.drop & 1) ? 1 : p.g.n[0] - 2;
+  const int iy = (p.g.drop & 2) ? 1 : p.g.n[1] - 2;
+  const int iz = (p.g.drop & 4) ? 1 : p.g.n[2] - 2;
   const int64_t total = (int64_t) ix * iy * iz;
   for (int64_t tid = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; tid < total;
        tid += (int64_t) gridDim.x * blockDim.x)
   {
-    const int z = (int) (tid % iz) + (p.g.flat == 2 ? 0 : 1);
+    const int z = (int) (tid % iz) + ((p.g.drop & 4) ? 0 : 1);
     const int64_t r = tid / iz;
-    const int y = (int) (r % iy) + (p.g.flat == 1 ? 0 : 1);
-    const int x = (int) (r / iy) + (p.g.flat == 0 ? 0 : 1);
+    const int y = (int) (r % iy) + ((p.g.drop & 2) ? 0 : 1);
+    const int x = (int) (r / iy) + ((p.g.drop & 1) ? 0 : 1);
 #pragma unroll 1
     for (int ci = 0; ci < 3; ++ci)
     {
@@ -311,9 +311,9 @@ int grid_for (size_t n, int sm_count)
 
 int launch_fast_half (const FastHalf &p, int *err, int sm_count, cudaStream_t s)
 {
-  const int ix = p.g.flat == 0 ? 1 : p.g.n[0] - 2;
-  const int iy = p.g.flat == 1 ? 1 : p.g.n[1] - 2;
-  const int iz = p.g.flat == 2 ? 1 : p.g.n[2] - 2;
+  const int ix = (p.g.drop & 1) ? 1 : p.g.n[0] - 2;
+  const int iy = (p.g.drop & 2) ? 1 : p.g.n[1] - 2;
+  const int iz = (p.g.drop & 4) ? 1 : p.g.n[2] - 2;
   int64_t total = (int64_t) ix * iy * iz;
   int64_t blocks = (total + 255) / 256;
   int64_t cap = (int64_t) sm_count * 8 * 16;

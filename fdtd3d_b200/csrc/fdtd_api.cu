@@ -177,7 +177,7 @@ GeomDev make_geom_dev (const Geometry &g)
   std::memset (&d, 0, sizeof (d));
   for (int a = 0; a < 3; ++a)
     d.n[a] = g.n[a];
-  d.flat = g.flat;
+  d.drop = g.drop;
   for (int j = 0; j < 2; ++j)
   {
     d.inc_ax[j] = g.inc_ax[j];
@@ -328,9 +328,9 @@ int alloc_fast (fdtd_ctx *ctx)
 {
   const Geometry &g = ctx->g;
   size_t n = (size_t) g.cells;
-  if (g.cfg.use_metamaterials && g.flat >= 0)
-    return fail (ctx, FDTD_ERR_UNSUPPORTED, "2-D metamaterials are provided by the FP64 plain form only");
-  ctx->has_second = g.flat < 0;
+  if (g.cfg.use_metamaterials && g.drop != 0)
+    return fail (ctx, FDTD_ERR_UNSUPPORTED, "2-D and 1-D metamaterials are provided by the FP64 plain form only");
+  ctx->has_second = g.drop == 0;
   for (int b = 0; b < (ctx->has_second ? 2 : 1); ++b)
   {
     for (int k = 0; k < 6; ++k)
@@ -741,7 +741,7 @@ bool point_source_index (const Geometry &g, size_t *idx)
   int p[3];
   for (int a = 0; a < 3; ++a)
   {
-    p[a] = a == g.flat ? 0 : g.cfg.point_source[a];
+    p[a] = ((g.drop >> a) & 1) ? 0 : g.cfg.point_source[a];
     if (p[a] < 0 || p[a] >= g.n[a])
       return false;
   }

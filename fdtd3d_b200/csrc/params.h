@@ -45,8 +45,8 @@ struct CompDev
 struct GeomDev
 {
   int n[3];
-  int flat;                   // axis a 2-D mode drops (-1: 3-D)
-  int inc_ax[2];              // 2-D: incident distance u k0 + v k1 along these axes
+  int drop;                   // bit a: axis a has size 1 (2-D / 1-D modes)
+  int inc_ax[2];              // 2-D / 1-D: incident distance u k0 + v k1 along these axes
   double inc_k[2];
   double dt, dx;
   double s1, c1, s2, c2;

@@ -76,7 +76,7 @@ FDTDB_HD inline double incident_value (const GeomDev &g, const double *inc, int 
   double d_diff = k >= 3 ? 0.5 : 0.0;
   double d;
   const int pos[3] = {px, py, pz};
-  if (g.flat < 0)
+  if (g.drop == 0)
   {
     double x = ((double) px + g.min_fp[k][0]) - g.zero_inc[0];
     double y = ((double) py + g.min_fp[k][1]) - g.zero_inc[1];
@@ -85,7 +85,7 @@ FDTDB_HD inline double incident_value (const GeomDev &g, const double *inc, int 
   }
   else
   {
-    // 2-D: the mode's own two-axis form (InternalScheme.cpp:229-307)
+    // 2-D / 1-D: the mode's own form (InternalScheme.cpp:110-307)
     const int a0 = g.inc_ax[0], a1 = g.inc_ax[1];
     double u = ((double) pos[a0] + g.min_fp[k][a0]) - g.zero_inc[a0];
     double v = ((double) pos[a1] + g.min_fp[k][a1]) - g.zero_inc[a1];

@@ -154,26 +154,45 @@ Pred pred (int k0, int a0, int b0, int k1, int a1, int b1, int k2, int a2, int b
 
 namespace {
 
-// One mode of the reference (SchemeType): the axis a 2-D mode drops, its
+// One mode of the reference (SchemeType): the axes it drops, its
 // components, and how the incident wave enters (Source/Scheme/InternalScheme.cpp:
-// 229-324 distance along the wave vector, Source/Layout/YeeGridLayout.h:
-// 1765-2270 projections, Source/Layout/YeeGridLayout.cpp:2318-2580 origin).
+// 110-324 distance along the wave vector, Source/Layout/YeeGridLayout.h:
+// 1240-2270 projections, Source/Layout/YeeGridLayout.cpp:2050-2580 origin).
+enum IncForm
+{
+  INC_3D,        // x sin(teta) cos(phi) + y sin(teta) sin(phi) + z cos(teta)
+  INC_TETA,      // 2-D: u sin(teta) + v cos(teta)
+  INC_PHI,       // 2-D: u cos(phi) + v sin(phi)
+  INC_1D         // 1-D: the coordinate itself
+};
+
 struct ModeSpec
 {
   int mode;
-  int flat;          // dropped axis, -1 in 3-D
+  unsigned drop;     // bit a: axis a has size 1
   unsigned comps;    // bit k: component k exists
-  bool by_teta;      // 2-D distance y sin(teta) + z cos(teta) form (else x cos(phi) + y sin(phi))
+  IncForm form;
 };
 
+constexpr unsigned bit (int k)
+{
+  return 1u << k;
+}
+
 const ModeSpec kModes[] = {
-    {FDTD_MODE_DIM3, -1, 0x3f, false},
-    {FDTD_MODE_TMZ, 2, (1u << EZ) | (1u << HX) | (1u << HY), false},
-    {FDTD_MODE_TEZ, 2, (1u << EX) | (1u << EY) | (1u << HZ), false},
-    {FDTD_MODE_TEX, 0, (1u << EY) | (1u << EZ) | (1u << HX), true},
-    {FDTD_MODE_TMX, 0, (1u << EX) | (1u << HY) | (1u << HZ), true},
-    {FDTD_MODE_TEY, 1, (1u << EX) | (1u << EZ) | (1u << HY), true},
-    {FDTD_MODE_TMY, 1, (1u << EY) | (1u << HX) | (1u << HZ), true},
+    {FDTD_MODE_DIM3, 0, 0x3f, INC_3D},
+    {FDTD_MODE_TMZ, bit (2), bit (EZ) | bit (HX) | bit (HY), INC_PHI},
+    {FDTD_MODE_TEZ, bit (2), bit (EX) | bit (EY) | bit (HZ), INC_PHI},
+    {FDTD_MODE_TEX, bit (0), bit (EY) | bit (EZ) | bit (HX), INC_TETA},
+    {FDTD_MODE_TMX, bit (0), bit (EX) | bit (HY) | bit (HZ), INC_TETA},
+    {FDTD_MODE_TEY, bit (1), bit (EX) | bit (EZ) | bit (HY), INC_TETA},
+    {FDTD_MODE_TMY, bit (1), bit (EY) | bit (HX) | bit (HZ), INC_TETA},
+    {FDTD_MODE_EXHY, bit (0) | bit (1), bit (EX) | bit (HY), INC_1D},
+    {FDTD_MODE_EXHZ, bit (0) | bit (2), bit (EX) | bit (HZ), INC_1D},
+    {FDTD_MODE_EYHX, bit (0) | bit (1), bit (EY) | bit (HX), INC_1D},
+    {FDTD_MODE_EYHZ, bit (1) | bit (2), bit (EY) | bit (HZ), INC_1D},
+    {FDTD_MODE_EZHX, bit (0) | bit (2), bit (EZ) | bit (HX), INC_1D},
+    {FDTD_MODE_EZHY, bit (1) | bit (2), bit (EZ) | bit (HY), INC_1D},
 };
 
 const ModeSpec *mode_spec (int mode)
@@ -184,9 +203,9 @@ const ModeSpec *mode_spec (int mode)
   return nullptr;
 }
 
-// Dim3 E_CENTERED layout of component k; a 2-D mode then drops one axis
-// (YeeGridLayout's initAxesCoordinate keeps the plane's coordinates of
-// every offset and position).
+// Dim3 E_CENTERED layout of component k; a 2-D or 1-D mode then drops its
+// axes (YeeGridLayout's initAxesCoordinate keeps the coordinates of the
+// kept axes of every offset and position).
 void init_components (Geometry &g, unsigned comps, Pred preds[6][6], int slot_dir[6][4])
 {
   for (int k = 0; k < 6; ++k)
@@ -270,11 +289,12 @@ void init_components (Geometry &g, unsigned comps, Pred preds[6][6], int slot_di
 
   for (int k = 0; k < 6; ++k)
     g.comp[k].exists = (comps >> k) & 1u;
-  const int f = g.flat;
-  if (f >= 0)
+  // border directions along each axis: x left/right, y down/up, z back/front
+  const int dir_lo[3] = {DL, DD, DB}, dir_hi[3] = {DR, DU, DF};
+  for (int f = 0; f < 3; ++f)
   {
-    // border directions along each axis: x left/right, y down/up, z back/front
-    const int dir_lo[3] = {DL, DD, DB}, dir_hi[3] = {DR, DU, DF};
+    if (!((g.drop >> f) & 1u))
+      continue;
     for (int k = 0; k < 6; ++k)
     {
       CompLayout &cc = g.comp[k];
@@ -313,7 +333,7 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
   g.cfg = cfg;
   const ModeSpec *ms = mode_spec (cfg.mode);
   if (!ms)
-    return "unknown mode (FDTD_MODE_DIM3 or one of the six 2-D modes)";
+    return "unknown mode (FDTD_MODE_DIM3, a 2-D or a 1-D mode)";
   if (cfg.layout != 0)
     return "only the E_CENTERED layout (0) is provided";
   if (cfg.precision < FDTD_PREC_FP64_PLAIN || cfg.precision > FDTD_PREC_FP16S)
@@ -325,10 +345,10 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
   if (cfg.point_source_kind == FDTD_SOURCE_GAUSSIAN && !(cfg.point_source_bandwidth > 0))
     return "Gaussian point source needs a positive bandwidth";
   g.tmz = cfg.mode == FDTD_MODE_TMZ;
-  g.flat = ms->flat;
+  g.drop = (int) ms->drop;
+  auto active = [&] (int a) { return !((g.drop >> a) & 1); };
   for (int a = 0; a < 3; ++a)
-    g.n[a] = a == g.flat ? 1 : cfg.size[a];
-  auto active = [&] (int a) { return a != g.flat; };
+    g.n[a] = active (a) ? cfg.size[a] : 1;
   for (int a = 0; a < 3; ++a)
   {
     if (!active (a))
@@ -368,7 +388,7 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
   double s3 = std::sin (g.a3), c3 = std::cos (g.a3);
   for (int k = 0; k < 6; ++k)
     g.proj[k] = 0;
-  if (g.flat < 0)
+  if (ms->form == INC_3D)
   {
     // the Hz projection carries the reference's leading minus sign
     g.proj[EX] = c3 * g.s2 - s3 * g.c1 * g.c2;
@@ -381,15 +401,36 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
     g.zero_inc[1] = cfg.tfsf_left[1] - 2.5 * std::sin (g.a1) * std::sin (g.a2);
     g.zero_inc[2] = cfg.tfsf_left[2] - 2.5 * std::cos (g.a1);
   }
+  else if (ms->form == INC_1D)
+  {
+    // the one kept axis; the origin is 2.5 cells before the left TF/SF border
+    int a0 = 0;
+    while (!active (a0))
+      ++a0;
+    g.inc_ax[0] = g.inc_ax[1] = a0;
+    g.inc_k[0] = 1.0;
+    g.inc_k[1] = 0.0;
+    g.zero_inc[0] = g.zero_inc[1] = g.zero_inc[2] = 0;
+    g.zero_inc[a0] = cfg.tfsf_left[a0] - 2.5;
+    switch (cfg.mode)
+    {
+      case FDTD_MODE_EXHY: g.proj[EX] = -1.0; g.proj[HY] = -1.0; break;
+      case FDTD_MODE_EXHZ: g.proj[EX] = 1.0; g.proj[HZ] = -1.0; break;
+      case FDTD_MODE_EYHX: g.proj[EY] = -1.0; g.proj[HX] = 1.0; break;
+      case FDTD_MODE_EYHZ: g.proj[EY] = -1.0; g.proj[HZ] = -1.0; break;
+      case FDTD_MODE_EZHX: g.proj[EZ] = 1.0; g.proj[HX] = 1.0; break;
+      default: g.proj[EZ] = 1.0; g.proj[HY] = -1.0; break;   // FDTD_MODE_EZHY
+    }
+  }
   else
   {
     // plane axes (a0, a1) in x, y, z order; the origin is the left TF/SF
     // corner moved back 2.5 cells along the in-plane wave vector
-    const int a0 = g.flat == 0 ? 1 : 0, a1 = g.flat == 2 ? 1 : 2;
+    const int a0 = active (0) ? 0 : 1, a1 = active (2) ? 2 : 1;
     g.inc_ax[0] = a0;
     g.inc_ax[1] = a1;
     g.zero_inc[0] = g.zero_inc[1] = g.zero_inc[2] = 0;
-    if (ms->by_teta)
+    if (ms->form == INC_TETA)
     {
       g.inc_k[0] = std::sin (g.a1);
       g.inc_k[1] = std::cos (g.a1);
@@ -443,7 +484,7 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
   {
     g.sigma[a].assign (g.n[a], 0.0);
     if (cfg.use_pml && active (a))
-      sigma_profile (g.sigma[a], a == (g.flat == 0 ? 1 : 0), g.n[a], cfg.pml[a], cfg.dx);
+      sigma_profile (g.sigma[a], a == (active (0) ? 0 : (active (1) ? 1 : 2)), g.n[a], cfg.pml[a], cfg.dx);
   }
 
   Pred preds[6][6];
@@ -544,7 +585,7 @@ std::vector<double> sigma_at (const Geometry &g, int k, int b)
   int a = k % 3;
   bool isH = k >= 3;
   bool averaged = isH ? (b != a) : (b == a);
-  if (b == g.flat)
+  if ((g.drop >> b) & 1)
     averaged = false;
   for (int i = 0; i < n; ++i)
     out[i] = (averaged && i + 1 < n) ? (s[i] + s[i + 1]) / 2.0 : s[i];

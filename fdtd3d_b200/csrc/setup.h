@@ -55,10 +55,10 @@ struct Geometry
   int n[3];                   // grid size (1 along the axis a 2-D mode drops)
   int64_t cells;
   bool tmz;                   // Dim2_TMz (the mode of the adjoint and the batches)
-  int flat = -1;              // axis a 2-D mode drops, -1 in 3-D
-  // 2-D modes: distance of the incident wave along the wave vector is
+  int drop = 0;               // bit a: axis a has size 1 (one axis in 2-D, two in 1-D)
+  // 2-D / 1-D modes: distance of the incident wave along the wave vector is
   // u k0 + v k1 with u, v the positions along inc_ax[0], inc_ax[1]
-  // (InternalScheme.cpp:229-307)
+  // (InternalScheme.cpp:110-307)
   int inc_ax[2] = {0, 1};
   double inc_k[2] = {0, 0};
   int levels;                 // stored time levels (2, or 3 with metamaterials)

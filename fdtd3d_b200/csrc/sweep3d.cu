@@ -1363,7 +1363,7 @@ std::string sweep3d_plan (SweepPlan &plan, const FusedParams &p, void *const e[2
                           unsigned long long *ctr, bool lean)
 {
   const int *n = p.g.n;
-  if (p.g.flat >= 0)
+  if (p.g.drop != 0)
     return "2-D grid";
   if (p.use_meta)
     return "metamaterials";

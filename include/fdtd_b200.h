@@ -54,6 +54,13 @@ typedef struct fdtd_ctx fdtd_ctx;
 #define FDTD_MODE_TEZ 6          /* Dim2_TEz: Ex, Ey, Hz in the x-y plane */
 #define FDTD_MODE_TMX 7          /* Dim2_TMx: Ex, Hy, Hz in the y-z plane */
 #define FDTD_MODE_TMY 8          /* Dim2_TMy: Ey, Hx, Hz in the x-z plane */
+/* 1-D modes keep one axis (sizes of the other two are ignored) */
+#define FDTD_MODE_EXHY 10        /* Dim1_ExHy: Ex, Hy along z */
+#define FDTD_MODE_EXHZ 11        /* Dim1_ExHz: Ex, Hz along y */
+#define FDTD_MODE_EYHX 12        /* Dim1_EyHx: Ey, Hx along z */
+#define FDTD_MODE_EYHZ 13        /* Dim1_EyHz: Ey, Hz along x */
+#define FDTD_MODE_EZHX 14        /* Dim1_EzHx: Ez, Hx along y */
+#define FDTD_MODE_EZHY 15        /* Dim1_EzHy: Ez, Hy along x */
 
 /* arithmetic forms */
 #define FDTD_PREC_FP64_PLAIN 0   /* reference formulation, FP64, bit-faithful */
@@ -82,7 +89,7 @@ typedef struct fdtd_ctx fdtd_ctx;
 
 /*
  * Run configuration.  Mirrors fdtd3d's Settings flags (Source/Settings/Settings.inc.h):
- * --3d/--2d-te{x,y,z}/--2d-tm{x,y,z}, --size, --pml-size, --tfsf-size-left/right, --dx, --wavelength,
+ * --3d/--2d-te{x,y,z}/--2d-tm{x,y,z}/--1d-*, --size, --pml-size, --tfsf-size-left/right, --dx, --wavelength,
  * --courant-factor, --angle-teta/phi/psi, --use-pml, --use-tfsf,
  * --use-metamaterials, --point-source, --point-source-e*, --layout-type.
  * Float flags hold the values exactly as the reference parses them

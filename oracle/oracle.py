@@ -191,23 +191,27 @@ def write_material_txt(path: str, arr: np.ndarray) -> None:
             f.write(" ".join(str(int(q)) for q in i) + " " + repr(float(v)) + "\n")
 
 
-# reference mode flags (Source/Settings/Settings.inc.h:48-60) and the axis
-# each 2-D mode drops
-MODE_FLAGS = {2: "--2d-tmz", 3: "--3d", 4: "--2d-tex", 5: "--2d-tey", 6: "--2d-tez", 7: "--2d-tmx", 8: "--2d-tmy"}
-MODE_FLAT = {2: 2, 4: 0, 5: 1, 6: 2, 7: 0, 8: 1}
+# reference mode flags (Source/Settings/Settings.inc.h:48-60) and the axes
+# each mode keeps
+MODE_FLAGS = {2: "--2d-tmz", 3: "--3d", 4: "--2d-tex", 5: "--2d-tey", 6: "--2d-tez", 7: "--2d-tmx", 8: "--2d-tmy",
+              10: "--1d-exhy", 11: "--1d-exhz", 12: "--1d-eyhx", 13: "--1d-eyhz", 14: "--1d-ezhx", 15: "--1d-ezhy"}
+MODE_KEPT = {2: (0, 1), 3: (0, 1, 2), 4: (1, 2), 5: (0, 2), 6: (0, 1), 7: (1, 2), 8: (0, 2),
+             10: (2,), 11: (1,), 12: (2,), 13: (0,), 14: (1,), 15: (0,)}
 
 
 def mode_axes(mode):
     """The axes a mode keeps (x, y, z order)."""
-    return tuple(a for a in range(3) if a != MODE_FLAT.get(mode))
+    return MODE_KEPT[mode]
 
 
 def _plane(v, mode, default):
-    """Per-axis triple of a mode: a pair gives the kept axes of a 2-D mode."""
+    """Per-axis triple of a mode: a sequence as long as the kept axes gives
+    those axes of a 2-D or 1-D mode."""
     axes = mode_axes(mode)
-    if v is not None and not isinstance(v, (int, np.integer)) and len(v) == 2 and len(axes) == 2:
+    if v is not None and not isinstance(v, (int, np.integer)) and len(v) == len(axes) and len(axes) < 3:
         t = [default] * 3
-        t[axes[0]], t[axes[1]] = int(v[0]), int(v[1])
+        for a, val in zip(axes, v):
+            t[a] = int(val)
         return tuple(t)
     return _triple(v, default)
 
