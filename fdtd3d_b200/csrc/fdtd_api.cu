@@ -105,6 +105,12 @@ struct fdtd_ctx
   std::string sweep_why;
   const char *step_kernel = "not_stepped";
   TfsfBand band;                          // TF/SF post pass of the sweep (band.cells > 0 when in use)
+  std::vector<BandBox> band_host;         // its boxes, on the host
+  // metamaterials with the sweep: the box of the Drude cells, fixed up after
+  // each sweep step (drude_fix), and its device scratch
+  bool drude_fix = false;
+  DrudeBox drude_box{};
+  int *drude_box_dev = nullptr;
 
   // running DFT of one component on one plane (dft_comp < 0: none)
   int dft_comp = -1, dft_axis = 0, dft_index = 0, dft_nf = 0;
@@ -630,6 +636,7 @@ int plan_sweep (fdtd_ctx *ctx)
       ctx->band.nblk = (int) blk.size ();
       CK (cudaStreamSynchronize (ctx->stream));
       ctx->band.nbox = (int) boxes.size ();
+      ctx->band_host = boxes;
       long long cells = 0;
       for (const BandBox &bb : boxes)
         cells += (long long) (bb.hi[0] - bb.lo[0]) * (bb.hi[1] - bb.lo[1]) * (bb.hi[2] - bb.lo[2]);
@@ -647,6 +654,58 @@ int plan_sweep (fdtd_ctx *ctx)
       chunk = std::max (1, std::atoi (v));
     why = sweep3d_plan (ctx->sweep, ctx->fused, e, h, aux, ctx->mat32[0], ctx->sm_count, wy, chunk,
                         ctx->sweep_ctr, lean);
+  }
+  // Drude cells: fixed up after each sweep step when their box (and the H
+  // cells one step below it) holds no PML cell, no TF/SF band cell and no
+  // point source, and the TF/SF corrections (if any) run as the post pass
+  ctx->drude_fix = false;
+  if (why.empty () && g.cfg.use_metamaterials)
+  {
+    if (!ctx->drude_box_dev)
+      DALLOC (ctx->drude_box_dev, 6 * sizeof (int));
+    ctx->launches += launch_drude_box (ctx->dflag, g.n[0], g.n[1], g.n[2], ctx->drude_box_dev, ctx->stream);
+    int hb[6];
+    CK (cudaMemcpyAsync (hb, ctx->drude_box_dev, sizeof (hb), cudaMemcpyDeviceToHost, ctx->stream));
+    CK (cudaStreamSynchronize (ctx->stream));
+    if (hb[3] >= 0)
+    {
+      DrudeBox b;
+      for (int a = 0; a < 3; ++a)
+      {
+        b.lo[a] = hb[a];
+        b.hi[a] = hb[3 + a] + 1;
+      }
+      int ext_lo[3];
+      for (int a = 0; a < 3; ++a)
+        ext_lo[a] = std::max (b.lo[a] - 1, 1);
+      for (int k = 0; k < 6 && why.empty (); ++k)
+        for (int a = 0; a < 3; ++a)
+          if (ext_lo[a] < ctx->fused.ilo[k][a] || b.hi[a] > ctx->fused.ihi[k][a])
+            why = "Drude cells next to the PML";
+      if (why.empty () && g.cfg.use_tfsf && !ctx->fused.tfsf_post)
+        why = "Drude cells with TF/SF corrections inside the sweep";
+      for (const BandBox &bb : ctx->band_host)
+      {
+        bool hit = true;
+        for (int a = 0; a < 3; ++a)
+          hit = hit && bb.lo[a] < b.hi[a] && ext_lo[a] < bb.hi[a];
+        if (hit && why.empty ())
+          why = "Drude cells on the TF/SF band";
+      }
+      if (why.empty () && g.cfg.point_source_mask)
+      {
+        bool in = true;
+        for (int a = 0; a < 3; ++a)
+          in = in && g.cfg.point_source[a] >= ext_lo[a] && g.cfg.point_source[a] < b.hi[a];
+        if (in)
+          why = "a point source among the Drude cells";
+      }
+      if (why.empty ())
+      {
+        ctx->drude_box = b;
+        ctx->drude_fix = true;
+      }
+    }
   }
   ctx->sweep_why = why;
   if (why.empty ())
@@ -939,6 +998,8 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
       if (ctx->sweep_state == 1)
       {
         ctx->launches += launch_sweep3d (ctx->sweep, o, f, ctx->d_err, s);
+        if (ctx->drude_fix)
+          ctx->launches += launch_drude_fixup (f, ctx->drude_box, s);
         if (f.tfsf_post)
           ctx->launches += launch_tfsf_post (ctx->band, f, ctx->d_err, s);
         ctx->step_kernel = "sweep3d_tma";
@@ -1114,6 +1175,8 @@ int fdtd_upload_material_device (fdtd_ctx *ctx, int which, const double *dev)
     ctx->launches += launch_drude_flags (ctx->dflag, ctx->drude32[0], ctx->drude32[2], ctx->drude32[1],
                                          ctx->drude32[3], ctx->g.n[0], ctx->g.n[1], ctx->g.n[2], ctx->stream);
     CK (cudaGetLastError ());
+    if (ctx->sweep_state != 0)
+      ctx->sweep_state = 0;   // the Drude cells changed: plan again at the next step
     return FDTD_OK;
   }
   if (!ctx->mat32[which])

@@ -19,6 +19,8 @@
 // The arithmetic is the formulation of fast_kernels.cu (H stored as
 // eta0*H, PML auxiliaries D/eps0 and c*B touched only in PML cells).
 #include <cuda_fp16.h>
+#include <climits>
+#include <algorithm>
 #include <cuda_runtime.h>
 
 #include "fused3d.h"
@@ -561,6 +563,174 @@ int launch_fused3d (const FusedParams &p, int *err, cudaStream_t s)
     default: launch_shape<6, 4> (p, err, s); break;
   }
   return 1;
+}
+
+namespace {
+
+// Bounding box of the cells with any Drude flag: box[0..2] = lowest x, y, z
+// (atomicMin from INT_MAX), box[3..5] = highest (atomicMax from -1).
+__global__ void drude_box_kernel (const unsigned char *flags, int nx, int ny, int nz, int *box)
+{
+  const size_t n = (size_t) nx * ny * nz;
+  int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {-1, -1, -1};
+  for (size_t id = (size_t) blockIdx.x * blockDim.x + threadIdx.x; id < n; id += (size_t) gridDim.x * blockDim.x)
+  {
+    if (!flags[id])
+      continue;
+    const int pos[3] = {(int) (id / ((size_t) ny * nz)), (int) ((id / nz) % ny), (int) (id % nz)};
+    for (int a = 0; a < 3; ++a)
+    {
+      lo[a] = min (lo[a], pos[a]);
+      hi[a] = max (hi[a], pos[a]);
+    }
+  }
+  for (int a = 0; a < 3; ++a)
+  {
+    for (int o = 16; o > 0; o >>= 1)
+    {
+      lo[a] = min (lo[a], __shfl_xor_sync (0xffffffffu, lo[a], o));
+      hi[a] = max (hi[a], __shfl_xor_sync (0xffffffffu, hi[a], o));
+    }
+    if ((threadIdx.x & 31) == 0 && hi[a] >= 0)
+    {
+      atomicMin (box + a, lo[a]);
+      atomicMax (box + 3 + a, hi[a]);
+    }
+  }
+}
+
+// Drude fix-up after a TMA sweep step, which updates every cell with the
+// plain (or PML) rule.  E pass: the Drude components of the cells of the box
+// are recomputed from the old buffers with update_drude (curl of H_old, the
+// sweep's operation order).  H pass, after it, over the box moved out by one
+// cell on the low sides (every H cell whose curl reads an E value of the
+// box): H_new recomputed from H_old and the corrected E_new with the rule of
+// the cell (Drude, PML or plain).  The box holds no point source, no PML
+// cell and no TF/SF band cell (the host checks), so no other rule applies.
+template <typename T>
+__global__ void __launch_bounds__ (256) drude_fix_e_kernel (const __grid_constant__ FusedParams p, DrudeBox b)
+{
+  const int ny = p.g.n[1], nz = p.g.n[2];
+  const size_t sx = (size_t) ny * nz;
+  const int ez = b.hi[2] - b.lo[2], ey = b.hi[1] - b.lo[1];
+  const long long total = (long long) (b.hi[0] - b.lo[0]) * ey * ez;
+  const T *Ho0 = (const T *) p.h_old[0], *Ho1 = (const T *) p.h_old[1], *Ho2 = (const T *) p.h_old[2];
+  for (long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long) gridDim.x * blockDim.x)
+  {
+    const int z = b.lo[2] + (int) (t % ez);
+    const int y = b.lo[1] + (int) ((t / ez) % ey);
+    const int x = b.lo[0] + (int) (t / ((long long) ez * ey));
+    const size_t id = (size_t) x * sx + (size_t) y * nz + z;
+    const unsigned fl = p.dflag[id];
+    if (!(fl & 7u))
+      continue;
+    if (fl & 1u)
+    {
+      const float c = (ldf (Ho2, id) - ldf (Ho2, id - nz)) - (ldf (Ho1, id) - ldf (Ho1, id - 1));
+      stf ((T *) p.e_new[0], id, update_drude (p, 0, ldf ((const T *) p.e_old[0], id), c, x, y, z, id, true));
+    }
+    if (fl & 2u)
+    {
+      const float c = (ldf (Ho0, id) - ldf (Ho0, id - 1)) - (ldf (Ho2, id) - ldf (Ho2, id - sx));
+      stf ((T *) p.e_new[1], id, update_drude (p, 1, ldf ((const T *) p.e_old[1], id), c, x, y, z, id, true));
+    }
+    if (fl & 4u)
+    {
+      const float c = (ldf (Ho1, id) - ldf (Ho1, id - sx)) - (ldf (Ho0, id) - ldf (Ho0, id - nz));
+      stf ((T *) p.e_new[2], id, update_drude (p, 2, ldf ((const T *) p.e_old[2], id), c, x, y, z, id, true));
+    }
+  }
+}
+
+// E_new values the H pass reads were written by the E pass (or the sweep)
+// before this launch, so plain loads (not the read-only path) are used.
+template <typename T>
+__device__ __forceinline__ float ld_new (const T *p, size_t i);
+template <>
+__device__ __forceinline__ float ld_new<float> (const float *p, size_t i)
+{
+  return p[i];
+}
+template <>
+__device__ __forceinline__ float ld_new<__half> (const __half *p, size_t i)
+{
+  return __half2float (p[i]);
+}
+
+template <typename T>
+__global__ void __launch_bounds__ (256) drude_fix_h_kernel (const __grid_constant__ FusedParams p, DrudeBox b)
+{
+  const int ny = p.g.n[1], nz = p.g.n[2];
+  const size_t sx = (size_t) ny * nz;
+  const int ez = b.hi[2] - b.lo[2], ey = b.hi[1] - b.lo[1];
+  const long long total = (long long) (b.hi[0] - b.lo[0]) * ey * ez;
+  const T *E0 = (const T *) p.e_new[0], *E1 = (const T *) p.e_new[1], *E2 = (const T *) p.e_new[2];
+  for (long long t = (long long) blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long) gridDim.x * blockDim.x)
+  {
+    const int z = b.lo[2] + (int) (t % ez);
+    const int y = b.lo[1] + (int) ((t / ez) % ey);
+    const int x = b.lo[0] + (int) (t / ((long long) ez * ey));
+    const size_t id = (size_t) x * sx + (size_t) y * nz + z;
+    const unsigned fl = p.dflag[id];
+    const float ex = ld_new (E0, id), ey_ = ld_new (E1, id), ez_ = ld_new (E2, id);
+    const float a = (ld_new (E1, id + 1) - ey_) - (ld_new (E2, id + nz) - ez_);
+    const float bb = (ld_new (E2, id + sx) - ez_) - (ld_new (E0, id + 1) - ex);
+    const float c = (ld_new (E0, id + nz) - ex) - (ld_new (E1, id + sx) - ey_);
+    auto inside = [&] (int k) {
+      return x >= p.ilo[k][0] && x < p.ihi[k][0] && y >= p.ilo[k][1] && y < p.ihi[k][1] && z >= p.ilo[k][2] &&
+             z < p.ihi[k][2];
+    };
+    const float h0 = update_any<3, true> (p, fl, inside (3), ldf ((const T *) p.h_old[0], id), a, 1.f, x, y, z, id,
+                                          true);
+    const float h1 = update_any<4, true> (p, fl, inside (4), ldf ((const T *) p.h_old[1], id), bb, 1.f, x, y, z, id,
+                                          true);
+    const float h2 = update_any<5, true> (p, fl, inside (5), ldf ((const T *) p.h_old[2], id), c, 1.f, x, y, z, id,
+                                          true);
+    stf ((T *) p.h_new[0], id, h0);
+    stf ((T *) p.h_new[1], id, h1);
+    stf ((T *) p.h_new[2], id, h2);
+  }
+}
+
+}  // namespace
+
+int launch_drude_box (const unsigned char *flags, int nx, int ny, int nz, int *box, cudaStream_t s)
+{
+  const int init[6] = {INT_MAX, INT_MAX, INT_MAX, -1, -1, -1};
+  if (cudaMemcpyAsync (box, init, sizeof (init), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return 0;
+  size_t n = (size_t) nx * ny * nz;
+  size_t blocks = (n + 255) / 256;
+  if (blocks > 148 * 16)
+    blocks = 148 * 16;
+  drude_box_kernel<<<(unsigned) blocks, 256, 0, s>>> (flags, nx, ny, nz, box);
+  return 1;
+}
+
+int launch_drude_fixup (const FusedParams &p, const DrudeBox &box, cudaStream_t s)
+{
+  DrudeBox hb = box;   // H pass: one more cell on the low sides, within the updated cells
+  for (int a = 0; a < 3; ++a)
+    hb.lo[a] = max (box.lo[a] - 1, 1);
+  auto blocks = [] (const DrudeBox &b) {
+    long long n = 1;
+    for (int a = 0; a < 3; ++a)
+      n *= b.hi[a] - b.lo[a];
+    return (unsigned) std::min<long long> ((n + 255) / 256, 148 * 16);
+  };
+  if (p.fp16)
+  {
+    drude_fix_e_kernel<__half><<<blocks (box), 256, 0, s>>> (p, box);
+    drude_fix_h_kernel<__half><<<blocks (hb), 256, 0, s>>> (p, hb);
+  }
+  else
+  {
+    drude_fix_e_kernel<float><<<blocks (box), 256, 0, s>>> (p, box);
+    drude_fix_h_kernel<float><<<blocks (hb), 256, 0, s>>> (p, hb);
+  }
+  return 2;
 }
 
 int launch_drude_flags (unsigned char *flags, const float *ome, const float *gae, const float *omm, const float *gam,

@@ -58,6 +58,20 @@ int launch_fused3d (const FusedParams &p, int *err, cudaStream_t s);
 // owned y rows of one CTA for a shape variant
 int fused_rows_per_cta (int shape);
 
+// Cells x = lo[0] .. hi[0] - 1 (and the same for y, z).
+struct DrudeBox
+{
+  int lo[3], hi[3];
+};
+
+// Bounding box of the cells with a Drude flag into box[6] (device ints:
+// lowest x, y, z, then highest; INT_MAX / -1 when no cell has one).
+int launch_drude_box (const unsigned char *flags, int nx, int ny, int nz, int *box, cudaStream_t s);
+
+// Drude fix-up of a TMA sweep step over the Drude cells of `box` (two
+// launches; returns how many).
+int launch_drude_fixup (const FusedParams &p, const DrudeBox &box, cudaStream_t s);
+
 // Recomputes the per-cell Drude bitmask from the four material arrays.
 int launch_drude_flags (unsigned char *flags, const float *ome, const float *gae, const float *omm, const float *gam,
                         int nx, int ny, int nz, cudaStream_t s);

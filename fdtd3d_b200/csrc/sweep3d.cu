@@ -1365,8 +1365,6 @@ std::string sweep3d_plan (SweepPlan &plan, const FusedParams &p, void *const e[2
   const int *n = p.g.n;
   if (p.g.drop != 0)
     return "2-D grid";
-  if (p.use_meta)
-    return "metamaterials";
   const int unit = p.fp16 ? 8 : 4;
   if (n[2] % unit != 0)
     return "nz is not a multiple of one 16-byte unit";

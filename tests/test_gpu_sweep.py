@@ -166,3 +166,64 @@ def test_sweep_inline_tfsf_matches_oracle(fdtd, monkeypatch, case):
     assert kernel == "sweep3d_tma", kernel
     errs = _family_err(got, _oracle(case, 36))
     assert errs["E"] <= 1e-5 and errs["H"] <= 1e-5, (case, errs)
+
+
+def _drude_block_case():
+    """A Drude block (eps_inf = 1, omega_p = 2 pi 30 GHz, gamma = 2 pi 1 GHz
+    for eps and mu) two cells inside the TF/SF box, next to a sphere of
+    eps = 4, under an oblique plane wave: the sweep runs with the Drude
+    fix-up."""
+    kw = dict(mode=3, size=(24, 22, 40), use_pml=True, pml=3, use_tfsf=True, tfsf_left=6, tfsf_right=6,
+              teta=20, phi=30, psi=10, use_metamaterials=True)
+    n = kw["size"]
+    om = np.zeros(n)
+    ga = np.zeros(n)
+    om[8:16, 9:15, 17:25] = np.float32(2 * np.pi * 30e9)
+    ga[8:16, 9:15, 17:25] = np.float32(2 * np.pi * 1e9)
+    x, y, z = np.indices(n)
+    eps = np.where((x - 12) ** 2 + (y - 11) ** 2 + (z - 10) ** 2 < 9, 4.0, 1.0)
+    return kw, {"eps": eps, "omegape": om, "omegapm": om, "gammae": ga, "gammam": ga}
+
+
+@pytest.mark.parametrize("prec,tol", [(1, 1e-5), (2, 2e-2)])
+def test_sweep_drude_fixup_matches_oracle(fdtd, monkeypatch, prec, tol):
+    """Metamaterials through the sweep: the Drude cells and the H cells next
+    to them are recomputed after each sweep step.  FP32 / FP16 storage
+    against the FP64 oracle, and FP32 against the register-blocked kernel
+    (same formulation) to <= 1e-6."""
+    kw, mats = _drude_block_case()
+    steps = 60
+    monkeypatch.setenv("FDTDB_SWEEP_VERBOSE", "1")
+    with fdtd.Simulation(materials=mats, precision=prec, **kw) as sim:
+        sim.step(steps)
+        sim.sync()
+        assert sim.step_kernel == "sweep3d_tma", sim.step_kernel
+        got = {c: sim.field(c) for c in COMPS}
+    o = Oracle(materials=mats, **kw)
+    o.step(steps)
+    ref = {c: o.field(c) for c in COMPS}
+    o.close()
+    errs = _family_err(got, ref)
+    assert errs["E"] <= tol and errs["H"] <= tol, (prec, errs)
+    if prec == 1:
+        monkeypatch.setenv("FDTDB_SWEEP", "0")
+        with fdtd.Simulation(materials=mats, precision=prec, **kw) as sim:
+            sim.step(steps)
+            sim.sync()
+            assert sim.step_kernel == "fused3d_regblock", sim.step_kernel
+            rb = {c: sim.field(c) for c in COMPS}
+        errs = _family_err(got, rb)
+        assert errs["E"] <= 1e-6 and errs["H"] <= 1e-6, errs
+
+
+def test_sweep_drude_in_pml_keeps_register_blocked_kernel(fdtd):
+    """Drude cells that reach the PML are not fixed up after the sweep: the
+    register-blocked kernel serves the run."""
+    kw, mats = _drude_block_case()
+    om = np.zeros(kw["size"])
+    om[:, :, 17:25] = np.float32(2 * np.pi * 30e9)
+    mats = dict(mats, omegape=om, omegapm=om)
+    with fdtd.Simulation(materials=mats, precision=1, **kw) as sim:
+        sim.step(4)
+        sim.sync()
+        assert sim.step_kernel == "fused3d_regblock", sim.step_kernel
