@@ -203,18 +203,37 @@ __global__ void __launch_bounds__ (512) tmz_batch_kernel (BatchParams p)
         hy_prev = p.hy[o][id];
         hx_prev = p.hx[o][id];
       }
+      // the old fields of plane x are loaded three planes ahead (a register
+      // ring), so each warp keeps four planes of loads in flight; loads read
+      // only the old buffers and stores go to the new ones
+      const float *Hx = p.hx[o], *Hy = p.hy[o], *Ez = p.ez[o];
+      auto load = [&] (int x, float &a, float &b, float &c, float &d) {
+        a = b = c = 0.f;
+        d = 1.f;
+        if (valid && x <= td.xb + 1)
+        {
+          const long long id = base + (long long) x * ny;
+          a = Hx[id];
+          b = Hy[id];
+          c = Ez[id];
+          if (p.eps)
+            d = p.eps[id];
+        }
+      };
+      float c_hx, c_hy, c_ez, c_ep, n1_hx, n1_hy, n1_ez, n1_ep, n2_hx, n2_hy, n2_ez, n2_ep, n3_hx, n3_hy, n3_ez,
+          n3_ep;
+      load (td.xa, c_hx, c_hy, c_ez, c_ep);
+      load (td.xa + 1, n1_hx, n1_hy, n1_ez, n1_ep);
+      load (td.xa + 2, n2_hx, n2_hy, n2_ez, n2_ep);
+      load (td.xa + 3, n3_hx, n3_hy, n3_ez, n3_ep);
       for (int x = td.xa; x <= td.xb + 1; ++x)
       {
         const long long id = base + (long long) x * ny;
-        float hx = 0.f, hy = 0.f, ez = 0.f, ep = 1.f;
-        if (valid)
-        {
-          hx = p.hx[o][id];
-          hy = p.hy[o][id];
-          ez = p.ez[o][id];
-          if (p.eps)
-            ep = p.eps[id];
-        }
+        const float hx = c_hx, hy = c_hy, ez = c_ez, ep = c_ep;
+        c_hx = n1_hx, c_hy = n1_hy, c_ez = n1_ez, c_ep = n1_ep;
+        n1_hx = n2_hx, n1_hy = n2_hy, n1_ez = n2_ez, n1_ep = n2_ep;
+        n2_hx = n3_hx, n2_hy = n3_hy, n2_ez = n3_ez, n2_ep = n3_ep;
+        load (x + 4, n3_hx, n3_hy, n3_ez, n3_ep);
         const float hx_m = __shfl_up_sync (0xffffffffu, hx, 1);
         float ezn = ez;
         if (lane >= 1 && inner && x <= nx - 2)
