@@ -87,7 +87,8 @@ class Config(ctypes.Structure):
         ("point_source_bandwidth", ctypes.c_double),
         ("precision", ctypes.c_int),
         ("layout", ctypes.c_int),
-        ("reserved", ctypes.c_int * 8),
+        ("source_phase", ctypes.c_int),
+        ("reserved", ctypes.c_int * 7),
     ]
 
 
@@ -182,7 +183,7 @@ def make_config(*, mode=MODE_DIM3, size=(20, 20, 20), pml=None, tfsf_left=None, 
                 dx=0.0005, wavelength=0.02, courant=0.5, teta=90.0, phi=0.0, psi=90.0,
                 use_pml=False, use_tfsf=False, use_metamaterials=False,
                 point_source=(0, 0, 0), point_source_mask=0, point_source_kind=0, point_source_bandwidth=0.0,
-                precision=PREC_FP64_PLAIN) -> Config:
+                precision=PREC_FP64_PLAIN, source_phase=0) -> Config:
     c = Config()
     c.mode = mode
     kept = KEPT_AXES.get(mode, (0, 1, 2))
@@ -199,6 +200,7 @@ def make_config(*, mode=MODE_DIM3, size=(20, 20, 20), pml=None, tfsf_left=None, 
     c.point_source_bandwidth = float(point_source_bandwidth)
     c.precision = int(precision)
     c.layout = 0
+    c.source_phase = int(source_phase)
     return c
 
 

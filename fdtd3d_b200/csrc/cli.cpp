@@ -22,7 +22,12 @@
 // to y and z at the point where they are parsed, so a later coordinate flag
 // overrides them (Source/Settings/Settings.cpp:249-261).
 //
-// Extra flag: --precision fp64|fp32|fp16s (default fp64 = the plain form).
+// Extra flags: --precision fp64|fp32|fp16s (default fp64 = the plain form);
+// --complex-field-values writes what the reference's complex-field build
+// (COMPLEX_FIELD_VALUES) writes: two runs, sine and cosine sources, give
+// the real and imaginary parts ("coords re im" in TXT dumps, (re, im)
+// pairs in DAT dumps); material files then hold complex values, whose
+// imaginary parts must vanish.
 // Flags of subsystems outside the step path (MPI, NTFF, BMP output, test
 // callbacks) are rejected with a message instead of being ignored.
 #include <sys/time.h>
@@ -48,6 +53,7 @@ struct Opts
   fdtd_config cfg;
   int steps = 100;
   bool save_res = false, save_txt = false, save_dat = false, manual = false;
+  bool complex_values = false;   // --complex-field-values: the reference's complex-field build
   int save_start[3] = {0, 0, 0}, save_end[3] = {0, 0, 0};
   std::string mat_file[6];
   int device = 0;
@@ -159,9 +165,12 @@ int parse (std::vector<std::string> args, Opts &o)
     c.tfsf_left[a] = 4;
     c.tfsf_right[a] = 4;
   }
-  c.dx = stof_like ("0.0005");
-  c.wavelength = stof_like ("0.02");
-  c.courant = stof_like ("0.5");
+  // defaults are the reference's double literals, used as they are; only
+  // values given on the command line pass through stof
+  // (Source/Settings/Settings.inc.h:192-194, Settings.h:200-215)
+  c.dx = 0.0005;
+  c.wavelength = 0.02;
+  c.courant = 0.5;
   c.angle_teta = 90.0;
   c.angle_phi = 0.0;
   c.angle_psi = 90.0;
@@ -272,6 +281,8 @@ int parse (std::vector<std::string> args, Opts &o)
       o.save_txt = true;
     else if (a == "--save-as-dat")
       o.save_dat = true;
+    else if (a == "--complex-field-values")
+      o.complex_values = true;
     else if (a == "--manual-save-coords")
       o.manual = true;
     else if (a == "--save-start-coord" && next (v))
@@ -344,7 +355,7 @@ int parse (std::vector<std::string> args, Opts &o)
 
 // TXT grid loader: "x y [z] value" per line, z fastest; values through stof
 // (Source/File-Management/Loader/TXTLoader.h:60-100).
-bool load_txt (const std::string &path, size_t n, int coords, std::vector<double> &out)
+bool load_txt (const std::string &path, size_t n, int coords, bool complex_values, std::vector<double> &out)
 {
   std::ifstream f (path);
   if (!f)
@@ -359,40 +370,62 @@ bool load_txt (const std::string &path, size_t n, int coords, std::vector<double
     for (int k = 0; k <= coords; ++k)
       ss >> tok;
     out[i++] = (double) std::stof (tok);
+    if (complex_values)
+    {
+      // complex build: "coords re im"; the imaginary part must vanish
+      std::string im;
+      if (!(ss >> im) || std::stof (im) != 0.0f)
+        return false;
+    }
   }
   return i == n;
 }
 
 // DAT grid loader: raw FP64 values of the whole grid, z fastest, and
-// nothing after them (Source/File-Management/Loader/DATLoader.h:52-90).
-bool load_dat (const std::string &path, size_t n, std::vector<double> &out)
+// nothing after them (Source/File-Management/Loader/DATLoader.h:52-90);
+// (re, im) pairs in the complex build, whose imaginary parts must vanish.
+bool load_dat (const std::string &path, size_t n, bool complex_values, std::vector<double> &out)
 {
   std::ifstream f (path, std::ios::binary);
   if (!f)
     return false;
-  out.assign (n, 0.0);
-  f.read (reinterpret_cast<char *> (out.data ()), (std::streamsize) (n * sizeof (double)));
-  if (!f || (size_t) f.gcount () != n * sizeof (double))
+  const size_t per = complex_values ? 2 : 1;
+  std::vector<double> raw (n * per);
+  f.read (reinterpret_cast<char *> (raw.data ()), (std::streamsize) (raw.size () * sizeof (double)));
+  if (!f || (size_t) f.gcount () != raw.size () * sizeof (double))
     return false;
   f.peek ();
-  return f.eof ();
+  if (!f.eof ())
+    return false;
+  out.assign (n, 0.0);
+  for (size_t i = 0; i < n; ++i)
+  {
+    out[i] = raw[i * per];
+    if (complex_values && raw[i * per + 1] != 0.0)
+      return false;
+  }
+  return true;
 }
 
 // Material file by extension (GridFileManager::getFileType, Commons.cpp:46-67).
-bool load_material (const std::string &path, size_t n, int coords, std::vector<double> &out, std::string &why)
+bool load_material (const std::string &path, size_t n, int coords, bool complex_values, std::vector<double> &out,
+                    std::string &why)
 {
   const size_t dot = path.find_last_of ('.');
   const std::string ext = dot == std::string::npos ? "" : path.substr (dot + 1);
+  const std::string note = complex_values ? " (complex values with zero imaginary parts)" : "";
   if (ext == "txt")
-    return load_txt (path, n, coords, out) || (why = "cannot read " + path, false);
+    return load_txt (path, n, coords, complex_values, out) || (why = "cannot read " + path + note, false);
   if (ext == "dat")
-    return load_dat (path, n, out) || (why = "cannot read " + path + " (expects " + std::to_string (n) +
-                                               " FP64 values)", false);
+    return load_dat (path, n, complex_values, out) ||
+           (why = "cannot read " + path + " (expects " + std::to_string (n) + " FP64 values)" + note, false);
   why = path + ": material files are .txt or .dat";
   return false;
 }
 
-bool save_dat (const std::string &name, const std::vector<double> &v, const int n[3], const int lo[3], const int hi[3])
+// im: imaginary parts (complex build: (re, im) pairs), or null
+bool save_dat (const std::string &name, const std::vector<double> &v, const std::vector<double> *im, const int n[3],
+               const int lo[3], const int hi[3])
 {
   std::ofstream f (name, std::ios::binary);
   if (!f)
@@ -401,13 +434,22 @@ bool save_dat (const std::string &name, const std::vector<double> &v, const int 
     for (int y = lo[1]; y < hi[1]; ++y)
     {
       const size_t id = ((size_t) x * n[1] + y) * n[2] + lo[2];
-      f.write (reinterpret_cast<const char *> (v.data () + id), (std::streamsize) ((hi[2] - lo[2]) * sizeof (double)));
+      if (!im)
+      {
+        f.write (reinterpret_cast<const char *> (v.data () + id), (std::streamsize) ((hi[2] - lo[2]) * sizeof (double)));
+        continue;
+      }
+      for (int z = lo[2]; z < hi[2]; ++z)
+      {
+        const double pair[2] = {v[id + (z - lo[2])], (*im)[id + (z - lo[2])]};
+        f.write (reinterpret_cast<const char *> (pair), sizeof (pair));
+      }
     }
   return (bool) f;
 }
 
-bool save_txt (const std::string &name, const std::vector<double> &v, const int n[3], unsigned drop,
-               const int lo[3], const int hi[3])
+bool save_txt (const std::string &name, const std::vector<double> &v, const std::vector<double> *im, const int n[3],
+               unsigned drop, const int lo[3], const int hi[3])
 {
   std::ofstream f (name);
   if (!f)
@@ -426,7 +468,10 @@ bool save_txt (const std::string &name, const std::vector<double> &v, const int 
             f << (first ? "" : " ") << c[a];
             first = false;
           }
-        f << " " << v[id] << std::endl;
+        f << " " << v[id];
+        if (im)
+          f << " " << (*im)[id];
+        f << std::endl;
       }
   return true;
 }
@@ -439,10 +484,29 @@ int main (int argc, char **argv)
   std::vector<std::string> args (argv + 1, argv + argc);
   if (parse (args, o))
     return 1;
-  fdtd_ctx *ctx = nullptr;
-  int st = fdtd_create (&o.cfg, o.device, &ctx);
-  if (st)
-    return fail (std::string ("fdtd_create: ") + fdtd_status_str (st) + ": " + fdtd_last_error ());
+  // the complex-field build's run is the sine-source run (real part) plus i
+  // times the cosine-source run (imaginary part): one context for each
+  const int nrun = o.complex_values ? 2 : 1;
+  std::vector<fdtd_ctx *> ctx (nrun, nullptr);
+  struct Release
+  {
+    std::vector<fdtd_ctx *> &c;
+    ~Release ()
+    {
+      for (fdtd_ctx *x : c)
+        if (x)
+          fdtd_destroy (x);
+    }
+  } release{ctx};
+  int st = 0;
+  for (int r = 0; r < nrun; ++r)
+  {
+    fdtd_config cfg = o.cfg;
+    cfg.source_phase = r;
+    st = fdtd_create (&cfg, o.device, &ctx[r]);
+    if (st)
+      return fail (std::string ("fdtd_create: ") + fdtd_status_str (st) + ": " + fdtd_last_error ());
+  }
   const unsigned drop = dropped_axes (o.cfg.mode);
   int n[3] = {o.cfg.size[0], o.cfg.size[1], o.cfg.size[2]};
   int kept = 0;
@@ -460,17 +524,21 @@ int main (int argc, char **argv)
       continue;
     std::vector<double> a;
     std::string why;
-    if (!load_material (o.mat_file[m], cells, kept, a, why))
+    if (!load_material (o.mat_file[m], cells, kept, o.complex_values, a, why))
       return fail (why);
-    st = fdtd_upload_material (ctx, m, a.data ());
-    if (st)
-      return fail (std::string ("fdtd_upload_material: ") + fdtd_last_error ());
+    for (int r = 0; r < nrun; ++r)
+    {
+      st = fdtd_upload_material (ctx[r], m, a.data ());
+      if (st)
+        return fail (std::string ("fdtd_upload_material: ") + fdtd_last_error ());
+    }
   }
   struct timeval tv1, tv2;
   gettimeofday (&tv1, nullptr);
-  st = fdtd_step (ctx, 0, (uint32_t) o.steps);
-  if (!st)
-    st = fdtd_sync (ctx, -1);
+  for (int r = 0; r < nrun && !st; ++r)
+    st = fdtd_step (ctx[r], 0, (uint32_t) o.steps);
+  for (int r = 0; r < nrun && !st; ++r)
+    st = fdtd_sync (ctx[r], -1);
   gettimeofday (&tv2, nullptr);
   if (st)
     return fail (std::string ("step: ") + fdtd_status_str (st) + ": " + fdtd_last_error ());
@@ -499,21 +567,25 @@ int main (int argc, char **argv)
       lo[2] = n[2] / 2;
       hi[2] = n[2] / 2 + 1;
     }
-    std::vector<double> buf (cells);
+    std::vector<double> buf[2];
     for (int k = 0; k < 6; ++k)
     {
       if (!((mode_components (o.cfg.mode) >> k) & 1u))
         continue;
-      st = fdtd_download_field (ctx, k, buf.data ());
-      if (st)
-        return fail (std::string ("download: ") + fdtd_last_error ());
+      for (int r = 0; r < nrun; ++r)
+      {
+        buf[r].resize (cells);
+        st = fdtd_download_field (ctx[r], k, buf[r].data ());
+        if (st)
+          return fail (std::string ("download: ") + fdtd_last_error ());
+      }
+      const std::vector<double> *im = o.complex_values ? &buf[1] : nullptr;
       const std::string base = "previous-1_[timestep=" + std::to_string (o.steps) + "]_[pid=0]_[name=" + names[k] + "]";
-      if (o.save_txt && !save_txt (base + ".txt", buf, n, drop, lo, hi))
+      if (o.save_txt && !save_txt (base + ".txt", buf[0], im, n, drop, lo, hi))
         return fail ("cannot write " + base + ".txt");
-      if (o.save_dat && !save_dat (base + ".dat", buf, n, lo, hi))
+      if (o.save_dat && !save_dat (base + ".dat", buf[0], im, n, lo, hi))
         return fail ("cannot write " + base + ".dat");
     }
   }
-  fdtd_destroy (ctx);
   return 0;
 }

@@ -344,6 +344,8 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
     return "unknown point-source kind";
   if (cfg.point_source_kind == FDTD_SOURCE_GAUSSIAN && !(cfg.point_source_bandwidth > 0))
     return "Gaussian point source needs a positive bandwidth";
+  if (cfg.source_phase != 0 && cfg.source_phase != 1)
+    return "source_phase must be 0 (sine) or 1 (cosine)";
   g.tmz = cfg.mode == FDTD_MODE_TMZ;
   g.drop = (int) ms->drop;
   auto active = [&] (int a) { return !((g.drop >> a) & 1); };
@@ -594,7 +596,8 @@ std::vector<double> sigma_at (const Geometry &g, int k, int b)
 
 double incident_source (const Geometry &g, uint32_t t)
 {
-  return std::sin (g.dt * t * 2 * kPi * g.freq);
+  const double arg = g.dt * t * 2 * kPi * g.freq;
+  return g.cfg.source_phase ? std::cos (arg) : std::sin (arg);
 }
 
 double point_source (const Geometry &g, uint32_t t, bool h)
@@ -605,9 +608,11 @@ double point_source (const Geometry &g, uint32_t t, bool h)
     // Gaussian-modulated pulse: spectral FWHM = bandwidth * f
     double w = 4.0 * std::sqrt (std::log (2.0)) / (kPi * g.freq * g.cfg.point_source_bandwidth);
     double tau = g.dt * ts - 3.0 * w;
-    return std::exp (-(tau / w) * (tau / w)) * std::sin (2 * kPi * g.freq * tau);
+    const double carrier = g.cfg.source_phase ? std::cos (2 * kPi * g.freq * tau) : std::sin (2 * kPi * g.freq * tau);
+    return std::exp (-(tau / w) * (tau / w)) * carrier;
   }
-  return std::sin (g.dt * ts * 2 * kPi * g.freq);
+  const double arg = g.dt * ts * 2 * kPi * g.freq;
+  return g.cfg.source_phase ? std::cos (arg) : std::sin (arg);
 }
 
 }  // namespace fdtdb

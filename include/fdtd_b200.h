@@ -117,7 +117,11 @@ typedef struct
   double point_source_bandwidth; /* kind 1: spectral FWHM / f (e.g. 0.5) */
   int precision;            /* FDTD_PREC_* */
   int layout;               /* 0 = E_CENTERED (the only layout provided) */
-  int reserved[8];
+  int source_phase;         /* 0: sine sources; 1: cosine sources.  The reference's complex-field
+                               build drives sin + i cos (InternalScheme.inc.h:2888-2890, 3312-3313);
+                               with real materials its fields are the run with phase 0 plus i times
+                               the run with phase 1 */
+  int reserved[7];
 } fdtd_config;
 
 /* Point-source kinds.  Kind 0 is the reference's hard source

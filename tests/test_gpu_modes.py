@@ -140,3 +140,54 @@ def test_exhy_1d_reproduces_reference_unit_test_vector(fdtd, monkeypatch):
     for k, (re, _im) in g["ex"].items():
         assert abs(ex[int(k)] - re) <= 1e-15, (k, ex[int(k)], re)
     assert ex[6] == 0.0 and ex[13] == 0.0
+
+
+REF_COMPLEX = os.path.join(os.path.dirname(REF_BIN), "fdtd3d_complex")
+
+
+def _write_complex_txt(path, arr):
+    """Material TXT of the complex build: "coords re im" per line."""
+    arr = np.asarray(arr, dtype=np.float64)
+    idx = np.indices(arr.shape).reshape(arr.ndim, -1).T
+    with open(path, "w") as f:
+        for i, v in zip(idx, arr.reshape(-1)):
+            f.write(" ".join(str(int(q)) for q in i) + " " + repr(float(v)) + " 0\n")
+
+
+@pytest.mark.parametrize("mode,source", [(3, False), (6, True), (7, False)], ids=["3d", "2d-tez-source", "2d-tmx"])
+def test_cli_complex_matches_reference_complex_build(fdtd, tmp_path, mode, source):
+    """--complex-field-values (two runs: sine and cosine sources) writes the
+    same "coords re im" TXT dumps as the reference's complex-field build."""
+    if not os.path.exists(REF_COMPLEX):
+        pytest.skip("complex reference binary not built")
+    cli = os.path.join(os.path.dirname(fdtd.__file__), "fdtd3d-b200")
+    if mode == 3:
+        flags = ["--3d", "--size", "x:16,y:14,z:18", "--use-pml", "--pml-size", "x:3", "--same-size-pml",
+                 "--use-tfsf", "--tfsf-size-left", "x:5", "--same-size-tfsf", "--tfsf-size-right", "x:5",
+                 "--angle-teta", "30", "--angle-phi", "40", "--angle-psi", "10", "--time-steps", "25",
+                 "--save-res", "--save-as-txt", "--manual-save-coords", "--save-start-coord", "x:0,y:0,z:0",
+                 "--save-end-coord", "x:16,y:14,z:18"]
+        shape = (16, 14, 18)
+    else:
+        flags = _flags(mode, 30, source)
+        shape = _plane_shape(mode)
+    eps = np.where(np.random.default_rng(mode).random(shape) < 0.3, 4.0, 1.0)
+    _write_complex_txt(str(tmp_path / "eps.txt"), eps)
+    flags += ["--load-eps-from-file", str(tmp_path / "eps.txt")]
+    out = {}
+    for name, exe, extra in (("ref", REF_COMPLEX, ["--use-ca-cb", "--use-ca-cb-pml"]),
+                             ("b200", cli, ["--complex-field-values"])):
+        d = tmp_path / name
+        d.mkdir()
+        r = subprocess.run([exe] + flags + extra, cwd=d, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+        out[name] = {f.name: f.read_text() for f in d.iterdir()}
+    assert sorted(out["ref"]) == sorted(out["b200"]) and out["ref"]
+    for fname, ref in out["ref"].items():
+        mine = out["b200"][fname]
+        assert len(ref.splitlines()[0].split()) == len(shape) + 2
+        if mine != ref:
+            diffs = [(a, b) for a, b in zip(ref.splitlines(), mine.splitlines()) if a != b]
+            raise AssertionError(f"{fname}: {len(diffs)} lines differ, first: {diffs[:4]}")
+        im = np.array([float(line.split()[-1]) for line in ref.splitlines()])
+        assert np.max(np.abs(im)) > 0, fname
