@@ -38,6 +38,8 @@ KEPT_AXES = {MODE_DIM3: (0, 1, 2), MODE_TMZ: (0, 1), MODE_TEZ: (0, 1), MODE_TEX:
 PREC_FP64_PLAIN = 0
 PREC_FP32 = 1
 PREC_FP16S = 2
+LAYOUT_E_CENTERED = 0   # --layout-type 0
+LAYOUT_H_CENTERED = 1   # --layout-type 1
 COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
 MODE_COMPONENTS = {MODE_DIM3: COMPONENTS, MODE_TMZ: ("Ez", "Hx", "Hy"), MODE_TEZ: ("Ex", "Ey", "Hz"),
                    MODE_TEX: ("Ey", "Ez", "Hx"), MODE_TMX: ("Ex", "Hy", "Hz"), MODE_TEY: ("Ex", "Ez", "Hy"),
@@ -183,7 +185,7 @@ def make_config(*, mode=MODE_DIM3, size=(20, 20, 20), pml=None, tfsf_left=None, 
                 dx=0.0005, wavelength=0.02, courant=0.5, teta=90.0, phi=0.0, psi=90.0,
                 use_pml=False, use_tfsf=False, use_metamaterials=False,
                 point_source=(0, 0, 0), point_source_mask=0, point_source_kind=0, point_source_bandwidth=0.0,
-                precision=PREC_FP64_PLAIN, source_phase=0) -> Config:
+                precision=PREC_FP64_PLAIN, source_phase=0, layout=LAYOUT_E_CENTERED) -> Config:
     c = Config()
     c.mode = mode
     kept = KEPT_AXES.get(mode, (0, 1, 2))
@@ -199,13 +201,14 @@ def make_config(*, mode=MODE_DIM3, size=(20, 20, 20), pml=None, tfsf_left=None, 
     c.point_source_kind = int(point_source_kind)
     c.point_source_bandwidth = float(point_source_bandwidth)
     c.precision = int(precision)
-    c.layout = 0
+    c.layout = int(layout)
     c.source_phase = int(source_phase)
     return c
 
 
 class Simulation:
-    """One device-resident simulation (one fdtd_ctx), fdtd3d E_CENTERED layout.
+    """One device-resident simulation (one fdtd_ctx); ``layout`` picks the
+    reference's E_CENTERED (default) or H_CENTERED Yee layout.
 
     Arrays are x-major with z fastest (3-D) or (x, y) with y fastest (TMz),
     the reference's CudaGrid linear order.  ``step`` is asynchronous; reads

@@ -337,9 +337,14 @@ int parse (std::vector<std::string> args, Opts &o)
     {
       if (a == ignored_arg[m])
       {
-        if (a == "--layout-type" && next (v) && std::atoi (v.c_str ()) != 0)
-          return fail ("only --layout-type 0 (E_CENTERED) is provided");
-        else if (a != "--layout-type")
+        if (a == "--layout-type")
+        {
+          // Settings.inc.h: 0 = E_CENTERED, 1 = H_CENTERED (main.cpp asserts one of the two)
+          if (!next (v) || (v != "0" && v != "1"))
+            return fail ("--layout-type takes 0 (E_CENTERED) or 1 (H_CENTERED)");
+          c.layout = std::atoi (v.c_str ());
+        }
+        else
           next (v);
         done = true;
       }

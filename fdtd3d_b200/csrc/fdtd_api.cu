@@ -336,7 +336,10 @@ int alloc_fast (fdtd_ctx *ctx)
   size_t n = (size_t) g.cells;
   if (g.cfg.use_metamaterials && g.drop != 0)
     return fail (ctx, FDTD_ERR_UNSUPPORTED, "2-D and 1-D metamaterials are provided by the FP64 plain form only");
-  ctx->has_second = g.drop == 0;
+  // the one-sweep 3-D kernels (register-blocked and TMA) are written for the
+  // E_CENTERED stencil; H_CENTERED and the 2-D / 1-D modes run the per-cell
+  // kernels on one buffer set
+  ctx->has_second = g.drop == 0 && g.cfg.layout == 0;
   for (int b = 0; b < (ctx->has_second ? 2 : 1); ++b)
   {
     for (int k = 0; k < 6; ++k)
@@ -946,7 +949,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
   const bool fused = ctx->kind != 0 && ctx->has_second && !ctx->mat32[1] && ctx->ps_interior;
   if (ctx->kind != 0 && g.cfg.use_metamaterials && !fused)
     return fail (ctx, FDTD_ERR_UNSUPPORTED,
-                 "FP32/FP16 metamaterials need the one-sweep 3-D kernel (uniform mu, interior point source)");
+                 "FP32/FP16 metamaterials need the one-sweep 3-D kernel (E_CENTERED, uniform mu, interior point source)");
 
   for (uint32_t i = 0; i < n; ++i)
   {
@@ -1388,8 +1391,8 @@ int adjoint_entry (fdtd_ctx *ctx, const fdtd_adjoint_cfg *cfg, double *objective
   if (cfg->precision != FDTD_PREC_FP32 && cfg->precision != FDTD_PREC_FP64_PLAIN)
     return fail (ctx, FDTD_ERR_ARG, "adjoint precision must be FP32 or FP64");
   const Geometry &g = ctx->g;
-  if (!g.tmz || g.cfg.use_tfsf || g.cfg.use_metamaterials)
-    return fail (ctx, FDTD_ERR_UNSUPPORTED, "the adjoint covers 2-D TMz point-source runs");
+  if (!g.tmz || g.cfg.use_tfsf || g.cfg.use_metamaterials || g.cfg.layout != 0)
+    return fail (ctx, FDTD_ERR_UNSUPPORTED, "the adjoint covers 2-D TMz point-source runs (E_CENTERED)");
   int r = set_device (ctx);
   if (r != FDTD_OK)
     return r;

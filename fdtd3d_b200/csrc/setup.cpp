@@ -4,7 +4,8 @@
 //   dt, frequency, relPhaseVelocity ... Scheme/InternalScheme.inc.h:3359-3394
 //   numerical phase velocity .......... Layout/Approximation.cpp:259-359
 //   sigma profiles (x vs y/z quirk) ... Scheme/SchemeHelper.h:574-718
-//   Yee offsets / circuit diffs ....... Layout/YeeGridLayout.cpp:1937-1990
+//   Yee offsets / circuit diffs ....... Layout/YeeGridLayout.cpp:1937-2035
+//                                       (E_CENTERED and H_CENTERED)
 //   TF/SF border predicates ........... Layout/YeeGridLayout.h:498-512,
 //                                       Layout/YeeGridLayout.cpp:257-1720
 //   incident projections .............. Layout/YeeGridLayout.h:2227-2357
@@ -203,23 +204,35 @@ const ModeSpec *mode_spec (int mode)
   return nullptr;
 }
 
-// Dim3 E_CENTERED layout of component k; a 2-D or 1-D mode then drops its
-// axes (YeeGridLayout's initAxesCoordinate keeps the coordinates of the
-// kept axes of every offset and position).
-void init_components (Geometry &g, unsigned comps, Pred preds[6][6], int slot_dir[6][4])
+// Dim3 layout of component k; a 2-D or 1-D mode then drops its axes
+// (YeeGridLayout's initAxesCoordinate keeps the coordinates of the kept axes
+// of every offset and position).
+//
+// E_CENTERED (YeeGridLayout.cpp:1937-1990): E_a sits at 1.0 on its own axis
+// and 0.5 on the others, H_a at 0.5 / 1.0.  H_CENTERED (YeeGridLayout.cpp:
+// 1990-2035) swaps the two families: E_a takes E_CENTERED H_a's position,
+// material stencil (YeeGridLayout.h:866-1030) and TF/SF border predicates
+// (YeeGridLayout.cpp:257-1720, checked component by component), and H_a
+// takes E_CENTERED E_a's.  The circuits keep their partners and directions
+// (InternalScheme.inc.h:1840-1895) but their offsets move to the other side:
+// an E circuit spans (0, +1) and an H circuit (-1, 0).
+void init_components (Geometry &g, unsigned comps, bool h_centered, Pred preds[6][6], int slot_dir[6][4])
 {
   for (int k = 0; k < 6; ++k)
   {
     CompLayout &c = g.comp[k];
     std::memset (&c, 0, sizeof (c));
     int a = k % 3;
-    bool isH = k >= 3;
+    // "edge" components sit at 1.0 on their own axis (E in E_CENTERED, H in
+    // H_CENTERED) and average two material cells along it; the others sit at
+    // 0.5 on their own axis and average four
+    bool edge = (k >= 3) == h_centered;
     for (int ax = 0; ax < 3; ++ax)
-      c.min_fp[ax] = isH ? (ax == a ? 0.5 : 1.0) : (ax == a ? 1.0 : 0.5);
+      c.min_fp[ax] = edge ? (ax == a ? 1.0 : 0.5) : (ax == a ? 0.5 : 1.0);
     c.sig_cacb = (a + 1) % 3;
     c.sig4 = a;
     c.sig5 = (a + 2) % 3;
-    if (!isH)
+    if (edge)
     {
       c.nmat = 2;
       c.m[1][a] = 1;
@@ -237,55 +250,62 @@ void init_components (Geometry &g, unsigned comps, Pred preds[6][6], int slot_di
     for (int d = 0; d < 6; ++d)
       preds[k][d].valid = false;
   }
+  // predicates are written for E_CENTERED; H_CENTERED reads them with the
+  // families swapped (Ex <-> Hx, ...)
+  const int pe[3] = {h_centered ? HX : EX, h_centered ? HY : EY, h_centered ? HZ : EZ};
+  const int ph[3] = {h_centered ? EX : HX, h_centered ? EY : HY, h_centered ? EZ : HZ};
+  // circuit offset of the lower and the upper neighbour
+  const int elo = h_centered ? 0 : -1, ehi = h_centered ? 1 : 0;
+  const int hlo = h_centered ? -1 : 0, hhi = h_centered ? 0 : 1;
   CompLayout *c;
   c = &g.comp[EX];
   c->opp1 = HZ; c->opp2 = HY;
-  set3 (c->d11, 0, -1, 0); set3 (c->d12, 0, 0, 0); set3 (c->d21, 0, 0, -1); set3 (c->d22, 0, 0, 0);
+  set3 (c->d11, 0, elo, 0); set3 (c->d12, 0, ehi, 0); set3 (c->d21, 0, 0, elo); set3 (c->d22, 0, 0, ehi);
   slot_dir[EX][0] = DD; slot_dir[EX][1] = DU; slot_dir[EX][2] = DB; slot_dir[EX][3] = DF;
-  preds[EX][DD] = pred (T_RANGE, -1, 1, T_EXL, -5, 0, T_RANGE, 4, -4);
-  preds[EX][DU] = pred (T_RANGE, -1, 1, T_EXR, 5, 0, T_RANGE, 4, -4);
-  preds[EX][DB] = pred (T_RANGE, -1, 1, T_RANGE, 4, -4, T_EXL, -5, 0);
-  preds[EX][DF] = pred (T_RANGE, -1, 1, T_RANGE, 4, -4, T_EXR, 5, 0);
+  preds[pe[0]][DD] = pred (T_RANGE, -1, 1, T_EXL, -5, 0, T_RANGE, 4, -4);
+  preds[pe[0]][DU] = pred (T_RANGE, -1, 1, T_EXR, 5, 0, T_RANGE, 4, -4);
+  preds[pe[0]][DB] = pred (T_RANGE, -1, 1, T_RANGE, 4, -4, T_EXL, -5, 0);
+  preds[pe[0]][DF] = pred (T_RANGE, -1, 1, T_RANGE, 4, -4, T_EXR, 5, 0);
   c = &g.comp[EY];
   c->opp1 = HX; c->opp2 = HZ;
-  set3 (c->d11, 0, 0, -1); set3 (c->d12, 0, 0, 0); set3 (c->d21, -1, 0, 0); set3 (c->d22, 0, 0, 0);
+  set3 (c->d11, 0, 0, elo); set3 (c->d12, 0, 0, ehi); set3 (c->d21, elo, 0, 0); set3 (c->d22, ehi, 0, 0);
   slot_dir[EY][0] = DB; slot_dir[EY][1] = DF; slot_dir[EY][2] = DL; slot_dir[EY][3] = DR;
-  preds[EY][DL] = pred (T_EXL, -5, 0, T_RANGE, -1, 1, T_RANGE, 4, -4);
-  preds[EY][DR] = pred (T_EXR, 5, 0, T_RANGE, -1, 1, T_RANGE, 4, -4);
-  preds[EY][DB] = pred (T_RANGE, 4, -4, T_RANGE, -1, 1, T_EXL, -5, 0);
-  preds[EY][DF] = pred (T_RANGE, 4, -4, T_RANGE, -1, 1, T_EXR, 5, 0);
+  preds[pe[1]][DL] = pred (T_EXL, -5, 0, T_RANGE, -1, 1, T_RANGE, 4, -4);
+  preds[pe[1]][DR] = pred (T_EXR, 5, 0, T_RANGE, -1, 1, T_RANGE, 4, -4);
+  preds[pe[1]][DB] = pred (T_RANGE, 4, -4, T_RANGE, -1, 1, T_EXL, -5, 0);
+  preds[pe[1]][DF] = pred (T_RANGE, 4, -4, T_RANGE, -1, 1, T_EXR, 5, 0);
   c = &g.comp[EZ];
   c->opp1 = HY; c->opp2 = HX;
-  set3 (c->d11, -1, 0, 0); set3 (c->d12, 0, 0, 0); set3 (c->d21, 0, -1, 0); set3 (c->d22, 0, 0, 0);
+  set3 (c->d11, elo, 0, 0); set3 (c->d12, ehi, 0, 0); set3 (c->d21, 0, elo, 0); set3 (c->d22, 0, ehi, 0);
   slot_dir[EZ][0] = DL; slot_dir[EZ][1] = DR; slot_dir[EZ][2] = DD; slot_dir[EZ][3] = DU;
-  preds[EZ][DL] = pred (T_EXL, -5, 0, T_RANGE, 4, -4, T_RANGE, -1, 1);
-  preds[EZ][DR] = pred (T_EXR, 5, 0, T_RANGE, 4, -4, T_RANGE, -1, 1);
-  preds[EZ][DD] = pred (T_RANGE, 4, -4, T_EXL, -5, 0, T_RANGE, -1, 1);
-  preds[EZ][DU] = pred (T_RANGE, 4, -4, T_EXR, 5, 0, T_RANGE, -1, 1);
+  preds[pe[2]][DL] = pred (T_EXL, -5, 0, T_RANGE, 4, -4, T_RANGE, -1, 1);
+  preds[pe[2]][DR] = pred (T_EXR, 5, 0, T_RANGE, 4, -4, T_RANGE, -1, 1);
+  preds[pe[2]][DD] = pred (T_RANGE, 4, -4, T_EXL, -5, 0, T_RANGE, -1, 1);
+  preds[pe[2]][DU] = pred (T_RANGE, 4, -4, T_EXR, 5, 0, T_RANGE, -1, 1);
   c = &g.comp[HX];
   c->opp1 = EY; c->opp2 = EZ;
-  set3 (c->d11, 0, 0, 0); set3 (c->d12, 0, 0, 1); set3 (c->d21, 0, 0, 0); set3 (c->d22, 0, 1, 0);
+  set3 (c->d11, 0, 0, hlo); set3 (c->d12, 0, 0, hhi); set3 (c->d21, 0, hlo, 0); set3 (c->d22, 0, hhi, 0);
   slot_dir[HX][0] = DB; slot_dir[HX][1] = DF; slot_dir[HX][2] = DD; slot_dir[HX][3] = DU;
-  preds[HX][DD] = pred (T_RANGE, 4, -4, T_EXL, 0, 0, T_RANGE, -1, 1);
-  preds[HX][DU] = pred (T_RANGE, 4, -4, T_EXR, 0, 0, T_RANGE, -1, 1);
-  preds[HX][DB] = pred (T_RANGE, 4, -4, T_RANGE, -1, 1, T_EXL, 0, 0);
-  preds[HX][DF] = pred (T_RANGE, 4, -4, T_RANGE, -1, 1, T_EXR, 0, 0);
+  preds[ph[0]][DD] = pred (T_RANGE, 4, -4, T_EXL, 0, 0, T_RANGE, -1, 1);
+  preds[ph[0]][DU] = pred (T_RANGE, 4, -4, T_EXR, 0, 0, T_RANGE, -1, 1);
+  preds[ph[0]][DB] = pred (T_RANGE, 4, -4, T_RANGE, -1, 1, T_EXL, 0, 0);
+  preds[ph[0]][DF] = pred (T_RANGE, 4, -4, T_RANGE, -1, 1, T_EXR, 0, 0);
   c = &g.comp[HY];
   c->opp1 = EZ; c->opp2 = EX;
-  set3 (c->d11, 0, 0, 0); set3 (c->d12, 1, 0, 0); set3 (c->d21, 0, 0, 0); set3 (c->d22, 0, 0, 1);
+  set3 (c->d11, hlo, 0, 0); set3 (c->d12, hhi, 0, 0); set3 (c->d21, 0, 0, hlo); set3 (c->d22, 0, 0, hhi);
   slot_dir[HY][0] = DL; slot_dir[HY][1] = DR; slot_dir[HY][2] = DB; slot_dir[HY][3] = DF;
-  preds[HY][DL] = pred (T_EXL, 0, 0, T_RANGE, 4, -4, T_RANGE, -1, 1);
-  preds[HY][DR] = pred (T_EXR, 0, 0, T_RANGE, 4, -4, T_RANGE, -1, 1);
-  preds[HY][DB] = pred (T_RANGE, -1, 1, T_RANGE, 4, -4, T_EXL, 0, 0);
-  preds[HY][DF] = pred (T_RANGE, -1, 1, T_RANGE, 4, -4, T_EXR, 0, 0);
+  preds[ph[1]][DL] = pred (T_EXL, 0, 0, T_RANGE, 4, -4, T_RANGE, -1, 1);
+  preds[ph[1]][DR] = pred (T_EXR, 0, 0, T_RANGE, 4, -4, T_RANGE, -1, 1);
+  preds[ph[1]][DB] = pred (T_RANGE, -1, 1, T_RANGE, 4, -4, T_EXL, 0, 0);
+  preds[ph[1]][DF] = pred (T_RANGE, -1, 1, T_RANGE, 4, -4, T_EXR, 0, 0);
   c = &g.comp[HZ];
   c->opp1 = EX; c->opp2 = EY;
-  set3 (c->d11, 0, 0, 0); set3 (c->d12, 0, 1, 0); set3 (c->d21, 0, 0, 0); set3 (c->d22, 1, 0, 0);
+  set3 (c->d11, 0, hlo, 0); set3 (c->d12, 0, hhi, 0); set3 (c->d21, hlo, 0, 0); set3 (c->d22, hhi, 0, 0);
   slot_dir[HZ][0] = DD; slot_dir[HZ][1] = DU; slot_dir[HZ][2] = DL; slot_dir[HZ][3] = DR;
-  preds[HZ][DL] = pred (T_EXL, 0, 0, T_RANGE, -1, 1, T_RANGE, 4, -4);
-  preds[HZ][DR] = pred (T_EXR, 0, 0, T_RANGE, -1, 1, T_RANGE, 4, -4);
-  preds[HZ][DD] = pred (T_RANGE, -1, 1, T_EXL, 0, 0, T_RANGE, 4, -4);
-  preds[HZ][DU] = pred (T_RANGE, -1, 1, T_EXR, 0, 0, T_RANGE, 4, -4);
+  preds[ph[2]][DL] = pred (T_EXL, 0, 0, T_RANGE, -1, 1, T_RANGE, 4, -4);
+  preds[ph[2]][DR] = pred (T_EXR, 0, 0, T_RANGE, -1, 1, T_RANGE, 4, -4);
+  preds[ph[2]][DD] = pred (T_RANGE, -1, 1, T_EXL, 0, 0, T_RANGE, 4, -4);
+  preds[ph[2]][DU] = pred (T_RANGE, -1, 1, T_EXR, 0, 0, T_RANGE, 4, -4);
 
   for (int k = 0; k < 6; ++k)
     g.comp[k].exists = (comps >> k) & 1u;
@@ -334,8 +354,8 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
   const ModeSpec *ms = mode_spec (cfg.mode);
   if (!ms)
     return "unknown mode (FDTD_MODE_DIM3, a 2-D or a 1-D mode)";
-  if (cfg.layout != 0)
-    return "only the E_CENTERED layout (0) is provided";
+  if (cfg.layout != 0 && cfg.layout != 1)
+    return "unknown layout (0 = E_CENTERED, 1 = H_CENTERED)";
   if (cfg.precision < FDTD_PREC_FP64_PLAIN || cfg.precision > FDTD_PREC_FP16S)
     return "unknown precision";
   if (cfg.use_metamaterials && !cfg.use_pml)
@@ -491,7 +511,8 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
 
   Pred preds[6][6];
   int slot_dir[6][4];
-  init_components (g, ms->comps, preds, slot_dir);
+  const bool h_centered = cfg.layout == 1;
+  init_components (g, ms->comps, h_centered, preds, slot_dir);
 
   if (cfg.use_tfsf)
   {
@@ -558,9 +579,14 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
           if (overlap)
             return "TF/SF slots overlap";
         }
+        // the reference's isRevertVals: the correction lands on the far
+        // neighbour for E in E_CENTERED and for H in H_CENTERED, and the
+        // incident value is negated for H in E_CENTERED and for E in
+        // H_CENTERED (InternalScheme.inc.h:1386-1835)
+        const bool revert = isH == h_centered;
         TfsfTerm t;
         t.comp = k;
-        t.slot = isH ? s : (s ^ 1);
+        t.slot = revert ? (s ^ 1) : s;
         t.inc_comp = s < 2 ? c.opp1 : c.opp2;
         const int *diffs[4] = {c.d11, c.d12, c.d21, c.d22};
         for (int a = 0; a < 3; ++a)
@@ -569,7 +595,7 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
           t.hi[a] = slot_box[s][1][a];
           t.aux[a] = diffs[t.slot][a];
         }
-        t.negate = isH ? -1.0 : 1.0;
+        t.negate = isH != h_centered ? -1.0 : 1.0;
         if (!g.comp[t.inc_comp].exists)
           continue;
         g.tfsf.push_back (t);
@@ -585,8 +611,9 @@ std::vector<double> sigma_at (const Geometry &g, int k, int b)
   int n = g.n[b];
   std::vector<double> out (n, 0.0);
   int a = k % 3;
-  bool isH = k >= 3;
-  bool averaged = isH ? (b != a) : (b == a);
+  // sigma grids vary along one axis: the two-cell material average of an
+  // edge component spans its own axis, the four-cell one the other two
+  bool averaged = g.comp[k].nmat == 2 ? (b == a) : (b != a);
   if ((g.drop >> b) & 1)
     averaged = false;
   for (int i = 0; i < n; ++i)

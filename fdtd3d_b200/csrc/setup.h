@@ -34,10 +34,10 @@ struct TfsfTerm
   int lo[3];
   int hi[3];       // exclusive
   int aux[3];
-  double negate;   // -1 for H components (E_CENTERED), +1 for E
+  double negate;   // -1 for H in E_CENTERED and for E in H_CENTERED, else +1
 };
 
-// Per-component layout (E_CENTERED).  YeeGridLayout.cpp:1937-1990.
+// Per-component layout (E_CENTERED or H_CENTERED).  YeeGridLayout.cpp:1937-2035.
 struct CompLayout
 {
   bool exists;

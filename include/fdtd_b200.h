@@ -116,7 +116,7 @@ typedef struct
   int point_source_kind;    /* 0: the reference's sin(2 pi f t); 1: Gaussian-modulated (see below) */
   double point_source_bandwidth; /* kind 1: spectral FWHM / f (e.g. 0.5) */
   int precision;            /* FDTD_PREC_* */
-  int layout;               /* 0 = E_CENTERED (the only layout provided) */
+  int layout;               /* 0 = E_CENTERED, 1 = H_CENTERED (--layout-type) */
   int source_phase;         /* 0: sine sources; 1: cosine sources.  The reference's complex-field
                                build drives sin + i cos (InternalScheme.inc.h:2888-2890, 3312-3313);
                                with real materials its fields are the run with phase 0 plus i times

@@ -219,7 +219,7 @@ def _plane(v, mode, default):
 def reference_args(*, mode=3, size=(20, 20, 20), pml=None, tfsf_left=None, tfsf_right=None,
                    dx=0.0005, wavelength=0.02, courant=0.5, teta=90.0, phi=0.0, psi=90.0,
                    use_pml=False, use_tfsf=False, use_metamaterials=False,
-                   point_source=(0, 0, 0), point_source_mask=0, steps=10):
+                   point_source=(0, 0, 0), point_source_mask=0, steps=10, layout=0):
     size = _plane(size, mode, 1)
     names = ("x", "y", "z")
 
@@ -231,6 +231,8 @@ def reference_args(*, mode=3, size=(20, 20, 20), pml=None, tfsf_left=None, tfsf_
             "--dx", repr(dx), "--wavelength", repr(wavelength), "--courant-factor", repr(courant),
             "--angle-teta", repr(teta), "--angle-phi", repr(phi), "--angle-psi", repr(psi),
             "--time-steps", str(steps), "--use-ca-cb", "--log-level", "0"]
+    if layout:
+        args += ["--layout-type", str(layout)]
     if use_pml:
         args += ["--use-pml", "--pml-size", coord(pml), "--use-ca-cb-pml"]
     if use_tfsf:

@@ -43,6 +43,7 @@ def test_status_strings(fdtd):
     dict(use_tfsf=True, tfsf_left=0, tfsf_right=3),
     dict(use_metamaterials=True),
     dict(dx=-1.0),
+    dict(layout=2),
 ])
 def test_create_rejects_bad_config(fdtd, bad):
     lib = fdtd.load_library()

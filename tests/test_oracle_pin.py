@@ -69,3 +69,34 @@ def test_oracle_scalars_are_physical():
     assert s["dt"] == f32(0.0005) * f32(0.5) / 299792458.0
     # oblique propagation is numerically faster than along an axis: pv0 / pv < 1
     assert 0.99 < s["rel_phase_velocity"] < 1.0
+
+
+def test_unit_test_1d_fixture_is_consistent():
+    """unit_test_1d_modes.json (all six 1-D modes, both layouts) holds the same
+    ExHy E_CENTERED block as exhy_1d_unit_test.json, and the oracle's 1-D
+    ExHy run reproduces it."""
+    g = json.load(open(os.path.join(GOLDEN, "unit_test_1d_modes.json")))
+    old = json.load(open(os.path.join(GOLDEN, "exhy_1d_unit_test.json")))
+    assert sorted(g["modes"]) == ["ExHy", "ExHz", "EyHx", "EyHz", "EzHx", "EzHy"]
+    blk = g["modes"]["ExHy"]["E_CENTERED"]
+    for k, v in old["ex"].items():
+        assert blk[k] == v, k
+    s, c = exhy_1d(g["size"], g["tfsf"], g["dx"], g["wavelength"], g["courant"], g["steps"])
+    for k, (re, im) in blk.items():
+        assert abs(s[int(k)] - re) <= 1e-15 and abs(c[int(k)] - im) <= 1e-15, k
+
+
+@pytest.mark.skipif(not os.path.exists(REF_BIN), reason="reference binary not built (make -C oracle ref)")
+@pytest.mark.parametrize("name", ["ref_dim3_hc_pml_tfsf", "ref_tez_hc_pml_tfsf"])
+def test_h_centered_fixtures_match_live_reference(name):
+    """The committed H_CENTERED dumps (checked against the CUDA path in the GPU
+    tests) are what the reference binary writes for their arguments."""
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    kw = json.loads(str(z["args"]))
+    assert kw["layout"] == 1
+    mats = {k[4:]: z[k] for k in z.files if k.startswith("mat_")}
+    ref, _ = run_reference(materials=mats or None, **kw)
+    comps = [k for k in z.files if k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")]
+    assert sorted(comps) == sorted(ref)
+    for comp in comps:
+        assert np.array_equal(ref[comp], z[comp]), comp
