@@ -90,7 +90,10 @@ class Config(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("layout", ctypes.c_int),
         ("source_phase", ctypes.c_int),
-        ("reserved", ctypes.c_int * 7),
+        ("current_source", ctypes.c_int * 3),
+        ("current_source_mask", ctypes.c_int),
+        ("current_phase", ctypes.c_int),
+        ("reserved", ctypes.c_int * 2),
     ]
 
 
@@ -185,7 +188,8 @@ def make_config(*, mode=MODE_DIM3, size=(20, 20, 20), pml=None, tfsf_left=None, 
                 dx=0.0005, wavelength=0.02, courant=0.5, teta=90.0, phi=0.0, psi=90.0,
                 use_pml=False, use_tfsf=False, use_metamaterials=False,
                 point_source=(0, 0, 0), point_source_mask=0, point_source_kind=0, point_source_bandwidth=0.0,
-                precision=PREC_FP64_PLAIN, source_phase=0, layout=LAYOUT_E_CENTERED) -> Config:
+                precision=PREC_FP64_PLAIN, source_phase=0, layout=LAYOUT_E_CENTERED,
+                current_source=(0, 0, 0), current_source_mask=0, current_phase=0) -> Config:
     c = Config()
     c.mode = mode
     kept = KEPT_AXES.get(mode, (0, 1, 2))
@@ -203,6 +207,9 @@ def make_config(*, mode=MODE_DIM3, size=(20, 20, 20), pml=None, tfsf_left=None, 
     c.precision = int(precision)
     c.layout = int(layout)
     c.source_phase = int(source_phase)
+    c.current_source[:] = _triple(current_source, 0, kept)
+    c.current_source_mask = int(current_source_mask)
+    c.current_phase = int(current_phase)
     return c
 
 

@@ -180,6 +180,8 @@ int parse (std::vector<std::string> args, Opts &o)
                                      "--load-gammam-from-file"};
   static const char *ps_flags[6] = {"--point-source-ex", "--point-source-ey", "--point-source-ez",
                                     "--point-source-hx", "--point-source-hy", "--point-source-hz"};
+  static const char *cs_flags[6] = {"--current-source-jx", "--current-source-jy", "--current-source-jz",
+                                    "--current-source-mx", "--current-source-my", "--current-source-mz"};
   static const char *ignored[] = {"--use-ca-cb", "--use-ca-cb-pml", "--use-ca-cb-pml-metamaterials", "--use-cuda",
                                   "--same-size-ntff", nullptr};
   static const char *ignored_arg[] = {"--log-level", "--cuda-buffer-size", "--num-cuda-threads", "--layout-type",
@@ -275,6 +277,11 @@ int parse (std::vector<std::string> args, Opts &o)
       if (!parse_coord (v, c.point_source))
         return fail ("bad --point-source");
     }
+    else if (a == "--current-source" && next (v))
+    {
+      if (!parse_coord (v, c.current_source))
+        return fail ("bad --current-source");
+    }
     else if (a == "--save-res")
       o.save_res = true;
     else if (a == "--save-as-txt")
@@ -328,6 +335,11 @@ int parse (std::vector<std::string> args, Opts &o)
       else if (a == ps_flags[m])
       {
         c.point_source_mask |= 1 << m;
+        done = true;
+      }
+      else if (a == cs_flags[m])
+      {
+        c.current_source_mask |= 1 << m;
         done = true;
       }
     }
@@ -508,6 +520,8 @@ int main (int argc, char **argv)
   {
     fdtd_config cfg = o.cfg;
     cfg.source_phase = r;
+    // the complex build's current is cos(w (t - 1)) - i sin(w (t - 1))
+    cfg.current_phase = o.complex_values ? 1 + r : 0;
     st = fdtd_create (&cfg, o.device, &ctx[r]);
     if (st)
       return fail (std::string ("fdtd_create: ") + fdtd_status_str (st) + ": " + fdtd_last_error ());

@@ -125,7 +125,11 @@ __device__ __forceinline__ void fast_component (const FastHalf &p, int ci, int *
       }
     }
   }
-  const float curl = (v1 - v0) - (v3 - v2);
+  float curl = (v1 - v0) - (v3 - v2);
+  // J / M current source: the reference subtracts I dx Cb from the new D
+  // (or E), i.e. I dx from the curl, here in the curl's scaled units
+  if (((p.cs_mask >> ci) & 1) && x == p.cs[0] && y == p.cs[1] && z == p.cs[2])
+    curl -= (float) (*p.cs_val * p.g.dx) * p.cs_scale;
 
   float inv_m = 1.f;
   if (p.mat)

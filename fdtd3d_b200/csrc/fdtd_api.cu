@@ -32,6 +32,9 @@ using namespace fdtdb;
 namespace {
 
 constexpr double kEta0 = 376.730313461770655;  // sqrt(mu0/eps0) for the reference constants
+// per time step on the host and the device: incident-grid source, point
+// source on E and on H, J and M current
+constexpr int kSrcStride = 5;
 
 thread_local std::string g_last_error;
 
@@ -95,6 +98,8 @@ struct fdtd_ctx
   FastHalf fast_e, fast_h;
   FusedParams fused;
   bool ps_interior = true;
+  int cs_mask[2] = {0, 0};     // per family: bit ci = current source on component ci (interior cells only)
+  int cs_pos[3] = {0, 0, 0};   // its cell (0 on an axis the mode drops)
   // TMA-pipelined one-sweep kernel: plan built at the first step (and again
   // when the permittivity buffer appears); state 0 = not built, 1 = in use,
   // -1 = not applicable (the register-blocked kernel runs instead)
@@ -285,8 +290,8 @@ int ensure_src (fdtd_ctx *ctx, size_t steps)
       ctx->h_src = nullptr;
     }
     size_t cap = std::max<size_t> (steps, 1024);
-    DALLOC (ctx->d_src, cap * 3 * sizeof (double));
-    CK (cudaMallocHost ((void **) &ctx->h_src, cap * 3 * sizeof (double)));
+    DALLOC (ctx->d_src, cap * kSrcStride * sizeof (double));
+    CK (cudaMallocHost ((void **) &ctx->h_src, cap * kSrcStride * sizeof (double)));
     ctx->src_cap = cap;
   }
   else
@@ -415,6 +420,10 @@ int alloc_fast (fdtd_ctx *ctx)
     for (int k = 0; k < 6; ++k)
       p.inc_scale[k] = (float) (k >= 3 ? kEta0 : 1.0);
     p.inc_len = g.inc_len;
+    p.cs_mask = ctx->cs_mask[h];
+    for (int a = 0; a < 3; ++a)
+      p.cs[a] = ctx->cs_pos[a];
+    p.cs_scale = (float) (h ? 1.0 : kEta0);
     for (int ci = 0; ci < 3; ++ci)
     {
       int k = ci + 3 * h;
@@ -741,6 +750,24 @@ int create_impl (const fdtd_config *cfg, int device, fdtd_ctx *ctx)
     return fail (ctx, FDTD_ERR_ARG, "device index out of range");
   ctx->device = device;
   ctx->prec = cfg->precision;
+  {
+    // a current source acts on interior cells only: the reference's
+    // precomputed Cb is zero on the outer shell, and a cell outside the grid
+    // is skipped (InternalScheme.inc.h:2439-2448)
+    // (a mode's dropped axes ignore the coordinate, as initAxesCoordinate does)
+    const Geometry &g = ctx->g;
+    bool inside = true;
+    for (int a = 0; a < 3; ++a)
+    {
+      const bool dropped = (g.drop >> a) & 1;
+      const int c = dropped ? 0 : g.cfg.current_source[a];
+      ctx->cs_pos[a] = c;
+      inside = inside && (dropped || (c >= 1 && c <= g.n[a] - 2));
+    }
+    for (int k = 0; k < 6; ++k)
+      if (inside && ((g.cfg.current_source_mask >> k) & 1) && g.comp[k].exists)
+        ctx->cs_mask[k / 3] |= 1 << (k % 3);
+  }
   ctx->kind = kind_of (cfg->precision);
   ctx->eta0 = ctx->kind == 0 ? 1.0 : kEta0;
   CK (cudaSetDevice (device));
@@ -850,6 +877,9 @@ PlainHalf plain_half (fdtd_ctx *ctx, int h)
   for (int a = 0; a < 3; ++a)
     p.sigma[a] = ctx->sig64[a];
   p.inc = h ? ctx->einc[ctx->ecur] : ctx->hinc[ctx->hcur];
+  p.cs_mask = ctx->cs_mask[h];
+  for (int a = 0; a < 3; ++a)
+    p.cs[a] = ctx->cs_pos[a];
   return p;
 }
 
@@ -934,11 +964,14 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
   for (uint32_t i = 0; i < n; ++i)
   {
     uint32_t t = t_start + i;
-    ctx->h_src[3 * i + 0] = incident_source (g, t);
-    ctx->h_src[3 * i + 1] = point_source (g, t, false);
-    ctx->h_src[3 * i + 2] = point_source (g, t, true);
+    double *hs = ctx->h_src + kSrcStride * i;
+    hs[0] = incident_source (g, t);
+    hs[1] = point_source (g, t, false);
+    hs[2] = point_source (g, t, true);
+    hs[3] = current_source (g, t, false);
+    hs[4] = current_source (g, t, true);
   }
-  CK (cudaMemcpyAsync (ctx->d_src, ctx->h_src, (size_t) n * 3 * sizeof (double), cudaMemcpyHostToDevice,
+  CK (cudaMemcpyAsync (ctx->d_src, ctx->h_src, (size_t) n * kSrcStride * sizeof (double), cudaMemcpyHostToDevice,
                        ctx->stream));
   CK (cudaEventRecord (ctx->src_ev, ctx->stream));
   if ((r = dft_prepare (ctx, t_start, n)) != FDTD_OK)
@@ -946,10 +979,13 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
   size_t ps_idx = 0;
   bool ps_ok = g.cfg.point_source_mask && point_source_index (g, &ps_idx);
   cudaStream_t s = ctx->stream;
-  const bool fused = ctx->kind != 0 && ctx->has_second && !ctx->mat32[1] && ctx->ps_interior;
+  // current sources run the per-cell kernels
+  const bool fused = ctx->kind != 0 && ctx->has_second && !ctx->mat32[1] && ctx->ps_interior && !ctx->cs_mask[0]
+                     && !ctx->cs_mask[1];
   if (ctx->kind != 0 && g.cfg.use_metamaterials && !fused)
     return fail (ctx, FDTD_ERR_UNSUPPORTED,
-                 "FP32/FP16 metamaterials need the one-sweep 3-D kernel (E_CENTERED, uniform mu, interior point source)");
+                 "FP32/FP16 metamaterials need the one-sweep 3-D kernel (E_CENTERED, uniform mu, interior point "
+                 "source, no current source)");
 
   for (uint32_t i = 0; i < n; ++i)
   {
@@ -961,7 +997,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
       if (g.cfg.use_tfsf)
       {
         ctx->launches += launch_incident_e (ctx->einc[1 - ctx->ecur], ctx->einc[ctx->ecur], ctx->hinc[ctx->hcur],
-                                            g.inc_len, g.mod_e, ctx->d_src, 3 * i, s);
+                                            g.inc_len, g.mod_e, ctx->d_src, kSrcStride * i, s);
         ctx->ecur ^= 1;
         ctx->launches += launch_incident_h (ctx->hinc[1 - ctx->hcur], ctx->hinc[ctx->hcur], ctx->einc[ctx->ecur],
                                             g.inc_len, g.mod_h, s);
@@ -991,7 +1027,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
       f.inc_h = ctx->hinc[hprev];
       f.inc_e = ctx->einc[ctx->ecur];
       f.src = ctx->d_src;
-      f.src_index = 3 * i + 1;
+      f.src_index = kSrcStride * i + 1;
       if (ctx->sweep_state == 0 || (ctx->sweep_state == 1 && ctx->sweep_eps != ctx->mat32[0]))
         if ((r = plan_sweep (ctx)) != FDTD_OK)
           return r;
@@ -1026,7 +1062,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
         if (!h)
         {
           ctx->launches += launch_incident_e (ctx->einc[1 - ctx->ecur], ctx->einc[ctx->ecur],
-                                              ctx->hinc[ctx->hcur], g.inc_len, g.mod_e, ctx->d_src, 3 * i, s);
+                                              ctx->hinc[ctx->hcur], g.inc_len, g.mod_e, ctx->d_src, kSrcStride * i, s);
           ctx->ecur ^= 1;
         }
         else
@@ -1041,6 +1077,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
         if (t > 0)
         {
           PlainHalf p = plain_half (ctx, h);
+          p.cs_val = ctx->d_src + kSrcStride * i + 3 + h;
           cudaEvent_t pe;
           if ((r = prof_begin (ctx, &pe)) != FDTD_OK)
             return r;
@@ -1053,7 +1090,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
         {
           int k = ci + 3 * h;
           if (ps_ok && (g.cfg.point_source_mask & (1 << k)) && g.comp[k].exists)
-            ctx->launches += launch_point_source (ctx->f[k][0], ps_idx, ctx->d_src, 3 * i + 1 + h, s);
+            ctx->launches += launch_point_source (ctx->f[k][0], ps_idx, ctx->d_src, kSrcStride * i + 1 + h, s);
         }
         for (int ci = 0; ci < 3; ++ci)
         {
@@ -1072,6 +1109,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
           FastHalf &p = h ? ctx->fast_h : ctx->fast_e;
           p.inc = h ? ctx->einc[ctx->ecur] : ctx->hinc[ctx->hcur];
           p.mat = ctx->mat32[h];
+          p.cs_val = ctx->d_src + kSrcStride * i + 3 + h;
           cudaEvent_t pe;
           if ((r = prof_begin (ctx, &pe)) != FDTD_OK)
             return r;
@@ -1085,7 +1123,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
           int k = ci + 3 * h;
           if (ps_ok && (g.cfg.point_source_mask & (1 << k)) && g.comp[k].exists)
             ctx->launches += launch_fast_point_source (ctx->ff[k], ctx->kind == 2, ps_idx, ctx->d_src,
-                                                       3 * i + 1 + h, (float) (h ? kEta0 : 1.0), s);
+                                                       kSrcStride * i + 1 + h, (float) (h ? kEta0 : 1.0), s);
         }
       }
     }

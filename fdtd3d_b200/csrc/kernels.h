@@ -31,6 +31,10 @@ struct FastHalf
   int ilo[3][3], ihi[3][3];   // per component per axis: sigma == 0 range
   const double *inc;          // incident grid at level 1
   int inc_len;
+  int cs_mask;                // bit ci: a J / M current source on component ci of this family
+  int cs[3];                  // its cell
+  const double *cs_val;       // this half step's current I (device)
+  float cs_scale;             // I dx -> curl units (eta0 for E, 1 for H)
 };
 
 int launch_plain_half (const PlainHalf &p, int inc_len, int *err, int sm_count, cudaStream_t s);

@@ -72,6 +72,9 @@ struct PlainHalf
   const double *gamma;         // gammae / gammam
   const double *sigma[3];      // 1-D sigma profiles
   const double *inc;           // incident grid at level 1 (HInc for E, EInc for H)
+  int cs_mask;                 // bit ci: a J / M current source on component ci of this family
+  int cs[3];                   // its cell
+  const double *cs_val;        // this half step's current I (device)
 };
 
 }  // namespace fdtdb

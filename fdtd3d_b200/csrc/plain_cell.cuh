@@ -17,6 +17,7 @@
 //   ...PMLMetamaterials / calcFieldDrude  InternalScheme.inc.h:2452-2549, 775-780
 //   ...PML / calcFieldFromDOrB ..... InternalScheme.inc.h:2551-2640, 783-787
 //   getMaterial / getMetaMaterial .. InternalScheme.inc.h:2897-3213
+//   J / M current sources .......... Scheme.inc.h:1171-1260, InternalScheme.inc.h:2423-2449
 #pragma once
 
 #include "params.h"
@@ -164,7 +165,12 @@ FDTDB_HD inline void plain_component (const PlainHalf &p, int ci, int inc_len, i
     }
   }
   double tmp = v[1] - v[0] - v[3] + v[2] - 0.0 * dx;
-  grid[0][id] = val * ca + tmp * cb;
+  double nv = val * ca + tmp * cb;
+  // J / M current source: -= (I dx) Cb on the freshly updated value, before
+  // D -> E (Scheme.inc.h:1171-1260, InternalScheme.inc.h:792-795, 2423-2449)
+  if (((p.cs_mask >> ci) & 1) && x == p.cs[0] && y == p.cs[1] && z == p.cs[2])
+    nv -= *p.cs_val * dx * cb;
+  grid[0][id] = nv;
 
   if (!p.use_pml)
     return;

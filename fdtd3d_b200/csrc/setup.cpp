@@ -366,6 +366,10 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
     return "Gaussian point source needs a positive bandwidth";
   if (cfg.source_phase != 0 && cfg.source_phase != 1)
     return "source_phase must be 0 (sine) or 1 (cosine)";
+  if (cfg.current_phase < 0 || cfg.current_phase > 2)
+    return "current_phase must be 0 (sin), 1 (complex real part) or 2 (complex imaginary part)";
+  if (cfg.current_source_mask & ~0x3f)
+    return "current_source_mask has bits beyond the six components";
   g.tmz = cfg.mode == FDTD_MODE_TMZ;
   g.drop = (int) ms->drop;
   auto active = [&] (int a) { return !((g.drop >> a) & 1); };
@@ -640,6 +644,22 @@ double point_source (const Geometry &g, uint32_t t, bool h)
   }
   const double arg = g.dt * ts * 2 * kPi * g.freq;
   return g.cfg.source_phase ? std::cos (arg) : std::sin (arg);
+}
+
+// Scheme.inc.h:1228-1236: the component's time (t on E, t + 1/2 on H), the
+// real build's sin or the complex build's cos(w (t - 1)) - i sin(w (t - 1)),
+// times mu0 / dt / 2 (mu0 for J as for M, as the reference has it).
+double current_source (const Geometry &g, uint32_t t, bool h)
+{
+  const double ts = h ? t + 0.5 : (double) t;
+  double s;
+  if (g.cfg.current_phase == 0)
+    s = std::sin (g.dt * ts * 2.0 * kPi * g.freq);
+  else if (g.cfg.current_phase == 1)
+    s = std::cos (g.dt * (ts - 1) * 2.0 * kPi * g.freq);
+  else
+    s = -std::sin (g.dt * (ts - 1) * 2.0 * kPi * g.freq);
+  return s * kMu0 / g.dt / 2.0;
 }
 
 }  // namespace fdtdb

@@ -78,13 +78,16 @@ struct Geometry
 std::string build_geometry (const fdtd_config &cfg, Geometry &g);
 
 // Sigma profile of axis b averaged at the position of component k, as the
-// reference's getMaterial averages the sigma grids (two points along the
-// component's own axis for E, along the other two axes for H).
+// reference's getMaterial averages the sigma grids (two points along an
+// edge component's own axis, along the other two axes for the others).
 std::vector<double> sigma_at (const Geometry &g, int k, int b);
 
 // sin(2 pi f dt t) hard source of the incident grid at time step t.
 double incident_source (const Geometry &g, uint32_t t);
 // point-source value for an E (h = false) or H (h = true) component.
 double point_source (const Geometry &g, uint32_t t, bool h);
+// current I of the J (h = false) or M (h = true) current sources at time
+// step t; the cell takes -= I dx Cb after its curl update.
+double current_source (const Geometry &g, uint32_t t, bool h);
 
 }  // namespace fdtdb

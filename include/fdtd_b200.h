@@ -121,7 +121,15 @@ typedef struct
                                build drives sin + i cos (InternalScheme.inc.h:2888-2890, 3312-3313);
                                with real materials its fields are the run with phase 0 plus i times
                                the run with phase 1 */
-  int reserved[7];
+  int current_source[3];    /* --current-source: the cell of the J / M current sources */
+  int current_source_mask;  /* bit c: current on component c (Jx Jy Jz = 0-2, Mx My Mz = 3-5;
+                               --current-source-jx .. -mz).  After the curl update of that
+                               component, before D -> E, the cell takes -= I dx Cb with
+                               I = s(t) mu0 / dt / 2, t the component's time (t on E, t + 1/2
+                               on H) (Scheme.inc.h:1171-1260, InternalScheme.inc.h:2423-2449) */
+  int current_phase;        /* s(t): 0 = sin(w t), the real build; 1 / 2 = the real / imaginary
+                               part of the complex build's cos(w (t - 1)) - i sin(w (t - 1)) */
+  int reserved[2];
 } fdtd_config;
 
 /* Point-source kinds.  Kind 0 is the reference's hard source

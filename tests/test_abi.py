@@ -44,6 +44,8 @@ def test_status_strings(fdtd):
     dict(use_metamaterials=True),
     dict(dx=-1.0),
     dict(layout=2),
+    dict(current_phase=3),
+    dict(current_source_mask=1 << 6),
 ])
 def test_create_rejects_bad_config(fdtd, bad):
     lib = fdtd.load_library()
