@@ -93,7 +93,8 @@ class Config(ctypes.Structure):
         ("current_source", ctypes.c_int * 3),
         ("current_source_mask", ctypes.c_int),
         ("current_phase", ctypes.c_int),
-        ("reserved", ctypes.c_int * 2),
+        ("double_material_precision", ctypes.c_int),
+        ("reserved", ctypes.c_int * 1),
     ]
 
 
@@ -189,7 +190,8 @@ def make_config(*, mode=MODE_DIM3, size=(20, 20, 20), pml=None, tfsf_left=None, 
                 use_pml=False, use_tfsf=False, use_metamaterials=False,
                 point_source=(0, 0, 0), point_source_mask=0, point_source_kind=0, point_source_bandwidth=0.0,
                 precision=PREC_FP64_PLAIN, source_phase=0, layout=LAYOUT_E_CENTERED,
-                current_source=(0, 0, 0), current_source_mask=0, current_phase=0) -> Config:
+                current_source=(0, 0, 0), current_source_mask=0, current_phase=0,
+                double_material_precision=False) -> Config:
     c = Config()
     c.mode = mode
     kept = KEPT_AXES.get(mode, (0, 1, 2))
@@ -210,6 +212,7 @@ def make_config(*, mode=MODE_DIM3, size=(20, 20, 20), pml=None, tfsf_left=None, 
     c.current_source[:] = _triple(current_source, 0, kept)
     c.current_source_mask = int(current_source_mask)
     c.current_phase = int(current_phase)
+    c.double_material_precision = int(bool(double_material_precision))
     return c
 
 
@@ -229,6 +232,9 @@ class Simulation:
         size = tuple(self.cfg.size)
         self.shape = tuple(size[a] for a in KEPT_AXES.get(self.mode, (0, 1, 2)))
         self.cells = int(np.prod(self.shape))
+        # eps and mu on the doubled grid with double_material_precision
+        self.material_shape = (tuple(2 * s for s in self.shape) if self.cfg.double_material_precision
+                               else self.shape)
         h = ctypes.c_void_p()
         self._check(self.lib.fdtd_create(ctypes.byref(self.cfg), device, ctypes.byref(h)), "fdtd_create")
         self._h = h
@@ -243,7 +249,8 @@ class Simulation:
 
     def set_material(self, name: str, arr) -> None:
         a = np.ascontiguousarray(arr, dtype=np.float64).reshape(-1)
-        if a.size != self.cells:
+        want = int(np.prod(self.material_shape)) if name in ("eps", "mu") else self.cells
+        if a.size != want:
             raise ValueError("material array size does not match the grid")
         self._check(self.lib.fdtd_upload_material(self._h, MATERIALS.index(name), a.ctypes.data), "upload_material")
 

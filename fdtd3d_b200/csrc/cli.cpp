@@ -272,6 +272,8 @@ int parse (std::vector<std::string> args, Opts &o)
       c.use_tfsf = 1;
     else if (a == "--use-metamaterials")
       c.use_metamaterials = 1;
+    else if (a == "--use-double-material-precision")
+      c.double_material_precision = 1;
     else if (a == "--point-source" && next (v))
     {
       if (!parse_coord (v, c.point_source))
@@ -537,13 +539,19 @@ int main (int argc, char **argv)
       ++kept;
   }
   size_t cells = (size_t) n[0] * n[1] * n[2];
+  // --use-double-material-precision: eps and mu files hold the grid of twice
+  // the resolution on every kept axis
+  size_t fine = cells;
+  if (o.cfg.double_material_precision)
+    for (int a = 0; a < kept; ++a)
+      fine *= 2;
   for (int m = 0; m < 6; ++m)
   {
     if (o.mat_file[m].empty ())
       continue;
     std::vector<double> a;
     std::string why;
-    if (!load_material (o.mat_file[m], cells, kept, o.complex_values, a, why))
+    if (!load_material (o.mat_file[m], m < 2 ? fine : cells, kept, o.complex_values, a, why))
       return fail (why);
     for (int r = 0; r < nrun; ++r)
     {

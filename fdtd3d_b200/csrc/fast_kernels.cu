@@ -132,15 +132,18 @@ __device__ __forceinline__ void fast_component (const FastHalf &p, int ci, int *
     curl -= (float) (*p.cs_val * p.g.dx) * p.cs_scale;
 
   float inv_m = 1.f;
-  if (p.mat)
+  const float *mp = p.matc[ci] ? p.matc[ci] : p.mat;
+  if (mp)
   {
     float m;
-    if (c.nmat == 2)
-      m = 0.5f * (p.mat[flin (g, x, y, z)] + p.mat[flin (g, x + c.m[1][0], y + c.m[1][1], z + c.m[1][2])]);
+    if (c.nmat == 1)
+      m = mp[id];
+    else if (c.nmat == 2)
+      m = 0.5f * (mp[flin (g, x, y, z)] + mp[flin (g, x + c.m[1][0], y + c.m[1][1], z + c.m[1][2])]);
     else
-      m = 0.25f * (p.mat[flin (g, x, y, z)] + p.mat[flin (g, x + c.m[1][0], y + c.m[1][1], z + c.m[1][2])]
-                   + p.mat[flin (g, x + c.m[2][0], y + c.m[2][1], z + c.m[2][2])]
-                   + p.mat[flin (g, x + c.m[3][0], y + c.m[3][1], z + c.m[3][2])]);
+      m = 0.25f * (mp[flin (g, x, y, z)] + mp[flin (g, x + c.m[1][0], y + c.m[1][1], z + c.m[1][2])]
+                   + mp[flin (g, x + c.m[2][0], y + c.m[2][1], z + c.m[2][2])]
+                   + mp[flin (g, x + c.m[3][0], y + c.m[3][1], z + c.m[3][2])]);
     inv_m = 1.f / m;
   }
 

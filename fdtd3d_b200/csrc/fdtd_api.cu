@@ -79,6 +79,13 @@ struct fdtd_ctx
   double *d1[6][3] = {};
   double *mat64[6] = {};
   double *sig64[3] = {};
+  // double material precision: eps / mu per component averaged from the fine
+  // grid at upload (null until then), sigma per component and axis, and the
+  // fine upload buffer
+  double *matc64[6] = {};
+  float *matc32[6] = {};
+  double *sigc64[6][3] = {};
+  double *fine_tmp = nullptr;
 
   // fused forms: two buffer sets; set fcur holds the current time level.
   // The per-cell path updates set fcur in place; the one-sweep 3-D kernel
@@ -230,10 +237,12 @@ CompDev make_comp_dev (const Geometry &g, int k)
   c.sig_cacb = l.sig_cacb;
   c.sig4 = l.sig4;
   c.sig5 = l.sig5;
-  c.nmat = l.nmat;
+  // double material precision: the material and sigma arrive pre-averaged
+  // per component, a one-point stencil
+  c.nmat = g.dmp ? 1 : l.nmat;
   for (int j = 0; j < 4; ++j)
     for (int a = 0; a < 3; ++a)
-      c.m[j][a] = l.m[j][a];
+      c.m[j][a] = g.dmp ? 0 : l.m[j][a];
   c.nterms = 0;
   for (const TfsfTerm &t : g.tfsf)
   {
@@ -331,6 +340,63 @@ int alloc_plain (fdtd_ctx *ctx)
     CK (cudaMemcpyAsync (ctx->sig64[a], g.sigma[a].data (), g.sigma[a].size () * sizeof (double),
                          cudaMemcpyHostToDevice, ctx->stream));
   }
+  if (g.dmp)
+  {
+    for (int k = 0; k < 6; ++k)
+    {
+      if (!g.comp[k].exists)
+        continue;
+      for (int a = 0; a < 3; ++a)
+      {
+        std::vector<double> s = sigma_at (g, k, a);
+        DALLOC (ctx->sigc64[k][a], s.size () * sizeof (double));
+        CK (cudaMemcpyAsync (ctx->sigc64[k][a], s.data (), s.size () * sizeof (double), cudaMemcpyHostToDevice,
+                             ctx->stream));
+        CK (cudaStreamSynchronize (ctx->stream));
+      }
+    }
+  }
+  CK (cudaStreamSynchronize (ctx->stream));
+  return FDTD_OK;
+}
+
+// Double material precision: eps (which 0) or mu (which 1) on the fine grid,
+// from host or device memory, averaged into every component of its family.
+int upload_fine_material (fdtd_ctx *ctx, int which, const double *src, cudaMemcpyKind kind)
+{
+  const Geometry &g = ctx->g;
+  if (!ctx->fine_tmp)
+    DALLOC (ctx->fine_tmp, (size_t) g.fine_cells * sizeof (double));
+  CK (cudaMemcpyAsync (ctx->fine_tmp, src, (size_t) g.fine_cells * sizeof (double), kind, ctx->stream));
+  FineAvg a;
+  std::memset (&a, 0, sizeof (a));
+  for (int b = 0; b < 3; ++b)
+  {
+    a.n[b] = g.n[b];
+    a.nf[b] = g.nf[b];
+    a.mul[b] = ((g.drop >> b) & 1) ? 0 : 2;
+  }
+  const size_t n = (size_t) g.cells;
+  for (int ci = 0; ci < 3; ++ci)
+  {
+    const int k = ci + 3 * which;
+    if (!g.comp[k].exists)
+      continue;
+    std::memcpy (a.off, g.fine_off[k], sizeof (a.off));
+    if (ctx->kind == 0)
+    {
+      if (!ctx->matc64[k])
+        DALLOC (ctx->matc64[k], n * sizeof (double));
+      ctx->launches += launch_fine_average (ctx->fine_tmp, ctx->matc64[k], nullptr, a, ctx->sm_count, ctx->stream);
+    }
+    else
+    {
+      if (!ctx->matc32[k])
+        DALLOC (ctx->matc32[k], n * sizeof (float));
+      ctx->launches += launch_fine_average (ctx->fine_tmp, nullptr, ctx->matc32[k], a, ctx->sm_count, ctx->stream);
+    }
+  }
+  CK (cudaGetLastError ());
   CK (cudaStreamSynchronize (ctx->stream));
   return FDTD_OK;
 }
@@ -342,9 +408,9 @@ int alloc_fast (fdtd_ctx *ctx)
   if (g.cfg.use_metamaterials && g.drop != 0)
     return fail (ctx, FDTD_ERR_UNSUPPORTED, "2-D and 1-D metamaterials are provided by the FP64 plain form only");
   // the one-sweep 3-D kernels (register-blocked and TMA) are written for the
-  // E_CENTERED stencil; H_CENTERED and the 2-D / 1-D modes run the per-cell
-  // kernels on one buffer set
-  ctx->has_second = g.drop == 0 && g.cfg.layout == 0;
+  // E_CENTERED stencil on cell-centred materials; H_CENTERED, double material
+  // precision and the 2-D / 1-D modes run the per-cell kernels on one buffer set
+  ctx->has_second = g.drop == 0 && g.cfg.layout == 0 && !g.dmp;
   for (int b = 0; b < (ctx->has_second ? 2 : 1); ++b)
   {
     for (int k = 0; k < 6; ++k)
@@ -880,6 +946,12 @@ PlainHalf plain_half (fdtd_ctx *ctx, int h)
   p.cs_mask = ctx->cs_mask[h];
   for (int a = 0; a < 3; ++a)
     p.cs[a] = ctx->cs_pos[a];
+  for (int ci = 0; ci < 3; ++ci)
+  {
+    p.matc[ci] = ctx->matc64[ci + 3 * h];
+    for (int a = 0; a < 3; ++a)
+      p.sigc[ci][a] = ctx->sigc64[ci + 3 * h][a];
+  }
   return p;
 }
 
@@ -1109,6 +1181,8 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
           FastHalf &p = h ? ctx->fast_h : ctx->fast_e;
           p.inc = h ? ctx->einc[ctx->ecur] : ctx->hinc[ctx->hcur];
           p.mat = ctx->mat32[h];
+          for (int ci = 0; ci < 3; ++ci)
+            p.matc[ci] = ctx->matc32[ci + 3 * h];
           p.cs_val = ctx->d_src + kSrcStride * i + 3 + h;
           cudaEvent_t pe;
           if ((r = prof_begin (ctx, &pe)) != FDTD_OK)
@@ -1174,6 +1248,8 @@ int fdtd_upload_material (fdtd_ctx *ctx, int which, const double *host)
   if (r != FDTD_OK)
     return r;
   size_t n = (size_t) ctx->g.cells;
+  if (ctx->g.dmp && which < 2)
+    return upload_fine_material (ctx, which, host, cudaMemcpyHostToDevice);
   if (ctx->kind == 0)
   {
     if (!ctx->mat64[which])
@@ -1200,6 +1276,8 @@ int fdtd_upload_material_device (fdtd_ctx *ctx, int which, const double *dev)
   if (r != FDTD_OK)
     return r;
   size_t n = (size_t) ctx->g.cells;
+  if (ctx->g.dmp && which < 2)
+    return upload_fine_material (ctx, which, dev, cudaMemcpyDeviceToDevice);
   if (ctx->kind == 0)
   {
     if (!ctx->mat64[which])
@@ -1369,15 +1447,16 @@ int fdtd_reduce (fdtd_ctx *ctx, int what, double *out)
     bool isH = k >= 3;
     if (what == FDTD_REDUCE_ENERGY)
     {
+      // (double material precision: the component's own averaged material)
       if (ctx->kind == 0)
       {
-        w = ctx->mat64[isH ? 1 : 0];
+        w = ctx->matc64[k] ? ctx->matc64[k] : ctx->mat64[isH ? 1 : 0];
         wkind = 2;
         scale = isH ? kEta0 * kEta0 : 1.0;
       }
       else
       {
-        w = ctx->mat32[isH ? 1 : 0];
+        w = ctx->matc32[k] ? ctx->matc32[k] : ctx->mat32[isH ? 1 : 0];
         wkind = w ? 1 : 0;
       }
     }
@@ -1429,7 +1508,7 @@ int adjoint_entry (fdtd_ctx *ctx, const fdtd_adjoint_cfg *cfg, double *objective
   if (cfg->precision != FDTD_PREC_FP32 && cfg->precision != FDTD_PREC_FP64_PLAIN)
     return fail (ctx, FDTD_ERR_ARG, "adjoint precision must be FP32 or FP64");
   const Geometry &g = ctx->g;
-  if (!g.tmz || g.cfg.use_tfsf || g.cfg.use_metamaterials || g.cfg.layout != 0)
+  if (!g.tmz || g.cfg.use_tfsf || g.cfg.use_metamaterials || g.cfg.layout != 0 || g.dmp)
     return fail (ctx, FDTD_ERR_UNSUPPORTED, "the adjoint covers 2-D TMz point-source runs (E_CENTERED)");
   int r = set_device (ctx);
   if (r != FDTD_OK)

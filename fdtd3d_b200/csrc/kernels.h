@@ -35,6 +35,7 @@ struct FastHalf
   int cs[3];                  // its cell
   const double *cs_val;       // this half step's current I (device)
   float cs_scale;             // I dx -> curl units (eta0 for E, 1 for H)
+  const float *matc[3];       // double material precision: per-component averaged material (null: mat)
 };
 
 int launch_plain_half (const PlainHalf &p, int inc_len, int *err, int sm_count, cudaStream_t s);
@@ -43,6 +44,16 @@ int launch_incident_e (double *e_new, const double *e_old, const double *h_old, 
 int launch_incident_h (double *h_new, const double *h_old, const double *e_new, int len, double modifier,
                        cudaStream_t s);
 int launch_point_source (double *f, size_t index, const double *src, int src_index, cudaStream_t s);
+
+// Double material precision: per coarse cell, the average of the fine cells
+// (mul * p + off[j]) of a grid nf (mul = 2 on a kept axis, 0 on a dropped one).
+struct FineAvg
+{
+  int n[3], nf[3], mul[3];
+  int off[8][3];
+};
+int launch_fine_average (const double *fine, double *out64, float *out32, const FineAvg &a, int sm_count,
+                         cudaStream_t s);
 
 int launch_fast_half (const FastHalf &p, int *err, int sm_count, cudaStream_t s);
 int launch_fast_point_source (void *f, int fp16, size_t index, const double *src, int src_index, float scale,

@@ -75,6 +75,11 @@ struct PlainHalf
   int cs_mask;                 // bit ci: a J / M current source on component ci of this family
   int cs[3];                   // its cell
   const double *cs_val;        // this half step's current I (device)
+  // double material precision: per component, the material averaged over its
+  // eight fine cells and the sigma profiles averaged at its position (the
+  // component's stencil is then one point); null: mat and sigma
+  const double *matc[3];
+  const double *sigc[3][3];
 };
 
 }  // namespace fdtdb

@@ -33,6 +33,8 @@ FDTDB_HD inline size_t lin (const GeomDev &g, int x, int y, int z)
 
 FDTDB_HD inline double avg_points (const CompDev &c, const double *v)
 {
+  if (c.nmat == 1)
+    return v[0];
   if (c.nmat == 2)
     return (v[0] + v[1]) / 2.0;
   return ((v[0] + v[1]) / 2.0 + (v[2] + v[3]) / 2.0) / 2.0;
@@ -120,18 +122,20 @@ FDTDB_HD inline void plain_component (const PlainHalf &p, int ci, int inc_len, i
   const double dx = g.dx;
 
   double *const *grid = p.use_pml ? p.dd[ci] : p.f[ci];
+  const double *mat = p.matc[ci] ? p.matc[ci] : p.mat;
+  const double *const *sig = p.sigc[ci][0] ? p.sigc[ci] : p.sigma;
   double val = grid[1][id];
   double ca, cb;
   if (p.use_pml)
   {
-    double material = sigma_avg (c, p.sigma[c.sig_cacb], c.sig_cacb, x, y, z);
+    double material = sigma_avg (c, sig[c.sig_cacb], c.sig_cacb, x, y, z);
     double dd = (2 * eps0 * 1.0 + material * dt);
     ca = (2 * eps0 * 1.0 - material * dt) / dd;
     cb = (2 * eps0 * dt / dx) / dd;
   }
   else
   {
-    double material = material_avg (g, c, p.mat, x, y, z);
+    double material = material_avg (g, c, mat, x, y, z);
     ca = 1.0;
     cb = dt / (material * p.mat_modifier * dx);
   }
@@ -180,7 +184,7 @@ FDTDB_HD inline void plain_component (const PlainHalf &p, int ci, int inc_len, i
   {
     double cur = p.dd[ci][0][id], prev = p.dd[ci][1][id], pprev = p.dd[ci][2][id];
     double prev1 = p.d1[ci][1][id], pprev1 = p.d1[ci][2][id];
-    double material = material_avg (g, c, p.mat, x, y, z);
+    double material = material_avg (g, c, mat, x, y, z);
     double omega = drude_avg (g, c, p.omega, x, y, z);
     double gamma = drude_avg (g, c, p.gamma, x, y, z);
     double sq = dt * omega;
@@ -197,9 +201,9 @@ FDTDB_HD inline void plain_component (const PlainHalf &p, int ci, int inc_len, i
   double *const *src = p.use_meta ? p.d1[ci] : p.dd[ci];
   double cur_db = src[0][id];
   double prev_db = src[1][id];
-  double material1 = material_avg (g, c, p.mat, x, y, z);
-  double material4 = sigma_avg (c, p.sigma[c.sig4], c.sig4, x, y, z);
-  double material5 = sigma_avg (c, p.sigma[c.sig5], c.sig5, x, y, z);
+  double material1 = material_avg (g, c, mat, x, y, z);
+  double material4 = sigma_avg (c, sig[c.sig4], c.sig4, x, y, z);
+  double material5 = sigma_avg (c, sig[c.sig5], c.sig5, x, y, z);
   double modifier = material1 * mm;
   if (p.use_meta)
     modifier = 1;

@@ -10,6 +10,9 @@
 // * incident_e_kernel / incident_h_kernel: the 1-D auxiliary TF/SF grid
 //   (InternalScheme.inc.h:3276-3357), FP64 for every form.
 // * point_source_kernel: hard sinusoidal source (InternalScheme.inc.h:2818-2895).
+// * fine_average_kernel: double material precision - one component's
+//   material, averaged over the eight fine cells around it
+//   (YeeGridLayout.h:866-1030, Approximation.cpp:34-54), once per upload.
 #include <cuda_runtime.h>
 
 #include "kernels.h"
@@ -100,6 +103,47 @@ int launch_incident_h (double *h_new, const double *h_old, const double *e_new, 
 int launch_point_source (double *f, size_t index, const double *src, int src_index, cudaStream_t s)
 {
   point_source_kernel<<<1, 32, 0, s>>> (f, index, src, src_index);
+  return 1;
+}
+
+__global__ void fine_average_kernel (const double *fine, double *out64, float *out32, FineAvg a)
+{
+  const int64_t total = (int64_t) a.n[0] * a.n[1] * a.n[2];
+  for (int64_t id = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; id < total;
+       id += (int64_t) gridDim.x * blockDim.x)
+  {
+    const int z = (int) (id % a.n[2]);
+    const int64_t r = id / a.n[2];
+    const int y = (int) (r % a.n[1]);
+    const int x = (int) (r / a.n[1]);
+    const int p[3] = {x, y, z};
+    double v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+    {
+      // the outer shell's last cell would reach one fine cell past the grid;
+      // its material is never used, so clamp
+      int q[3];
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+        q[b] = min (a.mul[b] * p[b] + a.off[j][b], a.nf[b] - 1);
+      v[j] = fine[((int64_t) q[0] * a.nf[1] + q[1]) * a.nf[2] + q[2]];
+    }
+    // ((v1 + v2) / 2 + (v3 + v4) / 2) / 2, twice, then / 2
+    const double lo = ((v[0] + v[1]) / 2.0 + (v[2] + v[3]) / 2.0) / 2.0;
+    const double hi = ((v[4] + v[5]) / 2.0 + (v[6] + v[7]) / 2.0) / 2.0;
+    const double m = (lo + hi) / 2.0;
+    if (out64)
+      out64[id] = m;
+    if (out32)
+      out32[id] = (float) m;
+  }
+}
+
+int launch_fine_average (const double *fine, double *out64, float *out32, const FineAvg &a, int sm_count,
+                         cudaStream_t s)
+{
+  fine_average_kernel<<<sm_count * 4, 256, 0, s>>> (fine, out64, out32, a);
   return 1;
 }
 

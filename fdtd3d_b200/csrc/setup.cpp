@@ -330,6 +330,21 @@ void init_components (Geometry &g, unsigned comps, bool h_centered, Pred preds[6
   }
 }
 
+// The eight fine cells a component averages with double material precision,
+// as offsets from (2i, 2j, 2k), in the order of the reference's absPos11,
+// 12, 21, 22, 31, 32, 41, 42 (YeeGridLayout.h:866-1030): "edge" components
+// (E in E_CENTERED, H in H_CENTERED) along x, y, z, then the others.
+const int kFineEdge[3][8][3] = {
+    {{1, 0, 0}, {1, 1, 0}, {2, 0, 0}, {2, 1, 0}, {1, 0, 1}, {1, 1, 1}, {2, 0, 1}, {2, 1, 1}},
+    {{0, 1, 0}, {1, 1, 0}, {0, 2, 0}, {1, 2, 0}, {0, 1, 1}, {1, 1, 1}, {0, 2, 1}, {1, 2, 1}},
+    {{0, 0, 1}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}, {0, 0, 2}, {0, 1, 2}, {1, 0, 2}, {1, 1, 2}},
+};
+const int kFineFace[3][8][3] = {
+    {{0, 1, 1}, {1, 1, 1}, {0, 1, 2}, {1, 1, 2}, {0, 2, 1}, {1, 2, 1}, {0, 2, 2}, {1, 2, 2}},
+    {{1, 0, 1}, {1, 1, 1}, {1, 0, 2}, {1, 1, 2}, {2, 0, 1}, {2, 1, 1}, {2, 0, 2}, {2, 1, 2}},
+    {{1, 1, 0}, {1, 1, 1}, {1, 2, 0}, {1, 2, 1}, {2, 1, 0}, {2, 1, 1}, {2, 2, 0}, {2, 2, 1}},
+};
+
 bool axis_ok (const AxisTest &t, double coord, double left, double right)
 {
   switch (t.kind)
@@ -370,6 +385,9 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
     return "current_phase must be 0 (sin), 1 (complex real part) or 2 (complex imaginary part)";
   if (cfg.current_source_mask & ~0x3f)
     return "current_source_mask has bits beyond the six components";
+  if (cfg.double_material_precision && cfg.use_metamaterials)
+    return "double material precision with metamaterials is not provided (the reference's eight-point Drude "
+           "average is unreachable, Approximation.cpp:167-197)";
   g.tmz = cfg.mode == FDTD_MODE_TMZ;
   g.drop = (int) ms->drop;
   auto active = [&] (int a) { return !((g.drop >> a) & 1); };
@@ -390,6 +408,10 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
   if (!(cfg.dx > 0) || !(cfg.wavelength > 0) || !(cfg.courant > 0))
     return "dx, wavelength and courant factor must be positive";
   g.cells = (int64_t) g.n[0] * g.n[1] * g.n[2];
+  g.dmp = cfg.double_material_precision != 0;
+  for (int a = 0; a < 3; ++a)
+    g.nf[a] = (g.dmp && active (a)) ? 2 * g.n[a] : g.n[a];
+  g.fine_cells = (int64_t) g.nf[0] * g.nf[1] * g.nf[2];
   g.levels = (cfg.use_metamaterials && cfg.use_pml) ? 3 : 2;
   g.dx = cfg.dx;
 
@@ -506,17 +528,28 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
   }
   g.inc_len = 500 * g.n[0];
 
+  // with double material precision the sigma grids are the fine ones:
+  // 2 n cells, a PML of 2 p cells, the same dx (SchemeHelper.h:596-718)
+  const int fmul = g.dmp ? 2 : 1;
   for (int a = 0; a < 3; ++a)
   {
-    g.sigma[a].assign (g.n[a], 0.0);
+    g.sigma[a].assign (g.nf[a], 0.0);
     if (cfg.use_pml && active (a))
-      sigma_profile (g.sigma[a], a == (active (0) ? 0 : (active (1) ? 1 : 2)), g.n[a], cfg.pml[a], cfg.dx);
+      sigma_profile (g.sigma[a], a == (active (0) ? 0 : (active (1) ? 1 : 2)), g.nf[a], fmul * cfg.pml[a], cfg.dx);
   }
 
   Pred preds[6][6];
   int slot_dir[6][4];
   const bool h_centered = cfg.layout == 1;
   init_components (g, ms->comps, h_centered, preds, slot_dir);
+  for (int k = 0; k < 6; ++k)
+  {
+    const bool edge = (k >= 3) == h_centered;
+    const int(*tab)[3] = edge ? kFineEdge[k % 3] : kFineFace[k % 3];
+    for (int j = 0; j < 8; ++j)
+      for (int a = 0; a < 3; ++a)
+        g.fine_off[k][j][a] = active (a) ? tab[j][a] : 0;
+  }
 
   if (cfg.use_tfsf)
   {
@@ -615,6 +648,22 @@ std::vector<double> sigma_at (const Geometry &g, int k, int b)
   int n = g.n[b];
   std::vector<double> out (n, 0.0);
   int a = k % 3;
+  if (g.dmp)
+  {
+    // the eight fine cells span two fine cells on every kept axis, starting
+    // at 2i + 1 where the component sits at i + 1.0 and at 2i where it sits
+    // at i + 0.5; a sigma grid varies along one axis, so the reference's
+    // eight-point average reduces to this pair exactly
+    if ((g.drop >> b) & 1)
+      return std::vector<double> (n, s[0]);
+    const int shift = g.comp[k].min_fp[b] == 1.0 ? 1 : 0;
+    for (int i = 0; i < n; ++i)
+    {
+      const int lo = 2 * i + shift;
+      out[i] = lo + 1 < (int) s.size () ? (s[lo] + s[lo + 1]) / 2.0 : s[lo];
+    }
+    return out;
+  }
   // sigma grids vary along one axis: the two-cell material average of an
   // edge component spans its own axis, the four-cell one the other two
   bool averaged = g.comp[k].nmat == 2 ? (b == a) : (b != a);

@@ -70,7 +70,15 @@ struct Geometry
   int inc_len;
   double mod_e, mod_h;        // incident-grid update modifiers
   CompLayout comp[6];
-  std::vector<double> sigma[3];   // 1-D sigma profiles (zero when PML off)
+  // --use-double-material-precision: eps, mu and sigma on a grid of twice
+  // the resolution (nf = 2 n on a kept axis, 1 on a dropped one); component
+  // k averages the fine cells (2i, 2j, 2k) + fine_off[k][0..7] in the
+  // reference's order (YeeGridLayout.h:866-1030)
+  bool dmp = false;
+  int nf[3] = {1, 1, 1};
+  int64_t fine_cells = 0;
+  int fine_off[6][8][3] = {};
+  std::vector<double> sigma[3];   // 1-D sigma profiles (zero when PML off; on the fine grid with dmp)
   std::vector<TfsfTerm> tfsf;     // every TF/SF correction term
 };
 

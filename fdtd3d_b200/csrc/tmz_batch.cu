@@ -496,8 +496,9 @@ int create_batch (fdtd_batch *b, const fdtd_config *base, int count, const int *
     return bfail (b, FDTD_ERR_UNSUPPORTED, "batches are 2-D TMz, FP32");
   if (base->use_tfsf || base->use_metamaterials)
     return bfail (b, FDTD_ERR_UNSUPPORTED, "batches provide PML and a centred point source (no TF/SF, no Drude)");
-  if (base->layout != 0)
-    return bfail (b, FDTD_ERR_UNSUPPORTED, "batches use the E_CENTERED layout");
+  if (base->layout != 0 || base->double_material_precision || base->current_source_mask)
+    return bfail (b, FDTD_ERR_UNSUPPORTED,
+                  "batches use the E_CENTERED layout, cell-centred materials and no current source");
   if (count < 1 || !sizes)
     return bfail (b, FDTD_ERR_ARG, "empty batch");
   int ndev = 0;

@@ -129,7 +129,14 @@ typedef struct
                                on H) (Scheme.inc.h:1171-1260, InternalScheme.inc.h:2423-2449) */
   int current_phase;        /* s(t): 0 = sin(w t), the real build; 1 / 2 = the real / imaginary
                                part of the complex build's cos(w (t - 1)) - i sin(w (t - 1)) */
-  int reserved[2];
+  int double_material_precision; /* --use-double-material-precision: eps, mu and the PML sigma
+                               live on a grid of twice the resolution on every kept axis (2 n, PML
+                               2 p cells); a component averages the 2 x 2 x 2 fine cells around it
+                               (YeeGridLayout.h:866-1030, Approximation.cpp:48-54,
+                               SchemeHelper.h:596-718).  fdtd_upload_material then takes eps and mu
+                               on that grid.  Not with metamaterials (the reference's eight-point
+                               Drude average is unreachable, Approximation.cpp:167-197) */
+  int reserved[1];
 } fdtd_config;
 
 /* Point-source kinds.  Kind 0 is the reference's hard source

@@ -46,6 +46,7 @@ def test_status_strings(fdtd):
     dict(layout=2),
     dict(current_phase=3),
     dict(current_source_mask=1 << 6),
+    dict(double_material_precision=True, use_metamaterials=True, use_pml=True, pml=2),
 ])
 def test_create_rejects_bad_config(fdtd, bad):
     lib = fdtd.load_library()
