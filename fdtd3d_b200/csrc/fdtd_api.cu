@@ -948,9 +948,11 @@ PlainHalf plain_half (fdtd_ctx *ctx, int h)
     p.cs[a] = ctx->cs_pos[a];
   for (int ci = 0; ci < 3; ++ci)
   {
-    p.matc[ci] = ctx->matc64[ci + 3 * h];
+    const int k = ci + 3 * h;
+    p.dmp = g.dmp ? 1 : 0;
+    p.matc[ci] = ctx->matc64[k] ? ctx->matc64[k] : p.mat;
     for (int a = 0; a < 3; ++a)
-      p.sigc[ci][a] = ctx->sigc64[ci + 3 * h][a];
+      p.sigc[ci][a] = ctx->sigc64[k][a] ? ctx->sigc64[k][a] : p.sigma[a];
   }
   return p;
 }

@@ -75,11 +75,13 @@ struct PlainHalf
   int cs_mask;                 // bit ci: a J / M current source on component ci of this family
   int cs[3];                   // its cell
   const double *cs_val;        // this half step's current I (device)
-  // double material precision: per component, the material averaged over its
-  // eight fine cells and the sigma profiles averaged at its position (the
-  // component's stencil is then one point); null: mat and sigma
+  // per component: its material grid and its three sigma profiles - mat and
+  // sigma, or with double material precision the material averaged over its
+  // eight fine cells and the profiles averaged at its position (the
+  // component's stencil is then one point)
   const double *matc[3];
   const double *sigc[3][3];
+  int dmp;                     // 1: the kernel reads matc / sigc (double material precision)
 };
 
 }  // namespace fdtdb

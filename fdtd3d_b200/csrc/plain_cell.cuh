@@ -112,6 +112,10 @@ FDTDB_HD inline double incident_value (const GeomDev &g, const double *inc, int 
 
 // One component of one half-step at one interior cell: curl (+ TF/SF) into
 // level 0 of E/H (no PML) or D/B (PML), then Drude and E-from-D.
+// DMP: per-component material and sigma arrays (double material precision);
+// CS: a current source on this family.  Both are template switches so the
+// common form keeps the shared arrays and no extra test.
+template <bool DMP, bool CS>
 FDTDB_HD inline void plain_component (const PlainHalf &p, int ci, int inc_len, int *err, int x, int y, int z)
 {
   const GeomDev &g = p.g;
@@ -122,8 +126,8 @@ FDTDB_HD inline void plain_component (const PlainHalf &p, int ci, int inc_len, i
   const double dx = g.dx;
 
   double *const *grid = p.use_pml ? p.dd[ci] : p.f[ci];
-  const double *mat = p.matc[ci] ? p.matc[ci] : p.mat;
-  const double *const *sig = p.sigc[ci][0] ? p.sigc[ci] : p.sigma;
+  const double *mat = DMP ? p.matc[ci] : p.mat;
+  const double *const *sig = DMP ? p.sigc[ci] : p.sigma;
   double val = grid[1][id];
   double ca, cb;
   if (p.use_pml)
@@ -172,7 +176,7 @@ FDTDB_HD inline void plain_component (const PlainHalf &p, int ci, int inc_len, i
   double nv = val * ca + tmp * cb;
   // J / M current source: -= (I dx) Cb on the freshly updated value, before
   // D -> E (Scheme.inc.h:1171-1260, InternalScheme.inc.h:792-795, 2423-2449)
-  if (((p.cs_mask >> ci) & 1) && x == p.cs[0] && y == p.cs[1] && z == p.cs[2])
+  if (CS && ((p.cs_mask >> ci) & 1) && x == p.cs[0] && y == p.cs[1] && z == p.cs[2])
     nv -= *p.cs_val * dx * cb;
   grid[0][id] = nv;
 

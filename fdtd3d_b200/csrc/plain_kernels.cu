@@ -20,6 +20,7 @@
 
 namespace fdtdb {
 
+template <bool DMP, bool CS>
 __global__ void __launch_bounds__ (256) plain_half_kernel (PlainHalf p, int inc_len, int *err)
 {
   // interior cells: 1 .. n - 2 on every axis a mode keeps, 0 on a dropped one
@@ -38,7 +39,7 @@ __global__ void __launch_bounds__ (256) plain_half_kernel (PlainHalf p, int inc_
     for (int ci = 0; ci < 3; ++ci)
     {
       if (p.comp[ci].exists)
-        plain_component (p, ci, inc_len, err, x, y, z);
+        plain_component<DMP, CS> (p, ci, inc_len, err, x, y, z);
     }
   }
 }
@@ -80,7 +81,17 @@ int launch_plain_half (const PlainHalf &p, int inc_len, int *err, int sm_count, 
     blocks = cap;
   if (blocks < 1)
     blocks = 1;
-  plain_half_kernel<<<(unsigned) blocks, 256, 0, s>>> (p, inc_len, err);
+  if (p.dmp)
+  {
+    if (p.cs_mask)
+      plain_half_kernel<true, true><<<(unsigned) blocks, 256, 0, s>>> (p, inc_len, err);
+    else
+      plain_half_kernel<true, false><<<(unsigned) blocks, 256, 0, s>>> (p, inc_len, err);
+  }
+  else if (p.cs_mask)
+    plain_half_kernel<false, true><<<(unsigned) blocks, 256, 0, s>>> (p, inc_len, err);
+  else
+    plain_half_kernel<false, false><<<(unsigned) blocks, 256, 0, s>>> (p, inc_len, err);
   return 1;
 }
 
