@@ -57,7 +57,7 @@ EXPORTED = (
     "fdtd_last_error", "fdtd_stream", "fdtd_profile", "fdtd_kernel_time", "fdtd_step_kernel",
     "fdtd_batch_create", "fdtd_batch_upload_eps", "fdtd_batch_tune", "fdtd_batch_step", "fdtd_batch_sync",
     "fdtd_batch_download", "fdtd_batch_info", "fdtd_batch_last_error", "fdtd_batch_destroy",
-    "fdtd_objective", "fdtd_backward", "fdtd_dft_setup", "fdtd_dft_read",
+    "fdtd_objective", "fdtd_backward", "fdtd_dft_setup", "fdtd_dft_read", "fdtd_ntff",
 )
 
 
@@ -153,6 +153,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fdtd_dft_setup": ([vp, i, i, i, i, vp], i),
         "fdtd_dft_read": ([vp, vp], i),
         "fdtd_backward": ([vp, ctypes.POINTER(AdjointCfg), vp, vp], i),
+        "fdtd_ntff": ([vp, vp, vp, vp, d, i, vp, vp], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -453,3 +454,17 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def ntff(sim_re: "Simulation", sim_im: "Simulation", left, right, teta: float, phis) -> np.ndarray:
+    """NTFF values of the complex field sim_re + i sim_im (the sine- and
+    cosine-source runs, FP64 plain form, 3-D) over the box with faces at
+    left / right, at polar angle teta and each azimuth in phis (radians)."""
+    lib = sim_re.lib
+    lo = (ctypes.c_int * 3)(*[int(v) for v in left])
+    hi = (ctypes.c_int * 3)(*[int(v) for v in right])
+    ph = np.ascontiguousarray(phis, dtype=np.float64)
+    out = np.empty(ph.size, dtype=np.float64)
+    st = lib.fdtd_ntff(sim_re._h, sim_im._h, lo, hi, float(teta), int(ph.size), ph.ctypes.data, out.ctypes.data)
+    sim_re._check(st, "fdtd_ntff")
+    return out

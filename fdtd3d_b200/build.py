@@ -47,7 +47,7 @@ def _units():
     ]
     if os.path.exists(os.path.join(CSRC, "fused3d.cu")):
         units.append(("fused3d.cu", [nvcc] + common))
-    for extra in ("sweep3d.cu", "tmz_batch.cu", "adjoint.cu", "noalloc.cu"):
+    for extra in ("sweep3d.cu", "tmz_batch.cu", "adjoint.cu", "noalloc.cu", "ntff.cu"):
         if os.path.exists(os.path.join(CSRC, extra)):
             units.append((extra, [nvcc] + common))
     return units

@@ -26,9 +26,10 @@
 // --complex-field-values writes what the reference's complex-field build
 // (COMPLEX_FIELD_VALUES) writes: two runs, sine and cosine sources, give
 // the real and imaginary parts ("coords re im" in TXT dumps, (re, im)
-// pairs in DAT dumps); material files then hold complex values, whose
-// imaginary parts must vanish.
-// Flags of subsystems outside the step path (MPI, NTFF, BMP output, test
+// pairs in DAT dumps); material files then hold complex values, of which
+// the step uses the real parts, as the reference's does.  With it, --use-ntff (3-D) writes the
+// reference's NTFF files from the two runs (fdtd_ntff).
+// Flags of subsystems outside the step path (MPI, BMP output, test
 // callbacks) are rejected with a message instead of being ignored.
 #include <sys/time.h>
 
@@ -40,6 +41,7 @@
 #include <iomanip>
 #include <limits>
 #include <map>
+#include <iostream>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -57,6 +59,14 @@ struct Opts
   int save_start[3] = {0, 0, 0}, save_end[3] = {0, 0, 0};
   std::string mat_file[6];
   int device = 0;
+  // --use-ntff and its settings, with the reference's defaults
+  // (Source/Settings/Settings.inc.h:83-88, 124, 181-187)
+  bool use_ntff = false, ntff_reverse = false, ntff_stdout = false;
+  int ntff_size[3] = {3, 3, 3};
+  int ntff_diff = 1;
+  double ntff_angle_step = 10.0;
+  int ntff_interm = 100;
+  std::string ntff_file = "ntff-res";
 };
 
 // Axes a mode drops (bit a) and the components it keeps (bit k).
@@ -183,7 +193,7 @@ int parse (std::vector<std::string> args, Opts &o)
   static const char *cs_flags[6] = {"--current-source-jx", "--current-source-jy", "--current-source-jz",
                                     "--current-source-mx", "--current-source-my", "--current-source-mz"};
   static const char *ignored[] = {"--use-ca-cb", "--use-ca-cb-pml", "--use-ca-cb-pml-metamaterials", "--use-cuda",
-                                  "--same-size-ntff", nullptr};
+                                  nullptr};
   static const char *ignored_arg[] = {"--log-level", "--cuda-buffer-size", "--num-cuda-threads", "--layout-type",
                                       nullptr};
   for (size_t i = 0; i < args.size (); ++i)
@@ -292,6 +302,27 @@ int parse (std::vector<std::string> args, Opts &o)
       o.save_dat = true;
     else if (a == "--complex-field-values")
       o.complex_values = true;
+    else if (a == "--use-ntff")
+      o.use_ntff = true;
+    else if (a == "--ntff-size" && next (v))
+    {
+      if (!parse_coord (v, o.ntff_size))
+        return fail ("bad --ntff-size");
+    }
+    else if (a == "--same-size-ntff")
+      o.ntff_size[1] = o.ntff_size[2] = o.ntff_size[0];
+    else if (a == "--ntff-diff" && next (v))
+      o.ntff_diff = std::atoi (v.c_str ());
+    else if (a == "--ntff-reverse")
+      o.ntff_reverse = true;
+    else if (a == "--ntff-filename" && next (v))
+      o.ntff_file = v;
+    else if (a == "--ntff-to-stdout")
+      o.ntff_stdout = true;
+    else if (a == "--ntff-step-angle" && next (v))
+      o.ntff_angle_step = stof_like (v);
+    else if (a == "--interm-ntff-step" && next (v))
+      o.ntff_interm = std::atoi (v.c_str ());
     else if (a == "--manual-save-coords")
       o.manual = true;
     else if (a == "--save-start-coord" && next (v))
@@ -391,9 +422,10 @@ bool load_txt (const std::string &path, size_t n, int coords, bool complex_value
     out[i++] = (double) std::stof (tok);
     if (complex_values)
     {
-      // complex build: "coords re im"; the imaginary part must vanish
+      // complex build: "coords re im"; the step reads the real part of every
+      // material value (Approximation::getMaterial, Approximation.cpp:250-255)
       std::string im;
-      if (!(ss >> im) || std::stof (im) != 0.0f)
+      if (!(ss >> im))
         return false;
     }
   }
@@ -402,7 +434,7 @@ bool load_txt (const std::string &path, size_t n, int coords, bool complex_value
 
 // DAT grid loader: raw FP64 values of the whole grid, z fastest, and
 // nothing after them (Source/File-Management/Loader/DATLoader.h:52-90);
-// (re, im) pairs in the complex build, whose imaginary parts must vanish.
+// (re, im) pairs in the complex build, of which the step reads the real part.
 bool load_dat (const std::string &path, size_t n, bool complex_values, std::vector<double> &out)
 {
   std::ifstream f (path, std::ios::binary);
@@ -418,11 +450,7 @@ bool load_dat (const std::string &path, size_t n, bool complex_values, std::vect
     return false;
   out.assign (n, 0.0);
   for (size_t i = 0; i < n; ++i)
-  {
     out[i] = raw[i * per];
-    if (complex_values && raw[i * per + 1] != 0.0)
-      return false;
-  }
   return true;
 }
 
@@ -432,7 +460,7 @@ bool load_material (const std::string &path, size_t n, int coords, bool complex_
 {
   const size_t dot = path.find_last_of ('.');
   const std::string ext = dot == std::string::npos ? "" : path.substr (dot + 1);
-  const std::string note = complex_values ? " (complex values with zero imaginary parts)" : "";
+  const std::string note = complex_values ? " (complex values: coordinates, real and imaginary part)" : "";
   if (ext == "txt")
     return load_txt (path, n, coords, complex_values, out) || (why = "cannot read " + path + note, false);
   if (ext == "dat")
@@ -497,12 +525,75 @@ bool save_txt (const std::string &name, const std::vector<double> &v, const std:
 
 }  // namespace
 
+// Scheme::saveNTFF (Source/Scheme/Scheme.inc.h:4535-4645): for every box of
+// --ntff-diff (moved in by one cell each), the forward diagram (azimuths 0 ..
+// 2 pi + pi / 180 by --ntff-step-angle at the incident polar angle) or the
+// reverse one (the incident azimuth), to ntff-res_[timestep=T]_[step=S].txt
+// or to stdout, in the reference's words and default stream formatting.
+bool save_ntff (const Opts &o, fdtd_ctx *re, fdtd_ctx *im, uint32_t t, std::string &why)
+{
+  const double pi = 3.14159265358979323846;
+  const double a1 = o.cfg.angle_teta * pi / 180.0;
+  const double a2 = o.cfg.angle_phi * pi / 180.0;
+  const double a3 = o.cfg.angle_psi * pi / 180.0;
+  for (int s = 0; s < o.ntff_diff; ++s)
+  {
+    int left[3], right[3];
+    for (int a = 0; a < 3; ++a)
+    {
+      left[a] = o.ntff_size[a] + s;
+      right[a] = o.cfg.size[a] - o.ntff_size[a] + 1 - s;
+    }
+    double start, end, step;
+    const char *name;
+    if (o.ntff_reverse)
+    {
+      name = "Reverse diagram";
+      start = end = a2;
+      step = 1.0;
+    }
+    else
+    {
+      name = "Forward diagram";
+      start = 0.0;
+      end = 2 * pi + pi / 180;
+      step = pi * o.ntff_angle_step / 180;
+    }
+    std::vector<double> phi;
+    for (double angle = start; angle <= end; angle += step)
+      phi.push_back (angle);
+    std::vector<double> val (phi.size ());
+    if (fdtd_ntff (re, im, left, right, a1, (int) phi.size (), phi.data (), val.data ()))
+      return why = std::string ("fdtd_ntff: ") + fdtd_last_error (), false;
+    std::ofstream file;
+    std::ostream *out = &std::cout;
+    if (!o.ntff_stdout)
+    {
+      const std::string fname = o.ntff_file + "_[timestep=" + std::to_string (t) + "]_[step=" + std::to_string (s)
+                                + "].txt";
+      file.open (fname);
+      if (!file)
+        return why = "cannot write " + fname, false;
+      out = &file;
+    }
+    (*out) << "==== NTFF (step=" << s << ") ====" << std::endl;
+    (*out) << name << std::endl << std::endl;
+    for (size_t i = 0; i < phi.size (); ++i)
+      (*out) << "timestep = " << t << ", incident wave angle=(" << a1 << "," << a2 << "," << a3 << ","
+             << "), angle NTFF = " << phi[i] << ", NTFF value = " << val[i] << std::endl;
+  }
+  return true;
+}
+
 int main (int argc, char **argv)
 {
   Opts o;
   std::vector<std::string> args (argv + 1, argv + argc);
   if (parse (args, o))
     return 1;
+  if (o.use_ntff && (!o.complex_values || o.cfg.mode != FDTD_MODE_DIM3 || o.cfg.precision != FDTD_PREC_FP64_PLAIN))
+    return fail ("--use-ntff needs --3d, --complex-field-values and the FP64 form (the reference computes the NTFF "
+                 "in its complex-field build only, for 3-D grids)");
   // the complex-field build's run is the sine-source run (real part) plus i
   // times the cosine-source run (imaginary part): one context for each
   const int nrun = o.complex_values ? 2 : 1;
@@ -562,10 +653,27 @@ int main (int argc, char **argv)
   }
   struct timeval tv1, tv2;
   gettimeofday (&tv1, nullptr);
-  for (int r = 0; r < nrun && !st; ++r)
-    st = fdtd_step (ctx[r], 0, (uint32_t) o.steps);
-  for (int r = 0; r < nrun && !st; ++r)
-    st = fdtd_sync (ctx[r], -1);
+  // the reference saves the NTFF after every step that ends on a multiple
+  // of --interm-ntff-step (SchemeHelper.h:100-104): step in chunks up to
+  // those times
+  uint32_t done = 0;
+  while (!st && done < (uint32_t) o.steps)
+  {
+    uint32_t stop = (uint32_t) o.steps;
+    if (o.use_ntff && o.ntff_interm > 0)
+      stop = std::min<uint32_t> (stop, (done / o.ntff_interm + 1) * o.ntff_interm);
+    for (int r = 0; r < nrun && !st; ++r)
+      st = fdtd_step (ctx[r], done, stop - done);
+    for (int r = 0; r < nrun && !st; ++r)
+      st = fdtd_sync (ctx[r], -1);
+    done = stop;
+    if (!st && o.use_ntff && o.ntff_interm > 0 && done % o.ntff_interm == 0)
+    {
+      std::string why;
+      if (!save_ntff (o, ctx[0], ctx[1], done, why))
+        return fail (why);
+    }
+  }
   gettimeofday (&tv2, nullptr);
   if (st)
     return fail (std::string ("step: ") + fdtd_status_str (st) + ": " + fdtd_last_error ());

@@ -25,6 +25,7 @@
 #include "fused3d.h"
 #include "sweep3d.h"
 #include "kernels.h"
+#include "ntff.h"
 #include "setup.h"
 
 using namespace fdtdb;
@@ -1595,6 +1596,98 @@ int fdtd_dft_read (fdtd_ctx *ctx, double *out)
   {
     out[2 * q] = acc[4 * q] + acc[4 * q + 1];
     out[2 * q + 1] = acc[4 * q + 2] + acc[4 * q + 3];
+  }
+  return FDTD_OK;
+}
+
+int fdtd_ntff (fdtd_ctx *re, fdtd_ctx *im, const int left[3], const int right[3], double teta, int nphi,
+               const double *phi, double *out)
+{
+  if (!re || !im || !left || !right || !phi || !out || nphi < 1 || re == im)
+    return fail (re, FDTD_ERR_ARG, "bad argument");
+  const Geometry &g = re->g;
+  const Geometry &gi = im->g;
+  if (re->kind != 0 || im->kind != 0)
+    return fail (re, FDTD_ERR_UNSUPPORTED, "the NTFF reads the FP64 plain form (it needs the previous H level)");
+  if (g.cfg.mode != FDTD_MODE_DIM3 || gi.cfg.mode != FDTD_MODE_DIM3)
+    return fail (re, FDTD_ERR_UNSUPPORTED, "the NTFF is 3-D (the reference's 2-D and 1-D forms are unreachable)");
+  if (re->device != im->device || g.cfg.layout != gi.cfg.layout)
+    return fail (re, FDTD_ERR_ARG, "the two runs must share the device and the layout");
+  for (int a = 0; a < 3; ++a)
+  {
+    if (g.n[a] != gi.n[a])
+      return fail (re, FDTD_ERR_ARG, "the two runs must have the same grid");
+    if (left[a] < 1 || right[a] <= left[a] || right[a] > g.n[a] - 1)
+      return fail (re, FDTD_ERR_ARG, "NTFF box out of range (1 <= left < right <= size - 1)");
+  }
+  fdtd_ctx *ctx = re;   // errors are reported on the first run
+  int r = set_device (re);
+  if (r != FDTD_OK)
+    return r;
+  CK (cudaStreamSynchronize (im->stream));
+  NtffParams p;
+  std::memset (&p, 0, sizeof (p));
+  int64_t len[3];
+  for (int a = 0; a < 3; ++a)
+  {
+    p.n[a] = g.n[a];
+    p.left[a] = left[a];
+    p.right[a] = right[a];
+    p.diff0[a] = (double) (g.n[a] / 2);
+    len[a] = right[a] - left[a];
+  }
+  p.points = 2 * (len[1] * len[2] + len[0] * len[2] + len[0] * len[1]);
+  p.dx = g.cfg.dx;
+  p.k = 2 * kPi / g.cfg.wavelength;
+  p.teta = teta;
+  p.h_centered = g.cfg.layout == 1;
+  fdtd_ctx *runs[2] = {re, im};
+  for (int k = 0; k < 6; ++k)
+  {
+    for (int a = 0; a < 3; ++a)
+      p.min_fp[k][a] = g.comp[k].min_fp[a];
+    for (int q = 0; q < 2; ++q)
+    {
+      // after a step the current level is 1 and the previous one 0 (two
+      // levels) or 2 (three), the reference's "after shift" accessors
+      p.cur[q][k] = runs[q]->f[k][1];
+      p.prev[q][k] = runs[q]->f[k][g.levels == 3 ? 2 : 0];
+    }
+  }
+  const int blocks = (int) std::max<int64_t> (1, std::min<int64_t> ((p.points + 255) / 256, 4 * re->sm_count));
+  double *phi_dev = nullptr, *partial = nullptr, *sums = nullptr;
+  struct Free
+  {
+    double **p[3];
+    ~Free ()
+    {
+      for (double **q : p)
+        if (*q)
+          cudaFree (*q);
+    }
+  } release{{&phi_dev, &partial, &sums}};
+  CK (cudaMalloc ((void **) &phi_dev, (size_t) nphi * sizeof (double)));
+  CK (cudaMalloc ((void **) &partial, (size_t) nphi * blocks * 8 * sizeof (double)));
+  CK (cudaMalloc ((void **) &sums, (size_t) nphi * 8 * sizeof (double)));
+  CK (cudaMemcpyAsync (phi_dev, phi, (size_t) nphi * sizeof (double), cudaMemcpyHostToDevice, re->stream));
+  re->launches += launch_ntff (p, phi_dev, nphi, partial, blocks, sums, re->stream);
+  CK (cudaGetLastError ());
+  std::vector<double> h ((size_t) nphi * 8);
+  CK (cudaMemcpyAsync (h.data (), sums, h.size () * sizeof (double), cudaMemcpyDeviceToHost, re->stream));
+  CK (cudaStreamSynchronize (re->stream));
+  // Pointing_scat over Pointing_inc (Scheme.inc.h:4080-4095)
+  const double k = 2 * kPi / g.cfg.wavelength;
+  const double n0 = std::sqrt (kMu0 / kEps0);
+  for (int i = 0; i < nphi; ++i)
+  {
+    const double *v = &h[(size_t) i * 8];
+    const double f_re = v[6] + v[0] * n0, f_im = v[7] + v[1] * n0;   // L.phi + N.teta n0
+    const double s_re = v[4] - v[2] * n0, s_im = v[5] - v[3] * n0;   // L.teta - N.phi n0
+    const double first_abs2 = f_re * f_re + f_im * f_im;
+    const double second_abs2 = s_re * s_re + s_im * s_im;
+    double val = (k * k) / (8 * kPi * n0) * (first_abs2 + second_abs2);
+    val /= std::sqrt (kEps0 / kMu0) / 2;
+    out[i] = val;
   }
   return FDTD_OK;
 }

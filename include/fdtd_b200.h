@@ -211,6 +211,21 @@ int64_t fdtd_launch_count (const fdtd_ctx *ctx);
 int fdtd_dft_setup (fdtd_ctx *ctx, int component, int axis, int index, int nfreq, const double *freq_hz);
 int fdtd_dft_read (fdtd_ctx *ctx, double *out);
 
+/* Near-to-far-field transform of the reference's complex-field build, 3-D;
+ * replaces Scheme::Pointing_scat / Pointing_inc and the ntffN3D_* /
+ * ntffL3D_* face sums behind Scheme::saveNTFF (Source/Scheme/Scheme.inc.h:
+ * 4037-4095, 4535-4645; Source/Scheme/SchemeHelper.h:1036-2121).  `re` and
+ * `im` are the two runs of one configuration with source_phase 0 and 1 (their
+ * fields are the real and imaginary parts of the complex build's), both in
+ * the FP64 plain form, stepped to the same time.  The box has its faces at
+ * left[a] and right[a] on axis a (the reference's leftNTFF / rightNTFF:
+ * right = size - left + 1, both moved in by the --ntff-diff step), with
+ * 1 <= left[a] < right[a] <= size[a] - 1.  For each azimuth phi[i]
+ * (radians) at polar angle teta, out[i] is the reference's "NTFF value": the
+ * scattered far-field Poynting value over the incident one. */
+int fdtd_ntff (fdtd_ctx *re, fdtd_ctx *im, const int left[3], const int right[3], double teta, int nphi,
+               const double *phi, double *out);
+
 /* Name of the kernel that performs this context's field update (no
  * reference counterpart): "plain_fp64" (FP64 plain form), "sweep3d_tma"
  * (TMA-pipelined one-sweep 3-D kernel), "fused3d_regblock" (register-blocked

@@ -191,3 +191,34 @@ def test_cli_complex_matches_reference_complex_build(fdtd, tmp_path, mode, sourc
             raise AssertionError(f"{fname}: {len(diffs)} lines differ, first: {diffs[:4]}")
         im = np.array([float(line.split()[-1]) for line in ref.splitlines()])
         assert np.max(np.abs(im)) > 0, fname
+
+
+def test_cli_complex_materials_use_real_parts(fdtd, tmp_path):
+    """Complex material files with nonzero imaginary parts: the reference's
+    step reads the real part of every material value
+    (Source/Layout/Approximation.cpp, Approximation::getMaterial), and so does
+    --complex-field-values; TXT dumps byte-identical to the complex build."""
+    if not os.path.exists(REF_COMPLEX):
+        pytest.skip("complex reference binary not built")
+    cli = os.path.join(os.path.dirname(fdtd.__file__), "fdtd3d-b200")
+    flags = _flags(6, 30, False)
+    shape = _plane_shape(6)
+    rng = np.random.default_rng(11)
+    eps = np.where(rng.random(shape) < 0.3, 4.0, 1.0)
+    im = np.round(rng.uniform(-2, 2, shape), 3)
+    idx = np.indices(shape).reshape(len(shape), -1).T
+    with open(tmp_path / "eps.txt", "w") as f:
+        for i, v, w in zip(idx, eps.reshape(-1), im.reshape(-1)):
+            f.write(" ".join(str(int(q)) for q in i) + f" {float(v)!r} {float(w)!r}\n")
+    flags += ["--load-eps-from-file", str(tmp_path / "eps.txt")]
+    out = {}
+    for name, exe, extra in (("ref", REF_COMPLEX, ["--use-ca-cb", "--use-ca-cb-pml"]),
+                             ("b200", cli, ["--complex-field-values"])):
+        d = tmp_path / name
+        d.mkdir()
+        r = subprocess.run([exe] + flags + extra, cwd=d, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+        out[name] = {f.name: f.read_text() for f in d.iterdir()}
+    assert sorted(out["ref"]) == sorted(out["b200"]) and out["ref"]
+    for fname, ref in out["ref"].items():
+        assert out["b200"][fname] == ref, fname
