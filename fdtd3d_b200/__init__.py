@@ -58,6 +58,7 @@ EXPORTED = (
     "fdtd_batch_create", "fdtd_batch_upload_eps", "fdtd_batch_tune", "fdtd_batch_step", "fdtd_batch_sync",
     "fdtd_batch_download", "fdtd_batch_info", "fdtd_batch_last_error", "fdtd_batch_destroy",
     "fdtd_objective", "fdtd_backward", "fdtd_dft_setup", "fdtd_dft_read", "fdtd_ntff",
+    "fdtd_upload_material_async", "fdtd_download_field_async",
 )
 
 
@@ -154,6 +155,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fdtd_dft_read": ([vp, vp], i),
         "fdtd_backward": ([vp, ctypes.POINTER(AdjointCfg), vp, vp], i),
         "fdtd_ntff": ([vp, vp, vp, vp, d, i, vp, vp], i),
+        "fdtd_upload_material_async": ([vp, i, vp], i),
+        "fdtd_download_field_async": ([vp, i, vp], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -87,6 +87,12 @@ struct fdtd_ctx
   float *matc32[6] = {};
   double *sigc64[6][3] = {};
   double *fine_tmp = nullptr;
+  // asynchronous host copies: a host-to-device and a device-to-host copy
+  // stream, their FP64 staging grids, and the events that order them against
+  // the context's stream (an event never recorded is complete)
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  double *stage_in = nullptr, *stage_out = nullptr;
+  cudaEvent_t in_ready = nullptr, in_free = nullptr, out_ready = nullptr, out_free = nullptr;
 
   // fused forms: two buffer sets; set fcur holds the current time level.
   // The per-cell path updates set fcur in place; the one-sweep 3-D kernel
@@ -279,6 +285,37 @@ int ensure_staging (fdtd_ctx *ctx)
   if (!ctx->staging)
     DALLOC (ctx->staging, (size_t) ctx->g.cells * sizeof (double));
   return FDTD_OK;
+}
+
+int ensure_copy_streams (fdtd_ctx *ctx)
+{
+  if (!ctx->h2d)
+  {
+    CK (cudaStreamCreateWithFlags (&ctx->h2d, cudaStreamNonBlocking));
+    CK (cudaStreamCreateWithFlags (&ctx->d2h, cudaStreamNonBlocking));
+    for (cudaEvent_t *e : {&ctx->in_ready, &ctx->in_free, &ctx->out_ready, &ctx->out_free})
+      CK (cudaEventCreateWithFlags (e, cudaEventDisableTiming));
+  }
+  if (!ctx->stage_in)
+    DALLOC (ctx->stage_in, (size_t) ctx->g.cells * sizeof (double));
+  if (!ctx->stage_out)
+    DALLOC (ctx->stage_out, (size_t) ctx->g.cells * sizeof (double));
+  return FDTD_OK;
+}
+
+// cudaSuccess once the context's stream and both copy streams are idle
+cudaError_t query_all (fdtd_ctx *ctx)
+{
+  cudaStream_t s[3] = {ctx->stream, ctx->h2d, ctx->d2h};
+  for (cudaStream_t q : s)
+  {
+    if (!q)
+      continue;
+    cudaError_t e = cudaStreamQuery (q);
+    if (e != cudaSuccess)
+      return e;
+  }
+  return cudaSuccess;
 }
 
 int ensure_src (fdtd_ctx *ctx, size_t steps)
@@ -873,6 +910,15 @@ void release (fdtd_ctx *ctx)
   cudaSetDevice (ctx->device);
   if (ctx->stream)
     cudaStreamSynchronize (ctx->stream);
+  for (cudaStream_t q : {ctx->h2d, ctx->d2h})
+    if (q)
+    {
+      cudaStreamSynchronize (q);
+      cudaStreamDestroy (q);
+    }
+  for (cudaEvent_t e : {ctx->in_ready, ctx->in_free, ctx->out_ready, ctx->out_free})
+    if (e)
+      cudaEventDestroy (e);
   for (void *p : ctx->allocs)
     cudaFree (p);
   ctx->allocs.clear ();
@@ -1357,13 +1403,18 @@ int fdtd_sync (fdtd_ctx *ctx, int64_t timeout_ns)
   if (timeout_ns < 0)
   {
     CK (cudaStreamSynchronize (ctx->stream));
+    if (ctx->h2d)
+    {
+      CK (cudaStreamSynchronize (ctx->h2d));
+      CK (cudaStreamSynchronize (ctx->d2h));
+    }
   }
   else
   {
     auto t0 = std::chrono::steady_clock::now ();
     for (;;)
     {
-      cudaError_t e = cudaStreamQuery (ctx->stream);
+      cudaError_t e = query_all (ctx);
       if (e == cudaSuccess)
         break;
       if (e != cudaErrorNotReady)
@@ -1401,6 +1452,51 @@ int fdtd_download_field_device (fdtd_ctx *ctx, int component, double *dev)
                                          component >= 3 ? 1.0 / kEta0 : 1.0, ctx->stream);
     CK (cudaGetLastError ());
   }
+  return FDTD_OK;
+}
+
+int fdtd_upload_material_async (fdtd_ctx *ctx, int which, const double *host)
+{
+  if (!ctx || !host || which < 0 || which > 5)
+    return fail (ctx, FDTD_ERR_ARG, "bad argument");
+  if (ctx->g.dmp && which < 2)
+    return fdtd_upload_material (ctx, which, host);   // the fine grid takes the synchronous path
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  if ((r = ensure_copy_streams (ctx)) != FDTD_OK)
+    return r;
+  const size_t bytes = (size_t) ctx->g.cells * sizeof (double);
+  // the staging grid is free once the previous upload has been applied
+  CK (cudaStreamWaitEvent (ctx->h2d, ctx->in_free, 0));
+  CK (cudaMemcpyAsync (ctx->stage_in, host, bytes, cudaMemcpyHostToDevice, ctx->h2d));
+  CK (cudaEventRecord (ctx->in_ready, ctx->h2d));
+  CK (cudaStreamWaitEvent (ctx->stream, ctx->in_ready, 0));
+  if ((r = fdtd_upload_material_device (ctx, which, ctx->stage_in)) != FDTD_OK)
+    return r;
+  CK (cudaEventRecord (ctx->in_free, ctx->stream));
+  return FDTD_OK;
+}
+
+int fdtd_download_field_async (fdtd_ctx *ctx, int component, double *host)
+{
+  if (!ctx || !host || component < 0 || component > 5 || !ctx->g.comp[component].exists)
+    return fail (ctx, FDTD_ERR_ARG, "bad argument");
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  if ((r = ensure_copy_streams (ctx)) != FDTD_OK)
+    return r;
+  const size_t bytes = (size_t) ctx->g.cells * sizeof (double);
+  // snapshot on the context's stream once the previous copy-out has read the
+  // staging grid, then copy out while later steps run
+  CK (cudaStreamWaitEvent (ctx->stream, ctx->out_free, 0));
+  if ((r = fdtd_download_field_device (ctx, component, ctx->stage_out)) != FDTD_OK)
+    return r;
+  CK (cudaEventRecord (ctx->out_ready, ctx->stream));
+  CK (cudaStreamWaitEvent (ctx->d2h, ctx->out_ready, 0));
+  CK (cudaMemcpyAsync (host, ctx->stage_out, bytes, cudaMemcpyDeviceToHost, ctx->d2h));
+  CK (cudaEventRecord (ctx->out_free, ctx->d2h));
   return FDTD_OK;
 }
 

@@ -160,6 +160,19 @@ int fdtd_create (const fdtd_config *cfg, int device, fdtd_ctx **out);
  * defaults (eps = mu = 1, Drude terms 0). */
 int fdtd_upload_material (fdtd_ctx *ctx, int which, const double *host);
 
+/* Host copies that overlap the time steps (no reference counterpart: the
+ * reference copies synchronously around each block, Source/Scheme/
+ * Scheme.inc.h:45-56, 461-472).  `host` should be pinned (cudaHostAlloc or
+ * cudaHostRegister; pageable memory works but does not overlap) and stays
+ * untouched until fdtd_sync returns.  fdtd_upload_material_async copies on a
+ * host-to-device copy stream and applies the grid on the context's stream
+ * ahead of every later fdtd_step; fdtd_download_field_async snapshots the
+ * component's current level on the context's stream, in order with the steps
+ * before and after it, and copies it out on a device-to-host copy stream
+ * while later steps run.  fdtd_sync also waits for both copy streams. */
+int fdtd_upload_material_async (fdtd_ctx *ctx, int which, const double *host);
+int fdtd_download_field_async (fdtd_ctx *ctx, int component, double *host);
+
 /* Sets the current time level (level 1 in the reference's Grid) of a field
  * component from size-N host doubles; replaces copyFromCPU for Ex..Hz. */
 int fdtd_upload_field (fdtd_ctx *ctx, int component, const double *host);
