@@ -58,7 +58,8 @@ EXPORTED = (
     "fdtd_batch_create", "fdtd_batch_upload_eps", "fdtd_batch_tune", "fdtd_batch_step", "fdtd_batch_sync",
     "fdtd_batch_download", "fdtd_batch_info", "fdtd_batch_last_error", "fdtd_batch_destroy",
     "fdtd_objective", "fdtd_backward", "fdtd_dft_setup", "fdtd_dft_read", "fdtd_ntff",
-    "fdtd_upload_material_async", "fdtd_download_field_async",
+    "fdtd_upload_material_async", "fdtd_download_field_async", "fdtd_download_field_scattered",
+    "fdtd_incident_length", "fdtd_download_incident",
 )
 
 
@@ -157,6 +158,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fdtd_ntff": ([vp, vp, vp, vp, d, i, vp, vp], i),
         "fdtd_upload_material_async": ([vp, i, vp], i),
         "fdtd_download_field_async": ([vp, i, vp], i),
+        "fdtd_download_field_scattered": ([vp, i, vp], i),
+        "fdtd_incident_length": ([vp], i),
+        "fdtd_download_incident": ([vp, i, vp, i], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -281,6 +285,21 @@ class Simulation:
             out = np.empty(self.cells, dtype=np.float64)
         self._check(self.lib.fdtd_download_field(self._h, k, out.ctypes.data), "download_field")
         return out.reshape(self.shape)
+
+    def scattered_field(self, comp) -> np.ndarray:
+        """The component minus the incident wave on the TF/SF box's cells."""
+        k = COMPONENTS.index(comp) if isinstance(comp, str) else comp
+        out = np.empty(self.cells, dtype=np.float64)
+        self._check(self.lib.fdtd_download_field_scattered(self._h, k, out.ctypes.data), "download_field_scattered")
+        return out.reshape(self.shape)
+
+    def incident(self, family: str = "E") -> np.ndarray:
+        """The current 1-D incident grid (EInc or HInc)."""
+        n = self.lib.fdtd_incident_length(self._h)
+        out = np.empty(n, dtype=np.float64)
+        self._check(self.lib.fdtd_download_incident(self._h, 0 if family == "E" else 1, out.ctypes.data, n),
+                    "download_incident")
+        return out
 
     def field_device(self, comp, dev_ptr: int) -> None:
         k = COMPONENTS.index(comp) if isinstance(comp, str) else comp

@@ -67,6 +67,11 @@ struct Opts
   double ntff_angle_step = 10.0;
   int ntff_interm = 100;
   std::string ntff_file = "ntff-res";
+  // dump options of Scheme::saveGrids (Settings.inc.h:199-217, 279-281)
+  bool save_interm = false, scattered_res = false, scattered_interm = false, save_no_pml = false;
+  bool save_einc = false, save_hinc = false;
+  int interm_save_step = 100;
+  bool orth[3] = {false, false, false};
 };
 
 // Axes a mode drops (bit a) and the components it keeps (bit k).
@@ -296,6 +301,22 @@ int parse (std::vector<std::string> args, Opts &o)
     }
     else if (a == "--save-res")
       o.save_res = true;
+    else if (a == "--save-interm-res")
+      o.save_interm = true;
+    else if (a == "--interm-save-step" && next (v))
+      o.interm_save_step = std::atoi (v.c_str ());
+    else if (a == "--save-scattered-field-res")
+      o.scattered_res = true;
+    else if (a == "--save-scattered--field-interm")   // the reference's spelling
+      o.scattered_interm = true;
+    else if (a == "--save-tfsf-e-incident")
+      o.save_einc = true;
+    else if (a == "--save-tfsf-h-incident")
+      o.save_hinc = true;
+    else if (a == "--save-no-pml")
+      o.save_no_pml = true;
+    else if (a == "--orth-axis-x" || a == "--orth-axis-y" || a == "--orth-axis-z")
+      o.orth[a.back () - 'x'] = true;
     else if (a == "--save-as-txt")
       o.save_txt = true;
     else if (a == "--save-as-dat")
@@ -525,6 +546,110 @@ bool save_txt (const std::string &name, const std::vector<double> &v, const std:
 
 }  // namespace
 
+// First position of component k on axis a (Source/Layout/YeeGridLayout.cpp:
+// 1937-2035): an "edge" component (E in E_CENTERED, H in H_CENTERED) sits at
+// 1.0 on its own axis and 0.5 on the others; the other family the reverse.
+double min_fp (int layout, int k, int a)
+{
+  const bool edge = (k >= 3) == (layout == 1);
+  return edge ? (a == k % 3 ? 1.0 : 0.5) : (a == k % 3 ? 0.5 : 1.0);
+}
+
+// Scheme::saveGrids (Source/Scheme/Scheme.inc.h:4367-4530) at time t: every
+// component of the mode over the save region (manual coordinates; else the
+// whole grid, inside the PML with --save-no-pml, one slice across the
+// orthogonal axis in 3-D), the scattered field when asked
+// (makeGridScattered), and the 1-D incident grids when asked, to
+// previous-1_[timestep=t]_[pid=0]_[name=F].{txt,dat}.
+bool save_grids (const Opts &o, std::vector<fdtd_ctx *> &ctx, uint32_t t, bool scattered, std::string &why)
+{
+  static const char *names[6] = {"Ex", "Ey", "Ez", "Hx", "Hy", "Hz"};
+  const unsigned drop = dropped_axes (o.cfg.mode);
+  int n[3];
+  for (int a = 0; a < 3; ++a)
+    n[a] = ((drop >> a) & 1u) ? 1 : o.cfg.size[a];
+  const size_t cells = (size_t) n[0] * n[1] * n[2];
+  const int nrun = (int) ctx.size ();
+  const int orth = o.orth[0] ? 0 : (o.orth[1] ? 1 : 2);
+  std::vector<double> buf[2];
+  for (int k = 0; k < 6; ++k)
+  {
+    if (!((mode_components (o.cfg.mode) >> k) & 1u))
+      continue;
+    int lo[3] = {0, 0, 0}, hi[3] = {n[0], n[1], n[2]};
+    if (o.manual)
+    {
+      for (int a = 0; a < 3; ++a)
+      {
+        lo[a] = o.save_start[a];
+        hi[a] = o.save_end[a];
+      }
+      for (int a = 0; a < 3; ++a)
+        if ((drop >> a) & 1u)
+        {
+          lo[a] = 0;
+          hi[a] = 1;
+        }
+    }
+    else
+    {
+      if (o.save_no_pml && o.cfg.use_pml)
+      {
+        // getStartCoord / getEndCoord (Scheme.inc.h:4645-4790): the PML
+        // borders less the component's position, truncated; the start one
+        // cell further in
+        for (int a = 0; a < 3; ++a)
+          if (!((drop >> a) & 1u))
+          {
+            lo[a] = (int) ((double) o.cfg.pml[a] - min_fp (o.cfg.layout, k, a)) + 1;
+            hi[a] = (int) ((double) (n[a] - o.cfg.pml[a]) - min_fp (o.cfg.layout, k, a));
+          }
+      }
+      if (drop == 0)
+      {
+        lo[orth] = n[orth] / 2;
+        hi[orth] = n[orth] / 2 + 1;
+      }
+    }
+    for (int r = 0; r < nrun; ++r)
+    {
+      buf[r].resize (cells);
+      const int st = scattered ? fdtd_download_field_scattered (ctx[r], k, buf[r].data ())
+                               : fdtd_download_field (ctx[r], k, buf[r].data ());
+      if (st)
+        return why = std::string ("download: ") + fdtd_last_error (), false;
+    }
+    const std::vector<double> *im = o.complex_values ? &buf[1] : nullptr;
+    const std::string base = "previous-1_[timestep=" + std::to_string (t) + "]_[pid=0]_[name=" + names[k] + "]";
+    if (o.save_txt && !save_txt (base + ".txt", buf[0], im, n, drop, lo, hi))
+      return why = "cannot write " + base + ".txt", false;
+    if (o.save_dat && !save_dat (base + ".dat", buf[0], im, n, lo, hi))
+      return why = "cannot write " + base + ".dat", false;
+  }
+  // the 1-D incident grids (a grid of one axis, dumped whole)
+  for (int fam = 0; fam < 2; ++fam)
+  {
+    if (!(fam ? o.save_hinc : o.save_einc) || !o.cfg.use_tfsf)
+      continue;
+    const int len = fdtd_incident_length (ctx[0]);
+    for (int r = 0; r < nrun; ++r)
+    {
+      buf[r].resize (len);
+      if (fdtd_download_incident (ctx[r], fam, buf[r].data (), len))
+        return why = std::string ("download_incident: ") + fdtd_last_error (), false;
+    }
+    const std::vector<double> *im = o.complex_values ? &buf[1] : nullptr;
+    const int n1[3] = {1, 1, len}, lo1[3] = {0, 0, 0}, hi1[3] = {1, 1, len};
+    const std::string base = std::string ("previous-1_[timestep=") + std::to_string (t) + "]_[pid=0]_[name="
+                             + (fam ? "HInc" : "EInc") + "]";
+    if (o.save_txt && !save_txt (base + ".txt", buf[0], im, n1, 3u, lo1, hi1))
+      return why = "cannot write " + base + ".txt", false;
+    if (o.save_dat && !save_dat (base + ".dat", buf[0], im, n1, lo1, hi1))
+      return why = "cannot write " + base + ".dat", false;
+  }
+  return true;
+}
+
 // Scheme::saveNTFF (Source/Scheme/Scheme.inc.h:4535-4645): for every box of
 // --ntff-diff (moved in by one cell each), the forward diagram (azimuths 0 ..
 // 2 pi + pi / 180 by --ntff-step-angle at the incident polar angle) or the
@@ -591,6 +716,18 @@ int main (int argc, char **argv)
   std::vector<std::string> args (argv + 1, argv + argc);
   if (parse (args, o))
     return 1;
+  if (o.save_no_pml && !o.manual && o.cfg.use_pml)
+  {
+    // the reference's getStartCoord expands the PML border to 3-D and
+    // narrows it back by position, which matches the grid's axes only when
+    // a mode keeps the leading ones; otherwise it indexes out of its grid
+    const unsigned d = dropped_axes (o.cfg.mode);
+    if (d != 0 && d != 4u && d != 6u)
+      return fail ("--save-no-pml: the reference's save region is defined for 3-D and for modes that keep x "
+                   "(and y); for this mode it indexes outside its grid");
+  }
+  if ((o.scattered_res || o.scattered_interm) && !o.cfg.use_tfsf)
+    return fail ("the scattered field needs --use-tfsf");
   if (o.use_ntff && (!o.complex_values || o.cfg.mode != FDTD_MODE_DIM3 || o.cfg.precision != FDTD_PREC_FP64_PLAIN))
     return fail ("--use-ntff needs --3d, --complex-field-values and the FP64 form (the reference computes the NTFF "
                  "in its complex-field build only, for 3-D grids)");
@@ -662,17 +799,23 @@ int main (int argc, char **argv)
     uint32_t stop = (uint32_t) o.steps;
     if (o.use_ntff && o.ntff_interm > 0)
       stop = std::min<uint32_t> (stop, (done / o.ntff_interm + 1) * o.ntff_interm);
+    if (o.save_interm && o.interm_save_step > 0)
+      stop = std::min<uint32_t> (stop, (done / o.interm_save_step + 1) * o.interm_save_step);
     for (int r = 0; r < nrun && !st; ++r)
       st = fdtd_step (ctx[r], done, stop - done);
     for (int r = 0; r < nrun && !st; ++r)
       st = fdtd_sync (ctx[r], -1);
     done = stop;
+    std::string why;
     if (!st && o.use_ntff && o.ntff_interm > 0 && done % o.ntff_interm == 0)
-    {
-      std::string why;
       if (!save_ntff (o, ctx[0], ctx[1], done, why))
         return fail (why);
-    }
+    // intermediate dumps after the NTFF, as performNSteps orders them
+    // (SchemeHelper.h:100-120)
+    if (!st && o.save_interm && o.interm_save_step > 0 && done % o.interm_save_step == 0 &&
+        (o.save_txt || o.save_dat))
+      if (!save_grids (o, ctx, done, o.scattered_interm, why))
+        return fail (why);
   }
   gettimeofday (&tv2, nullptr);
   if (st)
@@ -681,46 +824,9 @@ int main (int argc, char **argv)
                (double) (tv2.tv_usec - tv1.tv_usec) / 1000000 + (double) (tv2.tv_sec - tv1.tv_sec));
   if (o.save_res && (o.save_txt || o.save_dat))
   {
-    static const char *names[6] = {"Ex", "Ey", "Ez", "Hx", "Hy", "Hz"};
-    int lo[3] = {0, 0, 0}, hi[3] = {n[0], n[1], n[2]};
-    if (o.manual)
-    {
-      for (int a = 0; a < 3; ++a)
-      {
-        lo[a] = o.save_start[a];
-        hi[a] = o.save_end[a];
-      }
-      for (int a = 0; a < 3; ++a)
-        if ((drop >> a) & 1u)
-        {
-          lo[a] = 0;
-          hi[a] = 1;
-        }
-    }
-    else if (drop == 0)
-    {
-      lo[2] = n[2] / 2;
-      hi[2] = n[2] / 2 + 1;
-    }
-    std::vector<double> buf[2];
-    for (int k = 0; k < 6; ++k)
-    {
-      if (!((mode_components (o.cfg.mode) >> k) & 1u))
-        continue;
-      for (int r = 0; r < nrun; ++r)
-      {
-        buf[r].resize (cells);
-        st = fdtd_download_field (ctx[r], k, buf[r].data ());
-        if (st)
-          return fail (std::string ("download: ") + fdtd_last_error ());
-      }
-      const std::vector<double> *im = o.complex_values ? &buf[1] : nullptr;
-      const std::string base = "previous-1_[timestep=" + std::to_string (o.steps) + "]_[pid=0]_[name=" + names[k] + "]";
-      if (o.save_txt && !save_txt (base + ".txt", buf[0], im, n, drop, lo, hi))
-        return fail ("cannot write " + base + ".txt");
-      if (o.save_dat && !save_dat (base + ".dat", buf[0], im, n, lo, hi))
-        return fail ("cannot write " + base + ".dat");
-    }
+    std::string why;
+    if (!save_grids (o, ctx, (uint32_t) o.steps, o.scattered_res, why))
+      return fail (why);
   }
   return 0;
 }

@@ -1500,6 +1500,58 @@ int fdtd_download_field_async (fdtd_ctx *ctx, int component, double *host)
   return FDTD_OK;
 }
 
+int fdtd_incident_length (const fdtd_ctx *ctx)
+{
+  return ctx && ctx->g.cfg.use_tfsf ? ctx->g.inc_len : 0;
+}
+
+int fdtd_download_incident (fdtd_ctx *ctx, int family, double *host, int len)
+{
+  if (!ctx || !host || (family != 0 && family != 1))
+    return fail (ctx, FDTD_ERR_ARG, "bad argument");
+  if (!ctx->g.cfg.use_tfsf)
+    return fail (ctx, FDTD_ERR_STATE, "no incident grid without TF/SF");
+  if (len != ctx->g.inc_len)
+    return fail (ctx, FDTD_ERR_ARG, "the incident grid holds fdtd_incident_length () values");
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  const double *src = family ? ctx->hinc[ctx->hcur] : ctx->einc[ctx->ecur];
+  CK (cudaMemcpyAsync (host, src, (size_t) len * sizeof (double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK (cudaStreamSynchronize (ctx->stream));
+  return FDTD_OK;
+}
+
+int fdtd_download_field_scattered (fdtd_ctx *ctx, int component, double *host)
+{
+  if (!ctx || !host || component < 0 || component > 5 || !ctx->g.comp[component].exists)
+    return fail (ctx, FDTD_ERR_ARG, "bad argument");
+  const Geometry &g = ctx->g;
+  if (!g.cfg.use_tfsf)
+    return fail (ctx, FDTD_ERR_STATE, "the scattered field needs TF/SF");
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  if ((r = ensure_staging (ctx)) != FDTD_OK)
+    return r;
+  if ((r = fdtd_download_field_device (ctx, component, ctx->staging)) != FDTD_OK)
+    return r;
+  double left[3], right[3];
+  for (int a = 0; a < 3; ++a)
+  {
+    left[a] = (double) g.cfg.tfsf_left[a];
+    right[a] = (double) (g.n[a] - g.cfg.tfsf_right[a]);
+  }
+  const double *inc = component >= 3 ? ctx->hinc[ctx->hcur] : ctx->einc[ctx->ecur];
+  ctx->launches += launch_scattered (ctx->staging, make_geom_dev (g), component, inc, g.inc_len, left, right,
+                                     ctx->d_err, ctx->sm_count, ctx->stream);
+  CK (cudaGetLastError ());
+  const size_t n = (size_t) g.cells;
+  CK (cudaMemcpyAsync (host, ctx->staging, n * sizeof (double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK (cudaStreamSynchronize (ctx->stream));
+  return FDTD_OK;
+}
+
 int fdtd_download_field (fdtd_ctx *ctx, int component, double *host)
 {
   if (!ctx || !host || component < 0 || component > 5 || !ctx->g.comp[component].exists)

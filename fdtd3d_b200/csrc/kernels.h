@@ -54,6 +54,10 @@ struct FineAvg
 };
 int launch_fine_average (const double *fine, double *out64, float *out32, const FineAvg &a, int sm_count,
                          cudaStream_t s);
+// f -= incident value of component k on the TF/SF box's cells (a dump of the
+// scattered field)
+int launch_scattered (double *f, const GeomDev &g, int k, const double *inc, int inc_len, const double left[3],
+                      const double right[3], int *err, int sm_count, cudaStream_t s);
 
 int launch_fast_half (const FastHalf &p, int *err, int sm_count, cudaStream_t s);
 int launch_fast_point_source (void *f, int fp16, size_t index, const double *src, int src_index, float scale,

@@ -151,6 +151,43 @@ __global__ void fine_average_kernel (const double *fine, double *out64, float *o
   }
 }
 
+// Scattered field for a dump (Scheme::makeGridScattered, Source/Scheme/
+// Scheme.inc.h:4113-4226): inside the TF/SF box (real coordinates within
+// [left, right] on every kept axis) the component minus its incident value.
+__global__ void scattered_kernel (double *f, GeomDev g, int k, const double *inc, int inc_len, double3 left,
+                                  double3 right, int *err)
+{
+  const int64_t total = (int64_t) g.n[0] * g.n[1] * g.n[2];
+  const double lo[3] = {left.x, left.y, left.z}, hi[3] = {right.x, right.y, right.z};
+  for (int64_t id = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; id < total;
+       id += (int64_t) gridDim.x * blockDim.x)
+  {
+    const int z = (int) (id % g.n[2]);
+    const int64_t r = id / g.n[2];
+    const int y = (int) (r % g.n[1]);
+    const int x = (int) (r / g.n[1]);
+    const int p[3] = {x, y, z};
+    bool inside = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+    {
+      const double c = (double) p[a] + g.min_fp[k][a];
+      if (!((g.drop >> a) & 1) && (c < lo[a] || c > hi[a]))
+        inside = false;
+    }
+    if (inside)
+      f[id] = f[id] - incident_value (g, inc, inc_len, err, k, x, y, z);
+  }
+}
+
+int launch_scattered (double *f, const GeomDev &g, int k, const double *inc, int inc_len, const double left[3],
+                      const double right[3], int *err, int sm_count, cudaStream_t s)
+{
+  scattered_kernel<<<sm_count * 4, 256, 0, s>>> (f, g, k, inc, inc_len, make_double3 (left[0], left[1], left[2]),
+                                                 make_double3 (right[0], right[1], right[2]), err);
+  return 1;
+}
+
 int launch_fine_average (const double *fine, double *out64, float *out32, const FineAvg &a, int sm_count,
                          cudaStream_t s)
 {

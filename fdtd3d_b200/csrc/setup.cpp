@@ -526,7 +526,9 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
         break;
     }
   }
-  g.inc_len = 500 * g.n[0];
+  // 500 times the grid's first coordinate: x in 3-D, the first kept axis of
+  // a 2-D or 1-D mode (InternalScheme.specific.h:105-106)
+  g.inc_len = 500 * g.n[active (0) ? 0 : (active (1) ? 1 : 2)];
 
   // with double material precision the sigma grids are the fine ones:
   // 2 n cells, a PML of 2 p cells, the same dx (SchemeHelper.h:596-718)

@@ -160,6 +160,16 @@ int fdtd_create (const fdtd_config *cfg, int device, fdtd_ctx **out);
  * defaults (eps = mu = 1, Drude terms 0). */
 int fdtd_upload_material (fdtd_ctx *ctx, int which, const double *host);
 
+/* Dump helpers of Scheme::saveGrids (Source/Scheme/Scheme.inc.h:4113-4530):
+ * fdtd_download_field_scattered writes the component's current level minus
+ * the incident wave on the TF/SF box's cells (makeGridScattered; needs
+ * TF/SF); fdtd_download_incident writes the current 1-D incident grid,
+ * family 0 = EInc, 1 = HInc, of fdtd_incident_length () values (0 without
+ * TF/SF), as --save-tfsf-e-incident / --save-tfsf-h-incident dump it. */
+int fdtd_download_field_scattered (fdtd_ctx *ctx, int component, double *host);
+int fdtd_incident_length (const fdtd_ctx *ctx);
+int fdtd_download_incident (fdtd_ctx *ctx, int family, double *host, int len);
+
 /* Host copies that overlap the time steps (no reference counterpart: the
  * reference copies synchronously around each block, Source/Scheme/
  * Scheme.inc.h:45-56, 461-472).  `host` should be pinned (cudaHostAlloc or
