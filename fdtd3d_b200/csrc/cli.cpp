@@ -69,7 +69,7 @@ struct Opts
   std::string ntff_file = "ntff-res";
   // dump options of Scheme::saveGrids (Settings.inc.h:199-217, 279-281)
   bool save_interm = false, scattered_res = false, scattered_interm = false, save_no_pml = false;
-  bool save_einc = false, save_hinc = false;
+  bool save_einc = false, save_hinc = false, save_materials = false;
   int interm_save_step = 100;
   bool orth[3] = {false, false, false};
 };
@@ -315,6 +315,8 @@ int parse (std::vector<std::string> args, Opts &o)
       o.save_hinc = true;
     else if (a == "--save-no-pml")
       o.save_no_pml = true;
+    else if (a == "--save-materials")
+      o.save_materials = true;
     else if (a == "--orth-axis-x" || a == "--orth-axis-y" || a == "--orth-axis-z")
       o.orth[a.back () - 'x'] = true;
     else if (a == "--save-as-txt")
@@ -426,12 +428,14 @@ int parse (std::vector<std::string> args, Opts &o)
 
 // TXT grid loader: "x y [z] value" per line, z fastest; values through stof
 // (Source/File-Management/Loader/TXTLoader.h:60-100).
-bool load_txt (const std::string &path, size_t n, int coords, bool complex_values, std::vector<double> &out)
+bool load_txt (const std::string &path, size_t n, int coords, bool complex_values, std::vector<double> &out,
+               std::vector<double> &im_out)
 {
   std::ifstream f (path);
   if (!f)
     return false;
   out.assign (n, 0.0);
+  im_out.assign (complex_values ? n : 0, 0.0);
   std::string line;
   size_t i = 0;
   while (i < n && std::getline (f, line))
@@ -440,15 +444,18 @@ bool load_txt (const std::string &path, size_t n, int coords, bool complex_value
     std::string tok;
     for (int k = 0; k <= coords; ++k)
       ss >> tok;
-    out[i++] = (double) std::stof (tok);
+    out[i] = (double) std::stof (tok);
     if (complex_values)
     {
       // complex build: "coords re im"; the step reads the real part of every
-      // material value (Approximation::getMaterial, Approximation.cpp:250-255)
+      // material value (Approximation::getMaterial, Approximation.cpp:250-255),
+      // --save-materials writes both
       std::string im;
       if (!(ss >> im))
         return false;
+      im_out[i] = (double) std::stof (im);
     }
+    ++i;
   }
   return i == n;
 }
@@ -456,7 +463,8 @@ bool load_txt (const std::string &path, size_t n, int coords, bool complex_value
 // DAT grid loader: raw FP64 values of the whole grid, z fastest, and
 // nothing after them (Source/File-Management/Loader/DATLoader.h:52-90);
 // (re, im) pairs in the complex build, of which the step reads the real part.
-bool load_dat (const std::string &path, size_t n, bool complex_values, std::vector<double> &out)
+bool load_dat (const std::string &path, size_t n, bool complex_values, std::vector<double> &out,
+               std::vector<double> &im_out)
 {
   std::ifstream f (path, std::ios::binary);
   if (!f)
@@ -470,22 +478,27 @@ bool load_dat (const std::string &path, size_t n, bool complex_values, std::vect
   if (!f.eof ())
     return false;
   out.assign (n, 0.0);
+  im_out.assign (complex_values ? n : 0, 0.0);
   for (size_t i = 0; i < n; ++i)
+  {
     out[i] = raw[i * per];
+    if (complex_values)
+      im_out[i] = raw[i * per + 1];
+  }
   return true;
 }
 
 // Material file by extension (GridFileManager::getFileType, Commons.cpp:46-67).
 bool load_material (const std::string &path, size_t n, int coords, bool complex_values, std::vector<double> &out,
-                    std::string &why)
+                    std::vector<double> &im, std::string &why)
 {
   const size_t dot = path.find_last_of ('.');
   const std::string ext = dot == std::string::npos ? "" : path.substr (dot + 1);
   const std::string note = complex_values ? " (complex values: coordinates, real and imaginary part)" : "";
   if (ext == "txt")
-    return load_txt (path, n, coords, complex_values, out) || (why = "cannot read " + path + note, false);
+    return load_txt (path, n, coords, complex_values, out, im) || (why = "cannot read " + path + note, false);
   if (ext == "dat")
-    return load_dat (path, n, complex_values, out) ||
+    return load_dat (path, n, complex_values, out, im) ||
            (why = "cannot read " + path + " (expects " + std::to_string (n) + " FP64 values)" + note, false);
   why = path + ": material files are .txt or .dat";
   return false;
@@ -650,6 +663,58 @@ bool save_grids (const Opts &o, std::vector<fdtd_ctx *> &ctx, uint32_t t, bool s
   return true;
 }
 
+// --save-materials (Source/Scheme/Scheme.inc.h:3168-3225): the material
+// grids as set, before the first step, to previous-0_[timestep=0]_[pid=0]_
+// [name=Eps|Mu|OmegaPE|OmegaPM|GammaE|GammaM] (the Drude grids with
+// metamaterials only), over the save region of a grid with no component
+// offset (the doubled grid with double material precision).
+bool save_materials (const Opts &o, const std::vector<double> mat[6], const std::vector<double> mat_im[6],
+                     std::string &why)
+{
+  static const char *names[6] = {"Eps", "Mu", "OmegaPE", "OmegaPM", "GammaE", "GammaM"};
+  const unsigned drop = dropped_axes (o.cfg.mode);
+  const int orth = o.orth[0] ? 0 : (o.orth[1] ? 1 : 2);
+  for (int m = 0; m < (o.cfg.use_metamaterials ? 6 : 2); ++m)
+  {
+    const int mul = (m < 2 && o.cfg.double_material_precision) ? 2 : 1;
+    int n[3];
+    for (int a = 0; a < 3; ++a)
+      n[a] = ((drop >> a) & 1u) ? 1 : mul * o.cfg.size[a];
+    int lo[3] = {0, 0, 0}, hi[3] = {n[0], n[1], n[2]};
+    if (o.manual)
+    {
+      for (int a = 0; a < 3; ++a)
+        if (!((drop >> a) & 1u))
+        {
+          lo[a] = o.save_start[a];
+          hi[a] = o.save_end[a];
+        }
+    }
+    else
+    {
+      if (o.save_no_pml && o.cfg.use_pml)
+        for (int a = 0; a < 3; ++a)
+          if (!((drop >> a) & 1u))
+          {
+            lo[a] = o.cfg.pml[a] + 1;
+            hi[a] = n[a] - o.cfg.pml[a];
+          }
+      if (drop == 0)
+      {
+        lo[orth] = n[orth] / 2;
+        hi[orth] = n[orth] / 2 + 1;
+      }
+    }
+    const std::vector<double> *im = o.complex_values ? &mat_im[m] : nullptr;
+    const std::string base = std::string ("previous-0_[timestep=0]_[pid=0]_[name=") + names[m] + "]";
+    if (o.save_txt && !save_txt (base + ".txt", mat[m], im, n, drop, lo, hi))
+      return why = "cannot write " + base + ".txt", false;
+    if (o.save_dat && !save_dat (base + ".dat", mat[m], im, n, lo, hi))
+      return why = "cannot write " + base + ".dat", false;
+  }
+  return true;
+}
+
 // Scheme::saveNTFF (Source/Scheme/Scheme.inc.h:4535-4645): for every box of
 // --ntff-diff (moved in by one cell each), the forward diagram (azimuths 0 ..
 // 2 pi + pi / 180 by --ntff-step-angle at the incident polar angle) or the
@@ -773,20 +838,31 @@ int main (int argc, char **argv)
   if (o.cfg.double_material_precision)
     for (int a = 0; a < kept; ++a)
       fine *= 2;
+  // material grids as set (defaults eps = mu = 1, Drude terms 0), kept for
+  // --save-materials
+  std::vector<double> mat[6], mat_im[6];
   for (int m = 0; m < 6; ++m)
   {
+    mat[m].assign (m < 2 ? fine : cells, m < 2 ? 1.0 : 0.0);
+    if (o.complex_values)
+      mat_im[m].assign (mat[m].size (), 0.0);
     if (o.mat_file[m].empty ())
       continue;
-    std::vector<double> a;
     std::string why;
-    if (!load_material (o.mat_file[m], m < 2 ? fine : cells, kept, o.complex_values, a, why))
+    if (!load_material (o.mat_file[m], m < 2 ? fine : cells, kept, o.complex_values, mat[m], mat_im[m], why))
       return fail (why);
     for (int r = 0; r < nrun; ++r)
     {
-      st = fdtd_upload_material (ctx[r], m, a.data ());
+      st = fdtd_upload_material (ctx[r], m, mat[m].data ());
       if (st)
         return fail (std::string ("fdtd_upload_material: ") + fdtd_last_error ());
     }
+  }
+  if (o.save_materials && (o.save_txt || o.save_dat))
+  {
+    std::string why;
+    if (!save_materials (o, mat, mat_im, why))
+      return fail (why);
   }
   struct timeval tv1, tv2;
   gettimeofday (&tv1, nullptr);

@@ -78,3 +78,40 @@ def test_cli_complex_interm_scattered_match_reference(fdtd, tmp_path):
     flags = CASES["3d_interm_scattered_incident"] + ["--use-pml", "--pml-size", "x:3", "--same-size-pml",
                                                      "--time-steps", "25", "--save-res", "--save-as-txt"]
     _compare(_run_pair(fdtd, REF_COMPLEX, flags, tmp_path, ["--complex-field-values"]), 2)
+
+
+def _material_txt(path, shape, seed, imag=False):
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    v = np.where(rng.random(shape) < 0.3, 4.0, 1.0)
+    w = np.round(rng.uniform(-1, 1, shape), 3)
+    idx = np.indices(shape).reshape(len(shape), -1).T
+    with open(path, "w") as f:
+        for i, a, b in zip(idx, v.reshape(-1), w.reshape(-1)):
+            f.write(" ".join(str(int(q)) for q in i) + f" {float(a)!r}" + (f" {float(b)!r}" if imag else "") + "\n")
+
+
+@pytest.mark.parametrize("variant", ["3d", "3d_meta_no_pml", "tmz_manual", "3d_dmp", "complex"])
+def test_cli_save_materials_matches_reference(fdtd, tmp_path, variant):
+    ref = REF_COMPLEX if variant == "complex" else REF_BIN
+    if not os.path.exists(ref):
+        pytest.skip("reference binary not built")
+    if variant == "tmz_manual":
+        flags = ["--2d-tmz", "--size", "x:20,y:18", "--manual-save-coords", "--save-start-coord", "x:2,y:3",
+                 "--save-end-coord", "x:15,y:11"]
+        shape = (20, 18)
+    else:
+        flags = ["--3d", "--size", "x:12,y:10,z:14"]
+        shape = (12, 10, 14)
+    if variant == "3d_dmp":
+        flags.append("--use-double-material-precision")
+        shape = tuple(2 * s for s in shape)
+    _material_txt(str(tmp_path / "eps.txt"), shape, 4, imag=variant == "complex")
+    flags += ["--use-pml", "--pml-size", "x:2", "--same-size-pml", "--time-steps", "4", "--save-res", "--save-as-txt",
+              "--save-materials", "--load-eps-from-file", str(tmp_path / "eps.txt")]
+    if variant == "3d_meta_no_pml":
+        flags += ["--use-metamaterials", "--save-no-pml"]
+    out = _run_pair(fdtd, ref, flags, tmp_path, ["--complex-field-values"] if variant == "complex" else [])
+    _compare(out, 4)
+    assert any("name=Eps" in f for f in out["ref"])
