@@ -547,9 +547,10 @@ struct Arena
   std::vector<size_t> off;
   size_t total = 0;
   char *base = nullptr;
+  AdjointCache *cache = nullptr;   // when set, the allocation outlives the run
   ~Arena ()
   {
-    if (base)
+    if (base && !cache)
       cudaFree (base);
   }
   template <typename Q>
@@ -561,7 +562,26 @@ struct Arena
   }
   bool allocate ()
   {
-    return cudaMalloc (&base, std::max<size_t> (total, 256)) == cudaSuccess;
+    const size_t need = std::max<size_t> (total, 256);
+    if (cache && cache->base && cache->bytes >= need)
+    {
+      base = (char *) cache->base;
+      return true;
+    }
+    if (cache && cache->base)
+    {
+      cudaFree (cache->base);
+      cache->base = nullptr;
+      cache->bytes = 0;
+    }
+    if (cudaMalloc (&base, need) != cudaSuccess)
+      return false;
+    if (cache)
+    {
+      cache->base = base;
+      cache->bytes = need;
+    }
+    return true;
   }
   template <typename Q>
   Q *at (int i) const
@@ -713,6 +733,7 @@ std::string run_t (const Geometry &g, const void *eps_dev, bool eps_is_double, c
   const uint32_t K = std::min (run.every, run.steps);
   const uint32_t nck = (run.steps + K - 1) / K;
   Arena ar;
+  ar.cache = run.cache;
   std::vector<int> i_tab;
   for (const auto &v : tabs)
     i_tab.push_back (ar.reserve<R> (v.size ()));

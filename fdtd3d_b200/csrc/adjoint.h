@@ -20,6 +20,14 @@
 
 namespace fdtdb {
 
+// Device memory kept between runs of one context: a run takes it when it is
+// large enough and replaces it otherwise (freed by the owner).
+struct AdjointCache
+{
+  void *base = nullptr;
+  size_t bytes = 0;
+};
+
 struct AdjointRun
 {
   uint32_t steps = 0;
@@ -27,6 +35,7 @@ struct AdjointRun
   int probe_lo[2] = {0, 0};
   int probe_hi[2] = {0, 0};    // exclusive
   bool fp64 = false;
+  AdjointCache *cache = nullptr;   // null: allocate and free per run
 };
 
 // eps_dev: per-cell permittivity on the device (float when eps_is_double is

@@ -87,6 +87,7 @@ struct fdtd_ctx
   float *matc32[6] = {};
   double *sigc64[6][3] = {};
   double *fine_tmp = nullptr;
+  AdjointCache adj_cache;      // the adjoint's device memory, kept between calls
   // asynchronous host copies: a host-to-device and a device-to-host copy
   // stream, their FP64 staging grids, and the events that order them against
   // the context's stream (an event never recorded is complete)
@@ -919,6 +920,8 @@ void release (fdtd_ctx *ctx)
   for (cudaEvent_t e : {ctx->in_ready, ctx->in_free, ctx->out_ready, ctx->out_free})
     if (e)
       cudaEventDestroy (e);
+  if (ctx->adj_cache.base)
+    cudaFree (ctx->adj_cache.base);
   for (void *p : ctx->allocs)
     cudaFree (p);
   ctx->allocs.clear ();
@@ -1667,6 +1670,7 @@ int adjoint_entry (fdtd_ctx *ctx, const fdtd_adjoint_cfg *cfg, double *objective
   AdjointRun run;
   run.steps = cfg->steps;
   run.every = cfg->checkpoint_every;
+  run.cache = &ctx->adj_cache;
   for (int a = 0; a < 2; ++a)
   {
     run.probe_lo[a] = cfg->probe_lo[a];
