@@ -88,6 +88,7 @@ struct fdtd_ctx
   double *sigc64[6][3] = {};
   double *fine_tmp = nullptr;
   AdjointCache adj_cache;      // the adjoint's device memory, kept between calls
+  SweepStreams sweep_streams;  // side streams of the sweep's item classes (FDTDB_SWEEP_CONCURRENT=0: none)
   // asynchronous host copies: a host-to-device and a device-to-host copy
   // stream, their FP64 staging grids, and the events that order them against
   // the context's stream (an event never recorded is complete)
@@ -714,6 +715,20 @@ int plan_sweep (fdtd_ctx *ctx)
       return FDTD_OK;
     }
   const int wy = 8;
+  if (!ctx->sweep_streams.side[0])
+  {
+    bool conc = true;
+    if (const char *v = std::getenv ("FDTDB_SWEEP_CONCURRENT"))
+      conc = std::atoi (v) != 0;
+    if (conc)
+    {
+      SweepStreams &ss = ctx->sweep_streams;
+      for (cudaStream_t &q : ss.side)
+        CK (cudaStreamCreateWithFlags (&q, cudaStreamNonBlocking));
+      for (cudaEvent_t *e : {&ss.fork, &ss.join[0], &ss.join[1]})
+        CK (cudaEventCreateWithFlags (e, cudaEventDisableTiming));
+    }
+  }
   bool lean = true;
   if (const char *v = std::getenv ("FDTDB_SWEEP_LEAN"))
     lean = std::atoi (v) != 0;
@@ -922,6 +937,15 @@ void release (fdtd_ctx *ctx)
       cudaEventDestroy (e);
   if (ctx->adj_cache.base)
     cudaFree (ctx->adj_cache.base);
+  for (cudaStream_t q : ctx->sweep_streams.side)
+    if (q)
+    {
+      cudaStreamSynchronize (q);
+      cudaStreamDestroy (q);
+    }
+  for (cudaEvent_t e : {ctx->sweep_streams.fork, ctx->sweep_streams.join[0], ctx->sweep_streams.join[1]})
+    if (e)
+      cudaEventDestroy (e);
   for (void *p : ctx->allocs)
     cudaFree (p);
   ctx->allocs.clear ();
@@ -1160,7 +1184,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
         return r;
       if (ctx->sweep_state == 1)
       {
-        ctx->launches += launch_sweep3d (ctx->sweep, o, f, ctx->d_err, s);
+        ctx->launches += launch_sweep3d (ctx->sweep, o, f, ctx->d_err, s, ctx->sweep_streams);
         if (ctx->drude_fix)
           ctx->launches += launch_drude_fixup (f, ctx->drude_box, s);
         if (f.tfsf_post)

@@ -1289,10 +1289,22 @@ std::string plan_t (SweepPlan &pl, const FusedParams &p, void *const e[2][3], vo
 }
 
 template <typename T, int WY>
-int launch_t (const SweepPlan &pl, int set, const FusedParams &p, int *err, cudaStream_t s)
+int launch_t (const SweepPlan &pl, int set, const FusedParams &p, int *err, cudaStream_t s, const SweepStreams &ss)
 {
-  // heaviest class first, so that the lighter items fill in behind it
+  // heaviest class first, so that the lighter items fill in behind it; on
+  // side streams the next class's CTAs take the SMs as the previous class's
+  // persistent CTAs run out of items
   constexpr unsigned sm = Smem<T, WY>::TOTAL;
+  const bool conc = ss.side[0] && ss.side[1];
+  cudaStream_t s1 = s, s0 = s;
+  if (conc)
+  {
+    cudaEventRecord (ss.fork, s);
+    cudaStreamWaitEvent (ss.side[0], ss.fork, 0);
+    cudaStreamWaitEvent (ss.side[1], ss.fork, 0);
+    s1 = ss.side[0];
+    s0 = ss.side[1];
+  }
   int n = 0;
   if (pl.items[2] > 0)
   {
@@ -1306,13 +1318,20 @@ int launch_t (const SweepPlan &pl, int set, const FusedParams &p, int *err, cuda
   }
   if (pl.items[1] > 0)
   {
-    sweep3d_kernel<T, WY, 1><<<pl.ctas, dim3 (32, WY), sm, s>>> (pl.maps[set], p, pl.work, err);
+    sweep3d_kernel<T, WY, 1><<<pl.ctas, dim3 (32, WY), sm, s1>>> (pl.maps[set], p, pl.work, err);
     ++n;
   }
   if (pl.items[0] > 0)
   {
-    sweep3d_kernel<T, WY, 0><<<pl.ctas, dim3 (32, WY), sm, s>>> (pl.maps[set], p, pl.work, err);
+    sweep3d_kernel<T, WY, 0><<<pl.ctas, dim3 (32, WY), sm, s0>>> (pl.maps[set], p, pl.work, err);
     ++n;
+  }
+  if (conc)
+  {
+    cudaEventRecord (ss.join[0], ss.side[0]);
+    cudaEventRecord (ss.join[1], ss.side[1]);
+    cudaStreamWaitEvent (s, ss.join[0], 0);
+    cudaStreamWaitEvent (s, ss.join[1], 0);
   }
   return n;
 }
@@ -1393,9 +1412,10 @@ std::string sweep3d_plan (SweepPlan &plan, const FusedParams &p, void *const e[2
   return "";
 }
 
-int launch_sweep3d (const SweepPlan &plan, int set, const FusedParams &p, int *err, cudaStream_t s)
+int launch_sweep3d (const SweepPlan &plan, int set, const FusedParams &p, int *err, cudaStream_t s,
+                    const SweepStreams &ss)
 {
-  return p.fp16 ? launch_t<__half, 8> (plan, set, p, err, s) : launch_t<float, 8> (plan, set, p, err, s);
+  return p.fp16 ? launch_t<__half, 8> (plan, set, p, err, s, ss) : launch_t<float, 8> (plan, set, p, err, s, ss);
 }
 
 }  // namespace fdtdb

@@ -58,9 +58,22 @@ std::string sweep3d_plan (SweepPlan &plan, const FusedParams &p, void *const e[2
                           float *const aux[2][6], const float *eps, int sm_count, int wy, int chunk,
                           unsigned long long *ctr, bool lean = true);
 
+// Side streams for the item classes: the classes of one step write disjoint
+// items and read only the old set, so they may run concurrently; then the
+// SMs that one class's persistent CTAs leave take the next class's CTAs
+// instead of idling through its tail.  fork is recorded on the main stream,
+// join[j] on side[j] (all null: one stream).
+struct SweepStreams
+{
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
+};
+
 // One time step with buffer set `set` as the old set (one launch per item
-// class that has items; returns how many).
-int launch_sweep3d (const SweepPlan &plan, int set, const FusedParams &p, int *err, cudaStream_t s);
+// class that has items; returns how many).  With side streams the z-edge
+// and the lean class run on them, joined back into s before returning.
+int launch_sweep3d (const SweepPlan &plan, int set, const FusedParams &p, int *err, cudaStream_t s,
+                    const SweepStreams &ss = SweepStreams ());
 
 }  // namespace fdtdb
 
