@@ -1291,9 +1291,8 @@ std::string plan_t (SweepPlan &pl, const FusedParams &p, void *const e[2][3], vo
 template <typename T, int WY>
 int launch_t (const SweepPlan &pl, int set, const FusedParams &p, int *err, cudaStream_t s, const SweepStreams &ss)
 {
-  // heaviest class first, so that the lighter items fill in behind it; on
-  // side streams the next class's CTAs take the SMs as the previous class's
-  // persistent CTAs run out of items
+  // on side streams the next class's CTAs take the SMs as the previous
+  // class's persistent CTAs run out of items
   constexpr unsigned sm = Smem<T, WY>::TOTAL;
   const bool conc = ss.side[0] && ss.side[1];
   cudaStream_t s1 = s, s0 = s;
@@ -1311,19 +1310,30 @@ int launch_t (const SweepPlan &pl, int set, const FusedParams &p, int *err, cuda
     sweep3d_kernel<T, WY, 2><<<pl.ctas, dim3 (32, WY), sm, s>>> (pl.maps[set], p, pl.work, err);
     ++n;
   }
-  if (pl.items[3] > 0)
+  // launch order of the PML (3), z-edge (1) and lean (0) classes on s, s1,
+  // s0: z-edge, lean, PML measured best at 512^3 (1.680 ms per step against
+  // 1.689 for PML, z-edge, lean and 1.723 for PML, lean, z-edge);
+  // FDTDB_SWEEP_ORDER (tuning runs) permutes it
+  static const std::string order = [] {
+    const char *v = std::getenv ("FDTDB_SWEEP_ORDER");
+    const std::string o = v ? v : "103";
+    return (o.size () == 3 && o.find ('0') != std::string::npos && o.find ('1') != std::string::npos &&
+            o.find ('3') != std::string::npos)
+               ? o
+               : std::string ("103");
+  }();
+  const cudaStream_t on[3] = {s, s1, s0};
+  for (int j = 0; j < 3; ++j)
   {
-    sweep3d_kernel<T, WY, 3><<<pl.ctas, dim3 (32, WY), sm, s>>> (pl.maps[set], p, pl.work, err);
-    ++n;
-  }
-  if (pl.items[1] > 0)
-  {
-    sweep3d_kernel<T, WY, 1><<<pl.ctas, dim3 (32, WY), sm, s1>>> (pl.maps[set], p, pl.work, err);
-    ++n;
-  }
-  if (pl.items[0] > 0)
-  {
-    sweep3d_kernel<T, WY, 0><<<pl.ctas, dim3 (32, WY), sm, s0>>> (pl.maps[set], p, pl.work, err);
+    const int c = order[j] - '0';
+    if (pl.items[c] <= 0)
+      continue;
+    if (c == 3)
+      sweep3d_kernel<T, WY, 3><<<pl.ctas, dim3 (32, WY), sm, on[j]>>> (pl.maps[set], p, pl.work, err);
+    else if (c == 1)
+      sweep3d_kernel<T, WY, 1><<<pl.ctas, dim3 (32, WY), sm, on[j]>>> (pl.maps[set], p, pl.work, err);
+    else
+      sweep3d_kernel<T, WY, 0><<<pl.ctas, dim3 (32, WY), sm, on[j]>>> (pl.maps[set], p, pl.work, err);
     ++n;
   }
   if (conc)
