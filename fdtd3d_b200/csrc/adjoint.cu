@@ -637,13 +637,11 @@ std::string run_t (const Geometry &g, const void *eps_dev, bool eps_is_double, c
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor (&per_sm, adjoint_kernel<R>, kThreads, 0) != cudaSuccess ||
       per_sm < 1)
     return "the adjoint kernel does not fit on an SM";
-  int cap = 3;
-  if (const char *e = std::getenv ("FDTDB_ADJ_CTAS_PER_SM"))
-    cap = std::max (1, std::atoi (e));
+  // 3 CTAs per SM and an even split between the reversing and the
+  // recomputing group measured fastest
+  const int cap = 3;
   const int ctas = sm_count * std::min (per_sm, cap);
-  double split = 0.5;
-  if (const char *e = std::getenv ("FDTDB_ADJ_SPLIT"))
-    split = std::min (0.9, std::max (0.1, std::atof (e)));
+  const double split = 0.5;
   const int fwd_split = std::max (1, std::min (ctas - 1, (int) std::lround (ctas * split)));
 
   AdjDev<R> p{};

@@ -399,6 +399,26 @@ int launch_reduce_final (const double *partials, int nblocks, double *out, cudaS
   return 1;
 }
 
+// The same two launches through cudaLaunchKernel, so that each returns its
+// own launch status and an earlier, unrelated error pending on the calling
+// thread is neither reported nor cleared.
+cudaError_t launch_reduce_sq_checked (const void *src, int kind, size_t n, const void *weight, int wkind,
+                                      double scale, double *partials, int nblocks, cudaStream_t s)
+{
+  const void *fn = kind == 0 ? (const void *) reduce_sq_kernel<0>
+                   : kind == 1 ? (const void *) reduce_sq_kernel<1>
+                               : (const void *) reduce_sq_kernel<2>;
+  void *args[] = {(void *) &src, (void *) &n, (void *) &weight, (void *) &wkind, (void *) &scale,
+                  (void *) &partials};
+  return cudaLaunchKernel (fn, dim3 (nblocks), dim3 (256), args, 0, s);
+}
+
+cudaError_t launch_reduce_final_checked (const double *partials, int nblocks, double *out, cudaStream_t s)
+{
+  void *args[] = {(void *) &partials, (void *) &nblocks, (void *) &out};
+  return cudaLaunchKernel ((const void *) reduce_final_kernel, dim3 (1), dim3 (32), args, 0, s);
+}
+
 }  // namespace fdtdb
 
 // ------------------------------------------------------------ running DFT

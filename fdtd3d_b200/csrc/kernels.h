@@ -79,5 +79,12 @@ int launch_fill (double *dst, size_t n, double value, cudaStream_t s);
 int launch_dft (const void *src, int kind, int axis, int index, const int n[3], double scale, const double *phase,
                 int nf, double *acc, int sm_count, cudaStream_t s);
 int launch_reduce_final (const double *partials, int nblocks, double *out, cudaStream_t s);
+// the two reduction launches with their own launch status (cudaLaunchKernel)
+cudaError_t launch_reduce_sq_checked (const void *src, int kind, size_t n, const void *weight, int wkind,
+                                      double scale, double *partials, int nblocks, cudaStream_t s);
+cudaError_t launch_reduce_final_checked (const double *partials, int nblocks, double *out, cudaStream_t s);
+
+// Sets the text fdtd_last_error() returns on the calling host thread.
+void set_last_error (const char *msg);
 
 }  // namespace fdtdb

@@ -8,15 +8,15 @@
 // per-block partial sums live in a fixed file-scope device array instead of
 // memory allocated per call or per context.
 //
-// The array is kNoAllocMaxBlocks pairs of doubles (16 KiB plus a small
-// tail).  Every GPU that loads the library holds it until the process
-// exits.  All calls share it, so calls that overlap on the GPU (different
-// streams, or different host threads on one device) race on it and must be
-// ordered by the caller.  Each call rewrites every partial it reads before
-// reading it, so nothing has to be cleared between calls.
+// The array is kNoAllocMaxBlocks pairs of doubles (16 KiB).  Every GPU that
+// loads the library holds it until the process exits.  All calls share it,
+// so calls that overlap on the GPU (different streams, or different host
+// threads on one device) race on it and must be ordered by the caller.
+// Each call rewrites every partial it reads before reading it, so nothing
+// has to be cleared between calls.
 #include <cuda_runtime.h>
 
-#include <mutex>
+#include <string>
 
 #include "../../include/fdtd_b200.h"
 #include "kernels.h"
@@ -27,32 +27,34 @@ namespace {
 
 constexpr int kNoAllocMaxBlocks = 1024;
 
-// (sum, compensation) per block; never addressed from host code directly:
-// on the host the name is only a stand-in, so its device address is looked
-// up per device at set-up.
+// (sum, compensation) per block.  In host code this name is only a
+// stand-in for the device array, never a device address: its address on the
+// current device comes from cudaGetSymbolAddress.
 __device__ __align__ (256) double g_noalloc_partials[2 * kNoAllocMaxBlocks];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-double *g_partials_addr[kMaxDevices] = {};
+int refuse (int code, const std::string &msg)
+{
+  set_last_error (msg.c_str ());
+  return code;
+}
 
-// First call on a device (with that device current): resolve the device
-// address of the static array once and cache it.
+// Device address of the static array on the current device.  The first call
+// on a device loads the library's device code there (the set-up); later
+// calls are a lookup in the runtime's table.  Looking the address up on
+// every call (rather than caching it per device ordinal) keeps it right
+// after a cudaDeviceReset, which reloads the device code at a new address.
 int partials_for_current_device (double **out)
 {
-  int dev = -1;
-  if (cudaGetDevice (&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
-    return FDTD_ERR_CUDA;
-  std::lock_guard<std::mutex> lock (g_setup_mutex);
-  if (!g_partials_addr[dev])
+  void *ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress (&ptr, g_noalloc_partials);
+  if (e != cudaSuccess || !ptr)
   {
-    void *ptr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress (&ptr, g_noalloc_partials);
-    if (e != cudaSuccess || !ptr)
-      return FDTD_ERR_CUDA;
-    g_partials_addr[dev] = (double *) ptr;
+    if (e != cudaSuccess)
+      cudaGetLastError ();   // the failure above is this call's own: do not leave it pending
+    return refuse (FDTD_ERR_CUDA, std::string ("cudaGetSymbolAddress of the static scratch: ") +
+                                      cudaGetErrorString (e));
   }
-  *out = g_partials_addr[dev];
+  *out = (double *) ptr;
   return FDTD_OK;
 }
 
@@ -64,22 +66,34 @@ extern "C" int fdtd_reduce_sq_noalloc (const void *src, int src_kind, size_t n, 
                                        double scale, int blocks, double *out_dev, void *stream)
 {
   using namespace fdtdb;
-  if (!out_dev || (n > 0 && !src) || src_kind < 0 || src_kind > 2 || weight_kind < 0 || weight_kind > 2
-      || (weight_kind != 0 && !weight) || blocks < 0)
-    return FDTD_ERR_ARG;
-  if (blocks > kNoAllocMaxBlocks)
-    return FDTD_ERR_ARG;   // more partials than the static scratch holds
+  if (!out_dev || (n > 0 && !src))
+    return refuse (FDTD_ERR_ARG, "fdtd_reduce_sq_noalloc: null output, or null input with n > 0");
+  if (src_kind < 0 || src_kind > 2)
+    return refuse (FDTD_ERR_ARG, "fdtd_reduce_sq_noalloc: src_kind must be 0 (double), 1 (float) or 2 (half)");
+  if (weight_kind < 0 || weight_kind > 2)
+    return refuse (FDTD_ERR_ARG, "fdtd_reduce_sq_noalloc: weight_kind must be 0 (none), 1 (float) or 2 (double)");
+  if (weight_kind != 0 && !weight)
+    return refuse (FDTD_ERR_ARG, "fdtd_reduce_sq_noalloc: weight_kind != 0 needs a weight buffer");
+  if (blocks < 0 || blocks > kNoAllocMaxBlocks)
+    return refuse (FDTD_ERR_ARG, "fdtd_reduce_sq_noalloc: blocks must be 0 (automatic) .. 1024, the size of the "
+                                 "static scratch");
   if (blocks == 0)
   {
-    size_t want = (n + 255) / 256;
+    const size_t want = (n + 255) / 256;
     blocks = (int) (want < 1 ? 1 : (want > (size_t) kNoAllocMaxBlocks ? kNoAllocMaxBlocks : want));
   }
   double *partials = nullptr;
-  int r = partials_for_current_device (&partials);
+  const int r = partials_for_current_device (&partials);
   if (r != FDTD_OK)
     return r;
-  cudaStream_t s = (cudaStream_t) stream;
-  launch_reduce_sq (src, src_kind, n, weight, weight_kind, scale, partials, blocks, s);
-  launch_reduce_final (partials, blocks, out_dev, s);
-  return cudaGetLastError () == cudaSuccess ? FDTD_OK : FDTD_ERR_CUDA;
+  const cudaStream_t s = (cudaStream_t) stream;
+  cudaError_t e = launch_reduce_sq_checked (src, src_kind, n, weight, weight_kind, scale, partials, blocks, s);
+  if (e == cudaSuccess)
+    e = launch_reduce_final_checked (partials, blocks, out_dev, s);
+  if (e != cudaSuccess)
+  {
+    cudaGetLastError ();   // clear this call's own launch error
+    return refuse (FDTD_ERR_CUDA, std::string ("fdtd_reduce_sq_noalloc: launch failed: ") + cudaGetErrorString (e));
+  }
+  return FDTD_OK;
 }

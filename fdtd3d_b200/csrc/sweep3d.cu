@@ -1207,17 +1207,10 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn ()
 // 3-D map over an (nx, ny, nz) array, z fastest, box bw x bh x 1
 bool make_map (CUtensorMap &m, const void *base, bool half, const int n[3], int bw, int bh)
 {
-  // L2 fetch granularity of the copies (FDTDB_TMA_L2PROMO 0..3 = none,
-  // 64, 128, 256 bytes; tuning runs): 64 bytes measured best at 512^3 with
-  // the concurrent class launches (1.673 ms per step against 1.681 for 128
-  // and none, 1.700 for 256)
-  static const CUtensorMapL2promotion promo = [] {
-    const char *v = std::getenv ("FDTDB_TMA_L2PROMO");
-    const int k = v ? std::atoi (v) : 1;
-    return k == 0 ? CU_TENSOR_MAP_L2_PROMOTION_NONE
-                  : (k == 1 ? CU_TENSOR_MAP_L2_PROMOTION_L2_64B
-                            : (k == 3 ? CU_TENSOR_MAP_L2_PROMOTION_L2_256B : CU_TENSOR_MAP_L2_PROMOTION_L2_128B));
-  }();
+  // L2 fetch granularity of the copies: 64 bytes measured best at 512^3
+  // with the concurrent class launches (1.673 ms per step against 1.681 for
+  // 128 bytes and none, 1.700 for 256)
+  constexpr CUtensorMapL2promotion promo = CU_TENSOR_MAP_L2_PROMOTION_L2_64B;
   auto fn = encode_fn ();
   if (!fn)
     return false;
@@ -1314,16 +1307,8 @@ int launch_t (const SweepPlan &pl, int set, const FusedParams &p, int *err, cuda
   }
   // launch order of the PML (3), z-edge (1) and lean (0) classes on s, s1,
   // s0: z-edge, lean, PML measured best at 512^3 (1.680 ms per step against
-  // 1.689 for PML, z-edge, lean and 1.723 for PML, lean, z-edge);
-  // FDTDB_SWEEP_ORDER (tuning runs) permutes it
-  static const std::string order = [] {
-    const char *v = std::getenv ("FDTDB_SWEEP_ORDER");
-    const std::string o = v ? v : "103";
-    return (o.size () == 3 && o.find ('0') != std::string::npos && o.find ('1') != std::string::npos &&
-            o.find ('3') != std::string::npos)
-               ? o
-               : std::string ("103");
-  }();
+  // 1.689 for PML, z-edge, lean and 1.723 for PML, lean, z-edge)
+  constexpr char order[4] = "103";
   const cudaStream_t on[3] = {s, s1, s0};
   for (int j = 0; j < 3; ++j)
   {

@@ -340,13 +340,19 @@ void fdtd_batch_destroy (fdtd_batch *b);
  * allocator owns the device memory budget, or a real-time step loop where
  * cudaMalloc can stall and cudaFree synchronises the device).  It allocates
  * nothing: the per-block partial sums live in one fixed static device array
- * of 1024 (sum, compensation) pairs.  src_kind / weight_kind: 0 double,
- * 1 float, 2 half (weight: 0 = no weight).  blocks = 0 picks the block
- * count; blocks > 1024 is rejected with FDTD_ERR_ARG.  The first call on a
- * device resolves the array's address with that device current and caches
- * it, so that call must come before any capture of work into a stream.
- * All calls share the array: calls that overlap on the GPU race, and the
- * caller must order them.  No counterpart in the reference. */
+ * of 1024 (sum, compensation) pairs.  src (n elements) by src_kind:
+ * 0 double, 1 float, 2 half.  weight (n elements, or null) by weight_kind:
+ * 0 no weight (weight ignored), 1 float, 2 double; any other kind is
+ * rejected with FDTD_ERR_ARG.  blocks = 0 picks the block count;
+ * blocks > 1024 is rejected with FDTD_ERR_ARG.  Every call looks the
+ * array's address up with cudaGetSymbolAddress on the caller's current
+ * device; the first call on a device also loads the library's device code
+ * there, so that first call must come before any capture of work into a
+ * stream.  Looking the address up per call keeps it valid after a
+ * cudaDeviceReset.  All calls share the array: calls that overlap on the
+ * GPU race, and the caller must order them.  Failures set
+ * fdtd_last_error(); an error left pending by earlier, unrelated CUDA work
+ * is neither reported nor cleared.  No counterpart in the reference. */
 int fdtd_reduce_sq_noalloc (const void *src, int src_kind, size_t n, const void *weight, int weight_kind,
                             double scale, int blocks, double *out_dev, void *stream);
 

@@ -106,7 +106,9 @@ def extract_1d_modes(src_root):
 
 
 def main():
-    src_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference source root>")
+    src_root = sys.argv[1]
     with open(os.path.join(HERE, "exhy_1d_unit_test.json"), "w") as f:
         json.dump(extract_exhy(src_root), f, indent=1)
     with open(os.path.join(HERE, "unit_test_1d_modes.json"), "w") as f:
