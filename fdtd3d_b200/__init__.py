@@ -59,7 +59,8 @@ EXPORTED = (
     "fdtd_batch_download", "fdtd_batch_info", "fdtd_batch_last_error", "fdtd_batch_destroy",
     "fdtd_objective", "fdtd_backward", "fdtd_dft_setup", "fdtd_dft_read", "fdtd_ntff",
     "fdtd_upload_material_async", "fdtd_download_field_async", "fdtd_download_field_scattered",
-    "fdtd_incident_length", "fdtd_download_incident",
+    "fdtd_incident_length", "fdtd_download_incident", "fdtd_set_wait_limit", "fdtd_batch_set_wait_limit",
+    "fdtd_inject_alloc_failure",
 )
 
 
@@ -161,6 +162,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fdtd_download_field_scattered": ([vp, i, vp], i),
         "fdtd_incident_length": ([vp], i),
         "fdtd_download_incident": ([vp, i, vp, i], i),
+        "fdtd_set_wait_limit": ([vp, i64], i),
+        "fdtd_batch_set_wait_limit": ([vp, i64], i),
+        "fdtd_inject_alloc_failure": ([i64], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -168,6 +172,13 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         fn.restype = res
     _lib = lib
     return lib
+
+
+def inject_alloc_failure(after: int) -> None:
+    """Host-side fault injection: the next ``after`` device / pinned allocations
+    of the library succeed, later ones fail with FDTD_ERR_NOMEM; ``after`` < 0
+    turns it off (fdtd_inject_alloc_failure)."""
+    load_library().fdtd_inject_alloc_failure(int(after))
 
 
 def f32(x: float) -> float:
@@ -318,6 +329,10 @@ class Simulation:
     def launch_count(self) -> int:
         return int(self.lib.fdtd_launch_count(self._h))
 
+    def set_wait_limit(self, limit_ns: int) -> None:
+        """Time limit of one grid-barrier wait of the adjoint kernel (<= 0: the default, 2 s)."""
+        self._check(self.lib.fdtd_set_wait_limit(self._h, int(limit_ns)), "set_wait_limit")
+
     def _adjoint_cfg(self, steps, every, probe_lo, probe_hi, precision):
         c = AdjointCfg()
         c.steps = int(steps)
@@ -451,6 +466,10 @@ class Batch:
         out = np.empty(nx * ny)
         self._check(self.lib.fdtd_batch_download(self._h, i, k, out.ctypes.data), "batch_download")
         return out.reshape(nx, ny)
+
+    def set_wait_limit(self, limit_ns: int) -> None:
+        """Time limit of one wait at the batch kernel's grid barrier (<= 0: the default, 5 s)."""
+        self._check(self.lib.fdtd_batch_set_wait_limit(self._h, int(limit_ns)), "batch_set_wait_limit")
 
     def info(self) -> dict:
         cells = ctypes.c_int64()

@@ -35,6 +35,7 @@
 #include <vector>
 
 #include "adjoint.h"
+#include "kernels.h"
 
 namespace fdtdb {
 
@@ -44,7 +45,7 @@ constexpr int kEz = 0, kHx = 1, kHy = 2;   // local component slots
 constexpr double kEta0Adj = 376.730313461770655;
 constexpr int kThreads = 512;
 constexpr int kBarStride = 64;             // words per group barrier: arrivals at [0], generation at [32]
-constexpr long long kBarrierTimeoutNs = 2000000000LL;
+constexpr long long kDefaultBarrierLimitNs = 2000000000LL;   // 2 s
 
 template <typename R>
 struct AdjDev
@@ -93,6 +94,7 @@ struct Launch
   // 128-byte line, so polling does not slow the arrivals)
   unsigned *bar;
   int *err;
+  long long limit_ns;          // time limit of one barrier wait
 };
 
 // values that other CTAs of the launch write are read through L2
@@ -111,7 +113,7 @@ __device__ __forceinline__ long long globaltimer ()
 
 // Barrier over the `ctas` CTAs of one group, with a time limit.  Returns
 // false (and sets *err) when any CTA gave up; every CTA then leaves.
-__device__ bool group_barrier (unsigned *bar, unsigned ctas, int *err)
+__device__ bool group_barrier (unsigned *bar, unsigned ctas, int *err, long long limit_ns)
 {
   __shared__ int ok;
   __syncthreads ();
@@ -131,7 +133,7 @@ __device__ bool group_barrier (unsigned *bar, unsigned ctas, int *err)
       const long long t0 = globaltimer ();
       while (*gen == g)
       {
-        if (*((volatile int *) err) != 0 || globaltimer () - t0 > kBarrierTimeoutNs)
+        if (*((volatile int *) err) != 0 || globaltimer () - t0 > limit_ns)
         {
           atomicExch (err, 1);
           break;
@@ -267,7 +269,7 @@ __device__ void forward_part (const Launch<R> &L, int cta, int ctas)
     for (int i = tid; i < N; i += stride)
       for (int q = 0; q < 6; ++q)
         L.F[q][i] = L.load[(size_t) q * N + i];
-    if (!group_barrier (bar, ctas, L.err))
+    if (!group_barrier (bar, ctas, L.err, L.limit_ns))
       return;
   }
   const bool accum = L.acc && cta == 0 && threadIdx.x == 0;
@@ -300,7 +302,7 @@ __device__ void forward_part (const Launch<R> &L, int cta, int ctas)
       if (dd)
         dd[i] = d;
     }
-    if (!group_barrier (bar, ctas, L.err))
+    if (!group_barrier (bar, ctas, L.err, L.limit_ns))
       return;
     // probe term of Ez_k, then the H half-step
     if (cta == 0 && (L.acc || kept))
@@ -328,7 +330,7 @@ __device__ void forward_part (const Launch<R> &L, int cta, int ctas)
           Hy[i] = p.src[2 * k + 1];
       }
     }
-    if (!group_barrier (bar, ctas, L.err))
+    if (!group_barrier (bar, ctas, L.err, L.limit_ns))
       return;
   }
   if (accum)
@@ -460,13 +462,13 @@ __device__ void reverse_part (const Launch<R> &L, int cta, int ctas)
     const size_t off = (size_t) (k - L.rk0);
     for (int t = tid; t < N; t += stride)
       adj_h_cell (L, t);
-    if (!group_barrier (bar, ctas, L.err))
+    if (!group_barrier (bar, ctas, L.err, L.limit_ns))
       return;
     const R *dedm = L.rdedm + off * N;
     const double *probe = L.rprobe + off * L.npr;
     for (int t = tid; t < N; t += stride)
       adj_e_cell (L, t, dedm, probe);
-    if (!group_barrier (bar, ctas, L.err))
+    if (!group_barrier (bar, ctas, L.err, L.limit_ns))
       return;
   }
 }
@@ -574,7 +576,7 @@ struct Arena
       cache->base = nullptr;
       cache->bytes = 0;
     }
-    if (cudaMalloc (&base, need) != cudaSuccess)
+    if (device_malloc ((void **) &base, need) != cudaSuccess)
       return false;
     if (cache)
     {
@@ -795,6 +797,7 @@ std::string run_t (const Geometry &g, const void *eps_dev, bool eps_is_double, c
   L.npr = npr;
   L.bar = bar;
   L.err = err;
+  L.limit_ns = run.wait_limit_ns > 0 ? run.wait_limit_ns : kDefaultBarrierLimitNs;
   for (int q = 0; q < 6; ++q)
     L.F[q] = state + (size_t) q * N;
 

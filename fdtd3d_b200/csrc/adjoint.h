@@ -36,6 +36,7 @@ struct AdjointRun
   int probe_hi[2] = {0, 0};    // exclusive
   bool fp64 = false;
   AdjointCache *cache = nullptr;   // null: allocate and free per run
+  long long wait_limit_ns = 0;     // time limit of one grid-barrier wait (<= 0: 2 s)
 };
 
 // eps_dev: per-cell permittivity on the device (float when eps_is_double is

@@ -357,6 +357,24 @@ int launch_convert_in (void *dst, int dst_kind, const double *src, size_t n, dou
   return 1;
 }
 
+namespace {
+
+// lowest index of a non-finite value (NaN or +-Inf) into *first
+__global__ void find_nonfinite_kernel (const double *src, size_t n, unsigned long long *first)
+{
+  for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
+    if (!isfinite (src[i]))
+      atomicMin (first, (unsigned long long) i);
+}
+
+}  // namespace
+
+int launch_find_nonfinite (const double *src, size_t n, unsigned long long *first, cudaStream_t s)
+{
+  find_nonfinite_kernel<<<grid_for (n, 148), 256, 0, s>>> (src, n, first);
+  return 1;
+}
+
 int launch_convert_out (double *dst, const void *src, int src_kind, size_t n, double scale, cudaStream_t s)
 {
   int blocks = grid_for (n, 148);

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -38,6 +39,10 @@ constexpr double kEta0 = 376.730313461770655;  // sqrt(mu0/eps0) for the referen
 constexpr int kSrcStride = 5;
 
 thread_local std::string g_last_error;
+
+// device / pinned allocations that still succeed before the injected
+// failures of fdtd_inject_alloc_failure (-1: no injection)
+std::atomic<long long> g_alloc_budget{-1};
 
 int kind_of (int prec)
 {
@@ -142,6 +147,8 @@ struct fdtd_ctx
   std::vector<double> h_dft_phase;
 
   double *staging = nullptr;
+  unsigned long long *d_first_bad = nullptr;   // index of a non-finite material value (check on upload)
+  long long wait_limit_ns = 0;                 // grid-barrier wait limit of the adjoint (<= 0: default)
   double *partials = nullptr;
   double *d_out = nullptr;
   int nparts = 0;
@@ -174,7 +181,7 @@ int fail (fdtd_ctx *ctx, int code, const std::string &msg)
 
 int dalloc (fdtd_ctx *ctx, void **p, size_t bytes, bool zero = true)
 {
-  cudaError_t e = cudaMalloc (p, bytes ? bytes : 16);
+  cudaError_t e = device_malloc (p, bytes ? bytes : 16);
   if (e != cudaSuccess)
   {
     *p = nullptr;
@@ -340,7 +347,7 @@ int ensure_src (fdtd_ctx *ctx, size_t steps)
     }
     size_t cap = std::max<size_t> (steps, 1024);
     DALLOC (ctx->d_src, cap * kSrcStride * sizeof (double));
-    CK (cudaMallocHost ((void **) &ctx->h_src, cap * kSrcStride * sizeof (double)));
+    CK (pinned_malloc ((void **) &ctx->h_src, cap * kSrcStride * sizeof (double)));
     ctx->src_cap = cap;
   }
   else
@@ -1317,17 +1324,24 @@ int fdtd_upload_material (fdtd_ctx *ctx, int which, const double *host)
   size_t n = (size_t) ctx->g.cells;
   if (ctx->g.dmp && which < 2)
     return upload_fine_material (ctx, which, host, cudaMemcpyHostToDevice);
-  if (ctx->kind == 0)
-  {
-    if (!ctx->mat64[which])
-      return fail (ctx, FDTD_ERR_UNSUPPORTED, "Drude grids need use_metamaterials");
-    CK (cudaMemcpyAsync (ctx->mat64[which], host, n * sizeof (double), cudaMemcpyHostToDevice, ctx->stream));
-    CK (cudaStreamSynchronize (ctx->stream));
-    return FDTD_OK;
-  }
+  if (ctx->kind == 0 && !ctx->mat64[which])
+    return fail (ctx, FDTD_ERR_UNSUPPORTED, "Drude grids need use_metamaterials");
+  // staged on the device and checked there: a NaN or an infinity is refused
+  // before anything the step reads changes
   if ((r = ensure_staging (ctx)) != FDTD_OK)
     return r;
+  if (!ctx->d_first_bad)
+    DALLOC (ctx->d_first_bad, sizeof (unsigned long long));
   CK (cudaMemcpyAsync (ctx->staging, host, n * sizeof (double), cudaMemcpyHostToDevice, ctx->stream));
+  CK (cudaMemsetAsync (ctx->d_first_bad, 0xff, sizeof (unsigned long long), ctx->stream));
+  ctx->launches += launch_find_nonfinite (ctx->staging, n, ctx->d_first_bad, ctx->stream);
+  unsigned long long first = 0;
+  CK (cudaMemcpyAsync (&first, ctx->d_first_bad, sizeof (first), cudaMemcpyDeviceToHost, ctx->stream));
+  CK (cudaStreamSynchronize (ctx->stream));
+  if (first < n)
+    return fail (ctx, FDTD_ERR_ARG, std::string ("material ") + std::to_string (which) +
+                                        " holds a non-finite value (cell " + std::to_string (first) +
+                                        "); nothing was uploaded");
   r = fdtd_upload_material_device (ctx, which, ctx->staging);
   if (r != FDTD_OK)
     return r;
@@ -1692,12 +1706,19 @@ int adjoint_entry (fdtd_ctx *ctx, const fdtd_adjoint_cfg *cfg, double *objective
     run.probe_hi[a] = cfg->probe_hi[a];
   }
   run.fp64 = cfg->precision == FDTD_PREC_FP64_PLAIN;
+  run.wait_limit_ns = ctx->wait_limit_ns;
   // eps as the context holds it: FP64 (plain form) or FP32 (null = uniform 1)
   const void *eps = ctx->kind == 0 ? (const void *) ctx->mat64[0] : (const void *) ctx->mat32[0];
   CK (cudaStreamSynchronize (ctx->stream));
   std::string why = adjoint_run (g, eps, ctx->kind == 0, run, objective, grad, ctx->sm_count, ctx->stream);
   if (!why.empty ())
-    return fail (ctx, why.find ("failed") != std::string::npos ? FDTD_ERR_CUDA : FDTD_ERR_ARG, why);
+    return fail (ctx,
+                 why.find ("timed out") != std::string::npos
+                     ? FDTD_ERR_DEVICE
+                     : (why.find ("allocation") != std::string::npos
+                            ? FDTD_ERR_NOMEM
+                            : (why.find ("failed") != std::string::npos ? FDTD_ERR_CUDA : FDTD_ERR_ARG)),
+                 why);
   return FDTD_OK;
 }
 
@@ -1833,9 +1854,9 @@ int fdtd_ntff (fdtd_ctx *re, fdtd_ctx *im, const int left[3], const int right[3]
           cudaFree (*q);
     }
   } release{{&phi_dev, &partial, &sums}};
-  CK (cudaMalloc ((void **) &phi_dev, (size_t) nphi * sizeof (double)));
-  CK (cudaMalloc ((void **) &partial, (size_t) nphi * blocks * 8 * sizeof (double)));
-  CK (cudaMalloc ((void **) &sums, (size_t) nphi * 8 * sizeof (double)));
+  CK (device_malloc ((void **) &phi_dev, (size_t) nphi * sizeof (double)));
+  CK (device_malloc ((void **) &partial, (size_t) nphi * blocks * 8 * sizeof (double)));
+  CK (device_malloc ((void **) &sums, (size_t) nphi * 8 * sizeof (double)));
   CK (cudaMemcpyAsync (phi_dev, phi, (size_t) nphi * sizeof (double), cudaMemcpyHostToDevice, re->stream));
   re->launches += launch_ntff (p, phi_dev, nphi, partial, blocks, sums, re->stream);
   CK (cudaGetLastError ());
@@ -1934,11 +1955,57 @@ const char *fdtd_last_error (void)
   return g_last_error.c_str ();
 }
 
+int fdtd_set_wait_limit (fdtd_ctx *ctx, int64_t limit_ns)
+{
+  if (!ctx)
+    return FDTD_ERR_ARG;
+  ctx->wait_limit_ns = limit_ns > 0 ? limit_ns : 0;
+  return FDTD_OK;
+}
+
+int fdtd_inject_alloc_failure (int64_t after)
+{
+  g_alloc_budget.store (after < 0 ? -1 : after);
+  return FDTD_OK;
+}
+
 }  // extern "C"
 
 void fdtdb::set_last_error (const char *msg)
 {
   g_last_error = msg ? msg : "";
+}
+
+namespace {
+
+bool injected_alloc_failure ()
+{
+  long long b = g_alloc_budget.load ();
+  while (b > 0 && !g_alloc_budget.compare_exchange_weak (b, b - 1))
+    ;
+  return b == 0;
+}
+
+}  // namespace
+
+cudaError_t fdtdb::device_malloc (void **p, size_t bytes)
+{
+  if (injected_alloc_failure ())
+  {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc (p, bytes);
+}
+
+cudaError_t fdtdb::pinned_malloc (void **p, size_t bytes)
+{
+  if (injected_alloc_failure ())
+  {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMallocHost (p, bytes);
 }
 
 extern "C" {

@@ -67,6 +67,8 @@ int launch_fast_point_source (void *f, int fp16, size_t index, const double *src
 int launch_convert_in (void *dst, int dst_kind, const double *src, size_t n, double scale, cudaStream_t s);
 int launch_convert_out (double *dst, const void *src, int src_kind, size_t n, double scale, cudaStream_t s);
 // kinds: 0 = double, 1 = float, 2 = __half
+// *first = min(*first, index of every NaN / Inf among src[0 .. n))
+int launch_find_nonfinite (const double *src, size_t n, unsigned long long *first, cudaStream_t s);
 
 // compensated FP64 reductions: out[0..parts) partial pairs (sum, compensation)
 // weight kinds: 0 = none, 1 = float, 2 = double
@@ -86,5 +88,11 @@ cudaError_t launch_reduce_final_checked (const double *partials, int nblocks, do
 
 // Sets the text fdtd_last_error() returns on the calling host thread.
 void set_last_error (const char *msg);
+
+// Every device and pinned host allocation of the library goes through these
+// two, so that fdtd_inject_alloc_failure can make them fail on the host as
+// an out-of-memory error would (cudaErrorMemoryAllocation, *p = null).
+cudaError_t device_malloc (void **p, size_t bytes);
+cudaError_t pinned_malloc (void **p, size_t bytes);
 
 }  // namespace fdtdb

@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "../../include/fdtd_b200.h"
+#include "kernels.h"
 #include "setup.h"
 
 namespace fdtdb {
@@ -323,6 +324,7 @@ struct fdtd_batch
   bool graph_ok = false;
   double last_ms = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  long long wait_limit_ns = 0;        // grid-barrier wait limit (<= 0: 5 s)
   std::string err;
   std::vector<void *> allocs;
 };
@@ -349,7 +351,7 @@ int bfail (fdtd_batch *b, int code, const std::string &m)
 
 int balloc (fdtd_batch *b, void **p, size_t bytes)
 {
-  cudaError_t e = cudaMalloc (p, bytes ? bytes : 16);
+  cudaError_t e = fdtdb::device_malloc (p, bytes ? bytes : 16);
   if (e != cudaSuccess)
     return bfail (b, FDTD_ERR_NOMEM, std::string ("cudaMalloc: ") + cudaGetErrorString (e));
   b->allocs.push_back (*p);
@@ -433,7 +435,7 @@ BatchParams params (fdtd_batch *b, uint32_t t_start, uint32_t n)
   p.counters = b->d_counters;
   p.generation = b->d_generation;
   p.err = b->d_err;
-  p.timeout_ns = 5000000000LL;
+  p.timeout_ns = b->wait_limit_ns > 0 ? b->wait_limit_ns : 5000000000LL;
   p.t_start = t_start;
   p.nsteps = n;
   p.cur = b->cur;
@@ -632,7 +634,7 @@ int ensure_src (fdtd_batch *b, size_t n)
   }
   size_t cap = std::max<size_t> (n, 1024);
   BALLOC (b->d_src, cap * sizeof (double));
-  BCK (cudaMallocHost ((void **) &b->h_src, cap * sizeof (double)));
+  BCK (fdtdb::pinned_malloc ((void **) &b->h_src, cap * sizeof (double)));
   b->src_cap = cap;
   drop_graph (b);
   return FDTD_OK;
@@ -907,6 +909,14 @@ void fdtd_batch_destroy (fdtd_batch *b)
   if (b->stream)
     cudaStreamDestroy (b->stream);
   delete b;
+}
+
+int fdtd_batch_set_wait_limit (fdtd_batch *b, int64_t limit_ns)
+{
+  if (!b)
+    return FDTD_ERR_ARG;
+  b->wait_limit_ns = limit_ns > 0 ? limit_ns : 0;
+  return FDTD_OK;
 }
 
 const char *fdtd_batch_last_error (const fdtd_batch *b)

@@ -157,7 +157,11 @@ int fdtd_create (const fdtd_config *cfg, int device, fdtd_ctx **out);
 /* Replaces the material half of InternalSchemeGPU::copyFromCPU/copyToGPU
  * (InternalScheme.specific.h:200-362) for Eps, Mu, OmegaPE, OmegaPM, GammaE,
  * GammaM.  `host` holds size-N doubles.  Unset grids keep the reference
- * defaults (eps = mu = 1, Drude terms 0). */
+ * defaults (eps = mu = 1, Drude terms 0).  The values are staged and checked
+ * on the device first: a NaN or an infinity returns FDTD_ERR_ARG (the
+ * message names the first such cell) and changes nothing.  (The
+ * asynchronous and device-pointer uploads below do not check: a non-finite
+ * value there propagates into the fields.) */
 int fdtd_upload_material (fdtd_ctx *ctx, int which, const double *host);
 
 /* Dump helpers of Scheme::saveGrids (Source/Scheme/Scheme.inc.h:4113-4530):
@@ -332,6 +336,14 @@ int fdtd_batch_download (fdtd_batch *b, int instance, int component, double *hos
  * milliseconds of the last launch (valid after fdtd_batch_sync) */
 int fdtd_batch_info (const fdtd_batch *b, int64_t *cells, int *graph_used, double *last_ms);
 const char *fdtd_batch_last_error (const fdtd_batch *b);
+/* Time limit of one wait at the batch kernel's grid barrier between steps
+ * (limit_ns <= 0 restores the default, 5 s).  A barrier that runs out sets
+ * the device error flag and every CTA leaves the launch; fdtd_batch_sync
+ * then returns FDTD_ERR_DEVICE and the batch's fields are left part-way
+ * through a step (destroy it).  No counterpart in the reference, whose
+ * kernels have no waits; it exits on any CUDA error
+ * (Source/Helpers/CudaInclude.h:41-47). */
+int fdtd_batch_set_wait_limit (fdtd_batch *b, int64_t limit_ns);
 void fdtd_batch_destroy (fdtd_batch *b);
 
 /* Compensated FP64 sum of weight[i] * src[i]^2 * scale over n elements,
@@ -355,6 +367,22 @@ void fdtd_batch_destroy (fdtd_batch *b);
  * is neither reported nor cleared.  No counterpart in the reference. */
 int fdtd_reduce_sq_noalloc (const void *src, int src_kind, size_t n, const void *weight, int weight_kind,
                             double scale, int blocks, double *out_dev, void *stream);
+
+/* Time limit of one wait at the grid barriers of the context's adjoint
+ * kernel (fdtd_objective / fdtd_backward); limit_ns <= 0 restores the
+ * default, 2 s.  A barrier that runs out sets the device error flag, every
+ * CTA leaves, and the call returns FDTD_ERR_DEVICE; the next call starts
+ * afresh.  (The TMA pipeline waits of the 3-D sweep keep their fixed 1 s
+ * limit.)  No counterpart in the reference (see above). */
+int fdtd_set_wait_limit (fdtd_ctx *ctx, int64_t limit_ns);
+
+/* Host-side fault injection: the next `after` device and pinned host
+ * allocations the library makes succeed and every later one fails as an
+ * out-of-memory error would, so the call that needs it returns
+ * FDTD_ERR_NOMEM and releases what it had taken; after < 0 turns the
+ * injection off.  Process-wide.  No counterpart in the reference (which
+ * exits on any CUDA error, Source/Helpers/CudaInclude.h:41-47). */
+int fdtd_inject_alloc_failure (int64_t after);
 
 const char *fdtd_status_str (int status);
 
