@@ -567,6 +567,11 @@ def main() -> None:
                             "hbm_frac": cells * bc * spl / (kms / max(kl, 1) * 1e-3) / 1e9 / peaks["hbm_gbs"]}
         if "plain_fp64" in extras:
             extras["speedup_vs_plain_fp64"] = value / world / extras["plain_fp64"]["value"]
+        # the reference's own CUDA FP64 path, measured on this GPU type by its
+        # GPU test (tests/test_gpu_reference_cuda.py; not run by the bench)
+        ref_cuda = os.path.join(ROOT, "profiles", "reference_cuda_fp64.json")
+        if os.path.exists(ref_cuda):
+            extras["reference_cuda_fp64"] = json.load(open(ref_cuda))
         for name, fn in (("adjoint_tmz", lambda: adjoint_extra(fd)), ("batch_tmz", lambda: batch_extra(fd)),
                          ("drude_slab", lambda: drude_extra(fd)),
                          ("precision", lambda: precision_extra(fd, n, args.precision_steps, args.precision_every,

@@ -27,6 +27,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 LIB_PATH = os.path.join(REF_DIR, "liboracle.so")
 REF_BIN = os.path.join(REF_DIR, "fdtd3d")
+# the reference built with its own CUDA path (oracle/Makefile target ref_cuda)
+REF_CUDA_BIN = os.path.join(os.path.dirname(REF_BIN), "fdtd3d_cuda")
 
 COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
 MATERIALS = ("eps", "mu", "omegape", "omegapm", "gammae", "gammam")
@@ -247,10 +249,14 @@ def reference_args(*, mode=3, size=(20, 20, 20), pml=None, tfsf_left=None, tfsf_
     return args
 
 
-def run_reference(materials=None, timeout=600, **kw):
-    """Run the reference CPU build; returns ({component: array}, total_seconds)."""
-    if not os.path.exists(REF_BIN):
-        raise FileNotFoundError(REF_BIN)
+def run_reference(materials=None, timeout=600, binary=None, extra_args=(), save=True, **kw):
+    """Run the reference (the CPU build, or `binary` with `extra_args`, e.g.
+    the CUDA build with --use-cuda); returns ({component: array}, the
+    reference's own 'Total time' of the step loop in seconds).  save=False
+    skips the field dumps (timing runs)."""
+    binary = binary or REF_BIN
+    if not os.path.exists(binary):
+        raise FileNotFoundError(binary)
     mode = kw.get("mode", 3)
     size = _plane(kw.get("size", (20, 20, 20)), mode, 1)
     shape = tuple(size[a] for a in mode_axes(mode))
@@ -266,9 +272,11 @@ def run_reference(materials=None, timeout=600, **kw):
         names = ("x", "y", "z")
         end = ",".join(f"{names[a]}:{size[a]}" for a in mode_axes(mode))
         start = ",".join(f"{names[a]}:0" for a in mode_axes(mode))
-        args += ["--save-res", "--save-as-txt", "--manual-save-coords",
-                 "--save-start-coord", start, "--save-end-coord", end]
-        r = subprocess.run([REF_BIN] + args, cwd=tmp, capture_output=True, text=True, timeout=timeout)
+        if save:
+            args += ["--save-res", "--save-as-txt", "--manual-save-coords",
+                     "--save-start-coord", start, "--save-end-coord", end]
+        args += list(extra_args)
+        r = subprocess.run([binary] + args, cwd=tmp, capture_output=True, text=True, timeout=timeout)
         if r.returncode != 0:
             raise RuntimeError(f"reference failed ({r.returncode}): {r.stdout[-2000:]} {r.stderr[-2000:]}")
         total = None
