@@ -8,6 +8,7 @@ Translation units and flags:
   csrc/fast_kernels.cu    nvcc                          FP32 / FP16-storage fused form, reductions
   csrc/fused3d.cu         nvcc                          3-D single-sweep E+H kernel (register-blocked)
   csrc/sweep3d.cu         nvcc                          3-D single-sweep E+H kernel (TMA-pipelined)
+  csrc/sweep2.cu          nvcc                          3-D two-step (temporally blocked) sweep
   csrc/fdtd_api.cu        nvcc                          C ABI, context, launch sequence
   csrc/cli.cpp            g++ -> fdtd3d-b200            command-line drop-in over the C ABI
 """
@@ -47,7 +48,7 @@ def _units():
     ]
     if os.path.exists(os.path.join(CSRC, "fused3d.cu")):
         units.append(("fused3d.cu", [nvcc] + common))
-    for extra in ("sweep3d.cu", "tmz_batch.cu", "adjoint.cu", "noalloc.cu", "ntff.cu"):
+    for extra in ("sweep3d.cu", "sweep2.cu", "tmz_batch.cu", "adjoint.cu", "noalloc.cu", "ntff.cu"):
         if os.path.exists(os.path.join(CSRC, extra)):
             units.append((extra, [nvcc] + common))
     return units

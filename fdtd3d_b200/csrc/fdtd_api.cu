@@ -24,6 +24,7 @@
 #include "../../include/fdtd_b200.h"
 #include "adjoint.h"
 #include "fused3d.h"
+#include "sweep2.h"
 #include "sweep3d.h"
 #include "kernels.h"
 #include "ntff.h"
@@ -130,6 +131,12 @@ struct fdtd_ctx
   unsigned long long *sweep_ctr = nullptr;
   std::string sweep_why;
   const char *step_kernel = "not_stepped";
+  // two-step (temporally blocked) sweep: used for pairs of steps when it can
+  // serve the geometry (tb2_state 1), planned with the single-step sweep
+  Sweep2Plan tb2;
+  int tb2_state = 0;
+  std::string tb2_why;
+  unsigned long long *tb2_ctr = nullptr;
   TfsfBand band;                          // TF/SF post pass of the sweep (band.cells > 0 when in use)
   std::vector<BandBox> band_host;         // its boxes, on the host
   // metamaterials with the sweep: the box of the Drude cells, fixed up after
@@ -843,6 +850,26 @@ int plan_sweep (fdtd_ctx *ctx)
     ctx->sweep_state = 1;
     ctx->sweep_eps = ctx->mat32[0];
   }
+  // the two-step sweep for pairs of steps (FDTDB_TB2=0 keeps single steps:
+  // a test hook)
+  ctx->tb2_state = -1;
+  ctx->tb2_why = "the single-step sweep is not in use";
+  if (ctx->sweep_state == 1)
+  {
+    bool tb2 = true;
+    if (const char *v = std::getenv ("FDTDB_TB2"))
+      tb2 = std::atoi (v) != 0;
+    if (!tb2)
+      ctx->tb2_why = "disabled by FDTDB_TB2=0";
+    else
+    {
+      if (!ctx->tb2_ctr)
+        DALLOC (ctx->tb2_ctr, 4 * sizeof (unsigned long long));
+      ctx->tb2_why = sweep2_plan (ctx->tb2, ctx->fused, e, h, ctx->mat32[0], ctx->sm_count, 64, ctx->tb2_ctr);
+      if (ctx->tb2_why.empty ())
+        ctx->tb2_state = 1;
+    }
+  }
   if (const char *v = std::getenv ("FDTDB_SWEEP_VERBOSE"))
     if (std::atoi (v) != 0)
     {
@@ -852,6 +879,10 @@ int plan_sweep (fdtd_ctx *ctx)
                     why.empty () ? "in use" : why.c_str (), ctx->sweep.wy, ctx->sweep.ctas, ctx->sweep.smem, w.nzt,
                     w.nyt, w.nch, w.chunk, w.nitems, ctx->sweep.items[0], ctx->sweep.items[1], ctx->sweep.items[2], ctx->sweep.items[3],
                     ctx->band.nbox, ctx->band.cells);
+      std::fprintf (stderr, "sweep2: %s ctas=%d smem=%u tiles z=%d y=%d chunks=%d items=%d lean/PML=%d/%d\n",
+                    ctx->tb2_state == 1 ? "in use" : ctx->tb2_why.c_str (), ctx->tb2.ctas, ctx->tb2.smem,
+                    ctx->tb2.work.nzt, ctx->tb2.work.nyt, ctx->tb2.work.nch, ctx->tb2.work.nitems,
+                    ctx->tb2.items[0], ctx->tb2.items[1]);
     }
   return FDTD_OK;
 }
@@ -1178,6 +1209,21 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
         if ((r = plan_sweep (ctx)) != FDTD_OK)
           return r;
       cudaEvent_t pe;
+      if (ctx->tb2_state == 1 && i + 1 < n && ctx->dft_comp < 0)
+      {
+        // steps t and t + 1 in one pass (no TF/SF, point source or Drude
+        // medium: the incident grid is not stepped)
+        if ((r = prof_begin (ctx, &pe)) != FDTD_OK)
+          return r;
+        ctx->launches += launch_sweep2 (ctx->tb2, o, f, ctx->d_err, s, ctx->sweep_streams);
+        ctx->step_kernel = "sweep2_tma";
+        if ((r = prof_end (ctx, pe)) != FDTD_OK)
+          return r;
+        ctx->fcur = nw;
+        select_fast_set (ctx);
+        ++i;
+        continue;
+      }
       if ((r = prof_begin (ctx, &pe)) != FDTD_OK)
         return r;
       if (ctx->sweep_state == 1)

@@ -1,0 +1,823 @@
+// sweep2.cu - two leapfrog time steps per pass over HBM (temporal blocking)
+// for the 3-D FP32 and FP16-storage forms.
+//
+// The single-step sweep (sweep3d.cu) reads every field once and writes it
+// once per step.  Here a CTA advances its tile by two steps in one sweep
+// along x, so the fields cross HBM once per two steps:
+//
+//  * A CTA holds 16 warps, warp w on row Y + w, lane l on the two z cells
+//    zs + 2l, zs + 2l + 1.  The tile's own cells are rows Y + 1 .. Y + 13 and
+//    z cells zs + 2 .. zs + 61; the rest is halo.  The first step is computed
+//    on the whole 16 x 64 tile, and each later half-step loses one row or
+//    column on the side its stencil reaches (H needs E at y + 1 / z + 1, E
+//    needs H at y - 1 / z - 1), so the second step is exact on the own cells
+//    and the halo costs recomputation, never communication.
+//  * Per plane x, one elected thread streams H(x) (with the y - 1 row and a
+//    16-byte z halo), E(x), eps(x) and eps(x + 1) of the old buffer set into
+//    shared memory with cp.async.bulk.tensor, three stages deep (bounded
+//    mbarrier waits).  Iteration x then computes E1(x), H1(x - 1) | barrier |
+//    E2(x - 1), H2(x - 2), where E1, H1 are the first step's values and E2,
+//    H2 the second's: one barrier per plane.  Neighbours along z come from
+//    warp shuffles, along y from shared exchange rows (double-buffered by
+//    plane parity) written one phase earlier, along x from registers carried
+//    over from the previous plane.  Only E2 and H2 of the own cells go to
+//    the new buffer set.
+//  * CTAs are persistent and take (z tile, y tile, x chunk) items from an
+//    atomic counter.
+// The arithmetic of each half-step is the one-sweep kernel's (the same
+// expressions in the same order), so two steps here equal two single steps.
+#include <cuda.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <vector>
+
+#include "sweep2.h"
+#include "tma.cuh"
+
+namespace fdtdb {
+
+namespace {
+
+constexpr int NW = kTb2Warps;   // warps = rows per CTA
+constexpr int ZW = kTb2Zw;      // z cells per warp row
+constexpr int NST2 = 3;         // pipeline stages
+
+template <typename T>
+struct L2
+{
+  // z tiling: tile k's warp rows start at zs = ZOWN k - ZOFF (a multiple of
+  // one 16-byte unit, as TMA requires) and own the cells
+  // zs + 2 OLO .. zs + 2 OHI + 1 (lanes OLO .. OHI)
+  static constexpr int ZOWN = sizeof (T) == 4 ? 60 : 56;
+  static constexpr int ZOFF = sizeof (T) == 4 ? 4 : 8;
+  static constexpr int OLO = sizeof (T) == 4 ? 1 : 2;
+  static constexpr int OHI = OLO + ZOWN / 2 - 1;
+  static constexpr int HZ = 16 / (int) sizeof (T);   // z halo: one 16-byte unit
+  static constexpr int HW = ZW + HZ;                 // H row: zs - HZ .. zs + 63
+  static constexpr int HR = NW + 1;                  // H rows: Y - 1 .. Y + 15
+  static constexpr int EW = ZW;                      // E row: zs .. zs + 63
+  static constexpr int ER = NW;                      // E rows: Y .. Y + 15
+  static constexpr int PW = ZW + 4;                  // eps row (float): zs .. zs + 67
+  static constexpr int PR = NW + 1;                  // eps rows: Y .. Y + 16
+  static constexpr unsigned rnd (unsigned b) { return (b + 127u) / 128u * 128u; }
+  static constexpr unsigned H_B = rnd (sizeof (T) * HW * HR);
+  static constexpr unsigned E_B = rnd (sizeof (T) * EW * ER);
+  static constexpr unsigned P_B = rnd (4u * PW * PR);
+  static constexpr unsigned OFF_E = 3 * H_B;
+  static constexpr unsigned OFF_P = OFF_E + 3 * E_B;
+  static constexpr unsigned STAGE = OFF_P + 2 * P_B;
+  // exchange rows, NW x ZW floats each: XE1[parity][Ex, Ez],
+  // XH1[parity][Hx, Hz], XE2[parity][Ex, Ez]
+  static constexpr int XN = NW * ZW;
+  static constexpr unsigned OFF_X = NST2 * STAGE;
+  // PML coefficient pairs of the item (PML class): per component k and pair
+  // element e, along z [(2k + e) ZW + column], y [(2k + e) NW + row],
+  // x [(2k + e) XTW + plane - (xa - 2)]
+  static constexpr int XTW = kTb2MaxChunk + 4;
+  static constexpr int TY0 = 12 * ZW;
+  static constexpr int TX0 = TY0 + 12 * NW;
+  static constexpr unsigned OFF_T = OFF_X + 12u * 4u * XN;
+  static constexpr unsigned OFF_BAR = OFF_T + rnd (4u * (TX0 + 12 * XTW));
+  static constexpr unsigned TOTAL = OFF_BAR + 64 + 128;   // + room to align the base to 128 bytes
+  // bytes each stage's copies deliver (full boxes, fill included)
+  static constexpr unsigned TX_HE = 3u * sizeof (T) * HW * HR + 3u * sizeof (T) * EW * ER;
+  static constexpr unsigned TX_P = 2u * 4u * PW * PR;
+};
+
+template <typename T>
+struct V2;
+
+template <>
+struct V2<float>
+{
+  static __device__ __forceinline__ void ld (const float *s, float v[2])
+  {
+    const float2 t = *reinterpret_cast<const float2 *> (s);
+    v[0] = t.x;
+    v[1] = t.y;
+  }
+  static __device__ __forceinline__ float ld1 (const float *s) { return *s; }
+  static __device__ __forceinline__ void st (float *g, const float v[2])
+  {
+    __stcs (reinterpret_cast<float2 *> (g), make_float2 (v[0], v[1]));
+  }
+};
+
+template <>
+struct V2<__half>
+{
+  static __device__ __forceinline__ void ld (const __half *s, float v[2])
+  {
+    const float2 t = __half22float2 (*reinterpret_cast<const __half2 *> (s));
+    v[0] = t.x;
+    v[1] = t.y;
+  }
+  static __device__ __forceinline__ float ld1 (const __half *s) { return __half2float (*s); }
+  static __device__ __forceinline__ void st (__half *g, const float v[2])
+  {
+    const __half2 h = __floats2half2_rn (v[0], v[1]);
+    __stcs (reinterpret_cast<unsigned *> (g), *reinterpret_cast<const unsigned *> (&h));
+  }
+};
+
+__device__ __forceinline__ void lds2 (const float *s, float v[2])
+{
+  V2<float>::ld (s, v);
+}
+
+__device__ __forceinline__ void sts2 (float *s, const float v[2])
+{
+  *reinterpret_cast<float2 *> (s) = make_float2 (v[0], v[1]);
+}
+
+// ------------------------------------------------------------------ kernel
+
+// Pair (0: ca1, sq1; 1: p5, q5; 2: g4p, g4m) of component k that runs along
+// an axis.
+__device__ __forceinline__ int pair_along (int k, int axis)
+{
+  return (k + 1) % 3 == axis ? 0 : ((k + 2) % 3 == axis ? 1 : 2);
+}
+
+// Axis along which coefficient pair q (0: ca1, sq1; 1: p5, q5; 2: g4p, g4m)
+// of component k runs: the reference's sigma choice per component
+// (InternalScheme.inc.h:2551-2640), as the single-step kernels stage it.
+__device__ __forceinline__ int pair_axis (int k, int q)
+{
+  const int a = k % 3;
+  return q == 0 ? (a + 1) % 3 : (q == 1 ? (a + 2) % 3 : a);
+}
+
+// Element e of coefficient pair q of component k at (plane index xi, row w,
+// column zcol) from the item's staged tables.
+template <int XTW>
+__device__ __forceinline__ float pml_coef (const float *T, int k, int q, int e, int xi, int w, int zcol)
+{
+  const int a = pair_axis (k, q);
+  return a == 0 ? T[12 * ZW + 12 * NW + (2 * k + e) * XTW + xi]
+                : (a == 1 ? T[12 * ZW + (2 * k + e) * NW + w] : T[(2 * k + e) * ZW + zcol]);
+}
+
+// PML update of component k on one cell (the single-step kernels' pml_vec):
+//   X_new = ca1 X + sq1 curl,  F_new = p5 F + (g4p X_new - g4m X) q5 im.
+// Returns F_new; xn gets X_new.
+template <int XTW>
+__device__ __forceinline__ float pml_cell (const float *T, int k, int xi, int w, int zcol, float xo, float cu,
+                                           float im, float fo, float &xn)
+{
+  const float ca1 = pml_coef<XTW> (T, k, 0, 0, xi, w, zcol), sq1 = pml_coef<XTW> (T, k, 0, 1, xi, w, zcol);
+  const float p5 = pml_coef<XTW> (T, k, 1, 0, xi, w, zcol), q5 = pml_coef<XTW> (T, k, 1, 1, xi, w, zcol);
+  const float g4p = pml_coef<XTW> (T, k, 2, 0, xi, w, zcol), g4m = pml_coef<XTW> (T, k, 2, 1, xi, w, zcol);
+  const float n = ca1 * xo + sq1 * cu;
+  xn = n;
+  return p5 * fo + (g4p * n - g4m * xo) * q5 * im;
+}
+
+// MODE 0 (lean): no cell of the item's extended region is a PML cell of any
+// component.  MODE 1 (PML): PML cells anywhere; each lane updates the cells
+// that are PML cells of a component with the PML form (masks per component
+// and cell, coefficients from the 1-D tables), carries the auxiliary of the
+// first step in registers to the second, and loads the old auxiliaries one
+// plane ahead with plain loads (only lanes with PML cells).
+template <typename T, int MODE>
+__global__ void __launch_bounds__ (32 * NW, 1)
+    sweep2_kernel (const __grid_constant__ Sweep2Maps maps, const __grid_constant__ FusedParams p,
+                   const Sweep2Work wk, int *err)
+{
+  using L = L2<T>;
+  constexpr int HZ = L::HZ, HW = L::HW, EW = L::EW, PW = L::PW, XN = L::XN;
+  constexpr int HS = L::H_B / sizeof (T), ES = L::E_B / sizeof (T), PS = L::P_B / sizeof (float);
+  constexpr unsigned kLanes = 0xffffffffu;
+  constexpr bool kPml = MODE == 1;
+  extern __shared__ __align__ (128) unsigned char smem_raw[];
+  __shared__ int s_item;
+  __shared__ int s_abort;
+
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const bool leader = w == 0 && lane == 0;
+  const int nx = p.g.n[0], ny = p.g.n[1], nz = p.g.n[2];
+  const size_t sx = (size_t) ny * nz;
+  const uint32_t raw = tma::smem_addr (smem_raw);
+  const uint32_t sbase = (raw + 127u) & ~127u;
+  unsigned char *const smem = smem_raw + (sbase - raw);
+  const uint32_t bar = sbase + L::OFF_BAR;
+  const bool has_eps = p.eps != nullptr;
+  const float S = p.courant;
+  float *const X = reinterpret_cast<float *> (smem + L::OFF_X);
+  float *const Tab = reinterpret_cast<float *> (smem + L::OFF_T);
+  constexpr int XTW = L::XTW;
+
+  if (leader)
+  {
+#pragma unroll
+    for (int st = 0; st < NST2; ++st)
+      tma::mbar_init (bar + 8 * st, 1);
+    asm volatile ("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_abort = 0;
+  }
+  __syncthreads ();
+
+  // stage st <- plane x of the tile at (zs, Y)
+  auto issue = [&] (int st, int x, int zs, int Y) {
+    const uint32_t s = sbase + st * L::STAGE;
+    const uint32_t b = bar + 8 * st;
+    tma::mbar_expect_tx (b, L::TX_HE + (has_eps ? L::TX_P : 0u));
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      tma::load_3d (s + c * L::H_B, &maps.h[c], zs - HZ, Y - 1, x, b);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      tma::load_3d (s + L::OFF_E + c * L::E_B, &maps.e[c], zs, Y, x, b);
+    if (has_eps)
+    {
+      tma::load_3d (s + L::OFF_P, &maps.eps, zs, Y, x, b);
+      tma::load_3d (s + L::OFF_P + L::P_B, &maps.eps, zs, Y, x + 1, b);
+    }
+  };
+
+  unsigned phase = 0;   // bit s: parity of the next completion of stage s
+  bool aborted = false;
+  for (;;)
+  {
+    __syncthreads ();   // every thread has read the previous item's index
+    if (leader)
+      s_item = (int) atomicAdd (wk.ctr + 2 * MODE, 1ull);
+    __syncthreads ();
+    const int item = s_item;
+    if (item >= wk.nitems)
+      break;
+    if (sweep2_item_class (p, wk, item) != MODE)
+      continue;
+    const int zt = item % wk.nzt;
+    const int yt = (item / wk.nzt) % wk.nyt;
+    const int ch = item / (wk.nzt * wk.nyt);
+    const int zs = L::ZOWN * zt - L::ZOFF;   // first z cell of the warp rows
+    const int Y = kTb2Yown * yt;             // row of warp 0
+    const int xa = wk.xcut[ch];
+    const int xb = wk.xcut[ch + 1] - 1;
+    const int np = xb - xa + 5;              // planes xa - 2 .. xb + 2
+
+    if (leader)
+    {
+#pragma unroll
+      for (int k = 0; k < NST2; ++k)
+        issue (k, xa - 2 + k, zs, Y);
+    }
+    if constexpr (kPml)
+    {
+      // the item's PML coefficient pairs (read after the first plane's
+      // barrier; coordinates outside the grid take the edge value, which no
+      // updated cell reads)
+      const int tid = w * 32 + lane;
+      for (int q = tid; q < 12 * ZW; q += 32 * NW)
+      {
+        const int k = q / (2 * ZW), e = (q / ZW) % 2, col = q % ZW;
+        const int z = min (max (zs + col, 0), nz - 1);
+        Tab[q] = __ldg (p.tab[k][2 * pair_along (k, 2) + e] + z);
+      }
+      for (int q = tid; q < 12 * NW; q += 32 * NW)
+      {
+        const int k = q / (2 * NW), e = (q / NW) % 2, row = min (max (Y + q % NW, 0), ny - 1);
+        Tab[12 * ZW + q] = __ldg (p.tab[k][2 * pair_along (k, 1) + e] + row);
+      }
+      for (int q = tid; q < 12 * XTW; q += 32 * NW)
+      {
+        const int k = q / (2 * XTW), e = (q / XTW) % 2, xx = min (max (xa - 2 + q % XTW, 0), nx - 1);
+        Tab[12 * ZW + 12 * NW + q] = __ldg (p.tab[k][2 * pair_along (k, 0) + e] + xx);
+      }
+    }
+
+    // ---- per-lane constants of this item
+    const int r = Y + w;
+    const int zl = 2 * lane;
+    const int zc = zs + zl;
+    unsigned cupd = 0;   // bit j: cell zc + j of this row is updated (on an updated plane)
+    if (r >= 1 && r <= ny - 2)
+    {
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+        if (zc + j >= 1 && zc + j <= nz - 2)
+          cupd |= 1u << j;
+    }
+    const bool own = w >= 1 && w <= kTb2Yown && r <= ny - 2 && lane >= L::OLO && lane <= L::OHI && zc >= 0 && zc < nz;
+    const size_t rowoff = (size_t) r * nz + zc;
+    // PML cells of the family (E: kb = 0, H: kb = 3) among this lane's
+    // updated cells on plane xx: bit 2c + j for component kb + c, cell j
+    auto pmask = [&] (int kb, int xx) -> unsigned {
+      const unsigned u = (xx >= 1 && xx <= nx - 2) ? cupd : 0u;
+      if (!kPml || !u)
+        return 0u;
+      unsigned m = 0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+      {
+        const int k = kb + c;
+        const bool xy = xx >= p.ilo[k][0] && xx < p.ihi[k][0] && r >= p.ilo[k][1] && r < p.ihi[k][1];
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+          if (!(xy && zc + j >= p.ilo[k][2] && zc + j < p.ihi[k][2]))
+            m |= 1u << (2 * c + j);
+      }
+      return m & (u * 0x15u);   // the update mask of each component's two bits
+    };
+    // masks of the planes in flight: E1 (x), H1 (x - 1), E2 (x - 1), H2 (x - 2)
+    unsigned mE1 = 0, mH1 = 0, mE2 = 0, mH2 = 0;
+    (void) mE2;
+    (void) mH2;
+
+    float hp[3][2] = {};    // H0(x - 1)
+    float e1p[3][2] = {};   // E1(x - 1)
+    float ip[3][2] = {};    // 2 / (eps + eps') of E at x - 1
+    float h1p[3][2] = {};   // H1(x - 2)
+    float e2p[3][2] = {};   // E2(x - 2)
+    // PML: old auxiliaries loaded one plane ahead (E at x, H at x - 1), and
+    // the first step's auxiliaries carried to the second
+    float axe[3][2] = {}, axh[3][2] = {}, xe1p[3][2] = {}, xh1p[3][2] = {};
+    (void) axe;
+    (void) axh;
+    (void) xe1p;
+    (void) xh1p;
+
+    for (int i = 0; i < np; ++i)
+    {
+      const int st = i % NST2;
+      const int x = xa - 2 + i;
+      if (!tma::mbar_wait (bar + 8 * st, (phase >> st) & 1u))
+      {
+        s_abort = 1;
+        atomicOr (err, 4);
+      }
+      phase ^= 1u << st;
+      const unsigned char *stg = smem + st * L::STAGE;
+      const T *sH = reinterpret_cast<const T *> (stg);
+      const T *sE = reinterpret_cast<const T *> (stg + L::OFF_E);
+      const float *sP = reinterpret_cast<const float *> (stg + L::OFF_P);
+      // exchange rows by plane parity: this plane's (written) and the
+      // previous plane's (read).  Every set is rewritten two planes after it
+      // was written, and the one barrier per plane lies between its readers
+      // and that rewrite.
+      float *XE1w = X + (i & 1) * 2 * XN;
+      const float *XE1r = X + ((i + 1) & 1) * 2 * XN;
+      float *XH1 = X + (4 + (i & 1) * 2) * XN;
+      float *XE2w = X + (8 + (i & 1) * 2) * XN;
+      const float *XE2r = X + (8 + ((i + 1) & 1) * 2) * XN;
+
+      // H0(x) on this row
+      float hc[3][2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        V2<T>::ld (sH + c * HS + (w + 1) * HW + HZ + zl, hc[c]);
+
+      // ================= phase 1: E1(x) on every row, H1(x - 1) on rows 0 .. 14
+      float e1[3][2] = {}, im[3][2] = {}, xe1[3][2] = {};
+      (void) xe1;
+      if (i >= 1)
+      {
+        const unsigned u = (x >= 1 && x <= nx - 2) ? cupd : 0u;
+        float hzm[2], hxm[2], eo[3][2];
+        V2<T>::ld (sH + 2 * HS + w * HW + HZ + zl, hzm);
+        V2<T>::ld (sH + 0 * HS + w * HW + HZ + zl, hxm);
+        const float hym1 = V2<T>::ld1 (sH + 1 * HS + (w + 1) * HW + HZ + zl - 1);
+        const float hxm1 = V2<T>::ld1 (sH + 0 * HS + (w + 1) * HW + HZ + zl - 1);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          V2<T>::ld (sE + c * ES + w * EW + zl, eo[c]);
+        if (has_eps)
+        {
+          float p0[2], px[2], py[2];
+          lds2 (sP + w * PW + zl, p0);
+          lds2 (sP + PS + w * PW + zl, px);
+          lds2 (sP + (w + 1) * PW + zl, py);
+          const float pz = sP[w * PW + zl + 2];
+#pragma unroll
+          for (int j = 0; j < 2; ++j)
+          {
+            im[0][j] = __fdividef (2.f, p0[j] + px[j]);
+            im[1][j] = __fdividef (2.f, p0[j] + py[j]);
+            im[2][j] = __fdividef (2.f, p0[j] + (j == 0 ? p0[1] : pz));
+          }
+        }
+        else
+        {
+#pragma unroll
+          for (int j = 0; j < 2; ++j)
+            im[0][j] = im[1][j] = im[2][j] = 1.f;
+        }
+        float cu[3][2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+        {
+          const float hyl = j ? hc[1][0] : hym1;
+          const float hxl = j ? hc[0][0] : hxm1;
+          cu[0][j] = (hc[2][j] - hzm[j]) - (hc[1][j] - hyl);
+          cu[1][j] = (hc[0][j] - hxl) - (hc[2][j] - hp[2][j]);
+          cu[2][j] = (hc[1][j] - hp[1][j]) - (hc[0][j] - hxm[j]);
+          const bool up = (u >> j) & 1u;
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            e1[c][j] = up ? eo[c][j] + (S * im[c][j]) * cu[c][j] : eo[c][j];
+        }
+        if constexpr (kPml)
+        {
+          if (mE1)
+          {
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+              for (int j = 0; j < 2; ++j)
+                if ((mE1 >> (2 * c + j)) & 1u)
+                  e1[c][j] = pml_cell<XTW> (Tab, c, i, w, zl + j, axe[c][j], cu[c][j], im[c][j], eo[c][j], xe1[c][j]);
+          }
+        }
+        sts2 (XE1w + 0 * XN + w * ZW + zl, e1[0]);
+        sts2 (XE1w + 1 * XN + w * ZW + zl, e1[2]);
+      }
+      float h1[3][2] = {}, xh1[3][2] = {};
+      (void) xh1;
+      if (i >= 2 && w < NW - 1)
+      {
+        // H1(x - 1): E1(x - 1) in e1p, its y + 1 row from the previous
+        // plane's exchange rows, its z + 1 cell from the next lane
+        const int xh = x - 1;
+        const unsigned u = (xh >= 1 && xh <= nx - 2) ? cupd : 0u;
+        const float exn = __shfl_down_sync (kLanes, e1p[0][0], 1);
+        const float eyn = __shfl_down_sync (kLanes, e1p[1][0], 1);
+        float exy[2], ezy[2];
+        lds2 (XE1r + 0 * XN + (w + 1) * ZW + zl, exy);
+        lds2 (XE1r + 1 * XN + (w + 1) * ZW + zl, ezy);
+        float a[3][2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+        {
+          const float eyz = j ? eyn : e1p[1][1];
+          const float exz = j ? exn : e1p[0][1];
+          a[0][j] = (eyz - e1p[1][j]) - (ezy[j] - e1p[2][j]);
+          a[1][j] = (e1[2][j] - e1p[2][j]) - (exz - e1p[0][j]);
+          a[2][j] = (exy[j] - e1p[0][j]) - (e1[1][j] - e1p[1][j]);
+          const bool up = (u >> j) & 1u;
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            h1[c][j] = up ? hp[c][j] + S * a[c][j] : hp[c][j];
+        }
+        if constexpr (kPml)
+        {
+          if (mH1)
+          {
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+              for (int j = 0; j < 2; ++j)
+                if ((mH1 >> (2 * c + j)) & 1u)
+                  h1[c][j] = pml_cell<XTW> (Tab, 3 + c, i - 1, w, zl + j, axh[c][j], a[c][j], 1.f, hp[c][j], xh1[c][j]);
+          }
+        }
+        sts2 (XH1 + 0 * XN + w * ZW + zl, h1[0]);
+        sts2 (XH1 + 1 * XN + w * ZW + zl, h1[2]);
+      }
+
+      __syncthreads ();   // E1 / H1 rows visible, stage st read
+      if (s_abort)
+      {
+        // wait (bounded) for the copies still in flight into the other stages
+        aborted = true;
+        if (leader)
+          for (int k = 1; k < NST2 && i + k < np; ++k)
+          {
+            const int so = (st + k) % NST2;
+            tma::mbar_wait (bar + 8 * so, (phase >> so) & 1u);
+          }
+        break;
+      }
+      if (leader && i + NST2 < np)
+        issue (st, x + NST2, zs, Y);
+
+      // ================= phase 2: E2(x - 1) on rows 1 .. 14, H2(x - 2) on rows 1 .. 13
+      float e2[3][2] = {};
+      if (i >= 3 && w >= 1 && w < NW - 1)
+      {
+        const int xe = x - 1;
+        const unsigned u = (xe >= 1 && xe <= nx - 2) ? cupd : 0u;
+        const float hyl = __shfl_up_sync (kLanes, h1[1][1], 1);
+        const float hxl = __shfl_up_sync (kLanes, h1[0][1], 1);
+        float hzm[2], hxm[2];
+        lds2 (XH1 + 1 * XN + (w - 1) * ZW + zl, hzm);
+        lds2 (XH1 + 0 * XN + (w - 1) * ZW + zl, hxm);
+        float cu[3][2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+        {
+          const float hyz = j ? h1[1][0] : hyl;
+          const float hxz = j ? h1[0][0] : hxl;
+          cu[0][j] = (h1[2][j] - hzm[j]) - (h1[1][j] - hyz);
+          cu[1][j] = (h1[0][j] - hxz) - (h1[2][j] - h1p[2][j]);
+          cu[2][j] = (h1[1][j] - h1p[1][j]) - (h1[0][j] - hxm[j]);
+          const bool up = (u >> j) & 1u;
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            e2[c][j] = up ? e1p[c][j] + (S * ip[c][j]) * cu[c][j] : e1p[c][j];
+        }
+        const bool store = own && xe >= xa && xe <= xb;
+        const size_t id = (size_t) xe * sx + rowoff;
+        if constexpr (kPml)
+        {
+          if (mE2)
+          {
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+            {
+              float xn[2] = {0.f, 0.f};
+#pragma unroll
+              for (int j = 0; j < 2; ++j)
+                if ((mE2 >> (2 * c + j)) & 1u)
+                  e2[c][j] = pml_cell<XTW> (Tab, c, i - 1, w, zl + j, xe1p[c][j], cu[c][j], ip[c][j], e1p[c][j], xn[j]);
+              if (store)
+              {
+#pragma unroll
+                for (int j = 0; j < 2; ++j)
+                  if ((mE2 >> (2 * c + j)) & 1u)
+                    __stcs (p.aux_new[c] + id + j, xn[j]);
+              }
+            }
+          }
+        }
+        if (store)
+        {
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            V2<T>::st (reinterpret_cast<T *> (p.e_new[c]) + id, e2[c]);
+        }
+        sts2 (XE2w + 0 * XN + w * ZW + zl, e2[0]);
+        sts2 (XE2w + 1 * XN + w * ZW + zl, e2[2]);
+      }
+      if (i >= 4 && w >= 1 && w <= kTb2Yown)
+      {
+        const int xh = x - 2;
+        const unsigned u = (xh >= 1 && xh <= nx - 2) ? cupd : 0u;
+        const float exn = __shfl_down_sync (kLanes, e2p[0][0], 1);
+        const float eyn = __shfl_down_sync (kLanes, e2p[1][0], 1);
+        float exy[2], ezy[2];
+        lds2 (XE2r + 0 * XN + (w + 1) * ZW + zl, exy);
+        lds2 (XE2r + 1 * XN + (w + 1) * ZW + zl, ezy);
+        float h2[3][2], a[3][2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+        {
+          const float eyz = j ? eyn : e2p[1][1];
+          const float exz = j ? exn : e2p[0][1];
+          a[0][j] = (eyz - e2p[1][j]) - (ezy[j] - e2p[2][j]);
+          a[1][j] = (e2[2][j] - e2p[2][j]) - (exz - e2p[0][j]);
+          a[2][j] = (exy[j] - e2p[0][j]) - (e2[1][j] - e2p[1][j]);
+          const bool up = (u >> j) & 1u;
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            h2[c][j] = up ? h1p[c][j] + S * a[c][j] : h1p[c][j];
+        }
+        const bool store = own && xh >= xa && xh <= xb;
+        const size_t id = (size_t) xh * sx + rowoff;
+        if constexpr (kPml)
+        {
+          if (mH2)
+          {
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+            {
+              float xn[2] = {0.f, 0.f};
+#pragma unroll
+              for (int j = 0; j < 2; ++j)
+                if ((mH2 >> (2 * c + j)) & 1u)
+                  h2[c][j] = pml_cell<XTW> (Tab, 3 + c, i - 2, w, zl + j, xh1p[c][j], a[c][j], 1.f, h1p[c][j], xn[j]);
+              if (store)
+              {
+#pragma unroll
+                for (int j = 0; j < 2; ++j)
+                  if ((mH2 >> (2 * c + j)) & 1u)
+                    __stcs (p.aux_new[3 + c] + id + j, xn[j]);
+              }
+            }
+          }
+        }
+        if (store)
+        {
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            V2<T>::st (reinterpret_cast<T *> (p.h_new[c]) + id, h2[c]);
+        }
+      }
+
+      if constexpr (kPml)
+      {
+        // masks and old auxiliaries of the next plane's first step: E at
+        // x + 1, H at x
+        mE2 = mE1;
+        mH2 = mH1;
+        mE1 = pmask (0, x + 1);
+        mH1 = pmask (3, x);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+        {
+          if ((mE1 >> (2 * c)) & 3u)
+          {
+            const float2 v = __ldg (reinterpret_cast<const float2 *> (p.aux_old[c] + (size_t) (x + 1) * sx + rowoff));
+            axe[c][0] = v.x;
+            axe[c][1] = v.y;
+          }
+          if ((mH1 >> (2 * c)) & 3u)
+          {
+            const float2 v = __ldg (reinterpret_cast<const float2 *> (p.aux_old[3 + c] + (size_t) x * sx + rowoff));
+            axh[c][0] = v.x;
+            axh[c][1] = v.y;
+          }
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+        {
+          hp[c][j] = hc[c][j];
+          e1p[c][j] = e1[c][j];
+          ip[c][j] = im[c][j];
+          h1p[c][j] = h1[c][j];
+          e2p[c][j] = e2[c][j];
+          if constexpr (kPml)
+          {
+            xe1p[c][j] = xe1[c][j];
+            xh1p[c][j] = xh1[c][j];
+          }
+        }
+    }
+    if (aborted)
+      break;
+  }
+
+  if (leader)
+  {
+    __threadfence ();
+    const unsigned long long done = atomicAdd (wk.ctr + 2 * MODE + 1, 1ull);
+    if (done == gridDim.x - 1)
+    {
+      atomicExch (wk.ctr + 2 * MODE, 0ull);
+      atomicExch (wk.ctr + 2 * MODE + 1, 0ull);
+    }
+  }
+}
+
+template <typename T>
+std::string plan_t (Sweep2Plan &pl, const FusedParams &p, void *const e[2][3], void *const h[2][3], const float *eps,
+                    int sm_count)
+{
+  using L = L2<T>;
+  const bool half = sizeof (T) == 2;
+  for (int b = 0; b < 2; ++b)
+  {
+    Sweep2Maps &m = pl.maps[b];
+    for (int c = 0; c < 3; ++c)
+      if (!make_map (m.h[c], h[b][c], half, p.g.n, L::HW, L::HR) ||
+          !make_map (m.e[c], e[b][c], half, p.g.n, L::EW, L::ER))
+        return "tensor map encoding failed";
+    if (eps)
+    {
+      if (!make_map (m.eps, eps, false, p.g.n, L::PW, L::PR))
+        return "tensor map encoding failed";
+    }
+    else
+      m.eps = m.e[0];   // never used
+  }
+  int per_sm = 0;
+  for (int mode = 0; mode < 2; ++mode)
+  {
+    auto kern = mode == 0 ? sweep2_kernel<T, 0> : sweep2_kernel<T, 1>;
+    if (cudaFuncSetAttribute (kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) L::TOTAL) != cudaSuccess)
+    {
+      cudaGetLastError ();
+      return "shared memory request refused";
+    }
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor (&n, kern, 32 * NW, L::TOTAL) != cudaSuccess || n < 1)
+    {
+      cudaGetLastError ();
+      return "kernel does not fit on an SM";
+    }
+    per_sm = mode ? std::min (per_sm, n) : n;
+  }
+  pl.smem = L::TOTAL;
+  pl.ctas = sm_count * per_sm;
+  pl.work.zown = L::ZOWN;
+  pl.work.zoff = L::ZOFF;
+  pl.work.nzt = 1;
+  // tiles until the last one's own cells reach z = nz - 2
+  const int zrel = 2 * L::OHI + 2 - L::ZOFF;
+  while (L::ZOWN * (pl.work.nzt - 1) + zrel < p.g.n[2] - 1)
+    ++pl.work.nzt;
+  return "";
+}
+
+template <typename T>
+int launch_t (const Sweep2Plan &pl, int set, const FusedParams &p, int *err, cudaStream_t s, const SweepStreams &ss)
+{
+  const dim3 block (32, NW);
+  constexpr unsigned sm = L2<T>::TOTAL;
+  const bool conc = ss.side[0] && pl.items[0] > 0 && pl.items[1] > 0;
+  cudaStream_t s0 = s;
+  if (conc)
+  {
+    cudaEventRecord (ss.fork, s);
+    cudaStreamWaitEvent (ss.side[0], ss.fork, 0);
+    s0 = ss.side[0];
+  }
+  int n = 0;
+  if (pl.items[1] > 0)
+  {
+    sweep2_kernel<T, 1><<<pl.ctas, block, sm, s>>> (pl.maps[set], p, pl.work, err);
+    ++n;
+  }
+  if (pl.items[0] > 0)
+  {
+    sweep2_kernel<T, 0><<<pl.ctas, block, sm, s0>>> (pl.maps[set], p, pl.work, err);
+    ++n;
+  }
+  if (conc)
+  {
+    cudaEventRecord (ss.join[0], s0);
+    cudaStreamWaitEvent (s, ss.join[0], 0);
+  }
+  return n;
+}
+
+}  // namespace
+
+std::string sweep2_plan (Sweep2Plan &plan, const FusedParams &p, void *const e[2][3], void *const h[2][3],
+                         const float *eps, int sm_count, int chunk, unsigned long long *ctr)
+{
+  const int *n = p.g.n;
+  chunk = std::min (std::max (chunk, 1), kTb2MaxChunk);
+  if (p.g.drop != 0)
+    return "2-D grid";
+  if (p.use_tfsf)
+    return "TF/SF corrections";
+  if (p.ps_mask)
+    return "point source";
+  if (p.use_meta)
+    return "metamaterials";
+  const int unit = p.fp16 ? 8 : 4;
+  if (n[2] % unit != 0)
+    return "nz is not a multiple of one 16-byte unit";
+  if (n[0] < 3 || n[1] < 3 || n[2] < 3)
+    return "grid too small";
+  std::string why = p.fp16 ? plan_t<__half> (plan, p, e, h, eps, sm_count)
+                           : plan_t<float> (plan, p, e, h, eps, sm_count);
+  if (!why.empty ())
+    return why;
+  Sweep2Work &w = plan.work;
+  w.nyt = (n[1] - 2 + kTb2Yown - 1) / kTb2Yown;
+  // x chunks of about `chunk` planes over the updated planes 1 .. nx - 2;
+  // with PML, the planes where every component is PML-free (with the two
+  // halo planes) form their own segment, so that no chunk mixes them
+  std::vector<int> seg = {1};
+  if (p.use_pml)
+  {
+    int lo = 1, hi = n[0] - 2;
+    for (int k = 0; k < 6; ++k)
+    {
+      lo = std::max (lo, p.ilo[k][0] + 2);
+      hi = std::min (hi, p.ihi[k][0] - 3);
+    }
+    if (lo > 1 && lo <= hi)
+      seg.push_back (lo);
+    if (hi + 1 <= n[0] - 2 && lo <= hi)
+      seg.push_back (hi + 1);
+  }
+  seg.push_back (n[0] - 1);
+  w.nch = 0;
+  w.xcut[0] = 1;
+  for (size_t sg = 0; sg + 1 < seg.size (); ++sg)
+  {
+    const int len = seg[sg + 1] - seg[sg];
+    int m = std::max (1, (len + chunk - 1) / chunk);
+    m = std::min (m, kMaxChunks - w.nch);
+    for (int j = 1; j <= m; ++j)
+      w.xcut[++w.nch] = seg[sg] + (int) ((long long) len * j / m);
+  }
+  for (int j = 0; j < w.nch; ++j)
+    if (w.xcut[j + 1] - w.xcut[j] > kTb2MaxChunk)
+      return "grid too long in x for the staged PML coefficients";
+  w.nitems = w.nzt * w.nyt * w.nch;
+  w.ctr = ctr;
+  plan.items[0] = plan.items[1] = 0;
+  for (int it = 0; it < w.nitems; ++it)
+    ++plan.items[sweep2_item_class (p, w, it)];
+  if (plan.ctas > w.nitems)
+    plan.ctas = w.nitems;
+  return "";
+}
+
+int launch_sweep2 (const Sweep2Plan &plan, int set, const FusedParams &p, int *err, cudaStream_t s,
+                   const SweepStreams &ss)
+{
+  return p.fp16 ? launch_t<__half> (plan, set, p, err, s, ss) : launch_t<float> (plan, set, p, err, s, ss);
+}
+
+}  // namespace fdtdb

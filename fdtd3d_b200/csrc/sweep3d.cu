@@ -40,10 +40,23 @@
 
 #include "incident_dev.cuh"
 #include "sweep3d.h"
+#include "tma.cuh"
 
 namespace fdtdb {
 
 namespace {
+
+using tma::global_ns;
+using tma::mbar_expect_tx;
+using tma::mbar_init;
+using tma::mbar_wait;
+using tma::smem_addr;
+
+__device__ __forceinline__ void tma_load_3d (uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                             uint32_t bar)
+{
+  tma::load_3d (dst, map, c0, c1, c2, bar);
+}
 
 constexpr int TZ = 128;           // z cells per tile: 32 lanes x 4
 constexpr int PW = TZ + 4;        // eps / auxiliary / exchange row width in floats (z0 .. z0 + 131)
@@ -82,65 +95,6 @@ struct Smem
   static constexpr unsigned TX_AN = 6u * sizeof (float) * AN * WY;
   static constexpr unsigned TX_AN4 = 4u * sizeof (float) * AN * WY;   // z-edge items: no Ex / Hx auxiliary
 };
-
-// ---------------------------------------------------------------- PTX helpers
-
-__device__ __forceinline__ uint32_t smem_addr (const void *p)
-{
-  return (uint32_t) __cvta_generic_to_shared (p);
-}
-
-__device__ __forceinline__ void mbar_init (uint32_t bar, unsigned count)
-{
-  asm volatile ("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx (uint32_t bar, unsigned bytes)
-{
-  asm volatile ("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait (uint32_t bar, unsigned parity)
-{
-  unsigned ok;
-  asm volatile (
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-__device__ __forceinline__ unsigned long long global_ns ()
-{
-  unsigned long long t;
-  asm volatile ("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Wait for the phase with the given parity; false after about one second.
-__device__ __noinline__ bool mbar_wait (uint32_t bar, unsigned parity)
-{
-  if (mbar_try_wait (bar, parity))
-    return true;
-  const unsigned long long t0 = global_ns ();
-  while (!mbar_try_wait (bar, parity))
-    if (global_ns () - t0 > 1000000000ull)
-      return false;
-  return true;
-}
-
-__device__ __forceinline__ void tma_load_3d (uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2,
-                                             uint32_t bar)
-{
-  asm volatile (
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
-      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
-      : "memory");
-}
 
 // ------------------------------------------------------- element conversions
 
@@ -1204,6 +1158,8 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn ()
   return fn;
 }
 
+}  // namespace
+
 // 3-D map over an (nx, ny, nz) array, z fastest, box bw x bh x 1
 bool make_map (CUtensorMap &m, const void *base, bool half, const int n[3], int bw, int bh)
 {
@@ -1224,6 +1180,8 @@ bool make_map (CUtensorMap &m, const void *base, bool half, const int n[3], int 
                    CU_TENSOR_MAP_SWIZZLE_NONE, promo, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
+
+namespace {
 
 template <typename T, int WY>
 std::string plan_t (SweepPlan &pl, const FusedParams &p, void *const e[2][3], void *const h[2][3],

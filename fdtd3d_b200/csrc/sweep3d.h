@@ -25,6 +25,10 @@ struct SweepMaps
   CUtensorMap auxn[6];         // narrow (32-cell) boxes for planes whose PML cells are all at a z edge
 };
 
+// Tiled 3-D tensor map over an (n[0], n[1], n[2]) array (z fastest, FP32 or
+// FP16), box bw (z) x bh (y) x 1 (x), 64-byte L2 promotion, zero fill.
+bool make_map (CUtensorMap &m, const void *base, bool half, const int n[3], int bw, int bh);
+
 constexpr int kMaxChunks = 256;   // x chunks per step (the chunk grows for larger grids)
 
 struct SweepWork
