@@ -134,9 +134,20 @@ struct fdtd_ctx
   // two-step (temporally blocked) sweep: used for pairs of steps when it can
   // serve the geometry (tb2_state 1), planned with the single-step sweep
   Sweep2Plan tb2;
-  int tb2_state = 0;
+  int tb2_state = 0;           // 1: whole grid two-step; 2: two-step core + PML shell in single steps
   std::string tb2_why;
   unsigned long long *tb2_ctr = nullptr;
+  // PML shell of the two-step scheme (tb2_state 2): the x / y PML slabs with
+  // a 2-cell margin advance by two single steps (step 1 into the third
+  // buffer set T over the shell and one more cell, step 2 from T), while the
+  // two-step kernel advances the core on its own stream
+  SweepPlan shell1, shell2;
+  int *shell_list[2] = {nullptr, nullptr};
+  unsigned long long *shell_ctr[2] = {nullptr, nullptr};
+  void *tfb[6] = {};                      // set T: fields
+  float *tauxb[6] = {};                   // set T: PML auxiliaries
+  cudaStream_t core_stream = nullptr;
+  cudaEvent_t core_fork = nullptr, core_join = nullptr;
   TfsfBand band;                          // TF/SF post pass of the sweep (band.cells > 0 when in use)
   std::vector<BandBox> band_host;         // its boxes, on the host
   // metamaterials with the sweep: the box of the Drude cells, fixed up after
@@ -712,6 +723,140 @@ int sweep_chunk (const FusedParams &p, int wy, int ctas, int overlap)
   return best;
 }
 
+// Plans the PML shell of the two-step scheme and the two-step core.  The core
+// owns the planes cx0 .. cx1 - 1 and rows cy0 .. cy1 - 1 (all z) that are at
+// least two cells from every x / y PML cell (so the two-step kernel never
+// evaluates an x / y PML cell for it); cy0 and cy1 sit on the single-step
+// sweep's 7-row tile boundaries.  The shell (the rest) takes two single
+// steps: step 1 over the shell and the cells next to it into set T, step 2
+// from T over the shell.  Returns "" or why the scheme does not apply.
+std::string plan_shell (fdtd_ctx *ctx, void *const e[2][3], void *const h[2][3], float *const aux[2][6])
+{
+  const Geometry &g = ctx->g;
+  const FusedParams &f = ctx->fused;
+  const int nx = g.n[0], ny = g.n[1];
+  int X0 = 1, X1 = nx - 1, Y0 = 1, Y1 = ny - 1;
+  for (int k = 0; k < 6; ++k)
+  {
+    X0 = std::max (X0, f.ilo[k][0]);
+    X1 = std::min (X1, f.ihi[k][0]);
+    Y0 = std::max (Y0, f.ilo[k][1]);
+    Y1 = std::min (Y1, f.ihi[k][1]);
+  }
+  const int cx0 = X0 + 2, cx1 = X1 - 2;
+  const int ty = kSweepTileY;
+  const int cy0 = 1 + ty * ((Y0 + 2 - 1 + ty - 1) / ty);
+  const int cy1 = 1 + ty * ((Y1 - 2 - 1) / ty);
+  if (cx1 - cx0 < 1 || cy1 - cy0 < 1)
+    return "the PML shell leaves no core";
+  // set T (fields as the step stores them, PML auxiliaries), starting as a
+  // copy of the current set (its never-updated faces must hold the fields)
+  const size_t n = (size_t) g.cells;
+  for (int k = 0; k < 6; ++k)
+  {
+    if (!ctx->tfb[k])
+    {
+      if (dalloc (ctx, &ctx->tfb[k], n * elem_size (ctx->kind), false) != FDTD_OK)
+        return "allocation of the shell buffer set failed";
+      if (dalloc (ctx, (void **) &ctx->tauxb[k], n * sizeof (float)) != FDTD_OK)
+        return "allocation of the shell buffer set failed";
+    }
+    if (cudaMemcpyAsync (ctx->tfb[k], ctx->ffb[ctx->fcur][k], n * elem_size (ctx->kind), cudaMemcpyDeviceToDevice,
+                         ctx->stream) != cudaSuccess)
+      return "shell buffer copy failed";
+  }
+  // x cuts: step 1 owns planes < cx0 + 1 and >= cx1 - 1 of the x slabs, step
+  // 2 those < cx0 and >= cx1; the core planes in chunks of at most 64
+  auto cuts_for = [&] (int a, int b) {
+    std::vector<int> c = {1};
+    auto add = [&] (int v) {
+      if (v > c.back () && v < nx - 1)
+        c.push_back (v);
+    };
+    for (int v = 1 + 64; v < a; v += 64)
+      add (v);
+    add (a);
+    const int len = b - a, m = std::max (1, (len + 63) / 64);
+    for (int j = 1; j < m; ++j)
+      add (a + (int) ((long long) len * j / m));
+    add (b);
+    for (int v = b + 64; v < nx - 1; v += 64)
+      add (v);
+    c.push_back (nx - 1);
+    return c;
+  };
+  const std::vector<int> c1 = cuts_for (cx0 + 1, cx1 - 1), c2 = cuts_for (cx0, cx1);
+  const int nzt = (g.n[2] - 1 + kSweepTileZ - 1) / kSweepTileZ;
+  const int nyt = (ny - 2 + ty - 1) / ty;
+  // items: x-slab chunks with every y tile, core chunks with the y-slab tiles
+  auto items_for = [&] (const std::vector<int> &c, int xa, int xb, int ya, int yb) {
+    std::vector<int> it;
+    const int nch = (int) c.size () - 1;
+    for (int ch = 0; ch < nch; ++ch)
+    {
+      const bool xslab = c[ch + 1] <= xa || c[ch] >= xb;
+      for (int yt = 0; yt < nyt; ++yt)
+      {
+        const int r0 = 1 + ty * yt, r1 = std::min (r0 + ty, ny - 1);   // rows r0 .. r1 - 1
+        const bool yslab = r1 <= ya || r0 >= yb;
+        if (!xslab && !yslab)
+          continue;
+        for (int zt = 0; zt < nzt; ++zt)
+          it.push_back ((ch * nyt + yt) * nzt + zt);
+      }
+    }
+    return it;
+  };
+  // step 1 rows: the shell rows and the first core row on each side
+  const std::vector<int> l1 = items_for (c1, cx0 + 1, cx1 - 1, cy0 + ty, cy1 - ty);
+  const std::vector<int> l2 = items_for (c2, cx0, cx1, cy0, cy1);
+  for (int q = 0; q < 2; ++q)
+  {
+    const size_t len = q == 0 ? l1.size () : l2.size ();
+    if (!ctx->shell_list[q])
+    {
+      const size_t cap = (size_t) nzt * nyt * (kMaxChunks + 1);
+      if (len > cap || dalloc (ctx, (void **) &ctx->shell_list[q], cap * sizeof (int)) != FDTD_OK)
+        return "allocation of the shell item lists failed";
+      if (dalloc (ctx, (void **) &ctx->shell_ctr[q], 8 * sizeof (unsigned long long)) != FDTD_OK)
+        return "allocation of the shell counters failed";
+    }
+  }
+  std::string why = sweep3d_plan_list (ctx->shell1, f, e, h, aux, ctx->mat32[0], ctx->sm_count, c1, l1,
+                                       ctx->shell_list[0], ctx->shell_ctr[0], ctx->stream);
+  if (!why.empty ())
+    return "shell step 1: " + why;
+  void *te[2][3], *th[2][3];
+  float *ta[2][6];
+  for (int b = 0; b < 2; ++b)
+  {
+    for (int c = 0; c < 3; ++c)
+    {
+      te[b][c] = ctx->tfb[c];
+      th[b][c] = ctx->tfb[c + 3];
+    }
+    for (int k = 0; k < 6; ++k)
+      ta[b][k] = ctx->tauxb[k];
+  }
+  why = sweep3d_plan_list (ctx->shell2, f, te, th, ta, ctx->mat32[0], ctx->sm_count, c2, l2, ctx->shell_list[1],
+                           ctx->shell_ctr[1], ctx->stream);
+  if (!why.empty ())
+    return "shell step 2: " + why;
+  why = sweep2_plan (ctx->tb2, f, e, h, ctx->mat32[0], ctx->sm_count, 64, ctx->tb2_ctr, cx0, cx1, cy0, cy1);
+  if (!why.empty ())
+    return "core: " + why;
+  if (!ctx->core_stream)
+  {
+    if (cudaStreamCreateWithFlags (&ctx->core_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags (&ctx->core_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags (&ctx->core_join, cudaEventDisableTiming) != cudaSuccess)
+      return "core stream creation failed";
+  }
+  if (cudaStreamSynchronize (ctx->stream) != cudaSuccess)
+    return "shell set-up failed";
+  return "";
+}
+
 // (Re)builds the TMA sweep plan for the current buffers.  FDTDB_SWEEP=0
 // keeps the register-blocked kernel; FDTDB_SWEEP_CHUNK overrides the x
 // chunk and FDTDB_SWEEP_VERBOSE=1 prints the plan, for tuning runs.
@@ -864,10 +1009,20 @@ int plan_sweep (fdtd_ctx *ctx)
     else
     {
       if (!ctx->tb2_ctr)
-        DALLOC (ctx->tb2_ctr, 4 * sizeof (unsigned long long));
-      ctx->tb2_why = sweep2_plan (ctx->tb2, ctx->fused, e, h, ctx->mat32[0], ctx->sm_count, 64, ctx->tb2_ctr);
-      if (ctx->tb2_why.empty ())
-        ctx->tb2_state = 1;
+        DALLOC (ctx->tb2_ctr, 6 * sizeof (unsigned long long));
+      if (g.cfg.use_pml)
+      {
+        // PML: the x / y PML shell in single steps beside the two-step core
+        ctx->tb2_why = plan_shell (ctx, e, h, aux);
+        if (ctx->tb2_why.empty ())
+          ctx->tb2_state = 2;
+      }
+      else
+      {
+        ctx->tb2_why = sweep2_plan (ctx->tb2, ctx->fused, e, h, ctx->mat32[0], ctx->sm_count, 64, ctx->tb2_ctr);
+        if (ctx->tb2_why.empty ())
+          ctx->tb2_state = 1;
+      }
     }
   }
   if (const char *v = std::getenv ("FDTDB_SWEEP_VERBOSE"))
@@ -879,10 +1034,15 @@ int plan_sweep (fdtd_ctx *ctx)
                     why.empty () ? "in use" : why.c_str (), ctx->sweep.wy, ctx->sweep.ctas, ctx->sweep.smem, w.nzt,
                     w.nyt, w.nch, w.chunk, w.nitems, ctx->sweep.items[0], ctx->sweep.items[1], ctx->sweep.items[2], ctx->sweep.items[3],
                     ctx->band.nbox, ctx->band.cells);
-      std::fprintf (stderr, "sweep2: %s ctas=%d smem=%u tiles z=%d y=%d chunks=%d items=%d lean/PML=%d/%d\n",
-                    ctx->tb2_state == 1 ? "in use" : ctx->tb2_why.c_str (), ctx->tb2.ctas, ctx->tb2.smem,
-                    ctx->tb2.work.nzt, ctx->tb2.work.nyt, ctx->tb2.work.nch, ctx->tb2.work.nitems,
-                    ctx->tb2.items[0], ctx->tb2.items[1]);
+      std::fprintf (stderr, "sweep2: %s ctas=%d smem=%u tiles z=%d y=%d chunks=%d items=%d lean/PML/z-edge=%d/%d/%d\n",
+                    ctx->tb2_state >= 1 ? (ctx->tb2_state == 2 ? "in use (core)" : "in use") : ctx->tb2_why.c_str (),
+                    ctx->tb2.ctas, ctx->tb2.smem, ctx->tb2.work.nzt, ctx->tb2.work.nyt, ctx->tb2.work.nch,
+                    ctx->tb2.work.nitems, ctx->tb2.items[0], ctx->tb2.items[1], ctx->tb2.items[2]);
+      if (ctx->tb2_state == 2)
+        std::fprintf (stderr, "shell: step 1 items %d (lean/z-edge/full/PML %d/%d/%d/%d), step 2 items %d "
+                      "(%d/%d/%d/%d)\n", ctx->shell1.work.nlist, ctx->shell1.items[0], ctx->shell1.items[1],
+                      ctx->shell1.items[2], ctx->shell1.items[3], ctx->shell2.work.nlist, ctx->shell2.items[0],
+                      ctx->shell2.items[1], ctx->shell2.items[2], ctx->shell2.items[3]);
     }
   return FDTD_OK;
 }
@@ -972,6 +1132,14 @@ void release (fdtd_ctx *ctx)
       cudaStreamSynchronize (q);
       cudaStreamDestroy (q);
     }
+  if (ctx->core_stream)
+  {
+    cudaStreamSynchronize (ctx->core_stream);
+    cudaStreamDestroy (ctx->core_stream);
+  }
+  for (cudaEvent_t e : {ctx->core_fork, ctx->core_join})
+    if (e)
+      cudaEventDestroy (e);
   for (cudaEvent_t e : {ctx->sweep_streams.fork, ctx->sweep_streams.join[0], ctx->sweep_streams.join[1]})
     if (e)
       cudaEventDestroy (e);
@@ -1209,13 +1377,35 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
         if ((r = plan_sweep (ctx)) != FDTD_OK)
           return r;
       cudaEvent_t pe;
-      if (ctx->tb2_state == 1 && i + 1 < n && ctx->dft_comp < 0)
+      if (ctx->tb2_state >= 1 && i + 1 < n && ctx->dft_comp < 0)
       {
         // steps t and t + 1 in one pass (no TF/SF, point source or Drude
         // medium: the incident grid is not stepped)
         if ((r = prof_begin (ctx, &pe)) != FDTD_OK)
           return r;
-        ctx->launches += launch_sweep2 (ctx->tb2, o, f, ctx->d_err, s, ctx->sweep_streams);
+        if (ctx->tb2_state == 1)
+          ctx->launches += launch_sweep2 (ctx->tb2, o, f, ctx->d_err, s, ctx->sweep_streams);
+        else
+        {
+          // the shell's two single steps on s, the core on its own stream
+          // (launched after the shell's first step, so that its CTAs take
+          // the SMs that step leaves as it drains)
+          CK (cudaEventRecord (ctx->core_fork, s));
+          CK (cudaStreamWaitEvent (ctx->core_stream, ctx->core_fork, 0));
+          FusedParams f1 = f;
+          for (int c = 0; c < 3; ++c)
+          {
+            f1.e_new[c] = ctx->tfb[c];
+            f1.h_new[c] = ctx->tfb[c + 3];
+          }
+          for (int k = 0; k < 6; ++k)
+            f1.aux_new[k] = ctx->tauxb[k];
+          ctx->launches += launch_sweep3d (ctx->shell1, o, f1, ctx->d_err, s, ctx->sweep_streams);
+          ctx->launches += launch_sweep2 (ctx->tb2, o, f, ctx->d_err, ctx->core_stream);
+          ctx->launches += launch_sweep3d (ctx->shell2, 0, f, ctx->d_err, s, ctx->sweep_streams);
+          CK (cudaEventRecord (ctx->core_join, ctx->core_stream));
+          CK (cudaStreamWaitEvent (s, ctx->core_join, 0));
+        }
         ctx->step_kernel = "sweep2_tma";
         if ((r = prof_end (ctx, pe)) != FDTD_OK)
           return r;
@@ -1449,11 +1639,15 @@ int fdtd_upload_field (fdtd_ctx *ctx, int component, const double *host)
     if ((r = ensure_staging (ctx)) != FDTD_OK)
       return r;
     CK (cudaMemcpyAsync (ctx->staging, host, n * sizeof (double), cudaMemcpyHostToDevice, ctx->stream));
-    // both buffer sets: cells the step never updates must keep these values
-    for (int b = 0; b < 2; ++b)
-      if (ctx->ffb[b][component])
-        ctx->launches += launch_convert_in (ctx->ffb[b][component], ctx->kind, ctx->staging, n,
-                                            component >= 3 ? kEta0 : 1.0, ctx->stream);
+    // every buffer set (the two of the one-sweep kernels and the shell's
+    // set T): cells the step never updates must keep these values
+    for (int b = 0; b < 3; ++b)
+    {
+      void *dst = b < 2 ? ctx->ffb[b][component] : ctx->tfb[component];
+      if (dst)
+        ctx->launches += launch_convert_in (dst, ctx->kind, ctx->staging, n, component >= 3 ? kEta0 : 1.0,
+                                            ctx->stream);
+    }
   }
   CK (cudaStreamSynchronize (ctx->stream));
   return FDTD_OK;

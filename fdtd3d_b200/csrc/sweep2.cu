@@ -32,6 +32,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <type_traits>
 #include <vector>
 
 #include "sweep2.h"
@@ -133,6 +134,21 @@ __device__ __forceinline__ void sts2 (float *s, const float v[2])
   *reinterpret_cast<float2 *> (s) = make_float2 (v[0], v[1]);
 }
 
+// Auxiliary values of a lane's two cells (bits: which are PML cells; the
+// pair starts on an 8-byte boundary).
+__device__ __forceinline__ void store_aux (float *g, unsigned bits, const float v[2])
+{
+  if (bits == 3u)
+    __stcs (reinterpret_cast<float2 *> (g), make_float2 (v[0], v[1]));
+  else
+  {
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+      if ((bits >> j) & 1u)
+        __stcs (g + j, v[j]);
+  }
+}
+
 // ------------------------------------------------------------------ kernel
 
 // Pair (0: ca1, sq1; 1: p5, q5; 2: g4p, g4m) of component k that runs along
@@ -151,29 +167,80 @@ __device__ __forceinline__ int pair_axis (int k, int q)
   return q == 0 ? (a + 1) % 3 : (q == 1 ? (a + 2) % 3 : a);
 }
 
-// Element e of coefficient pair q of component k at (plane index xi, row w,
-// column zcol) from the item's staged tables.
+// PML update of component k on a lane's two cells (the single-step kernels'
+// pml_vec), on the cells of `bits`:
+//   X_new = ca1 X + sq1 curl,  F_new = p5 F + (g4p X_new - g4m X) q5 im;
+// fn gets F_new, xn X_new there.  Coefficient pairs come from the item's
+// staged tables: along x at plane index xi, along y at row w, along z at the
+// columns zcol, zcol + 1.
 template <int XTW>
-__device__ __forceinline__ float pml_coef (const float *T, int k, int q, int e, int xi, int w, int zcol)
+__device__ __forceinline__ void pml_two (const float *T, int k, int xi, int w, int zcol, unsigned bits,
+                                         const float xo[2], const float cu[2], const float im[2], const float fo[2],
+                                         float fn[2], float xn[2])
 {
-  const int a = pair_axis (k, q);
-  return a == 0 ? T[12 * ZW + 12 * NW + (2 * k + e) * XTW + xi]
-                : (a == 1 ? T[12 * ZW + (2 * k + e) * NW + w] : T[(2 * k + e) * ZW + zcol]);
+  float c[3][2][2];   // [pair][element][cell]
+#pragma unroll
+  for (int q = 0; q < 3; ++q)
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+    {
+      const int a = pair_axis (k, q);
+      if (a == 2)
+        lds2 (T + (2 * k + e) * ZW + zcol, c[q][e]);
+      else
+        c[q][e][0] = c[q][e][1] =
+            a == 0 ? T[12 * ZW + 12 * NW + (2 * k + e) * XTW + xi] : T[12 * ZW + (2 * k + e) * NW + w];
+    }
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+  {
+    const float n = c[0][0][j] * xo[j] + c[0][1][j] * cu[j];
+    const float f = c[1][0][j] * fo[j] + (c[2][0][j] * n - c[2][1][j] * xo[j]) * c[1][1][j] * im[j];
+    const bool on = (bits >> j) & 1u;
+    fn[j] = on ? f : fn[j];
+    xn[j] = on ? n : xn[j];
+  }
 }
 
-// PML update of component k on one cell (the single-step kernels' pml_vec):
-//   X_new = ca1 X + sq1 curl,  F_new = p5 F + (g4p X_new - g4m X) q5 im.
-// Returns F_new; xn gets X_new.
-template <int XTW>
-__device__ __forceinline__ float pml_cell (const float *T, int k, int xi, int w, int zcol, float xo, float cu,
-                                           float im, float fo, float &xn)
+// z-edge items (x and y interior for every component, PML cells only along
+// z): the single-step kernel's branch-free form, in which only the z pair
+// of each component differs from the sigma = 0 identity and the item's z
+// table holds it pre-combined (zedge_pair in sweep3d.cu): for the pair
+// (p5, q5) along z (Ex, Hx) F = p5 F + S q5 im curl (no auxiliary); for
+// (ca1, sq1) (Ey, Hy) X_new = ca1 X + sq1 curl, F = F + ((ca1 - 1) X +
+// sq1 curl) im; for (g4p, g4m) (Ez, Hz) X_new = X + S curl,
+// F = F + ((g4p - g4m) X + S g4p curl) im, with X = 0 on cells that are not
+// PML cells of the component.  With the identity values each form is the
+// plain update F + (S im) curl bit for bit.  fn gets F_new on the updated
+// cells (upd) and F elsewhere, xn X_new on the PML cells (pm), 0 elsewhere.
+__device__ __forceinline__ void zedge_two (const float *Tz, int k, int zl, float S, unsigned upd, unsigned pm,
+                                           const float xo[2], const float cu[2], const float im[2], const float fo[2],
+                                           float fn[2], float xn[2])
 {
-  const float ca1 = pml_coef<XTW> (T, k, 0, 0, xi, w, zcol), sq1 = pml_coef<XTW> (T, k, 0, 1, xi, w, zcol);
-  const float p5 = pml_coef<XTW> (T, k, 1, 0, xi, w, zcol), q5 = pml_coef<XTW> (T, k, 1, 1, xi, w, zcol);
-  const float g4p = pml_coef<XTW> (T, k, 2, 0, xi, w, zcol), g4m = pml_coef<XTW> (T, k, 2, 1, xi, w, zcol);
-  const float n = ca1 * xo + sq1 * cu;
-  xn = n;
-  return p5 * fo + (g4p * n - g4m * xo) * q5 * im;
+  const int pz = pair_along (k, 2);
+  float c0[2], c1[2];
+  lds2 (Tz + (2 * k) * ZW + zl, c0);
+  lds2 (Tz + (2 * k + 1) * ZW + zl, c1);
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+  {
+    const bool on = (pm >> j) & 1u;
+    const float x = on ? xo[j] : 0.f;
+    float f;
+    if (pz == 1)
+      f = fmaf (im[j] * c1[j], cu[j], c0[j] * fo[j]);
+    else if (pz == 0)
+    {
+      f = fmaf (c1[j] * im[j], cu[j], fmaf (c0[j] * im[j], x, fo[j]));
+      xn[j] = on ? fmaf (c0[j], x, fmaf (c1[j], cu[j], x)) : 0.f;
+    }
+    else
+    {
+      f = fmaf (c0[j] * im[j], cu[j], fmaf (c1[j] * im[j], x, fo[j]));
+      xn[j] = on ? fmaf (S, cu[j], x) : 0.f;
+    }
+    fn[j] = ((upd >> j) & 1u) ? f : fo[j];
+  }
 }
 
 // MODE 0 (lean): no cell of the item's extended region is a PML cell of any
@@ -181,7 +248,10 @@ __device__ __forceinline__ float pml_cell (const float *T, int k, int xi, int w,
 // that are PML cells of a component with the PML form (masks per component
 // and cell, coefficients from the 1-D tables), carries the auxiliary of the
 // first step in registers to the second, and loads the old auxiliaries one
-// plane ahead with plain loads (only lanes with PML cells).
+// plane ahead with plain loads (only lanes with PML cells).  MODE 2 (z
+// edge): PML cells only along z; every lane runs the branch-free z-edge form
+// (zedge_two), auxiliaries as in MODE 1 but only for the four components
+// that keep one.
 template <typename T, int MODE>
 __global__ void __launch_bounds__ (32 * NW, 1)
     sweep2_kernel (const __grid_constant__ Sweep2Maps maps, const __grid_constant__ FusedParams p,
@@ -192,6 +262,8 @@ __global__ void __launch_bounds__ (32 * NW, 1)
   constexpr int HS = L::H_B / sizeof (T), ES = L::E_B / sizeof (T), PS = L::P_B / sizeof (float);
   constexpr unsigned kLanes = 0xffffffffu;
   constexpr bool kPml = MODE == 1;
+  constexpr bool kZedge = MODE == 2;
+  constexpr bool kAux = kPml || kZedge;   // PML masks and auxiliaries
   extern __shared__ __align__ (128) unsigned char smem_raw[];
   __shared__ int s_item;
   __shared__ int s_abort;
@@ -240,6 +312,7 @@ __global__ void __launch_bounds__ (32 * NW, 1)
 
   unsigned phase = 0;   // bit s: parity of the next completion of stage s
   bool aborted = false;
+  static_assert (MODE >= 0 && MODE <= 2, "item class");
   for (;;)
   {
     __syncthreads ();   // every thread has read the previous item's index
@@ -255,7 +328,7 @@ __global__ void __launch_bounds__ (32 * NW, 1)
     const int yt = (item / wk.nzt) % wk.nyt;
     const int ch = item / (wk.nzt * wk.nyt);
     const int zs = L::ZOWN * zt - L::ZOFF;   // first z cell of the warp rows
-    const int Y = kTb2Yown * yt;             // row of warp 0
+    const int Y = wk.yoff + kTb2Yown * yt;   // row of warp 0
     const int xa = wk.xcut[ch];
     const int xb = wk.xcut[ch + 1] - 1;
     const int np = xb - xa + 5;              // planes xa - 2 .. xb + 2
@@ -265,6 +338,35 @@ __global__ void __launch_bounds__ (32 * NW, 1)
 #pragma unroll
       for (int k = 0; k < NST2; ++k)
         issue (k, xa - 2 + k, zs, Y);
+    }
+    if constexpr (kZedge)
+    {
+      // the item's z pairs in the z-edge form (read after the first plane's
+      // barrier)
+      const int tid = w * 32 + lane;
+      for (int q = tid; q < 6 * ZW; q += 32 * NW)
+      {
+        const int k = q / ZW, col = q % ZW, z = min (max (zs + col, 0), nz - 1), pz = pair_along (k, 2);
+        const float a = __ldg (p.tab[k][2 * pz] + z), b = __ldg (p.tab[k][2 * pz + 1] + z);
+        float c0, c1;
+        if (pz == 1)
+        {
+          c0 = a;
+          c1 = S * b;
+        }
+        else if (pz == 0)
+        {
+          c0 = a - 1.f;
+          c1 = b;
+        }
+        else
+        {
+          c0 = S * a;
+          c1 = a - b;
+        }
+        Tab[(2 * k) * ZW + col] = c0;
+        Tab[(2 * k + 1) * ZW + col] = c1;
+      }
     }
     if constexpr (kPml)
     {
@@ -302,47 +404,56 @@ __global__ void __launch_bounds__ (32 * NW, 1)
         if (zc + j >= 1 && zc + j <= nz - 2)
           cupd |= 1u << j;
     }
-    const bool own = w >= 1 && w <= kTb2Yown && r <= ny - 2 && lane >= L::OLO && lane <= L::OHI && zc >= 0 && zc < nz;
+    const bool own = w >= 1 && w <= kTb2Yown && r < wk.yend && lane >= L::OLO && lane <= L::OHI && zc >= 0 && zc < nz;
     const size_t rowoff = (size_t) r * nz + zc;
+    // y / z membership of this lane's cells in each component's sigma = 0
+    // box: bit 2k + j (k = 0 .. 5, cell j) of yz_in
+    unsigned yz_in = 0;
+    if (kAux)
+    {
+#pragma unroll
+      for (int k = 0; k < 6; ++k)
+        if (r >= p.ilo[k][1] && r < p.ihi[k][1])
+#pragma unroll
+          for (int j = 0; j < 2; ++j)
+            if (zc + j >= p.ilo[k][2] && zc + j < p.ihi[k][2])
+              yz_in |= 1u << (2 * k + j);
+    }
     // PML cells of the family (E: kb = 0, H: kb = 3) among this lane's
     // updated cells on plane xx: bit 2c + j for component kb + c, cell j
     auto pmask = [&] (int kb, int xx) -> unsigned {
       const unsigned u = (xx >= 1 && xx <= nx - 2) ? cupd : 0u;
-      if (!kPml || !u)
+      if (!kAux || !u)
         return 0u;
-      unsigned m = 0;
+      unsigned xin = 0;
 #pragma unroll
       for (int c = 0; c < 3; ++c)
-      {
-        const int k = kb + c;
-        const bool xy = xx >= p.ilo[k][0] && xx < p.ihi[k][0] && r >= p.ilo[k][1] && r < p.ihi[k][1];
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-          if (!(xy && zc + j >= p.ilo[k][2] && zc + j < p.ihi[k][2]))
-            m |= 1u << (2 * c + j);
-      }
-      return m & (u * 0x15u);   // the update mask of each component's two bits
+        if (xx >= p.ilo[kb + c][0] && xx < p.ihi[kb + c][0])
+          xin |= 3u << (2 * c);
+      return ~(xin & (yz_in >> (2 * kb))) & (u * 0x15u);   // the update mask of each component's two bits
     };
-    // masks of the planes in flight: E1 (x), H1 (x - 1), E2 (x - 1), H2 (x - 2)
-    unsigned mE1 = 0, mH1 = 0, mE2 = 0, mH2 = 0;
-    (void) mE2;
-    (void) mH2;
-
-    float hp[3][2] = {};    // H0(x - 1)
-    float e1p[3][2] = {};   // E1(x - 1)
-    float ip[3][2] = {};    // 2 / (eps + eps') of E at x - 1
-    float h1p[3][2] = {};   // H1(x - 2)
-    float e2p[3][2] = {};   // E2(x - 2)
-    // PML: old auxiliaries loaded one plane ahead (E at x, H at x - 1), and
-    // the first step's auxiliaries carried to the second
-    float axe[3][2] = {}, axh[3][2] = {}, xe1p[3][2] = {}, xh1p[3][2] = {};
+    // State carried from one plane to the next.  Two sets are used in turn
+    // (set P holds this plane's values, set 1 - P the previous plane's) and
+    // the plane loop is unrolled by two, so nothing is copied.
+    struct PlaneState
+    {
+      float h0[3][2];    // H0 of the plane
+      float e1[3][2];    // E1 of the plane
+      float im[3][2];    // 2 / (eps + eps') of E on the plane
+      float h1[3][2];    // H1 of the plane before
+      float e2[3][2];    // E2 of the plane before
+      float xe1[3][2];   // PML: X of E after the first step on the plane
+      float xh1[3][2];   // PML: X of H after the first step on the plane before
+      unsigned mE, mH;   // PML cells: E on the plane, H on the plane before (pmask bits)
+    };
+    PlaneState sa = {}, sb = {};
+    // PML: old auxiliaries loaded one plane ahead (E of the plane, H of the plane before)
+    float axe[3][2] = {}, axh[3][2] = {};
     (void) axe;
     (void) axh;
-    (void) xe1p;
-    (void) xh1p;
 
-    for (int i = 0; i < np; ++i)
-    {
+    auto plane = [&] (int i, auto par_c, PlaneState &cur, PlaneState &prev) __attribute__ ((always_inline)) -> bool {
+      constexpr int P = decltype (par_c)::value;
       const int st = i % NST2;
       const int x = xa - 2 + i;
       if (!tma::mbar_wait (bar + 8 * st, (phase >> st) & 1u))
@@ -359,21 +470,18 @@ __global__ void __launch_bounds__ (32 * NW, 1)
       // previous plane's (read).  Every set is rewritten two planes after it
       // was written, and the one barrier per plane lies between its readers
       // and that rewrite.
-      float *XE1w = X + (i & 1) * 2 * XN;
-      const float *XE1r = X + ((i + 1) & 1) * 2 * XN;
-      float *XH1 = X + (4 + (i & 1) * 2) * XN;
-      float *XE2w = X + (8 + (i & 1) * 2) * XN;
-      const float *XE2r = X + (8 + ((i + 1) & 1) * 2) * XN;
+      float *XE1w = X + P * 2 * XN;
+      const float *XE1r = X + (1 - P) * 2 * XN;
+      float *XH1 = X + (4 + P * 2) * XN;
+      float *XE2w = X + (8 + P * 2) * XN;
+      const float *XE2r = X + (8 + (1 - P) * 2) * XN;
 
       // H0(x) on this row
-      float hc[3][2];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
-        V2<T>::ld (sH + c * HS + (w + 1) * HW + HZ + zl, hc[c]);
+        V2<T>::ld (sH + c * HS + (w + 1) * HW + HZ + zl, cur.h0[c]);
 
       // ================= phase 1: E1(x) on every row, H1(x - 1) on rows 0 .. 14
-      float e1[3][2] = {}, im[3][2] = {}, xe1[3][2] = {};
-      (void) xe1;
       if (i >= 1)
       {
         const unsigned u = (x >= 1 && x <= nx - 2) ? cupd : 0u;
@@ -395,56 +503,71 @@ __global__ void __launch_bounds__ (32 * NW, 1)
 #pragma unroll
           for (int j = 0; j < 2; ++j)
           {
-            im[0][j] = __fdividef (2.f, p0[j] + px[j]);
-            im[1][j] = __fdividef (2.f, p0[j] + py[j]);
-            im[2][j] = __fdividef (2.f, p0[j] + (j == 0 ? p0[1] : pz));
+            cur.im[0][j] = __fdividef (2.f, p0[j] + px[j]);
+            cur.im[1][j] = __fdividef (2.f, p0[j] + py[j]);
+            cur.im[2][j] = __fdividef (2.f, p0[j] + (j == 0 ? p0[1] : pz));
           }
         }
         else
         {
 #pragma unroll
           for (int j = 0; j < 2; ++j)
-            im[0][j] = im[1][j] = im[2][j] = 1.f;
+            cur.im[0][j] = cur.im[1][j] = cur.im[2][j] = 1.f;
         }
         float cu[3][2];
 #pragma unroll
         for (int j = 0; j < 2; ++j)
         {
-          const float hyl = j ? hc[1][0] : hym1;
-          const float hxl = j ? hc[0][0] : hxm1;
-          cu[0][j] = (hc[2][j] - hzm[j]) - (hc[1][j] - hyl);
-          cu[1][j] = (hc[0][j] - hxl) - (hc[2][j] - hp[2][j]);
-          cu[2][j] = (hc[1][j] - hp[1][j]) - (hc[0][j] - hxm[j]);
-          const bool up = (u >> j) & 1u;
-#pragma unroll
-          for (int c = 0; c < 3; ++c)
-            e1[c][j] = up ? eo[c][j] + (S * im[c][j]) * cu[c][j] : eo[c][j];
-        }
-        if constexpr (kPml)
-        {
-          if (mE1)
+          const float hyl = j ? cur.h0[1][0] : hym1;
+          const float hxl = j ? cur.h0[0][0] : hxm1;
+          cu[0][j] = (cur.h0[2][j] - hzm[j]) - (cur.h0[1][j] - hyl);
+          cu[1][j] = (cur.h0[0][j] - hxl) - (cur.h0[2][j] - prev.h0[2][j]);
+          cu[2][j] = (cur.h0[1][j] - prev.h0[1][j]) - (cur.h0[0][j] - hxm[j]);
+          if constexpr (!kZedge)
           {
 #pragma unroll
             for (int c = 0; c < 3; ++c)
-#pragma unroll
-              for (int j = 0; j < 2; ++j)
-                if ((mE1 >> (2 * c + j)) & 1u)
-                  e1[c][j] = pml_cell<XTW> (Tab, c, i, w, zl + j, axe[c][j], cu[c][j], im[c][j], eo[c][j], xe1[c][j]);
+              cur.e1[c][j] = eo[c][j] + (S * cur.im[c][j]) * cu[c][j];
           }
         }
-        sts2 (XE1w + 0 * XN + w * ZW + zl, e1[0]);
-        sts2 (XE1w + 1 * XN + w * ZW + zl, e1[2]);
+        if constexpr (kZedge)
+        {
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            zedge_two (Tab, c, zl, S, u, (cur.mE >> (2 * c)) & 3u, axe[c], cu[c], cur.im[c], eo[c], cur.e1[c],
+                       cur.xe1[c]);
+        }
+        else if (u != 3u)   // cells the step does not update keep their values (grid faces)
+        {
+#pragma unroll
+          for (int j = 0; j < 2; ++j)
+            if (!((u >> j) & 1u))
+#pragma unroll
+              for (int c = 0; c < 3; ++c)
+                cur.e1[c][j] = eo[c][j];
+        }
+        if constexpr (kPml)
+        {
+          if (cur.mE)
+          {
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+              if ((cur.mE >> (2 * c)) & 3u)
+                pml_two<XTW> (Tab, c, i, w, zl, (cur.mE >> (2 * c)) & 3u, axe[c], cu[c], cur.im[c], eo[c],
+                              cur.e1[c], cur.xe1[c]);
+          }
+        }
+        sts2 (XE1w + 0 * XN + w * ZW + zl, cur.e1[0]);
+        sts2 (XE1w + 1 * XN + w * ZW + zl, cur.e1[2]);
       }
-      float h1[3][2] = {}, xh1[3][2] = {};
-      (void) xh1;
       if (i >= 2 && w < NW - 1)
       {
-        // H1(x - 1): E1(x - 1) in e1p, its y + 1 row from the previous
+        // H1(x - 1): E1(x - 1) in prev.e1, its y + 1 row from the previous
         // plane's exchange rows, its z + 1 cell from the next lane
         const int xh = x - 1;
         const unsigned u = (xh >= 1 && xh <= nx - 2) ? cupd : 0u;
-        const float exn = __shfl_down_sync (kLanes, e1p[0][0], 1);
-        const float eyn = __shfl_down_sync (kLanes, e1p[1][0], 1);
+        const float exn = __shfl_down_sync (kLanes, prev.e1[0][0], 1);
+        const float eyn = __shfl_down_sync (kLanes, prev.e1[1][0], 1);
         float exy[2], ezy[2];
         lds2 (XE1r + 0 * XN + (w + 1) * ZW + zl, exy);
         lds2 (XE1r + 1 * XN + (w + 1) * ZW + zl, ezy);
@@ -452,56 +575,73 @@ __global__ void __launch_bounds__ (32 * NW, 1)
 #pragma unroll
         for (int j = 0; j < 2; ++j)
         {
-          const float eyz = j ? eyn : e1p[1][1];
-          const float exz = j ? exn : e1p[0][1];
-          a[0][j] = (eyz - e1p[1][j]) - (ezy[j] - e1p[2][j]);
-          a[1][j] = (e1[2][j] - e1p[2][j]) - (exz - e1p[0][j]);
-          a[2][j] = (exy[j] - e1p[0][j]) - (e1[1][j] - e1p[1][j]);
-          const bool up = (u >> j) & 1u;
-#pragma unroll
-          for (int c = 0; c < 3; ++c)
-            h1[c][j] = up ? hp[c][j] + S * a[c][j] : hp[c][j];
-        }
-        if constexpr (kPml)
-        {
-          if (mH1)
+          const float eyz = j ? eyn : prev.e1[1][1];
+          const float exz = j ? exn : prev.e1[0][1];
+          a[0][j] = (eyz - prev.e1[1][j]) - (ezy[j] - prev.e1[2][j]);
+          a[1][j] = (cur.e1[2][j] - prev.e1[2][j]) - (exz - prev.e1[0][j]);
+          a[2][j] = (exy[j] - prev.e1[0][j]) - (cur.e1[1][j] - prev.e1[1][j]);
+          if constexpr (!kZedge)
           {
 #pragma unroll
             for (int c = 0; c < 3; ++c)
-#pragma unroll
-              for (int j = 0; j < 2; ++j)
-                if ((mH1 >> (2 * c + j)) & 1u)
-                  h1[c][j] = pml_cell<XTW> (Tab, 3 + c, i - 1, w, zl + j, axh[c][j], a[c][j], 1.f, hp[c][j], xh1[c][j]);
+              cur.h1[c][j] = prev.h0[c][j] + S * a[c][j];
           }
         }
-        sts2 (XH1 + 0 * XN + w * ZW + zl, h1[0]);
-        sts2 (XH1 + 1 * XN + w * ZW + zl, h1[2]);
+        if constexpr (kZedge)
+        {
+          const float one[2] = {1.f, 1.f};
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            zedge_two (Tab, 3 + c, zl, S, u, (cur.mH >> (2 * c)) & 3u, axh[c], a[c], one, prev.h0[c], cur.h1[c],
+                       cur.xh1[c]);
+        }
+        else if (u != 3u)
+        {
+#pragma unroll
+          for (int j = 0; j < 2; ++j)
+            if (!((u >> j) & 1u))
+#pragma unroll
+              for (int c = 0; c < 3; ++c)
+                cur.h1[c][j] = prev.h0[c][j];
+        }
+        if constexpr (kPml)
+        {
+          if (cur.mH)
+          {
+            const float one[2] = {1.f, 1.f};
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+              if ((cur.mH >> (2 * c)) & 3u)
+                pml_two<XTW> (Tab, 3 + c, i - 1, w, zl, (cur.mH >> (2 * c)) & 3u, axh[c], a[c], one, prev.h0[c],
+                              cur.h1[c], cur.xh1[c]);
+          }
+        }
+        sts2 (XH1 + 0 * XN + w * ZW + zl, cur.h1[0]);
+        sts2 (XH1 + 1 * XN + w * ZW + zl, cur.h1[2]);
       }
 
       __syncthreads ();   // E1 / H1 rows visible, stage st read
       if (s_abort)
       {
         // wait (bounded) for the copies still in flight into the other stages
-        aborted = true;
         if (leader)
           for (int k = 1; k < NST2 && i + k < np; ++k)
           {
             const int so = (st + k) % NST2;
             tma::mbar_wait (bar + 8 * so, (phase >> so) & 1u);
           }
-        break;
+        return false;
       }
       if (leader && i + NST2 < np)
         issue (st, x + NST2, zs, Y);
 
       // ================= phase 2: E2(x - 1) on rows 1 .. 14, H2(x - 2) on rows 1 .. 13
-      float e2[3][2] = {};
       if (i >= 3 && w >= 1 && w < NW - 1)
       {
         const int xe = x - 1;
         const unsigned u = (xe >= 1 && xe <= nx - 2) ? cupd : 0u;
-        const float hyl = __shfl_up_sync (kLanes, h1[1][1], 1);
-        const float hxl = __shfl_up_sync (kLanes, h1[0][1], 1);
+        const float hyl = __shfl_up_sync (kLanes, cur.h1[1][1], 1);
+        const float hxl = __shfl_up_sync (kLanes, cur.h1[0][1], 1);
         float hzm[2], hxm[2];
         lds2 (XH1 + 1 * XN + (w - 1) * ZW + zl, hzm);
         lds2 (XH1 + 0 * XN + (w - 1) * ZW + zl, hxm);
@@ -509,36 +649,55 @@ __global__ void __launch_bounds__ (32 * NW, 1)
 #pragma unroll
         for (int j = 0; j < 2; ++j)
         {
-          const float hyz = j ? h1[1][0] : hyl;
-          const float hxz = j ? h1[0][0] : hxl;
-          cu[0][j] = (h1[2][j] - hzm[j]) - (h1[1][j] - hyz);
-          cu[1][j] = (h1[0][j] - hxz) - (h1[2][j] - h1p[2][j]);
-          cu[2][j] = (h1[1][j] - h1p[1][j]) - (h1[0][j] - hxm[j]);
-          const bool up = (u >> j) & 1u;
+          const float hyz = j ? cur.h1[1][0] : hyl;
+          const float hxz = j ? cur.h1[0][0] : hxl;
+          cu[0][j] = (cur.h1[2][j] - hzm[j]) - (cur.h1[1][j] - hyz);
+          cu[1][j] = (cur.h1[0][j] - hxz) - (cur.h1[2][j] - prev.h1[2][j]);
+          cu[2][j] = (cur.h1[1][j] - prev.h1[1][j]) - (cur.h1[0][j] - hxm[j]);
+          if constexpr (!kZedge)
+          {
 #pragma unroll
-          for (int c = 0; c < 3; ++c)
-            e2[c][j] = up ? e1p[c][j] + (S * ip[c][j]) * cu[c][j] : e1p[c][j];
+            for (int c = 0; c < 3; ++c)
+              cur.e2[c][j] = prev.e1[c][j] + (S * prev.im[c][j]) * cu[c][j];
+          }
         }
         const bool store = own && xe >= xa && xe <= xb;
         const size_t id = (size_t) xe * sx + rowoff;
+        if constexpr (kZedge)
+        {
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+          {
+            const unsigned b = (prev.mE >> (2 * c)) & 3u;
+            float xn[2] = {0.f, 0.f};
+            zedge_two (Tab, c, zl, S, u, b, prev.xe1[c], cu[c], prev.im[c], prev.e1[c], cur.e2[c], xn);
+            if (pair_along (c, 2) != 1 && b && store)
+              store_aux (p.aux_new[c] + id, b, xn);
+          }
+        }
+        else if (u != 3u)
+        {
+#pragma unroll
+          for (int j = 0; j < 2; ++j)
+            if (!((u >> j) & 1u))
+#pragma unroll
+              for (int c = 0; c < 3; ++c)
+                cur.e2[c][j] = prev.e1[c][j];
+        }
         if constexpr (kPml)
         {
-          if (mE2)
+          if (prev.mE)
           {
 #pragma unroll
             for (int c = 0; c < 3; ++c)
             {
-              float xn[2] = {0.f, 0.f};
-#pragma unroll
-              for (int j = 0; j < 2; ++j)
-                if ((mE2 >> (2 * c + j)) & 1u)
-                  e2[c][j] = pml_cell<XTW> (Tab, c, i - 1, w, zl + j, xe1p[c][j], cu[c][j], ip[c][j], e1p[c][j], xn[j]);
-              if (store)
+              const unsigned b = (prev.mE >> (2 * c)) & 3u;
+              if (b)
               {
-#pragma unroll
-                for (int j = 0; j < 2; ++j)
-                  if ((mE2 >> (2 * c + j)) & 1u)
-                    __stcs (p.aux_new[c] + id + j, xn[j]);
+                float xn[2] = {0.f, 0.f};
+                pml_two<XTW> (Tab, c, i - 1, w, zl, b, prev.xe1[c], cu[c], prev.im[c], prev.e1[c], cur.e2[c], xn);
+                if (store)
+                  store_aux (p.aux_new[c] + id, b, xn);
               }
             }
           }
@@ -547,17 +706,17 @@ __global__ void __launch_bounds__ (32 * NW, 1)
         {
 #pragma unroll
           for (int c = 0; c < 3; ++c)
-            V2<T>::st (reinterpret_cast<T *> (p.e_new[c]) + id, e2[c]);
+            V2<T>::st (reinterpret_cast<T *> (p.e_new[c]) + id, cur.e2[c]);
         }
-        sts2 (XE2w + 0 * XN + w * ZW + zl, e2[0]);
-        sts2 (XE2w + 1 * XN + w * ZW + zl, e2[2]);
+        sts2 (XE2w + 0 * XN + w * ZW + zl, cur.e2[0]);
+        sts2 (XE2w + 1 * XN + w * ZW + zl, cur.e2[2]);
       }
       if (i >= 4 && w >= 1 && w <= kTb2Yown)
       {
         const int xh = x - 2;
         const unsigned u = (xh >= 1 && xh <= nx - 2) ? cupd : 0u;
-        const float exn = __shfl_down_sync (kLanes, e2p[0][0], 1);
-        const float eyn = __shfl_down_sync (kLanes, e2p[1][0], 1);
+        const float exn = __shfl_down_sync (kLanes, prev.e2[0][0], 1);
+        const float eyn = __shfl_down_sync (kLanes, prev.e2[1][0], 1);
         float exy[2], ezy[2];
         lds2 (XE2r + 0 * XN + (w + 1) * ZW + zl, exy);
         lds2 (XE2r + 1 * XN + (w + 1) * ZW + zl, ezy);
@@ -565,36 +724,57 @@ __global__ void __launch_bounds__ (32 * NW, 1)
 #pragma unroll
         for (int j = 0; j < 2; ++j)
         {
-          const float eyz = j ? eyn : e2p[1][1];
-          const float exz = j ? exn : e2p[0][1];
-          a[0][j] = (eyz - e2p[1][j]) - (ezy[j] - e2p[2][j]);
-          a[1][j] = (e2[2][j] - e2p[2][j]) - (exz - e2p[0][j]);
-          a[2][j] = (exy[j] - e2p[0][j]) - (e2[1][j] - e2p[1][j]);
-          const bool up = (u >> j) & 1u;
-#pragma unroll
-          for (int c = 0; c < 3; ++c)
-            h2[c][j] = up ? h1p[c][j] + S * a[c][j] : h1p[c][j];
-        }
-        const bool store = own && xh >= xa && xh <= xb;
-        const size_t id = (size_t) xh * sx + rowoff;
-        if constexpr (kPml)
-        {
-          if (mH2)
+          const float eyz = j ? eyn : prev.e2[1][1];
+          const float exz = j ? exn : prev.e2[0][1];
+          a[0][j] = (eyz - prev.e2[1][j]) - (ezy[j] - prev.e2[2][j]);
+          a[1][j] = (cur.e2[2][j] - prev.e2[2][j]) - (exz - prev.e2[0][j]);
+          a[2][j] = (exy[j] - prev.e2[0][j]) - (cur.e2[1][j] - prev.e2[1][j]);
+          if constexpr (!kZedge)
           {
 #pragma unroll
             for (int c = 0; c < 3; ++c)
+              h2[c][j] = prev.h1[c][j] + S * a[c][j];
+          }
+        }
+        const bool store = own && xh >= xa && xh <= xb;
+        const size_t id = (size_t) xh * sx + rowoff;
+        if constexpr (kZedge)
+        {
+          const float one[2] = {1.f, 1.f};
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+          {
+            const unsigned b = (prev.mH >> (2 * c)) & 3u;
+            float xn[2] = {0.f, 0.f};
+            zedge_two (Tab, 3 + c, zl, S, u, b, prev.xh1[c], a[c], one, prev.h1[c], h2[c], xn);
+            if (pair_along (3 + c, 2) != 1 && b && store)
+              store_aux (p.aux_new[3 + c] + id, b, xn);
+          }
+        }
+        else if (u != 3u)
+        {
+#pragma unroll
+          for (int j = 0; j < 2; ++j)
+            if (!((u >> j) & 1u))
+#pragma unroll
+              for (int c = 0; c < 3; ++c)
+                h2[c][j] = prev.h1[c][j];
+        }
+        if constexpr (kPml)
+        {
+          if (prev.mH)
+          {
+            const float one[2] = {1.f, 1.f};
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
             {
-              float xn[2] = {0.f, 0.f};
-#pragma unroll
-              for (int j = 0; j < 2; ++j)
-                if ((mH2 >> (2 * c + j)) & 1u)
-                  h2[c][j] = pml_cell<XTW> (Tab, 3 + c, i - 2, w, zl + j, xh1p[c][j], a[c][j], 1.f, h1p[c][j], xn[j]);
-              if (store)
+              const unsigned b = (prev.mH >> (2 * c)) & 3u;
+              if (b)
               {
-#pragma unroll
-                for (int j = 0; j < 2; ++j)
-                  if ((mH2 >> (2 * c + j)) & 1u)
-                    __stcs (p.aux_new[3 + c] + id + j, xn[j]);
+                float xn[2] = {0.f, 0.f};
+                pml_two<XTW> (Tab, 3 + c, i - 2, w, zl, b, prev.xh1[c], a[c], one, prev.h1[c], h2[c], xn);
+                if (store)
+                  store_aux (p.aux_new[3 + c] + id, b, xn);
               }
             }
           }
@@ -607,24 +787,24 @@ __global__ void __launch_bounds__ (32 * NW, 1)
         }
       }
 
-      if constexpr (kPml)
+      if constexpr (kAux)
       {
-        // masks and old auxiliaries of the next plane's first step: E at
-        // x + 1, H at x
-        mE2 = mE1;
-        mH2 = mH1;
-        mE1 = pmask (0, x + 1);
-        mH1 = pmask (3, x);
+        // masks and old auxiliaries of the next plane's first step (E at
+        // x + 1, H at x), into the set the next plane writes
+        prev.mE = pmask (0, x + 1);
+        prev.mH = pmask (3, x);
 #pragma unroll
         for (int c = 0; c < 3; ++c)
         {
-          if ((mE1 >> (2 * c)) & 3u)
+          if (kZedge && pair_along (c, 2) == 1)
+            continue;   // no auxiliary in the z-edge form
+          if ((prev.mE >> (2 * c)) & 3u)
           {
             const float2 v = __ldg (reinterpret_cast<const float2 *> (p.aux_old[c] + (size_t) (x + 1) * sx + rowoff));
             axe[c][0] = v.x;
             axe[c][1] = v.y;
           }
-          if ((mH1 >> (2 * c)) & 3u)
+          if ((prev.mH >> (2 * c)) & 3u)
           {
             const float2 v = __ldg (reinterpret_cast<const float2 *> (p.aux_old[3 + c] + (size_t) x * sx + rowoff));
             axh[c][0] = v.x;
@@ -632,22 +812,23 @@ __global__ void __launch_bounds__ (32 * NW, 1)
           }
         }
       }
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-        {
-          hp[c][j] = hc[c][j];
-          e1p[c][j] = e1[c][j];
-          ip[c][j] = im[c][j];
-          h1p[c][j] = h1[c][j];
-          e2p[c][j] = e2[c][j];
-          if constexpr (kPml)
-          {
-            xe1p[c][j] = xe1[c][j];
-            xh1p[c][j] = xh1[c][j];
-          }
-        }
+      return true;
+    };
+
+    using P0 = std::integral_constant<int, 0>;
+    using P1 = std::integral_constant<int, 1>;
+    for (int i = 0; i < np; i += 2)
+    {
+      if (!plane (i, P0{}, sa, sb))
+      {
+        aborted = true;
+        break;
+      }
+      if (i + 1 < np && !plane (i + 1, P1{}, sb, sa))
+      {
+        aborted = true;
+        break;
+      }
     }
     if (aborted)
       break;
@@ -687,9 +868,9 @@ std::string plan_t (Sweep2Plan &pl, const FusedParams &p, void *const e[2][3], v
       m.eps = m.e[0];   // never used
   }
   int per_sm = 0;
-  for (int mode = 0; mode < 2; ++mode)
+  for (int mode = 0; mode < 3; ++mode)
   {
-    auto kern = mode == 0 ? sweep2_kernel<T, 0> : sweep2_kernel<T, 1>;
+    auto kern = mode == 0 ? sweep2_kernel<T, 0> : (mode == 1 ? sweep2_kernel<T, 1> : sweep2_kernel<T, 2>);
     if (cudaFuncSetAttribute (kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) L::TOTAL) != cudaSuccess)
     {
       cudaGetLastError ();
@@ -720,7 +901,7 @@ int launch_t (const Sweep2Plan &pl, int set, const FusedParams &p, int *err, cud
 {
   const dim3 block (32, NW);
   constexpr unsigned sm = L2<T>::TOTAL;
-  const bool conc = ss.side[0] && pl.items[0] > 0 && pl.items[1] > 0;
+  const bool conc = ss.side[0] && pl.items[0] > 0 && pl.items[1] + pl.items[2] > 0;
   cudaStream_t s0 = s;
   if (conc)
   {
@@ -732,6 +913,11 @@ int launch_t (const Sweep2Plan &pl, int set, const FusedParams &p, int *err, cud
   if (pl.items[1] > 0)
   {
     sweep2_kernel<T, 1><<<pl.ctas, block, sm, s>>> (pl.maps[set], p, pl.work, err);
+    ++n;
+  }
+  if (pl.items[2] > 0)
+  {
+    sweep2_kernel<T, 2><<<pl.ctas, block, sm, s>>> (pl.maps[set], p, pl.work, err);
     ++n;
   }
   if (pl.items[0] > 0)
@@ -750,7 +936,8 @@ int launch_t (const Sweep2Plan &pl, int set, const FusedParams &p, int *err, cud
 }  // namespace
 
 std::string sweep2_plan (Sweep2Plan &plan, const FusedParams &p, void *const e[2][3], void *const h[2][3],
-                         const float *eps, int sm_count, int chunk, unsigned long long *ctr)
+                         const float *eps, int sm_count, int chunk, unsigned long long *ctr, int x0, int x1, int y0,
+                         int y1)
 {
   const int *n = p.g.n;
   chunk = std::min (std::max (chunk, 1), kTb2MaxChunk);
@@ -767,16 +954,24 @@ std::string sweep2_plan (Sweep2Plan &plan, const FusedParams &p, void *const e[2
     return "nz is not a multiple of one 16-byte unit";
   if (n[0] < 3 || n[1] < 3 || n[2] < 3)
     return "grid too small";
+  if (x1 < 0)
+    x1 = n[0] - 1;
+  if (y1 < 0)
+    y1 = n[1] - 1;
+  if (x0 < 1 || x1 > n[0] - 1 || x0 >= x1 || y0 < 1 || y1 > n[1] - 1 || y0 >= y1)
+    return "bad owned range";
   std::string why = p.fp16 ? plan_t<__half> (plan, p, e, h, eps, sm_count)
                            : plan_t<float> (plan, p, e, h, eps, sm_count);
   if (!why.empty ())
     return why;
   Sweep2Work &w = plan.work;
-  w.nyt = (n[1] - 2 + kTb2Yown - 1) / kTb2Yown;
-  // x chunks of about `chunk` planes over the updated planes 1 .. nx - 2;
+  w.yoff = y0 - 1;
+  w.yend = y1;
+  w.nyt = (y1 - y0 + kTb2Yown - 1) / kTb2Yown;
+  // x chunks of about `chunk` planes over the owned planes x0 .. x1 - 1;
   // with PML, the planes where every component is PML-free (with the two
   // halo planes) form their own segment, so that no chunk mixes them
-  std::vector<int> seg = {1};
+  std::vector<int> seg = {x0};
   if (p.use_pml)
   {
     int lo = 1, hi = n[0] - 2;
@@ -785,14 +980,14 @@ std::string sweep2_plan (Sweep2Plan &plan, const FusedParams &p, void *const e[2
       lo = std::max (lo, p.ilo[k][0] + 2);
       hi = std::min (hi, p.ihi[k][0] - 3);
     }
-    if (lo > 1 && lo <= hi)
+    if (lo > x0 && lo < x1 && lo <= hi)
       seg.push_back (lo);
-    if (hi + 1 <= n[0] - 2 && lo <= hi)
+    if (hi + 1 > x0 && hi + 1 < x1 && lo <= hi)
       seg.push_back (hi + 1);
   }
-  seg.push_back (n[0] - 1);
+  seg.push_back (x1);
   w.nch = 0;
-  w.xcut[0] = 1;
+  w.xcut[0] = x0;
   for (size_t sg = 0; sg + 1 < seg.size (); ++sg)
   {
     const int len = seg[sg + 1] - seg[sg];
@@ -806,7 +1001,7 @@ std::string sweep2_plan (Sweep2Plan &plan, const FusedParams &p, void *const e[2
       return "grid too long in x for the staged PML coefficients";
   w.nitems = w.nzt * w.nyt * w.nch;
   w.ctr = ctr;
-  plan.items[0] = plan.items[1] = 0;
+  plan.items[0] = plan.items[1] = plan.items[2] = 0;
   for (int it = 0; it < w.nitems; ++it)
     ++plan.items[sweep2_item_class (p, w, it)];
   if (plan.ctas > w.nitems)

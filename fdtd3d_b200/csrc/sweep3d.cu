@@ -495,7 +495,10 @@ __global__ void __launch_bounds__ (32 * WY, 1)
   for (;;)
   {
     if (leader)
-      s_item[grab & 1u] = (int) atomicAdd (wk.ctr + 2 * MODE, 1ull);
+    {
+      const int idx = (int) atomicAdd (wk.ctr + 2 * MODE, 1ull);
+      s_item[grab & 1u] = wk.list ? (idx < wk.nlist ? wk.list[idx] : wk.nitems) : idx;
+    }
     __syncthreads ();
     const int item = s_item[grab & 1u];
     ++grab;
@@ -1330,6 +1333,8 @@ void sweep3d_items (const FusedParams &p, int wy, int chunk, SweepWork &w)
       w.xcut[++w.nch] = seg[sg] + (int) ((long long) len * j / m);
   }
   w.nitems = w.nzt * w.nyt * w.nch;
+  w.list = nullptr;
+  w.nlist = 0;
 }
 
 std::string sweep3d_plan (SweepPlan &plan, const FusedParams &p, void *const e[2][3], void *const h[2][3],
@@ -1364,6 +1369,43 @@ std::string sweep3d_plan (SweepPlan &plan, const FusedParams &p, void *const e[2
     ++plan.items[sweep_item_class (p, plan.work, wy, it, tfsf_in)];
   if (plan.ctas > plan.work.nitems)
     plan.ctas = plan.work.nitems;
+  return "";
+}
+
+std::string sweep3d_plan_list (SweepPlan &plan, const FusedParams &p, void *const e[2][3], void *const h[2][3],
+                               float *const aux[2][6], const float *eps, int sm_count, const std::vector<int> &cuts,
+                               const std::vector<int> &host_list, int *dev_list, unsigned long long *ctr,
+                               cudaStream_t s)
+{
+  std::string why = sweep3d_plan (plan, p, e, h, aux, eps, sm_count, 8, 32, ctr, true);
+  if (!why.empty ())
+    return why;
+  if (cuts.size () < 2 || cuts.size () > (size_t) kMaxChunks + 1 || cuts.front () != 1 ||
+      cuts.back () != p.g.n[0] - 1)
+    return "bad x cuts";
+  SweepWork &w = plan.work;
+  w.nch = (int) cuts.size () - 1;
+  for (int j = 0; j <= w.nch; ++j)
+    w.xcut[j] = cuts[j];
+  for (int j = 0; j < w.nch; ++j)
+    if (w.xcut[j + 1] <= w.xcut[j] || (p.use_pml && w.xcut[j + 1] - w.xcut[j] > MAXC))
+      return "bad x cuts";
+  w.chunk = 0;
+  w.nitems = w.nzt * w.nyt * w.nch;
+  for (int it : host_list)
+    if (it < 0 || it >= w.nitems)
+      return "item out of range";
+  w.list = dev_list;
+  w.nlist = (int) host_list.size ();
+  if (!host_list.empty () &&
+      cudaMemcpyAsync (dev_list, host_list.data (), host_list.size () * sizeof (int), cudaMemcpyHostToDevice, s) !=
+          cudaSuccess)
+    return "item list upload failed";
+  const bool tfsf_in = p.use_tfsf && !p.tfsf_post;
+  plan.items[0] = plan.items[1] = plan.items[2] = plan.items[3] = 0;
+  for (int it : host_list)
+    ++plan.items[sweep_item_class (p, w, 8, it, tfsf_in)];
+  plan.ctas = std::min (plan.ctas, std::max (1, w.nlist));
   return "";
 }
 

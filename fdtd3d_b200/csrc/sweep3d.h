@@ -38,6 +38,8 @@ struct SweepWork
   int lean;                    // 0: every item goes to the full class
   unsigned long long *ctr;     // per item class c: [2c] next item, [2c + 1] CTAs finished; the last
                                // CTA of a launch resets both
+  const int *list;             // device list of the items to run (null: items 0 .. nitems - 1)
+  int nlist;                   // its length
 };
 
 struct SweepPlan
@@ -61,6 +63,21 @@ void sweep3d_items (const FusedParams &p, int wy, int chunk, SweepWork &w);
 std::string sweep3d_plan (SweepPlan &plan, const FusedParams &p, void *const e[2][3], void *const h[2][3],
                           float *const aux[2][6], const float *eps, int sm_count, int wy, int chunk,
                           unsigned long long *ctr, bool lean = true);
+
+// A plan that runs only some items: x chunks cut at `cuts` (increasing, from
+// 1 to nx - 1), and the items of `host_list` (ids over the z tile, y tile and
+// x chunk grid of those cuts), copied to the device array `dev_list` (at least
+// host_list.size () ints, owned by the caller).  Used for the PML shell of the
+// two-step scheme.
+std::string sweep3d_plan_list (SweepPlan &plan, const FusedParams &p, void *const e[2][3], void *const h[2][3],
+                               float *const aux[2][6], const float *eps, int sm_count, const std::vector<int> &cuts,
+                               const std::vector<int> &host_list, int *dev_list, unsigned long long *ctr,
+                               cudaStream_t s);
+
+// Tiles of the single-step sweep (8-warp CTAs): z tile zt owns z cells
+// 128 zt .. 128 zt + 127, y tile yt rows 1 + 7 yt .. 7 + 7 yt.
+constexpr int kSweepTileZ = 128;
+constexpr int kSweepTileY = 7;
 
 // Side streams for the item classes: the classes of one step write disjoint
 // items and read only the old set, so they may run concurrently; then the

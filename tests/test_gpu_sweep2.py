@@ -115,16 +115,21 @@ PML_CASES = {
     "pml_all_faces": dict(size=(62, 44, 128), pml=(5, 6, 7), steps=9),
     # thick z PML only in the last z tile, thin x / y PML, odd update count
     "pml_thick_z": dict(size=(40, 30, 120), pml=(3, 3, 16), steps=8),
+    # a core of several two-step tiles and x chunks inside a PML shell of
+    # several single-step tiles on every side
+    "pml_large_core": dict(size=(150, 96, 200), pml=(10, 9, 12), steps=9),
 }
 
 
 @pytest.mark.parametrize("case", sorted(PML_CASES))
 def test_fp32_pairs_with_pml_match_single_steps(fdtd, monkeypatch, case):
-    """With PML the two-step kernel evaluates every PML cell with the general
-    PML form, where the single-step kernel uses a rearranged form on cells
-    whose only PML axis is z: the two agree to FP32 rounding (<= 1e-6
-    relative L2 per field family) and the auxiliary state they carry agrees
-    as well (checked through the fields of later steps)."""
+    """With PML, the x / y PML slabs (and a 2-cell margin) take two single
+    steps through a third buffer set while the two-step kernel advances the
+    rest; it evaluates the z PML cells with the general PML form, where the
+    single-step kernel uses a rearranged form on cells whose only PML axis is
+    z: the two agree to FP32 rounding (<= 1e-6 relative L2 per field family)
+    and the auxiliary state they carry agrees as well (checked through the
+    fields of later steps)."""
     spec = PML_CASES[case]
     shape = spec["size"]
     fields, eps = _inputs(shape, 17 + len(case))
