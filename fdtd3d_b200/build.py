@@ -48,7 +48,7 @@ def _units():
     ]
     if os.path.exists(os.path.join(CSRC, "fused3d.cu")):
         units.append(("fused3d.cu", [nvcc] + common))
-    for extra in ("sweep3d.cu", "sweep2.cu", "tmz_batch.cu", "adjoint.cu", "noalloc.cu", "ntff.cu"):
+    for extra in ("sweep3d.cu", "sweep2.cu", "tfsf2.cu", "tmz_batch.cu", "adjoint.cu", "noalloc.cu", "ntff.cu"):
         if os.path.exists(os.path.join(CSRC, extra)):
             units.append((extra, [nvcc] + common))
     return units

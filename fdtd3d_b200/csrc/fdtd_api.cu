@@ -25,6 +25,7 @@
 #include "adjoint.h"
 #include "fused3d.h"
 #include "sweep2.h"
+#include "tfsf2.h"
 #include "sweep3d.h"
 #include "kernels.h"
 #include "ntff.h"
@@ -148,6 +149,12 @@ struct fdtd_ctx
   float *tauxb[6] = {};                   // set T: PML auxiliaries
   cudaStream_t core_stream = nullptr;
   cudaEvent_t core_fork = nullptr, core_join = nullptr;
+  // TF/SF with the two-step scheme: the pair's corrections (tfsf2.cu), and a
+  // copy of the incident H level the first step's E corrections read (the
+  // second step's H-incident update overwrites it)
+  Tf2Pass tf2;
+  bool tf2_on = false;
+  double *hinc_keep = nullptr;
   TfsfBand band;                          // TF/SF post pass of the sweep (band.cells > 0 when in use)
   std::vector<BandBox> band_host;         // its boxes, on the host
   // metamaterials with the sweep: the box of the Drude cells, fixed up after
@@ -842,7 +849,7 @@ std::string plan_shell (fdtd_ctx *ctx, void *const e[2][3], void *const h[2][3],
                            ctx->shell_ctr[1], ctx->stream);
   if (!why.empty ())
     return "shell step 2: " + why;
-  why = sweep2_plan (ctx->tb2, f, e, h, ctx->mat32[0], ctx->sm_count, 64, ctx->tb2_ctr, cx0, cx1, cy0, cy1);
+  why = sweep2_plan (ctx->tb2, f, e, h, aux, ctx->mat32[0], ctx->sm_count, 64, ctx->tb2_ctr, cx0, cx1, cy0, cy1);
   if (!why.empty ())
     return "core: " + why;
   if (!ctx->core_stream)
@@ -854,6 +861,63 @@ std::string plan_shell (fdtd_ctx *ctx, void *const e[2][3], void *const h[2][3],
   }
   if (cudaStreamSynchronize (ctx->stream) != cudaSuccess)
     return "shell set-up failed";
+  return "";
+}
+
+// TF/SF with the two-step scheme: the regions of the pair's correction
+// passes (which must keep two cells clear of the PML shell the single steps
+// take), their CTA tables and scratch arrays.
+std::string plan_tfsf2 (fdtd_ctx *ctx)
+{
+  std::vector<Tf2Box> rg[3];
+  std::string why = tfsf2_regions (ctx->fused, rg);
+  if (!why.empty ())
+    return why;
+  if (ctx->tb2_state == 2)
+  {
+    const Sweep2Work &w = ctx->tb2.work;
+    const int cx0 = w.xcut[0], cx1 = w.xcut[w.nch], cy0 = w.yoff + 1, cy1 = w.yend;
+    for (int q = 0; q < 3; ++q)
+      for (const Tf2Box &b : rg[q])
+        if (b.lo[0] < cx0 + 2 || b.hi[0] > cx1 - 2 || b.lo[1] < cy0 + 2 || b.hi[1] > cy1 - 2)
+          return "the TF/SF corrections reach the PML shell";
+  }
+  std::vector<int2> bl[3];
+  for (int q = 0; q < 3; ++q)
+    if (!(why = tfsf2_blocks (rg[q], bl[q])).empty ())
+      return why;
+  Tf2Pass &t = ctx->tf2;
+  const Geometry &g = ctx->g;
+  const size_t n = (size_t) g.cells;
+  if (!t.scratch[0])
+  {
+    for (int k = 0; k < 6; ++k)
+      if (dalloc (ctx, (void **) &t.scratch[k], n * sizeof (float)) != FDTD_OK)
+        return "allocation of the TF/SF scratch failed";
+    if (dalloc (ctx, (void **) &ctx->hinc_keep, (size_t) g.inc_len * sizeof (double)) != FDTD_OK)
+      return "allocation of the TF/SF scratch failed";
+  }
+  // tables (re)allocated at their sizes
+  auto upload = [&] (void **dst, const void *src, size_t bytes) -> bool {
+    if (dalloc (ctx, dst, bytes, false) != FDTD_OK)
+      return false;
+    return cudaMemcpyAsync (*dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream) == cudaSuccess;
+  };
+  for (int q = 0; q < 3; ++q)
+  {
+    if (!upload ((void **) &t.boxes[q], rg[q].data (), rg[q].size () * sizeof (Tf2Box)) ||
+        !upload ((void **) &t.blk[q], bl[q].data (), bl[q].size () * sizeof (int2)))
+      return "upload of the TF/SF tables failed";
+    t.nblk[q] = (int) bl[q].size ();
+  }
+  // the scratch must be zero outside the regions: clear it whenever they may
+  // have changed
+  for (int k = 0; k < 6; ++k)
+    if (cudaMemsetAsync (t.scratch[k], 0, n * sizeof (float), ctx->stream) != cudaSuccess)
+      return "TF/SF scratch clear failed";
+  if (cudaStreamSynchronize (ctx->stream) != cudaSuccess)
+    return "TF/SF set-up failed";
+  ctx->tf2_on = true;
   return "";
 }
 
@@ -1019,9 +1083,15 @@ int plan_sweep (fdtd_ctx *ctx)
       }
       else
       {
-        ctx->tb2_why = sweep2_plan (ctx->tb2, ctx->fused, e, h, ctx->mat32[0], ctx->sm_count, 64, ctx->tb2_ctr);
+        ctx->tb2_why = sweep2_plan (ctx->tb2, ctx->fused, e, h, aux, ctx->mat32[0], ctx->sm_count, 64, ctx->tb2_ctr);
         if (ctx->tb2_why.empty ())
           ctx->tb2_state = 1;
+      }
+      if (ctx->tb2_state >= 1 && g.cfg.use_tfsf)
+      {
+        ctx->tb2_why = plan_tfsf2 (ctx);
+        if (!ctx->tb2_why.empty ())
+          ctx->tb2_state = -1;
       }
     }
   }
@@ -1379,8 +1449,26 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
       cudaEvent_t pe;
       if (ctx->tb2_state >= 1 && i + 1 < n && ctx->dft_comp < 0)
       {
-        // steps t and t + 1 in one pass (no TF/SF, point source or Drude
-        // medium: the incident grid is not stepped)
+        // steps t and t + 1 in one pass (no point source or Drude medium).
+        // With TF/SF the incident grid takes both steps first (this step's
+        // E and H updates were issued above), keeping the levels the pair's
+        // corrections read
+        const double *inc_h1 = nullptr, *inc_e1 = nullptr, *inc_h2 = nullptr, *inc_e2 = nullptr;
+        if (g.cfg.use_tfsf)
+        {
+          CK (cudaMemcpyAsync (ctx->hinc_keep, ctx->hinc[hprev], (size_t) g.inc_len * sizeof (double),
+                               cudaMemcpyDeviceToDevice, s));
+          inc_h1 = ctx->hinc_keep;
+          inc_e1 = ctx->einc[ctx->ecur];
+          inc_h2 = ctx->hinc[ctx->hcur];
+          ctx->launches += launch_incident_e (ctx->einc[1 - ctx->ecur], ctx->einc[ctx->ecur], ctx->hinc[ctx->hcur],
+                                              g.inc_len, g.mod_e, ctx->d_src, kSrcStride * (i + 1), s);
+          ctx->ecur ^= 1;
+          inc_e2 = ctx->einc[ctx->ecur];
+          ctx->launches += launch_incident_h (ctx->hinc[1 - ctx->hcur], ctx->hinc[ctx->hcur], ctx->einc[ctx->ecur],
+                                              g.inc_len, g.mod_h, s);
+          ctx->hcur ^= 1;
+        }
         if ((r = prof_begin (ctx, &pe)) != FDTD_OK)
           return r;
         if (ctx->tb2_state == 1)
@@ -1406,6 +1494,8 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
           CK (cudaEventRecord (ctx->core_join, ctx->core_stream));
           CK (cudaStreamWaitEvent (s, ctx->core_join, 0));
         }
+        if (g.cfg.use_tfsf)
+          ctx->launches += launch_tfsf2 (ctx->tf2, f, inc_h1, inc_e1, inc_h2, inc_e2, ctx->d_err, s);
         ctx->step_kernel = "sweep2_tma";
         if ((r = prof_end (ctx, pe)) != FDTD_OK)
           return r;

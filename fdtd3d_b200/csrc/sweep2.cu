@@ -67,25 +67,25 @@ struct L2
   static constexpr unsigned H_B = rnd (sizeof (T) * HW * HR);
   static constexpr unsigned E_B = rnd (sizeof (T) * EW * ER);
   static constexpr unsigned P_B = rnd (4u * PW * PR);
+  static constexpr unsigned A_B = rnd (4u * ZW * NW);   // one auxiliary box (float): zs .. zs + 63 x Y .. Y + 15
   static constexpr unsigned OFF_E = 3 * H_B;
   static constexpr unsigned OFF_P = OFF_E + 3 * E_B;
-  static constexpr unsigned STAGE = OFF_P + 2 * P_B;
+  // z-edge class: old auxiliaries of Ey, Ez at x and Hy, Hz at x - 1
+  static constexpr unsigned OFF_A = OFF_P + 2 * P_B;
+  static constexpr unsigned STAGE = OFF_A + 4 * A_B;
   // exchange rows, NW x ZW floats each: XE1[parity][Ex, Ez],
   // XH1[parity][Hx, Hz], XE2[parity][Ex, Ez]
   static constexpr int XN = NW * ZW;
   static constexpr unsigned OFF_X = NST2 * STAGE;
-  // PML coefficient pairs of the item (PML class): per component k and pair
-  // element e, along z [(2k + e) ZW + column], y [(2k + e) NW + row],
-  // x [(2k + e) XTW + plane - (xa - 2)]
-  static constexpr int XTW = kTb2MaxChunk + 4;
-  static constexpr int TY0 = 12 * ZW;
-  static constexpr int TX0 = TY0 + 12 * NW;
+  // z-edge class: the item's z coefficient pairs, pre-combined, per
+  // component k and element e at [(2k + e) ZW + column]
   static constexpr unsigned OFF_T = OFF_X + 12u * 4u * XN;
-  static constexpr unsigned OFF_BAR = OFF_T + rnd (4u * (TX0 + 12 * XTW));
+  static constexpr unsigned OFF_BAR = OFF_T + rnd (4u * 12 * ZW);
   static constexpr unsigned TOTAL = OFF_BAR + 64 + 128;   // + room to align the base to 128 bytes
   // bytes each stage's copies deliver (full boxes, fill included)
   static constexpr unsigned TX_HE = 3u * sizeof (T) * HW * HR + 3u * sizeof (T) * EW * ER;
   static constexpr unsigned TX_P = 2u * 4u * PW * PR;
+  static constexpr unsigned TX_A = 4u * 4u * ZW * NW;
 };
 
 template <typename T>
@@ -158,50 +158,6 @@ __device__ __forceinline__ int pair_along (int k, int axis)
   return (k + 1) % 3 == axis ? 0 : ((k + 2) % 3 == axis ? 1 : 2);
 }
 
-// Axis along which coefficient pair q (0: ca1, sq1; 1: p5, q5; 2: g4p, g4m)
-// of component k runs: the reference's sigma choice per component
-// (InternalScheme.inc.h:2551-2640), as the single-step kernels stage it.
-__device__ __forceinline__ int pair_axis (int k, int q)
-{
-  const int a = k % 3;
-  return q == 0 ? (a + 1) % 3 : (q == 1 ? (a + 2) % 3 : a);
-}
-
-// PML update of component k on a lane's two cells (the single-step kernels'
-// pml_vec), on the cells of `bits`:
-//   X_new = ca1 X + sq1 curl,  F_new = p5 F + (g4p X_new - g4m X) q5 im;
-// fn gets F_new, xn X_new there.  Coefficient pairs come from the item's
-// staged tables: along x at plane index xi, along y at row w, along z at the
-// columns zcol, zcol + 1.
-template <int XTW>
-__device__ __forceinline__ void pml_two (const float *T, int k, int xi, int w, int zcol, unsigned bits,
-                                         const float xo[2], const float cu[2], const float im[2], const float fo[2],
-                                         float fn[2], float xn[2])
-{
-  float c[3][2][2];   // [pair][element][cell]
-#pragma unroll
-  for (int q = 0; q < 3; ++q)
-#pragma unroll
-    for (int e = 0; e < 2; ++e)
-    {
-      const int a = pair_axis (k, q);
-      if (a == 2)
-        lds2 (T + (2 * k + e) * ZW + zcol, c[q][e]);
-      else
-        c[q][e][0] = c[q][e][1] =
-            a == 0 ? T[12 * ZW + 12 * NW + (2 * k + e) * XTW + xi] : T[12 * ZW + (2 * k + e) * NW + w];
-    }
-#pragma unroll
-  for (int j = 0; j < 2; ++j)
-  {
-    const float n = c[0][0][j] * xo[j] + c[0][1][j] * cu[j];
-    const float f = c[1][0][j] * fo[j] + (c[2][0][j] * n - c[2][1][j] * xo[j]) * c[1][1][j] * im[j];
-    const bool on = (bits >> j) & 1u;
-    fn[j] = on ? f : fn[j];
-    xn[j] = on ? n : xn[j];
-  }
-}
-
 // z-edge items (x and y interior for every component, PML cells only along
 // z): the single-step kernel's branch-free form, in which only the z pair
 // of each component differs from the sigma = 0 identity and the item's z
@@ -244,14 +200,13 @@ __device__ __forceinline__ void zedge_two (const float *Tz, int k, int zl, float
 }
 
 // MODE 0 (lean): no cell of the item's extended region is a PML cell of any
-// component.  MODE 1 (PML): PML cells anywhere; each lane updates the cells
-// that are PML cells of a component with the PML form (masks per component
-// and cell, coefficients from the 1-D tables), carries the auxiliary of the
-// first step in registers to the second, and loads the old auxiliaries one
-// plane ahead with plain loads (only lanes with PML cells).  MODE 2 (z
-// edge): PML cells only along z; every lane runs the branch-free z-edge form
-// (zedge_two), auxiliaries as in MODE 1 but only for the four components
-// that keep one.
+// component.  MODE 2 (z edge): PML cells only along z; every lane runs the
+// branch-free z-edge form (zedge_two), carries the first step's auxiliaries
+// in registers to the second, and loads the old auxiliaries of the four
+// components that keep one a plane ahead with plain loads (lanes with PML
+// cells only), issued at the start of the plane before so that a whole
+// plane hides their latency.  (Class 1, x or y PML cells, is left to the
+// single-step kernels: the two-step plan refuses it.)
 template <typename T, int MODE>
 __global__ void __launch_bounds__ (32 * NW, 1)
     sweep2_kernel (const __grid_constant__ Sweep2Maps maps, const __grid_constant__ FusedParams p,
@@ -261,9 +216,8 @@ __global__ void __launch_bounds__ (32 * NW, 1)
   constexpr int HZ = L::HZ, HW = L::HW, EW = L::EW, PW = L::PW, XN = L::XN;
   constexpr int HS = L::H_B / sizeof (T), ES = L::E_B / sizeof (T), PS = L::P_B / sizeof (float);
   constexpr unsigned kLanes = 0xffffffffu;
-  constexpr bool kPml = MODE == 1;
   constexpr bool kZedge = MODE == 2;
-  constexpr bool kAux = kPml || kZedge;   // PML masks and auxiliaries
+  constexpr bool kAux = kZedge;   // PML masks and auxiliaries
   extern __shared__ __align__ (128) unsigned char smem_raw[];
   __shared__ int s_item;
   __shared__ int s_abort;
@@ -280,7 +234,6 @@ __global__ void __launch_bounds__ (32 * NW, 1)
   const float S = p.courant;
   float *const X = reinterpret_cast<float *> (smem + L::OFF_X);
   float *const Tab = reinterpret_cast<float *> (smem + L::OFF_T);
-  constexpr int XTW = L::XTW;
 
   if (leader)
   {
@@ -296,7 +249,17 @@ __global__ void __launch_bounds__ (32 * NW, 1)
   auto issue = [&] (int st, int x, int zs, int Y) {
     const uint32_t s = sbase + st * L::STAGE;
     const uint32_t b = bar + 8 * st;
-    tma::mbar_expect_tx (b, L::TX_HE + (has_eps ? L::TX_P : 0u));
+    tma::mbar_expect_tx (b, L::TX_HE + (has_eps ? L::TX_P : 0u) + (kAux ? L::TX_A : 0u));
+    if (kAux)
+    {
+      // the components that keep an auxiliary in the z-edge form: Ey, Ez, Hy, Hz
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+      {
+        const int k = q < 2 ? 1 + q : 2 + q;
+        tma::load_3d (s + L::OFF_A + q * L::A_B, &maps.aux[k], zs, Y, k < 3 ? x : x - 1, b);
+      }
+    }
 #pragma unroll
     for (int c = 0; c < 3; ++c)
       tma::load_3d (s + c * L::H_B, &maps.h[c], zs - HZ, Y - 1, x, b);
@@ -312,7 +275,7 @@ __global__ void __launch_bounds__ (32 * NW, 1)
 
   unsigned phase = 0;   // bit s: parity of the next completion of stage s
   bool aborted = false;
-  static_assert (MODE >= 0 && MODE <= 2, "item class");
+  static_assert (MODE == 0 || MODE == 2, "item class");
   for (;;)
   {
     __syncthreads ();   // every thread has read the previous item's index
@@ -368,30 +331,6 @@ __global__ void __launch_bounds__ (32 * NW, 1)
         Tab[(2 * k + 1) * ZW + col] = c1;
       }
     }
-    if constexpr (kPml)
-    {
-      // the item's PML coefficient pairs (read after the first plane's
-      // barrier; coordinates outside the grid take the edge value, which no
-      // updated cell reads)
-      const int tid = w * 32 + lane;
-      for (int q = tid; q < 12 * ZW; q += 32 * NW)
-      {
-        const int k = q / (2 * ZW), e = (q / ZW) % 2, col = q % ZW;
-        const int z = min (max (zs + col, 0), nz - 1);
-        Tab[q] = __ldg (p.tab[k][2 * pair_along (k, 2) + e] + z);
-      }
-      for (int q = tid; q < 12 * NW; q += 32 * NW)
-      {
-        const int k = q / (2 * NW), e = (q / NW) % 2, row = min (max (Y + q % NW, 0), ny - 1);
-        Tab[12 * ZW + q] = __ldg (p.tab[k][2 * pair_along (k, 1) + e] + row);
-      }
-      for (int q = tid; q < 12 * XTW; q += 32 * NW)
-      {
-        const int k = q / (2 * XTW), e = (q / XTW) % 2, xx = min (max (xa - 2 + q % XTW, 0), nx - 1);
-        Tab[12 * ZW + 12 * NW + q] = __ldg (p.tab[k][2 * pair_along (k, 0) + e] + xx);
-      }
-    }
-
     // ---- per-lane constants of this item
     const int r = Y + w;
     const int zl = 2 * lane;
@@ -444,13 +383,8 @@ __global__ void __launch_bounds__ (32 * NW, 1)
       float e2[3][2];    // E2 of the plane before
       float xe1[3][2];   // PML: X of E after the first step on the plane
       float xh1[3][2];   // PML: X of H after the first step on the plane before
-      unsigned mE, mH;   // PML cells: E on the plane, H on the plane before (pmask bits)
     };
     PlaneState sa = {}, sb = {};
-    // PML: old auxiliaries loaded one plane ahead (E of the plane, H of the plane before)
-    float axe[3][2] = {}, axh[3][2] = {};
-    (void) axe;
-    (void) axh;
 
     auto plane = [&] (int i, auto par_c, PlaneState &cur, PlaneState &prev) __attribute__ ((always_inline)) -> bool {
       constexpr int P = decltype (par_c)::value;
@@ -466,6 +400,7 @@ __global__ void __launch_bounds__ (32 * NW, 1)
       const T *sH = reinterpret_cast<const T *> (stg);
       const T *sE = reinterpret_cast<const T *> (stg + L::OFF_E);
       const float *sP = reinterpret_cast<const float *> (stg + L::OFF_P);
+      const float *sA = reinterpret_cast<const float *> (stg + L::OFF_A);
       // exchange rows by plane parity: this plane's (written) and the
       // previous plane's (read).  Every set is rewritten two planes after it
       // was written, and the one barrier per plane lies between its readers
@@ -532,10 +467,15 @@ __global__ void __launch_bounds__ (32 * NW, 1)
         }
         if constexpr (kZedge)
         {
+          const unsigned m = pmask (0, x);
 #pragma unroll
           for (int c = 0; c < 3; ++c)
-            zedge_two (Tab, c, zl, S, u, (cur.mE >> (2 * c)) & 3u, axe[c], cu[c], cur.im[c], eo[c], cur.e1[c],
-                       cur.xe1[c]);
+          {
+            float xo[2] = {0.f, 0.f};
+            if (c > 0)
+              lds2 (sA + (c - 1) * (L::A_B / 4) + w * ZW + zl, xo);
+            zedge_two (Tab, c, zl, S, u, (m >> (2 * c)) & 3u, xo, cu[c], cur.im[c], eo[c], cur.e1[c], cur.xe1[c]);
+          }
         }
         else if (u != 3u)   // cells the step does not update keep their values (grid faces)
         {
@@ -545,17 +485,6 @@ __global__ void __launch_bounds__ (32 * NW, 1)
 #pragma unroll
               for (int c = 0; c < 3; ++c)
                 cur.e1[c][j] = eo[c][j];
-        }
-        if constexpr (kPml)
-        {
-          if (cur.mE)
-          {
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-              if ((cur.mE >> (2 * c)) & 3u)
-                pml_two<XTW> (Tab, c, i, w, zl, (cur.mE >> (2 * c)) & 3u, axe[c], cu[c], cur.im[c], eo[c],
-                              cur.e1[c], cur.xe1[c]);
-          }
         }
         sts2 (XE1w + 0 * XN + w * ZW + zl, cur.e1[0]);
         sts2 (XE1w + 1 * XN + w * ZW + zl, cur.e1[2]);
@@ -590,10 +519,15 @@ __global__ void __launch_bounds__ (32 * NW, 1)
         if constexpr (kZedge)
         {
           const float one[2] = {1.f, 1.f};
+          const unsigned m = pmask (3, xh);
 #pragma unroll
           for (int c = 0; c < 3; ++c)
-            zedge_two (Tab, 3 + c, zl, S, u, (cur.mH >> (2 * c)) & 3u, axh[c], a[c], one, prev.h0[c], cur.h1[c],
-                       cur.xh1[c]);
+          {
+            float xo[2] = {0.f, 0.f};
+            if (c > 0)
+              lds2 (sA + (1 + c) * (L::A_B / 4) + w * ZW + zl, xo);
+            zedge_two (Tab, 3 + c, zl, S, u, (m >> (2 * c)) & 3u, xo, a[c], one, prev.h0[c], cur.h1[c], cur.xh1[c]);
+          }
         }
         else if (u != 3u)
         {
@@ -603,18 +537,6 @@ __global__ void __launch_bounds__ (32 * NW, 1)
 #pragma unroll
               for (int c = 0; c < 3; ++c)
                 cur.h1[c][j] = prev.h0[c][j];
-        }
-        if constexpr (kPml)
-        {
-          if (cur.mH)
-          {
-            const float one[2] = {1.f, 1.f};
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-              if ((cur.mH >> (2 * c)) & 3u)
-                pml_two<XTW> (Tab, 3 + c, i - 1, w, zl, (cur.mH >> (2 * c)) & 3u, axh[c], a[c], one, prev.h0[c],
-                              cur.h1[c], cur.xh1[c]);
-          }
         }
         sts2 (XH1 + 0 * XN + w * ZW + zl, cur.h1[0]);
         sts2 (XH1 + 1 * XN + w * ZW + zl, cur.h1[2]);
@@ -665,10 +587,11 @@ __global__ void __launch_bounds__ (32 * NW, 1)
         const size_t id = (size_t) xe * sx + rowoff;
         if constexpr (kZedge)
         {
+          const unsigned mE2 = pmask (0, xe);
 #pragma unroll
           for (int c = 0; c < 3; ++c)
           {
-            const unsigned b = (prev.mE >> (2 * c)) & 3u;
+            const unsigned b = (mE2 >> (2 * c)) & 3u;
             float xn[2] = {0.f, 0.f};
             zedge_two (Tab, c, zl, S, u, b, prev.xe1[c], cu[c], prev.im[c], prev.e1[c], cur.e2[c], xn);
             if (pair_along (c, 2) != 1 && b && store)
@@ -683,24 +606,6 @@ __global__ void __launch_bounds__ (32 * NW, 1)
 #pragma unroll
               for (int c = 0; c < 3; ++c)
                 cur.e2[c][j] = prev.e1[c][j];
-        }
-        if constexpr (kPml)
-        {
-          if (prev.mE)
-          {
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-            {
-              const unsigned b = (prev.mE >> (2 * c)) & 3u;
-              if (b)
-              {
-                float xn[2] = {0.f, 0.f};
-                pml_two<XTW> (Tab, c, i - 1, w, zl, b, prev.xe1[c], cu[c], prev.im[c], prev.e1[c], cur.e2[c], xn);
-                if (store)
-                  store_aux (p.aux_new[c] + id, b, xn);
-              }
-            }
-          }
         }
         if (store)
         {
@@ -741,10 +646,11 @@ __global__ void __launch_bounds__ (32 * NW, 1)
         if constexpr (kZedge)
         {
           const float one[2] = {1.f, 1.f};
+          const unsigned mH2 = pmask (3, xh);
 #pragma unroll
           for (int c = 0; c < 3; ++c)
           {
-            const unsigned b = (prev.mH >> (2 * c)) & 3u;
+            const unsigned b = (mH2 >> (2 * c)) & 3u;
             float xn[2] = {0.f, 0.f};
             zedge_two (Tab, 3 + c, zl, S, u, b, prev.xh1[c], a[c], one, prev.h1[c], h2[c], xn);
             if (pair_along (3 + c, 2) != 1 && b && store)
@@ -760,25 +666,6 @@ __global__ void __launch_bounds__ (32 * NW, 1)
               for (int c = 0; c < 3; ++c)
                 h2[c][j] = prev.h1[c][j];
         }
-        if constexpr (kPml)
-        {
-          if (prev.mH)
-          {
-            const float one[2] = {1.f, 1.f};
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-            {
-              const unsigned b = (prev.mH >> (2 * c)) & 3u;
-              if (b)
-              {
-                float xn[2] = {0.f, 0.f};
-                pml_two<XTW> (Tab, 3 + c, i - 2, w, zl, b, prev.xh1[c], a[c], one, prev.h1[c], h2[c], xn);
-                if (store)
-                  store_aux (p.aux_new[3 + c] + id, b, xn);
-              }
-            }
-          }
-        }
         if (store)
         {
 #pragma unroll
@@ -787,31 +674,6 @@ __global__ void __launch_bounds__ (32 * NW, 1)
         }
       }
 
-      if constexpr (kAux)
-      {
-        // masks and old auxiliaries of the next plane's first step (E at
-        // x + 1, H at x), into the set the next plane writes
-        prev.mE = pmask (0, x + 1);
-        prev.mH = pmask (3, x);
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-        {
-          if (kZedge && pair_along (c, 2) == 1)
-            continue;   // no auxiliary in the z-edge form
-          if ((prev.mE >> (2 * c)) & 3u)
-          {
-            const float2 v = __ldg (reinterpret_cast<const float2 *> (p.aux_old[c] + (size_t) (x + 1) * sx + rowoff));
-            axe[c][0] = v.x;
-            axe[c][1] = v.y;
-          }
-          if ((prev.mH >> (2 * c)) & 3u)
-          {
-            const float2 v = __ldg (reinterpret_cast<const float2 *> (p.aux_old[3 + c] + (size_t) x * sx + rowoff));
-            axh[c][0] = v.x;
-            axh[c][1] = v.y;
-          }
-        }
-      }
       return true;
     };
 
@@ -847,8 +709,8 @@ __global__ void __launch_bounds__ (32 * NW, 1)
 }
 
 template <typename T>
-std::string plan_t (Sweep2Plan &pl, const FusedParams &p, void *const e[2][3], void *const h[2][3], const float *eps,
-                    int sm_count)
+std::string plan_t (Sweep2Plan &pl, const FusedParams &p, void *const e[2][3], void *const h[2][3],
+                    float *const aux[2][6], const float *eps, int sm_count)
 {
   using L = L2<T>;
   const bool half = sizeof (T) == 2;
@@ -866,11 +728,21 @@ std::string plan_t (Sweep2Plan &pl, const FusedParams &p, void *const e[2][3], v
     }
     else
       m.eps = m.e[0];   // never used
+    for (int k = 0; k < 6; ++k)
+    {
+      if (p.use_pml && aux && aux[b][k])
+      {
+        if (!make_map (m.aux[k], aux[b][k], false, p.g.n, ZW, NW))
+          return "tensor map encoding failed";
+      }
+      else
+        m.aux[k] = m.e[0];   // never used
+    }
   }
   int per_sm = 0;
-  for (int mode = 0; mode < 3; ++mode)
+  for (int mode = 0; mode < 3; mode += 2)
   {
-    auto kern = mode == 0 ? sweep2_kernel<T, 0> : (mode == 1 ? sweep2_kernel<T, 1> : sweep2_kernel<T, 2>);
+    auto kern = mode == 0 ? sweep2_kernel<T, 0> : sweep2_kernel<T, 2>;
     if (cudaFuncSetAttribute (kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) L::TOTAL) != cudaSuccess)
     {
       cudaGetLastError ();
@@ -901,7 +773,7 @@ int launch_t (const Sweep2Plan &pl, int set, const FusedParams &p, int *err, cud
 {
   const dim3 block (32, NW);
   constexpr unsigned sm = L2<T>::TOTAL;
-  const bool conc = ss.side[0] && pl.items[0] > 0 && pl.items[1] + pl.items[2] > 0;
+  const bool conc = ss.side[0] && pl.items[0] > 0 && pl.items[2] > 0;
   cudaStream_t s0 = s;
   if (conc)
   {
@@ -910,11 +782,6 @@ int launch_t (const Sweep2Plan &pl, int set, const FusedParams &p, int *err, cud
     s0 = ss.side[0];
   }
   int n = 0;
-  if (pl.items[1] > 0)
-  {
-    sweep2_kernel<T, 1><<<pl.ctas, block, sm, s>>> (pl.maps[set], p, pl.work, err);
-    ++n;
-  }
   if (pl.items[2] > 0)
   {
     sweep2_kernel<T, 2><<<pl.ctas, block, sm, s>>> (pl.maps[set], p, pl.work, err);
@@ -936,15 +803,13 @@ int launch_t (const Sweep2Plan &pl, int set, const FusedParams &p, int *err, cud
 }  // namespace
 
 std::string sweep2_plan (Sweep2Plan &plan, const FusedParams &p, void *const e[2][3], void *const h[2][3],
-                         const float *eps, int sm_count, int chunk, unsigned long long *ctr, int x0, int x1, int y0,
-                         int y1)
+                         float *const aux[2][6], const float *eps, int sm_count, int chunk, unsigned long long *ctr,
+                         int x0, int x1, int y0, int y1)
 {
   const int *n = p.g.n;
   chunk = std::min (std::max (chunk, 1), kTb2MaxChunk);
   if (p.g.drop != 0)
     return "2-D grid";
-  if (p.use_tfsf)
-    return "TF/SF corrections";
   if (p.ps_mask)
     return "point source";
   if (p.use_meta)
@@ -960,8 +825,8 @@ std::string sweep2_plan (Sweep2Plan &plan, const FusedParams &p, void *const e[2
     y1 = n[1] - 1;
   if (x0 < 1 || x1 > n[0] - 1 || x0 >= x1 || y0 < 1 || y1 > n[1] - 1 || y0 >= y1)
     return "bad owned range";
-  std::string why = p.fp16 ? plan_t<__half> (plan, p, e, h, eps, sm_count)
-                           : plan_t<float> (plan, p, e, h, eps, sm_count);
+  std::string why = p.fp16 ? plan_t<__half> (plan, p, e, h, aux, eps, sm_count)
+                           : plan_t<float> (plan, p, e, h, aux, eps, sm_count);
   if (!why.empty ())
     return why;
   Sweep2Work &w = plan.work;
@@ -1004,6 +869,8 @@ std::string sweep2_plan (Sweep2Plan &plan, const FusedParams &p, void *const e[2
   plan.items[0] = plan.items[1] = plan.items[2] = 0;
   for (int it = 0; it < w.nitems; ++it)
     ++plan.items[sweep2_item_class (p, w, it)];
+  if (plan.items[1] > 0)
+    return "x / y PML cells in the two-step region (the single-step shell takes them)";
   if (plan.ctas > w.nitems)
     plan.ctas = w.nitems;
   return "";

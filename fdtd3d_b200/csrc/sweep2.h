@@ -27,6 +27,7 @@ struct Sweep2Maps
   CUtensorMap h[3];            // box (zs - 4 .. zs + 63) x (Y - 1 .. Y + 15)
   CUtensorMap e[3];            // box (zs .. zs + 63) x (Y .. Y + 15)
   CUtensorMap eps;             // box (zs .. zs + 67) x (Y .. Y + 16)
+  CUtensorMap aux[6];          // PML auxiliaries (float), box (zs .. zs + 63) x (Y .. Y + 15)
 };
 
 struct Sweep2Work
@@ -81,13 +82,14 @@ struct Sweep2Plan
 };
 
 // Builds the plan, or returns why the two-step kernel cannot serve the
-// geometry (it serves grids without TF/SF, point sources or Drude media,
-// with uniform mu; PML anywhere).  The plan owns the cells of rows
+// geometry (it serves grids without point sources or Drude media, with
+// uniform mu; PML anywhere).  The kernel applies no TF/SF correction: with
+// TF/SF the caller adds the pair's corrections afterwards (tfsf2.h).  The plan owns the cells of rows
 // y0 .. y1 - 1 and planes x0 .. x1 - 1 (all z); y0 = 1, y1 = ny - 1,
 // x0 = 1, x1 = nx - 1 is the whole grid.
 std::string sweep2_plan (Sweep2Plan &plan, const FusedParams &p, void *const e[2][3], void *const h[2][3],
-                         const float *eps, int sm_count, int chunk, unsigned long long *ctr, int x0 = 1, int x1 = -1,
-                         int y0 = 1, int y1 = -1);
+                         float *const aux[2][6], const float *eps, int sm_count, int chunk, unsigned long long *ctr,
+                         int x0 = 1, int x1 = -1, int y0 = 1, int y1 = -1);
 
 // Two time steps: buffer set `set` holds time t on entry; the kernel writes
 // time t + 2 into set 1 - set (one launch per item class that has items;

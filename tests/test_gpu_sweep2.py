@@ -150,3 +150,47 @@ def test_fp32_pairs_with_pml_match_single_steps(fdtd, monkeypatch, case):
         r = np.concatenate([ref[c].ravel() for c in fam])
         g = np.concatenate([got[c].ravel() for c in fam])
         assert np.linalg.norm(g - r) / np.linalg.norm(r) <= 1e-5, (case, fam)
+
+
+def _sphere(shape, frac=0.3):
+    c = [np.arange(n) + 0.5 - n / 2.0 for n in shape]
+    r2 = (frac * min(shape)) ** 2
+    return np.where(c[0][:, None, None] ** 2 + c[1][None, :, None] ** 2 + c[2][None, None, :] ** 2 < r2, 4.0, 1.0)
+
+
+TFSF_CASES = {
+    # PML shell and core, oblique plane wave, dielectric sphere
+    "pml_tfsf_sphere": dict(kw=dict(size=(96, 90, 120), use_pml=True, pml=6, use_tfsf=True, tfsf_left=22,
+                                    tfsf_right=22, teta=30, phi=45, psi=0), steps=61),
+    # no PML (the whole grid two-step), another polarisation
+    "tfsf_no_pml": dict(kw=dict(size=(40, 36, 64), use_tfsf=True, tfsf_left=(8, 7, 9), tfsf_right=(7, 8, 9),
+                                teta=60, phi=20, psi=45), steps=41),
+}
+
+
+@pytest.mark.parametrize("case", sorted(TFSF_CASES))
+def test_fp32_pairs_with_tfsf(fdtd, monkeypatch, case):
+    """The pair's TF/SF corrections are added after the uncorrected pair as
+    its linear response (two passes over the TF/SF band): the result agrees
+    with single steps whose corrections are added after each step to FP32
+    rounding (<= 1e-6 per field family) and with the FP64 oracle to the
+    FP32 bar (1e-5)."""
+    from oracle.oracle import Oracle
+
+    spec = TFSF_CASES[case]
+    kw = dict(mode=3, dx=0.0005, wavelength=0.02, courant=0.5, **spec["kw"])
+    shape = kw["size"]
+    eps = _sphere(shape)
+    got, k2 = _run(fdtd, monkeypatch, dict(kw, precision=fdtd.PREC_FP32), spec["steps"], {}, eps, True)
+    ref, k1 = _run(fdtd, monkeypatch, dict(kw, precision=fdtd.PREC_FP32), spec["steps"], {}, eps, False)
+    assert k1 == "sweep3d_tma"
+    assert k2 == "sweep2_tma"
+    o = Oracle(materials={"eps": eps}, **kw)
+    o.step(spec["steps"])
+    for fam in (COMPS[:3], COMPS[3:]):
+        r = np.concatenate([ref[c].ravel() for c in fam])
+        g = np.concatenate([got[c].ravel() for c in fam])
+        assert np.linalg.norm(r) > 0
+        assert np.linalg.norm(g - r) / np.linalg.norm(r) <= 1e-6, (case, fam)
+        ro = np.concatenate([o.field(c).ravel() for c in fam])
+        assert np.linalg.norm(g - ro) / np.linalg.norm(ro) <= 1e-5, (case, fam)
