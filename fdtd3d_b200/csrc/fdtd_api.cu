@@ -869,7 +869,7 @@ std::string plan_shell (fdtd_ctx *ctx, void *const e[2][3], void *const h[2][3],
 // take), their CTA tables and scratch arrays.
 std::string plan_tfsf2 (fdtd_ctx *ctx)
 {
-  std::vector<Tf2Box> rg[3];
+  std::vector<Tf2Box> rg[4];
   std::string why = tfsf2_regions (ctx->fused, rg);
   if (!why.empty ())
     return why;
@@ -877,13 +877,13 @@ std::string plan_tfsf2 (fdtd_ctx *ctx)
   {
     const Sweep2Work &w = ctx->tb2.work;
     const int cx0 = w.xcut[0], cx1 = w.xcut[w.nch], cy0 = w.yoff + 1, cy1 = w.yend;
-    for (int q = 0; q < 3; ++q)
+    for (int q = 0; q < 4; ++q)
       for (const Tf2Box &b : rg[q])
         if (b.lo[0] < cx0 + 2 || b.hi[0] > cx1 - 2 || b.lo[1] < cy0 + 2 || b.hi[1] > cy1 - 2)
           return "the TF/SF corrections reach the PML shell";
   }
-  std::vector<int2> bl[3];
-  for (int q = 0; q < 3; ++q)
+  std::vector<int2> bl[4];
+  for (int q = 0; q < 4; ++q)
     if (!(why = tfsf2_blocks (rg[q], bl[q])).empty ())
       return why;
   Tf2Pass &t = ctx->tf2;
@@ -891,7 +891,7 @@ std::string plan_tfsf2 (fdtd_ctx *ctx)
   const size_t n = (size_t) g.cells;
   if (!t.scratch[0])
   {
-    for (int k = 0; k < 6; ++k)
+    for (int k = 0; k < 9; ++k)
       if (dalloc (ctx, (void **) &t.scratch[k], n * sizeof (float)) != FDTD_OK)
         return "allocation of the TF/SF scratch failed";
     if (dalloc (ctx, (void **) &ctx->hinc_keep, (size_t) g.inc_len * sizeof (double)) != FDTD_OK)
@@ -903,7 +903,7 @@ std::string plan_tfsf2 (fdtd_ctx *ctx)
       return false;
     return cudaMemcpyAsync (*dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream) == cudaSuccess;
   };
-  for (int q = 0; q < 3; ++q)
+  for (int q = 0; q < 4; ++q)
   {
     if (!upload ((void **) &t.boxes[q], rg[q].data (), rg[q].size () * sizeof (Tf2Box)) ||
         !upload ((void **) &t.blk[q], bl[q].data (), bl[q].size () * sizeof (int2)))
@@ -912,7 +912,7 @@ std::string plan_tfsf2 (fdtd_ctx *ctx)
   }
   // the scratch must be zero outside the regions: clear it whenever they may
   // have changed
-  for (int k = 0; k < 6; ++k)
+  for (int k = 0; k < 9; ++k)
     if (cudaMemsetAsync (t.scratch[k], 0, n * sizeof (float), ctx->stream) != cudaSuccess)
       return "TF/SF scratch clear failed";
   if (cudaStreamSynchronize (ctx->stream) != cudaSuccess)

@@ -11,7 +11,8 @@
 //   dE2 = dE1 + S im (curlE dH1 + dE(t2)) dH2 = dH1 + S (curlH dE2 + dH(t2))
 // with curlH / curlE the step's own curls (E at c and c + e_a for H, H at c
 // and c - e_a for E), evaluated in four passes over the supports (the term
-// boxes grown by up to two cells), each cell evaluating its own terms once.
+// boxes grown by up to two cells), each cell evaluating the terms that cover
+// it (a mask per region box) once.
 // Every cell of the supports takes the plain update in both steps (no PML,
 // no point source), which the host checks.
 #include <cuda_fp16.h>
@@ -74,6 +75,28 @@ __device__ __forceinline__ float term_curl (const FusedParams &p, int k, const d
   return d;
 }
 
+// The same over the terms of `mask` (bit t: term t of component k), those
+// that overlap the cell's box.
+__device__ __forceinline__ float term_curl_masked (const FusedParams &p, int k, unsigned mask, const double *inc,
+                                                   int *err, int x, int y, int z)
+{
+  const CompDev &c = p.comp[k];
+  float d = 0.f;
+#pragma unroll
+  for (int t = 0; t < kMaxTerms; ++t)
+    if ((mask >> t) & 1u)
+    {
+      const TermDev &tm = c.term[t];
+      if (!(x >= tm.lo[0] && x < tm.hi[0] && y >= tm.lo[1] && y < tm.hi[1] && z >= tm.lo[2] && z < tm.hi[2]))
+        continue;
+      const double diff = inc_at (p.g, inc, p.inc_len, err, tm.inc_comp, x + tm.aux[0], y + tm.aux[1],
+                                  z + tm.aux[2]);
+      const float dv = (float) (diff * tm.negate) * p.inc_scale[tm.inc_comp];
+      d += (tm.slot == 0 || tm.slot == 3) ? dv : -dv;
+    }
+  return d;
+}
+
 // 2 / (eps + eps') of E component k at cell index c (1 without eps)
 __device__ __forceinline__ float inv_m (const FusedParams &p, int k, size_t c, size_t sx, int nz)
 {
@@ -98,48 +121,52 @@ __device__ __forceinline__ bool box_cell (const Tf2Box &b, int first, int &x, in
 }
 
 // The four passes over their regions (one cell per thread; every cell
-// evaluates its own TF/SF terms once):
-//   A over R_E: dE1 = S im dE(t1)                          -> sE (0 off the terms)
-//   B over R_H1: dH1 = S (curlH sE + dH(t1))               -> sH
-//   C over R_E: dE2 = sE + S im (curlE sH + dE(t2))        -> sE, E_new += dE2
-//   D over R_H2: dH2 = sH + S (curlH sE + dH(t2))          -> H_new += dH2
-// R_E holds the support of dE1 and dE2, R_H1 that of dH1, R_H2 that of dH2.
-// sE and sH are zero outside R_E and R_H1 (never written there).
+// evaluates only the terms of its box's mask):
+//   A over T_E:  dE1 = S im dE(t1)                         -> sE1
+//   B over R_H1: dH1 = S (curlH sE1 + dH(t1))              -> sH1
+//   C over R_E:  dE2 = sE1 + S im (curlE sH1 + dE(t2))     -> sE2, E_new += dE2
+//   D over R_H2: dH2 = sH1 + S (curlH sE2 + dH(t2))        -> H_new += dH2
+// T_E holds the E term cells, R_H1 the support of dH1, R_E that of dE1 and
+// dE2, R_H2 that of dH2; sE1, sH1 and sE2 are zero outside T_E, R_H1 and R_E
+// (never written there).
 template <typename T, int PASS>
 __global__ void __launch_bounds__ (256) tfsf2_pass (const __grid_constant__ FusedParams p, const Tf2Pass pass,
                                                     const double *inc, int *err)
 {
-  const int r = PASS == 1 ? 1 : (PASS == 3 ? 2 : 0);   // region: 0 R_E, 1 R_H1, 2 R_H2
-  const int2 bk = pass.blk[r][blockIdx.x];
+  const int2 bk = pass.blk[PASS][blockIdx.x];
+  const Tf2Box &box = pass.boxes[PASS][bk.x];
   int x, y, z;
-  if (!box_cell (pass.boxes[r][bk.x], bk.y, x, y, z))
+  if (!box_cell (box, bk.y, x, y, z))
     return;
+  const unsigned mask = box.mask;
   const int ny = p.g.n[1], nz = p.g.n[2];
   const size_t sx = (size_t) ny * nz, sy = nz;
   const float S = p.courant;
-  float *const *sE = pass.scratch;
-  float *const *sH = pass.scratch + 3;
+  float *const *sE1 = pass.scratch;
+  float *const *sH1 = pass.scratch + 3;
+  float *const *sE2 = pass.scratch + 6;
   const size_t id = (size_t) x * sx + (size_t) y * sy + z;
   if (PASS == 0 || PASS == 2)
   {
-    float cu[3];
+    float cu[3] = {0.f, 0.f, 0.f};
     if (PASS == 2)
     {
-      cu[0] = (sH[2][id] - sH[2][id - sy]) - (sH[1][id] - sH[1][id - 1]);
-      cu[1] = (sH[0][id] - sH[0][id - 1]) - (sH[2][id] - sH[2][id - sx]);
-      cu[2] = (sH[1][id] - sH[1][id - sx]) - (sH[0][id] - sH[0][id - sy]);
+      cu[0] = (sH1[2][id] - sH1[2][id - sy]) - (sH1[1][id] - sH1[1][id - 1]);
+      cu[1] = (sH1[0][id] - sH1[0][id - 1]) - (sH1[2][id] - sH1[2][id - sx]);
+      cu[2] = (sH1[1][id] - sH1[1][id - sx]) - (sH1[0][id] - sH1[0][id - sy]);
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k)
     {
-      const float d = (PASS == 2 ? cu[k] : 0.f) + term_curl (p, k, inc, err, x, y, z);
+      const unsigned mk = (mask >> (4 * k)) & 15u;
+      const float d = cu[k] + (mk ? term_curl_masked (p, k, mk, inc, err, x, y, z) : 0.f);
       const float v = d == 0.f ? 0.f : (S * inv_m (p, k, id, sx, nz)) * d;
       if (PASS == 0)
-        sE[k][id] = v;
+        sE1[k][id] = v;
       else
       {
-        const float e2 = sE[k][id] + v;
-        sE[k][id] = e2;
+        const float e2 = sE1[k][id] + v;
+        sE2[k][id] = e2;
         if (e2 != 0.f)
         {
           T *f = reinterpret_cast<T *> (p.e_new[k]);
@@ -150,19 +177,21 @@ __global__ void __launch_bounds__ (256) tfsf2_pass (const __grid_constant__ Fuse
   }
   else
   {
-    // curlH of sE (dE1 in pass B, dE2 in pass D)
+    // curlH of the E corrections (dE1 in pass B, dE2 in pass D)
+    float *const *sE = PASS == 1 ? sE1 : sE2;
     const float ex = sE[0][id], ey = sE[1][id], ez = sE[2][id];
     const float a[3] = {(sE[1][id + 1] - ey) - (sE[2][id + sy] - ez), (sE[2][id + sx] - ez) - (sE[0][id + 1] - ex),
                         (sE[0][id + sy] - ex) - (sE[1][id + sx] - ey)};
 #pragma unroll
     for (int m = 0; m < 3; ++m)
     {
-      const float dh = S * (a[m] + term_curl (p, 3 + m, inc, err, x, y, z));
+      const unsigned mk = (mask >> (4 * (3 + m))) & 15u;
+      const float dh = S * (a[m] + (mk ? term_curl_masked (p, 3 + m, mk, inc, err, x, y, z) : 0.f));
       if (PASS == 1)
-        sH[m][id] = dh;
+        sH1[m][id] = dh;
       else
       {
-        const float h2 = sH[m][id] + dh;
+        const float h2 = sH1[m][id] + dh;
         if (h2 != 0.f)
         {
           T *f = reinterpret_cast<T *> (p.h_new[m]);
@@ -173,9 +202,10 @@ __global__ void __launch_bounds__ (256) tfsf2_pass (const __grid_constant__ Fuse
   }
 }
 
-// Disjoint cover of a union of boxes: coordinate compression (every box
-// edge is a cut), the covered elementary boxes, runs along z merged.
-std::vector<Tf2Box> disjoint_cover (const std::vector<Tf2Box> &in)
+// Disjoint cover of a union of boxes: coordinate compression (every box edge
+// is a cut), the covered elementary boxes, runs along z merged; each box
+// carries the mask of the TF/SF terms that overlap it.
+std::vector<Tf2Box> disjoint_cover (const std::vector<Tf2Box> &in, const FusedParams &p)
 {
   std::vector<Tf2Box> out;
   if (in.empty ())
@@ -199,6 +229,20 @@ std::vector<Tf2Box> disjoint_cover (const std::vector<Tf2Box> &in)
         return true;
     return false;
   };
+  // terms of each component that reach the box at all (bit 4k + t); a
+  // cell of the box still tests its own position against them
+  auto mask_of = [&] (size_t i, size_t j, size_t l, size_t e) {
+    unsigned m = 0;
+    for (int k = 0; k < 6; ++k)
+      for (int t = 0; t < p.comp[k].nterms; ++t)
+      {
+        const TermDev &tm = p.comp[k].term[t];
+        if (cut[0][i] < tm.hi[0] && cut[0][i + 1] > tm.lo[0] && cut[1][j] < tm.hi[1] && cut[1][j + 1] > tm.lo[1] &&
+            cut[2][l] < tm.hi[2] && cut[2][e] > tm.lo[2])
+          m |= 1u << (4 * k + t);
+      }
+    return m;
+  };
   for (size_t i = 0; i + 1 < cut[0].size (); ++i)
     for (size_t j = 0; j + 1 < cut[1].size (); ++j)
     {
@@ -213,6 +257,7 @@ std::vector<Tf2Box> disjoint_cover (const std::vector<Tf2Box> &in)
         size_t e = l + 1;
         while (e + 1 < cut[2].size () && covered (i, j, e))
           ++e;
+        const unsigned m = mask_of (i, j, l, e);
         Tf2Box b;
         b.lo[0] = cut[0][i];
         b.hi[0] = cut[0][i + 1];
@@ -220,6 +265,7 @@ std::vector<Tf2Box> disjoint_cover (const std::vector<Tf2Box> &in)
         b.hi[1] = cut[1][j + 1];
         b.lo[2] = cut[2][l];
         b.hi[2] = cut[2][e];
+        b.mask = m;
         out.push_back (b);
         l = e;
       }
@@ -229,36 +275,39 @@ std::vector<Tf2Box> disjoint_cover (const std::vector<Tf2Box> &in)
 
 }  // namespace
 
-std::string tfsf2_regions (const FusedParams &p, std::vector<Tf2Box> r[3])
+std::string tfsf2_regions (const FusedParams &p, std::vector<Tf2Box> r[4])
 {
-  std::vector<Tf2Box> g[3];
+  std::vector<Tf2Box> g[4];
   for (int k = 0; k < 6; ++k)
     for (int t = 0; t < p.comp[k].nterms; ++t)
     {
       const TermDev &tm = p.comp[k].term[t];
       if (tm.lo[0] >= tm.hi[0] || tm.lo[1] >= tm.hi[1] || tm.lo[2] >= tm.hi[2])
         continue;
-      // a term box T (E or H) grown per axis by (below, above):
-      //   R_E:  E (1, 1), H (0, 1);  R_H1: E (1, 0), H (0, 0);
-      //   R_H2: E (2, 1), H (1, 1)
+      // a term box (E or H) grown per axis by (below, above):
+      //   T_E: E (0, 0);  R_H1: E (1, 0), H (0, 0);
+      //   R_E: E (1, 1), H (0, 1);  R_H2: E (2, 1), H (1, 1)
       const bool e = k < 3;
-      const int grow[3][2] = {{e ? 1 : 0, 1}, {e ? 1 : 0, 0}, {e ? 2 : 1, 1}};
-      for (int q = 0; q < 3; ++q)
+      const int grow[4][2] = {{0, 0}, {e ? 1 : 0, 0}, {e ? 1 : 0, 1}, {e ? 2 : 1, 1}};
+      for (int q = 0; q < 4; ++q)
       {
+        if (q == 0 && !e)
+          continue;
         Tf2Box b;
         for (int ax = 0; ax < 3; ++ax)
         {
           b.lo[ax] = tm.lo[ax] - grow[q][0];
           b.hi[ax] = tm.hi[ax] + grow[q][1];
         }
+        b.mask = 0;
         g[q].push_back (b);
       }
     }
-  for (int q = 0; q < 3; ++q)
-    r[q] = disjoint_cover (g[q]);
+  for (int q = 0; q < 4; ++q)
+    r[q] = disjoint_cover (g[q], p);
   // every cell of the regions and its neighbours takes the plain update:
   // inside 2 .. n - 3 and outside every component's PML
-  for (int q = 0; q < 3; ++q)
+  for (int q = 0; q < 4; ++q)
     for (const Tf2Box &b : r[q])
       for (int a = 0; a < 3; ++a)
       {
@@ -290,23 +339,31 @@ std::string tfsf2_blocks (const std::vector<Tf2Box> &boxes, std::vector<int2> &b
 int launch_tfsf2 (const Tf2Pass &pass, const FusedParams &p, const double *inc_h1, const double *inc_e1,
                   const double *inc_h2, const double *inc_e2, int *err, cudaStream_t s)
 {
-  if (pass.nblk[0] <= 0)
+  if (pass.nblk[2] <= 0)
     return 0;
+  int n = 0;
+  auto go = [&] (auto kern, int q, const double *inc) {
+    if (pass.nblk[q] > 0)
+    {
+      kern<<<pass.nblk[q], 256, 0, s>>> (p, pass, inc, err);
+      ++n;
+    }
+  };
   if (p.fp16)
   {
-    tfsf2_pass<__half, 0><<<pass.nblk[0], 256, 0, s>>> (p, pass, inc_h1, err);
-    tfsf2_pass<__half, 1><<<pass.nblk[1], 256, 0, s>>> (p, pass, inc_e1, err);
-    tfsf2_pass<__half, 2><<<pass.nblk[0], 256, 0, s>>> (p, pass, inc_h2, err);
-    tfsf2_pass<__half, 3><<<pass.nblk[2], 256, 0, s>>> (p, pass, inc_e2, err);
+    go (tfsf2_pass<__half, 0>, 0, inc_h1);
+    go (tfsf2_pass<__half, 1>, 1, inc_e1);
+    go (tfsf2_pass<__half, 2>, 2, inc_h2);
+    go (tfsf2_pass<__half, 3>, 3, inc_e2);
   }
   else
   {
-    tfsf2_pass<float, 0><<<pass.nblk[0], 256, 0, s>>> (p, pass, inc_h1, err);
-    tfsf2_pass<float, 1><<<pass.nblk[1], 256, 0, s>>> (p, pass, inc_e1, err);
-    tfsf2_pass<float, 2><<<pass.nblk[0], 256, 0, s>>> (p, pass, inc_h2, err);
-    tfsf2_pass<float, 3><<<pass.nblk[2], 256, 0, s>>> (p, pass, inc_e2, err);
+    go (tfsf2_pass<float, 0>, 0, inc_h1);
+    go (tfsf2_pass<float, 1>, 1, inc_e1);
+    go (tfsf2_pass<float, 2>, 2, inc_h2);
+    go (tfsf2_pass<float, 3>, 3, inc_e2);
   }
-  return 4;
+  return n;
 }
 
 }  // namespace fdtdb

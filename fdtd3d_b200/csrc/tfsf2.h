@@ -14,23 +14,26 @@ namespace fdtdb {
 struct Tf2Box
 {
   int lo[3], hi[3];            // cells lo .. hi - 1 per axis
+  unsigned mask;               // bit 4k + t: term t of component k (Ex .. Hz) covers the box
 };
 
 struct Tf2Pass
 {
-  // regions as disjoint boxes (device): 0 R_E (supports of the E
-  // corrections), 1 R_H1 (of the first step's H corrections), 2 R_H2 (of
-  // the second step's)
-  Tf2Box *boxes[3] = {};
-  int2 *blk[3] = {};           // per CTA: the box and the first of its cells
-  int nblk[3] = {};
-  float *scratch[6] = {};      // E (3) and H (3) corrections: full-size, zero outside R_E and R_H1
+  // regions as disjoint boxes (device): 0 T_E (the E term cells), 1 R_H1
+  // (support of the first step's H corrections), 2 R_E (of the E
+  // corrections), 3 R_H2 (of the second step's H corrections)
+  Tf2Box *boxes[4] = {};
+  int2 *blk[4] = {};           // per CTA: the box and the first of its cells
+  int nblk[4] = {};
+  // first-step E (3) and H (3) and second-step E (3) corrections:
+  // full-size, zero outside T_E, R_H1 and R_E
+  float *scratch[9] = {};
 };
 
 // The passes' regions as disjoint boxes (from the TF/SF term boxes), or the
 // reason the scheme cannot serve the geometry (a region cell too close to
 // the grid's faces or to a PML cell).
-std::string tfsf2_regions (const FusedParams &p, std::vector<Tf2Box> r[3]);
+std::string tfsf2_regions (const FusedParams &p, std::vector<Tf2Box> r[4]);
 
 // CTA table of a region (256 cells per CTA).
 std::string tfsf2_blocks (const std::vector<Tf2Box> &boxes, std::vector<int2> &blk);
