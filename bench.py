@@ -17,12 +17,18 @@ no flush is needed between steps.
            library's asynchronous copies (fdtd_upload_material_async /
            fdtd_download_field_async): a step's upload and the previous
            step's download run on the copy engines while the GPU computes.
-  roofline: the field-update launches of one time step (the sweep kernel
-           of each item class and the TF/SF post pass, timed together by
-           CUDA events on the library's stream), algorithmic bytes per step
-           (cells * B, B = 4*(12 + m + 12*f_PML) bytes per cell-update) over
-           their measured time per step, against the measured HBM copy
-           bandwidth.
+  roofline: the field-update launches of one timed unit, timed together
+           by CUDA events on the library's streams: a pair of time steps on
+           the two-step path (PML shell, two-step core, TF/SF pair passes),
+           one time step on the single-step sweep (item classes, TF/SF post
+           pass).  achieved = algorithmic bytes of the unit's cell-updates
+           (cells * steps * B, B = 4*(12 + m + 12*f_PML) bytes per
+           cell-update) over its measured time, against the measured HBM
+           copy bandwidth.  A two-step pass reads and writes each value once
+           for two steps, so its compulsory traffic is cells * B per pair:
+           compulsory_frac (that over the time, against the same peak) is
+           the fraction of the bandwidth the pass actually needs, and
+           `traffic` (ncu DRAM bytes per unit, profiles/) shows what it moved.
   cpu_baseline: the reference fdtd3d CPU build (oracle/_ref/fdtd3d) on a
            bounded sample of the same physics (one process).
 
@@ -55,6 +61,9 @@ TFSF = 32
 
 
 def kernel_label(step_kernel: str) -> str:
+    if step_kernel == "sweep2_tma":
+        return ("sweep2_kernel (lean / z-edge core, two time steps per pass) + sweep3d_kernel (x/y PML shell, "
+                "two single steps) + tfsf2_pass x4: E and H of two time steps")
     if step_kernel == "sweep3d_tma":
         return ("sweep3d_kernel (lean / z-edge PML / PML / full item classes) + tfsf_post_kernel: "
                 "E and H of one time step")
@@ -497,9 +506,10 @@ def main() -> None:
     peaks = measured_peaks()
     b_cell, f_pml = algorithmic_bytes_per_cell(n, word)
     avg_launch_ms = kernel_ms / max(kernel_launches, 1)
-    # one timed unit per time step on the sweep path (the sweep kernels of
-    # the three item classes plus the TF/SF post pass); the per-cell kernels
-    # take two timed units (E, H) per step
+    # one timed unit per time step on the single-step sweep path (the sweep
+    # kernels of the three item classes plus the TF/SF post pass), one per
+    # pair of time steps on the two-step path (shell, core and the TF/SF pair
+    # passes); the per-cell kernels take two timed units (E, H) per step
     steps_per_launch = args.steps / max(kernel_launches, 1)
     bytes_per_launch = cells * b_cell * steps_per_launch
     achieved = bytes_per_launch / (avg_launch_ms * 1e-3) / 1e9
@@ -507,12 +517,22 @@ def main() -> None:
                 "frac": achieved / peaks["hbm_gbs"], "traffic": None,
                 "kernel": kernel_label(sim_kernel) if steps_per_launch > 0.75
                 else "fast_half_kernel (E or H family)", "avg_launch_ms": avg_launch_ms,
+                "time_steps_per_launch": round(steps_per_launch, 3),
                 "bytes_per_launch": bytes_per_launch,
                 "algorithmic_bytes_per_cell_update": b_cell, "f_pml": f_pml,
                 "peak_source": peaks["source"], "kernel_share_of_step": kernel_ms / ms}
+    if steps_per_launch > 1.5:
+        # a two-step pass needs each value read and written once for the
+        # pair: its compulsory bytes are those of one single step
+        compulsory = cells * b_cell
+        roofline["compulsory_bytes_per_launch"] = compulsory
+        roofline["compulsory_frac"] = compulsory / (avg_launch_ms * 1e-3) / 1e9 / peaks["hbm_gbs"]
     traffic_file = os.path.join(ROOT, "profiles", f"traffic_{args.precision}.json")
     if os.path.exists(traffic_file):
-        roofline["traffic"] = json.load(open(traffic_file)).get("bytes_per_launch")
+        entry = json.load(open(traffic_file)).get(sim_kernel)
+        if entry and entry.get("grid") == n:
+            roofline["traffic"] = entry["bytes_per_launch"]
+            roofline["traffic_source"] = entry["source"]
 
     # e2e through the C ABI with pinned host buffers
     h_eps = torch.from_numpy(eps.reshape(-1)).pin_memory()

@@ -171,7 +171,7 @@ TFSF_CASES = {
 @pytest.mark.parametrize("case", sorted(TFSF_CASES))
 def test_fp32_pairs_with_tfsf(fdtd, monkeypatch, case):
     """The pair's TF/SF corrections are added after the uncorrected pair as
-    its linear response (two passes over the TF/SF band): the result agrees
+    its linear response (four passes over the TF/SF band): the result agrees
     with single steps whose corrections are added after each step to FP32
     rounding (<= 1e-6 per field family) and with the FP64 oracle to the
     FP32 bar (1e-5)."""
@@ -194,6 +194,25 @@ def test_fp32_pairs_with_tfsf(fdtd, monkeypatch, case):
         assert np.linalg.norm(g - r) / np.linalg.norm(r) <= 1e-6, (case, fam)
         ro = np.concatenate([o.field(c).ravel() for c in fam])
         assert np.linalg.norm(g - ro) / np.linalg.norm(ro) <= 1e-5, (case, fam)
+
+
+def test_fp16_storage_pairs_with_pml_and_tfsf(fdtd, monkeypatch):
+    """FP16 storage through the whole two-step scheme (PML shell, core, TF/SF
+    pair corrections) against the FP32 single-step form: within the FP16
+    bar (2e-2 per family), and no farther than FP16 single steps are."""
+    kw = dict(mode=3, size=(96, 90, 120), use_pml=True, pml=6, use_tfsf=True, tfsf_left=22, tfsf_right=22,
+              teta=30, phi=45, psi=0, dx=0.0005, wavelength=0.02, courant=0.5)
+    eps = _sphere(kw["size"])
+    got, k2 = _run(fdtd, monkeypatch, dict(kw, precision=fdtd.PREC_FP16S), 61, {}, eps, True)
+    one, _ = _run(fdtd, monkeypatch, dict(kw, precision=fdtd.PREC_FP16S), 61, {}, eps, False)
+    ref, _ = _run(fdtd, monkeypatch, dict(kw, precision=fdtd.PREC_FP32), 61, {}, eps, False)
+    assert k2 == "sweep2_tma"
+    for fam in (COMPS[:3], COMPS[3:]):
+        r = np.concatenate([ref[c].ravel() for c in fam])
+        g2 = np.concatenate([got[c].ravel() for c in fam])
+        g1 = np.concatenate([one[c].ravel() for c in fam])
+        assert np.linalg.norm(g2 - r) / np.linalg.norm(r) <= 2e-2
+        assert np.linalg.norm(g2 - r) <= 1.05 * np.linalg.norm(g1 - r)
 
 
 def test_fp16_storage_pairs_with_pml_and_tfsf(fdtd, monkeypatch):
