@@ -88,7 +88,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         raise RuntimeError(f"link failed: {' '.join(link)}\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, LIB)
     # the command-line drop-in, linked against the library next to it
-    cli = ["g++", "-O2", "-std=c++17", os.path.join(CSRC, "cli.cpp"), "-o", CLI + ".tmp", "-L", HERE,
+    cli = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", os.path.join(CSRC, "cli.cpp"), "-o", CLI + ".tmp", "-L", HERE,
            "-lfdtd_b200", "-Wl,-rpath,$ORIGIN"]
     r = subprocess.run(cli, capture_output=True, text=True)
     if r.returncode != 0:

@@ -33,6 +33,7 @@
 // callbacks) are rejected with a message instead of being ignored.
 #include <sys/time.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -72,6 +73,16 @@ struct Opts
   bool save_einc = false, save_hinc = false, save_materials = false;
   int interm_save_step = 100;
   bool orth[3] = {false, false, false};
+  // material spheres: eps, mu, omegape, omegapm (Settings.inc.h:232-249);
+  // a sphere is set when its value differs from the default (1, 1, 0, 0)
+  struct Sphere
+  {
+    double value;
+    int center[3] = {0, 0, 0};
+    int radius = 0;
+  } sphere[4] = {{1.0}, {1.0}, {0.0}, {0.0}};
+  bool stair_sphere = false;
+  int sphere_accuracy = 100;
 };
 
 // Axes a mode drops (bit a) and the components it keeps (bit k).
@@ -147,6 +158,155 @@ bool parse_coord (const std::string &s, int out[3])
 double stof_like (const std::string &s)
 {
   return (double) std::stof (s);
+}
+
+// --eps-sphere / --mu-sphere / --omegape-sphere / --omegapm-sphere and their
+// -center / -radius flags.  Returns true when `a` is one of them; `ok`
+// tells whether its argument parsed.
+bool sphere_flag (const std::string &a, Opts &o, const std::vector<std::string> &args, size_t &i, std::string &v,
+                  bool &ok)
+{
+  static const char *names[4] = {"--eps-sphere", "--mu-sphere", "--omegape-sphere", "--omegapm-sphere"};
+  for (int m = 0; m < 4; ++m)
+  {
+    const std::string base = names[m];
+    const int what = a == base ? 0 : (a == base + "-center" ? 1 : (a == base + "-radius" ? 2 : -1));
+    if (what < 0)
+      continue;
+    ok = i + 1 < args.size ();
+    if (!ok)
+      return true;
+    v = args[++i];
+    if (what == 0)
+      o.sphere[m].value = stof_like (v);
+    else if (what == 1)
+      ok = parse_coord (v, o.sphere[m].center);
+    else
+      o.sphere[m].radius = std::atoi (v.c_str ());
+    return true;
+  }
+  return false;
+}
+
+// Fraction of the unit cell centred at mid (its `dim` kept coordinates)
+// inside the sphere (centre c, radius r): the reference's column
+// integration with `steps` samples per axis, the height of the sphere's
+// surface above (or below) the cell's face clamped to the cell
+// (Approximation::approximateSphereAccurate, Source/Layout/Approximation.cpp:
+// 387-668; its 1-D form takes the interval overlap with the reference's
+// tests as written).  The arithmetic follows the reference expression by
+// expression, so the values agree bit for bit.
+double sphere_volume (int dim, const double mid[3], const double c[3], double r, int steps)
+{
+  double lo[3], hi[3];
+  for (int k = 0; k < dim; ++k)
+  {
+    lo[k] = mid[k] - 0.5;
+    hi[k] = mid[k] + 0.5;
+  }
+  double volume = 0;
+  if (dim == 1)
+  {
+    const double left = c[0] - r, right = c[0] + r;
+    if (hi[0] <= left || lo[0] >= right)
+      volume = 0;
+    else if (lo[0] >= left || hi[0] <= right)
+      volume = 1;
+    else if (lo[0] < left)
+      volume = hi[0] - left;
+    else if (hi[0] > right)
+      volume = right - lo[0];
+  }
+  else
+  {
+    // the last kept axis is the one solved for; the others are sampled
+    const int h = dim - 1;
+    const double step = 1.0 / steps;
+    const double cell = dim == 2 ? step : step * step;
+    const int n2 = dim == 2 ? 1 : steps;
+    for (int i = 0; i < steps; ++i)
+      for (int j = 0; j < n2; ++j)
+      {
+        const double u = lo[0] + i * step;
+        double rest = r * r - (u - c[0]) * (u - c[0]);
+        if (dim == 3)
+        {
+          const double w = lo[1] + j * step;
+          rest = rest - (w - c[1]) * (w - c[1]);
+        }
+        double height = 0.0;
+        if (rest >= 0)
+        {
+          const bool above = mid[h] > c[h];
+          height = above ? c[h] + std::sqrt (rest) : c[h] - std::sqrt (rest);
+          if (height < lo[h])
+            height = lo[h];
+          else if (height > hi[h])
+            height = hi[h];
+          height = above ? height - lo[h] : hi[h] - height;
+        }
+        volume += height * cell;
+      }
+  }
+  if (volume > 1)
+    volume = 1;
+  return volume;
+}
+
+// Whether every corner of the unit cell centred at mid lies in the sphere
+// (Approximation::approximateSphereStair, Approximation.cpp:678-764).
+bool sphere_stair (int dim, const double mid[3], const double c[3], double r)
+{
+  for (int corner = 0; corner < (1 << dim); ++corner)
+  {
+    double d2 = 0;
+    for (int k = 0; k < dim; ++k)
+    {
+      const double q = mid[k] + (((corner >> k) & 1) ? 0.5 : -0.5) - c[k];
+      d2 = d2 + q * q;
+    }
+    if (!(std::sqrt (d2) <= r))
+      return false;
+  }
+  return true;
+}
+
+// Fills a material grid (x-major over n[0] x n[1] x n[2], a mode's dropped
+// axes of size 1) with a sphere as Scheme::initGrids does for the
+// --*-sphere flags (Source/Scheme/Scheme.inc.h:2980-3160): every cell, at
+// its real position (index + 0.5 on each kept axis, YeeGridLayout's
+// minEpsCoordFP), gets value * volume + outside * (1 - volume), or value /
+// outside by the stair test; the centre is centre * modifier + 0.5 and the
+// radius radius * modifier (modifier 2 on the doubled grid of
+// --use-double-material-precision).
+void fill_sphere (std::vector<double> &grid, const int n[3], unsigned drop, const Opts::Sphere &sp, double value,
+                  double outside, double modifier, bool stair, int steps)
+{
+  int axes[3], dim = 0;
+  for (int a = 0; a < 3; ++a)
+    if (!((drop >> a) & 1u))
+      axes[dim++] = a;
+  double c[3];
+  for (int k = 0; k < dim; ++k)
+    c[k] = sp.center[axes[k]] * modifier + 0.5;
+  const double r = sp.radius * modifier;
+  size_t id = 0;
+  for (int x = 0; x < n[0]; ++x)
+    for (int y = 0; y < n[1]; ++y)
+      for (int z = 0; z < n[2]; ++z, ++id)
+      {
+        const int pos[3] = {x, y, z};
+        double mid[3];
+        for (int k = 0; k < dim; ++k)
+          mid[k] = (double) pos[axes[k]] + 0.5;
+        if (stair)
+          grid[id] = sphere_stair (dim, mid, c, r) ? value : outside;
+        else
+        {
+          const double vol = sphere_volume (dim, mid, c, r, steps);
+          grid[id] = value * vol + outside * (1 - vol);
+        }
+      }
 }
 
 std::vector<std::string> read_cmd_file (const std::string &path)
@@ -370,6 +530,15 @@ int parse (std::vector<std::string> args, Opts &o)
         c.precision = FDTD_PREC_FP16S;
       else
         return fail ("--precision must be fp64, fp32 or fp16s");
+    }
+    else if (a == "--stair-sphere-approx")
+      o.stair_sphere = true;
+    else if (a == "--sphere-accuracy" && next (v))
+      o.sphere_accuracy = std::atoi (v.c_str ());
+    else if (sphere_flag (a, o, args, i, v, handled))
+    {
+      if (!handled)
+        return fail ("bad " + a);
     }
     else if (a == "--cmd-from-file" && next (v))
     {
@@ -846,11 +1015,31 @@ int main (int argc, char **argv)
     mat[m].assign (m < 2 ? fine : cells, m < 2 ? 1.0 : 0.0);
     if (o.complex_values)
       mat_im[m].assign (mat[m].size (), 0.0);
-    if (o.mat_file[m].empty ())
+    // a material sphere replaces every value of its grid, the file's too
+    // (Scheme::initGrids: file first, then the sphere); the Drude spheres
+    // hold omega * 2 pi * (c / lambda) and only with --use-metamaterials
+    const bool sphere = m < 4 && o.sphere[m].value != (m < 2 ? 1.0 : 0.0) && (m < 2 || o.cfg.use_metamaterials);
+    if (o.mat_file[m].empty () && !sphere)
       continue;
     std::string why;
-    if (!load_material (o.mat_file[m], m < 2 ? fine : cells, kept, o.complex_values, mat[m], mat_im[m], why))
+    if (!o.mat_file[m].empty () &&
+        !load_material (o.mat_file[m], m < 2 ? fine : cells, kept, o.complex_values, mat[m], mat_im[m], why))
       return fail (why);
+    if (sphere)
+    {
+      int nm[3] = {n[0], n[1], n[2]};
+      if (m < 2 && o.cfg.double_material_precision)
+        for (int a = 0; a < 3; ++a)
+          if (!((drop >> a) & 1u))
+            nm[a] *= 2;
+      double value = o.sphere[m].value;
+      if (m >= 2)
+        value = value * 2 * M_PI * (299792458.0 / o.cfg.wavelength);
+      fill_sphere (mat[m], nm, drop, o.sphere[m], value, m < 2 ? 1.0 : 0.0,
+                   o.cfg.double_material_precision ? 2.0 : 1.0, o.stair_sphere, o.sphere_accuracy);
+      if (o.complex_values)
+        std::fill (mat_im[m].begin (), mat_im[m].end (), 0.0);
+    }
     for (int r = 0; r < nrun; ++r)
     {
       st = fdtd_upload_material (ctx[r], m, mat[m].data ());

@@ -31,30 +31,40 @@ FDTDB_HD inline size_t lin (const GeomDev &g, int x, int y, int z)
   return ((size_t) x * g.n[1] + y) * g.n[2] + z;
 }
 
-FDTDB_HD inline double avg_points (const CompDev &c, const double *v)
+// Average of a component's 1, 2 or 4 material points (v1 .. v3 unused
+// below their count).  Helpers here keep their values in scalars, never in
+// indexed local arrays, so that nothing goes through local memory.
+FDTDB_HD inline double avg_points (int nmat, double v0, double v1, double v2, double v3)
 {
-  if (c.nmat == 1)
-    return v[0];
-  if (c.nmat == 2)
-    return (v[0] + v[1]) / 2.0;
-  return ((v[0] + v[1]) / 2.0 + (v[2] + v[3]) / 2.0) / 2.0;
+  if (nmat == 1)
+    return v0;
+  if (nmat == 2)
+    return (v0 + v1) / 2.0;
+  return ((v0 + v1) / 2.0 + (v2 + v3) / 2.0) / 2.0;
+}
+
+FDTDB_HD inline double material_at (const GeomDev &g, const CompDev &c, const double *m, int j, int x, int y, int z)
+{
+  return m[lin (g, x + c.m[j][0], y + c.m[j][1], z + c.m[j][2])];
 }
 
 FDTDB_HD inline double material_avg (const GeomDev &g, const CompDev &c, const double *m, int x, int y, int z)
 {
-  double v[4];
-  for (int j = 0; j < c.nmat; ++j)
-    v[j] = m[lin (g, x + c.m[j][0], y + c.m[j][1], z + c.m[j][2])];
-  return avg_points (c, v);
+  const double v0 = material_at (g, c, m, 0, x, y, z);
+  const double v1 = c.nmat > 1 ? material_at (g, c, m, 1, x, y, z) : 0.0;
+  const double v2 = c.nmat > 2 ? material_at (g, c, m, 2, x, y, z) : 0.0;
+  const double v3 = c.nmat > 3 ? material_at (g, c, m, 3, x, y, z) : 0.0;
+  return avg_points (c.nmat, v0, v1, v2, v3);
 }
 
 FDTDB_HD inline double sigma_avg (const CompDev &c, const double *s, int axis, int x, int y, int z)
 {
-  int p[3] = {x, y, z};
-  double v[4];
-  for (int j = 0; j < c.nmat; ++j)
-    v[j] = s[p[axis] + c.m[j][axis]];
-  return avg_points (c, v);
+  const int q = axis == 0 ? x : (axis == 1 ? y : z);
+  const double v0 = s[q + c.m[0][axis]];
+  const double v1 = c.nmat > 1 ? s[q + c.m[1][axis]] : 0.0;
+  const double v2 = c.nmat > 2 ? s[q + c.m[2][axis]] : 0.0;
+  const double v3 = c.nmat > 3 ? s[q + c.m[3][axis]] : 0.0;
+  return avg_points (c.nmat, v0, v1, v2, v3);
 }
 
 // Drude averaging of plasma frequency / collision rate: the two-point form
@@ -62,12 +72,13 @@ FDTDB_HD inline double sigma_avg (const CompDev &c, const double *s, int axis, i
 // (Source/Layout/Approximation.cpp:58-165).
 FDTDB_HD inline double drude_avg (const GeomDev &g, const CompDev &c, const double *m, int x, int y, int z)
 {
-  double v[4];
-  for (int j = 0; j < c.nmat; ++j)
-    v[j] = m[lin (g, x + c.m[j][0], y + c.m[j][1], z + c.m[j][2])];
+  const double v0 = material_at (g, c, m, 0, x, y, z);
+  const double v1 = material_at (g, c, m, 1, x, y, z);
   if (c.nmat == 2)
-    return (v[0] + v[1]) / 2.0;
-  return (v[0] + v[1] + v[2] + v[3]) / 4.0;
+    return (v0 + v1) / 2.0;
+  const double v2 = material_at (g, c, m, 2, x, y, z);
+  const double v3 = material_at (g, c, m, 3, x, y, z);
+  return (v0 + v1 + v2 + v3) / 4.0;
 }
 
 // Incident value of absolute component `k` at integer cell position pos,
@@ -78,7 +89,6 @@ FDTDB_HD inline double incident_value (const GeomDev &g, const double *inc, int 
 {
   double d_diff = k >= 3 ? 0.5 : 0.0;
   double d;
-  const int pos[3] = {px, py, pz};
   if (g.drop == 0)
   {
     double x = ((double) px + g.min_fp[k][0]) - g.zero_inc[0];
@@ -90,8 +100,9 @@ FDTDB_HD inline double incident_value (const GeomDev &g, const double *inc, int 
   {
     // 2-D / 1-D: the mode's own form (InternalScheme.cpp:110-307)
     const int a0 = g.inc_ax[0], a1 = g.inc_ax[1];
-    double u = ((double) pos[a0] + g.min_fp[k][a0]) - g.zero_inc[a0];
-    double v = ((double) pos[a1] + g.min_fp[k][a1]) - g.zero_inc[a1];
+    const int p0 = a0 == 0 ? px : (a0 == 1 ? py : pz), p1 = a1 == 0 ? px : (a1 == 1 ? py : pz);
+    double u = ((double) p0 + g.min_fp[k][a0]) - g.zero_inc[a0];
+    double v = ((double) p1 + g.min_fp[k][a1]) - g.zero_inc[a1];
     d = u * g.inc_k[0] + v * g.inc_k[1] - d_diff;
   }
   double cd1 = (double) ((int) d);
@@ -144,18 +155,18 @@ FDTDB_HD inline void plain_component (const PlainHalf &p, int ci, int inc_len, i
     cb = dt / (material * p.mat_modifier * dx);
   }
 
-  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
   const double *o1 = p.opp[c.opp1];
   const double *o2 = p.opp[c.opp2];
   if (o1)
   {
-    v[0] = o1[lin (g, x + c.d11[0], y + c.d11[1], z + c.d11[2])];
-    v[1] = o1[lin (g, x + c.d12[0], y + c.d12[1], z + c.d12[2])];
+    v0 = o1[lin (g, x + c.d11[0], y + c.d11[1], z + c.d11[2])];
+    v1 = o1[lin (g, x + c.d12[0], y + c.d12[1], z + c.d12[2])];
   }
   if (o2)
   {
-    v[2] = o2[lin (g, x + c.d21[0], y + c.d21[1], z + c.d21[2])];
-    v[3] = o2[lin (g, x + c.d22[0], y + c.d22[1], z + c.d22[2])];
+    v2 = o2[lin (g, x + c.d21[0], y + c.d21[1], z + c.d21[2])];
+    v3 = o2[lin (g, x + c.d22[0], y + c.d22[1], z + c.d22[2])];
   }
   if (p.use_tfsf)
   {
@@ -168,11 +179,18 @@ FDTDB_HD inline void plain_component (const PlainHalf &p, int ci, int inc_len, i
                                       z + tm.aux[2]);
         if (tm.negate < 0)
           diff *= -1.0;
-        v[tm.slot] -= diff;
+        if (tm.slot == 0)
+          v0 -= diff;
+        else if (tm.slot == 1)
+          v1 -= diff;
+        else if (tm.slot == 2)
+          v2 -= diff;
+        else
+          v3 -= diff;
       }
     }
   }
-  double tmp = v[1] - v[0] - v[3] + v[2] - 0.0 * dx;
+  double tmp = v1 - v0 - v3 + v2 - 0.0 * dx;
   double nv = val * ca + tmp * cb;
   // J / M current source: -= (I dx) Cb on the freshly updated value, before
   // D -> E (Scheme.inc.h:1171-1260, InternalScheme.inc.h:792-795, 2423-2449)

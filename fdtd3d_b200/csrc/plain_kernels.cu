@@ -35,7 +35,7 @@ __global__ void __launch_bounds__ (256) plain_half_kernel (PlainHalf p, int inc_
     const int64_t r = tid / iz;
     const int y = (int) (r % iy) + ((p.g.drop & 2) ? 0 : 1);
     const int x = (int) (r / iy) + ((p.g.drop & 1) ? 0 : 1);
-#pragma unroll 1
+#pragma unroll
     for (int ci = 0; ci < 3; ++ci)
     {
       if (p.comp[ci].exists)

@@ -401,7 +401,10 @@ std::string build_geometry (const fdtd_config &cfg, Geometry &g)
       return "grid size out of range";
     if (cfg.use_pml && (cfg.pml[a] < 0 || 2 * cfg.pml[a] >= g.n[a]))
       return "PML size out of range";
-    if (cfg.use_tfsf && (cfg.tfsf_left[a] < 1 || cfg.tfsf_right[a] < 1
+    // a right size of 0 puts that face on the grid's last node, where no
+    // interior cell takes its terms (the reference's own tests run
+    // --tfsf-size-right x:0 for one-sided incidence, Tests/suite/t7.4)
+    if (cfg.use_tfsf && (cfg.tfsf_left[a] < 1 || cfg.tfsf_right[a] < 0
                          || cfg.tfsf_left[a] + cfg.tfsf_right[a] >= g.n[a]))
       return "TF/SF size out of range";
   }

@@ -100,8 +100,8 @@ typedef struct
   int mode;                 /* FDTD_MODE_* */
   int size[3];              /* the axis a 2-D mode drops is ignored */
   int pml[3];
-  int tfsf_left[3];
-  int tfsf_right[3];
+  int tfsf_left[3];         /* >= 1 */
+  int tfsf_right[3];        /* >= 0 (0: no face on that side) */
   double dx;
   double wavelength;
   double courant;

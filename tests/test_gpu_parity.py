@@ -37,6 +37,9 @@ CASES = {
                              tfsf_right=5, teta=60, phi=20, psi=45),
     "dim3_boundary_source": dict(mode=3, size=14, point_source=(0, 7, 7), point_source_mask=1 << 1,
                                  teta=0, phi=0, psi=0),
+    # one-sided TF/SF: a right size of 0 leaves those faces without terms
+    "dim3_tfsf_right_zero": dict(mode=3, size=(18, 16, 20), use_pml=True, pml=3, use_tfsf=True, tfsf_left=(5, 5, 6),
+                                 tfsf_right=(0, 5, 0), teta=30, phi=45, psi=20),
     "dim3_large_tiles": dict(mode=3, size=(40, 37, 70), use_pml=True, pml=(5, 4, 6), use_tfsf=True,
                              tfsf_left=(9, 8, 12), tfsf_right=(10, 9, 11), teta=30, phi=45, psi=0,
                              point_source=(20, 18, 35), point_source_mask=(1 << 0) | (1 << 5)),
