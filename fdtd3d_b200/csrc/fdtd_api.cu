@@ -154,6 +154,8 @@ struct fdtd_ctx
   // second step's H-incident update overwrites it)
   Tf2Pass tf2;
   bool tf2_on = false;
+  long long tf2_cells[4] = {0, 0, 0, 0};   // cells and boxes of each pass's region (verbose plan print)
+  int tf2_boxes[4] = {0, 0, 0, 0};
   double *hinc_keep = nullptr;
   TfsfBand band;                          // TF/SF post pass of the sweep (band.cells > 0 when in use)
   std::vector<BandBox> band_host;         // its boxes, on the host
@@ -864,9 +866,9 @@ std::string plan_shell (fdtd_ctx *ctx, void *const e[2][3], void *const h[2][3],
   return "";
 }
 
-// TF/SF with the two-step scheme: the regions of the pair's correction
-// passes (which must keep two cells clear of the PML shell the single steps
-// take), their CTA tables and scratch arrays.
+// TF/SF with the two-step scheme: the supports of the pair's corrections
+// (which must keep two cells clear of the PML shell the single steps take)
+// and the correction kernel's tiles.
 std::string plan_tfsf2 (fdtd_ctx *ctx)
 {
   std::vector<Tf2Box> rg[4];
@@ -882,39 +884,31 @@ std::string plan_tfsf2 (fdtd_ctx *ctx)
         if (b.lo[0] < cx0 + 2 || b.hi[0] > cx1 - 2 || b.lo[1] < cy0 + 2 || b.hi[1] > cy1 - 2)
           return "the TF/SF corrections reach the PML shell";
   }
-  std::vector<int2> bl[4];
   for (int q = 0; q < 4; ++q)
-    if (!(why = tfsf2_blocks (rg[q], bl[q])).empty ())
-      return why;
+  {
+    ctx->tf2_cells[q] = 0;
+    ctx->tf2_boxes[q] = (int) rg[q].size ();
+    for (const Tf2Box &b : rg[q])
+      ctx->tf2_cells[q] += (long long) (b.hi[0] - b.lo[0]) * (b.hi[1] - b.lo[1]) * (b.hi[2] - b.lo[2]);
+  }
+  std::vector<Tf2Tile> tiles;
+  unsigned smem = 0;
+  if (!(why = tfsf2_tiles (ctx->fused, rg, tiles, smem)).empty () || !(why = tfsf2_configure (smem)).empty ())
+    return why;
   Tf2Pass &t = ctx->tf2;
   const Geometry &g = ctx->g;
-  const size_t n = (size_t) g.cells;
-  if (!t.scratch[0])
+  if (!ctx->hinc_keep && dalloc (ctx, (void **) &ctx->hinc_keep, (size_t) g.inc_len * sizeof (double)) != FDTD_OK)
+    return "allocation of the TF/SF incident copy failed";
+  // the tile table (re)allocated at its size
+  if (!tiles.empty ())
   {
-    for (int k = 0; k < 9; ++k)
-      if (dalloc (ctx, (void **) &t.scratch[k], n * sizeof (float)) != FDTD_OK)
-        return "allocation of the TF/SF scratch failed";
-    if (dalloc (ctx, (void **) &ctx->hinc_keep, (size_t) g.inc_len * sizeof (double)) != FDTD_OK)
-      return "allocation of the TF/SF scratch failed";
+    const size_t bytes = tiles.size () * sizeof (Tf2Tile);
+    if (dalloc (ctx, (void **) &t.tiles, bytes, false) != FDTD_OK ||
+        cudaMemcpyAsync (t.tiles, tiles.data (), bytes, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+      return "upload of the TF/SF tiles failed";
   }
-  // tables (re)allocated at their sizes
-  auto upload = [&] (void **dst, const void *src, size_t bytes) -> bool {
-    if (dalloc (ctx, dst, bytes, false) != FDTD_OK)
-      return false;
-    return cudaMemcpyAsync (*dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream) == cudaSuccess;
-  };
-  for (int q = 0; q < 4; ++q)
-  {
-    if (!upload ((void **) &t.boxes[q], rg[q].data (), rg[q].size () * sizeof (Tf2Box)) ||
-        !upload ((void **) &t.blk[q], bl[q].data (), bl[q].size () * sizeof (int2)))
-      return "upload of the TF/SF tables failed";
-    t.nblk[q] = (int) bl[q].size ();
-  }
-  // the scratch must be zero outside the regions: clear it whenever they may
-  // have changed
-  for (int k = 0; k < 9; ++k)
-    if (cudaMemsetAsync (t.scratch[k], 0, n * sizeof (float), ctx->stream) != cudaSuccess)
-      return "TF/SF scratch clear failed";
+  t.ntiles = (int) tiles.size ();
+  t.smem = smem;
   if (cudaStreamSynchronize (ctx->stream) != cudaSuccess)
     return "TF/SF set-up failed";
   ctx->tf2_on = true;
@@ -1113,6 +1107,10 @@ int plan_sweep (fdtd_ctx *ctx)
                       "(%d/%d/%d/%d)\n", ctx->shell1.work.nlist, ctx->shell1.items[0], ctx->shell1.items[1],
                       ctx->shell1.items[2], ctx->shell1.items[3], ctx->shell2.work.nlist, ctx->shell2.items[0],
                       ctx->shell2.items[1], ctx->shell2.items[2], ctx->shell2.items[3]);
+      if (ctx->tb2_state >= 1 && ctx->tf2_on)
+        std::fprintf (stderr, "tfsf2: support boxes %d/%d/%d/%d cells %lld/%lld/%lld/%lld tiles %d smem %u\n",
+                      ctx->tf2_boxes[0], ctx->tf2_boxes[1], ctx->tf2_boxes[2], ctx->tf2_boxes[3], ctx->tf2_cells[0],
+                      ctx->tf2_cells[1], ctx->tf2_cells[2], ctx->tf2_cells[3], ctx->tf2.ntiles, ctx->tf2.smem);
     }
   return FDTD_OK;
 }

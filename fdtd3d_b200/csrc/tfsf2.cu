@@ -10,11 +10,13 @@
 //   dE1 = S im dE(t1)                     dH1 = S (curlH dE1 + dH(t1))
 //   dE2 = dE1 + S im (curlE dH1 + dE(t2)) dH2 = dH1 + S (curlH dE2 + dH(t2))
 // with curlH / curlE the step's own curls (E at c and c + e_a for H, H at c
-// and c - e_a for E), evaluated in four passes over the supports (the term
-// boxes grown by up to two cells), each cell evaluating the terms that cover
-// it (a mask per region box) once.
-// Every cell of the supports takes the plain update in both steps (no PML,
-// no point source), which the host checks.
+// and c - e_a for E).  One kernel evaluates the four in shared memory, tile
+// by tile: a tile owns a box of the support of dH2 (the TF/SF term boxes
+// grown by up to two cells, which holds the support of dE2) and recomputes
+// the intermediate corrections over a halo of one cell below and two above;
+// only the fields of its own cells are read and written in HBM (E += dE2,
+// H += dH2).  Every cell of the supports takes the plain update in both
+// steps (no PML, no point source), which the host checks.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -53,151 +55,238 @@ __device__ __forceinline__ void stf<__half> (__half *p, size_t i, float v)
   p[i] = __float2half_rn (v);
 }
 
-// TF/SF change of the curl of component k at (x, y, z) (the single-step
-// kernels' tfsf_curl): each term whose box holds the cell subtracts the
-// incident value from one neighbour of the curl (n1 - n0) - (n3 - n2).
-__device__ __forceinline__ float term_curl (const FusedParams &p, int k, const double *inc, int *err, int x, int y,
-                                            int z)
+// TF/SF change of the curl of component k at (x, y, z) over the terms of
+// `mask` (bit t: term t of component k; those that reach the tile): each
+// term whose box holds the cell subtracts the incident value from one
+// neighbour of the curl (n1 - n0) - (n3 - n2), as the single-step kernels'
+// tfsf_curl does.
+__device__ __noinline__ float term_value (const FusedParams &p, int k, int t, const double *inc, int *err, int x,
+                                         int y, int z)
 {
-  const CompDev &c = p.comp[k];
-  float d = 0.f;
-  for (int t = 0; t < c.nterms; ++t)
+  const TermDev &tm = p.comp[k].term[t];
+  const double diff = inc_at (p.g, inc, p.inc_len, err, tm.inc_comp, x + tm.aux[0], y + tm.aux[1], z + tm.aux[2]);
+  const float dv = (float) (diff * tm.negate) * p.inc_scale[tm.inc_comp];
+  return (tm.slot == 0 || tm.slot == 3) ? dv : -dv;
+}
+
+// The cells of an X x Y x Z box, z fastest, strided over the CTA's threads
+// (q = (x Y + y) Z + z); one division at the start, carries after it.
+struct Walk
+{
+  int q, x, y, z, Y, Z, dx, dy, dz;
+  __device__ Walk (int Yd, int Zd) : Y (Yd), Z (Zd)
   {
-    const TermDev &tm = c.term[t];
-    if (x >= tm.lo[0] && x < tm.hi[0] && y >= tm.lo[1] && y < tm.hi[1] && z >= tm.lo[2] && z < tm.hi[2])
-    {
-      const double diff = inc_at (p.g, inc, p.inc_len, err, tm.inc_comp, x + tm.aux[0], y + tm.aux[1],
-                                  z + tm.aux[2]);
-      const float dv = (float) (diff * tm.negate) * p.inc_scale[tm.inc_comp];
-      d += (tm.slot == 0 || tm.slot == 3) ? dv : -dv;
-    }
+    q = threadIdx.x;
+    z = q % Z;
+    y = (q / Z) % Y;
+    x = (q / Z) / Y;
+    const int s = blockDim.x;
+    dz = s % Z;
+    dy = (s / Z) % Y;
+    dx = (s / Z) / Y;
   }
-  return d;
-}
+  __device__ void next ()
+  {
+    q += blockDim.x;
+    z += dz;
+    int c = z >= Z;
+    z -= c ? Z : 0;
+    y += dy + c;
+    c = y >= Y;
+    y -= c ? Y : 0;
+    x += dx + c;
+  }
+};
 
-// The same over the terms of `mask` (bit t: term t of component k), those
-// that overlap the cell's box.
-__device__ __forceinline__ float term_curl_masked (const FusedParams &p, int k, unsigned mask, const double *inc,
-                                                   int *err, int x, int y, int z)
+// One tile: own box O = [lo, hi).  Shared memory holds, per axis, the E
+// corrections over D_E = [lo - 1, hi + 2), the H corrections over
+// D_H = [lo - 1, hi + 1) (three components each) and eps over
+// [lo - 1, hi + 3) (im = 2 / (eps + eps') of an E component at c reads eps
+// at c and c + e_k).  Both correction arrays start at zero.  Each step's
+// correction is its curl part, computed over the tile's phase box (where it
+// can be nonzero: the supports are slabs a few cells thick), plus its TF/SF
+// terms, added term by term over the cells of each term's box only:
+//   1. dE1 = S im dE(t1)                                  (terms only)
+//   2. dH1 = S curlH dE1 + S dH(t1)            (E at c, c + e_a: in D_E)
+//   3. dE2 = dE1 + S im curlE dH1 + S im dE(t2), in place (H at c, c - e_a)
+//   4. dH2 = dH1 + S curlH dE2 + S dH(t2) over O; the fields of O take
+//      E += dE2 and H += dH2 where nonzero.
+template <typename T>
+__global__ void __launch_bounds__ (256, 3) tfsf2_fused (const __grid_constant__ FusedParams p, const Tf2Tile *tiles,
+                                                        const double *inc_h1, const double *inc_e1,
+                                                        const double *inc_h2, const double *inc_e2, int *err)
 {
-  const CompDev &c = p.comp[k];
-  float d = 0.f;
-#pragma unroll
-  for (int t = 0; t < kMaxTerms; ++t)
-    if ((mask >> t) & 1u)
-    {
-      const TermDev &tm = c.term[t];
-      if (!(x >= tm.lo[0] && x < tm.hi[0] && y >= tm.lo[1] && y < tm.hi[1] && z >= tm.lo[2] && z < tm.hi[2]))
-        continue;
-      const double diff = inc_at (p.g, inc, p.inc_len, err, tm.inc_comp, x + tm.aux[0], y + tm.aux[1],
-                                  z + tm.aux[2]);
-      const float dv = (float) (diff * tm.negate) * p.inc_scale[tm.inc_comp];
-      d += (tm.slot == 0 || tm.slot == 3) ? dv : -dv;
-    }
-  return d;
-}
-
-// 2 / (eps + eps') of E component k at cell index c (1 without eps)
-__device__ __forceinline__ float inv_m (const FusedParams &p, int k, size_t c, size_t sx, int nz)
-{
-  if (!p.eps)
-    return 1.f;
-  const size_t st = k == 0 ? sx : (k == 1 ? (size_t) nz : 1);
-  return __fdividef (2.f, p.eps[c] + p.eps[c + st]);
-}
-
-__device__ __forceinline__ bool box_cell (const Tf2Box &b, int first, int &x, int &y, int &z)
-{
-  const unsigned ez = (unsigned) (b.hi[2] - b.lo[2]), ey = (unsigned) (b.hi[1] - b.lo[1]);
-  const unsigned n = ez * ey * (unsigned) (b.hi[0] - b.lo[0]);
-  const unsigned r = (unsigned) first + threadIdx.x;
-  if (r >= n)
-    return false;
-  const unsigned q = r / ez;
-  z = b.lo[2] + (int) (r - q * ez);
-  y = b.lo[1] + (int) (q % ey);
-  x = b.lo[0] + (int) (q / ey);
-  return true;
-}
-
-// The four passes over their regions (one cell per thread; every cell
-// evaluates only the terms of its box's mask):
-//   A over T_E:  dE1 = S im dE(t1)                         -> sE1
-//   B over R_H1: dH1 = S (curlH sE1 + dH(t1))              -> sH1
-//   C over R_E:  dE2 = sE1 + S im (curlE sH1 + dE(t2))     -> sE2, E_new += dE2
-//   D over R_H2: dH2 = sH1 + S (curlH sE2 + dH(t2))        -> H_new += dH2
-// T_E holds the E term cells, R_H1 the support of dH1, R_E that of dE1 and
-// dE2, R_H2 that of dH2; sE1, sH1 and sE2 are zero outside T_E, R_H1 and R_E
-// (never written there).
-template <typename T, int PASS>
-__global__ void __launch_bounds__ (256) tfsf2_pass (const __grid_constant__ FusedParams p, const Tf2Pass pass,
-                                                    const double *inc, int *err)
-{
-  const int2 bk = pass.blk[PASS][blockIdx.x];
-  const Tf2Box &box = pass.boxes[PASS][bk.x];
-  int x, y, z;
-  if (!box_cell (box, bk.y, x, y, z))
-    return;
-  const unsigned mask = box.mask;
-  const int ny = p.g.n[1], nz = p.g.n[2];
+  extern __shared__ float tf_smem[];
+  const Tf2Tile &t = tiles[blockIdx.x];
+  const unsigned mask = t.mask;
+  const int ex = t.hi[0] - t.lo[0], ey = t.hi[1] - t.lo[1], ez = t.hi[2] - t.lo[2];
+  const int eY = ey + 3, eZ = ez + 3, nE = (ex + 3) * eY * eZ, dEx = eY * eZ;
+  const int hY = ey + 2, hZ = ez + 2, nH = (ex + 2) * hY * hZ, dHx = hY * hZ;
+  const int pY = ey + 4, pZ = ez + 4, nP = (ex + 4) * pY * pZ;
+  float *const sE = tf_smem;
+  float *const sH = sE + 3 * nE;
+  float *const sP = sH + 3 * nH;
+  const int nx = p.g.n[0], ny = p.g.n[1], nz = p.g.n[2];
   const size_t sx = (size_t) ny * nz, sy = nz;
   const float S = p.courant;
-  float *const *sE1 = pass.scratch;
-  float *const *sH1 = pass.scratch + 3;
-  float *const *sE2 = pass.scratch + 6;
-  const size_t id = (size_t) x * sx + (size_t) y * sy + z;
-  if (PASS == 0 || PASS == 2)
+  const int o[3] = {t.lo[0] - 1, t.lo[1] - 1, t.lo[2] - 1};   // origin of every domain
+  const bool has_eps = p.eps != nullptr;
+
+  // zero corrections (both arrays: 3 (nE + nH) floats, sE 16-byte aligned)
   {
-    float cu[3] = {0.f, 0.f, 0.f};
-    if (PASS == 2)
+    const int n4 = 3 * (nE + nH) / 4;
+    float4 *z4 = reinterpret_cast<float4 *> (sE);
+    for (int i = threadIdx.x; i < n4; i += blockDim.x)
+      z4[i] = make_float4 (0.f, 0.f, 0.f, 0.f);
+    for (int i = 4 * n4 + threadIdx.x; i < 3 * (nE + nH); i += blockDim.x)
+      sE[i] = 0.f;
+  }
+  // eps over its domain (indices clamped to the grid: only cells of the
+  // supports, two cells inside the faces, use it)
+  if (has_eps)
+    for (Walk w (pY, pZ); w.q < nP; w.next ())
     {
-      cu[0] = (sH1[2][id] - sH1[2][id - sy]) - (sH1[1][id] - sH1[1][id - 1]);
-      cu[1] = (sH1[0][id] - sH1[0][id - 1]) - (sH1[2][id] - sH1[2][id - sx]);
-      cu[2] = (sH1[1][id] - sH1[1][id - sx]) - (sH1[0][id] - sH1[0][id - sy]);
+      const int x = min (o[0] + w.x, nx - 1), y = min (o[1] + w.y, ny - 1), z = min (o[2] + w.z, nz - 1);
+      sP[w.q] = p.eps[(size_t) x * sx + (size_t) y * sy + z];
+    }
+  __syncthreads ();
+  // S im of E component k at domain cell (qx, qy, qz)
+  auto s_im = [&] (int k, int qx, int qy, int qz) -> float {
+    if (!has_eps)
+      return S;
+    const int q = (qx * pY + qy) * pZ + qz;
+    const int st = k == 0 ? pY * pZ : (k == 1 ? pZ : 1);
+    return S * __fdividef (2.f, sP[q] + sP[q + st]);
+  };
+  // the TF/SF terms of the family kb .. kb + 2 (E: 0, H: 3) over the cells
+  // of the local domain d0 .. d1 - 1: for each cell of a term's box,
+  // add (k - kb, cell, term value).  Pass j takes every component's j-th
+  // term (the components write their own arrays); the CTA synchronises
+  // after each pass (two terms of a component may share a cell).
+  auto terms = [&] (int kb, const double *inc, int d0, const int d1[3], auto &&add) {
+    unsigned mk[3];
+    int passes = 0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+    {
+      mk[c] = (mask >> (4 * (kb + c))) & 15u;
+      passes = max (passes, __popc (mk[c]));
+    }
+#pragma unroll 1
+    for (int j = 0; j < passes; ++j)
+    {
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+      {
+        if (!mk[c])
+          continue;
+        const int tt = __ffs (mk[c]) - 1;
+        mk[c] &= mk[c] - 1;
+        const TermDev &tm = p.comp[kb + c].term[tt];
+        int b0[3], b1[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+        {
+          b0[a] = max (tm.lo[a] - o[a], d0);
+          b1[a] = min (tm.hi[a] - o[a], d1[a]);
+        }
+        if (b0[0] >= b1[0] || b0[1] >= b1[1] || b0[2] >= b1[2])
+          continue;
+        const int bY = b1[1] - b0[1], bZ = b1[2] - b0[2], nb = (b1[0] - b0[0]) * bY * bZ;
+        for (Walk w (bY, bZ); w.q < nb; w.next ())
+        {
+          const int qx = b0[0] + w.x, qy = b0[1] + w.y, qz = b0[2] + w.z;
+          add (c, qx, qy, qz, term_value (p, kb + c, tt, inc, err, o[0] + qx, o[1] + qy, o[2] + qz));
+        }
+      }
+      __syncthreads ();
+    }
+  };
+  // the cells of phase box f (local x, y, z)
+  auto box_walk = [&] (int f, auto &&body) {
+    const int b0 = t.ph[f][0], b1 = t.ph[f][1], b2 = t.ph[f][2];
+    const int bY = t.ph[f][4] - b1, bZ = t.ph[f][5] - b2, bX = t.ph[f][3] - b0;
+    if (bX <= 0 || bY <= 0 || bZ <= 0)
+      return;
+    for (Walk w (bY, bZ); w.q < bX * bY * bZ; w.next ())
+      body (b0 + w.x, b1 + w.y, b2 + w.z);
+  };
+  const int dE1[3] = {ex + 3, ey + 3, ez + 3}, dH1[3] = {ex + 2, ey + 2, ez + 2};
+  const int dO1[3] = {ex + 1, ey + 1, ez + 1};
+
+  // 1. dE1 on the E term cells
+  terms (0, inc_h1, 0, dE1, [&] (int k, int qx, int qy, int qz, float dv) {
+    sE[k * nE + (qx * eY + qy) * eZ + qz] += s_im (k, qx, qy, qz) * dv;
+  });
+  // 2. dH1: the curl of dE1 over its phase box, then the H terms
+  {
+    const float *E0 = sE, *E1 = sE + nE, *E2 = sE + 2 * nE;
+    box_walk (1, [&] (int qx, int qy, int qz) {
+      const int e = (qx * eY + qy) * eZ + qz, h = (qx * hY + qy) * hZ + qz;
+      sH[h] = S * ((E1[e + 1] - E1[e]) - (E2[e + eZ] - E2[e]));
+      sH[nH + h] = S * ((E2[e + dEx] - E2[e]) - (E0[e + 1] - E0[e]));
+      sH[2 * nH + h] = S * ((E0[e + eZ] - E0[e]) - (E1[e + dEx] - E1[e]));
+    });
+  }
+  __syncthreads ();
+  terms (3, inc_e1, 0, dH1, [&] (int m, int qx, int qy, int qz, float dv) {
+    sH[m * nH + (qx * hY + qy) * hZ + qz] += S * dv;
+  });
+  // 3. dE2: the curl of dH1 over its phase box, then the E terms (over U)
+  {
+    const float *H0 = sH, *H1 = sH + nH, *H2 = sH + 2 * nH;
+    box_walk (2, [&] (int qx, int qy, int qz) {
+      const int h = (qx * hY + qy) * hZ + qz, e = (qx * eY + qy) * eZ + qz;
+      const float cu[3] = {(H2[h] - H2[h - hZ]) - (H1[h] - H1[h - 1]), (H0[h] - H0[h - 1]) - (H2[h] - H2[h - dHx]),
+                           (H1[h] - H1[h - dHx]) - (H0[h] - H0[h - hZ])};
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        if (cu[k] != 0.f)
+          sE[k * nE + e] += s_im (k, qx, qy, qz) * cu[k];
+    });
+  }
+  __syncthreads ();
+  terms (0, inc_h2, 1, dH1, [&] (int k, int qx, int qy, int qz, float dv) {
+    sE[k * nE + (qx * eY + qy) * eZ + qz] += s_im (k, qx, qy, qz) * dv;
+  });
+  // 4. dH2 over O: the curl of dE2, then the H terms; then the fields
+  {
+    const float *E0 = sE, *E1 = sE + nE, *E2 = sE + 2 * nE;
+    for (Walk w (ey, ez); w.q < ex * ey * ez; w.next ())
+    {
+      const int qx = w.x + 1, qy = w.y + 1, qz = w.z + 1;
+      const int e = (qx * eY + qy) * eZ + qz, h = (qx * hY + qy) * hZ + qz;
+      sH[h] += S * ((E1[e + 1] - E1[e]) - (E2[e + eZ] - E2[e]));
+      sH[nH + h] += S * ((E2[e + dEx] - E2[e]) - (E0[e + 1] - E0[e]));
+      sH[2 * nH + h] += S * ((E0[e + eZ] - E0[e]) - (E1[e + dEx] - E1[e]));
+    }
+  }
+  __syncthreads ();
+  terms (3, inc_e2, 1, dO1, [&] (int m, int qx, int qy, int qz, float dv) {
+    sH[m * nH + (qx * hY + qy) * hZ + qz] += S * dv;
+  });
+  // the fields of O: all loads of a cell first, then the stores
+  for (Walk w (ey, ez); w.q < ex * ey * ez; w.next ())
+  {
+    const int qx = w.x + 1, qy = w.y + 1, qz = w.z + 1;
+    const int e = (qx * eY + qy) * eZ + qz, h = (qx * hY + qy) * hZ + qz;
+    const size_t id = (size_t) (o[0] + qx) * sx + (size_t) (o[1] + qy) * sy + (o[2] + qz);
+    float de[3], dh[3], fe[3], fh[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+    {
+      de[k] = sE[k * nE + e];
+      dh[k] = sH[k * nH + h];
+      fe[k] = de[k] != 0.f ? ldf (reinterpret_cast<const T *> (p.e_new[k]), id) : 0.f;
+      fh[k] = dh[k] != 0.f ? ldf (reinterpret_cast<const T *> (p.h_new[k]), id) : 0.f;
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k)
     {
-      const unsigned mk = (mask >> (4 * k)) & 15u;
-      const float d = cu[k] + (mk ? term_curl_masked (p, k, mk, inc, err, x, y, z) : 0.f);
-      const float v = d == 0.f ? 0.f : (S * inv_m (p, k, id, sx, nz)) * d;
-      if (PASS == 0)
-        sE1[k][id] = v;
-      else
-      {
-        const float e2 = sE1[k][id] + v;
-        sE2[k][id] = e2;
-        if (e2 != 0.f)
-        {
-          T *f = reinterpret_cast<T *> (p.e_new[k]);
-          stf (f, id, ldf (f, id) + e2);
-        }
-      }
-    }
-  }
-  else
-  {
-    // curlH of the E corrections (dE1 in pass B, dE2 in pass D)
-    float *const *sE = PASS == 1 ? sE1 : sE2;
-    const float ex = sE[0][id], ey = sE[1][id], ez = sE[2][id];
-    const float a[3] = {(sE[1][id + 1] - ey) - (sE[2][id + sy] - ez), (sE[2][id + sx] - ez) - (sE[0][id + 1] - ex),
-                        (sE[0][id + sy] - ex) - (sE[1][id + sx] - ey)};
-#pragma unroll
-    for (int m = 0; m < 3; ++m)
-    {
-      const unsigned mk = (mask >> (4 * (3 + m))) & 15u;
-      const float dh = S * (a[m] + (mk ? term_curl_masked (p, 3 + m, mk, inc, err, x, y, z) : 0.f));
-      if (PASS == 1)
-        sH1[m][id] = dh;
-      else
-      {
-        const float h2 = sH1[m][id] + dh;
-        if (h2 != 0.f)
-        {
-          T *f = reinterpret_cast<T *> (p.h_new[m]);
-          stf (f, id, ldf (f, id) + h2);
-        }
-      }
+      if (de[k] != 0.f)
+        stf (reinterpret_cast<T *> (p.e_new[k]), id, fe[k] + de[k]);
+      if (dh[k] != 0.f)
+        stf (reinterpret_cast<T *> (p.h_new[k]), id, fh[k] + dh[k]);
     }
   }
 }
@@ -321,49 +410,165 @@ std::string tfsf2_regions (const FusedParams &p, std::vector<Tf2Box> r[4])
   return "";
 }
 
-std::string tfsf2_blocks (const std::vector<Tf2Box> &boxes, std::vector<int2> &blk)
+// shared memory of a tile at most: three CTAs per SM
+constexpr unsigned kTileSmem = 74u * 1024u;
+
+std::string tfsf2_tiles (const FusedParams &p, const std::vector<Tf2Box> r[4], std::vector<Tf2Tile> &tiles,
+                         unsigned &smem)
 {
-  blk.clear ();
-  for (size_t q = 0; q < boxes.size (); ++q)
+  // the last support's boxes merged where two meet face to face with the
+  // same extent across (the cover cuts the thin slabs at every term box edge)
+  std::vector<Tf2Box> own = r[3];
+  for (bool merged = true; merged;)
   {
-    const Tf2Box &b = boxes[q];
-    const long long cells = (long long) (b.hi[0] - b.lo[0]) * (b.hi[1] - b.lo[1]) * (b.hi[2] - b.lo[2]);
-    if (cells >= (1ll << 31))
-      return "TF/SF box too large";
-    for (long long f = 0; f < cells; f += 256)
-      blk.push_back (make_int2 ((int) q, (int) f));
+    merged = false;
+    for (size_t i = 0; i < own.size () && !merged; ++i)
+      for (size_t j = 0; j < own.size () && !merged; ++j)
+      {
+        if (i == j)
+          continue;
+        for (int a = 0; a < 3 && !merged; ++a)
+        {
+          const int b = (a + 1) % 3, c = (a + 2) % 3;
+          if (own[i].hi[a] == own[j].lo[a] && own[i].lo[b] == own[j].lo[b] && own[i].hi[b] == own[j].hi[b] &&
+              own[i].lo[c] == own[j].lo[c] && own[i].hi[c] == own[j].hi[c])
+          {
+            own[i].hi[a] = own[j].hi[a];
+            own.erase (own.begin () + (long) j);
+            merged = true;
+          }
+        }
+      }
   }
+  tiles.clear ();
+  smem = 0;
+  for (const Tf2Box &b : own)
+  {
+    int ext[3], cnt[3];
+    for (int a = 0; a < 3; ++a)
+      ext[a] = b.hi[a] - b.lo[a];
+    // tile extents: up to 8 x 8 x 32 cells, or 16 x 16 across a box that is
+    // thin in z (a z face of the TF/SF box), shrunk until a tile's shared
+    // memory fits three CTAs per SM; boxes split evenly
+    const bool zthin = ext[2] <= 8;
+    int cap[3] = {zthin ? 16 : 8, zthin ? 16 : 8, 32};
+    for (;;)
+    {
+      unsigned nE = 1, nH = 1, nP = 1;
+      int big = 0;
+      for (int a = 0; a < 3; ++a)
+      {
+        const int d = std::min (ext[a], cap[a]);
+        nE *= (unsigned) (d + 3);
+        nH *= (unsigned) (d + 2);
+        nP *= (unsigned) (d + 4);
+        if (d > std::min (ext[big], cap[big]))
+          big = a;
+      }
+      if ((3u * (nE + nH) + nP) * sizeof (float) <= kTileSmem || std::min (ext[big], cap[big]) <= 2)
+        break;
+      cap[big] = std::min (ext[big], cap[big]) - 1;
+    }
+    for (int a = 0; a < 3; ++a)
+      cnt[a] = (ext[a] + cap[a] - 1) / cap[a];
+    for (int i = 0; i < cnt[0]; ++i)
+      for (int j = 0; j < cnt[1]; ++j)
+        for (int l = 0; l < cnt[2]; ++l)
+        {
+          Tf2Tile t;
+          const int idx[3] = {i, j, l};
+          for (int a = 0; a < 3; ++a)
+          {
+            t.lo[a] = b.lo[a] + ext[a] * idx[a] / cnt[a];
+            t.hi[a] = b.lo[a] + ext[a] * (idx[a] + 1) / cnt[a];
+          }
+          // the terms that reach the tile's E domain [lo - 1, hi + 2) (E
+          // components) or its H domain [lo - 1, hi + 1) (H components)
+          t.mask = 0;
+          for (int k = 0; k < 6; ++k)
+            for (int q = 0; q < p.comp[k].nterms; ++q)
+            {
+              const TermDev &tm = p.comp[k].term[q];
+              bool hit = true;
+              for (int a = 0; a < 3; ++a)
+                hit = hit && tm.lo[a] < t.hi[a] + (k < 3 ? 2 : 1) && tm.hi[a] > t.lo[a] - 1;
+              if (hit)
+                t.mask |= 1u << (4 * k + q);
+            }
+          // phase boxes: the supports of dE1, dH1 and dE2 within the phase
+          // domains D_E = [lo - 1, hi + 2), D_H = [lo - 1, hi + 1) and
+          // U = [lo, hi + 1), relative to lo - 1
+          for (int f = 0; f < 3; ++f)
+          {
+            int d0[3], d1[3], bl[3], bh[3];
+            for (int a = 0; a < 3; ++a)
+            {
+              d0[a] = f == 2 ? t.lo[a] : t.lo[a] - 1;
+              d1[a] = f == 1 ? t.hi[a] + 1 : t.hi[a] + (f == 0 ? 2 : 1);
+              bl[a] = 1 << 30;
+              bh[a] = -(1 << 30);
+            }
+            for (const Tf2Box &s : r[f])
+            {
+              int lo[3], hi[3];
+              bool ok = true;
+              for (int a = 0; a < 3; ++a)
+              {
+                lo[a] = std::max (s.lo[a], d0[a]);
+                hi[a] = std::min (s.hi[a], d1[a]);
+                ok = ok && lo[a] < hi[a];
+              }
+              if (!ok)
+                continue;
+              for (int a = 0; a < 3; ++a)
+              {
+                bl[a] = std::min (bl[a], lo[a]);
+                bh[a] = std::max (bh[a], hi[a]);
+              }
+            }
+            for (int a = 0; a < 3; ++a)
+            {
+              const bool empty = bl[a] >= bh[a];
+              t.ph[f][a] = (short) (empty ? 0 : bl[a] - (t.lo[a] - 1));
+              t.ph[f][3 + a] = (short) (empty ? 0 : bh[a] - (t.lo[a] - 1));
+            }
+          }
+          unsigned nE = 1, nH = 1, nP = 1;
+          for (int a = 0; a < 3; ++a)
+          {
+            nE *= (unsigned) (t.hi[a] - t.lo[a] + 3);
+            nH *= (unsigned) (t.hi[a] - t.lo[a] + 2);
+            nP *= (unsigned) (t.hi[a] - t.lo[a] + 4);
+          }
+          smem = std::max (smem, (3u * (nE + nH) + nP) * (unsigned) sizeof (float));
+          tiles.push_back (t);
+        }
+  }
+  if (smem > 200u * 1024u)
+    return "TF/SF tile too large";
   return "";
 }
 
 int launch_tfsf2 (const Tf2Pass &pass, const FusedParams &p, const double *inc_h1, const double *inc_e1,
                   const double *inc_h2, const double *inc_e2, int *err, cudaStream_t s)
 {
-  if (pass.nblk[2] <= 0)
+  if (pass.ntiles <= 0)
     return 0;
-  int n = 0;
-  auto go = [&] (auto kern, int q, const double *inc) {
-    if (pass.nblk[q] > 0)
-    {
-      kern<<<pass.nblk[q], 256, 0, s>>> (p, pass, inc, err);
-      ++n;
-    }
-  };
   if (p.fp16)
-  {
-    go (tfsf2_pass<__half, 0>, 0, inc_h1);
-    go (tfsf2_pass<__half, 1>, 1, inc_e1);
-    go (tfsf2_pass<__half, 2>, 2, inc_h2);
-    go (tfsf2_pass<__half, 3>, 3, inc_e2);
-  }
+    tfsf2_fused<__half><<<pass.ntiles, 256, pass.smem, s>>> (p, pass.tiles, inc_h1, inc_e1, inc_h2, inc_e2, err);
   else
-  {
-    go (tfsf2_pass<float, 0>, 0, inc_h1);
-    go (tfsf2_pass<float, 1>, 1, inc_e1);
-    go (tfsf2_pass<float, 2>, 2, inc_h2);
-    go (tfsf2_pass<float, 3>, 3, inc_e2);
-  }
-  return n;
+    tfsf2_fused<float><<<pass.ntiles, 256, pass.smem, s>>> (p, pass.tiles, inc_h1, inc_e1, inc_h2, inc_e2, err);
+  return 1;
+}
+
+std::string tfsf2_configure (unsigned smem)
+{
+  if (cudaFuncSetAttribute (tfsf2_fused<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute (tfsf2_fused<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem) !=
+          cudaSuccess)
+    return "TF/SF kernel shared-memory set-up failed";
+  return "";
 }
 
 }  // namespace fdtdb
