@@ -69,21 +69,33 @@ __device__ __noinline__ float term_value (const FusedParams &p, int k, int t, co
   return (tm.slot == 0 || tm.slot == 3) ? dv : -dv;
 }
 
+// q / d for 0 <= q < 2^22 and 1 <= d < 2^11 (rd = 1 / d rounded): the
+// float quotient is off by at most one, which the remainder corrects.
+__device__ __forceinline__ int small_div (int q, int d, float rd)
+{
+  int x = __float2int_rz (__int2float_rn (q) * rd);
+  const int r = q - x * d;
+  return x + (r >= d) - (r < 0);
+}
+
 // The cells of an X x Y x Z box, z fastest, strided over the CTA's threads
-// (q = (x Y + y) Z + z); one division at the start, carries after it.
+// (q = (x Y + y) Z + z); one decomposition at the start, carries after it.
 struct Walk
 {
   int q, x, y, z, Y, Z, dx, dy, dz;
   __device__ Walk (int Yd, int Zd) : Y (Yd), Z (Zd)
   {
+    const float rY = __frcp_rn ((float) Y), rZ = __frcp_rn ((float) Z);
     q = threadIdx.x;
-    z = q % Z;
-    y = (q / Z) % Y;
-    x = (q / Z) / Y;
+    int a = small_div (q, Z, rZ);
+    z = q - a * Z;
+    x = small_div (a, Y, rY);
+    y = a - x * Y;
     const int s = blockDim.x;
-    dz = s % Z;
-    dy = (s / Z) % Y;
-    dx = (s / Z) / Y;
+    a = small_div (s, Z, rZ);
+    dz = s - a * Z;
+    dx = small_div (a, Y, rY);
+    dy = a - dx * Y;
   }
   __device__ void next ()
   {
