@@ -63,7 +63,7 @@ TFSF = 32
 def kernel_label(step_kernel: str) -> str:
     if step_kernel == "sweep2_tma":
         return ("sweep2_kernel (lean / z-edge core, two time steps per pass) + sweep3d_kernel (x/y PML shell, "
-                "two single steps) + tfsf2_pass x4: E and H of two time steps")
+                "two single steps) + tfsf2_fused (TF/SF corrections of the pair): E and H of two time steps")
     if step_kernel == "sweep3d_tma":
         return ("sweep3d_kernel (lean / z-edge PML / PML / full item classes) + tfsf_post_kernel: "
                 "E and H of one time step")
