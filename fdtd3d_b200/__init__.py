@@ -57,7 +57,7 @@ EXPORTED = (
     "fdtd_last_error", "fdtd_stream", "fdtd_profile", "fdtd_kernel_time", "fdtd_step_kernel",
     "fdtd_batch_create", "fdtd_batch_upload_eps", "fdtd_batch_tune", "fdtd_batch_step", "fdtd_batch_sync",
     "fdtd_batch_download", "fdtd_batch_info", "fdtd_batch_last_error", "fdtd_batch_destroy",
-    "fdtd_objective", "fdtd_backward", "fdtd_dft_setup", "fdtd_dft_read", "fdtd_ntff",
+    "fdtd_objective", "fdtd_backward", "fdtd_dft_setup", "fdtd_dft_read", "fdtd_ntff", "fdtd_keep_previous_level",
     "fdtd_upload_material_async", "fdtd_download_field_async", "fdtd_download_field_scattered",
     "fdtd_incident_length", "fdtd_download_incident", "fdtd_set_wait_limit", "fdtd_batch_set_wait_limit",
     "fdtd_inject_alloc_failure",
@@ -157,6 +157,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "fdtd_dft_read": ([vp, vp], i),
         "fdtd_backward": ([vp, ctypes.POINTER(AdjointCfg), vp, vp], i),
         "fdtd_ntff": ([vp, vp, vp, vp, d, i, vp, vp], i),
+        "fdtd_keep_previous_level": ([vp, i], i),
         "fdtd_upload_material_async": ([vp, i, vp], i),
         "fdtd_download_field_async": ([vp, i, vp], i),
         "fdtd_download_field_scattered": ([vp, i, vp], i),
@@ -329,6 +330,10 @@ class Simulation:
     def launch_count(self) -> int:
         return int(self.lib.fdtd_launch_count(self._h))
 
+    def keep_previous_level(self, on: bool = True) -> None:
+        """FP32 / FP16 storage: keep the previous H level after every step() call (for ntff)."""
+        self._check(self.lib.fdtd_keep_previous_level(self._h, int(bool(on))), "keep_previous_level")
+
     def set_wait_limit(self, limit_ns: int) -> None:
         """Time limit of one grid-barrier wait of the adjoint kernel (<= 0: the default, 2 s)."""
         self._check(self.lib.fdtd_set_wait_limit(self._h, int(limit_ns)), "set_wait_limit")
@@ -499,7 +504,8 @@ class Batch:
 
 def ntff(sim_re: "Simulation", sim_im: "Simulation", left, right, teta: float, phis) -> np.ndarray:
     """NTFF values of the complex field sim_re + i sim_im (the sine- and
-    cosine-source runs, FP64 plain form, 3-D) over the box with faces at
+    cosine-source runs of one form, 3-D; FP32 / FP16-storage runs call
+    keep_previous_level before stepping) over the box with faces at
     left / right, at polar angle teta and each azimuth in phis (radians)."""
     lib = sim_re.lib
     lo = (ctypes.c_int * 3)(*[int(v) for v in left])

@@ -28,7 +28,8 @@
 // the real and imaginary parts ("coords re im" in TXT dumps, (re, im)
 // pairs in DAT dumps); material files then hold complex values, of which
 // the step uses the real parts, as the reference's does.  With it, --use-ntff (3-D) writes the
-// reference's NTFF files from the two runs (fdtd_ntff).
+// reference's NTFF files from the two runs (fdtd_ntff; with --precision fp32
+// or fp16s from the fast forms' fields).
 // Flags of subsystems outside the step path (MPI, BMP output, test
 // callbacks) are rejected with a message instead of being ignored.
 #include <sys/time.h>
@@ -962,9 +963,9 @@ int main (int argc, char **argv)
   }
   if ((o.scattered_res || o.scattered_interm) && !o.cfg.use_tfsf)
     return fail ("the scattered field needs --use-tfsf");
-  if (o.use_ntff && (!o.complex_values || o.cfg.mode != FDTD_MODE_DIM3 || o.cfg.precision != FDTD_PREC_FP64_PLAIN))
-    return fail ("--use-ntff needs --3d, --complex-field-values and the FP64 form (the reference computes the NTFF "
-                 "in its complex-field build only, for 3-D grids)");
+  if (o.use_ntff && (!o.complex_values || o.cfg.mode != FDTD_MODE_DIM3))
+    return fail ("--use-ntff needs --3d and --complex-field-values (the reference computes the NTFF in its "
+                 "complex-field build only, for 3-D grids)");
   // the complex-field build's run is the sine-source run (real part) plus i
   // times the cosine-source run (imaginary part): one context for each
   const int nrun = o.complex_values ? 2 : 1;
@@ -989,6 +990,9 @@ int main (int argc, char **argv)
     st = fdtd_create (&cfg, o.device, &ctx[r]);
     if (st)
       return fail (std::string ("fdtd_create: ") + fdtd_status_str (st) + ": " + fdtd_last_error ());
+    // the NTFF of an FP32 / FP16 run reads the previous H level
+    if (o.use_ntff && (st = fdtd_keep_previous_level (ctx[r], 1)))
+      return fail (std::string ("fdtd_keep_previous_level: ") + fdtd_last_error ());
   }
   const unsigned drop = dropped_axes (o.cfg.mode);
   int n[3] = {o.cfg.size[0], o.cfg.size[1], o.cfg.size[2]};

@@ -131,11 +131,10 @@ __device__ __forceinline__ void fast_component (const FastHalf &p, int ci, int *
   if (((p.cs_mask >> ci) & 1) && x == p.cs[0] && y == p.cs[1] && z == p.cs[2])
     curl -= (float) (*p.cs_val * p.g.dx) * p.cs_scale;
 
-  float inv_m = 1.f;
+  float inv_m = 1.f, m = 1.f;
   const float *mp = p.matc[ci] ? p.matc[ci] : p.mat;
   if (mp)
   {
-    float m;
     if (c.nmat == 1)
       m = mp[id];
     else if (c.nmat == 2)
@@ -156,7 +155,56 @@ __device__ __forceinline__ void fast_component (const FastHalf &p, int ci, int *
       interior = interior && pos[a] >= p.ilo[ci][a] && pos[a] < p.ihi[ci][a];
   }
   float f = ld (F, id);
-  if (interior)
+  // Drude cell: a nonzero plasma frequency or collision rate on the
+  // component's averaging stencil (getMetaMaterial: the mean of its two or
+  // four points; metamaterials run with PML, as the reference's do)
+  float w = 0.f, gm = 0.f;
+  if (p.meta)
+  {
+    for (int j = 0; j < c.nmat; ++j)
+    {
+      const size_t q = flin (g, x + c.m[j][0], y + c.m[j][1], z + c.m[j][2]);
+      w += p.om[q];
+      gm += p.ga[q];
+    }
+    const float inv_n = c.nmat == 4 ? 0.25f : (c.nmat == 2 ? 0.5f : 1.f);
+    w *= inv_n;
+    gm *= inv_n;
+  }
+  if (p.meta && (w != 0.f || gm != 0.f))
+  {
+    // X by the curl step (PML coefficients; sigma = 0 gives ca1 = 1,
+    // sq1 = S), the Drude recurrence to Z (the reference's b0 .. a2,
+    // InternalScheme.inc.h:2527-2532, in the scaled units), F from Z with
+    // material modifier 1 (InternalScheme.inc.h:2452-2640).  The recurrence
+    // Z_n = b0 X_n + b1 X_o + b2 X_pp - a1 Z_o - a2 Z_pp is evaluated on
+    // increments (b0 + b1 + b2 = 0 and 1 + a1 + a2 = 4 sq / A):
+    //   dZ = b0 dX - b2 dX_o + a2 dZ_o - (4 sq / A) Z_o,
+    // so that FP32 does not subtract nearly equal products of the fields;
+    // this path keeps the last increments dX_o, dZ_o per cell (xpp, zpp).
+    const int a0 = c.sig4, a1 = c.sig_cacb, a2 = c.sig5;
+    const float ca1 = p.tab[ci][0][pos[a1]];
+    const float sq1 = p.tab[ci][1][pos[a1]];
+    const float p5 = p.tab[ci][2][pos[a2]];
+    const float q5 = p.tab[ci][3][pos[a2]];
+    const float g4p = p.tab[ci][4][pos[a0]];
+    const float g4m = p.tab[ci][5][pos[a0]];
+    float *X = p.aux[ci];
+    const float xo = X[id], dxo = p.xpp[ci][id], zo = p.zd[ci][id], dzo = p.zpp[ci][id];
+    const float dt = p.dt;
+    const float sq = (dt * w) * (dt * w);
+    const float inv = 1.f / (4.f * m + 2.f * dt * m * gm + sq);
+    const float b0 = (4.f + 2.f * dt * gm) * inv, b2 = (4.f - 2.f * dt * gm) * inv;
+    const float a2c = (4.f * m - 2.f * dt * m * gm + sq) * inv;
+    const float dx = (ca1 - 1.f) * xo + sq1 * curl;
+    const float dz = b0 * dx - b2 * dxo + a2c * dzo - (4.f * sq * inv) * zo;
+    X[id] = xo + dx;
+    p.xpp[ci][id] = dx;
+    p.zd[ci][id] = zo + dz;
+    p.zpp[ci][id] = dz;
+    f = p5 * f + ((g4p - g4m) * zo + g4p * dz) * q5;
+  }
+  else if (interior)
   {
     f += p.courant * inv_m * curl;
   }

@@ -154,6 +154,13 @@ struct fdtd_ctx
   // second step's H-incident update overwrites it)
   Tf2Pass tf2;
   bool tf2_on = false;
+  bool stepped = false;   // a field update has run (the Drude state has a form)
+  // FP32 / FP16: keep the previous field level after every fdtd_step call
+  // (the NTFF averages H over two levels).  prev_src: where the previous H
+  // level is after the last call: 0 nowhere, 1 buffer set 1 - fcur, 2 hprev
+  bool keep_prev = false;
+  int prev_src = 0;
+  void *hprev[3] = {nullptr, nullptr, nullptr};
   long long tf2_cells[4] = {0, 0, 0, 0};   // cells and boxes of each pass's region (verbose plan print)
   int tf2_boxes[4] = {0, 0, 0, 0};
   double *hinc_keep = nullptr;
@@ -479,8 +486,6 @@ int alloc_fast (fdtd_ctx *ctx)
 {
   const Geometry &g = ctx->g;
   size_t n = (size_t) g.cells;
-  if (g.cfg.use_metamaterials && g.drop != 0)
-    return fail (ctx, FDTD_ERR_UNSUPPORTED, "2-D and 1-D metamaterials are provided by the FP64 plain form only");
   // the one-sweep 3-D kernels (register-blocked and TMA) are written for the
   // E_CENTERED stencil on cell-centred materials; H_CENTERED, double material
   // precision and the 2-D / 1-D modes run the per-cell kernels on one buffer set
@@ -564,9 +569,16 @@ int alloc_fast (fdtd_ctx *ctx)
     for (int a = 0; a < 3; ++a)
       p.cs[a] = ctx->cs_pos[a];
     p.cs_scale = (float) (h ? 1.0 : kEta0);
+    p.meta = g.cfg.use_metamaterials && g.cfg.use_pml;
+    p.dt = (float) g.dt;
+    p.om = ctx->drude32[h];       // omegape (E) / omegapm (H)
+    p.ga = ctx->drude32[2 + h];   // gammae (E) / gammam (H)
     for (int ci = 0; ci < 3; ++ci)
     {
       int k = ci + 3 * h;
+      p.xpp[ci] = ctx->xppb[0][k];
+      p.zd[ci] = ctx->zb[0][k];
+      p.zpp[ci] = ctx->zppb[0][k];
       p.comp[ci] = make_comp_dev (g, k);
       p.f[ci] = ctx->ff[k];
       p.aux[ci] = ctx->aux[k];
@@ -612,6 +624,9 @@ void select_fast_set (fdtd_ctx *ctx)
       p.f[ci] = ctx->ff[ci + 3 * h];
       p.aux[ci] = ctx->aux[ci + 3 * h];
       p.opp[ci] = ctx->ff[ci + 3 * (1 - h)];
+      p.xpp[ci] = ctx->xppb[ctx->fcur][ci + 3 * h];
+      p.zd[ci] = ctx->zb[ctx->fcur][ci + 3 * h];
+      p.zpp[ci] = ctx->zppb[ctx->fcur][ci + 3 * h];
     }
   }
 }
@@ -1389,16 +1404,14 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
   CK (cudaEventRecord (ctx->src_ev, ctx->stream));
   if ((r = dft_prepare (ctx, t_start, n)) != FDTD_OK)
     return r;
+  if (n > 1 || t_start > 0)
+    ctx->stepped = true;
   size_t ps_idx = 0;
   bool ps_ok = g.cfg.point_source_mask && point_source_index (g, &ps_idx);
   cudaStream_t s = ctx->stream;
   // current sources run the per-cell kernels
   const bool fused = ctx->kind != 0 && ctx->has_second && !ctx->mat32[1] && ctx->ps_interior && !ctx->cs_mask[0]
                      && !ctx->cs_mask[1];
-  if (ctx->kind != 0 && g.cfg.use_metamaterials && !fused)
-    return fail (ctx, FDTD_ERR_UNSUPPORTED,
-                 "FP32/FP16 metamaterials need the one-sweep 3-D kernel (E_CENTERED, uniform mu, interior point "
-                 "source, no current source)");
 
   for (uint32_t i = 0; i < n; ++i)
   {
@@ -1445,7 +1458,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
         if ((r = plan_sweep (ctx)) != FDTD_OK)
           return r;
       cudaEvent_t pe;
-      if (ctx->tb2_state >= 1 && i + 1 < n && ctx->dft_comp < 0)
+      if (ctx->tb2_state >= 1 && i + (ctx->keep_prev ? 2 : 1) < n && ctx->dft_comp < 0)
       {
         // steps t and t + 1 in one pass (no point source or Drude medium).
         // With TF/SF the incident grid takes both steps first (this step's
@@ -1498,6 +1511,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
         if ((r = prof_end (ctx, pe)) != FDTD_OK)
           return r;
         ctx->fcur = nw;
+        ctx->prev_src = 0;   // set 1 - fcur holds two steps back
         select_fast_set (ctx);
         ++i;
         continue;
@@ -1521,6 +1535,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
       if ((r = prof_end (ctx, pe)) != FDTD_OK)
         return r;
       ctx->fcur = nw;
+      ctx->prev_src = 1;   // set 1 - fcur holds the previous level
       select_fast_set (ctx);
       dft_step (ctx, i);
       continue;
@@ -1574,6 +1589,20 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
       }
       else
       {
+        if (h == 1)
+        {
+          // the per-cell kernels update in place: with keep_prev the last
+          // step of the call copies H before its H update
+          ctx->prev_src = 0;
+          if (ctx->keep_prev && i + 1 == n && ctx->hprev[0])
+          {
+            for (int ci = 0; ci < 3; ++ci)
+              if (g.comp[3 + ci].exists)
+                CK (cudaMemcpyAsync (ctx->hprev[ci], ctx->ff[3 + ci], (size_t) g.cells * elem_size (ctx->kind),
+                                     cudaMemcpyDeviceToDevice, s));
+            ctx->prev_src = 2;
+          }
+        }
         if (t > 0)
         {
           FastHalf &p = h ? ctx->fast_h : ctx->fast_e;
@@ -1690,6 +1719,10 @@ int fdtd_upload_material_device (fdtd_ctx *ctx, int which, const double *dev)
     CK (cudaMemcpyAsync (ctx->mat64[which], dev, n * sizeof (double), cudaMemcpyDeviceToDevice, ctx->stream));
     return FDTD_OK;
   }
+  if (which == 1 && ctx->g.cfg.use_metamaterials && ctx->stepped && !ctx->mat32[1] && ctx->has_second)
+    return fail (ctx, FDTD_ERR_UNSUPPORTED, "a 3-D FP32 / FP16 Drude run takes its mu map before its first step "
+                                            "(the map moves the run from the one-sweep to the per-cell kernels, "
+                                            "whose Drude state differs)");
   if (which > 1)
   {
     if (!ctx->dflag)
@@ -2123,8 +2156,11 @@ int fdtd_ntff (fdtd_ctx *re, fdtd_ctx *im, const int left[3], const int right[3]
     return fail (re, FDTD_ERR_ARG, "bad argument");
   const Geometry &g = re->g;
   const Geometry &gi = im->g;
-  if (re->kind != 0 || im->kind != 0)
-    return fail (re, FDTD_ERR_UNSUPPORTED, "the NTFF reads the FP64 plain form (it needs the previous H level)");
+  if (re->kind != im->kind)
+    return fail (re, FDTD_ERR_ARG, "the two runs must have the same form");
+  if (re->kind != 0 && (re->prev_src == 0 || im->prev_src == 0))
+    return fail (re, FDTD_ERR_STATE, "the NTFF needs the previous H level: call fdtd_keep_previous_level before "
+                                     "stepping an FP32 / FP16 run");
   if (g.cfg.mode != FDTD_MODE_DIM3 || gi.cfg.mode != FDTD_MODE_DIM3)
     return fail (re, FDTD_ERR_UNSUPPORTED, "the NTFF is 3-D (the reference's 2-D and 1-D forms are unreachable)");
   if (re->device != im->device || g.cfg.layout != gi.cfg.layout)
@@ -2157,6 +2193,7 @@ int fdtd_ntff (fdtd_ctx *re, fdtd_ctx *im, const int left[3], const int right[3]
   p.k = 2 * kPi / g.cfg.wavelength;
   p.teta = teta;
   p.h_centered = g.cfg.layout == 1;
+  p.kind = re->kind;
   fdtd_ctx *runs[2] = {re, im};
   for (int k = 0; k < 6; ++k)
   {
@@ -2164,11 +2201,23 @@ int fdtd_ntff (fdtd_ctx *re, fdtd_ctx *im, const int left[3], const int right[3]
       p.min_fp[k][a] = g.comp[k].min_fp[a];
     for (int q = 0; q < 2; ++q)
     {
-      // after a step the current level is 1 and the previous one 0 (two
-      // levels) or 2 (three), the reference's "after shift" accessors
-      p.cur[q][k] = runs[q]->f[k][1];
-      p.prev[q][k] = runs[q]->f[k][g.levels == 3 ? 2 : 0];
+      const fdtd_ctx *c = runs[q];
+      if (c->kind == 0)
+      {
+        // after a step the current level is 1 and the previous one 0 (two
+        // levels) or 2 (three), the reference's "after shift" accessors
+        p.cur[q][k] = c->f[k][1];
+        p.prev[q][k] = c->f[k][g.levels == 3 ? 2 : 0];
+      }
+      else
+      {
+        // FP32 / FP16 storage: the current set, the previous H where the
+        // last call left it (the E sums read the current level only)
+        p.cur[q][k] = c->ffb[c->fcur][k];
+        p.prev[q][k] = k < 3 ? nullptr : (c->prev_src == 1 ? c->ffb[1 - c->fcur][k] : c->hprev[k - 3]);
+      }
     }
+    p.scale[k] = k < 3 ? 1.0 : 1.0 / kEta0;
   }
   const int blocks = (int) std::max<int64_t> (1, std::min<int64_t> ((p.points + 255) / 256, 4 * re->sm_count));
   double *phi_dev = nullptr, *partial = nullptr, *sums = nullptr;
@@ -2205,6 +2254,24 @@ int fdtd_ntff (fdtd_ctx *re, fdtd_ctx *im, const int left[3], const int right[3]
     val /= std::sqrt (kEps0 / kMu0) / 2;
     out[i] = val;
   }
+  return FDTD_OK;
+}
+
+int fdtd_keep_previous_level (fdtd_ctx *ctx, int on)
+{
+  if (!ctx)
+    return fail (ctx, FDTD_ERR_ARG, "bad argument");
+  if (ctx->kind == 0)
+    return FDTD_OK;   // the FP64 plain form keeps its time levels anyway
+  int r = set_device (ctx);
+  if (r != FDTD_OK)
+    return r;
+  if (on && !ctx->hprev[0])
+    for (int ci = 0; ci < 3; ++ci)
+      if ((r = dalloc (ctx, &ctx->hprev[ci], (size_t) ctx->g.cells * elem_size (ctx->kind))) != FDTD_OK)
+        return r;
+  ctx->keep_prev = on != 0;
+  ctx->prev_src = 0;
   return FDTD_OK;
 }
 

@@ -36,6 +36,16 @@ struct FastHalf
   const double *cs_val;       // this half step's current I (device)
   float cs_scale;             // I dx -> curl units (eta0 for E, 1 for H)
   const float *matc[3];       // double material precision: per-component averaged material (null: mat)
+  // Drude media (metamaterials, with PML): the family's plasma frequency and
+  // collision rate per cell (FP32, rad/s), and per component the last
+  // increment of X, Z = D1 or eta0 B1 and the last increment of Z, updated
+  // in place (the one-sweep kernels keep the previous levels instead: a 3-D
+  // Drude run whose mu map is uploaded after it has stepped changes form
+  // with Drude state of the other meaning; upload mu before stepping)
+  int meta;
+  float dt;
+  const float *om, *ga;
+  float *xpp[3], *zd[3], *zpp[3];
 };
 
 int launch_plain_half (const PlainHalf &p, int inc_len, int *err, int sm_count, cudaStream_t s);

@@ -9,6 +9,8 @@
 // exp(i k r.u) about the grid centre n / 2, and the face signs.  Complex
 // arithmetic is the reference's CComplex: products with a real scale
 // component-wise, products of two complex values in full.
+#include <cuda_fp16.h>
+
 #include "ntff.h"
 
 namespace fdtdb {
@@ -55,13 +57,23 @@ __device__ __forceinline__ int64_t cell (const NtffParams &p, const double q[3])
   return ((int64_t) i[0] * p.n[1] + i[1]) * p.n[2] + i[2];
 }
 
+// A stored field value in physical units (FP64 as stored; FP32 / FP16
+// storage converted and scaled: H is kept as eta0 H there)
+__device__ __forceinline__ double fval (const NtffParams &p, const void *a, int c, int64_t id)
+{
+  if (p.kind == 0)
+    return static_cast<const double *> (a)[id];
+  if (p.kind == 1)
+    return (double) static_cast<const float *> (a)[id] * p.scale[c];
+  return (double) __half2float (static_cast<const __half *> (a)[id]) * p.scale[c];
+}
 __device__ __forceinline__ Cx cur (const NtffParams &p, int c, int64_t id)
 {
-  return {p.cur[0][c][id], p.cur[1][c][id]};
+  return {fval (p, p.cur[0][c], c, id), fval (p, p.cur[1][c], c, id)};
 }
 __device__ __forceinline__ Cx prev (const NtffParams &p, int c, int64_t id)
 {
-  return {p.prev[0][c][id], p.prev[1][c][id]};
+  return {fval (p, p.prev[0][c], c, id), fval (p, p.prev[1][c], c, id)};
 }
 
 // Component c at position x: one cell, or the two cells at -/+ 1/2 along

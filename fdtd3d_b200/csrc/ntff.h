@@ -24,9 +24,12 @@ struct NtffParams
   double min_fp[6][3];         // component positions
   // [0] real part (sine run), [1] imaginary part (cosine run): every
   // component's current level, and the previous level of H (the N sums
-  // average H over the two time levels)
-  const double *cur[2][6];
-  const double *prev[2][6];
+  // average H over the two time levels); stored as double (kind 0), float
+  // (1) or half (2), value = stored * scale[component]
+  const void *cur[2][6];
+  const void *prev[2][6];
+  int kind;
+  double scale[6];
   int64_t points;              // face points over the six faces
 };
 

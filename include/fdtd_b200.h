@@ -244,7 +244,10 @@ int fdtd_dft_read (fdtd_ctx *ctx, double *out);
  * 4037-4095, 4535-4645; Source/Scheme/SchemeHelper.h:1036-2121).  `re` and
  * `im` are the two runs of one configuration with source_phase 0 and 1 (their
  * fields are the real and imaginary parts of the complex build's), both in
- * the FP64 plain form, stepped to the same time.  The box has its faces at
+ * the same form, stepped to the same time; FP32 / FP16-storage runs need
+ * fdtd_keep_previous_level before they step (the N sums average H over the
+ * current and the previous level; the sums run in FP64 on the stored values
+ * either way).  The box has its faces at
  * left[a] and right[a] on axis a (the reference's leftNTFF / rightNTFF:
  * right = size - left + 1, both moved in by the --ntff-diff step), with
  * 1 <= left[a] < right[a] <= size[a] - 1.  For each azimuth phi[i]
@@ -253,8 +256,18 @@ int fdtd_dft_read (fdtd_ctx *ctx, double *out);
 int fdtd_ntff (fdtd_ctx *re, fdtd_ctx *im, const int left[3], const int right[3], double teta, int nphi,
                const double *phi, double *out);
 
+/* FP32 / FP16 storage: keep the previous level of H at the end of every
+ * fdtd_step call (on = 1), as the FP64 plain form's time levels do
+ * (Grid::shiftInTime; the reference's NTFF reads the previous H level,
+ * Source/Scheme/SchemeHelper.h:1036-2095).  The one-sweep 3-D path then ends
+ * each call on a single step (its other buffer set holds the previous
+ * level); the per-cell path copies H before the last H update of the call.
+ * No effect on the FP64 plain form.  Without a reference counterpart. */
+int fdtd_keep_previous_level (fdtd_ctx *ctx, int on);
+
 /* Name of the kernel that performs this context's field update (no
- * reference counterpart): "plain_fp64" (FP64 plain form), "sweep3d_tma"
+ * reference counterpart): "plain_fp64" (FP64 plain form), "sweep2_tma"
+ * (two steps per pass: the last call ended on a pair), "sweep3d_tma"
  * (TMA-pipelined one-sweep 3-D kernel), "fused3d_regblock" (register-blocked
  * one-sweep 3-D kernel), "per_cell" (one launch per half-step), or
  * "not_stepped" before the first update.  Null for a null context. */

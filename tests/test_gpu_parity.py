@@ -177,9 +177,11 @@ def test_sync_with_timeout_returns(fdtd):
 
 
 def test_unsupported_combination_is_reported(fdtd):
-    # 2-D metamaterials exist only in the FP64 plain form
+    # double material precision with metamaterials: the reference's
+    # eight-point Drude average is unreachable (Approximation.cpp:167-197)
     with pytest.raises(fdtd.FdtdError):
-        fdtd.Simulation(mode=2, size=(20, 20), use_pml=True, pml=2, use_metamaterials=True, precision=1)
+        fdtd.Simulation(mode=3, size=(12, 12, 12), use_pml=True, pml=2, use_metamaterials=True,
+                        double_material_precision=True, precision=1)
 
 
 def test_cli_dropin_matches_reference_txt(fdtd, tmp_path):
