@@ -386,8 +386,12 @@ __global__ void __launch_bounds__ (32 * NW, 1)
     };
     PlaneState sa = {}, sb = {};
 
-    auto plane = [&] (int i, auto par_c, PlaneState &cur, PlaneState &prev) __attribute__ ((always_inline)) -> bool {
+    // STEADY: a plane from the fifth on, where every phase runs (the first
+    // four fill the lag)
+    auto plane = [&] (int i, auto par_c, auto steady_c, PlaneState &cur, PlaneState &prev)
+                     __attribute__ ((always_inline)) -> bool {
       constexpr int P = decltype (par_c)::value;
+      constexpr bool STEADY = decltype (steady_c)::value;
       const int st = i % NST2;
       const int x = xa - 2 + i;
       if (!tma::mbar_wait (bar + 8 * st, (phase >> st) & 1u))
@@ -417,7 +421,7 @@ __global__ void __launch_bounds__ (32 * NW, 1)
         V2<T>::ld (sH + c * HS + (w + 1) * HW + HZ + zl, cur.h0[c]);
 
       // ================= phase 1: E1(x) on every row, H1(x - 1) on rows 0 .. 14
-      if (i >= 1)
+      if (STEADY || i >= 1)
       {
         const unsigned u = (x >= 1 && x <= nx - 2) ? cupd : 0u;
         float hzm[2], hxm[2], eo[3][2];
@@ -489,7 +493,7 @@ __global__ void __launch_bounds__ (32 * NW, 1)
         sts2 (XE1w + 0 * XN + w * ZW + zl, cur.e1[0]);
         sts2 (XE1w + 1 * XN + w * ZW + zl, cur.e1[2]);
       }
-      if (i >= 2 && w < NW - 1)
+      if ((STEADY || i >= 2) && w < NW - 1)
       {
         // H1(x - 1): E1(x - 1) in prev.e1, its y + 1 row from the previous
         // plane's exchange rows, its z + 1 cell from the next lane
@@ -558,7 +562,7 @@ __global__ void __launch_bounds__ (32 * NW, 1)
         issue (st, x + NST2, zs, Y);
 
       // ================= phase 2: E2(x - 1) on rows 1 .. 14, H2(x - 2) on rows 1 .. 13
-      if (i >= 3 && w >= 1 && w < NW - 1)
+      if ((STEADY || i >= 3) && w >= 1 && w < NW - 1)
       {
         const int xe = x - 1;
         const unsigned u = (xe >= 1 && xe <= nx - 2) ? cupd : 0u;
@@ -616,7 +620,7 @@ __global__ void __launch_bounds__ (32 * NW, 1)
         sts2 (XE2w + 0 * XN + w * ZW + zl, cur.e2[0]);
         sts2 (XE2w + 1 * XN + w * ZW + zl, cur.e2[2]);
       }
-      if (i >= 4 && w >= 1 && w <= kTb2Yown)
+      if ((STEADY || i >= 4) && w >= 1 && w <= kTb2Yown)
       {
         const int xh = x - 2;
         const unsigned u = (xh >= 1 && xh <= nx - 2) ? cupd : 0u;
@@ -679,14 +683,30 @@ __global__ void __launch_bounds__ (32 * NW, 1)
 
     using P0 = std::integral_constant<int, 0>;
     using P1 = std::integral_constant<int, 1>;
-    for (int i = 0; i < np; i += 2)
+    using FILL = std::integral_constant<bool, false>;
+    using RUN = std::integral_constant<bool, true>;
+    int i = 0;
+    for (; i < np && i < 4; i += 2)
     {
-      if (!plane (i, P0{}, sa, sb))
+      if (!plane (i, P0{}, FILL{}, sa, sb))
       {
         aborted = true;
         break;
       }
-      if (i + 1 < np && !plane (i + 1, P1{}, sb, sa))
+      if (i + 1 < np && !plane (i + 1, P1{}, FILL{}, sb, sa))
+      {
+        aborted = true;
+        break;
+      }
+    }
+    for (; !aborted && i < np; i += 2)
+    {
+      if (!plane (i, P0{}, RUN{}, sa, sb))
+      {
+        aborted = true;
+        break;
+      }
+      if (i + 1 < np && !plane (i + 1, P1{}, RUN{}, sb, sa))
       {
         aborted = true;
         break;
