@@ -87,6 +87,7 @@ struct fdtd_ctx
   double *d1[6][3] = {};
   double *mat64[6] = {};
   double *sig64[3] = {};
+  double *ptab[6][6] = {};   // FP64 plain form: PML coefficient tables per component (PlainTabs)
   // double material precision: eps / mu per component averaged from the fine
   // grid at upload (null until then), sigma per component and axis, and the
   // fine upload buffer
@@ -391,6 +392,8 @@ int ensure_src (fdtd_ctx *ctx, size_t steps)
   return FDTD_OK;
 }
 
+PlainHalf plain_half (fdtd_ctx *ctx, int h);
+
 int alloc_plain (fdtd_ctx *ctx)
 {
   const Geometry &g = ctx->g;
@@ -436,6 +439,26 @@ int alloc_plain (fdtd_ctx *ctx)
         CK (cudaStreamSynchronize (ctx->stream));
       }
     }
+  }
+  // PML coefficient tables of the per-component kernels (computed on the
+  // device by the per-cell expressions)
+  if (g.cfg.use_pml)
+  {
+    const int nmax = std::max (g.n[0], std::max (g.n[1], g.n[2]));
+    for (int k = 0; k < 6; ++k)
+      if (g.comp[k].exists)
+        for (int j = 0; j < 6; ++j)
+          DALLOC (ctx->ptab[k][j], (size_t) nmax * sizeof (double));
+    for (int h = 0; h < 2; ++h)
+    {
+      const PlainHalf p = plain_half (ctx, h);
+      double *out[3][6];
+      for (int ci = 0; ci < 3; ++ci)
+        for (int j = 0; j < 6; ++j)
+          out[ci][j] = ctx->ptab[ci + 3 * h][j];
+      ctx->launches += launch_plain_tables (p, out, ctx->stream);
+    }
+    CK (cudaGetLastError ());
   }
   CK (cudaStreamSynchronize (ctx->stream));
   return FDTD_OK;
@@ -1566,7 +1589,17 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
           cudaEvent_t pe;
           if ((r = prof_begin (ctx, &pe)) != FDTD_OK)
             return r;
-          ctx->launches += launch_plain_half (p, g.inc_len, ctx->d_err, ctx->sm_count, s);
+          if (p.cs_mask == 0 && (!g.cfg.use_pml || ctx->ptab[3 * h][0] || ctx->ptab[3 * h + 1][0] ||
+                                 ctx->ptab[3 * h + 2][0]))
+          {
+            PlainTabs tb;
+            for (int ci = 0; ci < 3; ++ci)
+              for (int j = 0; j < 6; ++j)
+                tb.t[ci][j] = ctx->ptab[ci + 3 * h][j];
+            ctx->launches += launch_plain_fast (p, tb, g.inc_len, ctx->d_err, ctx->sm_count, s);
+          }
+          else
+            ctx->launches += launch_plain_half (p, g.inc_len, ctx->d_err, ctx->sm_count, s);
           ctx->step_kernel = "plain_fp64";
           if ((r = prof_end (ctx, pe)) != FDTD_OK)
             return r;

@@ -49,6 +49,24 @@ struct FastHalf
 };
 
 int launch_plain_half (const PlainHalf &p, int inc_len, int *err, int sm_count, cudaStream_t s);
+
+// FP64 plain form, PML coefficients per component as 1-D tables along the
+// axis each one varies on: [0] ca, [1] cb (curl step, axis sig_cacb),
+// [2] ca2, [3] the E-from-D denominator (axis sig5), [4], [5] the E-from-D
+// numerators 2 eps0 +/- sigma dt (axis sig4).  Computed on the device by
+// the per-cell code's own expressions (bit-identical values); entries whose
+// averaging stencil leaves the axis stay 0 (no cell reads them).
+struct PlainTabs
+{
+  const double *t[3][6];
+};
+int launch_plain_tables (const PlainHalf &p, double *const out[3][6], cudaStream_t s);
+// One half-step of the FP64 plain form without a current source: one launch
+// per component, the component's parameters resolved once per thread and
+// the PML coefficients read from the tables; the same arithmetic per cell
+// as plain_half_kernel.  Returns the launches.
+int launch_plain_fast (const PlainHalf &p, const PlainTabs &t, int inc_len, int *err, int sm_count,
+                       cudaStream_t s);
 int launch_incident_e (double *e_new, const double *e_old, const double *h_old, int len, double modifier,
                        const double *src, int src_index, cudaStream_t s);
 int launch_incident_h (double *h_new, const double *h_old, const double *e_new, int len, double modifier,

@@ -69,6 +69,239 @@ __global__ void point_source_kernel (double *f, size_t index, const double *src,
     f[index] = src[src_index];
 }
 
+// The PML coefficient tables (PlainTabs): block y = component, block z =
+// table pair; the expressions are plain_component's, so every value is the
+// one the per-cell code computes at that coordinate.
+struct PlainTabOut
+{
+  double *t[3][6];
+};
+
+__global__ void plain_tables_kernel (PlainHalf p, PlainTabOut o)
+{
+  const int ci = blockIdx.y, role = blockIdx.z;
+  const CompDev &c = p.comp[ci];
+  if (!c.exists)
+    return;
+  const double *const *sig = p.dmp ? p.sigc[ci] : p.sigma;
+  const int axis = role == 0 ? c.sig_cacb : (role == 1 ? c.sig5 : c.sig4);
+  const int n = p.g.n[axis];
+  const double eps0 = kEps0Dev;
+  const double dt = p.g.dt;
+  const double dx = p.g.dx;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+  {
+    bool inside = true;
+    for (int j = 0; j < c.nmat; ++j)
+      inside = inside && q + c.m[j][axis] >= 0 && q + c.m[j][axis] < n;
+    if (!inside)
+      continue;
+    const double material = sigma_avg (c, sig[axis], axis, q, q, q);
+    if (role == 0)
+    {
+      double dd = (2 * eps0 * 1.0 + material * dt);
+      o.t[ci][0][q] = (2 * eps0 * 1.0 - material * dt) / dd;
+      o.t[ci][1][q] = (2 * eps0 * dt / dx) / dd;
+    }
+    else if (role == 1)
+    {
+      double dd5 = (2 * eps0 * 1.0 + material * dt);
+      o.t[ci][2][q] = (2 * eps0 * 1.0 - material * dt) / dd5;
+      o.t[ci][3][q] = dd5;
+    }
+    else
+    {
+      o.t[ci][4][q] = (2 * eps0 * 1.0 + material * dt);
+      o.t[ci][5][q] = (2 * eps0 * 1.0 - material * dt);
+    }
+  }
+}
+
+// One component of one half-step over every interior cell (the arithmetic
+// of plain_component, parameters resolved before the cell loop).
+template <bool PML, bool META, bool TFSF>
+__global__ void __launch_bounds__ (256) plain_fast_kernel (const __grid_constant__ PlainHalf p,
+                                                           const __grid_constant__ PlainTabs tb, int ci,
+                                                           int inc_len, int *err)
+{
+  const GeomDev &g = p.g;
+  const CompDev &c = p.comp[ci];
+  const int64_t sx = (int64_t) g.n[1] * g.n[2], sy = g.n[2];
+  const int64_t d11 = c.d11[0] * sx + c.d11[1] * sy + c.d11[2];
+  const int64_t d12 = c.d12[0] * sx + c.d12[1] * sy + c.d12[2];
+  const int64_t d21 = c.d21[0] * sx + c.d21[1] * sy + c.d21[2];
+  const int64_t d22 = c.d22[0] * sx + c.d22[1] * sy + c.d22[2];
+  const int nmat = c.nmat;
+  int64_t mo[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    mo[j] = c.m[j][0] * sx + c.m[j][1] * sy + c.m[j][2];
+  const double *o1 = p.opp[c.opp1];
+  const double *o2 = p.opp[c.opp2];
+  const double *mat = p.dmp ? p.matc[ci] : p.mat;
+  double *g0 = PML ? p.dd[ci][0] : p.f[ci][0];
+  const double *g1 = PML ? p.dd[ci][1] : p.f[ci][1];
+  const int ax_c = c.sig_cacb, ax5 = c.sig5, ax4 = c.sig4;
+  const double *t_ca = tb.t[ci][0], *t_cb = tb.t[ci][1], *t_ca2 = tb.t[ci][2], *t_dd5 = tb.t[ci][3];
+  const double *t_n4p = tb.t[ci][4], *t_n4m = tb.t[ci][5];
+  const double dt = g.dt, dx = g.dx, mm = p.mat_modifier;
+  double *f0 = p.f[ci][0];
+  const double *f1 = p.f[ci][1];
+  auto avg = [&] (const double *m, int64_t id) -> double {
+    const double v0 = m[id + mo[0]];
+    const double v1 = nmat > 1 ? m[id + mo[1]] : 0.0;
+    const double v2 = nmat > 2 ? m[id + mo[2]] : 0.0;
+    const double v3 = nmat > 3 ? m[id + mo[3]] : 0.0;
+    return avg_points (nmat, v0, v1, v2, v3);
+  };
+
+  const int ix = (g.drop & 1) ? 1 : g.n[0] - 2;
+  const int iy = (g.drop & 2) ? 1 : g.n[1] - 2;
+  const int iz = (g.drop & 4) ? 1 : g.n[2] - 2;
+  const int64_t total = (int64_t) ix * iy * iz;
+  for (int64_t tid = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; tid < total;
+       tid += (int64_t) gridDim.x * blockDim.x)
+  {
+    const int z = (int) (tid % iz) + ((g.drop & 4) ? 0 : 1);
+    const int64_t r = tid / iz;
+    const int y = (int) (r % iy) + ((g.drop & 2) ? 0 : 1);
+    const int x = (int) (r / iy) + ((g.drop & 1) ? 0 : 1);
+    const int64_t id = x * sx + y * sy + z;
+    const int pos[3] = {x, y, z};
+    double val = g1[id];
+    double ca, cb;
+    if (PML)
+    {
+      const int q = ax_c == 0 ? x : (ax_c == 1 ? y : z);
+      ca = t_ca[q];
+      cb = t_cb[q];
+    }
+    else
+    {
+      double material = avg (mat, id);
+      ca = 1.0;
+      cb = dt / (material * mm * dx);
+    }
+    double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+    if (o1)
+    {
+      v0 = o1[id + d11];
+      v1 = o1[id + d12];
+    }
+    if (o2)
+    {
+      v2 = o2[id + d21];
+      v3 = o2[id + d22];
+    }
+    if (TFSF)
+    {
+      for (int t = 0; t < c.nterms; ++t)
+      {
+        const TermDev &tm = c.term[t];
+        if (x >= tm.lo[0] && x < tm.hi[0] && y >= tm.lo[1] && y < tm.hi[1] && z >= tm.lo[2] && z < tm.hi[2])
+        {
+          double diff = incident_value (g, p.inc, inc_len, err, tm.inc_comp, x + tm.aux[0], y + tm.aux[1],
+                                        z + tm.aux[2]);
+          if (tm.negate < 0)
+            diff *= -1.0;
+          if (tm.slot == 0)
+            v0 -= diff;
+          else if (tm.slot == 1)
+            v1 -= diff;
+          else if (tm.slot == 2)
+            v2 -= diff;
+          else
+            v3 -= diff;
+        }
+      }
+    }
+    double tmp = v1 - v0 - v3 + v2 - 0.0 * dx;
+    double nv = val * ca + tmp * cb;
+    g0[id] = nv;
+    if (!PML)
+      continue;
+    if (META)
+    {
+      double cur = p.dd[ci][0][id], prev = p.dd[ci][1][id], pprev = p.dd[ci][2][id];
+      double prev1 = p.d1[ci][1][id], pprev1 = p.d1[ci][2][id];
+      double material = avg (mat, id);
+      const double *om = p.omega, *ga = p.gamma;
+      double omega, gamma;
+      if (nmat == 2)
+      {
+        omega = (om[id + mo[0]] + om[id + mo[1]]) / 2.0;
+        gamma = (ga[id + mo[0]] + ga[id + mo[1]]) / 2.0;
+      }
+      else
+      {
+        omega = (om[id + mo[0]] + om[id + mo[1]] + om[id + mo[2]] + om[id + mo[3]]) / 4.0;
+        gamma = (ga[id + mo[0]] + ga[id + mo[1]] + ga[id + mo[2]] + ga[id + mo[3]]) / 4.0;
+      }
+      double sq = dt * omega;
+      double A = 4 * mm * material + 2 * dt * mm * material * gamma + mm * (sq * sq);
+      double b0 = (4 + 2 * dt * gamma) / A;
+      double b1 = -8 / A;
+      double b2 = (4 - 2 * dt * gamma) / A;
+      double a1 = (2 * mm * (sq * sq) - 8 * mm * material) / A;
+      double a2 = (4 * mm * material - 2 * dt * mm * material * gamma + mm * (sq * sq)) / A;
+      p.d1[ci][0][id] = cur * b0 + prev * b1 + pprev * b2 - prev1 * a1 - pprev1 * a2;
+    }
+    double prev_eh = f1[id];
+    double *const *src = META ? p.d1[ci] : p.dd[ci];
+    double cur_db = src[0][id];
+    double prev_db = src[1][id];
+    double material1 = avg (mat, id);
+    double modifier = material1 * mm;
+    if (META)
+      modifier = 1;
+    const int q5 = pos[ax5], q4 = pos[ax4];
+    double dd5 = t_dd5[q5];
+    double ca2 = t_ca2[q5];
+    double cb2 = (t_n4p[q4] / (modifier)) / dd5;
+    double cc2 = (t_n4m[q4] / (modifier)) / dd5;
+    f0[id] = prev_eh * ca2 + cur_db * cb2 - prev_db * cc2;
+  }
+}
+
+int launch_plain_tables (const PlainHalf &p, double *const out[3][6], cudaStream_t s)
+{
+  PlainTabOut o;
+  for (int ci = 0; ci < 3; ++ci)
+    for (int j = 0; j < 6; ++j)
+      o.t[ci][j] = out[ci][j];
+  plain_tables_kernel<<<dim3 (4, 3, 3), 256, 0, s>>> (p, o);
+  return 1;
+}
+
+int launch_plain_fast (const PlainHalf &p, const PlainTabs &t, int inc_len, int *err, int sm_count,
+                       cudaStream_t s)
+{
+  const int ix = (p.g.drop & 1) ? 1 : p.g.n[0] - 2;
+  const int iy = (p.g.drop & 2) ? 1 : p.g.n[1] - 2;
+  const int iz = (p.g.drop & 4) ? 1 : p.g.n[2] - 2;
+  int64_t total = (int64_t) ix * iy * iz;
+  int64_t blocks = (total + 255) / 256;
+  int64_t cap = (int64_t) sm_count * 8 * 16;
+  if (blocks > cap)
+    blocks = cap;
+  if (blocks < 1)
+    blocks = 1;
+  int n = 0;
+  for (int ci = 0; ci < 3; ++ci)
+  {
+    if (!p.comp[ci].exists)
+      continue;
+    auto kern = p.use_pml ? (p.use_meta ? (p.use_tfsf ? plain_fast_kernel<true, true, true>
+                                                      : plain_fast_kernel<true, true, false>)
+                                        : (p.use_tfsf ? plain_fast_kernel<true, false, true>
+                                                      : plain_fast_kernel<true, false, false>))
+                          : (p.use_tfsf ? plain_fast_kernel<false, false, true> : plain_fast_kernel<false, false, false>);
+    kern<<<(unsigned) blocks, 256, 0, s>>> (p, t, ci, inc_len, err);
+    ++n;
+  }
+  return n;
+}
+
 int launch_plain_half (const PlainHalf &p, int inc_len, int *err, int sm_count, cudaStream_t s)
 {
   const int ix = (p.g.drop & 1) ? 1 : p.g.n[0] - 2;
