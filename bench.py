@@ -587,6 +587,15 @@ def main() -> None:
                             "hbm_frac": cells * bc * spl / (kms / max(kl, 1) * 1e-3) / 1e9 / peaks["hbm_gbs"]}
         if "plain_fp64" in extras:
             extras["speedup_vs_plain_fp64"] = value / world / extras["plain_fp64"]["value"]
+            # the plain form moves D / B for every cell (the reference's
+            # formulation): its own DRAM traffic per step, from an ncu capture
+            tf64 = os.path.join(ROOT, "profiles", "traffic_fp64.json")
+            entry = json.load(open(tf64)).get("plain_fp64") if os.path.exists(tf64) else None
+            if entry and entry.get("grid") == n:
+                pf = extras["plain_fp64"]
+                pf["own_bytes_per_step"] = entry["bytes_per_step"]
+                pf["own_traffic_frac"] = entry["bytes_per_step"] / (pf["ms_per_step"] * 1e-3) / 1e9 / peaks["hbm_gbs"]
+                pf["own_traffic_source"] = entry["source"]
         # the reference's own CUDA FP64 path, measured on this GPU type by its
         # GPU test (tests/test_gpu_reference_cuda.py; not run by the bench)
         ref_cuda = os.path.join(ROOT, "profiles", "reference_cuda_fp64.json")
