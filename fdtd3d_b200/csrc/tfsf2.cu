@@ -124,7 +124,7 @@ struct Walk
 //   4. dH2 = dH1 + S curlH dE2 + S dH(t2) over O; the fields of O take
 //      E += dE2 and H += dH2 where nonzero.
 template <typename T>
-__global__ void __launch_bounds__ (256, 3) tfsf2_fused (const __grid_constant__ FusedParams p, const Tf2Tile *tiles,
+__global__ void __launch_bounds__ (256, 4) tfsf2_fused (const __grid_constant__ FusedParams p, const Tf2Tile *tiles,
                                                         const double *inc_h1, const double *inc_e1,
                                                         const double *inc_h2, const double *inc_e2, int *err)
 {
@@ -422,8 +422,10 @@ std::string tfsf2_regions (const FusedParams &p, std::vector<Tf2Box> r[4])
   return "";
 }
 
-// shared memory of a tile at most: three CTAs per SM
-constexpr unsigned kTileSmem = 74u * 1024u;
+// shared memory of a tile at most: four CTAs per SM (measured at 512^3:
+// the step 1.1 % faster than with three CTAs of larger tiles, 2 % faster
+// than with two; five or six CTAs spill registers and are slower)
+constexpr unsigned kTileSmem = 54u * 1024u;
 
 std::string tfsf2_tiles (const FusedParams &p, const std::vector<Tf2Box> r[4], std::vector<Tf2Tile> &tiles,
                          unsigned &smem)
@@ -461,7 +463,7 @@ std::string tfsf2_tiles (const FusedParams &p, const std::vector<Tf2Box> r[4], s
       ext[a] = b.hi[a] - b.lo[a];
     // tile extents: up to 8 x 8 x 32 cells, or 16 x 16 across a box that is
     // thin in z (a z face of the TF/SF box), shrunk until a tile's shared
-    // memory fits three CTAs per SM; boxes split evenly
+    // memory fits four CTAs per SM; boxes split evenly
     const bool zthin = ext[2] <= 8;
     int cap[3] = {zthin ? 16 : 8, zthin ? 16 : 8, 32};
     for (;;)
