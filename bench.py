@@ -430,7 +430,7 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--grid", type=int, default=N_DEFAULT)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16s", "fp64"])
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--e2e-chunk", type=int, default=50)
     ap.add_argument("--plain-steps", type=int, default=10)
     ap.add_argument("--ref-grid", type=int, default=96)
