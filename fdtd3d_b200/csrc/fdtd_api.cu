@@ -1432,9 +1432,26 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
   size_t ps_idx = 0;
   bool ps_ok = g.cfg.point_source_mask && point_source_index (g, &ps_idx);
   cudaStream_t s = ctx->stream;
-  // current sources run the per-cell kernels
-  const bool fused = ctx->kind != 0 && ctx->has_second && !ctx->mat32[1] && ctx->ps_interior && !ctx->cs_mask[0]
-                     && !ctx->cs_mask[1];
+  // a current source runs with the one-sweep kernels as a fix-up after each
+  // step (launch_current_fix) when its cell and the cells around it update
+  // outside the PML, else with the per-cell kernels
+  const bool has_cs = ctx->cs_mask[0] || ctx->cs_mask[1];
+  bool cs_fix = has_cs && !g.cfg.use_metamaterials;
+  if (cs_fix && g.cfg.use_pml)
+    for (int k = 0; k < 6; ++k)
+      for (int a = 0; a < 3; ++a)
+        cs_fix = cs_fix && ctx->cs_pos[a] - 1 >= ctx->fused.ilo[k][a] && ctx->cs_pos[a] + 1 < ctx->fused.ihi[k][a];
+  const bool fused = ctx->kind != 0 && ctx->has_second && !ctx->mat32[1] && ctx->ps_interior && (!has_cs || cs_fix);
+  CurrentFix cfix{};
+  if (has_cs)
+  {
+    for (int a = 0; a < 3; ++a)
+      cfix.pos[a] = ctx->cs_pos[a];
+    cfix.mask_e = ctx->cs_mask[0];
+    cfix.mask_h = ctx->cs_mask[1];
+    cfix.scale_e = (float) kEta0;
+    cfix.scale_h = 1.f;
+  }
 
   for (uint32_t i = 0; i < n; ++i)
   {
@@ -1481,7 +1498,7 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
         if ((r = plan_sweep (ctx)) != FDTD_OK)
           return r;
       cudaEvent_t pe;
-      if (ctx->tb2_state >= 1 && i + (ctx->keep_prev ? 2 : 1) < n && ctx->dft_comp < 0)
+      if (ctx->tb2_state >= 1 && i + (ctx->keep_prev ? 2 : 1) < n && ctx->dft_comp < 0 && !has_cs)
       {
         // steps t and t + 1 in one pass (no point source or Drude medium).
         // With TF/SF the incident grid takes both steps first (this step's
@@ -1555,6 +1572,8 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
         ctx->launches += launch_fused3d (f, ctx->d_err, s);
         ctx->step_kernel = "fused3d_regblock";
       }
+      if (has_cs)
+        ctx->launches += launch_current_fix (f, cfix, ctx->d_src + kSrcStride * i + 3, s);
       if ((r = prof_end (ctx, pe)) != FDTD_OK)
         return r;
       ctx->fcur = nw;

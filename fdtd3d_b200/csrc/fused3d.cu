@@ -733,6 +733,65 @@ int launch_drude_fixup (const FusedParams &p, const DrudeBox &box, cudaStream_t 
   return 2;
 }
 
+__global__ void current_fix_kernel (FusedParams p, CurrentFix cf, const double *src)
+{
+  if (threadIdx.x != 0 || blockIdx.x != 0)
+    return;
+  const int ny = p.g.n[1], nz = p.g.n[2];
+  const size_t st[3] = {(size_t) ny * nz, (size_t) nz, 1};
+  const size_t c = (size_t) cf.pos[0] * st[0] + (size_t) cf.pos[1] * st[1] + cf.pos[2];
+  const float S = p.courant;
+  auto rmw = [&] (void *f, size_t id, float d) {
+    if (p.fp16)
+    {
+      __half *h = static_cast<__half *> (f);
+      h[id] = __float2half_rn (__half2float (h[id]) + d);
+    }
+    else
+      static_cast<float *> (f)[id] += d;
+  };
+  // H at cell q: the update adds S times its curl; a change dE of E
+  // component k at c changes the curls of the two other H components
+  // (E_CENTERED: Hx = (Ey(z+1) - Ey) - (Ez(y+1) - Ez), and its rotations)
+  auto h_at = [&] (int m, int dax, float d) {
+    // H component m at c - e_dax (dax = -1: at c itself) takes S d
+    int q[3] = {cf.pos[0], cf.pos[1], cf.pos[2]};
+    if (dax >= 0)
+      q[dax] -= 1;
+    for (int a = 0; a < 3; ++a)
+      if (!((p.g.drop >> a) & 1) && (q[a] < 1 || q[a] > p.g.n[a] - 2))
+        return;   // a face cell: the step does not update it
+    rmw (p.h_new[m], (size_t) q[0] * st[0] + (size_t) q[1] * st[1] + q[2], S * d);
+  };
+  const float ie = (float) (src[0] * p.g.dx) * cf.scale_e;
+  for (int k = 0; k < 3; ++k)
+  {
+    if (!((cf.mask_e >> k) & 1))
+      continue;
+    const float im = p.eps ? __fdividef (2.f, p.eps[c] + p.eps[c + st[k]]) : 1.f;
+    const float de = S * im * -ie;
+    rmw (p.e_new[k], c, de);
+    // the two H components whose curl holds E_k: m = k + 1 and k + 2 (mod 3)
+    const int m1 = (k + 1) % 3, m2 = (k + 2) % 3;
+    // H_m1 reads E_k along axis m2 with sign -, H_m2 reads it along m1 with sign +
+    // (Hx: +dz Ey - dy Ez; Hy: +dx Ez - dz Ex; Hz: +dy Ex - dx Ey)
+    h_at (m1, -1, de);
+    h_at (m1, m2, -de);
+    h_at (m2, -1, -de);
+    h_at (m2, m1, de);
+  }
+  const float ih = (float) (src[1] * p.g.dx) * cf.scale_h;
+  for (int m = 0; m < 3; ++m)
+    if ((cf.mask_h >> m) & 1)
+      rmw (p.h_new[m], c, S * -ih);
+}
+
+int launch_current_fix (const FusedParams &p, const CurrentFix &cf, const double *src, cudaStream_t s)
+{
+  current_fix_kernel<<<1, 32, 0, s>>> (p, cf, src);
+  return 1;
+}
+
 int launch_drude_flags (unsigned char *flags, const float *ome, const float *gae, const float *omm, const float *gam,
                         int nx, int ny, int nz, cudaStream_t s)
 {

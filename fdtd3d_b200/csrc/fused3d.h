@@ -72,6 +72,24 @@ int launch_drude_box (const unsigned char *flags, int nx, int ny, int nz, int *b
 // launches; returns how many).
 int launch_drude_fixup (const FusedParams &p, const DrudeBox &box, cudaStream_t s);
 
+// J / M current source of a one-sweep step (Scheme.inc.h:1171-1260,
+// InternalScheme.inc.h:2423-2449): the sweep updates every cell without it;
+// the source enters the curl of its components at one cell (curl -= I dx,
+// in the scaled units), so the step's fields take the linear response: the
+// E components at the cell, then the H components whose curl reads them
+// (at the cell and one cell below along the third axis), then the H
+// components at the cell.  Used when the cell and those neighbours are
+// outside the PML for every component involved (interior update F += S
+// im curl).  `src` is this step's row of the source table (E current at
+// [0], H current at [1]).
+struct CurrentFix
+{
+  int pos[3];
+  int mask_e, mask_h;          // bit c: a current on component c of the family
+  float scale_e, scale_h;      // I dx -> curl units (eta0 for E, 1 for H)
+};
+int launch_current_fix (const FusedParams &p, const CurrentFix &cf, const double *src, cudaStream_t s);
+
 // Recomputes the per-cell Drude bitmask from the four material arrays.
 int launch_drude_flags (unsigned char *flags, const float *ome, const float *gae, const float *omm, const float *gam,
                         int nx, int ny, int nz, cudaStream_t s);

@@ -100,17 +100,27 @@ def test_cli_complex_current_source_matches_reference_complex_build(fdtd, tmp_pa
     _compare(ref, mine)
 
 
-@pytest.mark.parametrize("layout", [0, 1])
-def test_fp32_current_source_matches_fp64(fdtd, layout):
-    kw = dict(mode=3, size=(24, 22, 26), use_pml=True, pml=4, current_source=(11, 10, 13),
-              current_source_mask=(1 << 2) | (1 << 4), layout=layout)
+@pytest.mark.parametrize("layout,mask,pos,nz,want", [
+    (0, (1 << 2) | (1 << 4), (11, 10, 13), 28, "sweep3d_tma"),     # the TMA sweep + the current fix-up
+    (0, (1 << 0) | (1 << 1) | (1 << 5), (12, 9, 14), 28, "sweep3d_tma"),
+    (0, (1 << 2) | (1 << 4), (11, 10, 13), 26, "fused3d_regblock"),   # the register-blocked sweep + fix-up
+    (0, (1 << 2) | (1 << 4), (4, 10, 13), 28, "per_cell"),         # next to the PML: the per-cell kernels
+    (1, (1 << 2) | (1 << 4), (11, 10, 13), 28, "per_cell")])       # H_CENTERED: the per-cell kernels
+def test_fp32_current_source_matches_fp64(fdtd, layout, mask, pos, nz, want):
+    """J / M currents in the FP32 forms against the FP64 plain form.  In 3-D
+    E_CENTERED with the cell and its neighbours outside the PML, the
+    one-sweep kernel runs every step and the current enters as the step's
+    linear response (launch_current_fix); otherwise the per-cell kernels,
+    which fold it into the curl."""
+    kw = dict(mode=3, size=(24, 22, nz), use_pml=True, pml=4, current_source=pos,
+              current_source_mask=mask, layout=layout)
     out = {}
     for prec in (fdtd.PREC_FP64_PLAIN, fdtd.PREC_FP32):
         with fdtd.Simulation(precision=prec, **kw) as sim:
             sim.step(40)
             out[prec] = {c: sim.field(c) for c in fdtd.COMPONENTS}
             if prec == fdtd.PREC_FP32:
-                assert sim.step_kernel == "per_cell", sim.step_kernel
+                assert sim.step_kernel == want, sim.step_kernel
     for fam in ("E", "H"):
         names = [c for c in fdtd.COMPONENTS if c[0] == fam]
         num = sum(np.sum((out[1][c] - out[0][c]) ** 2) for c in names)
