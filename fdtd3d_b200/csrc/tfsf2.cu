@@ -153,14 +153,33 @@ __global__ void __launch_bounds__ (256, 4) tfsf2_fused (const __grid_constant__ 
     for (int i = 4 * n4 + threadIdx.x; i < 3 * (nE + nH); i += blockDim.x)
       sE[i] = 0.f;
   }
-  // eps over its domain (indices clamped to the grid: only cells of the
-  // supports, two cells inside the faces, use it)
+  // eps where S im is taken: the E term cells (phase box 0) and the dE2
+  // curl cells (phase box 2), each with its +1 neighbours (indices clamped
+  // to the grid: only cells of the supports, two cells inside the faces,
+  // use it)
   if (has_eps)
-    for (Walk w (pY, pZ); w.q < nP; w.next ())
+  {
+    int b0[3], b1[3];
+    bool any = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
     {
-      const int x = min (o[0] + w.x, nx - 1), y = min (o[1] + w.y, ny - 1), z = min (o[2] + w.z, nz - 1);
-      sP[w.q] = p.eps[(size_t) x * sx + (size_t) y * sy + z];
+      const bool e0 = t.ph[0][a] >= t.ph[0][3 + a], e2 = t.ph[2][a] >= t.ph[2][3 + a];
+      any = any && !(e0 && e2);
+      b0[a] = e0 ? t.ph[2][a] : (e2 ? t.ph[0][a] : min (t.ph[0][a], t.ph[2][a]));
+      b1[a] = (e0 ? t.ph[2][3 + a] : (e2 ? t.ph[0][3 + a] : max (t.ph[0][3 + a], t.ph[2][3 + a]))) + 1;
     }
+    if (any)
+    {
+      const int bY = b1[1] - b0[1], bZ = b1[2] - b0[2], nb = (b1[0] - b0[0]) * bY * bZ;
+      for (Walk w (bY, bZ); w.q < nb; w.next ())
+      {
+        const int qx = b0[0] + w.x, qy = b0[1] + w.y, qz = b0[2] + w.z;
+        const int x = min (o[0] + qx, nx - 1), y = min (o[1] + qy, ny - 1), z = min (o[2] + qz, nz - 1);
+        sP[(qx * pY + qy) * pZ + qz] = p.eps[(size_t) x * sx + (size_t) y * sy + z];
+      }
+    }
+  }
   __syncthreads ();
   // S im of E component k at domain cell (qx, qy, qz)
   auto s_im = [&] (int k, int qx, int qy, int qz) -> float {
