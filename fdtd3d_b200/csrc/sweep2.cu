@@ -202,10 +202,9 @@ __device__ __forceinline__ void zedge_two (const float *Tz, int k, int zl, float
 // MODE 0 (lean): no cell of the item's extended region is a PML cell of any
 // component.  MODE 2 (z edge): PML cells only along z; every lane runs the
 // branch-free z-edge form (zedge_two), carries the first step's auxiliaries
-// in registers to the second, and loads the old auxiliaries of the four
-// components that keep one a plane ahead with plain loads (lanes with PML
-// cells only), issued at the start of the plane before so that a whole
-// plane hides their latency.  (Class 1, x or y PML cells, is left to the
+// in registers to the second, and takes the old auxiliaries of the four
+// components that keep one (Ey, Ez at x, Hy, Hz at x - 1) through the
+// plane's TMA stage.  (Class 1, x or y PML cells, is left to the
 // single-step kernels: the two-step plan refuses it.)
 template <typename T, int MODE>
 __global__ void __launch_bounds__ (32 * NW, 1)
