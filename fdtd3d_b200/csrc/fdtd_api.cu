@@ -96,7 +96,7 @@ struct fdtd_ctx
   double *sigc64[6][3] = {};
   double *fine_tmp = nullptr;
   AdjointCache adj_cache;      // the adjoint's device memory, kept between calls
-  SweepStreams sweep_streams;  // side streams of the sweep's item classes (FDTDB_SWEEP_CONCURRENT=0: none)
+  SweepStreams sweep_streams;  // side streams of the sweep's item classes
   // asynchronous host copies: a host-to-device and a device-to-host copy
   // stream, their FP64 staging grids, and the events that order them against
   // the context's stream (an event never recorded is complete)

@@ -61,10 +61,12 @@ struct PlainTabs
   const double *t[3][6];
 };
 int launch_plain_tables (const PlainHalf &p, double *const out[3][6], cudaStream_t s);
-// One half-step of the FP64 plain form without a current source: one launch
-// per component, the component's parameters resolved once per thread and
-// the PML coefficients read from the tables; the same arithmetic per cell
-// as plain_half_kernel.  Returns the launches.
+// One half-step of the FP64 plain form without a current source: one
+// launch, each block on one component (interleaved by block index, so that
+// the blocks reading the same opposite-family cells run together), the
+// component's parameters resolved once per thread and the PML coefficients
+// read from the tables; the same arithmetic per cell as plain_half_kernel.
+// Returns the launches.
 int launch_plain_fast (const PlainHalf &p, const PlainTabs &t, int inc_len, int *err, int sm_count,
                        cudaStream_t s);
 int launch_incident_e (double *e_new, const double *e_old, const double *h_old, int len, double modifier,

@@ -121,9 +121,20 @@ __global__ void plain_tables_kernel (PlainHalf p, PlainTabOut o)
 // of plain_component, parameters resolved before the cell loop).
 template <bool PML, bool META, bool TFSF>
 __global__ void __launch_bounds__ (256) plain_fast_kernel (const __grid_constant__ PlainHalf p,
-                                                           const __grid_constant__ PlainTabs tb, int ci,
+                                                           const __grid_constant__ PlainTabs tb, int ncomp,
                                                            int inc_len, int *err)
 {
+  // block b updates component b % ncomp (of the existing ones) on cell block
+  // b / ncomp: the blocks that read the same opposite-family cells run
+  // together, so the later ones find them in L2
+  int ci = 0;
+  for (int k = 0, left = (int) (blockIdx.x % ncomp); k < 3; ++k)
+    if (p.comp[k].exists && left-- == 0)
+    {
+      ci = k;
+      break;
+    }
+  const int64_t cblock = blockIdx.x / ncomp, cgrid = gridDim.x / ncomp;
   const GeomDev &g = p.g;
   const CompDev &c = p.comp[ci];
   const int64_t sx = (int64_t) g.n[1] * g.n[2], sy = g.n[2];
@@ -159,8 +170,7 @@ __global__ void __launch_bounds__ (256) plain_fast_kernel (const __grid_constant
   const int iy = (g.drop & 2) ? 1 : g.n[1] - 2;
   const int iz = (g.drop & 4) ? 1 : g.n[2] - 2;
   const int64_t total = (int64_t) ix * iy * iz;
-  for (int64_t tid = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; tid < total;
-       tid += (int64_t) gridDim.x * blockDim.x)
+  for (int64_t tid = cblock * blockDim.x + threadIdx.x; tid < total; tid += cgrid * blockDim.x)
   {
     const int z = (int) (tid % iz) + ((g.drop & 4) ? 0 : 1);
     const int64_t r = tid / iz;
@@ -286,20 +296,18 @@ int launch_plain_fast (const PlainHalf &p, const PlainTabs &t, int inc_len, int 
     blocks = cap;
   if (blocks < 1)
     blocks = 1;
-  int n = 0;
+  int ncomp = 0;
   for (int ci = 0; ci < 3; ++ci)
-  {
-    if (!p.comp[ci].exists)
-      continue;
-    auto kern = p.use_pml ? (p.use_meta ? (p.use_tfsf ? plain_fast_kernel<true, true, true>
-                                                      : plain_fast_kernel<true, true, false>)
-                                        : (p.use_tfsf ? plain_fast_kernel<true, false, true>
-                                                      : plain_fast_kernel<true, false, false>))
-                          : (p.use_tfsf ? plain_fast_kernel<false, false, true> : plain_fast_kernel<false, false, false>);
-    kern<<<(unsigned) blocks, 256, 0, s>>> (p, t, ci, inc_len, err);
-    ++n;
-  }
-  return n;
+    ncomp += p.comp[ci].exists ? 1 : 0;
+  if (ncomp == 0)
+    return 0;
+  auto kern = p.use_pml ? (p.use_meta ? (p.use_tfsf ? plain_fast_kernel<true, true, true>
+                                                    : plain_fast_kernel<true, true, false>)
+                                      : (p.use_tfsf ? plain_fast_kernel<true, false, true>
+                                                    : plain_fast_kernel<true, false, false>))
+                        : (p.use_tfsf ? plain_fast_kernel<false, false, true> : plain_fast_kernel<false, false, false>);
+  kern<<<(unsigned) (blocks * ncomp), 256, 0, s>>> (p, t, ncomp, inc_len, err);
+  return 1;
 }
 
 int launch_plain_half (const PlainHalf &p, int inc_len, int *err, int sm_count, cudaStream_t s)
