@@ -531,7 +531,10 @@ def main() -> None:
     if os.path.exists(traffic_file):
         entry = json.load(open(traffic_file)).get(sim_kernel)
         if entry and entry.get("grid") == n:
-            roofline["traffic"] = entry["bytes_per_launch"]
+            if "bytes_per_launch" in entry:
+                roofline["traffic"] = entry["bytes_per_launch"]
+            else:   # a per-step figure (the FP64 form times half-steps)
+                roofline["traffic"] = entry["bytes_per_step"] * steps_per_launch
             roofline["traffic_source"] = entry["source"]
 
     # e2e through the C ABI with pinned host buffers
