@@ -882,7 +882,7 @@ std::string sweep2_plan (Sweep2Plan &plan, const FusedParams &p, void *const e[2
   }
   for (int j = 0; j < w.nch; ++j)
     if (w.xcut[j + 1] - w.xcut[j] > kTb2MaxChunk)
-      return "grid too long in x for the staged PML coefficients";
+      return "grid too long in x for the chunk count";
   w.nitems = w.nzt * w.nyt * w.nch;
   w.ctr = ctr;
   plan.items[0] = plan.items[1] = plan.items[2] = 0;

@@ -20,7 +20,7 @@ namespace fdtdb {
 constexpr int kTb2Warps = 16;
 constexpr int kTb2Zw = 64;
 constexpr int kTb2Yown = 13;
-constexpr int kTb2MaxChunk = 64;   // x planes per item (the PML class stages an x table of chunk + 4)
+constexpr int kTb2MaxChunk = 64;   // x planes per item at most
 
 struct Sweep2Maps
 {
