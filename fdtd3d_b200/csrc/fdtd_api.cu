@@ -770,6 +770,15 @@ int sweep_chunk (const FusedParams &p, int wy, int ctas, int overlap)
   return best;
 }
 
+// x chunk of the two-step sweep; FDTDB_TB2_CHUNK overrides it (a test hook:
+// short chunks put chunk seams into small grids)
+int tb2_chunk ()
+{
+  if (const char *v = std::getenv ("FDTDB_TB2_CHUNK"))
+    return std::max (1, std::atoi (v));
+  return kTb2Chunk;
+}
+
 // Plans the PML shell of the two-step scheme and the two-step core.  The core
 // owns the planes cx0 .. cx1 - 1 and rows cy0 .. cy1 - 1 (all z) that are at
 // least two cells from every x / y PML cell (so the two-step kernel never
@@ -889,7 +898,7 @@ std::string plan_shell (fdtd_ctx *ctx, void *const e[2][3], void *const h[2][3],
                            ctx->shell_ctr[1], ctx->stream);
   if (!why.empty ())
     return "shell step 2: " + why;
-  why = sweep2_plan (ctx->tb2, f, e, h, aux, ctx->mat32[0], ctx->sm_count, 64, ctx->tb2_ctr, cx0, cx1, cy0, cy1);
+  why = sweep2_plan (ctx->tb2, f, e, h, aux, ctx->mat32[0], ctx->sm_count, tb2_chunk (), ctx->tb2_ctr, cx0, cx1, cy0, cy1);
   if (!why.empty ())
     return "core: " + why;
   if (!ctx->core_stream)
@@ -1115,7 +1124,8 @@ int plan_sweep (fdtd_ctx *ctx)
       }
       else
       {
-        ctx->tb2_why = sweep2_plan (ctx->tb2, ctx->fused, e, h, aux, ctx->mat32[0], ctx->sm_count, 64, ctx->tb2_ctr);
+        ctx->tb2_why = sweep2_plan (ctx->tb2, ctx->fused, e, h, aux, ctx->mat32[0], ctx->sm_count, tb2_chunk (),
+                                     ctx->tb2_ctr);
         if (ctx->tb2_why.empty ())
           ctx->tb2_state = 1;
       }

@@ -20,7 +20,11 @@ namespace fdtdb {
 constexpr int kTb2Warps = 16;
 constexpr int kTb2Zw = 64;
 constexpr int kTb2Yown = 13;
-constexpr int kTb2MaxChunk = 64;   // x planes per item at most
+constexpr int kTb2MaxChunk = 256;  // x planes per item at most
+// x planes per item by default: each item pays a four-plane pipeline fill,
+// so longer items do less redundant work while a 512^3 grid still gives
+// every SM several items
+constexpr int kTb2Chunk = 128;
 
 struct Sweep2Maps
 {

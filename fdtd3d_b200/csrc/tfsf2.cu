@@ -60,8 +60,8 @@ __device__ __forceinline__ void stf<__half> (__half *p, size_t i, float v)
 // term whose box holds the cell subtracts the incident value from one
 // neighbour of the curl (n1 - n0) - (n3 - n2), as the single-step kernels'
 // tfsf_curl does.
-__device__ __noinline__ float term_value (const FusedParams &p, int k, int t, const double *inc, int *err, int x,
-                                         int y, int z)
+__device__ __forceinline__ float term_value (const FusedParams &p, int k, int t, const double *inc, int *err, int x,
+                                            int y, int z)
 {
   const TermDev &tm = p.comp[k].term[t];
   const double diff = inc_at (p.g, inc, p.inc_len, err, tm.inc_comp, x + tm.aux[0], y + tm.aux[1], z + tm.aux[2]);
@@ -192,8 +192,11 @@ __global__ void __launch_bounds__ (256, 4) tfsf2_fused (const __grid_constant__ 
   // the TF/SF terms of the family kb .. kb + 2 (E: 0, H: 3) over the cells
   // of the local domain d0 .. d1 - 1: for each cell of a term's box,
   // add (k - kb, cell, term value).  Pass j takes every component's j-th
-  // term (the components write their own arrays); the CTA synchronises
-  // after each pass (two terms of a component may share a cell).
+  // term (the components write their own arrays, so a pass adds to a cell
+  // of an array at most once); the CTA synchronises after each pass (two
+  // terms of a component may share a cell).  The cells of a pass's boxes
+  // form one index range strided over the threads, two cells an iteration,
+  // so that the incident-grid loads of both are in flight at once.
   auto terms = [&] (int kb, const double *inc, int d0, const int d1[3], auto &&add) {
     unsigned mk[3];
     int passes = 0;
@@ -206,29 +209,71 @@ __global__ void __launch_bounds__ (256, 4) tfsf2_fused (const __grid_constant__ 
 #pragma unroll 1
     for (int j = 0; j < passes; ++j)
     {
+      // component c's box: cells bl[c] + (0 .. bX, 0 .. bY[c], 0 .. bZ[c]), n[c] of them
+      int n[3], tt[3], bl[3][3], bY[3], bZ[3];
+      float rY[3], rZ[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
       {
+        n[c] = 0;
+        tt[c] = 0;
+        bY[c] = 1;
+        bZ[c] = 1;
+        rY[c] = 1.f;
+        rZ[c] = 1.f;
+        bl[c][0] = bl[c][1] = bl[c][2] = 0;
         if (!mk[c])
           continue;
-        const int tt = __ffs (mk[c]) - 1;
+        tt[c] = __ffs (mk[c]) - 1;
         mk[c] &= mk[c] - 1;
-        const TermDev &tm = p.comp[kb + c].term[tt];
-        int b0[3], b1[3];
+        const TermDev &tm = p.comp[kb + c].term[tt[c]];
+        int ext[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a)
         {
-          b0[a] = max (tm.lo[a] - o[a], d0);
-          b1[a] = min (tm.hi[a] - o[a], d1[a]);
+          bl[c][a] = max (tm.lo[a] - o[a], d0);
+          ext[a] = min (tm.hi[a] - o[a], d1[a]) - bl[c][a];
         }
-        if (b0[0] >= b1[0] || b0[1] >= b1[1] || b0[2] >= b1[2])
-          continue;
-        const int bY = b1[1] - b0[1], bZ = b1[2] - b0[2], nb = (b1[0] - b0[0]) * bY * bZ;
-        for (Walk w (bY, bZ); w.q < nb; w.next ())
+        if (ext[0] > 0 && ext[1] > 0 && ext[2] > 0)
         {
-          const int qx = b0[0] + w.x, qy = b0[1] + w.y, qz = b0[2] + w.z;
-          add (c, qx, qy, qz, term_value (p, kb + c, tt, inc, err, o[0] + qx, o[1] + qy, o[2] + qz));
+          n[c] = ext[0] * ext[1] * ext[2];
+          bY[c] = ext[1];
+          bZ[c] = ext[2];
+          rY[c] = __frcp_rn ((float) ext[1]);
+          rZ[c] = __frcp_rn ((float) ext[2]);
         }
+      }
+      const int n01 = n[0] + n[1], N = n01 + n[2];
+      if (N == 0)
+        continue;   // nothing written: no barrier needed
+      // flat index f of the pass -> component c and local cell
+      auto cell = [&] (int f, int &c, int &qx, int &qy, int &qz) {
+        const bool a0 = f < n[0], a1 = f < n01;
+        c = a0 ? 0 : (a1 ? 1 : 2);
+        const int l = f - (a0 ? 0 : (a1 ? n[0] : n01));
+        const int Y = a0 ? bY[0] : (a1 ? bY[1] : bY[2]), Z = a0 ? bZ[0] : (a1 ? bZ[1] : bZ[2]);
+        const int q = small_div (l, Z, a0 ? rZ[0] : (a1 ? rZ[1] : rZ[2]));
+        const int x = small_div (q, Y, a0 ? rY[0] : (a1 ? rY[1] : rY[2]));
+        qx = x + (a0 ? bl[0][0] : (a1 ? bl[1][0] : bl[2][0]));
+        qy = q - x * Y + (a0 ? bl[0][1] : (a1 ? bl[1][1] : bl[2][1]));
+        qz = l - q * Z + (a0 ? bl[0][2] : (a1 ? bl[1][2] : bl[2][2]));
+      };
+      const int s = blockDim.x;
+      for (int f = threadIdx.x; f < N; f += 2 * s)
+      {
+        // the second cell (f + s) is evaluated even past the range (as the
+        // first again) so that both evaluations are straight-line code
+        const bool two = f + s < N;
+        int c0, x0, y0, z0, c1, x1, y1, z1;
+        cell (f, c0, x0, y0, z0);
+        cell (two ? f + s : f, c1, x1, y1, z1);
+        const int t0 = c0 == 0 ? tt[0] : (c0 == 1 ? tt[1] : tt[2]);
+        const int t1 = c1 == 0 ? tt[0] : (c1 == 1 ? tt[1] : tt[2]);
+        const float v0 = term_value (p, kb + c0, t0, inc, err, o[0] + x0, o[1] + y0, o[2] + z0);
+        const float v1 = term_value (p, kb + c1, t1, inc, err, o[0] + x1, o[1] + y1, o[2] + z1);
+        add (c0, x0, y0, z0, v0);
+        if (two)
+          add (c1, x1, y1, z1, v1);
       }
       __syncthreads ();
     }

@@ -21,8 +21,14 @@ pytestmark = pytest.mark.gpu
 COMPS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
 
 
-def _run(fdtd, monkeypatch, kw, steps, fields, eps, tb2):
+def _run(fdtd, monkeypatch, kw, steps, fields, eps, tb2, chunk=None):
     monkeypatch.setenv("FDTDB_TB2", "1" if tb2 else "0")
+    # the two-step kernel's x chunk (default 128 planes): short chunks put
+    # chunk seams into these small grids
+    if chunk:
+        monkeypatch.setenv("FDTDB_TB2_CHUNK", str(chunk))
+    else:
+        monkeypatch.delenv("FDTDB_TB2_CHUNK", raising=False)
     mats = {"eps": eps} if eps is not None else None
     with fdtd.Simulation(materials=mats, **kw) as sim:
         for c, a in fields.items():
@@ -45,12 +51,13 @@ def _inputs(shape, seed, with_eps=True):
 
 
 CASES = {
-    # 3 z tiles (the last partial), 5 y tiles (the last partial), 2 x chunks
-    "tiles": dict(size=(70, 58, 132), steps=9, eps=True),
+    # 3 z tiles (the last partial), 5 y tiles (the last partial), 3 x chunks
+    "tiles": dict(size=(70, 58, 132), steps=9, eps=True, chunk=32),
     # an odd number of updates (the last a single step), uniform permittivity,
     # one partial z tile
     "odd_uniform": dict(size=(23, 19, 40), steps=8, eps=False),
-    # nz just past one tile's own cells and a long x extent (several chunks)
+    # nz just past one tile's own cells and a long x extent (two chunks of
+    # the default length)
     "long_x": dict(size=(150, 16, 64), steps=7, eps=True),
 }
 
@@ -61,7 +68,7 @@ def test_fp32_pairs_equal_single_steps(fdtd, monkeypatch, case):
     shape = spec["size"]
     fields, eps = _inputs(shape, 3 + len(case), spec["eps"])
     kw = dict(mode=3, size=shape, precision=fdtd.PREC_FP32)
-    got, k2 = _run(fdtd, monkeypatch, kw, spec["steps"], fields, eps, True)
+    got, k2 = _run(fdtd, monkeypatch, kw, spec["steps"], fields, eps, True, spec.get("chunk"))
     ref, k1 = _run(fdtd, monkeypatch, kw, spec["steps"], fields, eps, False)
     assert k1 == "sweep3d_tma"
     # steps from t = 0 update the fields steps - 1 times (none at t = 0); an
@@ -117,7 +124,7 @@ PML_CASES = {
     "pml_thick_z": dict(size=(40, 30, 120), pml=(3, 3, 16), steps=8),
     # a core of several two-step tiles and x chunks inside a PML shell of
     # several single-step tiles on every side
-    "pml_large_core": dict(size=(150, 96, 200), pml=(10, 9, 12), steps=9),
+    "pml_large_core": dict(size=(150, 96, 200), pml=(10, 9, 12), steps=9, chunk=40),
 }
 
 
@@ -134,7 +141,7 @@ def test_fp32_pairs_with_pml_match_single_steps(fdtd, monkeypatch, case):
     shape = spec["size"]
     fields, eps = _inputs(shape, 17 + len(case))
     kw = dict(mode=3, size=shape, use_pml=True, pml=spec["pml"], precision=fdtd.PREC_FP32)
-    got, k2 = _run(fdtd, monkeypatch, kw, spec["steps"], fields, eps, True)
+    got, k2 = _run(fdtd, monkeypatch, kw, spec["steps"], fields, eps, True, spec.get("chunk"))
     ref, k1 = _run(fdtd, monkeypatch, kw, spec["steps"], fields, eps, False)
     assert k1 == "sweep3d_tma"
     assert k2 == ("sweep3d_tma" if (spec["steps"] - 1) % 2 else "sweep2_tma")
