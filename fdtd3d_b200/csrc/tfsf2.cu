@@ -55,18 +55,23 @@ __device__ __forceinline__ void stf<__half> (__half *p, size_t i, float v)
   p[i] = __float2half_rn (v);
 }
 
-// TF/SF change of the curl of component k at (x, y, z) over the terms of
-// `mask` (bit t: term t of component k; those that reach the tile): each
-// term whose box holds the cell subtracts the incident value from one
-// neighbour of the curl (n1 - n0) - (n3 - n2), as the single-step kernels'
+// TF/SF change of the curl of a component at a cell from one of its terms:
+// the incident value at distance d along the wave (linear interpolation of
+// the 1-D incident grid, as inc_at), times pp (the incident component's
+// projection and the term's sign, in FP64), rounded to float and times ss
+// (the component's incident scale and the sign of the curl neighbour the
+// term modifies, (n1 - n0) - (n3 - n2)), as the single-step kernels'
 // tfsf_curl does.
-__device__ __forceinline__ float term_value (const FusedParams &p, int k, int t, const double *inc, int *err, int x,
-                                            int y, int z)
+__device__ __forceinline__ float term_at (const double *inc, int inc_len, int *err, double d, double pp, float ss)
 {
-  const TermDev &tm = p.comp[k].term[t];
-  const double diff = inc_at (p.g, inc, p.inc_len, err, tm.inc_comp, x + tm.aux[0], y + tm.aux[1], z + tm.aux[2]);
-  const float dv = (float) (diff * tm.negate) * p.inc_scale[tm.inc_comp];
-  return (tm.slot == 0 || tm.slot == 3) ? dv : -dv;
+  const int i1 = (int) d;
+  const double pr2 = d - (double) i1;
+  if (i1 < 0 || i1 + 1 >= inc_len)
+  {
+    *err = 1;
+    return 0.f;
+  }
+  return (float) ((inc[i1] * (1 - pr2) + inc[i1 + 1] * pr2) * pp) * ss;
 }
 
 // q / d for 0 <= q < 2^22 and 1 <= d < 2^11 (rd = 1 / d rounded): the
@@ -143,6 +148,28 @@ __global__ void __launch_bounds__ (256, 4) tfsf2_fused (const __grid_constant__ 
   const float S = p.courant;
   const int o[3] = {t.lo[0] - 1, t.lo[1] - 1, t.lo[2] - 1};   // origin of every domain
   const bool has_eps = p.eps != nullptr;
+  // term (k, t) of the tile, entry 4 k + t: the incident distance at local
+  // cell q is d = A qx + B qy + C qz + tD (tD folds the tile origin, the
+  // term's neighbour offset, the incident component's position and the half
+  // cell of the H components), its value term_at (.., d, tP, tS)
+  __shared__ double tD[24], tP[24];
+  __shared__ float tS[24];
+  const double A = p.g.s1 * p.g.c2, B = p.g.s1 * p.g.s2, C = p.g.c1;
+  if (threadIdx.x < 24)
+  {
+    const int k = threadIdx.x >> 2, tt = threadIdx.x & 3;
+    if (tt < p.comp[k].nterms)
+    {
+      const TermDev &tm = p.comp[k].term[tt];
+      const int ic = tm.inc_comp;
+      const double x0 = ((double) (o[0] + tm.aux[0]) + p.g.min_fp[ic][0]) - p.g.zero_inc[0];
+      const double y0 = ((double) (o[1] + tm.aux[1]) + p.g.min_fp[ic][1]) - p.g.zero_inc[1];
+      const double z0 = ((double) (o[2] + tm.aux[2]) + p.g.min_fp[ic][2]) - p.g.zero_inc[2];
+      tD[threadIdx.x] = A * x0 + B * y0 + C * z0 - (ic >= 3 ? 0.5 : 0.0);
+      tP[threadIdx.x] = p.g.proj[ic] * tm.negate;
+      tS[threadIdx.x] = (tm.slot == 0 || tm.slot == 3) ? p.inc_scale[ic] : -p.inc_scale[ic];
+    }
+  }
 
   // zero corrections (both arrays: 3 (nE + nH) floats, sE 16-byte aligned)
   {
@@ -267,10 +294,12 @@ __global__ void __launch_bounds__ (256, 4) tfsf2_fused (const __grid_constant__ 
         int c0, x0, y0, z0, c1, x1, y1, z1;
         cell (f, c0, x0, y0, z0);
         cell (two ? f + s : f, c1, x1, y1, z1);
-        const int t0 = c0 == 0 ? tt[0] : (c0 == 1 ? tt[1] : tt[2]);
-        const int t1 = c1 == 0 ? tt[0] : (c1 == 1 ? tt[1] : tt[2]);
-        const float v0 = term_value (p, kb + c0, t0, inc, err, o[0] + x0, o[1] + y0, o[2] + z0);
-        const float v1 = term_value (p, kb + c1, t1, inc, err, o[0] + x1, o[1] + y1, o[2] + z1);
+        const int e0 = 4 * (kb + c0) + (c0 == 0 ? tt[0] : (c0 == 1 ? tt[1] : tt[2]));
+        const int e1 = 4 * (kb + c1) + (c1 == 0 ? tt[0] : (c1 == 1 ? tt[1] : tt[2]));
+        const double d0 = fma (A, (double) x0, fma (B, (double) y0, fma (C, (double) z0, tD[e0])));
+        const double d1 = fma (A, (double) x1, fma (B, (double) y1, fma (C, (double) z1, tD[e1])));
+        const float v0 = term_at (inc, p.inc_len, err, d0, tP[e0], tS[e0]);
+        const float v1 = term_at (inc, p.inc_len, err, d1, tP[e1], tS[e1]);
         add (c0, x0, y0, z0, v0);
         if (two)
           add (c1, x1, y1, z1, v1);
