@@ -1552,10 +1552,16 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
           ctx->launches += launch_sweep3d (ctx->shell1, o, f1, ctx->d_err, s, ctx->sweep_streams);
           ctx->launches += launch_sweep2 (ctx->tb2, o, f, ctx->d_err, ctx->core_stream);
           ctx->launches += launch_sweep3d (ctx->shell2, 0, f, ctx->d_err, s, ctx->sweep_streams);
+          // the TF/SF corrections touch only core cells two cells clear of
+          // the shell (plan_tfsf2) and read the incident levels issued on s
+          // before the fork: they follow the core on its stream, beside the
+          // shell's second step
+          if (g.cfg.use_tfsf)
+            ctx->launches += launch_tfsf2 (ctx->tf2, f, inc_h1, inc_e1, inc_h2, inc_e2, ctx->d_err, ctx->core_stream);
           CK (cudaEventRecord (ctx->core_join, ctx->core_stream));
           CK (cudaStreamWaitEvent (s, ctx->core_join, 0));
         }
-        if (g.cfg.use_tfsf)
+        if (g.cfg.use_tfsf && ctx->tb2_state == 1)
           ctx->launches += launch_tfsf2 (ctx->tf2, f, inc_h1, inc_e1, inc_h2, inc_e2, ctx->d_err, s);
         ctx->step_kernel = "sweep2_tma";
         if ((r = prof_end (ctx, pe)) != FDTD_OK)
