@@ -150,6 +150,9 @@ struct fdtd_ctx
   float *tauxb[6] = {};                   // set T: PML auxiliaries
   cudaStream_t core_stream = nullptr;
   cudaEvent_t core_fork = nullptr, core_join = nullptr;
+  // incident-grid steps of a pair beside the shell and the core
+  cudaStream_t inc_stream = nullptr;
+  cudaEvent_t inc_free = nullptr, inc_done = nullptr;
   // TF/SF with the two-step scheme: the pair's corrections (tfsf2.cu), and a
   // copy of the incident H level the first step's E corrections read (the
   // second step's H-incident update overwrites it)
@@ -1253,7 +1256,12 @@ void release (fdtd_ctx *ctx)
     cudaStreamSynchronize (ctx->core_stream);
     cudaStreamDestroy (ctx->core_stream);
   }
-  for (cudaEvent_t e : {ctx->core_fork, ctx->core_join})
+  if (ctx->inc_stream)
+  {
+    cudaStreamSynchronize (ctx->inc_stream);
+    cudaStreamDestroy (ctx->inc_stream);
+  }
+  for (cudaEvent_t e : {ctx->core_fork, ctx->core_join, ctx->inc_free, ctx->inc_done})
     if (e)
       cudaEventDestroy (e);
   for (cudaEvent_t e : {ctx->sweep_streams.fork, ctx->sweep_streams.join[0], ctx->sweep_streams.join[1]})
@@ -1342,6 +1350,17 @@ PlainHalf plain_half (fdtd_ctx *ctx, int h)
       p.sigc[ci][a] = ctx->sigc64[k][a] ? ctx->sigc64[k][a] : p.sigma[a];
   }
   return p;
+}
+
+// The side stream of a pair's incident-grid steps and its two events.
+int ensure_inc_stream (fdtd_ctx *ctx)
+{
+  if (ctx->inc_stream)
+    return FDTD_OK;
+  CK (cudaStreamCreateWithFlags (&ctx->inc_stream, cudaStreamNonBlocking));
+  CK (cudaEventCreateWithFlags (&ctx->inc_free, cudaEventDisableTiming));
+  CK (cudaEventCreateWithFlags (&ctx->inc_done, cudaEventDisableTiming));
+  return FDTD_OK;
 }
 
 int prof_begin (fdtd_ctx *ctx, cudaEvent_t *end_out)
@@ -1470,15 +1489,6 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
     {
       // incident E then H steps, then one sweep for both field families
       int hprev = ctx->hcur;
-      if (g.cfg.use_tfsf)
-      {
-        ctx->launches += launch_incident_e (ctx->einc[1 - ctx->ecur], ctx->einc[ctx->ecur], ctx->hinc[ctx->hcur],
-                                            g.inc_len, g.mod_e, ctx->d_src, kSrcStride * i, s);
-        ctx->ecur ^= 1;
-        ctx->launches += launch_incident_h (ctx->hinc[1 - ctx->hcur], ctx->hinc[ctx->hcur], ctx->einc[ctx->ecur],
-                                            g.inc_len, g.mod_h, s);
-        ctx->hcur ^= 1;
-      }
       FusedParams &f = ctx->fused;
       int o = ctx->fcur, nw = 1 - ctx->fcur;
       for (int c = 0; c < 3; ++c)
@@ -1500,15 +1510,39 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
         f.zpp_new[k] = ctx->zppb[nw][k];
       }
       f.eps = ctx->mat32[0];
-      f.inc_h = ctx->hinc[hprev];
-      f.inc_e = ctx->einc[ctx->ecur];
       f.src = ctx->d_src;
       f.src_index = kSrcStride * i + 1;
       if (ctx->sweep_state == 0 || (ctx->sweep_state == 1 && ctx->sweep_eps != ctx->mat32[0]))
         if ((r = plan_sweep (ctx)) != FDTD_OK)
           return r;
+      const bool pair = ctx->tb2_state >= 1 && i + (ctx->keep_prev ? 2 : 1) < n && ctx->dft_comp < 0 && !has_cs;
+      // On the two-step path with a PML shell only the pair's TF/SF kernel
+      // reads the incident grid: its steps run on a stream of their own
+      // beside the shell and the core, after every earlier reader (all on s
+      // or joined into s), and the TF/SF kernel waits for them
+      const bool inc_side = pair && ctx->tb2_state == 2 && g.cfg.use_tfsf;
+      cudaStream_t si = s;
+      if (inc_side)
+      {
+        if ((r = ensure_inc_stream (ctx)) != FDTD_OK)
+          return r;
+        si = ctx->inc_stream;
+        CK (cudaEventRecord (ctx->inc_free, s));
+        CK (cudaStreamWaitEvent (si, ctx->inc_free, 0));
+      }
+      if (g.cfg.use_tfsf)
+      {
+        ctx->launches += launch_incident_e (ctx->einc[1 - ctx->ecur], ctx->einc[ctx->ecur], ctx->hinc[ctx->hcur],
+                                            g.inc_len, g.mod_e, ctx->d_src, kSrcStride * i, si);
+        ctx->ecur ^= 1;
+        ctx->launches += launch_incident_h (ctx->hinc[1 - ctx->hcur], ctx->hinc[ctx->hcur], ctx->einc[ctx->ecur],
+                                            g.inc_len, g.mod_h, si);
+        ctx->hcur ^= 1;
+      }
+      f.inc_h = ctx->hinc[hprev];
+      f.inc_e = ctx->einc[ctx->ecur];
       cudaEvent_t pe;
-      if (ctx->tb2_state >= 1 && i + (ctx->keep_prev ? 2 : 1) < n && ctx->dft_comp < 0 && !has_cs)
+      if (pair)
       {
         // steps t and t + 1 in one pass (no point source or Drude medium).
         // With TF/SF the incident grid takes both steps first (this step's
@@ -1518,17 +1552,19 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
         if (g.cfg.use_tfsf)
         {
           CK (cudaMemcpyAsync (ctx->hinc_keep, ctx->hinc[hprev], (size_t) g.inc_len * sizeof (double),
-                               cudaMemcpyDeviceToDevice, s));
+                               cudaMemcpyDeviceToDevice, si));
           inc_h1 = ctx->hinc_keep;
           inc_e1 = ctx->einc[ctx->ecur];
           inc_h2 = ctx->hinc[ctx->hcur];
           ctx->launches += launch_incident_e (ctx->einc[1 - ctx->ecur], ctx->einc[ctx->ecur], ctx->hinc[ctx->hcur],
-                                              g.inc_len, g.mod_e, ctx->d_src, kSrcStride * (i + 1), s);
+                                              g.inc_len, g.mod_e, ctx->d_src, kSrcStride * (i + 1), si);
           ctx->ecur ^= 1;
           inc_e2 = ctx->einc[ctx->ecur];
           ctx->launches += launch_incident_h (ctx->hinc[1 - ctx->hcur], ctx->hinc[ctx->hcur], ctx->einc[ctx->ecur],
-                                              g.inc_len, g.mod_h, s);
+                                              g.inc_len, g.mod_h, si);
           ctx->hcur ^= 1;
+          if (inc_side)
+            CK (cudaEventRecord (ctx->inc_done, si));
         }
         if ((r = prof_begin (ctx, &pe)) != FDTD_OK)
           return r;
@@ -1553,11 +1589,14 @@ int step_impl (fdtd_ctx *ctx, uint32_t t_start, uint32_t n)
           ctx->launches += launch_sweep2 (ctx->tb2, o, f, ctx->d_err, ctx->core_stream);
           ctx->launches += launch_sweep3d (ctx->shell2, 0, f, ctx->d_err, s, ctx->sweep_streams);
           // the TF/SF corrections touch only core cells two cells clear of
-          // the shell (plan_tfsf2) and read the incident levels issued on s
-          // before the fork: they follow the core on its stream, beside the
-          // shell's second step
+          // the shell (plan_tfsf2): they follow the core on its stream,
+          // beside the shell's second step, once the incident levels they
+          // read are in place
           if (g.cfg.use_tfsf)
+          {
+            CK (cudaStreamWaitEvent (ctx->core_stream, ctx->inc_done, 0));
             ctx->launches += launch_tfsf2 (ctx->tf2, f, inc_h1, inc_e1, inc_h2, inc_e2, ctx->d_err, ctx->core_stream);
+          }
           CK (cudaEventRecord (ctx->core_join, ctx->core_stream));
           CK (cudaStreamWaitEvent (s, ctx->core_join, 0));
         }
