@@ -15,6 +15,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include "cell_walk.cuh"
 #include "kernels.h"
 
 namespace fdtdb {
@@ -233,14 +234,11 @@ __global__ void __launch_bounds__ (256) fast_half_kernel (FastHalf p, int *err)
   const int ix = (p.g.drop & 1) ? 1 : p.g.n[0] - 2;
   const int iy = (p.g.drop & 2) ? 1 : p.g.n[1] - 2;
   const int iz = (p.g.drop & 4) ? 1 : p.g.n[2] - 2;
-  const int64_t total = (int64_t) ix * iy * iz;
-  for (int64_t tid = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; tid < total;
-       tid += (int64_t) gridDim.x * blockDim.x)
+  const int oz = (p.g.drop & 4) ? 0 : 1, oy = (p.g.drop & 2) ? 0 : 1, ox = (p.g.drop & 1) ? 0 : 1;
+  for (CellWalk w ((int64_t) blockIdx.x * blockDim.x + threadIdx.x, (int64_t) gridDim.x * blockDim.x, ix, iy, iz);
+       w.ok (); w.next ())
   {
-    const int z = (int) (tid % iz) + ((p.g.drop & 4) ? 0 : 1);
-    const int64_t r = tid / iz;
-    const int y = (int) (r % iy) + ((p.g.drop & 2) ? 0 : 1);
-    const int x = (int) (r / iy) + ((p.g.drop & 1) ? 0 : 1);
+    const int z = w.cz + oz, y = w.cy + oy, x = w.cx + ox;
 #pragma unroll 1
     for (int ci = 0; ci < 3; ++ci)
     {

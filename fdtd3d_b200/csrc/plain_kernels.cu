@@ -15,6 +15,7 @@
 //   (YeeGridLayout.h:866-1030, Approximation.cpp:34-54), once per upload.
 #include <cuda_runtime.h>
 
+#include "cell_walk.cuh"
 #include "kernels.h"
 #include "plain_cell.cuh"
 
@@ -169,13 +170,10 @@ __global__ void __launch_bounds__ (256) plain_fast_kernel (const __grid_constant
   const int ix = (g.drop & 1) ? 1 : g.n[0] - 2;
   const int iy = (g.drop & 2) ? 1 : g.n[1] - 2;
   const int iz = (g.drop & 4) ? 1 : g.n[2] - 2;
-  const int64_t total = (int64_t) ix * iy * iz;
-  for (int64_t tid = cblock * blockDim.x + threadIdx.x; tid < total; tid += cgrid * blockDim.x)
+  const int oz = (g.drop & 4) ? 0 : 1, oy = (g.drop & 2) ? 0 : 1, ox = (g.drop & 1) ? 0 : 1;
+  for (CellWalk w (cblock * blockDim.x + threadIdx.x, cgrid * blockDim.x, ix, iy, iz); w.ok (); w.next ())
   {
-    const int z = (int) (tid % iz) + ((g.drop & 4) ? 0 : 1);
-    const int64_t r = tid / iz;
-    const int y = (int) (r % iy) + ((g.drop & 2) ? 0 : 1);
-    const int x = (int) (r / iy) + ((g.drop & 1) ? 0 : 1);
+    const int z = w.cz + oz, y = w.cy + oy, x = w.cx + ox;
     const int64_t id = x * sx + y * sy + z;
     const int pos[3] = {x, y, z};
     double val = g1[id];
